@@ -1,0 +1,201 @@
+"""Seeded scene builders: the reference's demo recipes that the solver
+configurations are derived from (Sources/PhysicsAVBD/Demos/*.swift) and the
+synthetic benchmark scenes built on them.
+
+Randomness comes from SplitMix64 (Sources/SimCore/Math/Random.swift), so a
+(recipe, seed) pair always produces the same scene.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import abi
+from .scene import PhysicsScene, SceneJoint, SceneSpring, SceneTet
+
+f32 = np.float32
+MASK64 = (1 << 64) - 1
+
+
+class SplitMix64:
+    """SplitMix64 (Random.swift:3-21)."""
+
+    def __init__(self, seed: int):
+        self.state = seed & MASK64
+
+    def next(self) -> int:
+        self.state = (self.state + 0x9E3779B97F4A7C15) & MASK64
+        z = self.state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK64
+        return z ^ (z >> 31)
+
+    def next_float(self) -> float:
+        """Uniform in [0, 1) with 24 random bits (Random.swift:17-20)."""
+        return float(f32(self.next() >> 40) / f32(1 << 24))
+
+    def uniform(self, lo: float, hi: float) -> float:
+        return lo + (hi - lo) * self.next_float()
+
+    def normal(self) -> float:
+        """Standard normal by Box-Muller over two draws."""
+        u1 = max(self.next_float(), 1.0 / (1 << 24))
+        u2 = self.next_float()
+        return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
+
+
+def add_ground(s: PhysicsScene, friction: float = 0.7) -> int:
+    """Demos.addGround (Demos.swift:191-196): static 200x200x2 box at z=-1."""
+    return s.add_body((200, 200, 2), 0.0, friction, (0, 0, -1))
+
+
+def stack(height: int) -> PhysicsScene:
+    """Demos.stack (Demos.swift:214-222)."""
+    s = PhysicsScene("stack")
+    add_ground(s)
+    for i in range(height):
+        s.add_body((1, 1, 1), 1.0, 0.7, (0, 0, 0.5 + i))
+    return s
+
+
+def add_soft_block(s: PhysicsScene, center, nx: int, ny: int, nz: int, spacing: float,
+                   mu: float = 3000, lam: float = 30000, mass_per_node: float = 0.05,
+                   friction: float = 0.8, self_collision: bool = False,
+                   jitter=None, exclusion_joints: bool = True):
+    """Demos.addSoftBlock (Demos5.swift:76-145): particle lattice, 5 tets per
+    cell (parity-alternated), inert lattice-neighbour exclusion joints.
+
+    `jitter(i, j, k) -> (dx, dy, dz)` optionally perturbs the spawn pose (and
+    therefore the rest shape) of each node."""
+    sp = f32(spacing)
+    half = np.array([nx - 1, ny - 1, nz - 1], dtype=np.float32) * sp / f32(2)
+    c = np.array(center, dtype=np.float32)
+    ids = np.full((nx, ny, nz), -1, dtype=np.int64)
+    flat = []
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nz):
+                p = c + np.array([i, j, k], dtype=np.float32) * sp - half
+                if jitter is not None:
+                    p = p + np.array(jitter(i, j, k), dtype=np.float32)
+                b = s.add_particle(float(sp * f32(0.32)), mass_per_node, friction, tuple(p))
+                ids[i, j, k] = b
+                flat.append(b)
+
+    def tet(a, b, c_, d):
+        s.add_tet(SceneTet((int(a), int(b), int(c_), int(d)), mu, lam, self_collision))
+
+    for i in range(nx - 1):
+        for j in range(ny - 1):
+            for k in range(nz - 1):
+                c000, c100 = ids[i, j, k], ids[i + 1, j, k]
+                c010, c110 = ids[i, j + 1, k], ids[i + 1, j + 1, k]
+                c001, c101 = ids[i, j, k + 1], ids[i + 1, j, k + 1]
+                c011, c111 = ids[i, j + 1, k + 1], ids[i + 1, j + 1, k + 1]
+                if (i + j + k) % 2 == 0:
+                    tet(c000, c100, c010, c001)
+                    tet(c110, c100, c010, c111)
+                    tet(c101, c100, c001, c111)
+                    tet(c011, c010, c001, c111)
+                    tet(c100, c010, c001, c111)
+                else:
+                    tet(c100, c000, c110, c101)
+                    tet(c010, c000, c110, c011)
+                    tet(c001, c000, c101, c011)
+                    tet(c111, c110, c101, c011)
+                    tet(c000, c110, c101, c011)
+    if exclusion_joints:
+        offs = [(1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (1, 0, 1), (0, 1, 1), (1, 1, 1)]
+        for i in range(nx):
+            for j in range(ny):
+                for k in range(nz):
+                    a = int(ids[i, j, k])
+                    for di, dj, dk in offs:
+                        if i + di < nx and j + dj < ny and k + dk < nz:
+                            s.add_joint(SceneJoint(a, int(ids[i + di, j + dj, k + dk]),
+                                                   (0, 0, 0), (0, 0, 0), 0.0, 0.0))
+    return flat
+
+
+# ---------------------------------------------------------------------------
+# Synthetic benchmark scenes (one per solver configuration)
+# ---------------------------------------------------------------------------
+
+def rigid_stack_scene(seed: int = 1, count: int = 20) -> PhysicsScene:
+    """Rigid stack: `count` unit cubes (density 1000) with 1e-3 m gaps on a
+    static ground, friction 0.5, lateral jitter U(+-1e-3) from the seed;
+    dt 1/60, 10 iterations, beta 1e5, alpha 0.95, gamma 0.99, g = -9.81."""
+    rng = SplitMix64(seed)
+    s = PhysicsScene("rigid-stack")
+    add_ground(s, friction=0.5)
+    for i in range(count):
+        jx = rng.uniform(-1e-3, 1e-3)
+        jy = rng.uniform(-1e-3, 1e-3)
+        s.add_body((1, 1, 1), 1000.0, 0.5, (jx, jy, 0.5 + i * (1.0 + 1e-3)))
+    st = s.settings
+    st.dt, st.gravity, st.iterations = 1.0 / 60.0, -9.81, 10
+    st.beta_lin, st.alpha, st.gamma = 1.0e5, 0.95, 0.99
+    return s
+
+
+def soft_cube_scene(seed: int = 2, n: int = 24, iterations: int = 20,
+                    exclusion_joints: bool = True) -> PhysicsScene:
+    """Soft cube: n^3-vertex lattice of a 1 m cube, 5 tets per cell, Stable
+    Neo-Hookean E=1e5 Pa, nu=0.4, density 1000 (lumped node mass), dropped
+    from 0.5 m onto the ground, friction 0.4, dt 1/60, static palette; rest
+    positions perturbed by N(0, 1e-4 m) from the seed."""
+    rng = SplitMix64(seed)
+    E, nu, rho = 1.0e5, 0.4, 1000.0
+    mu = E / (2.0 * (1.0 + nu))
+    lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+    spacing = 1.0 / (n - 1)
+    s = PhysicsScene("soft-cube")
+    add_ground(s, friction=0.4)
+    noise = {}
+
+    def jitter(i, j, k):
+        v = (rng.normal() * 1e-4, rng.normal() * 1e-4, rng.normal() * 1e-4)
+        noise[(i, j, k)] = v
+        return v
+
+    add_soft_block(s, (0.0, 0.0, 1.0), n, n, n, spacing, mu=mu, lam=lam,
+                   mass_per_node=rho * 1.0 / (n ** 3), friction=0.4, jitter=jitter,
+                   exclusion_joints=exclusion_joints)
+    st = s.settings
+    st.dt, st.gravity, st.iterations = 1.0 / 60.0, -9.81, iterations
+    return s
+
+
+def single_tet_scene() -> PhysicsScene:
+    """SoftBodyTests.testTetVolumePreservation (SoftBodyTests.swift:53-69)."""
+    s = PhysicsScene("tet1")
+    s.settings.iterations = 20
+    p0 = s.add_particle(0.05, 0.1, position=(0, 0, 3))
+    p1 = s.add_particle(0.05, 0.1, position=(0.5, 0, 3))
+    p2 = s.add_particle(0.05, 0.1, position=(0, 0.5, 3))
+    p3 = s.add_particle(0.05, 0.1, position=(0, 0, 3.5))
+    s.add_joint(SceneJoint(-1, p0, (0, 0, 3), (0, 0, 0)))
+    s.add_tet(SceneTet((p0, p1, p2, p3), 2000, 20000))
+    return s
+
+
+def particle_rod_chain_scene() -> PhysicsScene:
+    """SoftBodyTests.testParticleRodChainInextensible (SoftBodyTests.swift:27-51)."""
+    s = PhysicsScene("pc")
+    s.settings.iterations = 20
+    prev = -1
+    for k in range(12):
+        p = s.add_particle(0.05, 0.02, position=(k * 0.25, 0, 4))
+        if k == 0:
+            s.add_joint(SceneJoint(-1, p, (0, 0, 4), (0, 0, 0)))
+        else:
+            s.add_spring(SceneSpring(prev, p, (0, 0, 0), (0, 0, 0), 1e5, hard=True))
+        prev = p
+    return s
+
+
+SCENES = {
+    "rigid-stack": rigid_stack_scene,
+    "soft-cube": soft_cube_scene,
+}

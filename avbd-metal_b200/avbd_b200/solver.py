@@ -1,0 +1,229 @@
+"""`GPUSolver`: the Python host mirror of the reference's solver class
+(Sources/PhysicsAVBD/GPU/GPUSolver.swift:17) over the C ABI of include/avbd.h.
+
+The CUDA library is required: there is no CPU fallback.  Errors follow the
+reference's convention — construction errors raise `AVBDError`, runtime
+failures raise `RuntimeFailure` and are sticky (every later call raises).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+from .scene import PhysicsScene, SimSettings
+
+_LIB = None
+
+
+class AVBDError(RuntimeError):
+    """Construction error (AVBDError, GPUSolver.swift:640-661)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class RuntimeFailure(RuntimeError):
+    """Latched runtime failure (RuntimeFailure, GPUSolver.swift:663-751)."""
+
+    def __init__(self, kind: int, message: str):
+        super().__init__(message or f"runtime failure {kind}")
+        self.kind = kind
+
+
+def library_path() -> str:
+    here = os.path.dirname(os.path.abspath(__file__))
+    return os.path.join(here, "_lib", "libavbd_b200.so")
+
+
+def load_library() -> C.CDLL:
+    """Load the in-tree CUDA library (fails loudly when it is missing)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = library_path()
+    if not os.path.exists(path):
+        raise ImportError(f"CUDA solver library not built: {path} (run avbd_b200.build.build())")
+    lib = C.CDLL(path)
+    vp, u32, i32, sz = C.c_void_p, C.c_uint32, C.c_int, C.c_size_t
+    sig = {
+        "avbd_create": ([vp, C.POINTER(vp)], i32),
+        "avbd_destroy": ([vp], None),
+        "avbd_set_settings": ([vp, vp], i32),
+        "avbd_get_settings": ([vp, vp], i32),
+        "avbd_step": ([vp, u32], i32),
+        "avbd_sync": ([vp], i32),
+        "avbd_get_body_states": ([vp, vp, u32, vp], i32),
+        "avbd_set_body_states": ([vp, vp, u32, vp], i32),
+        "avbd_get_positions": ([vp, u32, vp, vp], i32),
+        "avbd_set_positions": ([vp, u32, vp], i32),
+        "avbd_set_motor_targets": ([vp, vp, u32, vp], i32),
+        "avbd_max_constraint_error": ([vp, C.POINTER(C.c_float)], i32),
+        "avbd_get_counters": ([vp, vp], i32),
+        "avbd_runtime_failure": ([vp, C.POINTER(i32)], i32),
+        "avbd_last_error": ([vp, C.c_char_p, sz], i32),
+        "avbd_snapshot_capture": ([vp, C.POINTER(vp)], i32),
+        "avbd_snapshot_restore": ([vp, vp], i32),
+        "avbd_snapshot_free": ([vp], None),
+        "avbd_debug_buffer_size": ([vp, i32], sz),
+        "avbd_debug_read": ([vp, i32, vp, sz], i32),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _LIB = lib
+    return lib
+
+
+def _last_error(h=None) -> str:
+    buf = C.create_string_buffer(512)
+    load_library().avbd_last_error(h, buf, 512)
+    return buf.value.decode(errors="replace")
+
+
+class GPUSolver:
+    """AVBD solver step on one CUDA device (GPUSolver.swift:17)."""
+
+    def __init__(self, scene: PhysicsScene, max_pairs_per_body: int = 16, device: int = -1,
+                 truncation: int = abi.TRUNCATION_AUTOMATIC, tet_inversion_prevention: bool = False):
+        lib = load_library()
+        desc, self._keep = scene.to_desc(max_pairs_per_body=max_pairs_per_body,
+                                         truncation=truncation,
+                                         tet_inversion_prevention=tet_inversion_prevention,
+                                         device=device)
+        h = C.c_void_p()
+        rc = lib.avbd_create(C.byref(desc), C.byref(h))
+        if rc != abi.OK:
+            raise AVBDError(rc, _last_error(None))
+        self._h = h
+        self.num_bodies = len(scene.bodies)
+        self.num_joints = len(scene.joints)
+        self._settings = scene.settings
+
+    # -- lifetime ------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().avbd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown
+            pass
+
+    def _check(self, rc: int):
+        if rc == abi.OK:
+            return
+        if rc == abi.ERR_RUNTIME_FAILURE:
+            raise RuntimeFailure(self.runtime_failure(), _last_error(self._h))
+        raise AVBDError(rc, _last_error(self._h))
+
+    # -- stepping (submitStep / synchronize) ----------------------------------
+    @property
+    def settings(self) -> SimSettings:
+        return self._settings
+
+    @settings.setter
+    def settings(self, st: SimSettings):
+        c = st.to_c()
+        self._check(load_library().avbd_set_settings(self._h, C.byref(c)))
+        self._settings = st
+
+    def submit_step(self, frames: int = 1):
+        self._check(load_library().avbd_step(self._h, frames))
+
+    def step(self, frames: int = 1):
+        self.submit_step(frames)
+
+    def synchronize(self):
+        self._check(load_library().avbd_sync(self._h))
+
+    # -- state ---------------------------------------------------------------
+    def positions(self):
+        """(posLin xyzw with w = mass, posAng xyzw) for every body."""
+        n = self.num_bodies
+        pos = np.empty((n, 4), np.float32)
+        rot = np.empty((n, 4), np.float32)
+        self._check(load_library().avbd_get_positions(self._h, n, pos.ctypes.data, rot.ctypes.data))
+        return pos, rot
+
+    def read_positions_into(self, pos: np.ndarray):
+        self._check(load_library().avbd_get_positions(self._h, pos.shape[0], pos.ctypes.data, None))
+
+    def set_positions(self, xyz: np.ndarray):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float32)
+        self._check(load_library().avbd_set_positions(self._h, xyz.shape[0], xyz.ctypes.data))
+
+    def body_states(self, ids=None):
+        n = self.num_bodies if ids is None else len(ids)
+        out = (abi.BodyState * n)()
+        idp = None
+        if ids is not None:
+            idarr = np.ascontiguousarray(ids, dtype=np.uint32)
+            idp = idarr.ctypes.data
+        self._check(load_library().avbd_get_body_states(self._h, idp, n, out))
+        return out
+
+    def body_position(self, i: int):
+        return tuple(self.body_states([i])[0].position)
+
+    def set_body_states(self, ids, states):
+        idarr = np.ascontiguousarray(ids, dtype=np.uint32)
+        arr = (abi.BodyState * len(states))(*states)
+        self._check(load_library().avbd_set_body_states(self._h, idarr.ctypes.data, len(states), arr))
+
+    def set_motor_targets(self, joints, targets):
+        ids = np.ascontiguousarray(joints, dtype=np.uint32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        self._check(load_library().avbd_set_motor_targets(self._h, ids.ctypes.data, len(ids), t.ctypes.data))
+
+    # -- diagnostics -----------------------------------------------------------
+    def max_constraint_error(self) -> float:
+        v = C.c_float()
+        self._check(load_library().avbd_max_constraint_error(self._h, C.byref(v)))
+        return v.value
+
+    def counters(self) -> abi.Counters:
+        c = abi.Counters()
+        load_library().avbd_get_counters(self._h, C.byref(c))
+        return c
+
+    def runtime_failure(self) -> int:
+        k = C.c_int()
+        load_library().avbd_runtime_failure(self._h, C.byref(k))
+        return k.value
+
+    def last_error(self) -> str:
+        return _last_error(self._h)
+
+    def snapshot(self):
+        s = C.c_void_p()
+        self._check(load_library().avbd_snapshot_capture(self._h, C.byref(s)))
+        return _Snapshot(s)
+
+    def restore(self, snap):
+        self._check(load_library().avbd_snapshot_restore(self._h, snap._h))
+
+    def debug_read(self, name: str, dtype=np.uint8):
+        lib = load_library()
+        which = abi.BUF[name]
+        n = lib.avbd_debug_buffer_size(self._h, which)
+        buf = np.zeros(n, np.uint8)
+        if n:
+            self._check(lib.avbd_debug_read(self._h, which, buf.ctypes.data, n))
+        return buf.view(dtype)
+
+
+class _Snapshot:
+    def __init__(self, h):
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.avbd_snapshot_free(self._h)
+            self._h = None

@@ -1,0 +1,100 @@
+// avbd_types.h — device-resident records of the solver step, shared by host
+// and CUDA code.
+//
+// Layouts are float4/uint4-granular and match the reference's GPU record ABI
+// field for field (Sources/PhysicsAVBD/Shaders/00_common.metal:233-468), so a
+// record read back with avbd_debug_read() can be compared byte-for-byte with
+// the reference's definition.  The parameter block below is the subset of
+// `SimParams` the implemented stages consume.
+#pragma once
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define AVBD_HD __host__ __device__
+#else
+#define AVBD_HD
+#endif
+
+namespace avbd {
+
+struct alignas(16) f4 { float x, y, z, w; };
+struct alignas(16) u4 { uint32_t x, y, z, w; };
+
+constexpr float PENALTY_MIN = 1.0f;
+constexpr float PENALTY_MAX = 1.0e10f;
+constexpr float PENALTY_MAX_T = 1.0e6f;
+constexpr float STICK_THRESH = 0.00001f;
+constexpr int MAX_COLORS = 64;
+constexpr int MAX_CONTACTS = 8;
+constexpr uint32_t WORLD_BODY = 0xFFFFFFFFu;
+constexpr uint32_t FK_JOINT = 0, FK_SPRING = 1, FK_MANIFOLD = 2, FK_TET = 3, FK_SOFT = 4,
+                   FK_MEMBRANE = 5, FK_BEND = 6;
+constexpr int ADJ_KIND_SHIFT = 28;
+constexpr uint32_t ADJ_INDEX_MASK = 0x0FFFFFFFu;
+constexpr uint32_t MOTOR_MODE_MASK = 3u << 4;
+constexpr uint32_t MOTOR_IMPLICIT = 1u << 4;
+constexpr uint32_t MOTOR_EXPLICIT = 2u << 4;
+constexpr uint32_t MOTOR_VELOCITY = 3u << 4;
+constexpr uint32_t SHAPE_KIND_MASK = 0xFu;
+constexpr uint32_t SHAPE_PARTICLE = 0x10u;
+constexpr uint32_t COLLIDER_WORLD_ROUND_ANCHOR = 0x20u;
+
+struct JointGPU {
+    u4 header;      // bodyA (WORLD_BODY = world), bodyB, broken, flags
+    f4 rA;          // w = stiffnessLin
+    f4 rB;          // w = stiffnessAng
+    f4 C0Lin;       // w = torqueArm
+    f4 C0Ang;       // w = fracture
+    f4 lambdaLin, lambdaAng, penaltyLin, penaltyAng;
+    f4 restRel;     // rest relative rotation qA^-1 qB
+    f4 hingeAxis;   // xyz axis in B local; w != 0 -> hinge
+    f4 motor;       // target, effort limit, pad, kp
+    f4 limits;      // lo, hi, kd, pad
+    f4 dynamics;    // armature, predicted twist, explicit effort
+};
+struct SpringGPU { u4 header; f4 rA, rB, dual; };      // dual: lambda, penalty, C0
+struct TetGPU { u4 ids; f4 r0, r1, r2; };               // DmInv rows; w: 6V, muV, lamV
+struct ContactGPU { f4 rA, rB, C0, lambda, penalty; };  // rA.w feature, rB.w stick
+struct ManifoldGPU {
+    u4 header;        // bodyA, bodyB, numContacts, flags (1 active, 2 roundA, 4 roundB)
+    u4 colliderPair;
+    f4 basisN;        // w = dynamic friction
+    f4 basisT1;       // w = static friction
+    ContactGPU contacts[MAX_CONTACTS];
+};
+static_assert(sizeof(JointGPU) == 224, "JointGPU layout");
+static_assert(sizeof(SpringGPU) == 64, "SpringGPU layout");
+static_assert(sizeof(TetGPU) == 64, "TetGPU layout");
+static_assert(sizeof(ManifoldGPU) == 704, "ManifoldGPU layout");
+
+// Per-frame parameters (SimParams, 00_common.metal:233-288), passed by value.
+struct Params {
+    float dt, gravity, alpha, betaLin, betaAng, gamma;
+    uint32_t numBodies, numJoints, numSprings, mapCapacity, maxPairs;
+    float cellSize;
+    uint32_t gridHashSize, numHashed, numGlobals;
+    float maxSpeed, lambdaMax;
+    uint32_t iterations, numTets, numTris, numParticles;
+    float rodDecayPow, particleDamping;
+    uint32_t numHashedRigid, frictionCombineMode;
+    float collisionMargin, rigidLinearDamping, rigidAngularDamping;
+    uint32_t surfaceTruncationMode, tetInversionPreventionEnabled;
+    float planarDATRelaxation;
+    uint32_t numExclusions;
+};
+
+// Device counters of one frame (the reference's CTR_* layout, trimmed).
+struct Counters {
+    uint32_t numPairs;
+    uint32_t pairCandidates;
+    uint32_t colorConflicts;
+    uint32_t ogcExceeded;
+    uint32_t usedColors;
+    uint32_t waitTimeouts;
+    uint32_t pad[2];
+    uint32_t colorCount[MAX_COLORS];
+    uint32_t colorStart[MAX_COLORS + 2];
+    uint32_t changed[32];
+};
+
+}  // namespace avbd

@@ -1,0 +1,271 @@
+// broadphase.cu — exclusive scan, counting-sort spatial hash and
+// deterministic candidate-pair generation.
+//
+// Follows Shaders/10_scan.metal and Shaders/20_broadphase.metal:69-131,
+// :287-512.  The hash grid is a counting sort (count -> scan -> scatter ->
+// per-bucket sort by collider id); pairs are produced in two passes (count
+// per producer, scan, emit in producer/cell order) so the pair list — and
+// with it the manifold index of every pair — is the same on every run.
+#include "dmath.cuh"
+#include "kernels.h"
+
+namespace avbd {
+
+// ---------------------------------------------------------------------------
+// Exclusive scan: 1024 words per block (256 threads x 4), a single-block scan
+// of the block sums, then a uniform add.
+// ---------------------------------------------------------------------------
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_GRAIN = 4;
+constexpr int SCAN_BLOCK = SCAN_THREADS * SCAN_GRAIN;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warpSums,
+                                                         uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warpSums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        uint32_t w = lane < nw ? warpSums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
+        }
+        if (lane < nw) warpSums[lane] = w;   // inclusive warp prefix
+    }
+    __syncthreads();
+    uint32_t warpBase = warp > 0 ? warpSums[warp - 1] : 0u;
+    total = warpSums[(blockDim.x >> 5) - 1];
+    return warpBase + x - v;
+}
+
+__global__ void k_scan_blocks(const uint32_t* __restrict__ in, uint32_t* __restrict__ out,
+                              uint32_t* __restrict__ blockSums, uint32_t n) {
+    __shared__ uint32_t warpSums[32];
+    const uint32_t base = blockIdx.x * SCAN_BLOCK + threadIdx.x * SCAN_GRAIN;
+    uint32_t v[SCAN_GRAIN];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_GRAIN; i++) {
+        v[i] = base + i < n ? in[base + i] : 0u;
+        sum += v[i];
+    }
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(sum, warpSums, total);
+#pragma unroll
+    for (int i = 0; i < SCAN_GRAIN; i++) {
+        if (base + i < n) out[base + i] = run;
+        run += v[i];
+    }
+    if (threadIdx.x == 0) blockSums[blockIdx.x] = total;
+}
+
+__global__ void k_scan_block_sums(uint32_t* __restrict__ blockSums, uint32_t nblocks) {
+    __shared__ uint32_t warpSums[32];
+    // nblocks <= SCAN_BLOCK: each thread owns up to 4 consecutive sums
+    const uint32_t base = threadIdx.x * SCAN_GRAIN;
+    uint32_t v[SCAN_GRAIN];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_GRAIN; i++) {
+        v[i] = base + i < nblocks ? blockSums[base + i] : 0u;
+        sum += v[i];
+    }
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(sum, warpSums, total);
+#pragma unroll
+    for (int i = 0; i < SCAN_GRAIN; i++) {
+        if (base + i < nblocks) blockSums[base + i] = run;
+        run += v[i];
+    }
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ out, const uint32_t* __restrict__ blockSums,
+                           uint32_t n) {
+    const uint32_t add = blockSums[blockIdx.x];
+    const uint32_t base = blockIdx.x * SCAN_BLOCK + threadIdx.x * SCAN_GRAIN;
+#pragma unroll
+    for (int i = 0; i < SCAN_GRAIN; i++)
+        if (base + i < n) out[base + i] += add;
+}
+
+void launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scratch,
+                           cudaStream_t st) {
+    if (n == 0) return;
+    const uint32_t nblocks = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    k_scan_blocks<<<nblocks, SCAN_THREADS, 0, st>>>(in, out, scratch, n);
+    if (nblocks > 1) {
+        k_scan_block_sums<<<1, SCAN_THREADS, 0, st>>>(scratch, nblocks);
+        k_scan_add<<<nblocks, SCAN_THREADS, 0, st>>>(out, scratch, n);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Spatial hash
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float3 collider_center(const DevPtrs& d, uint32_t c) {
+    const uint32_t b = d.colOwner[c];
+    return xyz(d.posLin[b]) + q_rotate(d.posAng[b], xyz(d.colLocalPos[c]));
+}
+
+__global__ void k_bp_count(const Params P, const DevPtrs d) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.numHashed) return;
+    const uint32_t c = d.hashedIdx[i];
+    int x, y, z;
+    cell_coord(collider_center(d, c), P.cellSize, x, y, z);
+    const uint32_t h = cell_hash(x, y, z, d.colGroup[c], P.gridHashSize);
+    const uint32_t slot = atomicAdd(&d.cellCount[h], 1u);
+    d.bodyCellSlot[i] = make_uint2(h, slot);
+    if (d.colShape[c].w >= 0.0f) d.cellRigid[h] = 1u;
+}
+
+__global__ void k_bp_scatter(const Params P, const DevPtrs d) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.numHashed) return;
+    const uint2 cs = d.bodyCellSlot[i];
+    d.cellBodies[d.cellStart[cs.x] + cs.y] = d.hashedIdx[i];
+}
+
+// Buckets are tiny: an insertion sort per bucket restores collider order.
+__global__ void k_bp_sort_cells(const Params P, const DevPtrs d) {
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= P.gridHashSize) return;
+    const uint32_t s = d.cellStart[h], n = d.cellCount[h];
+    uint32_t* b = d.cellBodies + s;
+    for (uint32_t i = 1; i < n; i++) {
+        const uint32_t v = b[i];
+        uint32_t j = i;
+        while (j > 0 && b[j - 1] > v) { b[j] = b[j - 1]; j--; }
+        b[j] = v;
+    }
+}
+
+__device__ __forceinline__ bool pair_excluded(const uint32_t* ex, uint32_t count, uint32_t a,
+                                              uint32_t b) {
+    uint32_t lo = 0, hi = count;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint32_t ea = ex[2 * mid], eb = ex[2 * mid + 1];
+        if (ea < a || (ea == a && eb < b)) lo = mid + 1; else hi = mid;
+    }
+    return lo < count && ex[2 * lo] == a && ex[2 * lo + 1] == b;
+}
+
+__device__ __forceinline__ bool domains_compatible(uint32_t ga, uint32_t gb, uint32_t sa,
+                                                   uint32_t sb) {
+    if (!(ga == 0u || gb == 0u || ga == gb)) return false;
+    if (ga == 0u && gb != 0u) return sb != 0u;
+    if (gb == 0u && ga != 0u) return sa != 0u;
+    return true;
+}
+
+// One producer (a hashed or global collider) in collider/cell order.
+template <bool EMIT>
+__global__ void k_bp_pairs(const Params P, const DevPtrs d) {
+    const uint32_t producer = blockIdx.x * blockDim.x + threadIdx.x;
+    if (producer >= P.numHashed + P.numGlobals) return;
+    const uint32_t base = EMIT ? d.pairStart[producer] : 0u;
+    uint32_t count = 0;
+    auto consider = [&](uint32_t b, uint32_t ownerA, float3 pa, float ra, bool aDyn,
+                        uint32_t outA, uint32_t outB) {
+        const uint32_t ownerB = d.colOwner[b];
+        if (ownerA == ownerB) return;
+        if (!aDyn && d.posLin[ownerB].w <= 0.0f) return;
+        const float rb = fabsf(d.colShape[b].w);
+        const float3 dp = pa - collider_center(d, b);
+        const float r = ra + rb;
+        if (dot(dp, dp) > r * r) return;
+        if (pair_excluded(d.exclusions, P.numExclusions, min(ownerA, ownerB), max(ownerA, ownerB))) return;
+        const uint32_t slot = base + count;
+        if (EMIT && slot < P.maxPairs) d.pairs[slot] = make_uint2(outA, outB);
+        count++;
+    };
+    if (producer < P.numHashed) {
+        const uint32_t a = d.hashedIdx[producer];
+        const uint32_t ownerA = d.colOwner[a], groupA = d.colGroup[a], sharedA = d.colShared[a];
+        const float3 pa = collider_center(d, a);
+        const float ra = fabsf(d.colShape[a].w);
+        const bool aDyn = d.posLin[ownerA].w > 0.0f;
+        const uint32_t ga = d.clothGroup[ownerA];
+        if (!(ga != 0 && P.numHashedRigid == 0)) {
+            int cx, cy, cz;
+            cell_coord(pa, P.cellSize, cx, cy, cz);
+            uint32_t visited[27];
+            uint32_t nv = 0;
+            for (int dz = -1; dz <= 1; dz++)
+                for (int dy = -1; dy <= 1; dy++)
+                    for (int dx = -1; dx <= 1; dx++) {
+                        const uint32_t h = cell_hash(cx + dx, cy + dy, cz + dz, groupA, P.gridHashSize);
+                        bool dup = false;
+                        for (uint32_t v = 0; v < nv; v++) dup = dup || visited[v] == h;
+                        if (dup) continue;
+                        visited[nv++] = h;
+                        if (ga != 0 && d.cellRigid[h] == 0) continue;
+                        const uint32_t s0 = d.cellStart[h], e0 = s0 + d.cellCount[h];
+                        for (uint32_t k = s0; k < e0; k++) {
+                            const uint32_t b = d.cellBodies[k];
+                            if (b <= a) continue;
+                            if (!domains_compatible(groupA, d.colGroup[b], sharedA, d.colShared[b])) continue;
+                            // soft surface vs soft surface belongs to element contacts
+                            if (ga != 0 && d.clothGroup[d.colOwner[b]] != 0) continue;
+                            consider(b, ownerA, pa, ra, aDyn, a, b);
+                        }
+                    }
+        }
+        for (uint32_t g = 0; g < P.numGlobals; g++) {
+            const uint32_t b = d.globalIdx[g];
+            if (!domains_compatible(groupA, d.colGroup[b], sharedA, d.colShared[b])) continue;
+            if (ga != 0 && d.clothGroup[d.colOwner[b]] == ga) continue;
+            consider(b, ownerA, pa, ra, aDyn, min(a, b), max(a, b));
+        }
+    } else {
+        const uint32_t gp = producer - P.numHashed;
+        const uint32_t a = d.globalIdx[gp];
+        const uint32_t ownerA = d.colOwner[a], groupA = d.colGroup[a], sharedA = d.colShared[a];
+        const float3 pa = collider_center(d, a);
+        const float ra = fabsf(d.colShape[a].w);
+        const bool aDyn = d.posLin[ownerA].w > 0.0f;
+        const uint32_t ga = d.clothGroup[ownerA];
+        for (uint32_t g = gp + 1; g < P.numGlobals; g++) {
+            const uint32_t b = d.globalIdx[g];
+            if (!domains_compatible(groupA, d.colGroup[b], sharedA, d.colShared[b])) continue;
+            if (ga != 0 && d.clothGroup[d.colOwner[b]] == ga) continue;
+            consider(b, ownerA, pa, ra, aDyn, min(a, b), max(a, b));
+        }
+    }
+    if (!EMIT) d.pairCount[producer] = count;
+}
+
+__global__ void k_bp_finalize(const Params P, const DevPtrs d, uint32_t producers) {
+    const uint32_t n = producers == 0 ? 0u : d.pairStart[producers - 1] + d.pairCount[producers - 1];
+    d.counters->pairCandidates = n;
+    d.counters->numPairs = n < P.maxPairs ? n : P.maxPairs;
+}
+
+void launch_broadphase(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    cudaMemsetAsync(d.cellCount, 0, sizeof(uint32_t) * P.gridHashSize, st);
+    cudaMemsetAsync(d.cellRigid, 0, sizeof(uint32_t) * P.gridHashSize, st);
+    const int T = 128;
+    if (P.numHashed > 0) {
+        k_bp_count<<<(P.numHashed + T - 1) / T, T, 0, st>>>(P, d);
+        launch_exclusive_scan(d.cellCount, d.cellStart, P.gridHashSize, d.scanScratch, st);
+        k_bp_scatter<<<(P.numHashed + T - 1) / T, T, 0, st>>>(P, d);
+        k_bp_sort_cells<<<(P.gridHashSize + T - 1) / T, T, 0, st>>>(P, d);
+    }
+    if (z.producers > 0) {
+        k_bp_pairs<false><<<(z.producers + T - 1) / T, T, 0, st>>>(P, d);
+        launch_exclusive_scan(d.pairCount, d.pairStart, z.producers, d.scanScratch, st);
+        k_bp_pairs<true><<<(z.producers + T - 1) / T, T, 0, st>>>(P, d);
+    }
+    k_bp_finalize<<<1, 1, 0, st>>>(P, d, z.producers);
+}
+
+}  // namespace avbd

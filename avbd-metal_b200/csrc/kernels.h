@@ -1,0 +1,93 @@
+// kernels.h — device buffers of one solver and the host launchers of every
+// stage kernel.  All launches go to the solver's stream, so one frame is a
+// fixed launch sequence that the runtime captures into a CUDA graph.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "avbd_types.h"
+
+namespace avbd {
+
+struct DevPtrs {
+    // bodies
+    float4 *posLin, *posAng, *initLin, *initAng, *inertLin, *inertAng;
+    float4 *velLin, *velAng, *prevVelLin, *props, *shape, *spinVel;
+    float* gravityScale;
+    uint32_t* clothGroup;
+    // colliders
+    uint32_t *colOwner, *colShapeType, *colGroup, *colShared;
+    float4 *colShape, *colLocalPos, *colLocalRot;
+    float2* colFriction;
+    uint32_t *hashedIdx, *globalIdx;
+    uint32_t* exclusions;                 // uint2 pairs
+    // broadphase
+    uint32_t *cellCount, *cellStart, *cellBodies, *cellRigid;
+    uint2* bodyCellSlot;
+    uint32_t *pairCount, *pairStart;
+    uint2* pairs;
+    // contacts (current frame and previous frame)
+    ManifoldGPU *manifolds, *prevManifolds;
+    uint32_t *mapKeyA, *mapKeyB, *mapVal;
+    // constraints
+    JointGPU* joints;
+    uint32_t* activeJoints;
+    SpringGPU* springs;
+    uint32_t* hardSprings;
+    TetGPU* tets;
+    // adjacency: static segments + per-frame contact segment
+    uint4* staticSeg;
+    uint32_t *preList, *postList;
+    uint32_t *dynCount, *dynStart, *dynCursor, *dynList;
+    // coloring
+    uint32_t *colorsA, *colorsB, *colorList, *bodySlot;
+    // control
+    Counters* counters;
+    uint32_t* scanScratch;                // block sums of the exclusive scans
+    float* diag;
+    uint32_t *colorStart;                 // static palette or counters->colorStart
+    float4 *initPenLin, *initPenAng;      // authored joint penalties (state resets)
+    uint32_t* resetFlags;                 // body flags for set_body_states
+    // kinematic drivers advanced at frame end
+    uint32_t* spinnerBody;
+    float4* spinnerAxisOmega;             // xyz axis, w omega
+    uint32_t* rateJoint;
+    float* rateValue;
+    uint32_t numSpinners, numRateMotors;
+    uint32_t* failureLatch;               // [0] kind, [1] frame, [2] detail
+    uint32_t* frameCounter;
+};
+
+struct Sizes {
+    uint32_t numBodies, numColliders, numActiveJoints, numHardSprings, numTets;
+    uint32_t maxPairs, producers, numDynamicBodies;
+    uint32_t scanScratchWords;
+    bool dynamicColoring;
+};
+
+// exclusive scan of n words (n <= 1024 * 1024); out may not alias in
+void launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scratch,
+                           cudaStream_t st);
+
+void launch_broadphase(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_narrowphase(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_map_rebuild(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_warmstart(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_adjacency(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_dynamic_coloring(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+// one color of the block-descent primal; `count` is the color's body count
+// when known on the host (static palette), else 0xFFFFFFFF (read on device)
+void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color,
+                         uint32_t count, cudaStream_t st);
+// every iteration of a small scene in one thread block
+void launch_solve_small(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t colorBound,
+                        cudaStream_t st);
+void launch_dual(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_finalize(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_max_constraint_error(const Params& P, const DevPtrs& d, const Sizes& z,
+                                 cudaStream_t st);
+void launch_reset_bodies(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+// spinners and legacy rate motors, then the end-of-frame failure check
+void launch_frame_end(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+
+}  // namespace avbd

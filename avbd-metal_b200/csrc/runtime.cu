@@ -1,0 +1,646 @@
+// runtime.cu — the solver object behind the C ABI of include/avbd.h.
+//
+// Owns every device buffer (GPUSolver.swift:445-608), builds one CUDA graph
+// per manifold-buffer parity for the whole frame (GPUSolver.swift:3138-4375
+// encodes the same stage order into one Metal command buffer), replays it per
+// frame, latches the first runtime failure (GPUSolver.swift:2800-2922) and
+// serves state reads and writes.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstddef>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/avbd.h"
+#include "kernels.h"
+#include "upload.h"
+
+using namespace avbd;
+
+namespace {
+thread_local std::string g_last_error;
+
+__global__ void k_set_positions(float4* posLin, const float* xyz, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = posLin[i];
+    posLin[i] = make_float4(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], p.w);
+}
+
+__global__ void k_set_states(DevPtrs d, const uint32_t* ids, const avbd_body_state* st, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t b = ids ? ids[i] : i;
+    const avbd_body_state s = st[i];
+    const float w = d.posLin[b].w;
+    d.posLin[b] = make_float4(s.position[0], s.position[1], s.position[2], w);
+    d.posAng[b] = make_float4(s.rotation[0], s.rotation[1], s.rotation[2], s.rotation[3]);
+    d.velLin[b] = make_float4(s.velocity[0], s.velocity[1], s.velocity[2], 0.0f);
+    d.velAng[b] = make_float4(s.angular_velocity[0], s.angular_velocity[1], s.angular_velocity[2], 0.0f);
+    d.prevVelLin[b] = d.velLin[b];
+    d.resetFlags[b] = 1u;
+}
+
+__global__ void k_set_motor_targets(JointGPU* joints, const uint32_t* ids, const float* targets, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    JointGPU& j = joints[ids[i]];
+    if ((j.header.w & MOTOR_MODE_MASK) == 0u) return;   // welded/disabled: a no-op
+    j.motor.x = targets[i];
+}
+}  // namespace
+
+struct avbd_snapshot {
+    std::vector<std::vector<uint8_t>> blobs;
+    uint64_t frame;
+};
+
+struct avbd_solver {
+    HostScene H;
+    DevPtrs d{};
+    Sizes z{};
+    Params P{};
+    avbd_settings settings{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graphsValid = false;
+    uint64_t frame = 0;
+    int failure = AVBD_FAIL_NONE;
+    std::string error;
+    bool smallSolve = false;
+    std::vector<void*> allocations;
+    struct StateBuf { void* ptr; size_t bytes; };
+    std::vector<StateBuf> state;       // buffers captured by snapshots
+    // staging for host-side writes
+    void* stage = nullptr;
+    size_t stageBytes = 0;
+    uint32_t* hostLatch = nullptr;     // pinned copy of the failure latch
+    Counters* hostCounters = nullptr;  // pinned copy of the last frame's counters
+
+    ~avbd_solver() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& g : graph) if (g) cudaGraphExecDestroy(g);
+        for (void* p : allocations) cudaFree(p);
+        if (stage) cudaFree(stage);
+        if (hostLatch) cudaFreeHost(hostLatch);
+        if (hostCounters) cudaFreeHost(hostCounters);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    bool check(cudaError_t e, const char* what) {
+        if (e == cudaSuccess) return true;
+        if (failure == AVBD_FAIL_NONE) {
+            failure = AVBD_FAIL_COMMAND_EXECUTION;
+            error = std::string(what) + ": " + cudaGetErrorString(e);
+        }
+        return false;
+    }
+
+    template <typename T>
+    bool alloc(T*& ptr, size_t count, const char* label, bool snapshot = false) {
+        size_t bytes = sizeof(T) * (count ? count : 1);
+        void* p = nullptr;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            error = std::string("allocation failed: ") + label;
+            return false;
+        }
+        cudaMemset(p, 0, bytes);
+        allocations.push_back(p);
+        ptr = static_cast<T*>(p);
+        if (snapshot) state.push_back({p, bytes});
+        return true;
+    }
+    template <typename T>
+    bool upload(T*& ptr, const std::vector<T>& host, const char* label, bool snapshot = false) {
+        if (!alloc(ptr, host.size(), label, snapshot)) return false;
+        if (!host.empty() && cudaMemcpy(ptr, host.data(), sizeof(T) * host.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+            error = std::string("upload failed: ") + label;
+            return false;
+        }
+        return true;
+    }
+
+    void sync_params() {
+        P.dt = settings.dt;
+        P.gravity = settings.gravity;
+        P.alpha = settings.alpha;
+        P.betaLin = settings.beta_lin;
+        P.betaAng = settings.beta_ang;
+        P.gamma = settings.gamma;
+        P.lambdaMax = settings.lambda_max;
+        P.iterations = (uint32_t)(settings.iterations < 0 ? 0 : settings.iterations);
+        P.rodDecayPow = settings.rod_decay_pow;
+        P.particleDamping = settings.particle_damping;
+        P.frictionCombineMode = settings.friction_combine_mode;
+        P.collisionMargin = settings.collision_margin > 0.0f ? settings.collision_margin : 0.0f;
+        P.rigidLinearDamping = settings.rigid_linear_damping > 0.0f ? settings.rigid_linear_damping : 0.0f;
+        P.rigidAngularDamping = settings.rigid_angular_damping > 0.0f ? settings.rigid_angular_damping : 0.0f;
+    }
+
+    // One frame, in the reference's stage order.  `parity` selects which
+    // manifold buffer is "current" (the buffers swap after every frame).
+    void encode_frame(int parity) {
+        DevPtrs f = d;
+        if (parity) std::swap(f.manifolds, f.prevManifolds);
+        cudaStream_t st = stream;
+        cudaMemsetAsync(f.counters, 0, sizeof(Counters), st);
+        launch_broadphase(P, f, z, st);
+        launch_narrowphase(P, f, z, st);
+        launch_map_rebuild(P, f, z, st);
+        launch_warmstart(P, f, z, st);
+        launch_adjacency(P, f, z, st);
+        if (z.dynamicColoring) launch_dynamic_coloring(P, f, z, st);
+        const uint32_t colorBound = z.dynamicColoring ? (uint32_t)MAX_COLORS : H.staticUsedColors;
+        if (smallSolve) {
+            launch_solve_small(P, f, z, colorBound, st);
+        } else {
+            for (uint32_t it = 0; it < P.iterations; it++) {
+                for (uint32_t c = 0; c < colorBound; c++)
+                    launch_primal_color(P, f, z, c, z.dynamicColoring ? 0xFFFFFFFFu : H.colorCounts[c], st);
+                launch_dual(P, f, z, st);
+            }
+        }
+        launch_finalize(P, f, z, st);
+        launch_frame_end(P, f, z, st);
+    }
+
+    bool build_graphs() {
+        for (int parity = 0; parity < 2; parity++) {
+            if (graph[parity]) { cudaGraphExecDestroy(graph[parity]); graph[parity] = nullptr; }
+            cudaGraph_t g = nullptr;
+            if (!check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture")) return false;
+            encode_frame(parity);
+            cudaError_t e = cudaStreamEndCapture(stream, &g);
+            if (!check(e, "end capture")) return false;
+            e = cudaGraphInstantiate(&graph[parity], g, 0);
+            cudaGraphDestroy(g);
+            if (!check(e, "graph instantiate")) return false;
+        }
+        graphsValid = true;
+        return true;
+    }
+
+    int create(const avbd_scene_desc* s) {
+        int rc = upload_scene(s, H, error);
+        if (rc != AVBD_OK) return rc;
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) { error = "no CUDA device"; return AVBD_ERR_NO_DEVICE; }
+        device = s->device >= 0 ? s->device : 0;
+        if (s->device < 0) cudaGetDevice(&device);
+        if (device >= count || cudaSetDevice(device) != cudaSuccess) { error = "cannot select CUDA device"; return AVBD_ERR_NO_DEVICE; }
+        if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) { error = "stream creation failed"; return AVBD_ERR_NO_DEVICE; }
+        settings = s->settings;
+        P = H.P;
+        sync_params();
+        const uint32_t nb = H.numBodies, nc = H.numColliders;
+        z.numBodies = nb;
+        z.numColliders = nc;
+        z.numActiveJoints = (uint32_t)H.activeJoints.size();
+        z.numHardSprings = (uint32_t)H.hardSprings.size();
+        z.numTets = (uint32_t)H.tets.size();
+        z.maxPairs = H.maxPairs;
+        z.producers = P.numHashed + P.numGlobals;
+        z.numDynamicBodies = H.numDynamicBodies;
+        z.dynamicColoring = H.dynamicColoring;
+        const uint32_t scanLimit = 1024u * 1024u;
+        if (P.gridHashSize > scanLimit || z.producers > scanLimit || nb > scanLimit) {
+            error = "scene exceeds the 1M-element scan limit of this build";
+            return AVBD_ERR_UNSUPPORTED;
+        }
+        bool ok = true;
+        // bodies
+        ok = ok && upload(reinterpret_cast<f4*&>(d.posLin), H.posLin, "posLin", true);
+        ok = ok && upload(reinterpret_cast<f4*&>(d.posAng), H.posAng, "posAng", true);
+        ok = ok && alloc(d.initLin, nb, "initLin", true) && alloc(d.initAng, nb, "initAng", true);
+        ok = ok && alloc(d.inertLin, nb, "inertLin", true) && alloc(d.inertAng, nb, "inertAng", true);
+        ok = ok && upload(reinterpret_cast<f4*&>(d.velLin), H.velLin, "velLin", true);
+        ok = ok && upload(reinterpret_cast<f4*&>(d.velAng), H.velAng, "velAng", true);
+        ok = ok && upload(reinterpret_cast<f4*&>(d.prevVelLin), H.prevVelLin, "prevVelLin", true);
+        ok = ok && upload(reinterpret_cast<f4*&>(d.props), H.props, "props");
+        ok = ok && upload(reinterpret_cast<f4*&>(d.shape), H.shape, "shape");
+        ok = ok && upload(reinterpret_cast<f4*&>(d.spinVel), H.spinVel, "spinVel");
+        ok = ok && upload(d.gravityScale, H.gravityScale, "gravityScale");
+        ok = ok && upload(d.clothGroup, H.clothGroup, "clothGroup");
+        // colliders
+        ok = ok && upload(d.colOwner, H.colOwner, "colliderOwner") && upload(d.colShapeType, H.colShapeType, "colliderShapeType");
+        ok = ok && upload(d.colGroup, H.colGroup, "colliderGroup") && upload(d.colShared, H.colShared, "colliderShared");
+        ok = ok && upload(reinterpret_cast<f4*&>(d.colShape), H.colShape, "colliderShape");
+        ok = ok && upload(reinterpret_cast<f4*&>(d.colLocalPos), H.colLocalPos, "colliderLocalPosition");
+        ok = ok && upload(reinterpret_cast<f4*&>(d.colLocalRot), H.colLocalRot, "colliderLocalRotation");
+        ok = ok && upload(reinterpret_cast<float*&>(d.colFriction), H.colFriction, "colliderFriction");
+        ok = ok && upload(d.hashedIdx, H.hashedIdx, "hashedIdx") && upload(d.globalIdx, H.globalIdx, "globalIdx");
+        ok = ok && upload(d.exclusions, H.exclusions, "exclusions");
+        // broadphase
+        ok = ok && alloc(d.cellCount, P.gridHashSize, "cellCount") && alloc(d.cellStart, P.gridHashSize, "cellStart");
+        ok = ok && alloc(d.cellRigid, P.gridHashSize, "cellRigid") && alloc(d.cellBodies, P.numHashed, "cellBodies");
+        ok = ok && alloc(d.bodyCellSlot, P.numHashed, "bodyCellSlot");
+        ok = ok && alloc(d.pairCount, z.producers, "pairCount") && alloc(d.pairStart, z.producers, "pairStart");
+        ok = ok && alloc(d.pairs, H.maxPairs, "pairs");
+        ok = ok && alloc(d.manifolds, H.maxPairs, "manifolds", true) && alloc(d.prevManifolds, H.maxPairs, "prevManifolds", true);
+        ok = ok && alloc(d.mapKeyA, H.mapCapacity, "mapKeyA", true) && alloc(d.mapKeyB, H.mapCapacity, "mapKeyB", true);
+        ok = ok && alloc(d.mapVal, H.mapCapacity, "mapVal", true);
+        // constraints
+        ok = ok && upload(d.joints, H.joints, "joints", true) && upload(d.activeJoints, H.activeJoints, "activeJoints");
+        ok = ok && upload(reinterpret_cast<f4*&>(d.initPenLin), H.initPenLin, "initialJointPenaltyLin");
+        ok = ok && upload(reinterpret_cast<f4*&>(d.initPenAng), H.initPenAng, "initialJointPenaltyAng");
+        ok = ok && upload(d.springs, H.springs, "springs", true) && upload(d.hardSprings, H.hardSprings, "hardSprings");
+        ok = ok && upload(d.tets, H.tets, "tets");
+        // adjacency
+        ok = ok && upload(reinterpret_cast<u4*&>(d.staticSeg), H.staticSeg, "staticSeg");
+        ok = ok && upload(d.preList, H.preList, "preList") && upload(d.postList, H.postList, "postList");
+        ok = ok && alloc(d.dynCount, nb, "dynCount") && alloc(d.dynStart, nb, "dynStart") && alloc(d.dynCursor, nb, "dynCursor");
+        ok = ok && alloc(d.dynList, 2 * (size_t)H.maxPairs, "dynList");
+        // coloring
+        ok = ok && upload(d.colorsA, H.colors, "colorsA", true) && upload(d.colorsB, H.colors, "colorsB");
+        ok = ok && alloc(d.bodySlot, nb, "bodySlot");
+        if (H.dynamicColoring) {
+            ok = ok && alloc(d.colorList, nb, "colorList");
+        } else {
+            ok = ok && upload(d.colorList, H.colorList, "colorList");
+            ok = ok && upload(d.colorStart, H.colorStart, "colorStart");
+        }
+        // control
+        ok = ok && alloc(d.counters, 1, "counters") && alloc(d.scanScratch, 1024 + 32, "scanScratch");
+        ok = ok && alloc(d.diag, 1, "diag") && alloc(d.resetFlags, nb, "resetFlags");
+        ok = ok && alloc(d.failureLatch, 4, "failureLatch") && alloc(d.frameCounter, 1, "frameCounter", true);
+        if (H.dynamicColoring)
+            d.colorStart = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(d.counters) + offsetof(Counters, colorStart));
+        std::vector<uint32_t> spB, rJ;
+        std::vector<f4> spA;
+        std::vector<float> rV;
+        for (const auto& sp : H.spinners) { spB.push_back((uint32_t)sp.body); spA.push_back(f4{sp.axis[0], sp.axis[1], sp.axis[2], sp.omega}); }
+        for (const auto& rm : H.rateMotors) { rJ.push_back(rm.first); rV.push_back(rm.second); }
+        ok = ok && upload(d.spinnerBody, spB, "spinnerBody") && upload(reinterpret_cast<f4*&>(d.spinnerAxisOmega), spA, "spinnerAxis");
+        ok = ok && upload(d.rateJoint, rJ, "rateJoint") && upload(d.rateValue, rV, "rateValue");
+        d.numSpinners = (uint32_t)spB.size();
+        d.numRateMotors = (uint32_t)rJ.size();
+        if (!ok) return AVBD_ERR_ALLOC_FAILED;
+        if (cudaMallocHost(&hostLatch, 4 * sizeof(uint32_t)) != cudaSuccess ||
+            cudaMallocHost(&hostCounters, sizeof(Counters)) != cudaSuccess) {
+            error = "pinned allocation failed";
+            return AVBD_ERR_ALLOC_FAILED;
+        }
+        std::memset(hostLatch, 0, 4 * sizeof(uint32_t));
+        std::memset(hostCounters, 0, sizeof(Counters));
+        // Small scenes run their whole iteration loop in one thread block.
+        smallSolve = z.numDynamicBodies <= 512;
+        if (cudaDeviceSynchronize() != cudaSuccess) { error = "device error during upload"; return AVBD_ERR_NO_DEVICE; }
+        return AVBD_OK;
+    }
+
+    // Wait for the stream, then surface an execution error or a latched
+    // capacity/coloring failure.
+    int retire() {
+        if (!check(cudaStreamSynchronize(stream), "frame execution")) return AVBD_ERR_RUNTIME_FAILURE;
+        if (!check(cudaMemcpy(hostLatch, d.failureLatch, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost), "latch readback"))
+            return AVBD_ERR_RUNTIME_FAILURE;
+        if (hostLatch[0] != 0 && failure == AVBD_FAIL_NONE) {
+            failure = (int)hostLatch[0];
+            char buf[160];
+            if (failure == AVBD_FAIL_RIGID_PAIR_CAPACITY)
+                std::snprintf(buf, sizeof buf, "rigid pair capacity exceeded at frame %u: %u candidates > %u",
+                              hostLatch[1], hostLatch[2], H.maxPairs);
+            else
+                std::snprintf(buf, sizeof buf, "unresolved dynamic coloring at frame %u: %u conflicting bodies",
+                              hostLatch[1], hostLatch[2]);
+            error = buf;
+        }
+        return failure == AVBD_FAIL_NONE ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+    }
+
+    int step(uint32_t frames) {
+        if (failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
+        if (!graphsValid && !build_graphs()) return AVBD_ERR_RUNTIME_FAILURE;
+        for (uint32_t f = 0; f < frames; f++) {
+            if (!check(cudaGraphLaunch(graph[frame & 1], stream), "graph launch")) return AVBD_ERR_RUNTIME_FAILURE;
+            frame++;
+        }
+        return AVBD_OK;
+    }
+
+    void* staging(size_t bytes) {
+        if (bytes > stageBytes) {
+            if (stage) cudaFree(stage);
+            stage = nullptr;
+            stageBytes = 0;
+            if (cudaMalloc(&stage, bytes) != cudaSuccess) return nullptr;
+            stageBytes = bytes;
+        }
+        return stage;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int avbd_create(const avbd_scene_desc* scene, avbd_solver** out) {
+    if (!out) return AVBD_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    avbd_solver* s = nullptr;
+    try {
+        s = new avbd_solver();
+        int rc = s->create(scene);
+        if (rc != AVBD_OK) {
+            g_last_error = s->error;
+            delete s;
+            return rc;
+        }
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        delete s;
+        return AVBD_ERR_ALLOC_FAILED;
+    }
+    g_last_error.clear();
+    *out = s;
+    return AVBD_OK;
+}
+
+void avbd_destroy(avbd_solver* s) { delete s; }
+
+int avbd_set_settings(avbd_solver* s, const avbd_settings* st) {
+    if (!s || !st) return AVBD_ERR_INVALID_ARGUMENT;
+    if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
+    if (!(st->dt > 0.0f) || st->iterations < 0) return AVBD_ERR_INVALID_ARGUMENT;
+    s->settings = *st;
+    s->sync_params();
+    s->graphsValid = false;   // parameters are baked into the frame graphs
+    return AVBD_OK;
+}
+
+int avbd_get_settings(const avbd_solver* s, avbd_settings* out) {
+    if (!s || !out) return AVBD_ERR_INVALID_ARGUMENT;
+    *out = s->settings;
+    return AVBD_OK;
+}
+
+int avbd_step(avbd_solver* s, uint32_t frames) {
+    if (!s) return AVBD_ERR_INVALID_ARGUMENT;
+    return s->step(frames);
+}
+
+int avbd_sync(avbd_solver* s) {
+    if (!s) return AVBD_ERR_INVALID_ARGUMENT;
+    return s->retire();
+}
+
+int avbd_get_positions(avbd_solver* s, uint32_t n, float* pos, float* rot) {
+    if (!s || n > s->z.numBodies) return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    if (pos && !s->check(cudaMemcpy(pos, s->d.posLin, (size_t)n * 16, cudaMemcpyDeviceToHost), "position readback")) return AVBD_ERR_RUNTIME_FAILURE;
+    if (rot && !s->check(cudaMemcpy(rot, s->d.posAng, (size_t)n * 16, cudaMemcpyDeviceToHost), "rotation readback")) return AVBD_ERR_RUNTIME_FAILURE;
+    return AVBD_OK;
+}
+
+int avbd_get_body_states(avbd_solver* s, const uint32_t* ids, uint32_t n, avbd_body_state* out) {
+    if (!s || !out) return AVBD_ERR_INVALID_ARGUMENT;
+    const uint32_t nb = s->z.numBodies;
+    if (!ids && n > nb) return AVBD_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; ids && i < n; i++) if (ids[i] >= nb) return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    std::vector<float4> pl(nb), pa(nb), vl(nb), va(nb);
+    if (!s->check(cudaMemcpy(pl.data(), s->d.posLin, nb * 16, cudaMemcpyDeviceToHost), "state readback") ||
+        !s->check(cudaMemcpy(pa.data(), s->d.posAng, nb * 16, cudaMemcpyDeviceToHost), "state readback") ||
+        !s->check(cudaMemcpy(vl.data(), s->d.velLin, nb * 16, cudaMemcpyDeviceToHost), "state readback") ||
+        !s->check(cudaMemcpy(va.data(), s->d.velAng, nb * 16, cudaMemcpyDeviceToHost), "state readback"))
+        return AVBD_ERR_RUNTIME_FAILURE;
+    for (uint32_t i = 0; i < n; i++) {
+        const uint32_t b = ids ? ids[i] : i;
+        avbd_body_state& o = out[i];
+        o.position[0] = pl[b].x; o.position[1] = pl[b].y; o.position[2] = pl[b].z;
+        o.rotation[0] = pa[b].x; o.rotation[1] = pa[b].y; o.rotation[2] = pa[b].z; o.rotation[3] = pa[b].w;
+        o.velocity[0] = vl[b].x; o.velocity[1] = vl[b].y; o.velocity[2] = vl[b].z;
+        o.angular_velocity[0] = va[b].x; o.angular_velocity[1] = va[b].y; o.angular_velocity[2] = va[b].z;
+    }
+    return AVBD_OK;
+}
+
+int avbd_set_body_states(avbd_solver* s, const uint32_t* ids, uint32_t n, const avbd_body_state* states) {
+    if (!s || (!states && n)) return AVBD_ERR_INVALID_ARGUMENT;
+    if (n == 0) return AVBD_OK;
+    const uint32_t nb = s->z.numBodies;
+    if (!ids && n > nb) return AVBD_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; ids && i < n; i++) if (ids[i] >= nb) return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    const size_t bytesStates = sizeof(avbd_body_state) * n, bytesIds = ids ? 4 * (size_t)n : 0;
+    uint8_t* st = static_cast<uint8_t*>(s->staging(bytesStates + bytesIds + 16));
+    if (!st) return AVBD_ERR_ALLOC_FAILED;
+    uint32_t* dIds = ids ? reinterpret_cast<uint32_t*>(st + bytesStates) : nullptr;
+    if (!s->check(cudaMemcpyAsync(st, states, bytesStates, cudaMemcpyHostToDevice, s->stream), "state upload")) return AVBD_ERR_RUNTIME_FAILURE;
+    if (ids && !s->check(cudaMemcpyAsync(dIds, ids, bytesIds, cudaMemcpyHostToDevice, s->stream), "state upload")) return AVBD_ERR_RUNTIME_FAILURE;
+    cudaMemsetAsync(s->d.resetFlags, 0, 4 * (size_t)nb, s->stream);
+    k_set_states<<<(n + 127) / 128, 128, 0, s->stream>>>(s->d, dIds, reinterpret_cast<const avbd_body_state*>(st), n);
+    launch_reset_bodies(s->P, s->d, s->z, s->stream);
+    return s->retire();
+}
+
+int avbd_set_positions(avbd_solver* s, uint32_t n, const float* xyz) {
+    if (!s || !xyz || n > s->z.numBodies) return AVBD_ERR_INVALID_ARGUMENT;
+    if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
+    float* st = static_cast<float*>(s->staging((size_t)n * 12 + 16));
+    if (!st) return AVBD_ERR_ALLOC_FAILED;
+    if (!s->check(cudaMemcpyAsync(st, xyz, (size_t)n * 12, cudaMemcpyHostToDevice, s->stream), "position upload")) return AVBD_ERR_RUNTIME_FAILURE;
+    k_set_positions<<<(n + 255) / 256, 256, 0, s->stream>>>(s->d.posLin, st, n);
+    return s->check(cudaGetLastError(), "position upload") ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+}
+
+int avbd_set_motor_targets(avbd_solver* s, const uint32_t* joints, uint32_t n, const float* targets) {
+    if (!s || (n && (!joints || !targets))) return AVBD_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < n; i++) {
+        if (joints[i] >= s->H.joints.size() || !std::isfinite(targets[i])) return AVBD_ERR_INVALID_ARGUMENT;
+        uint32_t mode = s->H.joints[joints[i]].header.w & MOTOR_MODE_MASK;
+        if (mode == MOTOR_VELOCITY) return AVBD_ERR_INVALID_ARGUMENT;  // requires a position-PD motor
+    }
+    if (n == 0) return AVBD_OK;
+    if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
+    uint8_t* st = static_cast<uint8_t*>(s->staging(8 * (size_t)n + 16));
+    if (!st) return AVBD_ERR_ALLOC_FAILED;
+    cudaMemcpyAsync(st, joints, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream);
+    cudaMemcpyAsync(st + 4 * (size_t)n, targets, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream);
+    k_set_motor_targets<<<(n + 127) / 128, 128, 0, s->stream>>>(s->d.joints, reinterpret_cast<uint32_t*>(st),
+                                                                 reinterpret_cast<float*>(st + 4 * (size_t)n), n);
+    return s->check(cudaGetLastError(), "motor targets") ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+}
+
+int avbd_max_constraint_error(avbd_solver* s, float* out) {
+    if (!s || !out) return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    DevPtrs f = s->d;
+    if (s->frame & 1) std::swap(f.manifolds, f.prevManifolds);
+    launch_max_constraint_error(s->P, f, s->z, s->stream);
+    if (!s->check(cudaMemcpyAsync(out, s->d.diag, 4, cudaMemcpyDeviceToHost, s->stream), "diag readback")) return AVBD_ERR_RUNTIME_FAILURE;
+    return s->retire();
+}
+
+int avbd_get_counters(avbd_solver* s, avbd_counters* out) {
+    if (!s || !out) return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = s->retire();
+    if (rc != AVBD_OK && rc != AVBD_ERR_RUNTIME_FAILURE) return rc;
+    Counters c{};
+    cudaMemcpy(&c, s->d.counters, sizeof(Counters), cudaMemcpyDeviceToHost);
+    std::memset(out, 0, sizeof(*out));
+    out->frame = s->frame;
+    out->num_pairs = c.numPairs;
+    out->pair_candidates = c.pairCandidates;
+    out->color_conflicts = c.colorConflicts;
+    out->ogc_exceeded = c.ogcExceeded;
+    if (s->z.dynamicColoring) {
+        out->used_colors = c.usedColors;
+        for (int i = 0; i < 64; i++) out->color_counts[i] = c.colorCount[i];
+    } else {
+        out->used_colors = s->H.staticUsedColors;
+        for (int i = 0; i < 64; i++) out->color_counts[i] = s->H.colorCounts[i];
+    }
+    return AVBD_OK;
+}
+
+int avbd_runtime_failure(const avbd_solver* s, int* kind) {
+    if (!s || !kind) return AVBD_ERR_INVALID_ARGUMENT;
+    *kind = s->failure;
+    return AVBD_OK;
+}
+
+int avbd_last_error(const avbd_solver* s, char* buf, size_t len) {
+    if (!buf || len == 0) return AVBD_ERR_INVALID_ARGUMENT;
+    const std::string& e = s ? s->error : g_last_error;
+    std::snprintf(buf, len, "%s", e.c_str());
+    return AVBD_OK;
+}
+
+int avbd_snapshot_capture(avbd_solver* s, avbd_snapshot** out) {
+    if (!s || !out) return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    avbd_snapshot* snap = new avbd_snapshot();
+    snap->frame = s->frame;
+    for (const auto& b : s->state) {
+        snap->blobs.emplace_back(b.bytes);
+        if (!s->check(cudaMemcpy(snap->blobs.back().data(), b.ptr, b.bytes, cudaMemcpyDeviceToHost), "snapshot")) {
+            delete snap;
+            return AVBD_ERR_RUNTIME_FAILURE;
+        }
+    }
+    *out = snap;
+    return AVBD_OK;
+}
+
+int avbd_snapshot_restore(avbd_solver* s, const avbd_snapshot* snap) {
+    if (!s || !snap || snap->blobs.size() != s->state.size()) return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    for (size_t i = 0; i < s->state.size(); i++)
+        if (!s->check(cudaMemcpy(s->state[i].ptr, snap->blobs[i].data(), s->state[i].bytes, cudaMemcpyHostToDevice), "restore"))
+            return AVBD_ERR_RUNTIME_FAILURE;
+    s->frame = snap->frame;
+    return AVBD_OK;
+}
+
+void avbd_snapshot_free(avbd_snapshot* snap) { delete snap; }
+
+size_t avbd_debug_buffer_size(avbd_solver* s, int which) {
+    if (!s) return 0;
+    const HostScene& H = s->H;
+    const size_t nb = H.numBodies;
+    switch (which) {
+    case AVBD_BUF_POS_LIN: case AVBD_BUF_POS_ANG: case AVBD_BUF_VEL_LIN: case AVBD_BUF_VEL_ANG:
+    case AVBD_BUF_INIT_LIN: case AVBD_BUF_INERT_LIN: return nb * 16;
+    case AVBD_BUF_PAIRS: case AVBD_BUF_MANIFOLDS: case AVBD_BUF_ADJ_LIST: {
+        Counters c{};
+        cudaStreamSynchronize(s->stream);
+        cudaMemcpy(&c, s->d.counters, sizeof(Counters), cudaMemcpyDeviceToHost);
+        if (which == AVBD_BUF_PAIRS) return (size_t)c.numPairs * 8;
+        if (which == AVBD_BUF_MANIFOLDS) return (size_t)c.numPairs * sizeof(ManifoldGPU);
+        std::vector<uint32_t> dc(nb);
+        cudaMemcpy(dc.data(), s->d.dynCount, 4 * nb, cudaMemcpyDeviceToHost);
+        size_t total = 0;
+        for (size_t b = 0; b < nb; b++) total += H.staticSeg[b].y + H.staticSeg[b].w + dc[b];
+        return total * 4;
+    }
+    case AVBD_BUF_ADJ_START: case AVBD_BUF_ADJ_COUNT: case AVBD_BUF_COLORS: return nb * 4;
+    case AVBD_BUF_COLOR_START: return (MAX_COLORS + 2) * 4;
+    case AVBD_BUF_COLOR_LIST: return (size_t)H.numDynamicBodies * 4;
+    case AVBD_BUF_CELL_START: case AVBD_BUF_CELL_COUNT: return (size_t)H.gridHashSize * 4;
+    case AVBD_BUF_CELL_BODIES: return H.hashedIdx.size() * 4;
+    case AVBD_BUF_MAP_KEY_A: case AVBD_BUF_MAP_KEY_B: case AVBD_BUF_MAP_VAL: return (size_t)H.mapCapacity * 4;
+    case AVBD_BUF_JOINTS: return H.joints.size() * sizeof(JointGPU);
+    case AVBD_BUF_SPRINGS: return H.springs.size() * sizeof(SpringGPU);
+    case AVBD_BUF_TETS: return H.tets.size() * sizeof(TetGPU);
+    case AVBD_BUF_EXCLUSIONS: return H.exclusions.size() * 4;
+    case AVBD_BUF_HASHED_IDX: return H.hashedIdx.size() * 4;
+    case AVBD_BUF_GLOBAL_IDX: return H.globalIdx.size() * 4;
+    default: return 0;
+    }
+}
+
+int avbd_debug_read(avbd_solver* s, int which, void* dst, size_t bytes) {
+    if (!s || !dst) return AVBD_ERR_INVALID_ARGUMENT;
+    if (bytes > avbd_debug_buffer_size(s, which)) return AVBD_ERR_INVALID_ARGUMENT;
+    if (!s->check(cudaStreamSynchronize(s->stream), "debug read")) return AVBD_ERR_RUNTIME_FAILURE;
+    const DevPtrs& d = s->d;
+    const HostScene& H = s->H;
+    const size_t nb = H.numBodies;
+    // the manifolds written by the last frame live in the buffer that is
+    // "previous" for the next frame
+    const bool odd = (s->frame & 1) != 0;
+    const void* src = nullptr;
+    switch (which) {
+    case AVBD_BUF_POS_LIN: src = d.posLin; break;
+    case AVBD_BUF_POS_ANG: src = d.posAng; break;
+    case AVBD_BUF_VEL_LIN: src = d.velLin; break;
+    case AVBD_BUF_VEL_ANG: src = d.velAng; break;
+    case AVBD_BUF_INIT_LIN: src = d.initLin; break;
+    case AVBD_BUF_INERT_LIN: src = d.inertLin; break;
+    case AVBD_BUF_PAIRS: src = d.pairs; break;
+    case AVBD_BUF_MANIFOLDS: src = odd ? d.manifolds : d.prevManifolds; break;
+    case AVBD_BUF_COLORS: src = d.colorsA; break;
+    case AVBD_BUF_COLOR_START: src = d.colorStart; break;
+    case AVBD_BUF_COLOR_LIST: src = d.colorList; break;
+    case AVBD_BUF_CELL_START: src = d.cellStart; break;
+    case AVBD_BUF_CELL_COUNT: src = d.cellCount; break;
+    case AVBD_BUF_CELL_BODIES: src = d.cellBodies; break;
+    case AVBD_BUF_MAP_KEY_A: src = d.mapKeyA; break;
+    case AVBD_BUF_MAP_KEY_B: src = d.mapKeyB; break;
+    case AVBD_BUF_MAP_VAL: src = d.mapVal; break;
+    case AVBD_BUF_JOINTS: src = d.joints; break;
+    case AVBD_BUF_SPRINGS: src = d.springs; break;
+    case AVBD_BUF_TETS: src = d.tets; break;
+    case AVBD_BUF_EXCLUSIONS: src = d.exclusions; break;
+    case AVBD_BUF_HASHED_IDX: src = d.hashedIdx; break;
+    case AVBD_BUF_GLOBAL_IDX: src = d.globalIdx; break;
+    case AVBD_BUF_ADJ_START: case AVBD_BUF_ADJ_COUNT: case AVBD_BUF_ADJ_LIST: {
+        // materialise the merged (pre, contacts, post) lists
+        std::vector<uint32_t> dc(nb), ds(nb);
+        std::vector<uint32_t> dl(2 * (size_t)H.maxPairs);
+        cudaMemcpy(dc.data(), d.dynCount, 4 * nb, cudaMemcpyDeviceToHost);
+        cudaMemcpy(ds.data(), d.dynStart, 4 * nb, cudaMemcpyDeviceToHost);
+        cudaMemcpy(dl.data(), d.dynList, 4 * dl.size(), cudaMemcpyDeviceToHost);
+        std::vector<uint32_t> start(nb), count(nb), list;
+        for (size_t b = 0; b < nb; b++) {
+            const u4 sg = H.staticSeg[b];
+            start[b] = (uint32_t)list.size();
+            count[b] = sg.y + dc[b] + sg.w;
+            list.insert(list.end(), H.preList.begin() + sg.x, H.preList.begin() + sg.x + sg.y);
+            list.insert(list.end(), dl.begin() + ds[b], dl.begin() + ds[b] + dc[b]);
+            list.insert(list.end(), H.postList.begin() + sg.z, H.postList.begin() + sg.z + sg.w);
+        }
+        const std::vector<uint32_t>& v = which == AVBD_BUF_ADJ_START ? start : (which == AVBD_BUF_ADJ_COUNT ? count : list);
+        std::memcpy(dst, v.data(), bytes);
+        return AVBD_OK;
+    }
+    default: return AVBD_ERR_INVALID_ARGUMENT;
+    }
+    if (!src) return AVBD_ERR_INVALID_ARGUMENT;
+    return s->check(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "debug read") ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+}
+
+}  // extern "C"

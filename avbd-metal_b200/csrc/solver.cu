@@ -1,0 +1,974 @@
+// solver.cu — warm start, per-frame adjacency, dynamic coloring, the
+// per-color block-descent primal, the augmented-Lagrangian dual, BDF1
+// finalize and the constraint-error diagnostic.
+//
+// Follows Shaders/40_solver.metal: warm start :546-722, adjacency :27-243,
+// coloring :250-540, force stamps :741-1152 and :1155-1230, the 8-lane
+// primal_particles_split :1544-1684, dual :1729-1906, finalize :2108-2147,
+// diag_error :2189-2229.
+//
+// The primal gives every body of the current color a group of 8 consecutive
+// lanes.  Lane l stamps adjacency entries l, l+8, l+16, ... of the body; the
+// lanes then sum their 6x6 systems with an xor butterfly (offsets 4, 2, 1)
+// and lane 0 solves.  The static part of the adjacency (joints, springs,
+// tets) is built once at upload; only contact entries are rebuilt per frame.
+#include "dmath.cuh"
+#include "kernels.h"
+
+namespace avbd {
+
+constexpr float FLT_BIG = 3.402823466e38f;
+// failure kinds (mirrors AVBD_FAIL_* of include/avbd.h)
+constexpr uint32_t AVBD_FAIL_RIGID_PAIR_CAPACITY_ = 2;
+constexpr uint32_t AVBD_FAIL_UNRESOLVED_COLORING_ = 5;
+
+__device__ __forceinline__ bool body_dynamic(const DevPtrs& d, uint32_t b) {
+    return b != WORLD_BODY && d.posLin[b].w > 0.0f;
+}
+
+static uint32_t stride_blocks(uint32_t upper, int threads) {
+    const uint32_t need = (upper + threads - 1) / threads;
+    const uint32_t cap = 148u * 8u;
+    return need == 0 ? 1u : (need < cap ? need : cap);
+}
+
+// ---------------------------------------------------------------------------
+// Warm start (40_solver.metal:546-722)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float twist_angle(float4 qAr, float4 qB, float3 axis) {
+    float4 r = q_mul(q_inv(qAr), qB);
+    if (r.w < 0.0f) r = neg4(r);
+    return 2.0f * atan2f(dot(xyz(r), axis), r.w);
+}
+
+__global__ void k_warmstart_constraints(const Params P, const DevPtrs d, uint32_t nJ, uint32_t nS) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nJ + nS) return;
+    if (t >= nJ) {
+        SpringGPU& sp = d.springs[d.hardSprings[t - nJ]];
+        const uint32_t a = sp.header.x, b = sp.header.y;
+        const float3 pA = xform(xyz(d.posLin[a]), d.posAng[a], xyz(sp.rA));
+        const float3 pB = xform(xyz(d.posLin[b]), d.posAng[b], xyz(sp.rB));
+        sp.dual.z = 0.5f * mx(len3(pA - pB) - sp.rB.w, 0.0f);
+        float warm = P.alpha * P.gamma;
+        if (P.rodDecayPow > 0.0f) {
+            const float3 dd = pA - pB;
+            const float3 dPrev = dd - (xyz(d.velLin[a]) - xyz(d.velLin[b])) * P.dt;
+            const float dl = len3(dd), dpl = len3(dPrev);
+            if (dl > 1e-7f && dpl > 1e-7f) {
+                const float ct = clampf(dot(dd / dl, dPrev / dpl), 0.0f, 1.0f);
+                warm *= powf(ct, P.rodDecayPow);
+            }
+        }
+        sp.dual.x *= warm;
+        sp.dual.y = mn(clampf(sp.dual.y * P.gamma, PENALTY_MIN, PENALTY_MAX), sp.rA.w);
+        return;
+    }
+    JointGPU& j = d.joints[d.activeJoints[t]];
+    if (j.header.z != 0) return;
+    const uint32_t a = j.header.x, b = j.header.y;
+    const float3 pA = a == WORLD_BODY ? xyz(j.rA) : xform(xyz(d.posLin[a]), d.posAng[a], xyz(j.rA));
+    const float3 pB = xform(xyz(d.posLin[b]), d.posAng[b], xyz(j.rB));
+    const float4 qA = a == WORLD_BODY ? make_float4(0, 0, 0, 1) : d.posAng[a];
+    const float4 qB = d.posAng[b];
+    const float torqueArm = j.C0Lin.w;
+    j.C0Lin = tof4(pA - pB, torqueArm);
+    const float3 axis = xyz(j.hingeAxis);
+    const float4 restRel = tof(j.restRel);
+    float3 c0a;
+    if (j.hingeAxis.w != 0.0f) {
+        const float3 aB = q_rotate(qB, axis);
+        const float3 aA = q_rotate(q_mul(qA, restRel), axis);
+        c0a = cross(aA, aB) * torqueArm;
+        if (j.dynamics.x > 0.0f) {
+            const float twist = twist_angle(q_mul(qA, restRel), qB, axis);
+            const float3 omegaA = a == WORLD_BODY ? s3(0) : xyz(d.velAng[a]);
+            const float twistRate = dot(xyz(d.velAng[b]) - omegaA, aB);
+            j.dynamics.y = twist + P.dt * twistRate;
+        }
+    } else {
+        c0a = q_sub(q_mul(qA, restRel), qB) * torqueArm;
+    }
+    j.C0Ang = tof4(c0a, j.C0Ang.w);
+    if (j.motor.y > 0.0f) {
+        j.motor.z = 0.0f;
+        j.dynamics.z = 0.0f;
+        const uint32_t mode = j.header.w & MOTOR_MODE_MASK;
+        if (mode == MOTOR_EXPLICIT || mode == MOTOR_VELOCITY) {
+            const float4 qAr = a == WORLD_BODY ? restRel : q_mul(d.posAng[a], restRel);
+            const float twist = twist_angle(qAr, qB, axis);
+            const float3 axisW = q_rotate(qB, axis);
+            const float3 omegaA = a == WORLD_BODY ? s3(0) : xyz(d.velAng[a]);
+            const float twistRate = dot(xyz(d.velAng[b]) - omegaA, axisW);
+            if (mode == MOTOR_VELOCITY)
+                j.dynamics.z = clampf(j.limits.z * (j.motor.x - twistRate), -j.motor.y, j.motor.y);
+            else
+                j.dynamics.z = clampf(j.motor.w * (j.motor.x - twist) - j.limits.z * twistRate, -j.motor.y, j.motor.y);
+        }
+    }
+    const float warm = P.alpha * P.gamma;
+    j.lambdaLin.x *= warm; j.lambdaLin.y *= warm; j.lambdaLin.z *= warm;
+    j.lambdaAng.x *= warm; j.lambdaAng.y *= warm; j.lambdaAng.z *= warm;
+    float3 pl = clamp3(xyz(j.penaltyLin) * P.gamma, s3(PENALTY_MIN), s3(PENALTY_MAX));
+    float3 pa = clamp3(xyz(j.penaltyAng) * P.gamma, s3(PENALTY_MIN), s3(PENALTY_MAX));
+    pl = mn3(pl, s3(j.rA.w));
+    pa = mn3(pa, s3(j.rB.w));
+    j.penaltyLin = tof4(pl, j.penaltyLin.w);
+    j.penaltyAng = tof4(pa, j.penaltyAng.w);
+}
+
+__global__ void k_warmstart_bodies(const Params P, const DevPtrs d) {
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= P.numBodies) return;
+    const float4 pl = d.posLin[gid], pa = d.posAng[gid];
+    const float mass = pl.w, dt = P.dt;
+    const float3 vl = xyz(d.velLin[gid]), va = xyz(d.velAng[gid]);
+    float3 inertial = xyz(pl) + vl * dt;
+    const float bodyGravity = P.gravity * d.gravityScale[gid];
+    if (mass > 0.0f) inertial += mk3(0, 0, bodyGravity) * (dt * dt);
+    d.inertLin[gid] = mk4(inertial, 0.0f);
+    d.inertAng[gid] = q_addw(pa, va * dt);
+    const float3 accel = (vl - xyz(d.prevVelLin[gid])) / dt;
+    const float gsign = P.gravity < 0.0f ? -1.0f : (P.gravity > 0.0f ? 1.0f : 0.0f);
+    float w = clampf(accel.z * gsign / fabsf(P.gravity), 0.0f, 1.0f);
+    if (!isfinite(w)) w = 0.0f;
+    d.initLin[gid] = mk4(xyz(pl), 0.0f);
+    d.initAng[gid] = pa;
+    if (mass > 0.0f) {
+        // Isotropic-OGC warm-start truncation is a no-op while every bound is
+        // "far" (no element contact emitted a bound), which holds for every
+        // scene this build accepts.
+        const float3 guess = xyz(pl) + vl * dt + mk3(0, 0, bodyGravity) * (w * dt * dt);
+        d.posLin[gid] = mk4(guess, mass);
+        d.posAng[gid] = q_addw(pa, va * dt);
+    }
+}
+
+void launch_warmstart(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    const uint32_t n = z.numActiveJoints + z.numHardSprings;
+    if (n) k_warmstart_constraints<<<(n + 127) / 128, 128, 0, st>>>(P, d, z.numActiveJoints, z.numHardSprings);
+    k_warmstart_bodies<<<(P.numBodies + 127) / 128, 128, 0, st>>>(P, d);
+}
+
+// ---------------------------------------------------------------------------
+// Per-frame contact adjacency: count, scan, scatter, sort per body.
+// ---------------------------------------------------------------------------
+__global__ void k_adj_dyn_count(const DevPtrs d) {
+    const uint32_t n = d.counters->numPairs;
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+        const u4 h = d.manifolds[m].header;
+        if (h.z == 0) continue;
+        if (body_dynamic(d, h.x)) atomicAdd(&d.dynCount[h.x], 1u);
+        if (body_dynamic(d, h.y)) atomicAdd(&d.dynCount[h.y], 1u);
+    }
+}
+__global__ void k_adj_dyn_scatter(const DevPtrs d) {
+    const uint32_t n = d.counters->numPairs;
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
+        const u4 h = d.manifolds[m].header;
+        if (h.z == 0) continue;
+        const uint32_t e = (FK_MANIFOLD << ADJ_KIND_SHIFT) | m;
+        if (body_dynamic(d, h.x)) d.dynList[atomicAdd(&d.dynCursor[h.x], 1u)] = e;
+        if (body_dynamic(d, h.y)) d.dynList[atomicAdd(&d.dynCursor[h.y], 1u)] = e;
+    }
+}
+__global__ void k_adj_dyn_sort(const DevPtrs d, uint32_t nb) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    uint32_t* l = d.dynList + d.dynStart[b];
+    const uint32_t n = d.dynCount[b];
+    for (uint32_t i = 1; i < n; i++) {
+        const uint32_t v = l[i];
+        uint32_t j = i;
+        while (j > 0 && l[j - 1] > v) { l[j] = l[j - 1]; j--; }
+        l[j] = v;
+    }
+}
+
+void launch_adjacency(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    cudaMemsetAsync(d.dynCount, 0, sizeof(uint32_t) * P.numBodies, st);
+    k_adj_dyn_count<<<stride_blocks(z.maxPairs, 128), 128, 0, st>>>(d);
+    launch_exclusive_scan(d.dynCount, d.dynStart, P.numBodies, d.scanScratch, st);
+    cudaMemcpyAsync(d.dynCursor, d.dynStart, sizeof(uint32_t) * P.numBodies, cudaMemcpyDeviceToDevice, st);
+    k_adj_dyn_scatter<<<stride_blocks(z.maxPairs, 128), 128, 0, st>>>(d);
+    k_adj_dyn_sort<<<(P.numBodies + 127) / 128, 128, 0, st>>>(d, P.numBodies);
+}
+
+// Adjacency entry k of a body in ascending order: static pre (joints,
+// springs), this frame's manifolds, static post (tets).
+struct AdjView {
+    const uint32_t* pre; uint32_t nPre;
+    const uint32_t* dyn; uint32_t nDyn;
+    const uint32_t* post; uint32_t nPost;
+    __device__ __forceinline__ uint32_t count() const { return nPre + nDyn + nPost; }
+    __device__ __forceinline__ uint32_t at(uint32_t k) const {
+        if (k < nPre) return pre[k];
+        k -= nPre;
+        if (k < nDyn) return dyn[k];
+        return post[k - nDyn];
+    }
+};
+__device__ __forceinline__ AdjView adj_view(const DevPtrs& d, uint32_t b) {
+    const uint4 s = d.staticSeg[b];
+    AdjView v;
+    v.pre = d.preList + s.x; v.nPre = s.y;
+    v.dyn = d.dynList + d.dynStart[b]; v.nDyn = d.dynCount[b];
+    v.post = d.postList + s.z; v.nPost = s.w;
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// Dynamic coloring for rigid-only scenes (40_solver.metal:250-540)
+// ---------------------------------------------------------------------------
+__device__ void neighbor_colors(const DevPtrs& d, uint32_t entry, uint32_t self, uint32_t myColor,
+                                const uint32_t* colorsIn, uint32_t& maskLo, uint32_t& maskHi,
+                                uint32_t& allLo, uint32_t& allHi, bool& conflict) {
+    const uint32_t kind = entry >> ADJ_KIND_SHIFT, idx = entry & ADJ_INDEX_MASK;
+    uint32_t nbs[3];
+    uint32_t n = 0;
+    if (kind == FK_TET) {
+        const u4 ids = d.tets[idx].ids;
+        if (ids.x != self && n < 3) nbs[n++] = ids.x;
+        if (ids.y != self && n < 3) nbs[n++] = ids.y;
+        if (ids.z != self && n < 3) nbs[n++] = ids.z;
+        if (ids.w != self && n < 3) nbs[n++] = ids.w;
+    } else {
+        uint32_t a, b;
+        if (kind == FK_JOINT) { a = d.joints[idx].header.x; b = d.joints[idx].header.y; }
+        else if (kind == FK_SPRING) { a = d.springs[idx].header.x; b = d.springs[idx].header.y; }
+        else { a = d.manifolds[idx].header.x; b = d.manifolds[idx].header.y; }
+        nbs[0] = a == self ? b : a;
+        n = 1;
+    }
+    for (uint32_t k = 0; k < n; k++) {
+        const uint32_t nb = nbs[k];
+        if (nb == WORLD_BODY || d.posLin[nb].w <= 0.0f) continue;
+        const uint32_t c = colorsIn[nb];
+        const uint32_t lo = c < 32 ? (1u << c) : 0u;
+        const uint32_t hi = (c >= 32 && c < 64) ? (1u << (c - 32)) : 0u;
+        allLo |= lo; allHi |= hi;
+        if (nb < self) { maskLo |= lo; maskHi |= hi; if (c == myColor) conflict = true; }
+    }
+}
+
+__device__ __forceinline__ void scan_neighbors(const DevPtrs& d, uint32_t b, uint32_t my, const uint32_t* colors,
+                                               uint32_t& mLo, uint32_t& mHi, uint32_t& aLo, uint32_t& aHi,
+                                               bool& conflict) {
+    const AdjView v = adj_view(d, b);
+    const uint32_t n = v.count();
+    for (uint32_t k = 0; k < n; k++) neighbor_colors(d, v.at(k), b, my, colors, mLo, mHi, aLo, aHi, conflict);
+}
+
+__device__ __forceinline__ uint32_t ctz32(uint32_t x) { return (uint32_t)(__ffs((int)x) - 1); }
+
+__global__ void k_color_iterate(const Params P, const DevPtrs d, const uint32_t* src, uint32_t* dst, uint32_t pass) {
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= P.numBodies) return;
+    if (pass > 0 && d.counters->changed[pass - 1] == 0u) return;
+    if (d.posLin[gid].w <= 0.0f) { dst[gid] = 0; return; }
+    const uint32_t my = src[gid];
+    uint32_t mLo = 0, mHi = 0, aLo = 0, aHi = 0;
+    bool conflict = false;
+    scan_neighbors(d, gid, my, src, mLo, mHi, aLo, aHi, conflict);
+    if (conflict) {
+        const uint32_t freeLo = ~mLo;
+        uint32_t nc;
+        if (freeLo != 0) nc = ctz32(freeLo);
+        else { const uint32_t freeHi = ~mHi; nc = freeHi != 0 ? 32 + ctz32(freeHi) : (MAX_COLORS - 1); }
+        dst[gid] = nc < (uint32_t)(MAX_COLORS - 1) ? nc : (uint32_t)(MAX_COLORS - 1);
+        atomicOr(&d.counters->changed[pass], 1u);
+    } else {
+        const uint32_t freeLo = ~aLo;
+        const uint32_t best = freeLo != 0 ? ctz32(freeLo) : (~aHi != 0 ? 32 + ctz32(~aHi) : my);
+        dst[gid] = best < my ? best : my;
+        if (best < my) atomicOr(&d.counters->changed[pass], 1u);
+    }
+}
+
+// Serial greedy completion when the bounded parallel phase has not settled.
+__global__ void k_color_repair(const Params P, const DevPtrs d, uint32_t* colors, uint32_t finalPass) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    if (d.counters->changed[finalPass] == 0u) return;
+    for (uint32_t self = 0; self < P.numBodies; self++) {
+        if (d.posLin[self].w <= 0.0f) { colors[self] = 0; continue; }
+        uint32_t mLo = 0, mHi = 0, aLo = 0, aHi = 0;
+        bool conflict = false;
+        scan_neighbors(d, self, colors[self], colors, mLo, mHi, aLo, aHi, conflict);
+        const uint32_t freeLo = ~mLo;
+        if (freeLo != 0) colors[self] = ctz32(freeLo);
+        else { const uint32_t freeHi = ~mHi; colors[self] = freeHi != 0 ? 32 + ctz32(freeHi) : (MAX_COLORS - 1); }
+    }
+}
+
+__global__ void k_color_validate_count(const Params P, const DevPtrs d, const uint32_t* colors) {
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= P.numBodies || d.posLin[gid].w <= 0.0f) return;
+    uint32_t mLo = 0, mHi = 0, aLo = 0, aHi = 0;
+    bool conflict = false;
+    scan_neighbors(d, gid, colors[gid], colors, mLo, mHi, aLo, aHi, conflict);
+    if (conflict) atomicAdd(&d.counters->colorConflicts, 1u);
+    d.bodySlot[gid] = atomicAdd(&d.counters->colorCount[colors[gid]], 1u);
+}
+
+__global__ void k_color_scan(const DevPtrs d) {
+    if (threadIdx.x != 0) return;
+    uint32_t run = 0, used = 0;
+    for (int c = 0; c < MAX_COLORS; c++) {
+        d.counters->colorStart[c] = run;
+        const uint32_t n = d.counters->colorCount[c];
+        run += n;
+        if (n > 0) used = c + 1;
+    }
+    d.counters->colorStart[MAX_COLORS] = run;
+    d.counters->colorStart[MAX_COLORS + 1] = used;
+    d.counters->usedColors = used;
+}
+
+__global__ void k_color_scatter(const Params P, const DevPtrs d, const uint32_t* colors) {
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= P.numBodies || d.posLin[gid].w <= 0.0f) return;
+    d.colorList[d.counters->colorStart[colors[gid]] + d.bodySlot[gid]] = gid;
+}
+
+void launch_dynamic_coloring(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    const int T = 128;
+    const uint32_t blocks = (P.numBodies + T - 1) / T;
+    const int passes = 20;
+    for (int pass = 0; pass < passes; pass++) {
+        const uint32_t* src = (pass & 1) ? d.colorsB : d.colorsA;
+        uint32_t* dst = (pass & 1) ? d.colorsA : d.colorsB;
+        k_color_iterate<<<blocks, T, 0, st>>>(P, d, src, dst, (uint32_t)pass);
+    }
+    k_color_repair<<<1, 1, 0, st>>>(P, d, d.colorsA, passes - 1);
+    k_color_validate_count<<<blocks, T, 0, st>>>(P, d, d.colorsA);
+    k_color_scan<<<1, 32, 0, st>>>(d);
+    k_color_scatter<<<blocks, T, 0, st>>>(P, d, d.colorsA);
+}
+
+// ---------------------------------------------------------------------------
+// Force stamps (40_solver.metal:733-1230)
+// ---------------------------------------------------------------------------
+struct Accum { M3 lhsLin, lhsAng, lhsCross; float3 rhsLin, rhsAng; };
+
+__device__ __forceinline__ M3 geom_stiff_ball_socket(int k, float3 v) {
+    M3 m = m3_diag(s3(-comp(v, k)));
+    if (k == 0) { m.r0.x += v.x; m.r1.x += v.y; m.r2.x += v.z; }
+    else if (k == 1) { m.r0.y += v.x; m.r1.y += v.y; m.r2.y += v.z; }
+    else { m.r0.z += v.x; m.r1.z += v.y; m.r2.z += v.z; }
+    return m;
+}
+__device__ __forceinline__ float wrap_pi(float x) {
+    return x - 6.2831853f * floorf((x + 3.14159265f) / 6.2831853f);
+}
+
+__device__ void stamp_joint(const Params& P, const DevPtrs& d, const JointGPU& j, uint32_t self, Accum& acc) {
+    const uint32_t a = j.header.x, b = j.header.y;
+    const bool isA = self == a;
+    const float torqueArm = j.C0Lin.w;
+    const float3 penLin = xyz(j.penaltyLin);
+    const float4 qBb = d.posAng[b];
+    if (dot(penLin, penLin) > 0.0f) {
+        const float3 pA = a == WORLD_BODY ? xyz(j.rA) : xform(xyz(d.posLin[a]), d.posAng[a], xyz(j.rA));
+        const float3 pB = xform(xyz(d.posLin[b]), qBb, xyz(j.rB));
+        float3 C = pA - pB;
+        if (j.header.w & 1) C -= xyz(j.C0Lin) * P.alpha;
+        const float3 F = penLin * C + xyz(j.lambdaLin);
+        const float jsign = isA ? 1.0f : -1.0f;
+        const float3 rW = isA ? q_rotate(d.posAng[a], xyz(j.rA)) : q_rotate(qBb, xyz(j.rB));
+        const M3 jAng = m3_skew(-jsign * rW);
+        const M3 jAngT = m3_transpose(jAng);
+        const M3 K = m3_diag(penLin);
+        const M3 jAngTk = m3_mulm(jAngT, K);
+        acc.lhsLin = m3_add(acc.lhsLin, K);
+        acc.lhsAng = m3_add(acc.lhsAng, m3_mulm(jAngTk, jAng));
+        acc.lhsCross = m3_add(acc.lhsCross, m3_scale(jAngTk, jsign));
+        const float3 r = jsign * rW;
+        const M3 H = m3_add(m3_add(m3_scale(geom_stiff_ball_socket(0, r), F.x),
+                                   m3_scale(geom_stiff_ball_socket(1, r), F.y)),
+                            m3_scale(geom_stiff_ball_socket(2, r), F.z));
+        acc.lhsAng = m3_add(acc.lhsAng, m3_diagonalize(H));
+        acc.rhsLin += jsign * F;
+        acc.rhsAng += m3_mul(jAngT, F);
+    }
+    const float3 penAng = xyz(j.penaltyAng);
+    if (dot(penAng, penAng) > 0.0f) {
+        const float4 qA = a == WORLD_BODY ? make_float4(0, 0, 0, 1) : d.posAng[a];
+        const float4 restRel = tof(j.restRel);
+        float3 C = q_sub(q_mul(qA, restRel), qBb) * torqueArm;
+        const float s = (isA ? 1.0f : -1.0f) * torqueArm;
+        if (j.hingeAxis.w != 0.0f) {
+            const float3 axis = xyz(j.hingeAxis);
+            const float3 aB = q_rotate(qBb, axis);
+            const float3 aA = q_rotate(q_mul(qA, restRel), axis);
+            C = cross(aA, aB) * torqueArm;
+            if (j.header.w & 2) C -= xyz(j.C0Ang) * P.alpha;
+            const float3 F = penAng * C + xyz(j.lambdaAng);
+            const float alignment = dot(aA, aB);
+            M3 J = isA ? m3_add(m3_outer(aA, aB), m3_scale(m3_identity(), -alignment))
+                       : m3_add(m3_scale(m3_identity(), alignment), m3_scale(m3_outer(aB, aA), -1.0f));
+            J = m3_scale(J, torqueArm);
+            const M3 JT = m3_transpose(J);
+            const M3 K = m3_diag(penAng);
+            acc.lhsAng = m3_add(acc.lhsAng, m3_mulm(m3_mulm(JT, K), J));
+            acc.rhsAng += m3_mul(JT, F);
+            if (j.motor.y > 0.0f || j.limits.x < j.limits.y) {
+                const float twist = twist_angle(q_mul(qA, restRel), qBb, axis);
+                if (j.dynamics.x > 0.0f) {
+                    const float Ca = wrap_pi(twist - j.dynamics.y);
+                    const float ka = j.dynamics.x / mx(P.dt * P.dt, 1e-12f);
+                    const float sm = (self == a) ? -1.0f : 1.0f;
+                    acc.lhsAng = m3_add(acc.lhsAng, m3_scale(m3_outer(aB, aB), ka));
+                    acc.rhsAng += aB * (ka * Ca * sm);
+                }
+                if (j.limits.x < j.limits.y) {
+                    const float over = mx(twist - j.limits.y, 0.0f) + mn(twist - j.limits.x, 0.0f);
+                    if (over != 0.0f) {
+                        const float kL = 4.0e4f;
+                        const float FL = clampf(kL * over, -3000.0f, 3000.0f);
+                        const float sm = (self == a) ? -1.0f : 1.0f;
+                        acc.lhsAng = m3_add(acc.lhsAng, m3_scale(m3_outer(aB, aB), kL));
+                        acc.rhsAng += aB * (FL * sm);
+                    }
+                }
+                if (j.motor.y > 0.0f) {
+                    const float sm = (self == a) ? -1.0f : 1.0f;
+                    const uint32_t mode = j.header.w & MOTOR_MODE_MASK;
+                    if (mode == MOTOR_EXPLICIT || mode == MOTOR_VELOCITY) {
+                        acc.rhsAng += aB * (-j.dynamics.z * sm);
+                    } else {
+                        const float Cm = wrap_pi(twist - j.motor.x);
+                        const float4 qA0 = a == WORLD_BODY ? make_float4(0, 0, 0, 1) : d.initAng[a];
+                        const float twist0 = twist_angle(q_mul(qA0, restRel), d.initAng[b], axis);
+                        const float dTwist = wrap_pi(twist - twist0);
+                        const float cD = j.limits.z / mx(P.dt, 1e-6f);
+                        const float raw = j.motor.w * Cm + cD * dTwist;
+                        const float effort = clampf(raw, -j.motor.y, j.motor.y);
+                        if (fabsf(raw) < j.motor.y)
+                            acc.lhsAng = m3_add(acc.lhsAng, m3_scale(m3_outer(aB, aB), j.motor.w + cD));
+                        acc.rhsAng += aB * (effort * sm);
+                    }
+                }
+            }
+        } else {
+            if (j.header.w & 2) C -= xyz(j.C0Ang) * P.alpha;
+            const float3 F = penAng * C + xyz(j.lambdaAng);
+            acc.lhsAng = m3_add(acc.lhsAng, m3_diag(penAng * (s * s)));
+            acc.rhsAng += F * s;
+        }
+    }
+}
+
+__device__ void stamp_spring(const Params& P, const DevPtrs& d, const SpringGPU& sp, uint32_t self, Accum& acc) {
+    const uint32_t a = sp.header.x, b = sp.header.y;
+    float stiffness = sp.rA.w;
+    const float rest = sp.rB.w;
+    const float3 pA = xform(xyz(d.posLin[a]), d.posAng[a], xyz(sp.rA));
+    const float3 pB = xform(xyz(d.posLin[b]), d.posAng[b], xyz(sp.rB));
+    const float3 dd = pA - pB;
+    const float dLen = len3(dd);
+    if (dLen <= 1.0e-6f) return;
+    const float3 n = dd / dLen;
+    float f;
+    if (sp.header.z != 0) {
+        const float C = dLen - rest - sp.dual.z * P.alpha;
+        stiffness = sp.dual.y;
+        f = stiffness * C + sp.dual.x;
+        if (f <= 0.0f) return;
+    } else {
+        f = stiffness * (dLen - rest);
+    }
+    const bool isA = self == a;
+    const float3 rW = isA ? q_rotate(d.posAng[a], xyz(sp.rA)) : q_rotate(d.posAng[b], xyz(sp.rB));
+    const float3 jLin = isA ? n : -n;
+    const float3 jAng = isA ? cross(rW, n) : -cross(rW, n);
+    acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(jLin, jLin), stiffness));
+    acc.lhsAng = m3_add(acc.lhsAng, m3_scale(m3_outer(jAng, jAng), stiffness));
+    acc.lhsCross = m3_add(acc.lhsCross, m3_scale(m3_outer(jAng, jLin), stiffness));
+    acc.rhsLin += jLin * f;
+    acc.rhsAng += jAng * f;
+    const float ft = mx(f, 0.0f) / dLen;
+    if (ft > 0.0f) acc.lhsLin = m3_add(acc.lhsLin, m3_add(m3_diag(s3(ft)), m3_scale(m3_outer(n, n), -ft)));
+}
+
+// Stable Neo-Hookean tet, VBD per-vertex Hessian (40_solver.metal:966-1020).
+__device__ void stamp_tet(const DevPtrs& d, const TetGPU& t, uint32_t self, Accum& acc) {
+    const float3 x0 = xyz(d.posLin[t.ids.x]), x1 = xyz(d.posLin[t.ids.y]);
+    const float3 x2 = xyz(d.posLin[t.ids.z]), x3 = xyz(d.posLin[t.ids.w]);
+    const float muV = t.r1.w, lamV = t.r2.w;
+    const float alphaT = 1.0f + muV / mx(lamV, 1e-9f);
+    const float3 d0 = x1 - x0, d1 = x2 - x0, d2 = x3 - x0;
+    const float3 m0 = xyz(t.r0), m1 = xyz(t.r1), m2 = xyz(t.r2);
+    const float3 f0 = d0 * m0.x + d1 * m1.x + d2 * m2.x;
+    const float3 f1 = d0 * m0.y + d1 * m1.y + d2 * m2.y;
+    const float3 f2 = d0 * m0.z + d1 * m1.z + d2 * m2.z;
+    const float J = dot(f0, cross(f1, f2));
+    const float3 j0 = cross(f1, f2), j1 = cross(f2, f0), j2 = cross(f0, f1);
+    const float s2 = lamV * (J - alphaT);
+    const float3 p0 = muV * f0 + s2 * j0;
+    const float3 p1 = muV * f1 + s2 * j1;
+    const float3 p2 = muV * f2 + s2 * j2;
+    float3 w;
+    if (self == t.ids.y) w = m0;
+    else if (self == t.ids.z) w = m1;
+    else if (self == t.ids.w) w = m2;
+    else w = -mk3(m0.x + m1.x + m2.x, m0.y + m1.y + m2.y, m0.z + m1.z + m2.z);
+    const float3 grad = p0 * w.x + p1 * w.y + p2 * w.z;
+    const float3 g = j0 * w.x + j1 * w.y + j2 * w.z;
+    acc.rhsLin += grad;
+    acc.lhsLin = m3_add(acc.lhsLin, m3_diag(s3(muV * dot(w, w))));
+    acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(g, g), lamV));
+}
+
+// Linearised contact constraint and its cone-projected force.
+__device__ __forceinline__ float3 contact_force(const ContactGPU& c, float3 nrm, float3 t1, float3 t2,
+                                                float dynF, float statF, float alpha,
+                                                float3 dqALin, float3 dqAAng, float3 dqBLin, float3 dqBAng,
+                                                float3 rAW, float3 rBW, float3& Cout, float& fs, float& bounds) {
+    float3 C = xyz(c.C0) * (1.0f - alpha);
+    C += mk3(dot(nrm, dqALin), dot(t1, dqALin), dot(t2, dqALin));
+    C -= mk3(dot(nrm, dqBLin), dot(t1, dqBLin), dot(t2, dqBLin));
+    C += mk3(dot(cross(rAW, nrm), dqAAng), dot(cross(rAW, t1), dqAAng), dot(cross(rAW, t2), dqAAng));
+    C -= mk3(dot(cross(rBW, nrm), dqBAng), dot(cross(rBW, t1), dqBAng), dot(cross(rBW, t2), dqBAng));
+    float3 F = xyz(c.penalty) * C + xyz(c.lambda);
+    F.x = mn(F.x, 0.0f);
+    bounds = fabsf(F.x) * statF;
+    fs = sqrtf(F.y * F.y + F.z * F.z);
+    if (fs > bounds && fs > 0.0f) {
+        const float db = fabsf(F.x) * dynF;
+        const float sc = db / fs;
+        F.y *= sc;
+        F.z *= sc;
+    }
+    Cout = C;
+    return F;
+}
+
+__device__ void stamp_manifold(const Params& P, const DevPtrs& d, const ManifoldGPU& m, uint32_t self, Accum& acc) {
+    const u4 h = m.header;
+    const uint32_t a = h.x, b = h.y, n = h.z;
+    const bool isA = self == a;
+    const bool sphA = (h.w & 2u) != 0, sphB = (h.w & 4u) != 0;
+    const float4 qa = d.posAng[a], qb = d.posAng[b];
+    const float3 dqALin = xyz(d.posLin[a]) - xyz(d.initLin[a]);
+    const float3 dqAAng = q_sub(qa, d.initAng[a]);
+    const float3 dqBLin = xyz(d.posLin[b]) - xyz(d.initLin[b]);
+    const float3 dqBAng = q_sub(qb, d.initAng[b]);
+    const float3 nrm = xyz(m.basisN), t1 = xyz(m.basisT1), t2 = cross(nrm, t1);
+    const float dynF = m.basisN.w, statF = m.basisT1.w;
+    for (uint32_t i = 0; i < n; i++) {
+        const ContactGPU c = m.contacts[i];
+        const float3 rAW = sphA ? xyz(c.rA) : q_rotate(qa, xyz(c.rA));
+        const float3 rBW = sphB ? xyz(c.rB) : q_rotate(qb, xyz(c.rB));
+        float3 C;
+        float fs, bnd;
+        const float3 F = contact_force(c, nrm, t1, t2, dynF, statF, P.alpha, dqALin, dqAAng, dqBLin, dqBAng,
+                                       rAW, rBW, C, fs, bnd);
+        const float s = isA ? 1.0f : -1.0f;
+        const M3 jLin = M3{nrm * s, t1 * s, t2 * s};
+        const float3 rW = isA ? rAW : rBW;
+        const M3 jAng = M3{cross(rW, jLin.r0), cross(rW, jLin.r1), cross(rW, jLin.r2)};
+        const M3 K = m3_diag(xyz(c.penalty));
+        const M3 jLinT = m3_transpose(jLin), jAngT = m3_transpose(jAng);
+        const M3 jAngTk = m3_mulm(jAngT, K);
+        acc.lhsLin = m3_add(acc.lhsLin, m3_mulm(m3_mulm(jLinT, K), jLin));
+        acc.lhsAng = m3_add(acc.lhsAng, m3_mulm(jAngTk, jAng));
+        acc.lhsCross = m3_add(acc.lhsCross, m3_mulm(jAngTk, jLin));
+        acc.rhsLin += m3_mul(jLinT, F);
+        acc.rhsAng += m3_mul(jAngT, F);
+    }
+}
+
+__device__ __forceinline__ void stamp_entry(const Params& P, const DevPtrs& d, uint32_t entry, uint32_t body,
+                                            Accum& acc) {
+    const uint32_t kind = entry >> ADJ_KIND_SHIFT, idx = entry & ADJ_INDEX_MASK;
+    if (kind == FK_TET) stamp_tet(d, d.tets[idx], body, acc);
+    else if (kind == FK_MANIFOLD) stamp_manifold(P, d, d.manifolds[idx], body, acc);
+    else if (kind == FK_JOINT) stamp_joint(P, d, d.joints[idx], body, acc);
+    else if (kind == FK_SPRING) stamp_spring(P, d, d.springs[idx], body, acc);
+}
+
+__device__ __forceinline__ float3 shfl3(unsigned mask, float3 v, int o) {
+    return mk3(__shfl_xor_sync(mask, v.x, o, 8), __shfl_xor_sync(mask, v.y, o, 8), __shfl_xor_sync(mask, v.z, o, 8));
+}
+__device__ __forceinline__ void add_shfl3(unsigned mask, float3& v, int o) { v = v + shfl3(mask, v, o); }
+
+// One body on an 8-lane group; lane 0 writes the result.
+__device__ void primal_body(const Params& P, const DevPtrs& d, uint32_t body, uint32_t lane, unsigned mask) {
+    const float4 shp = d.shape[body];
+    const bool rigid = shp.w >= 0.0f;
+    Accum acc{m3_zero(), m3_zero(), m3_zero(), s3(0), s3(0)};
+    const AdjView v = adj_view(d, body);
+    const uint32_t cnt = v.count();
+    for (uint32_t k = lane; k < cnt; k += 8) stamp_entry(P, d, v.at(k), body, acc);
+#pragma unroll
+    for (int o = 4; o >= 1; o >>= 1) {
+        add_shfl3(mask, acc.lhsLin.r0, o);
+        add_shfl3(mask, acc.lhsLin.r1, o);
+        add_shfl3(mask, acc.lhsLin.r2, o);
+        add_shfl3(mask, acc.rhsLin, o);
+        if (rigid) {
+            add_shfl3(mask, acc.lhsAng.r0, o);
+            add_shfl3(mask, acc.lhsAng.r1, o);
+            add_shfl3(mask, acc.lhsAng.r2, o);
+            add_shfl3(mask, acc.lhsCross.r0, o);
+            add_shfl3(mask, acc.lhsCross.r1, o);
+            add_shfl3(mask, acc.lhsCross.r2, o);
+            add_shfl3(mask, acc.rhsAng, o);
+        }
+    }
+    if (lane != 0) return;
+    const float4 pl = d.posLin[body];
+    const float mass = pl.w;
+    const float dt2 = P.dt * P.dt;
+    acc.lhsLin = m3_add(acc.lhsLin, m3_diag(s3(mass / dt2)));
+    acc.rhsLin += (xyz(pl) - xyz(d.inertLin[body])) * (mass / dt2);
+    float3 dxLin = s3(0), dxAng = s3(0);
+    if (rigid) {
+        const float4 q = d.posAng[body];
+        const M3 inertia = m3_scale(world_inertia(q, xyz(d.props[body])), 1.0f / dt2);
+        acc.lhsAng = m3_add(acc.lhsAng, inertia);
+        acc.rhsAng += m3_mul(inertia, q_sub(q, d.inertAng[body]));
+        solve6x6(acc.lhsLin, acc.lhsAng, acc.lhsCross, -acc.rhsLin, -acc.rhsAng, dxLin, dxAng);
+        if (!finite3(dxLin) || !finite3(dxAng)) return;
+        const float ang2 = dot(dxAng, dxAng);
+        const float maxAng = 0.5f;
+        if (ang2 > maxAng * maxAng) dxAng *= maxAng * rsq(ang2);
+    } else {
+        solve6x6(acc.lhsLin, m3_identity(), m3_zero(), -acc.rhsLin, s3(0), dxLin, dxAng);
+        if (!finite3(dxLin)) return;
+    }
+    const float maxLin = 0.35f * fabsf(shp.w);
+    const float lin2 = dot(dxLin, dxLin);
+    if (lin2 > maxLin * maxLin) dxLin *= maxLin * rsq(lin2);
+    // Isotropic OGC truncation needs an emitted conservative bound; with no
+    // element contacts every bound is "far" and the step is unchanged.
+    d.posLin[body] = mk4(xyz(pl) + dxLin, mass);
+    if (rigid) d.posAng[body] = q_addw(d.posAng[body], dxAng);
+}
+
+__global__ void k_primal(const Params P, const DevPtrs d, uint32_t color, uint32_t count) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t slot = tid >> 3, lane = tid & 7u;
+    const uint32_t s = d.colorStart[color];
+    const uint32_t n = count != 0xFFFFFFFFu ? count : d.colorStart[color + 1] - s;
+    if (slot >= n) return;                      // uniform across the 8-lane group
+    const unsigned mask = 0xFFu << (threadIdx.x & 24u);
+    primal_body(P, d, d.colorList[s + slot], lane, mask);
+}
+
+void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color, uint32_t count,
+                         cudaStream_t st) {
+    const int T = 128;
+    const uint32_t upper = count != 0xFFFFFFFFu ? count : z.numDynamicBodies;
+    if (upper == 0) return;
+    k_primal<<<(upper * 8 + T - 1) / T, T, 0, st>>>(P, d, color, count);
+}
+
+// ---------------------------------------------------------------------------
+// Dual (40_solver.metal:1729-1906)
+// ---------------------------------------------------------------------------
+__device__ void dual_joint(const Params& P, const DevPtrs& d, uint32_t gid) {
+    JointGPU& j = d.joints[gid];
+    if (j.header.z != 0) return;
+    const uint32_t a = j.header.x, b = j.header.y;
+    const float torqueArm = j.C0Lin.w, stiffLin = j.rA.w, stiffAng = j.rB.w;
+    const float3 penLin = xyz(j.penaltyLin);
+    if (dot(penLin, penLin) > 0.0f) {
+        const float3 pA = a == WORLD_BODY ? xyz(j.rA) : xform(xyz(d.posLin[a]), d.posAng[a], xyz(j.rA));
+        const float3 pB = xform(xyz(d.posLin[b]), d.posAng[b], xyz(j.rB));
+        float3 C = pA - pB;
+        if (j.header.w & 1) {
+            C -= xyz(j.C0Lin) * P.alpha;
+            const float3 l = clamp3(penLin * C + xyz(j.lambdaLin), s3(-P.lambdaMax), s3(P.lambdaMax));
+            j.lambdaLin = tof4(l, j.lambdaLin.w);
+        }
+        const float cap = mn(stiffLin, PENALTY_MAX);
+        j.penaltyLin = tof4(mn3(penLin + abs3(C) * P.betaLin, s3(cap)), j.penaltyLin.w);
+    }
+    const float3 penAng = xyz(j.penaltyAng);
+    if (dot(penAng, penAng) > 0.0f) {
+        const float4 qA = a == WORLD_BODY ? make_float4(0, 0, 0, 1) : d.posAng[a];
+        const float4 restRel = tof(j.restRel);
+        float3 C;
+        if (j.hingeAxis.w != 0.0f) {
+            const float3 axis = xyz(j.hingeAxis);
+            const float3 aB = q_rotate(d.posAng[b], axis);
+            const float3 aA = q_rotate(q_mul(qA, restRel), axis);
+            C = cross(aA, aB) * torqueArm;
+        } else {
+            C = q_sub(q_mul(qA, restRel), d.posAng[b]) * torqueArm;
+        }
+        if (j.header.w & 2) {
+            C -= xyz(j.C0Ang) * P.alpha;
+            const float3 l = clamp3(penAng * C + xyz(j.lambdaAng), s3(-P.lambdaMax), s3(P.lambdaMax));
+            j.lambdaAng = tof4(l, j.lambdaAng.w);
+        }
+        const float cap = mn(stiffAng, PENALTY_MAX);
+        j.penaltyAng = tof4(mn3(penAng + abs3(C) * P.betaAng, s3(cap)), j.penaltyAng.w);
+    }
+    const float fracture = j.C0Ang.w;
+    const float3 la = xyz(j.lambdaAng);
+    const float3 ll = xyz(j.lambdaLin);
+    const float lin2 = (j.header.w & 8) ? dot(ll, ll) : 0.0f;
+    if ((j.header.w & 4) && dot(la, la) + lin2 > fracture * fracture) {
+        j.penaltyLin = f4{0, 0, 0, 0};
+        j.penaltyAng = f4{0, 0, 0, 0};
+        j.lambdaLin = f4{0, 0, 0, 0};
+        j.lambdaAng = f4{0, 0, 0, 0};
+        j.header.z = 1;
+    }
+}
+
+__device__ void dual_spring(const Params& P, const DevPtrs& d, uint32_t si) {
+    SpringGPU& sp = d.springs[si];
+    const uint32_t a = sp.header.x, b = sp.header.y;
+    const float3 pA = xform(xyz(d.posLin[a]), d.posAng[a], xyz(sp.rA));
+    const float3 pB = xform(xyz(d.posLin[b]), d.posAng[b], xyz(sp.rB));
+    const float C = len3(pA - pB) - sp.rB.w - sp.dual.z * P.alpha;
+    const float mA = d.posLin[a].w, mB = d.posLin[b].w;
+    const float mMin = mn(mA > 0.0f ? mA : FLT_BIG, mB > 0.0f ? mB : FLT_BIG);
+    const float cap = mn(P.lambdaMax, mx(2.0f, 5.0e3f * mMin));
+    sp.dual.x = clampf(0.98f * sp.dual.x + sp.dual.y * C, 0.0f, cap);
+    if (C > 0.0f) sp.dual.y = mn(sp.dual.y + C * P.betaLin, mn(sp.rA.w, PENALTY_MAX));
+}
+
+__device__ void dual_manifold(const Params& P, const DevPtrs& d, uint32_t gid) {
+    ManifoldGPU& m = d.manifolds[gid];
+    const u4 h = m.header;
+    const uint32_t n = h.z;
+    if (n == 0) return;
+    const uint32_t a = h.x, b = h.y;
+    const bool sphA = (h.w & 2u) != 0, sphB = (h.w & 4u) != 0;
+    const float4 pa4 = d.posLin[a], pb4 = d.posLin[b], qa = d.posAng[a], qb = d.posAng[b];
+    const float3 dqALin = xyz(pa4) - xyz(d.initLin[a]);
+    const float3 dqAAng = q_sub(qa, d.initAng[a]);
+    const float3 dqBLin = xyz(pb4) - xyz(d.initLin[b]);
+    const float3 dqBAng = q_sub(qb, d.initAng[b]);
+    const float minMass = mn(pa4.w > 0.0f ? pa4.w : FLT_BIG, pb4.w > 0.0f ? pb4.w : FLT_BIG);
+    const float lamCap = mn(P.lambdaMax, mx(10.0f, 1.0e5f * minMass));
+    const float3 nrm = xyz(m.basisN), t1 = xyz(m.basisT1), t2 = cross(nrm, t1);
+    const float dynF = m.basisN.w, statF = m.basisT1.w;
+    for (uint32_t i = 0; i < n; i++) {
+        ContactGPU& c = m.contacts[i];
+        const float3 rAW = sphA ? xyz(c.rA) : q_rotate(qa, xyz(c.rA));
+        const float3 rBW = sphB ? xyz(c.rB) : q_rotate(qb, xyz(c.rB));
+        float3 C;
+        float fs, bounds;
+        float3 F = contact_force(c, nrm, t1, t2, dynF, statF, P.alpha, dqALin, dqAAng, dqBLin, dqBAng,
+                                 rAW, rBW, C, fs, bounds);
+        F.x = mx(F.x, -lamCap);
+        c.lambda = tof4(F, 0.0f);
+        float3 pen = xyz(c.penalty);
+        if (F.x < 0.0f) pen.x = mn(pen.x + P.betaLin * fabsf(C.x), PENALTY_MAX);
+        if (fs <= bounds) {
+            pen.y = mn(pen.y + P.betaLin * fabsf(C.y), PENALTY_MAX_T);
+            pen.z = mn(pen.z + P.betaLin * fabsf(C.z), PENALTY_MAX_T);
+            c.rB.w = sqrtf(C.y * C.y + C.z * C.z) < STICK_THRESH ? 1.0f : 0.0f;
+        }
+        c.penalty = tof4(pen, 0.0f);
+    }
+}
+
+__device__ __forceinline__ void dual_item(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t g,
+                                          uint32_t numPairs) {
+    if (g < z.numActiveJoints) { dual_joint(P, d, d.activeJoints[g]); return; }
+    g -= z.numActiveJoints;
+    if (g < z.numHardSprings) { dual_spring(P, d, d.hardSprings[g]); return; }
+    g -= z.numHardSprings;
+    if (g < numPairs) dual_manifold(P, d, g);
+}
+
+__global__ void k_dual(const Params P, const DevPtrs d, const Sizes z) {
+    const uint32_t total = z.numActiveJoints + z.numHardSprings + d.counters->numPairs;
+    const uint32_t numPairs = d.counters->numPairs;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x)
+        dual_item(P, d, z, g, numPairs);
+}
+
+void launch_dual(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    k_dual<<<stride_blocks(z.numActiveJoints + z.numHardSprings + z.maxPairs, 128), 128, 0, st>>>(P, d, z);
+}
+
+// ---------------------------------------------------------------------------
+// Small scenes: the whole iteration loop in one thread block.  Colors and the
+// dual are separated by __syncthreads(), which orders the same way as the
+// per-color launches.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_solve_small(const Params P, const DevPtrs d, const Sizes z,
+                                                     uint32_t colorBound) {
+    const uint32_t groups = blockDim.x >> 3;
+    const uint32_t group = threadIdx.x >> 3, lane = threadIdx.x & 7u;
+    const unsigned mask = 0xFFu << (threadIdx.x & 24u);
+    for (uint32_t it = 0; it < P.iterations; it++) {
+        for (uint32_t c = 0; c < colorBound; c++) {
+            const uint32_t s = d.colorStart[c], e = d.colorStart[c + 1];
+            if (s == e) continue;                // block-uniform
+            for (uint32_t slot = group; s + slot < e; slot += groups)
+                primal_body(P, d, d.colorList[s + slot], lane, mask);
+            __syncthreads();
+        }
+        const uint32_t numPairs = d.counters->numPairs;
+        const uint32_t total = z.numActiveJoints + z.numHardSprings + numPairs;
+        for (uint32_t g = threadIdx.x; g < total; g += blockDim.x) dual_item(P, d, z, g, numPairs);
+        __syncthreads();
+    }
+}
+
+void launch_solve_small(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t colorBound, cudaStream_t st) {
+    k_solve_small<<<1, 256, 0, st>>>(P, d, z, colorBound);
+}
+
+// ---------------------------------------------------------------------------
+// BDF1 velocity finalize (40_solver.metal:2108-2147)
+// ---------------------------------------------------------------------------
+__global__ void k_finalize(const Params P, const DevPtrs d) {
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= P.numBodies) return;
+    const float4 vold = d.velLin[gid];
+    d.prevVelLin[gid] = vold;
+    const float4 pl = d.posLin[gid];
+    if (pl.w <= 0.0f) return;
+    const float4 shp = d.shape[gid];
+    const float3 oldV = xyz(vold);
+    float3 v = (xyz(pl) - xyz(d.initLin[gid])) / P.dt;
+    const float s2 = dot(v, v);
+    if (s2 > P.maxSpeed * P.maxSpeed) v *= P.maxSpeed * rsq(s2);
+    if (shp.w < 0.0f && P.particleDamping > 0.0f) {
+        const float3 ballistic = oldV + mk3(0, 0, P.gravity * d.gravityScale[gid]) * P.dt;
+        v = ballistic + (v - ballistic) / (1.0f + P.particleDamping * P.dt);
+    }
+    if (shp.w >= 0.0f && P.rigidLinearDamping > 0.0f) v *= expf(-P.rigidLinearDamping * P.dt);
+    float3 omega = q_sub(d.posAng[gid], d.initAng[gid]) / P.dt;
+    if (shp.w >= 0.0f && P.rigidAngularDamping > 0.0f) omega *= expf(-P.rigidAngularDamping * P.dt);
+    d.velLin[gid] = mk4(v, 0.0f);
+    d.velAng[gid] = mk4(omega, 0.0f);
+}
+
+void launch_finalize(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    k_finalize<<<(P.numBodies + 127) / 128, 128, 0, st>>>(P, d);
+}
+
+// ---------------------------------------------------------------------------
+// max joint violation / contact penetration (40_solver.metal:2189-2229).
+// Manifolds were swapped at frame end: the last frame's are prevManifolds.
+// ---------------------------------------------------------------------------
+__global__ void k_diag(const Params P, const DevPtrs d, const Sizes z) {
+    const uint32_t numPairs = d.counters->numPairs;
+    const uint32_t total = P.numJoints + numPairs;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        float err = 0.0f;
+        if (g < P.numJoints) {
+            const JointGPU& j = d.joints[g];
+            if (!(j.header.z == 0 && (j.rA.w > 0.0f || j.rB.w > 0.0f))) continue;
+            const uint32_t a = j.header.x, b = j.header.y;
+            const float3 pA = a == WORLD_BODY ? xyz(j.rA) : xform(xyz(d.posLin[a]), d.posAng[a], xyz(j.rA));
+            const float3 pB = xform(xyz(d.posLin[b]), d.posAng[b], xyz(j.rB));
+            err = len3(pA - pB);
+        } else {
+            const ManifoldGPU& m = d.prevManifolds[g - P.numJoints];
+            const u4 h = m.header;
+            const bool sphA = (h.w & 2u) != 0, sphB = (h.w & 4u) != 0;
+            for (uint32_t i = 0; i < h.z; i++) {
+                const float3 xA = sphA ? xyz(d.posLin[h.x]) + xyz(m.contacts[i].rA)
+                                       : xform(xyz(d.posLin[h.x]), d.posAng[h.x], xyz(m.contacts[i].rA));
+                const float3 xB = sphB ? xyz(d.posLin[h.y]) + xyz(m.contacts[i].rB)
+                                       : xform(xyz(d.posLin[h.y]), d.posAng[h.y], xyz(m.contacts[i].rB));
+                const float pen = dot(xyz(m.basisN), xA - xB) + P.collisionMargin;
+                err = mx(err, mx(0.0f, -pen));
+            }
+        }
+        atomicMax(reinterpret_cast<uint32_t*>(d.diag), __float_as_uint(err));
+    }
+}
+
+void launch_max_constraint_error(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    cudaMemsetAsync(d.diag, 0, sizeof(float), st);
+    k_diag<<<stride_blocks(P.numJoints + z.maxPairs, 128), 128, 0, st>>>(P, d, z);
+}
+
+// ---------------------------------------------------------------------------
+// set_body_states: clear the AL state of every constraint incident to a
+// reset body (GPUSolver.swift:2429-2471).
+// ---------------------------------------------------------------------------
+__global__ void k_reset_incident(const Params P, const DevPtrs d, const Sizes z) {
+    const uint32_t total = P.numJoints + P.numSprings + 2 * z.maxPairs;
+    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        if (g < P.numJoints) {
+            JointGPU& j = d.joints[g];
+            const uint32_t a = j.header.x, b = j.header.y;
+            if (d.resetFlags[b] || (a != WORLD_BODY && d.resetFlags[a])) {
+                j.lambdaLin = f4{0, 0, 0, 0};
+                j.lambdaAng = f4{0, 0, 0, 0};
+                j.motor.z = 0.0f;
+                j.dynamics.y = 0.0f;
+                j.dynamics.z = 0.0f;
+                j.penaltyLin = tof4(d.initPenLin[g]);
+                j.penaltyAng = tof4(d.initPenAng[g]);
+            }
+            continue;
+        }
+        g -= P.numJoints;
+        if (g < P.numSprings) {
+            SpringGPU& sp = d.springs[g];
+            if (d.resetFlags[sp.header.x] || d.resetFlags[sp.header.y]) sp.dual = f4{0, 0, 0, 0};
+            continue;
+        }
+        g -= P.numSprings;
+        ManifoldGPU* buf = g < z.maxPairs ? d.manifolds : d.prevManifolds;
+        const uint32_t m = g < z.maxPairs ? g : g - z.maxPairs;
+        const u4 h = buf[m].header;
+        const bool hitA = h.x < P.numBodies && d.resetFlags[h.x];
+        const bool hitB = h.y < P.numBodies && d.resetFlags[h.y];
+        if (hitA || hitB) {
+            uint4* w = reinterpret_cast<uint4*>(&buf[m]);
+            for (int k = 0; k < (int)(sizeof(ManifoldGPU) / 16); k++) w[k] = make_uint4(0, 0, 0, 0);
+        }
+    }
+}
+
+void launch_reset_bodies(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    k_reset_incident<<<stride_blocks(P.numJoints + P.numSprings + 2 * z.maxPairs, 128), 128, 0, st>>>(P, d, z);
+}
+
+// ---------------------------------------------------------------------------
+// End of frame: kinematic spinners and legacy rate motors advance only after
+// a complete frame (GPUSolver.swift:4359-4363, :4407-4427), then the frame's
+// counters are checked and the first failure is latched with its frame index
+// (the checks of `retire`, GPUSolver.swift:2885-2918).
+// ---------------------------------------------------------------------------
+__global__ void k_frame_end(const Params P, const DevPtrs d, const Sizes z, float dt) {
+    const uint32_t t = threadIdx.x;
+    for (uint32_t i = t; i < d.numRateMotors; i += blockDim.x) {
+        JointGPU& j = d.joints[d.rateJoint[i]];
+        float target = j.motor.x + d.rateValue[i] * dt;
+        target -= 6.28318530717958647692f * roundf(target / 6.28318530717958647692f);
+        j.motor.x = target;
+    }
+    for (uint32_t i = t; i < d.numSpinners; i += blockDim.x) {
+        const uint32_t b = d.spinnerBody[i];
+        const float4 ao = d.spinnerAxisOmega[i];
+        const float half = 0.5f * ao.w * dt;
+        const float sn = sinf(half);
+        const float4 dq = make_float4(ao.x * sn, ao.y * sn, ao.z * sn, cosf(half));
+        const float4 nq = q_mul(dq, d.posAng[b]);
+        d.posAng[b] = nq / sqrtf(dot4(nq, nq));
+    }
+    if (t == 0) {
+        const uint32_t frame = d.frameCounter[0] + 1u;
+        d.frameCounter[0] = frame;
+        uint32_t kind = 0, detail = 0;
+        if (d.counters->pairCandidates > P.maxPairs) { kind = AVBD_FAIL_RIGID_PAIR_CAPACITY_; detail = d.counters->pairCandidates; }
+        else if (z.dynamicColoring && d.counters->colorConflicts > 0) { kind = AVBD_FAIL_UNRESOLVED_COLORING_; detail = d.counters->colorConflicts; }
+        if (kind != 0 && d.failureLatch[0] == 0u) {
+            d.failureLatch[0] = kind;
+            d.failureLatch[1] = frame;
+            d.failureLatch[2] = detail;
+        }
+    }
+}
+
+void launch_frame_end(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    k_frame_end<<<1, 64, 0, st>>>(P, d, z, P.dt);
+}
+
+}  // namespace avbd

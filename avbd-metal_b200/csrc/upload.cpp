@@ -1,0 +1,474 @@
+// upload.cpp — scene upload on the host (GPUSolver.swift:338-638, :901-2081).
+//
+// Computes per-body mass/inertia/radius, collider partition and cell size,
+// the joint/spring/tet records, the sorted collision-exclusion list, the tet
+// boundary surface groups, the static topology palette for soft scenes and
+// the static part of the per-body adjacency.  Compiled with
+// -ffp-contract=off so every float matches a plain float32 evaluation.
+#include "upload.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <map>
+#include <set>
+
+namespace avbd {
+namespace {
+
+struct V3 { float x, y, z; };
+inline V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+inline V3 add(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 sub(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 mul(V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; }
+inline V3 divs(V3 a, float s) { return V3{a.x / s, a.y / s, a.z / s}; }
+inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) { return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline float length(V3 a) { return std::sqrt(dot(a, a)); }
+inline float fmin_(float a, float b) { return a < b ? a : b; }
+inline float fmax_(float a, float b) { return a > b ? a : b; }
+inline V3 from(const float* p) { return V3{p[0], p[1], p[2]}; }
+
+inline f4 qmul(f4 a, f4 b) {
+    return f4{a.w * b.x + a.x * b.w + a.y * b.z - a.z * b.y,
+              a.w * b.y - a.x * b.z + a.y * b.w + a.z * b.x,
+              a.w * b.z + a.x * b.y - a.y * b.x + a.z * b.w,
+              a.w * b.w - a.x * b.x - a.y * b.y - a.z * b.z};
+}
+inline float dot4(f4 a, f4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+inline f4 qinv(f4 q) { float d = dot4(q, q); return f4{-q.x / d, -q.y / d, -q.z / d, q.w / d}; }
+inline V3 qrot(f4 q, V3 v) {
+    V3 u{q.x, q.y, q.z};
+    V3 c = cross(u, v);
+    V3 t{2.0f * c.x, 2.0f * c.y, 2.0f * c.z};
+    V3 wt{q.w * t.x, q.w * t.y, q.w * t.z};
+    return add(add(v, wt), cross(u, t));
+}
+
+uint32_t next_pow2(uint32_t v) { uint32_t p = 1; while (p < v) p <<= 1; return p; }
+
+bool desc_dynamic(const avbd_body_desc& b) {
+    return b.has_explicit_mass ? b.mass > 0.0f : b.density > 0.0f;
+}
+
+float collider_radius(const avbd_collider_desc& c) {
+    V3 sz = from(c.size);
+    if (c.shape == AVBD_SHAPE_SPHERE) return sz.x / 2.0f;
+    if (c.shape == AVBD_SHAPE_TORUS) return sz.x + sz.y;
+    if (c.shape == AVBD_SHAPE_CAPSULE) return sz.x / 2.0f + sz.y;
+    return length(mul(sz, 0.5f));
+}
+
+// Faces owned by exactly one tet, wound outward, in sorted order
+// (GPUSolver.swift:875-897).
+std::vector<std::array<int, 3>> boundary_faces(const avbd_scene_desc* s) {
+    std::vector<std::array<int, 3>> out;
+    if (s->num_tets == 0) return out;
+    struct Face { std::array<int, 3> tri; int opp; int count; };
+    std::map<std::array<int, 3>, Face> faces;
+    static const int order[4][4] = {{0, 1, 2, 3}, {0, 1, 3, 2}, {0, 2, 3, 1}, {1, 2, 3, 0}};
+    for (uint32_t t = 0; t < s->num_tets; t++) {
+        const int32_t* ids = s->tets[t].ids;
+        for (const auto& f : order) {
+            std::array<int, 3> tri{ids[f[0]], ids[f[1]], ids[f[2]]};
+            std::array<int, 3> key = tri;
+            std::sort(key.begin(), key.end());
+            auto it = faces.find(key);
+            if (it != faces.end()) it->second.count++;
+            else faces.emplace(key, Face{tri, ids[f[3]], 1});
+        }
+    }
+    for (const auto& kv : faces) {
+        if (kv.second.count != 1) continue;
+        int a = kv.second.tri[0], b = kv.second.tri[1], c = kv.second.tri[2];
+        V3 A = from(s->bodies[a].position), B = from(s->bodies[b].position), Cp = from(s->bodies[c].position);
+        V3 n = cross(sub(B, A), sub(Cp, A));
+        if (dot(n, sub(from(s->bodies[kv.second.opp].position), A)) > 0.0f) std::swap(b, c);
+        out.push_back({a, b, c});
+    }
+    std::sort(out.begin(), out.end());
+    return out;
+}
+
+}  // namespace
+
+int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
+    if (!s || s->abi_version != AVBD_ABI_VERSION) { err = "bad scene descriptor or ABI version"; return AVBD_ERR_INVALID_ARGUMENT; }
+    if (s->num_bodies > 0 && !s->bodies) { err = "null body array"; return AVBD_ERR_INVALID_ARGUMENT; }
+    if (!(s->settings.dt > 0.0f) || s->settings.iterations < 0) { err = "dt must be positive and iterations non-negative"; return AVBD_ERR_INVALID_ARGUMENT; }
+    const uint32_t nb = s->num_bodies, nc = s->num_colliders;
+    for (uint32_t i = 0; i < nc; i++) {
+        const avbd_collider_desc& c = s->colliders[i];
+        if (c.body < 0 || (uint32_t)c.body >= nb) { err = "collider owner out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
+        if (c.collision_enabled && (c.hull_count > 0 || c.shape == AVBD_SHAPE_TORUS || c.shape == AVBD_SHAPE_CAPSULE)) {
+            err = "torus, capsule and convex-hull colliders are not supported by this build";
+            return AVBD_ERR_UNSUPPORTED;
+        }
+    }
+    if (s->num_tris > 0) { err = "cloth triangles are not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+    for (uint32_t i = 0; i < s->num_joints; i++) {
+        const avbd_joint_desc& j = s->joints[i];
+        if (j.body_b < 0 || (uint32_t)j.body_b >= nb || j.body_a >= (int32_t)nb || j.body_a < -1) { err = "joint body out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
+        if (j.motor_torque > 0.0f && !j.has_hinge) { err = "a powered joint must define a hinge axis"; return AVBD_ERR_INVALID_ARGUMENT; }
+    }
+    for (uint32_t i = 0; i < s->num_springs; i++) {
+        const avbd_spring_desc& p = s->springs[i];
+        if (p.body_a < 0 || p.body_b < 0 || (uint32_t)p.body_a >= nb || (uint32_t)p.body_b >= nb) { err = "spring body out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
+    }
+    for (uint32_t i = 0; i < s->num_tets; i++)
+        for (int k = 0; k < 4; k++)
+            if (s->tets[i].ids[k] < 0 || (uint32_t)s->tets[i].ids[k] >= nb) { err = "tet vertex out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
+
+    H.numBodies = nb;
+    H.numColliders = nc;
+    uint32_t enabled = 0;
+    for (uint32_t i = 0; i < nc; i++) enabled += s->colliders[i].collision_enabled ? 1u : 0u;
+    const uint32_t mppb = s->max_pairs_per_body ? s->max_pairs_per_body : 16u;
+    H.maxPairs = std::max<uint32_t>(4096u, enabled * mppb);
+    H.mapCapacity = next_pow2(2 * H.maxPairs);
+    H.gridHashSize = next_pow2(std::max<uint32_t>(64u, 2u * std::max<uint32_t>(1u, enabled)));
+    std::vector<std::array<int, 3>> boundary = boundary_faces(s);
+    H.numTris = (uint32_t)boundary.size();
+
+    // ---- bodies (GPUSolver.swift:915-969)
+    H.posLin.assign(nb, f4{}); H.posAng.assign(nb, f4{}); H.velLin.assign(nb, f4{});
+    H.velAng.assign(nb, f4{}); H.prevVelLin.assign(nb, f4{}); H.props.assign(nb, f4{});
+    H.shape.assign(nb, f4{}); H.spinVel.assign(nb, f4{});
+    H.gravityScale.assign(nb, 1.0f); H.shapeType.assign(nb, 0); H.clothGroup.assign(nb, 0);
+    H.isDynamic.assign(nb, 0);
+    const float PI = 3.14159265358979323846f;
+    H.numDynamicBodies = 0;
+    for (uint32_t i = 0; i < nb; i++) {
+        const avbd_body_desc& b = s->bodies[i];
+        V3 size = from(b.size);
+        float mass, radius;
+        V3 moment;
+        if (b.shape == AVBD_SHAPE_BOX) {
+            mass = b.density > 0.0f ? size.x * size.y * size.z * b.density : 0.0f;
+            moment = V3{(size.y * size.y + size.z * size.z) / 12.0f * mass,
+                        (size.x * size.x + size.z * size.z) / 12.0f * mass,
+                        (size.x * size.x + size.y * size.y) / 12.0f * mass};
+            radius = length(mul(size, 0.5f));
+        } else if (b.shape == AVBD_SHAPE_SPHERE) {
+            float r = size.x / 2.0f;
+            mass = b.density > 0.0f ? 4.0f / 3.0f * PI * r * r * r * b.density : 0.0f;
+            float m = 0.4f * mass * r * r;
+            moment = V3{m, m, m};
+            radius = r;
+        } else if (b.shape == AVBD_SHAPE_TORUS) {
+            float R = size.x, r = size.y;
+            mass = b.density > 0.0f ? 2.0f * PI * PI * R * r * r * b.density : 0.0f;
+            float iDia = mass * (R * R / 2.0f + 5.0f * r * r / 8.0f);
+            float iAxis = mass * (R * R + 3.0f * r * r / 4.0f);
+            moment = V3{iDia, iDia, iAxis};
+            radius = R + r;
+        } else {
+            float L = size.x, r = size.y;
+            mass = b.density > 0.0f ? PI * r * r * (L + 4.0f * r / 3.0f) * b.density : 0.0f;
+            float iAxis = 0.5f * mass * r * r;
+            float iPerp = mass * (L * L / 12.0f + r * r / 4.0f);
+            moment = V3{iPerp, iPerp, iAxis};
+            radius = L / 2.0f + r;
+        }
+        if (b.has_explicit_mass) { mass = b.mass; moment = from(b.diagonal_inertia); }
+        H.posLin[i] = f4{b.position[0], b.position[1], b.position[2], mass};
+        H.posAng[i] = f4{b.rotation[0], b.rotation[1], b.rotation[2], b.rotation[3]};
+        H.velLin[i] = f4{b.velocity[0], b.velocity[1], b.velocity[2], 0.0f};
+        H.prevVelLin[i] = H.velLin[i];
+        H.props[i] = f4{moment.x, moment.y, moment.z, b.friction};
+        H.shape[i] = f4{size.x, size.y, size.z, b.is_particle ? -radius : radius};
+        H.gravityScale[i] = b.gravity_scale;
+        H.shapeType[i] = b.shape;
+        H.isDynamic[i] = desc_dynamic(b) ? 1 : 0;
+        if (mass > 0.0f) H.numDynamicBodies++;
+    }
+
+    // ---- colliders and broadphase partition (GPUSolver.swift:971-1089)
+    H.colOwner.assign(nc, 0); H.colShapeType.assign(nc, 0); H.colGroup.assign(nc, 0);
+    H.colShared.assign(nc, 0); H.colShape.assign(nc, f4{}); H.colLocalPos.assign(nc, f4{});
+    H.colLocalRot.assign(nc, f4{}); H.colFriction.assign(2 * nc, 0.0f);
+    std::vector<float> radii;
+    for (uint32_t i = 0; i < nc; i++) {
+        const avbd_collider_desc& c = s->colliders[i];
+        float r = collider_radius(c);
+        bool particle = s->bodies[c.body].is_particle != 0;
+        H.colOwner[i] = (uint32_t)c.body;
+        H.colGroup[i] = c.collision_group;
+        H.colShared[i] = c.collides_with_shared ? 1u : 0u;
+        H.colShape[i] = f4{c.size[0], c.size[1], c.size[2], particle ? -r : r};
+        H.colLocalPos[i] = f4{c.local_position[0], c.local_position[1], c.local_position[2], c.friction};
+        H.colLocalRot[i] = f4{c.local_rotation[0], c.local_rotation[1], c.local_rotation[2], c.local_rotation[3]};
+        H.colFriction[2 * i] = c.friction;
+        H.colFriction[2 * i + 1] = c.dynamic_friction;
+        uint32_t flags = c.shape;
+        if (particle) flags |= SHAPE_PARTICLE;
+        if (c.world_round_anchor) flags |= COLLIDER_WORLD_ROUND_ANCHOR;
+        H.colShapeType[i] = flags;
+        if (c.collision_enabled && H.isDynamic[c.body]) radii.push_back(r);
+    }
+    std::vector<float> sorted = radii;
+    std::sort(sorted.begin(), sorted.end());
+    const float median = sorted.empty() ? 0.5f : sorted[sorted.size() / 2];
+    const float threshold = median * 4.0f;
+    bool isolated = false;
+    for (uint32_t i = 0; i < nc; i++)
+        if (s->colliders[i].collision_enabled && s->colliders[i].collision_group != 0) isolated = true;
+    for (uint32_t i = 0; i < nc; i++) {
+        const avbd_collider_desc& c = s->colliders[i];
+        if (!c.collision_enabled) continue;
+        if (collider_radius(c) > threshold || (isolated && c.collision_group == 0)) H.globalIdx.push_back(i);
+        else H.hashedIdx.push_back(i);
+    }
+    float maxHashedRadius = 0.05f;
+    uint32_t numHashedRigid = 0;
+    for (uint32_t i : H.hashedIdx) {
+        maxHashedRadius = fmax_(maxHashedRadius, std::fabs(H.colShape[i].w));
+        if (!s->bodies[s->colliders[i].body].is_particle) numHashedRigid++;
+    }
+
+    // ---- joints (GPUSolver.swift:1092-1195)
+    const uint32_t nj = s->num_joints;
+    H.joints.assign(nj, JointGPU{});
+    const float dt = s->settings.dt;
+    for (uint32_t i = 0; i < nj; i++) {
+        const avbd_joint_desc& j = s->joints[i];
+        JointGPU g{};
+        uint32_t aIdx = j.body_a >= 0 ? (uint32_t)j.body_a : WORLD_BODY;
+        uint32_t flags = 0;
+        if (std::isinf(j.stiffness_lin)) flags |= 1;
+        if (std::isinf(j.stiffness_ang)) flags |= 2;
+        if (std::isfinite(j.fracture)) flags |= 4;
+        if (j.fracture_linear) flags |= 8;
+        g.header = u4{aIdx, (uint32_t)j.body_b, 0, flags};
+        const float bigK = 3.0e10f;
+        g.rA = f4{j.r_a[0], j.r_a[1], j.r_a[2], fmin_(j.stiffness_lin, bigK)};
+        g.rB = f4{j.r_b[0], j.r_b[1], j.r_b[2], fmin_(j.stiffness_ang, bigK)};
+        V3 sizeA = j.body_a >= 0 ? from(s->bodies[j.body_a].size) : V3{0, 0, 0};
+        V3 ss = add(sizeA, from(s->bodies[j.body_b].size));
+        g.C0Lin = f4{0, 0, 0, dot(ss, ss)};
+        g.C0Ang = f4{0, 0, 0, fmin_(j.fracture, 3.0e18f)};
+        f4 qA0 = j.body_a >= 0 ? H.posAng[j.body_a] : f4{0, 0, 0, 1};
+        f4 rel = qmul(qinv(qA0), H.posAng[j.body_b]);
+        float rl = std::sqrt(dot4(rel, rel));
+        g.restRel = f4{rel.x / rl, rel.y / rl, rel.z / rl, rel.w / rl};
+        if (j.has_hinge) {
+            g.hingeAxis = f4{j.hinge_axis[0], j.hinge_axis[1], j.hinge_axis[2], 1.0f};
+            g.dynamics.x = j.armature;
+            if (j.motor_torque > 0.0f) {
+                g.motor = f4{j.motor_target, j.motor_torque, 0.0f, j.motor_stiffness};
+                g.limits = f4{j.limit_lo, j.limit_hi, j.motor_damping, 0.0f};
+                if (j.motor_mode == AVBD_MOTOR_IMPLICIT_POSITION_PD) g.header.w |= MOTOR_IMPLICIT;
+                else if (j.motor_mode == AVBD_MOTOR_EXPLICIT_TORQUE_PD) g.header.w |= MOTOR_EXPLICIT;
+                else g.header.w |= MOTOR_VELOCITY;
+                if (j.motor_rate != 0.0f) H.rateMotors.push_back({i, j.motor_rate});
+            }
+            if (j.limit_lo < j.limit_hi && j.motor_torque == 0.0f) g.limits = f4{j.limit_lo, j.limit_hi, 0.0f, 0.0f};
+        }
+        float massA = j.body_a >= 0 ? H.posLin[j.body_a].w : 0.0f;
+        float massB = H.posLin[j.body_b].w;
+        float eff = 0.0f;
+        bool have = false;
+        for (float m : {massA, massB}) if (m > 0.0f) { eff = have ? fmin_(eff, m) : m; have = true; }
+        float floorK = fmin_(1.0e9f, fmax_(1.0f, eff / fmax_(dt * dt, 1.0e-12f)));
+        if (std::isinf(j.stiffness_lin)) g.penaltyLin = f4{floorK, floorK, floorK, floorK};
+        if (std::isinf(j.stiffness_ang)) g.penaltyAng = f4{floorK, floorK, floorK, floorK};
+        if (j.stiffness_lin > 0.0f && std::isfinite(j.stiffness_lin)) { float k = fmin_(j.stiffness_lin, 1e9f); g.penaltyLin = f4{k, k, k, k}; }
+        if (j.stiffness_ang > 0.0f && std::isfinite(j.stiffness_ang)) { float k = fmin_(j.stiffness_ang, 1e9f); g.penaltyAng = f4{k, k, k, k}; }
+        H.joints[i] = g;
+        // A joint with zero stiffness and no motor is an exclusion marker: no
+        // stage ever reads it (adjacency skips it, its penalties warm-start
+        // to zero so the dual is a no-op, and it is never breakable in effect).
+        bool inert = g.rA.w == 0.0f && g.rB.w == 0.0f && g.motor.y == 0.0f;
+        if (!inert) H.activeJoints.push_back(i);
+    }
+    H.initPenLin.resize(nj); H.initPenAng.resize(nj);
+    for (uint32_t i = 0; i < nj; i++) { H.initPenLin[i] = H.joints[i].penaltyLin; H.initPenAng[i] = H.joints[i].penaltyAng; }
+
+    // ---- springs (GPUSolver.swift:1197-1212)
+    H.springs.assign(s->num_springs, SpringGPU{});
+    for (uint32_t i = 0; i < s->num_springs; i++) {
+        const avbd_spring_desc& sp = s->springs[i];
+        SpringGPU g{};
+        g.header = u4{(uint32_t)sp.body_a, (uint32_t)sp.body_b, sp.hard ? 1u : 0u, 0};
+        float rest = sp.rest;
+        if (rest < 0.0f) {
+            V3 pA = add(qrot(H.posAng[sp.body_a], from(sp.r_a)), V3{H.posLin[sp.body_a].x, H.posLin[sp.body_a].y, H.posLin[sp.body_a].z});
+            V3 pB = add(qrot(H.posAng[sp.body_b], from(sp.r_b)), V3{H.posLin[sp.body_b].x, H.posLin[sp.body_b].y, H.posLin[sp.body_b].z});
+            rest = length(sub(pA, pB));
+        }
+        g.rA = f4{sp.r_a[0], sp.r_a[1], sp.r_a[2], sp.stiffness};
+        g.rB = f4{sp.r_b[0], sp.r_b[1], sp.r_b[2], rest};
+        H.springs[i] = g;
+        if (sp.hard) H.hardSprings.push_back(i);
+    }
+
+    // ---- tets (GPUSolver.swift:1214-1235): rows of Dm^-1 via the adjugate
+    H.tets.assign(s->num_tets, TetGPU{});
+    for (uint32_t i = 0; i < s->num_tets; i++) {
+        const avbd_tet_desc& t = s->tets[i];
+        auto P3 = [&](int id) { return V3{H.posLin[id].x, H.posLin[id].y, H.posLin[id].z}; };
+        V3 x0 = P3(t.ids[0]);
+        V3 d0 = sub(P3(t.ids[1]), x0), d1 = sub(P3(t.ids[2]), x0), d2 = sub(P3(t.ids[3]), x0);
+        float six = dot(d0, cross(d1, d2));
+        float vol = std::fabs(six) / 6.0f;
+        V3 r0 = divs(cross(d1, d2), six), r1 = divs(cross(d2, d0), six), r2 = divs(cross(d0, d1), six);
+        TetGPU g{};
+        g.ids = u4{(uint32_t)t.ids[0], (uint32_t)t.ids[1], (uint32_t)t.ids[2], (uint32_t)t.ids[3]};
+        g.r0 = f4{r0.x, r0.y, r0.z, six};
+        g.r1 = f4{r1.x, r1.y, r1.z, t.mu * vol};
+        g.r2 = f4{r2.x, r2.y, r2.z, t.lambda * vol};
+        H.tets[i] = g;
+    }
+
+    // ---- collision exclusions (GPUSolver.swift:1265-1287)
+    std::vector<uint64_t> ex;
+    auto key = [](int a, int b) { return ((uint64_t)std::min(a, b) << 32) | (uint64_t)std::max(a, b); };
+    for (uint32_t i = 0; i < nj; i++) if (s->joints[i].body_a >= 0) ex.push_back(key(s->joints[i].body_a, s->joints[i].body_b));
+    for (uint32_t i = 0; i < s->num_springs; i++) ex.push_back(key(s->springs[i].body_a, s->springs[i].body_b));
+    for (uint32_t i = 0; i < s->num_exclusions; i++) ex.push_back(key(s->exclusions[i].body_a, s->exclusions[i].body_b));
+    std::sort(ex.begin(), ex.end());
+    ex.erase(std::unique(ex.begin(), ex.end()), ex.end());
+    for (uint64_t k : ex) { H.exclusions.push_back((uint32_t)(k >> 32)); H.exclusions.push_back((uint32_t)k); }
+
+    // ---- collision-surface groups of tet boundaries (GPUSolver.swift:1461-1535)
+    if (!boundary.empty()) {
+        std::vector<int> parent(nb, -1);
+        auto find = [&](int x) {
+            int r = x;
+            while (parent[r] >= 0 && parent[r] != r) r = parent[r];
+            int c = x;
+            while (parent[c] >= 0 && parent[c] != r) { int n = parent[c]; parent[c] = r; c = n; }
+            if (parent[r] < 0) parent[r] = r;
+            return r;
+        };
+        for (const auto& f : boundary) { int r = find(f[0]); parent[find(f[1])] = r; parent[find(f[2])] = r; }
+        std::map<int, uint32_t> groupIndex;
+        std::vector<uint8_t> surf(nb, 0);
+        for (const auto& f : boundary) {
+            int root = find(f[0]);
+            auto it = groupIndex.find(root);
+            uint32_t g;
+            if (it == groupIndex.end()) { g = (uint32_t)groupIndex.size() + 1; groupIndex.emplace(root, g); }
+            else g = it->second;
+            for (int k = 0; k < 3; k++) if (s->bodies[f[k]].is_particle) { H.clothGroup[f[k]] = g; surf[f[k]] = 1; }
+        }
+        for (uint32_t i = 0; i < nb; i++) H.numParticles += surf[i];
+        // Element contacts (V-T, E-E, rigid feature vs triangle) are not in
+        // this build: accept only scenes where they cannot arise — one soft
+        // surface without self-collision and no rigid collider other than
+        // large static ground slabs whose corners lie far outside the scene.
+        if (groupIndex.size() > 1) { err = "contacts between separate soft surfaces (V-T/E-E) are not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+        for (uint32_t i = 0; i < s->num_tets; i++)
+            if (s->tets[i].self_collision) { err = "volumetric self-collision is not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+        for (uint32_t i = 0; i < nc; i++) {
+            const avbd_collider_desc& c = s->colliders[i];
+            if (!c.collision_enabled || s->bodies[c.body].is_particle) continue;
+            bool slab = !H.isDynamic[c.body] && c.shape == AVBD_SHAPE_BOX && c.size[0] >= 20.0f && c.size[1] >= 20.0f;
+            if (!slab) { err = "rigid-vs-soft-surface contacts are not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+        }
+    }
+
+    // ---- static palette for soft scenes (GPUSolver.swift:1956-2049)
+    H.dynamicColoring = (H.numTris == 0 && s->num_tets == 0);
+    H.colors.assign(nb, 0);
+    for (uint32_t i = 0; i < nb; i++) H.colors[i] = i % MAX_COLORS;
+    H.colorStart.assign(MAX_COLORS + 2, 0);
+    H.colorCounts.assign(MAX_COLORS, 0);
+    if (!H.dynamicColoring) {
+        std::vector<std::vector<uint32_t>> adj(nb);
+        auto link2 = [&](int a, int b) {
+            if (a < 0 || b < 0) return;
+            if (H.isDynamic[a] && H.isDynamic[b]) { adj[a].push_back((uint32_t)b); adj[b].push_back((uint32_t)a); }
+        };
+        for (uint32_t i = 0; i < nj; i++) {
+            const avbd_joint_desc& j = s->joints[i];
+            if (j.stiffness_lin != 0.0f || j.stiffness_ang != 0.0f || j.motor_torque != 0.0f) link2(j.body_a, j.body_b);
+        }
+        for (uint32_t i = 0; i < s->num_springs; i++) link2(s->springs[i].body_a, s->springs[i].body_b);
+        for (uint32_t i = 0; i < s->num_tets; i++)
+            for (int a = 0; a < 4; a++) for (int b = a + 1; b < 4; b++) link2(s->tets[i].ids[a], s->tets[i].ids[b]);
+        uint32_t maxColor = 0;
+        std::vector<uint32_t> colors(nb, 0);
+        for (uint32_t v = 0; v < nb; v++) {
+            if (!H.isDynamic[v]) continue;
+            uint64_t used = 0;
+            for (uint32_t n : adj[v]) if (n < v && colors[n] < 64) used |= 1ull << colors[n];
+            if (used == ~0ull) { err = "static coloring needs more than 64 colors"; return AVBD_ERR_RUNTIME_FAILURE; }
+            uint32_t c = 0;
+            while (used & (1ull << c)) c++;
+            colors[v] = c;
+            maxColor = std::max(maxColor, c);
+        }
+        H.staticUsedColors = maxColor + 1;
+        std::vector<std::vector<uint32_t>> buckets(MAX_COLORS);
+        for (uint32_t v = 0; v < nb; v++) if (H.isDynamic[v]) buckets[colors[v]].push_back(v);
+        for (int c = 0; c < MAX_COLORS; c++) {
+            H.colorStart[c] = (uint32_t)H.colorList.size();
+            H.colorCounts[c] = (uint32_t)buckets[c].size();
+            H.colorList.insert(H.colorList.end(), buckets[c].begin(), buckets[c].end());
+        }
+        H.colorStart[MAX_COLORS] = (uint32_t)H.colorList.size();
+        H.colorStart[MAX_COLORS + 1] = H.staticUsedColors;
+        for (uint32_t v = 0; v < nb; v++) H.colors[v] = colors[v];
+    }
+
+    // ---- static adjacency segments (40_solver.metal:27-243, static kinds)
+    std::vector<std::vector<uint32_t>> pre(nb), post(nb);
+    auto dyn = [&](uint32_t b) { return b != WORLD_BODY && H.posLin[b].w > 0.0f; };
+    for (uint32_t g : H.activeJoints) {
+        uint32_t e = (FK_JOINT << ADJ_KIND_SHIFT) | g;
+        if (dyn(H.joints[g].header.x)) pre[H.joints[g].header.x].push_back(e);
+        if (dyn(H.joints[g].header.y)) pre[H.joints[g].header.y].push_back(e);
+    }
+    for (uint32_t i = 0; i < H.springs.size(); i++) {
+        uint32_t e = (FK_SPRING << ADJ_KIND_SHIFT) | i;
+        if (dyn(H.springs[i].header.x)) pre[H.springs[i].header.x].push_back(e);
+        if (dyn(H.springs[i].header.y)) pre[H.springs[i].header.y].push_back(e);
+    }
+    for (uint32_t t = 0; t < H.tets.size(); t++) {
+        uint32_t e = (FK_TET << ADJ_KIND_SHIFT) | t;
+        for (uint32_t v : {H.tets[t].ids.x, H.tets[t].ids.y, H.tets[t].ids.z, H.tets[t].ids.w})
+            if (dyn(v)) post[v].push_back(e);
+    }
+    H.staticSeg.assign(nb, u4{});
+    for (uint32_t b = 0; b < nb; b++) {
+        std::sort(pre[b].begin(), pre[b].end());
+        std::sort(post[b].begin(), post[b].end());
+        H.staticSeg[b] = u4{(uint32_t)H.preList.size(), (uint32_t)pre[b].size(),
+                            (uint32_t)H.postList.size(), (uint32_t)post[b].size()};
+        H.preList.insert(H.preList.end(), pre[b].begin(), pre[b].end());
+        H.postList.insert(H.postList.end(), post[b].begin(), post[b].end());
+    }
+
+    // ---- spinners and parameters (GPUSolver.swift:630-637, :2052-2080)
+    H.spinners.assign(s->spinners, s->spinners + s->num_spinners);
+    for (const auto& sp : H.spinners) {
+        if (sp.body < 0 || (uint32_t)sp.body >= nb) { err = "spinner body out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
+        H.spinVel[sp.body] = f4{sp.axis[0] * sp.omega, sp.axis[1] * sp.omega, sp.axis[2] * sp.omega, 1.0f};
+    }
+    Params& P = H.P;
+    P.numBodies = nb;
+    P.numJoints = nj;
+    P.numSprings = (uint32_t)H.springs.size();
+    P.numTets = (uint32_t)H.tets.size();
+    P.mapCapacity = H.mapCapacity;
+    P.maxPairs = H.maxPairs;
+    P.cellSize = maxHashedRadius * 2.0f;
+    P.gridHashSize = H.gridHashSize;
+    P.numHashed = (uint32_t)H.hashedIdx.size();
+    P.numGlobals = (uint32_t)H.globalIdx.size();
+    P.numHashedRigid = numHashedRigid;
+    P.numTris = H.numTris;
+    P.numParticles = H.numTris == 0 ? 0 : H.numParticles;
+    P.maxSpeed = fmax_(30.0f, 1.5f * P.cellSize / dt * 0.5f);
+    P.surfaceTruncationMode = 0;
+    if (P.numParticles > 0)
+        P.surfaceTruncationMode = s->truncation_selection == AVBD_TRUNCATION_AUTOMATIC ? 1u : s->truncation_selection;
+    if (P.surfaceTruncationMode == 2u) { err = "Planar-DAT truncation is not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+    P.tetInversionPreventionEnabled = 0;
+    P.planarDATRelaxation = 0.85f;
+    P.numExclusions = (uint32_t)(H.exclusions.size() / 2);
+    return AVBD_OK;
+}
+
+}  // namespace avbd

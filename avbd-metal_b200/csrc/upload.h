@@ -1,0 +1,59 @@
+// upload.h — host-side scene upload: turns an avbd_scene_desc into the
+// device-ready arrays of one solver (GPUSolver.swift:338-638, :901-2081).
+#pragma once
+#include <string>
+#include <vector>
+
+#include "../../include/avbd.h"
+#include "avbd_types.h"
+
+namespace avbd {
+
+struct HostScene {
+    // capacities
+    uint32_t numBodies = 0, numColliders = 0;
+    uint32_t maxPairs = 0, mapCapacity = 0, gridHashSize = 0;
+    uint32_t numTris = 0, numParticles = 0;
+    bool dynamicColoring = true;
+    uint32_t staticUsedColors = 1;
+    uint32_t numDynamicBodies = 0;
+    Params P{};
+
+    // bodies (SoA float4)
+    std::vector<f4> posLin, posAng, velLin, velAng, prevVelLin, props, shape, spinVel;
+    std::vector<float> gravityScale;
+    std::vector<uint32_t> shapeType, clothGroup;
+    std::vector<uint8_t> isDynamic;
+
+    // colliders
+    std::vector<uint32_t> colOwner, colShapeType, colGroup, colShared;
+    std::vector<f4> colShape, colLocalPos, colLocalRot;
+    std::vector<float> colFriction;  // (static, dynamic) pairs
+    std::vector<uint32_t> hashedIdx, globalIdx;
+
+    // constraints
+    std::vector<JointGPU> joints;
+    std::vector<f4> initPenLin, initPenAng;
+    std::vector<uint32_t> activeJoints;   // non-inert joints: the only ones any stage reads
+    std::vector<SpringGPU> springs;
+    std::vector<uint32_t> hardSprings;
+    std::vector<TetGPU> tets;
+    std::vector<uint32_t> exclusions;     // sorted (lo, hi) pairs, flattened
+    std::vector<avbd_spinner_desc> spinners;
+    std::vector<std::pair<uint32_t, float>> rateMotors;
+
+    // static palette (soft scenes) in final form
+    std::vector<uint32_t> colors, colorStart, colorList, colorCounts;
+
+    // Static per-body adjacency, split around the per-frame contact entries:
+    // pre = joints + springs (kinds 0, 1), post = tets (kind 3), each sorted.
+    // The solver walks pre, then this frame's manifolds (kind 2), then post,
+    // which is exactly the ascending (kind << 28 | index) order.
+    std::vector<uint32_t> preList, postList;
+    std::vector<u4> staticSeg;            // preStart, preCount, postStart, postCount
+};
+
+// Returns an AVBD_* status; on failure `err` holds a message.
+int upload_scene(const avbd_scene_desc* s, HostScene& out, std::string& err);
+
+}  // namespace avbd

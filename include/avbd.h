@@ -1,0 +1,330 @@
+/*
+ * avbd.h — C ABI of the B200 AVBD solver step.
+ *
+ * This is the drop-in boundary for the reference's `GPUSolver` class
+ * (Sources/PhysicsAVBD/GPU/GPUSolver.swift:17) and the scene description it
+ * is built from (`PhysicsScene`, Sources/SimCore/Scenes/Scene.swift:547).
+ * Every entry point returns an `int` status (AVBD_OK on success) and never
+ * unwinds across the ABI.  All arguments are plain C types: pointers, sizes
+ * and the POD records below.  No CUDA or torch type appears here.
+ *
+ * Threading: one solver instance is driven by one host thread at a time, as
+ * the reference's caller is (GPUSolver.swift:2219-2222).
+ */
+#ifndef AVBD_H
+#define AVBD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AVBD_ABI_VERSION 1u
+
+/* ------------------------------------------------------------------------ */
+/* Status codes.  Construction errors mirror `AVBDError`                     */
+/* (GPUSolver.swift:640-661); runtime errors mirror `RuntimeFailure`         */
+/* (GPUSolver.swift:663-751) and are latched: once a runtime failure is      */
+/* recorded every later call on that solver returns AVBD_ERR_RUNTIME_FAILURE */
+/* until it is destroyed (GPUSolver.swift:2800-2809).                        */
+/* ------------------------------------------------------------------------ */
+enum {
+    AVBD_OK = 0,
+    AVBD_ERR_INVALID_ARGUMENT = 1,   /* bad pointer, index or size           */
+    AVBD_ERR_NO_DEVICE = 2,          /* AVBDError.noDevice                   */
+    AVBD_ERR_ALLOC_FAILED = 3,       /* AVBDError.allocFailed(label)         */
+    AVBD_ERR_KERNEL_MISSING = 4,     /* AVBDError.kernelMissing(name)        */
+    AVBD_ERR_RUNTIME_FAILURE = 5,    /* latched RuntimeFailure, see below    */
+    AVBD_ERR_UNSUPPORTED = 6         /* scene feature outside this build     */
+};
+
+/* Runtime failure kinds reported by avbd_runtime_failure(). */
+enum {
+    AVBD_FAIL_NONE = 0,
+    AVBD_FAIL_COMMAND_EXECUTION = 1,   /* CUDA error on the solver stream    */
+    AVBD_FAIL_RIGID_PAIR_CAPACITY = 2, /* broadphase demand > maxPairs       */
+    AVBD_FAIL_SOFT_CONTACT_CAPACITY = 3,
+    AVBD_FAIL_STATIC_COLOR_CAPACITY = 4,
+    AVBD_FAIL_UNRESOLVED_COLORING = 5,
+    AVBD_FAIL_PLANAR_DAT_PAIR_CAPACITY = 6,
+    AVBD_FAIL_PLANAR_DAT_SOFT_CAPACITY = 7,
+    AVBD_FAIL_PLANAR_DAT_INVALID = 8,
+    AVBD_FAIL_WAIT_TIMEOUT = 9         /* bounded device wait gave up        */
+};
+
+/* Body shape kinds (BodyShape, Scene.swift:6-11). */
+enum { AVBD_SHAPE_BOX = 0, AVBD_SHAPE_SPHERE = 1, AVBD_SHAPE_TORUS = 2,
+       AVBD_SHAPE_CAPSULE = 3 };
+
+/* Joint motor modes (JointMotorMode, Scene.swift:193-204). */
+enum { AVBD_MOTOR_IMPLICIT_POSITION_PD = 0, AVBD_MOTOR_EXPLICIT_TORQUE_PD = 1,
+       AVBD_MOTOR_VELOCITY = 2 };
+
+/* Surface truncation selection (GPUSolver.swift:23-35). */
+enum { AVBD_TRUNCATION_AUTOMATIC = 0, AVBD_TRUNCATION_ISOTROPIC = 1,
+       AVBD_TRUNCATION_PLANAR_DAT = 2 };
+
+/* SimSettings (Scene.swift:485-545); render-only fields are omitted. */
+typedef struct avbd_settings {
+    float dt;
+    float gravity;                 /* along z; negative pulls down            */
+    int32_t iterations;
+    float collision_margin;
+    uint32_t friction_combine_mode; /* 0 geometric .. 4 average               */
+    float alpha;
+    float beta_lin;
+    float beta_ang;
+    float gamma;
+    float lambda_max;
+    float rod_decay_pow;
+    float particle_damping;
+    float rigid_linear_damping;
+    float rigid_angular_damping;
+    float cloth_viscosity;
+} avbd_settings;
+
+/* SceneBody (Scene.swift:34-105). rotation is (x, y, z, w). */
+typedef struct avbd_body_desc {
+    float size[3];
+    float density;                 /* 0 = static unless explicit mass > 0    */
+    float friction;
+    float dynamic_friction;
+    float position[3];
+    float rotation[4];
+    float velocity[3];
+    uint32_t shape;                /* AVBD_SHAPE_*                            */
+    uint32_t is_particle;          /* 3-DOF particle (Scene.swift:57)         */
+    uint32_t has_explicit_mass;    /* mass/diagonal_inertia authoritative     */
+    float mass;
+    float diagonal_inertia[3];
+    float gravity_scale;
+} avbd_body_desc;
+
+/* SceneCollider (Scene.swift:114-186). */
+typedef struct avbd_collider_desc {
+    int32_t body;
+    float size[3];
+    float friction;
+    float dynamic_friction;
+    float local_position[3];
+    float local_rotation[4];
+    uint32_t shape;
+    uint32_t collision_group;
+    uint32_t collides_with_shared;
+    uint32_t collision_enabled;
+    uint32_t world_round_anchor;   /* usesWorldSpaceRoundAnchor              */
+    uint32_t hull_offset;          /* into avbd_scene_desc.hull_vertices     */
+    uint32_t hull_count;           /* 0 = analytic shape                     */
+} avbd_collider_desc;
+
+/* SceneJoint (Scene.swift:206-315). Infinite stiffness = hard constraint. */
+typedef struct avbd_joint_desc {
+    int32_t body_a;                /* -1 = world                             */
+    int32_t body_b;
+    float r_a[3];
+    float r_b[3];
+    float stiffness_lin;
+    float stiffness_ang;
+    float fracture;
+    uint32_t fracture_linear;
+    uint32_t has_hinge;
+    float hinge_axis[3];           /* body-B local, unit                     */
+    float motor_target;
+    float motor_torque;
+    float motor_rate;
+    float motor_stiffness;
+    float motor_damping;
+    uint32_t motor_mode;           /* AVBD_MOTOR_*                            */
+    float armature;
+    float limit_lo;
+    float limit_hi;
+} avbd_joint_desc;
+
+/* SceneSpring (Scene.swift:433-454). rest < 0: use spawn distance. */
+typedef struct avbd_spring_desc {
+    int32_t body_a;
+    int32_t body_b;
+    float r_a[3];
+    float r_b[3];
+    float stiffness;
+    float rest;
+    uint32_t hard;
+} avbd_spring_desc;
+
+/* SceneTet (Scene.swift:337-360). */
+typedef struct avbd_tet_desc {
+    int32_t ids[4];
+    float mu;
+    float lambda;
+    uint32_t self_collision;
+} avbd_tet_desc;
+
+/* SceneTri (Scene.swift:321-334). */
+typedef struct avbd_tri_desc {
+    int32_t ids[3];
+    float mu;
+    float lambda;
+    float bend;
+} avbd_tri_desc;
+
+/* SceneCollisionExclusion (Scene.swift:474-483). */
+typedef struct avbd_exclusion_desc {
+    int32_t body_a;
+    int32_t body_b;
+} avbd_exclusion_desc;
+
+/* SceneSpinner (Scene.swift:459-469). */
+typedef struct avbd_spinner_desc {
+    int32_t body;
+    float axis[3];
+    float omega;
+} avbd_spinner_desc;
+
+/* PhysicsScene + GPUSolver construction options. */
+typedef struct avbd_scene_desc {
+    uint32_t abi_version;          /* must be AVBD_ABI_VERSION               */
+    uint32_t num_bodies;
+    const avbd_body_desc* bodies;
+    uint32_t num_colliders;
+    const avbd_collider_desc* colliders;
+    uint32_t num_hull_vertices;
+    const float* hull_vertices;    /* xyz triples                            */
+    uint32_t num_joints;
+    const avbd_joint_desc* joints;
+    uint32_t num_springs;
+    const avbd_spring_desc* springs;
+    uint32_t num_tets;
+    const avbd_tet_desc* tets;
+    uint32_t num_tris;
+    const avbd_tri_desc* tris;
+    uint32_t num_exclusions;
+    const avbd_exclusion_desc* exclusions;
+    uint32_t num_spinners;
+    const avbd_spinner_desc* spinners;
+    avbd_settings settings;
+    uint32_t max_pairs_per_body;   /* GPUSolver init default 16              */
+    uint32_t truncation_selection; /* AVBD_TRUNCATION_*                       */
+    uint32_t tet_inversion_prevention;
+    int32_t device;                /* CUDA ordinal; -1 = current device      */
+} avbd_scene_desc;
+
+/* One body's kinematic state (bodyStates / BodyStateUpdate,
+ * GPUSolver.swift:2399-2479, :4431-4486). rotation is (x, y, z, w). */
+typedef struct avbd_body_state {
+    float position[3];
+    float rotation[4];
+    float velocity[3];
+    float angular_velocity[3];
+} avbd_body_state;
+
+/* Frame diagnostics (GPUSolver.swift:313-328). */
+typedef struct avbd_counters {
+    uint64_t frame;
+    uint32_t num_pairs;
+    uint32_t pair_candidates;
+    uint32_t num_soft;
+    uint32_t soft_candidates;
+    uint32_t used_colors;
+    uint32_t color_conflicts;
+    uint32_t ogc_exceeded;
+    uint32_t color_counts[64];
+} avbd_counters;
+
+typedef struct avbd_solver avbd_solver;
+typedef struct avbd_snapshot avbd_snapshot;
+
+/* Build a solver from a scene.  Replaces `GPUSolver.init(scene:device:
+ * maxPairsPerBody:)` (GPUSolver.swift:331-336, upload :901-2081).        */
+int avbd_create(const avbd_scene_desc* scene, avbd_solver** out);
+
+/* Release every device buffer owned by the solver. */
+void avbd_destroy(avbd_solver* solver);
+
+/* Replace the per-frame settings (`GPUSolver.settings`, GPUSolver.swift:45,
+ * mirrored into SimParams by syncParams :2097-2142).                        */
+int avbd_set_settings(avbd_solver* solver, const avbd_settings* settings);
+int avbd_get_settings(const avbd_solver* solver, avbd_settings* out);
+
+/* Encode and submit `frames` physics frames asynchronously (`submitStep`,
+ * GPUSolver.swift:3107-3136).  Errors latched during execution surface on
+ * the next call or at avbd_sync.                                           */
+int avbd_step(avbd_solver* solver, uint32_t frames);
+
+/* Wait for every submitted frame and retire its counters (`synchronize`,
+ * GPUSolver.swift:2924-2953).                                              */
+int avbd_sync(avbd_solver* solver);
+
+/* Read `n` body states by index (`bodyStates`, GPUSolver.swift:4471).
+ * ids == NULL reads bodies [0, n).  Synchronises first.                   */
+int avbd_get_body_states(avbd_solver* solver, const uint32_t* ids, uint32_t n,
+                         avbd_body_state* out);
+
+/* Overwrite `n` body states (`setBodyStates`, GPUSolver.swift:2409-2473):
+ * clears the augmented-Lagrangian state of every incident joint, spring and
+ * contact and restores the initial joint penalties.  ids == NULL writes
+ * bodies [0, n).                                                          */
+int avbd_set_body_states(avbd_solver* solver, const uint32_t* ids, uint32_t n,
+                         const avbd_body_state* states);
+
+/* Bulk position/orientation readback: xyzw position (w = mass) and xyzw
+ * quaternion for bodies [0, n).  Either output may be NULL.                */
+int avbd_get_positions(avbd_solver* solver, uint32_t n, float* pos_xyzw,
+                       float* rot_xyzw);
+
+/* Bulk position upload for bodies [0, n) from xyz triples, keeping the
+ * velocity and the augmented-Lagrangian state (used to replay host input). */
+int avbd_set_positions(avbd_solver* solver, uint32_t n, const float* pos_xyz);
+
+/* Motor targets for hinge joints (`setMotorTargets`,
+ * GPUSolver.swift:2496-2521).                                             */
+int avbd_set_motor_targets(avbd_solver* solver, const uint32_t* joints,
+                           uint32_t n, const float* targets);
+
+/* Largest joint violation / contact penetration (`maxConstraintErrorChecked`,
+ * GPUSolver.swift:4819-4865; kernel 40_solver.metal:2189-2229).            */
+int avbd_max_constraint_error(avbd_solver* solver, float* out);
+
+/* Counters of the last retired frame (`lastNumPairs`, `lastColorCounts`,
+ * `lastNumSoft`, GPUSolver.swift:313-328).                                */
+int avbd_get_counters(avbd_solver* solver, avbd_counters* out);
+
+/* Latched runtime failure kind (AVBD_FAIL_*) of this solver
+ * (`runtimeFailure`, GPUSolver.swift:2219-2229).                           */
+int avbd_runtime_failure(const avbd_solver* solver, int* kind);
+
+/* Copy the last error message (NUL-terminated, truncated to len). A NULL
+ * solver reads the last construction error of the calling thread.         */
+int avbd_last_error(const avbd_solver* solver, char* buf, size_t len);
+
+/* Bit-for-bit capture / restore of every solver buffer
+ * (`captureRigidSpeculationSnapshot` / `restore…`, GPUSolver.swift:2955-3057),
+ * extended to soft state.                                                  */
+int avbd_snapshot_capture(avbd_solver* solver, avbd_snapshot** out);
+int avbd_snapshot_restore(avbd_solver* solver, const avbd_snapshot* snap);
+void avbd_snapshot_free(avbd_snapshot* snap);
+
+/* Read-only access to one internal buffer for parity checks and tools
+ * (no counterpart in the reference's public API; its tests read the same
+ * buffers through @testable imports).  `which` is an AVBD_BUF_* id; `bytes`
+ * must not exceed avbd_debug_buffer_size().                                */
+enum {
+    AVBD_BUF_POS_LIN = 0, AVBD_BUF_POS_ANG = 1, AVBD_BUF_VEL_LIN = 2,
+    AVBD_BUF_VEL_ANG = 3, AVBD_BUF_PAIRS = 4, AVBD_BUF_MANIFOLDS = 5,
+    AVBD_BUF_ADJ_START = 6, AVBD_BUF_ADJ_COUNT = 7, AVBD_BUF_ADJ_LIST = 8,
+    AVBD_BUF_COLORS = 9, AVBD_BUF_COLOR_START = 10, AVBD_BUF_COLOR_LIST = 11,
+    AVBD_BUF_CELL_START = 12, AVBD_BUF_CELL_COUNT = 13,
+    AVBD_BUF_CELL_BODIES = 14, AVBD_BUF_MAP_KEY_A = 15, AVBD_BUF_MAP_KEY_B = 16,
+    AVBD_BUF_MAP_VAL = 17, AVBD_BUF_JOINTS = 18, AVBD_BUF_SPRINGS = 19,
+    AVBD_BUF_TETS = 20, AVBD_BUF_INIT_LIN = 21, AVBD_BUF_INERT_LIN = 22,
+    AVBD_BUF_EXCLUSIONS = 23, AVBD_BUF_HASHED_IDX = 24, AVBD_BUF_GLOBAL_IDX = 25,
+    AVBD_BUF_COUNT_ = 26
+};
+size_t avbd_debug_buffer_size(avbd_solver* solver, int which);
+int avbd_debug_read(avbd_solver* solver, int which, void* dst, size_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AVBD_H */

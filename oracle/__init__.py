@@ -1,0 +1,130 @@
+"""CPU oracle of the AVBD solver step — TEST INFRASTRUCTURE.
+
+A serial C++ restatement of the reference solver path (see avbd_oracle.cpp).
+Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg may
+import this package; the product library never calls it.
+"""
+import ctypes as C
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "build", "liboracle.so")
+SRC = [os.path.join(HERE, "avbd_oracle.cpp"), os.path.join(HERE, "oracle_math.h"),
+       os.path.join(HERE, "..", "include", "avbd.h")]
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with IEEE float32 semantics (no FMA contraction)."""
+    if not force and os.path.exists(LIB) and all(
+            os.path.getmtime(LIB) >= os.path.getmtime(s) for s in SRC):
+        return LIB
+    os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
+           "-fPIC", "-shared", "-o", LIB, SRC[0]]
+    subprocess.check_call(cmd)
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        _lib = C.CDLL(LIB)
+        _lib.oracle_create.argtypes = [C.c_void_p, C.POINTER(C.c_void_p)]
+        _lib.oracle_destroy.argtypes = [C.c_void_p]
+        _lib.oracle_set_threads.argtypes = [C.c_void_p, C.c_int]
+        _lib.oracle_set_settings.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.oracle_step.argtypes = [C.c_void_p, C.c_uint32]
+        _lib.oracle_runtime_failure.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+        _lib.oracle_get_positions.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        _lib.oracle_get_body_states.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        _lib.oracle_set_motor_targets.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        _lib.oracle_max_constraint_error.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
+        _lib.oracle_get_counters.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.oracle_debug_buffer_size.argtypes = [C.c_void_p, C.c_int]
+        _lib.oracle_debug_buffer_size.restype = C.c_size_t
+        _lib.oracle_debug_read.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+    return _lib
+
+
+class OracleSolver:
+    """Same surface as avbd_b200.GPUSolver, backed by the CPU oracle."""
+
+    def __init__(self, scene, threads: int = 1, **desc_kw):
+        from avbd_b200 import abi  # noqa: WPS433 (package path set by caller)
+        self._abi = abi
+        self.scene = scene
+        desc, self._keep = scene.to_desc(**desc_kw)
+        self._desc = desc
+        h = C.c_void_p()
+        rc = lib().oracle_create(C.byref(desc), C.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"oracle_create failed: status {rc}")
+        self._h = h
+        self.num_bodies = scene and len(scene.bodies)
+        lib().oracle_set_threads(self._h, threads)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().oracle_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def step(self, frames: int = 1) -> int:
+        return lib().oracle_step(self._h, frames)
+
+    def set_settings(self, settings):
+        st = settings.to_c()
+        lib().oracle_set_settings(self._h, C.byref(st))
+
+    def runtime_failure(self) -> int:
+        k = C.c_int()
+        lib().oracle_runtime_failure(self._h, C.byref(k))
+        return k.value
+
+    def positions(self):
+        n = self.num_bodies
+        pos = np.zeros((n, 4), np.float32)
+        rot = np.zeros((n, 4), np.float32)
+        lib().oracle_get_positions(self._h, n, pos.ctypes.data, rot.ctypes.data)
+        return pos, rot
+
+    def body_states(self):
+        n = self.num_bodies
+        out = (self._abi.BodyState * n)()
+        lib().oracle_get_body_states(self._h, n, out)
+        return out
+
+    def set_motor_targets(self, joints, targets):
+        ids = np.ascontiguousarray(joints, dtype=np.uint32)
+        t = np.ascontiguousarray(targets, dtype=np.float32)
+        lib().oracle_set_motor_targets(self._h, ids.ctypes.data, len(ids), t.ctypes.data)
+
+    def max_constraint_error(self) -> float:
+        v = C.c_float()
+        lib().oracle_max_constraint_error(self._h, C.byref(v))
+        return v.value
+
+    def counters(self):
+        c = self._abi.Counters()
+        lib().oracle_get_counters(self._h, C.byref(c))
+        return c
+
+    def debug_read(self, name: str, dtype=np.uint8):
+        which = self._abi.BUF[name]
+        n = lib().oracle_debug_buffer_size(self._h, which)
+        buf = np.zeros(n, np.uint8)
+        if n:
+            rc = lib().oracle_debug_read(self._h, which, buf.ctypes.data, n)
+            if rc != 0:
+                raise RuntimeError(f"oracle_debug_read({name}) failed: {rc}")
+        return buf.view(dtype)

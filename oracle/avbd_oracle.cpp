@@ -1,0 +1,2048 @@
+// avbd_oracle.cpp — CPU oracle of the AVBD solver step ("Oracle A").
+//
+// TEST INFRASTRUCTURE, NOT PRODUCT CODE.  This file is a serial C++
+// restatement of the reference's GPU solver path (LuckyIYI/avbd-metal,
+// Sources/PhysicsAVBD/GPU/GPUSolver.swift + Shaders/*.metal) written for one
+// purpose: to check the CUDA implementation.  Only tests/, the smoke() entry
+// point and the cpu_baseline leg of bench.py may load it; the product library
+// never links it.
+//
+// Semantics: the reference's stage order (GPUSolver.swift:3138-4375) with
+// colors solved serially, bodies of one color in colorList order, and the
+// 8-lane primal reduction order of primal_particles_split
+// (40_solver.metal:1544-1684) reproduced exactly, so that — with IEEE float32
+// arithmetic and no FMA contraction — the oracle is a bit-level reference for
+// the GPU path.  Parity is "unpinned" against the reference itself (Swift and
+// Metal cannot run here); it is pinned by the analytic gates of the
+// reference's own tests (see tests/test_oracle_gates.py).
+//
+// Optional OpenMP: bodies of one color are independent, so the per-color loop
+// may run in parallel without changing any result (used for the CPU baseline).
+#include "oracle_math.h"
+#include "../include/avbd.h"
+
+#include <algorithm>
+#include <array>
+#include <cfloat>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <set>
+#include <string>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace oracle {
+
+static const float PENALTY_MIN = 1.0f;
+static const float PENALTY_MAX = 1.0e10f;
+static const float PENALTY_MAX_T = 1.0e6f;
+static const float STICK_THRESH = 0.00001f;
+static const int MAX_COLORS = 64;
+static const uint32_t WORLD_BODY = 0xFFFFFFFFu;
+static const uint32_t FK_JOINT = 0, FK_SPRING = 1, FK_MANIFOLD = 2, FK_TET = 3,
+                      FK_SOFT = 4, FK_MEMBRANE = 5, FK_BEND = 6;
+static const int ADJ_KIND_SHIFT = 28;
+static const uint32_t ADJ_INDEX_MASK = 0x0FFFFFFFu;
+static const int MAX_CONTACTS = 8;
+static const uint32_t MOTOR_MODE_MASK = 3u << 4, MOTOR_IMPLICIT = 1u << 4,
+                      MOTOR_EXPLICIT = 2u << 4, MOTOR_VELOCITY = 3u << 4;
+
+// ---- GPU record layouts (00_common.metal:330-431) ------------------------
+struct JointGPU {
+    U4 header;  // bodyA, bodyB, broken, flags
+    F4 rA, rB, C0Lin, C0Ang, lambdaLin, lambdaAng, penaltyLin, penaltyAng,
+        restRel, hingeAxis, motor, limits, dynamics;
+};
+struct SpringGPU { U4 header; F4 rA, rB, dual; };
+struct TetGPU { U4 ids; F4 r0, r1, r2; };
+struct ContactGPU { F4 rA, rB, C0, lambda, penalty; };
+struct ManifoldGPU {
+    U4 header;  // bodyA, bodyB, numContacts, flags (1 active, 2 roundA, 4 roundB)
+    U4 colliderPair;
+    F4 basisN, basisT1;
+    ContactGPU contacts[MAX_CONTACTS];
+};
+static_assert(sizeof(JointGPU) == 224, "JointGPU layout");
+static_assert(sizeof(SpringGPU) == 64, "SpringGPU layout");
+static_assert(sizeof(TetGPU) == 64, "TetGPU layout");
+static_assert(sizeof(ManifoldGPU) == 704, "ManifoldGPU layout");
+
+struct Params {
+    float dt, gravity, alpha, betaLin, betaAng, gamma;
+    uint32_t numBodies, numJoints, numSprings, mapCapacity, maxPairs;
+    float cellSize;
+    uint32_t gridHashSize, numHashed, numGlobals;
+    float maxSpeed, lambdaMax;
+    uint32_t iterations, numTets, numTris, numParticles;
+    float rodDecayPow, particleDamping;
+    uint32_t numHashedRigid, frame, frictionCombineMode;
+    float collisionMargin, rigidLinearDamping, rigidAngularDamping;
+    uint32_t surfaceTruncationMode, tetInversionPreventionEnabled;
+    float planarDATRelaxation;
+};
+
+static uint32_t next_pow2(uint32_t v) {
+    uint32_t p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+// Hash of an integer cell (20_broadphase.metal:16-28).
+static inline uint32_t cell_hash(int cx, int cy, int cz, uint32_t group, uint32_t size) {
+    uint32_t h = ((uint32_t)cx * 92837111u) ^ ((uint32_t)cy * 689287499u)
+               ^ ((uint32_t)cz * 283923481u);
+    h ^= group * 0x9e3779b9u;
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    return h & (size - 1u);
+}
+static inline void cell_coord(F3 p, float cs, int& x, int& y, int& z) {
+    x = (int)std::floor(p.x / cs);
+    y = (int)std::floor(p.y / cs);
+    z = (int)std::floor(p.z / cs);
+}
+// Manifold persistence-map hash (20_broadphase.metal:547-553).
+static inline uint32_t pair_map_hash(uint32_t a, uint32_t b, uint32_t cap) {
+    uint32_t h = (a * 73856093u) ^ (b * 19349663u);
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    return h & (cap - 1u);
+}
+static inline bool groups_compatible(uint32_t a, uint32_t b) { return a == 0u || b == 0u || a == b; }
+static inline bool domains_compatible(uint32_t ga, uint32_t gb, uint32_t sa, uint32_t sb) {
+    if (!groups_compatible(ga, gb)) return false;
+    if (ga == 0u && gb != 0u) return sb != 0u;
+    if (gb == 0u && ga != 0u) return sa != 0u;
+    return true;
+}
+
+struct Accum { M3 lhsLin, lhsAng, lhsCross; F3 rhsLin, rhsAng; };
+static inline Accum accum_zero() { return Accum{m3_zero(), m3_zero(), m3_zero(), f3s(0), f3s(0)}; }
+static inline Accum accum_add(const Accum& a, const Accum& b) {
+    return Accum{m3_add(a.lhsLin, b.lhsLin), m3_add(a.lhsAng, b.lhsAng),
+                 m3_add(a.lhsCross, b.lhsCross), a.rhsLin + b.rhsLin, a.rhsAng + b.rhsAng};
+}
+
+struct Solver {
+    avbd_settings settings{};
+    Params P{};
+    uint32_t nb = 0, nc = 0;
+    uint64_t frameIndex = 0;
+    std::string error;
+    int failure = AVBD_FAIL_NONE;
+    int threads = 1;
+
+    // bodies
+    std::vector<F4> posLin, posAng, initLin, initAng, inertLin, inertAng, velLin, velAng,
+        prevVelLin, props, shape, spinVel, ogcPrev;
+    std::vector<float> gravityScale;
+    std::vector<uint32_t> shapeType, boundsBits, clothGroup, clothVert;
+    std::vector<uint8_t> isDynamic, isParticle;
+    // colliders
+    std::vector<uint32_t> colOwner, colShapeType, colGroup, colShared;
+    std::vector<F4> colShape, colLocalPos, colLocalRot;
+    std::vector<float> colFrictionS, colFrictionD;
+    std::vector<uint32_t> hashedIdx, globalIdx, hashedRigidIdx;
+    // constraints
+    std::vector<JointGPU> joints;
+    std::vector<F4> initPenLin, initPenAng;
+    std::vector<SpringGPU> springs;
+    std::vector<TetGPU> tets;
+    std::vector<uint32_t> exclusions;  // (a, b) pairs, sorted
+    std::vector<avbd_spinner_desc> spinners;
+    struct RateMotor { uint32_t joint; float rate; };
+    std::vector<RateMotor> rateMotors;
+    // capacities
+    uint32_t maxPairs = 0, mapCapacity = 0, gridHashSize = 0;
+    uint32_t numTris = 0, numParticles = 0;
+    bool dynamicColoring = true;
+    uint32_t staticUsedColors = 1;
+    // per-frame
+    std::vector<uint32_t> cellCount, cellStart, cellBodies, cellRigid, bodyCellSlot;
+    std::vector<uint32_t> pairCount, pairStart, pairs;
+    std::vector<ManifoldGPU> manifolds, prevManifolds;
+    std::vector<uint32_t> mapKeyA, mapKeyB, mapVal;
+    std::vector<uint32_t> adjStart, adjCount, adjList;
+    std::vector<uint32_t> colorsA, colorsB, colorStart, colorList;
+    uint32_t numPairs = 0, pairCandidates = 0, colorConflicts = 0, ogcExceeded = 0;
+    uint32_t colorCounts[MAX_COLORS] = {};
+
+    bool body_dynamic(uint32_t b) const { return b != WORLD_BODY && posLin[b].w > 0.0f; }
+
+    // ---------------------------------------------------------------- upload
+    int create(const avbd_scene_desc* s);
+    void sync_params();
+    void step();
+    // stages
+    void broadphase();
+    uint32_t process_producer(uint32_t producer, bool emit, uint32_t base);
+    void narrowphase();
+    void narrow_one(uint32_t gid);
+    void map_rebuild();
+    int map_find(uint32_t a, uint32_t b) const;
+    void warmstart_joints();
+    void warmstart_bodies();
+    void adjacency();
+    void dynamic_coloring();
+    void neighbor_colors(uint32_t entry, uint32_t self, uint32_t myColor,
+                         const std::vector<uint32_t>& colorsIn, uint32_t& maskLo,
+                         uint32_t& maskHi, uint32_t& allLo, uint32_t& allHi,
+                         bool& conflict) const;
+    void primal_color(uint32_t c);
+    void primal_body(uint32_t body);
+    void stamp_entry(uint32_t entry, uint32_t body, Accum& acc) const;
+    void stamp_joint(const JointGPU& j, uint32_t self, Accum& acc) const;
+    void stamp_spring(const SpringGPU& sp, uint32_t self, Accum& acc) const;
+    void stamp_tet(const TetGPU& t, uint32_t self, Accum& acc) const;
+    void stamp_manifold(const ManifoldGPU& m, uint32_t self, Accum& acc) const;
+    void dual_all();
+    void dual_joint(uint32_t gid);
+    void dual_spring(uint32_t si);
+    void dual_manifold(uint32_t mi);
+    void finalize();
+    void advance_spinners();
+    float max_constraint_error() const;
+};
+
+// ==========================================================================
+// Upload (GPUSolver.swift:338-638, :901-2081)
+// ==========================================================================
+static bool is_dynamic_desc(const avbd_body_desc& b) {
+    if (b.has_explicit_mass) return b.mass > 0.0f;
+    return b.density > 0.0f;
+}
+
+static std::vector<std::array<int, 3>> tet_boundary_faces(const avbd_scene_desc* s);
+
+int Solver::create(const avbd_scene_desc* s) {
+    if (!s || s->abi_version != AVBD_ABI_VERSION) { error = "bad scene descriptor"; return AVBD_ERR_INVALID_ARGUMENT; }
+    settings = s->settings;
+    nb = s->num_bodies;
+    nc = s->num_colliders;
+    for (uint32_t i = 0; i < nc; i++) {
+        const avbd_collider_desc& c = s->colliders[i];
+        if (c.body < 0 || (uint32_t)c.body >= nb) { error = "collider owner out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
+        if (c.collision_enabled && (c.hull_count > 0 || c.shape == AVBD_SHAPE_TORUS || c.shape == AVBD_SHAPE_CAPSULE)) {
+            error = "torus, capsule and convex-hull colliders are not supported by this build";
+            return AVBD_ERR_UNSUPPORTED;
+        }
+    }
+    if (s->num_tris > 0) { error = "cloth triangles are not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+
+    uint32_t enabled = 0;
+    for (uint32_t i = 0; i < nc; i++) enabled += s->colliders[i].collision_enabled ? 1u : 0u;
+    uint32_t mppb = s->max_pairs_per_body ? s->max_pairs_per_body : 16u;
+    maxPairs = std::max<uint32_t>(4096u, enabled * mppb);
+    mapCapacity = next_pow2(2 * maxPairs);
+    gridHashSize = next_pow2(std::max<uint32_t>(64u, 2u * std::max<uint32_t>(1u, enabled)));
+
+    std::vector<std::array<int, 3>> boundary = tet_boundary_faces(s);
+    numTris = (uint32_t)boundary.size();
+
+    posLin.assign(nb, F4{}); posAng.assign(nb, F4{}); initLin.assign(nb, F4{});
+    initAng.assign(nb, F4{}); inertLin.assign(nb, F4{}); inertAng.assign(nb, F4{});
+    velLin.assign(nb, F4{}); velAng.assign(nb, F4{}); prevVelLin.assign(nb, F4{});
+    props.assign(nb, F4{}); shape.assign(nb, F4{}); spinVel.assign(nb, F4{});
+    ogcPrev.assign(nb, F4{});
+    gravityScale.assign(nb, 1.0f); shapeType.assign(nb, 0); boundsBits.assign(nb, 0x7F7F7F7Fu);
+    clothGroup.assign(nb, 0); clothVert.assign(nb, 0);
+    isDynamic.assign(nb, 0); isParticle.assign(nb, 0);
+    colorsA.assign(nb, 0); colorsB.assign(nb, 0);
+
+    const float PI = 3.14159265358979323846f;
+    for (uint32_t i = 0; i < nb; i++) {
+        const avbd_body_desc& b = s->bodies[i];
+        float mass = 0.0f, radius = 0.0f;
+        F3 moment = f3s(0);
+        F3 size = f3(b.size[0], b.size[1], b.size[2]);
+        if (b.shape == AVBD_SHAPE_BOX) {
+            mass = b.density > 0.0f ? size.x * size.y * size.z * b.density : 0.0f;
+            moment = F3{(size.y * size.y + size.z * size.z) / 12.0f * mass,
+                        (size.x * size.x + size.z * size.z) / 12.0f * mass,
+                        (size.x * size.x + size.y * size.y) / 12.0f * mass};
+            radius = length(size * 0.5f);
+        } else if (b.shape == AVBD_SHAPE_SPHERE) {
+            float r = size.x / 2.0f;
+            mass = b.density > 0.0f ? 4.0f / 3.0f * PI * r * r * r * b.density : 0.0f;
+            moment = f3s(0.4f * mass * r * r);
+            radius = r;
+        } else if (b.shape == AVBD_SHAPE_TORUS) {
+            float R = size.x, r = size.y;
+            mass = b.density > 0.0f ? 2.0f * PI * PI * R * r * r * b.density : 0.0f;
+            float iDia = mass * (R * R / 2.0f + 5.0f * r * r / 8.0f);
+            float iAxis = mass * (R * R + 3.0f * r * r / 4.0f);
+            moment = f3(iDia, iDia, iAxis);
+            radius = R + r;
+        } else {
+            float L = size.x, r = size.y;
+            mass = b.density > 0.0f ? PI * r * r * (L + 4.0f * r / 3.0f) * b.density : 0.0f;
+            float iAxis = 0.5f * mass * r * r;
+            float iPerp = mass * (L * L / 12.0f + r * r / 4.0f);
+            moment = f3(iPerp, iPerp, iAxis);
+            radius = L / 2.0f + r;
+        }
+        if (b.has_explicit_mass) {
+            mass = b.mass;
+            moment = f3(b.diagonal_inertia[0], b.diagonal_inertia[1], b.diagonal_inertia[2]);
+        }
+        posLin[i] = f4(b.position[0], b.position[1], b.position[2], mass);
+        posAng[i] = f4(b.rotation[0], b.rotation[1], b.rotation[2], b.rotation[3]);
+        velLin[i] = f4(b.velocity[0], b.velocity[1], b.velocity[2], 0.0f);
+        prevVelLin[i] = velLin[i];
+        props[i] = f4(moment, b.friction);
+        shape[i] = f4(size, b.is_particle ? -radius : radius);
+        gravityScale[i] = b.gravity_scale;
+        shapeType[i] = b.shape;
+        colorsA[i] = colorsB[i] = i % MAX_COLORS;
+        isDynamic[i] = is_dynamic_desc(b) ? 1 : 0;
+        isParticle[i] = b.is_particle ? 1 : 0;
+    }
+
+    // colliders
+    colOwner.assign(nc, 0); colShapeType.assign(nc, 0); colGroup.assign(nc, 0); colShared.assign(nc, 0);
+    colShape.assign(nc, F4{}); colLocalPos.assign(nc, F4{}); colLocalRot.assign(nc, F4{});
+    colFrictionS.assign(nc, 0); colFrictionD.assign(nc, 0);
+    auto collider_radius = [](const avbd_collider_desc& c) -> float {
+        F3 sz = f3(c.size[0], c.size[1], c.size[2]);
+        if (c.shape == AVBD_SHAPE_SPHERE) return sz.x / 2.0f;
+        if (c.shape == AVBD_SHAPE_TORUS) return sz.x + sz.y;
+        if (c.shape == AVBD_SHAPE_CAPSULE) return sz.x / 2.0f + sz.y;
+        return length(sz * 0.5f);
+    };
+    std::vector<float> radii;
+    for (uint32_t i = 0; i < nc; i++) {
+        const avbd_collider_desc& c = s->colliders[i];
+        float r = collider_radius(c);
+        bool particle = s->bodies[c.body].is_particle != 0;
+        colOwner[i] = (uint32_t)c.body;
+        colGroup[i] = c.collision_group;
+        colShared[i] = c.collides_with_shared ? 1u : 0u;
+        colShape[i] = f4(c.size[0], c.size[1], c.size[2], particle ? -r : r);
+        colLocalPos[i] = f4(c.local_position[0], c.local_position[1], c.local_position[2], c.friction);
+        colLocalRot[i] = f4(c.local_rotation[0], c.local_rotation[1], c.local_rotation[2], c.local_rotation[3]);
+        colFrictionS[i] = c.friction;
+        colFrictionD[i] = c.dynamic_friction;
+        uint32_t flags = c.shape;
+        if (particle) flags |= 0x10u;
+        if (c.world_round_anchor) flags |= 0x20u;
+        colShapeType[i] = flags;
+        if (c.collision_enabled && isDynamic[c.body]) radii.push_back(r);
+    }
+    std::vector<float> sorted = radii;
+    std::sort(sorted.begin(), sorted.end());
+    float median = sorted.empty() ? 0.5f : sorted[sorted.size() / 2];
+    float threshold = median * 4.0f;
+    bool isolated = false;
+    for (uint32_t i = 0; i < nc; i++)
+        if (s->colliders[i].collision_enabled && s->colliders[i].collision_group != 0) isolated = true;
+    hashedIdx.clear(); globalIdx.clear(); hashedRigidIdx.clear();
+    for (uint32_t i = 0; i < nc; i++) {
+        const avbd_collider_desc& c = s->colliders[i];
+        if (!c.collision_enabled) continue;
+        if (collider_radius(c) > threshold || (isolated && c.collision_group == 0)) globalIdx.push_back(i);
+        else hashedIdx.push_back(i);
+    }
+    float maxHashedRadius = 0.05f;
+    for (uint32_t i : hashedIdx) maxHashedRadius = fmax_(maxHashedRadius, std::fabs(colShape[i].w));
+    for (uint32_t i : hashedIdx)
+        if (!s->bodies[s->colliders[i].body].is_particle) hashedRigidIdx.push_back(i);
+
+    // joints (GPUSolver.swift:1092-1195)
+    uint32_t nj = s->num_joints;
+    joints.assign(nj, JointGPU{});
+    const float dt = settings.dt;
+    for (uint32_t i = 0; i < nj; i++) {
+        const avbd_joint_desc& j = s->joints[i];
+        JointGPU g{};
+        uint32_t aIdx = j.body_a >= 0 ? (uint32_t)j.body_a : WORLD_BODY;
+        uint32_t flags = 0;
+        if (std::isinf(j.stiffness_lin)) flags |= 1;
+        if (std::isinf(j.stiffness_ang)) flags |= 2;
+        if (std::isfinite(j.fracture)) flags |= 4;
+        if (j.fracture_linear) flags |= 8;
+        g.header = U4{aIdx, (uint32_t)j.body_b, 0, flags};
+        const float bigK = 3.0e10f;
+        g.rA = f4(j.r_a[0], j.r_a[1], j.r_a[2], fmin_(j.stiffness_lin, bigK));
+        g.rB = f4(j.r_b[0], j.r_b[1], j.r_b[2], fmin_(j.stiffness_ang, bigK));
+        F3 sizeA = j.body_a >= 0 ? f3(s->bodies[j.body_a].size[0], s->bodies[j.body_a].size[1],
+                                      s->bodies[j.body_a].size[2]) : f3s(0);
+        F3 sizeB = f3(s->bodies[j.body_b].size[0], s->bodies[j.body_b].size[1], s->bodies[j.body_b].size[2]);
+        F3 ss = sizeA + sizeB;
+        float torqueArm = dot(ss, ss);
+        g.C0Lin = f4(0, 0, 0, torqueArm);
+        g.C0Ang = f4(0, 0, 0, fmin_(j.fracture, 3.0e18f));
+        F4 qA0 = j.body_a >= 0 ? posAng[j.body_a] : f4(0, 0, 0, 1);
+        F4 rel = q_mul(q_inv(qA0), posAng[j.body_b]);
+        rel = rel / std::sqrt(dot4(rel, rel));
+        g.restRel = rel;
+        if (j.has_hinge) {
+            g.hingeAxis = f4(j.hinge_axis[0], j.hinge_axis[1], j.hinge_axis[2], 1.0f);
+            g.dynamics.x = j.armature;
+            if (j.motor_torque > 0.0f) {
+                g.motor = f4(j.motor_target, j.motor_torque, 0.0f, j.motor_stiffness);
+                g.limits = f4(j.limit_lo, j.limit_hi, j.motor_damping, 0.0f);
+                if (j.motor_mode == AVBD_MOTOR_IMPLICIT_POSITION_PD) g.header.w |= MOTOR_IMPLICIT;
+                else if (j.motor_mode == AVBD_MOTOR_EXPLICIT_TORQUE_PD) g.header.w |= MOTOR_EXPLICIT;
+                else g.header.w |= MOTOR_VELOCITY;
+                if (j.motor_rate != 0.0f) rateMotors.push_back(RateMotor{i, j.motor_rate});
+            }
+            if (j.limit_lo < j.limit_hi && j.motor_torque == 0.0f)
+                g.limits = f4(j.limit_lo, j.limit_hi, 0.0f, 0.0f);
+        }
+        float massA = j.body_a >= 0 ? posLin[j.body_a].w : 0.0f;
+        float massB = posLin[j.body_b].w;
+        float eff = 0.0f;
+        bool have = false;
+        for (float m : {massA, massB}) if (m > 0.0f) { eff = have ? fmin_(eff, m) : m; have = true; }
+        float floorK = fmin_(1.0e9f, fmax_(1.0f, eff / fmax_(dt * dt, 1.0e-12f)));
+        if (std::isinf(j.stiffness_lin)) g.penaltyLin = f4(floorK, floorK, floorK, floorK);
+        if (std::isinf(j.stiffness_ang)) g.penaltyAng = f4(floorK, floorK, floorK, floorK);
+        if (j.stiffness_lin > 0.0f && std::isfinite(j.stiffness_lin)) {
+            float k = fmin_(j.stiffness_lin, 1e9f); g.penaltyLin = f4(k, k, k, k);
+        }
+        if (j.stiffness_ang > 0.0f && std::isfinite(j.stiffness_ang)) {
+            float k = fmin_(j.stiffness_ang, 1e9f); g.penaltyAng = f4(k, k, k, k);
+        }
+        joints[i] = g;
+    }
+    initPenLin.resize(nj); initPenAng.resize(nj);
+    for (uint32_t i = 0; i < nj; i++) { initPenLin[i] = joints[i].penaltyLin; initPenAng[i] = joints[i].penaltyAng; }
+
+    // springs (GPUSolver.swift:1197-1212)
+    springs.assign(s->num_springs, SpringGPU{});
+    for (uint32_t i = 0; i < s->num_springs; i++) {
+        const avbd_spring_desc& sp = s->springs[i];
+        SpringGPU g{};
+        g.header = U4{(uint32_t)sp.body_a, (uint32_t)sp.body_b, sp.hard ? 1u : 0u, 0};
+        float rest = sp.rest;
+        if (rest < 0.0f) {
+            F3 pA = xform(xyz(posLin[sp.body_a]), posAng[sp.body_a], f3(sp.r_a[0], sp.r_a[1], sp.r_a[2]));
+            F3 pB = xform(xyz(posLin[sp.body_b]), posAng[sp.body_b], f3(sp.r_b[0], sp.r_b[1], sp.r_b[2]));
+            rest = length(pA - pB);
+        }
+        g.rA = f4(sp.r_a[0], sp.r_a[1], sp.r_a[2], sp.stiffness);
+        g.rB = f4(sp.r_b[0], sp.r_b[1], sp.r_b[2], rest);
+        springs[i] = g;
+    }
+
+    // tets (GPUSolver.swift:1214-1235): DmInv rows via the adjugate.
+    tets.assign(s->num_tets, TetGPU{});
+    for (uint32_t i = 0; i < s->num_tets; i++) {
+        const avbd_tet_desc& t = s->tets[i];
+        F3 x0 = xyz(posLin[t.ids[0]]);
+        F3 d0 = xyz(posLin[t.ids[1]]) - x0;
+        F3 d1 = xyz(posLin[t.ids[2]]) - x0;
+        F3 d2 = xyz(posLin[t.ids[3]]) - x0;
+        float six = dot(d0, cross(d1, d2));
+        float vol = std::fabs(six) / 6.0f;
+        // Dm has columns d0, d1, d2; inverse rows are (d1 x d2, d2 x d0, d0 x d1) / det.
+        F3 r0 = cross(d1, d2) / six;
+        F3 r1 = cross(d2, d0) / six;
+        F3 r2 = cross(d0, d1) / six;
+        TetGPU g{};
+        g.ids = U4{(uint32_t)t.ids[0], (uint32_t)t.ids[1], (uint32_t)t.ids[2], (uint32_t)t.ids[3]};
+        g.r0 = f4(r0, six);
+        g.r1 = f4(r1, t.mu * vol);
+        g.r2 = f4(r2, t.lambda * vol);
+        tets[i] = g;
+    }
+
+    // exclusions (GPUSolver.swift:1265-1287)
+    std::vector<uint64_t> excl;
+    for (uint32_t i = 0; i < nj; i++)
+        if (s->joints[i].body_a >= 0) {
+            uint64_t lo = (uint64_t)std::min(s->joints[i].body_a, s->joints[i].body_b);
+            uint64_t hi = (uint64_t)std::max(s->joints[i].body_a, s->joints[i].body_b);
+            excl.push_back(lo << 32 | hi);
+        }
+    for (uint32_t i = 0; i < s->num_springs; i++) {
+        uint64_t lo = (uint64_t)std::min(s->springs[i].body_a, s->springs[i].body_b);
+        uint64_t hi = (uint64_t)std::max(s->springs[i].body_a, s->springs[i].body_b);
+        excl.push_back(lo << 32 | hi);
+    }
+    for (uint32_t i = 0; i < s->num_exclusions; i++) {
+        uint64_t lo = (uint64_t)std::min(s->exclusions[i].body_a, s->exclusions[i].body_b);
+        uint64_t hi = (uint64_t)std::max(s->exclusions[i].body_a, s->exclusions[i].body_b);
+        excl.push_back(lo << 32 | hi);
+    }
+    std::sort(excl.begin(), excl.end());
+    excl.erase(std::unique(excl.begin(), excl.end()), excl.end());
+    exclusions.clear();
+    for (uint64_t k : excl) { exclusions.push_back((uint32_t)(k >> 32)); exclusions.push_back((uint32_t)(k & 0xFFFFFFFFu)); }
+
+    // collision-surface groups for tet boundary faces (GPUSolver.swift:1461-1535)
+    if (!boundary.empty()) {
+        std::vector<int> parent(nb, -1);
+        auto find = [&](int x) { int r = x; while (parent[r] >= 0 && parent[r] != r) r = parent[r];
+            int c = x; while (parent[c] >= 0 && parent[c] != r) { int n = parent[c]; parent[c] = r; c = n; }
+            if (parent[r] < 0) parent[r] = r;
+            return r; };
+        for (auto& f : boundary) { int r = find(f[0]); parent[find(f[1])] = r; parent[find(f[2])] = r; }
+        std::map<int, uint32_t> groupIndex;
+        std::vector<uint8_t> surf(nb, 0);
+        for (auto& f : boundary) {
+            int root = find(f[0]);
+            if (!groupIndex.count(root)) { uint32_t g = (uint32_t)groupIndex.size() + 1; groupIndex[root] = g; }
+            uint32_t g = groupIndex[root];
+            for (int k = 0; k < 3; k++) if (isParticle[f[k]]) { clothGroup[f[k]] = g; surf[f[k]] = 1; }
+        }
+        numParticles = 0;
+        for (uint32_t i = 0; i < nb; i++) numParticles += surf[i];
+        // element contacts are not restated yet: refuse scenes that need them
+        if (groupIndex.size() > 1) { error = "soft-soft element contacts are not restated"; return AVBD_ERR_UNSUPPORTED; }
+        for (uint32_t i = 0; i < s->num_tets; i++)
+            if (s->tets[i].self_collision) { error = "volumetric self-collision is not restated"; return AVBD_ERR_UNSUPPORTED; }
+        for (uint32_t i = 0; i < nc; i++) {
+            const avbd_collider_desc& c = s->colliders[i];
+            if (!c.collision_enabled || isParticle[c.body]) continue;
+            bool slab = !isDynamic[c.body] && c.shape == AVBD_SHAPE_BOX && c.size[0] >= 20.0f && c.size[1] >= 20.0f;
+            if (!slab) { error = "rigid-vs-soft-surface contacts are not restated"; return AVBD_ERR_UNSUPPORTED; }
+        }
+    }
+
+    // static coloring (GPUSolver.swift:1956-2049)
+    dynamicColoring = (numTris == 0 && s->num_tets == 0);
+    colorStart.assign(MAX_COLORS + 2, 0);
+    if (!dynamicColoring) {
+        std::vector<std::set<uint32_t>> adj(nb);
+        auto link2 = [&](int a, int b) {
+            if (a < 0 || b < 0) return;
+            if (!(isDynamic[a] || isDynamic[b])) return;
+            if (isDynamic[a] && isDynamic[b]) { adj[a].insert((uint32_t)b); adj[b].insert((uint32_t)a); }
+        };
+        for (uint32_t i = 0; i < nj; i++) {
+            const avbd_joint_desc& j = s->joints[i];
+            if (j.stiffness_lin != 0.0f || j.stiffness_ang != 0.0f || j.motor_torque != 0.0f) link2(j.body_a, j.body_b);
+        }
+        for (uint32_t i = 0; i < s->num_springs; i++) link2(s->springs[i].body_a, s->springs[i].body_b);
+        for (uint32_t i = 0; i < s->num_tets; i++)
+            for (int a = 0; a < 4; a++) for (int b = a + 1; b < 4; b++) link2(s->tets[i].ids[a], s->tets[i].ids[b]);
+        std::vector<uint32_t> colors(nb, 0);
+        uint32_t maxColor = 0;
+        for (uint32_t v = 0; v < nb; v++) {
+            if (!isDynamic[v]) continue;
+            uint64_t used = 0;
+            for (uint32_t n : adj[v]) if (n < v && colors[n] < 64) used |= (1ull << colors[n]);
+            if (used == ~0ull) { error = "static coloring needs more than 64 colors"; failure = AVBD_FAIL_STATIC_COLOR_CAPACITY; return AVBD_ERR_RUNTIME_FAILURE; }
+            uint32_t c = 0;
+            while (used & (1ull << c)) c++;
+            colors[v] = c;
+            maxColor = std::max(maxColor, c);
+        }
+        staticUsedColors = maxColor + 1;
+        std::vector<std::vector<uint32_t>> buckets(MAX_COLORS);
+        for (uint32_t v = 0; v < nb; v++) if (isDynamic[v]) buckets[colors[v]].push_back(v);
+        colorList.clear();
+        for (int c = 0; c < MAX_COLORS; c++) {
+            colorStart[c] = (uint32_t)colorList.size();
+            colorCounts[c] = (uint32_t)buckets[c].size();
+            colorList.insert(colorList.end(), buckets[c].begin(), buckets[c].end());
+        }
+        colorStart[MAX_COLORS] = (uint32_t)colorList.size();
+        colorStart[MAX_COLORS + 1] = staticUsedColors;
+        for (uint32_t v = 0; v < nb; v++) colorsA[v] = colors[v];
+    }
+
+    // per-frame buffers
+    manifolds.assign(maxPairs, ManifoldGPU{});
+    prevManifolds.assign(maxPairs, ManifoldGPU{});
+    mapKeyA.assign(mapCapacity, 0); mapKeyB.assign(mapCapacity, 0); mapVal.assign(mapCapacity, 0);
+    cellCount.assign(gridHashSize, 0); cellStart.assign(gridHashSize, 0); cellRigid.assign(gridHashSize, 0);
+    cellBodies.assign(std::max<size_t>(1, hashedIdx.size()), 0);
+    pairs.assign(2 * maxPairs, 0);
+
+    // params
+    P.numBodies = nb; P.numJoints = nj; P.numSprings = (uint32_t)springs.size();
+    P.numTets = (uint32_t)tets.size(); P.mapCapacity = mapCapacity; P.maxPairs = maxPairs;
+    P.cellSize = maxHashedRadius * 2.0f; P.gridHashSize = gridHashSize;
+    P.numHashed = (uint32_t)hashedIdx.size(); P.numGlobals = (uint32_t)globalIdx.size();
+    P.numHashedRigid = (uint32_t)hashedRigidIdx.size();
+    P.numTris = numTris; P.numParticles = numTris == 0 ? 0 : numParticles;
+    P.maxSpeed = fmax_(30.0f, 1.5f * P.cellSize / settings.dt * 0.5f);
+
+    spinners.assign(s->spinners, s->spinners + s->num_spinners);
+    for (auto& sp : spinners)
+        spinVel[sp.body] = f4(sp.axis[0] * sp.omega, sp.axis[1] * sp.omega, sp.axis[2] * sp.omega, 1.0f);
+    P.surfaceTruncationMode = 0;
+    if (P.numParticles > 0) {
+        uint32_t sel = s->truncation_selection;
+        P.surfaceTruncationMode = sel == AVBD_TRUNCATION_AUTOMATIC ? 1u : sel;
+    }
+    P.tetInversionPreventionEnabled = (P.surfaceTruncationMode == 2u && s->tet_inversion_prevention) ? 1u : 0u;
+    P.planarDATRelaxation = 0.85f;
+    return AVBD_OK;
+}
+
+// Boundary faces of a tet mesh: faces owned by exactly one tet, wound
+// outward against the opposite vertex, sorted (GPUSolver.swift:875-897).
+static std::vector<std::array<int, 3>> tet_boundary_faces(const avbd_scene_desc* s) {
+    std::vector<std::array<int, 3>> out;
+    if (s->num_tets == 0) return out;
+    struct Face { std::array<int, 3> tri; int opp; int count; };
+    std::map<std::array<int, 3>, Face> faces;
+    static const int idx[4][4] = {{0, 1, 2, 3}, {0, 1, 3, 2}, {0, 2, 3, 1}, {1, 2, 3, 0}};
+    for (uint32_t t = 0; t < s->num_tets; t++) {
+        const int* ids = s->tets[t].ids;
+        for (auto& f : idx) {
+            std::array<int, 3> tri = {ids[f[0]], ids[f[1]], ids[f[2]]};
+            std::array<int, 3> key = tri;
+            std::sort(key.begin(), key.end());
+            auto it = faces.find(key);
+            if (it != faces.end()) it->second.count++;
+            else faces[key] = Face{tri, ids[f[3]], 1};
+        }
+    }
+    for (auto& kv : faces) {
+        if (kv.second.count != 1) continue;
+        int a = kv.second.tri[0], b = kv.second.tri[1], c = kv.second.tri[2];
+        const float* pa = s->bodies[a].position;
+        F3 A = f3(pa[0], pa[1], pa[2]);
+        F3 B = f3(s->bodies[b].position[0], s->bodies[b].position[1], s->bodies[b].position[2]);
+        F3 C = f3(s->bodies[c].position[0], s->bodies[c].position[1], s->bodies[c].position[2]);
+        const float* po = s->bodies[kv.second.opp].position;
+        F3 n = cross(B - A, C - A);
+        if (dot(n, f3(po[0], po[1], po[2]) - A) > 0.0f) std::swap(b, c);
+        out.push_back({a, b, c});
+    }
+    std::sort(out.begin(), out.end());
+    return out;
+}
+
+void Solver::sync_params() {
+    P.dt = settings.dt; P.gravity = settings.gravity; P.alpha = settings.alpha;
+    P.betaLin = settings.beta_lin; P.betaAng = settings.beta_ang; P.gamma = settings.gamma;
+    P.lambdaMax = settings.lambda_max; P.iterations = (uint32_t)settings.iterations;
+    P.rodDecayPow = settings.rod_decay_pow; P.particleDamping = settings.particle_damping;
+    P.frame = (uint32_t)frameIndex; P.frictionCombineMode = settings.friction_combine_mode;
+    P.collisionMargin = fmax_(settings.collision_margin, 0.0f);
+    P.rigidLinearDamping = fmax_(settings.rigid_linear_damping, 0.0f);
+    P.rigidAngularDamping = fmax_(settings.rigid_angular_damping, 0.0f);
+}
+
+// ==========================================================================
+// Broadphase (20_broadphase.metal:69-131, :287-512)
+// ==========================================================================
+static inline F3 collider_center(const Solver& S, uint32_t c) {
+    uint32_t b = S.colOwner[c];
+    return xyz(S.posLin[b]) + q_rotate(S.posAng[b], xyz(S.colLocalPos[c]));
+}
+
+static bool pair_excluded(const std::vector<uint32_t>& ex, uint32_t a, uint32_t b) {
+    uint32_t lo = 0, hi = (uint32_t)(ex.size() / 2);
+    uint32_t count = hi;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        uint32_t ex_ = ex[2 * mid], ey = ex[2 * mid + 1];
+        if (ex_ < a || (ex_ == a && ey < b)) lo = mid + 1; else hi = mid;
+    }
+    if (lo >= count) return false;
+    return ex[2 * lo] == a && ex[2 * lo + 1] == b;
+}
+
+uint32_t Solver::process_producer(uint32_t producer, bool emit, uint32_t base) {
+    uint32_t count = 0;
+    // Filters shared by the cell scan and the globals scan; every filter is a
+    // pure predicate, so their order does not change the emitted set.
+    auto test = [&](uint32_t a, uint32_t b, F3 pa, float ra, uint32_t ownerA, bool aDyn,
+                    uint32_t outA, uint32_t outB) {
+        (void)a;
+        uint32_t ownerB = colOwner[b];
+        if (ownerA == ownerB) return;
+        if (!aDyn && posLin[ownerB].w <= 0.0f) return;
+        float rb = std::fabs(colShape[b].w);
+        F3 pb = collider_center(*this, b);
+        F3 dp = pa - pb;
+        float r = ra + rb;
+        if (dot(dp, dp) > r * r) return;
+        uint32_t lo = std::min(ownerA, ownerB), hi = std::max(ownerA, ownerB);
+        if (pair_excluded(exclusions, lo, hi)) return;
+        uint32_t slot = base + count;
+        if (emit && slot < P.maxPairs) { pairs[2 * slot] = outA; pairs[2 * slot + 1] = outB; }
+        count++;
+    };
+    if (producer < P.numHashed) {
+        uint32_t a = hashedIdx[producer];
+        uint32_t ownerA = colOwner[a];
+        uint32_t groupA = colGroup[a];
+        F3 pa = collider_center(*this, a);
+        float ra = std::fabs(colShape[a].w);
+        bool aDyn = posLin[ownerA].w > 0.0f;
+        uint32_t ga = clothGroup[ownerA];
+        bool scanCells = !(ga != 0 && P.numHashedRigid == 0);
+        int cx, cy, cz;
+        cell_coord(pa, P.cellSize, cx, cy, cz);
+        if (scanCells) {
+            uint32_t visited[27];
+            uint32_t nv = 0;
+            for (int dz = -1; dz <= 1; dz++)
+                for (int dy = -1; dy <= 1; dy++)
+                    for (int dx = -1; dx <= 1; dx++) {
+                        uint32_t h = cell_hash(cx + dx, cy + dy, cz + dz, groupA, P.gridHashSize);
+                        bool dup = false;
+                        for (uint32_t v = 0; v < nv; v++) if (visited[v] == h) { dup = true; break; }
+                        if (dup) continue;
+                        visited[nv++] = h;
+                        if (ga != 0 && cellRigid[h] == 0) continue;
+                        uint32_t s0 = cellStart[h], e0 = s0 + cellCount[h];
+                        for (uint32_t k = s0; k < e0; k++) {
+                            uint32_t b = cellBodies[k];
+                            if (b <= a) continue;
+                            if (!domains_compatible(groupA, colGroup[b], colShared[a], colShared[b])) continue;
+                            // soft surface vs soft surface: element contacts own it
+                            if (ga != 0 && clothGroup[colOwner[b]] != 0) continue;
+                            test(a, b, pa, ra, ownerA, aDyn, a, b);
+                        }
+                    }
+        }
+        for (uint32_t g = 0; g < P.numGlobals; g++) {
+            uint32_t b = globalIdx[g];
+            if (!domains_compatible(groupA, colGroup[b], colShared[a], colShared[b])) continue;
+            if (ga != 0 && clothGroup[colOwner[b]] == ga) continue;
+            test(a, b, pa, ra, ownerA, aDyn, std::min(a, b), std::max(a, b));
+        }
+    } else {
+        uint32_t gp = producer - P.numHashed;
+        if (gp >= P.numGlobals) return 0;
+        uint32_t a = globalIdx[gp];
+        uint32_t ownerA = colOwner[a];
+        uint32_t groupA = colGroup[a];
+        F3 pa = collider_center(*this, a);
+        float ra = std::fabs(colShape[a].w);
+        bool aDyn = posLin[ownerA].w > 0.0f;
+        uint32_t ga = clothGroup[ownerA];
+        for (uint32_t g = gp + 1; g < P.numGlobals; g++) {
+            uint32_t b = globalIdx[g];
+            if (!domains_compatible(groupA, colGroup[b], colShared[a], colShared[b])) continue;
+            if (ga != 0 && clothGroup[colOwner[b]] == ga) continue;
+            test(a, b, pa, ra, ownerA, aDyn, std::min(a, b), std::max(a, b));
+        }
+    }
+    return count;
+}
+
+void Solver::broadphase() {
+    std::fill(cellCount.begin(), cellCount.end(), 0u);
+    std::fill(cellRigid.begin(), cellRigid.end(), 0u);
+    std::vector<uint32_t> cellOf(P.numHashed);
+    for (uint32_t i = 0; i < P.numHashed; i++) {
+        uint32_t b = hashedIdx[i];
+        F3 c = collider_center(*this, b);
+        int x, y, z;
+        cell_coord(c, P.cellSize, x, y, z);
+        uint32_t h = cell_hash(x, y, z, colGroup[b], P.gridHashSize);
+        cellOf[i] = h;
+        cellCount[h]++;
+        if (colShape[b].w >= 0.0f) cellRigid[h] = 1u;
+    }
+    uint32_t run = 0;
+    for (uint32_t h = 0; h < P.gridHashSize; h++) { cellStart[h] = run; run += cellCount[h]; }
+    std::vector<uint32_t> cursor(cellStart);
+    for (uint32_t i = 0; i < P.numHashed; i++) cellBodies[cursor[cellOf[i]]++] = hashedIdx[i];
+    for (uint32_t h = 0; h < P.gridHashSize; h++)
+        std::sort(cellBodies.begin() + cellStart[h], cellBodies.begin() + cellStart[h] + cellCount[h]);
+
+    uint32_t producers = P.numHashed + P.numGlobals;
+    pairCount.assign(producers, 0);
+    pairStart.assign(producers, 0);
+    for (uint32_t p = 0; p < producers; p++) pairCount[p] = process_producer(p, false, 0);
+    run = 0;
+    for (uint32_t p = 0; p < producers; p++) { pairStart[p] = run; run += pairCount[p]; }
+    for (uint32_t p = 0; p < producers; p++) process_producer(p, true, pairStart[p]);
+    pairCandidates = run;
+    numPairs = std::min(run, P.maxPairs);
+}
+
+// ==========================================================================
+// Narrowphase: sphere/sphere, sphere/box, box/box (30_narrowphase.metal)
+// ==========================================================================
+struct Box { F3 center, half; F3 ax[3]; };
+struct AxisBest { int type, ia, ib; float sep; F3 n; bool valid; };
+static const float SAT_EPS = 1.0e-6f, PLANE_EPS = 1.0e-5f, MERGE_DIST_SQ = 1.0e-6f;
+static const int NP_MAX_POLY = 16;
+
+static inline float box_half(const Box& b, int i) { return comp(b.half, i); }
+
+static float spec_cap(float ra, float rb, float margin) {
+    float r = fmin_(std::fabs(ra), std::fabs(rb));
+    return fmin_(0.25f, fmax_(4.0f * margin, 3.0f * r));
+}
+static float detect_margin(F3 n, F3 relVel, const Params& P, float ra, float rb) {
+    float approach = fmax_(0.0f, -dot(relVel, n));
+    float allowed = fmin_(approach * P.dt, spec_cap(ra, rb, P.collisionMargin));
+    return P.collisionMargin + allowed;
+}
+static bool test_axis(const Box& A, const Box& B, F3 delta, F3 axis, int type, int ia, int ib,
+                      F3 relVel, float cap, const Params& P, AxisBest& best) {
+    float lenSq = dot(axis, axis);
+    if (lenSq < SAT_EPS) return true;
+    F3 n = axis * rsqrt_(lenSq);
+    if (dot(n, delta) < 0.0f) n = -n;
+    float dist = std::fabs(dot(delta, n));
+    float rA = A.half.x * std::fabs(dot(n, A.ax[0])) + A.half.y * std::fabs(dot(n, A.ax[1]))
+             + A.half.z * std::fabs(dot(n, A.ax[2]));
+    float rB = B.half.x * std::fabs(dot(n, B.ax[0])) + B.half.y * std::fabs(dot(n, B.ax[1]))
+             + B.half.z * std::fabs(dot(n, B.ax[2]));
+    float sep = dist - (rA + rB);
+    float approach = fmax_(0.0f, -dot(relVel, n));
+    float allowed = fmin_(approach * P.dt, cap);
+    if (sep > allowed) return false;
+    if (!best.valid || sep > best.sep) { best.valid = true; best.type = type; best.ia = ia; best.ib = ib; best.sep = sep; best.n = n; }
+    return true;
+}
+static F3 support(const Box& b, F3 dir) {
+    float sx = dot(dir, b.ax[0]) >= 0.0f ? 1.0f : -1.0f;
+    float sy = dot(dir, b.ax[1]) >= 0.0f ? 1.0f : -1.0f;
+    float sz = dot(dir, b.ax[2]) >= 0.0f ? 1.0f : -1.0f;
+    return b.center + b.ax[0] * (b.half.x * sx) + b.ax[1] * (b.half.y * sy) + b.ax[2] * (b.half.z * sz);
+}
+static void face_axes(const Box& b, int i, F3& u, F3& v, float& eu, float& ev) {
+    if (i == 0) { u = b.ax[1]; v = b.ax[2]; eu = b.half.y; ev = b.half.z; }
+    else if (i == 1) { u = b.ax[0]; v = b.ax[2]; eu = b.half.x; ev = b.half.z; }
+    else { u = b.ax[0]; v = b.ax[1]; eu = b.half.x; ev = b.half.y; }
+}
+static int clip_poly(const F3* in, int n, F3 nrm, float off, F3* out) {
+    if (n <= 0) return 0;
+    int m = 0;
+    F3 a = in[n - 1];
+    float da = dot(nrm, a) - off;
+    for (int i = 0; i < n; i++) {
+        F3 b = in[i];
+        float db = dot(nrm, b) - off;
+        bool aIn = da <= PLANE_EPS, bIn = db <= PLANE_EPS;
+        if (aIn != bIn) {
+            float t = 0.0f, den = da - db;
+            if (std::fabs(den) > SAT_EPS) t = clampf_(da / den, 0.0f, 1.0f);
+            if (m < NP_MAX_POLY) out[m++] = a + (b - a) * t;
+        }
+        if (bIn && m < NP_MAX_POLY) out[m++] = b;
+        a = b; da = db;
+    }
+    return m;
+}
+static void support_edge(const Box& b, int axis, F3 dir, F3& eA, F3& eB) {
+    int a1 = (axis + 1) % 3, a2 = (axis + 2) % 3;
+    float s1 = dot(dir, b.ax[a1]) >= 0.0f ? 1.0f : -1.0f;
+    float s2 = dot(dir, b.ax[a2]) >= 0.0f ? 1.0f : -1.0f;
+    F3 c = b.center + b.ax[a1] * (box_half(b, a1) * s1) + b.ax[a2] * (box_half(b, a2) * s2);
+    eA = c - b.ax[axis] * box_half(b, axis);
+    eB = c + b.ax[axis] * box_half(b, axis);
+}
+static void closest_seg_seg(F3 p0, F3 p1, F3 q0, F3 q1, F3& c0, F3& c1) {
+    F3 d1 = p1 - p0, d2 = q1 - q0, r = p0 - q0;
+    float a = dot(d1, d1), e = dot(d2, d2), f = dot(d2, r);
+    float s = 0.0f, t = 0.0f;
+    if (a <= SAT_EPS && e <= SAT_EPS) { c0 = p0; c1 = q0; return; }
+    if (a <= SAT_EPS) {
+        t = clampf_(f / e, 0.0f, 1.0f);
+    } else {
+        float c = dot(d1, r);
+        if (e <= SAT_EPS) {
+            s = clampf_(-c / a, 0.0f, 1.0f);
+        } else {
+            float b = dot(d1, d2);
+            float den = a * e - b * b;
+            if (std::fabs(den) > SAT_EPS) s = clampf_((b * f - c * e) / den, 0.0f, 1.0f);
+            t = (b * s + f) / e;
+            if (t < 0.0f) { t = 0.0f; s = clampf_(-c / a, 0.0f, 1.0f); }
+            else if (t > 1.0f) { t = 1.0f; s = clampf_((b - c) / a, 0.0f, 1.0f); }
+        }
+    }
+    c0 = p0 + d1 * s;
+    c1 = q0 + d2 * t;
+}
+struct NPContact { F3 xA, xB; uint32_t feature; };
+static bool add_contact(NPContact* cs, int& count, F3* mids, F3 xA, F3 xB, uint32_t feature) {
+    F3 mid = (xA + xB) * 0.5f;
+    for (int i = 0; i < count; i++) if (distance2(mid, mids[i]) < MERGE_DIST_SQ) return false;
+    if (count >= MAX_CONTACTS) return false;
+    cs[count] = NPContact{xA, xB, feature};
+    mids[count] = mid;
+    count++;
+    return true;
+}
+// Tangential target shift of a kinematic spinner surface (30_narrowphase.metal:274-284).
+static void spin_shift(F4 wA, F4 wB, F3 rAoff, F3 rBoff, F3 t1, F3 t2, float dt, float alpha,
+                       float& sx, float& sy) {
+    F3 sA = wA.w != 0.0f ? cross(xyz(wA), rAoff) * dt : f3s(0);
+    F3 sB = wB.w != 0.0f ? cross(xyz(wB), rBoff) * dt : f3s(0);
+    F3 rel = sB - sA;
+    float k = 1.0f / fmax_(1.0f - alpha, 0.01f);
+    sx = dot(t1, rel) * k;
+    sy = dot(t2, rel) * k;
+}
+static F3 penalty_floor(const Solver& S, uint32_t ia, uint32_t ib) {
+    float mA = S.posLin[ia].w, mB = S.posLin[ib].w;
+    float minMass = fmin_(mA > 0.0f ? mA : FLT_MAX, mB > 0.0f ? mB : FLT_MAX);
+    if (minMass == FLT_MAX) return f3s(PENALTY_MIN);
+    float k = fmin_(PENALTY_MAX, fmax_(PENALTY_MIN, minMass / fmax_(S.P.dt * S.P.dt, 1e-12f)));
+    return f3(k, fmin_(k, PENALTY_MAX_T), fmin_(k, PENALTY_MAX_T));
+}
+
+int Solver::map_find(uint32_t a, uint32_t b) const {
+    uint32_t h = pair_map_hash(a, b, P.mapCapacity);
+    for (uint32_t probe = 0; probe < P.mapCapacity; probe++) {
+        uint32_t ka = mapKeyA[h];
+        if (ka == 0) return -1;
+        if (ka == a + 1 && mapKeyB[h] == b) return (int)mapVal[h];
+        h = (h + 1) & (P.mapCapacity - 1u);
+    }
+    return -1;
+}
+
+void Solver::narrow_one(uint32_t gid) {
+    uint32_t ia = pairs[2 * gid], ib = pairs[2 * gid + 1];
+    uint32_t ba = colOwner[ia], bb = colOwner[ib];
+    F4 bodyPA = posLin[ba], bodyPB = posLin[bb];
+    F4 qBodyA = posAng[ba], qBodyB = posAng[bb];
+    F3 centerA = xyz(bodyPA) + q_rotate(qBodyA, xyz(colLocalPos[ia]));
+    F3 centerB = xyz(bodyPB) + q_rotate(qBodyB, xyz(colLocalPos[ib]));
+    F4 qA = q_mul(qBodyA, colLocalRot[ia]);
+    F4 qB = q_mul(qBodyB, colLocalRot[ib]);
+    F3 vA = xyz(velLin[ba]) + cross(xyz(velAng[ba]), centerA - xyz(bodyPA));
+    F3 vB = xyz(velLin[bb]) + cross(xyz(velAng[bb]), centerB - xyz(bodyPB));
+    F3 relVel = vB - vA;
+    Box A, B;
+    A.center = centerA; A.half = xyz(colShape[ia]) * 0.5f;
+    A.ax[0] = q_rotate(qA, f3(1, 0, 0)); A.ax[1] = q_rotate(qA, f3(0, 1, 0)); A.ax[2] = q_rotate(qA, f3(0, 0, 1));
+    B.center = centerB; B.half = xyz(colShape[ib]) * 0.5f;
+    B.ax[0] = q_rotate(qB, f3(1, 0, 0)); B.ax[1] = q_rotate(qB, f3(0, 1, 0)); B.ax[2] = q_rotate(qB, f3(0, 0, 1));
+    F3 delta = B.center - A.center;
+    ManifoldGPU& outM = manifolds[gid];
+    outM.colliderPair = U4{ia, ib, 0, 0};
+    uint32_t stA = colShapeType[ia] & 0xFu, stB = colShapeType[ib] & 0xFu;
+    bool sphA = stA == 1, sphB = stB == 1;
+    if (stA >= 2 || stB >= 2) { outM.header = U4{ba, bb, 0, 0}; return; }
+
+    NPContact contacts[MAX_CONTACTS];
+    int count = 0;
+    F3 nrm;
+    const float warm = P.alpha * P.gamma;
+    if (sphA || sphB) {
+        float rA = colShape[ia].x * 0.5f, rB = colShape[ib].x * 0.5f;
+        if (sphA && sphB) {
+            F3 d = A.center - B.center;
+            float dist = length(d);
+            F3 nT = dist > 1e-9f ? d / dist : f3(0, 0, 1);
+            float dm = detect_margin(nT, vA - vB, P, rA, rB);
+            if (dist > rA + rB + dm) { outM.header = U4{ba, bb, 0, 0}; return; }
+            nrm = nT;
+            contacts[0] = NPContact{A.center - nrm * rA, B.center + nrm * rB, 0};
+            count = 1;
+        } else {
+            bool sIsA = sphA;
+            float r = sIsA ? rA : rB;
+            const Box& box = sIsA ? B : A;
+            F4 qBox = sIsA ? qB : qA;
+            F3 sc = sIsA ? A.center : B.center;
+            F3 local = q_rotate(q_conj(qBox), sc - box.center);
+            F3 h = box.half;
+            F3 cl = clamp3(local, -h, h);
+            F3 nLocal, qLocal;
+            if (cl.x == local.x && cl.y == local.y && cl.z == local.z) {
+                F3 pen = h - abs3(local);
+                int axis = 0;
+                if (pen.y < comp(pen, axis)) axis = 1;
+                if (pen.z < comp(pen, axis)) axis = 2;
+                F3 n = f3s(0);
+                setcomp(n, axis, comp(local, axis) >= 0.0f ? 1.0f : -1.0f);
+                nLocal = n;
+                qLocal = local;
+                setcomp(qLocal, axis, comp(n, axis) * comp(h, axis));
+            } else {
+                F3 d = local - cl;
+                float dist = length(d);
+                F3 nLT = d / fmax_(dist, 1e-9f);
+                F3 nWT = q_rotate(qBox, nLT);
+                F3 vS = sIsA ? vA : vB, vBx = sIsA ? vB : vA;
+                float dm = detect_margin(nWT, vS - vBx, P, r, sIsA ? colShape[ib].w : colShape[ia].w);
+                if (dist > r + dm) { outM.header = U4{ba, bb, 0, 0}; return; }
+                nLocal = nLT;
+                qLocal = cl;
+            }
+            F3 nW = q_rotate(qBox, nLocal);
+            F3 qW = q_rotate(qBox, qLocal) + box.center;
+            F3 xS = sc - nW * r;
+            nrm = sIsA ? nW : -nW;
+            contacts[0] = NPContact{sIsA ? xS : qW, sIsA ? qW : xS, 0};
+            count = 1;
+        }
+        F3 t1, t2;
+        orthonormal(nrm, t1, t2);
+        float sf = combine_friction(colFrictionS[ia], colFrictionS[ib], P.frictionCombineMode);
+        float df = combine_friction(colFrictionD[ia], colFrictionD[ib], P.frictionCombineMode);
+        int prev = map_find(ia, ib);
+        bool roundA = (colShapeType[ia] & 0x20u) != 0, roundB = (colShapeType[ib] & 0x20u) != 0;
+        uint32_t flags = 1u | (roundA ? 2u : 0u) | (roundB ? 4u : 0u);
+        outM.header = U4{ba, bb, (uint32_t)count, flags};
+        outM.basisN = f4(nrm, df);
+        outM.basisT1 = f4(t1, sf);
+        F4 qAc = q_conj(qBodyA), qBc = q_conj(qBodyB);
+        for (int i = 0; i < count; i++) {
+            F3 rA_ = roundA ? contacts[i].xA - xyz(bodyPA) : q_rotate(qAc, contacts[i].xA - xyz(bodyPA));
+            F3 rB_ = roundB ? contacts[i].xB - xyz(bodyPB) : q_rotate(qBc, contacts[i].xB - xyz(bodyPB));
+            F3 lambda = f3s(0), penalty = f3s(0);
+            float stick = 0.0f;
+            if (prev >= 0) {
+                const ManifoldGPU& pm = prevManifolds[prev];
+                uint32_t pn = pm.header.z;
+                float bestD = 0.5f * fmax_(rA, rB);
+                int bestJ = -1;
+                for (uint32_t j = 0; j < pn; j++) {
+                    float dj = distance(xyz(pm.contacts[j].rA), rA_);
+                    if (dj < bestD) { bestD = dj; bestJ = (int)j; }
+                }
+                if (bestJ >= 0) {
+                    lambda = xyz(pm.contacts[bestJ].lambda);
+                    penalty = xyz(pm.contacts[bestJ].penalty);
+                    F3 t1o = xyz(pm.basisT1);
+                    F3 t2o = cross(xyz(pm.basisN), t1o);
+                    F3 lt = t1o * lambda.y + t2o * lambda.z;
+                    lambda.y = dot(t1, lt);
+                    lambda.z = dot(t2, lt);
+                    bool partA = colShape[ia].w < 0.0f, partB = colShape[ib].w < 0.0f;
+                    if ((partA || !roundA) && (partB || !roundB)) {
+                        stick = pm.contacts[bestJ].rB.w;
+                        if (stick != 0.0f) { rA_ = xyz(pm.contacts[bestJ].rA); rB_ = xyz(pm.contacts[bestJ].rB); }
+                    }
+                }
+            }
+            F3 xAw = roundA ? xyz(bodyPA) + rA_ : xform(xyz(bodyPA), qBodyA, rA_);
+            F3 xBw = roundB ? xyz(bodyPB) + rB_ : xform(xyz(bodyPB), qBodyB, rB_);
+            F3 d = xAw - xBw;
+            F3 C0 = f3(dot(nrm, d) + P.collisionMargin, dot(t1, d), dot(t2, d));
+            float sx, sy;
+            spin_shift(spinVel[ba], spinVel[bb], xAw - xyz(bodyPA), xBw - xyz(bodyPB), t1, t2, P.dt, P.alpha, sx, sy);
+            C0.y -= sx; C0.z -= sy;
+            lambda *= warm;
+            F3 lo = penalty_floor(*this, ba, bb);
+            F3 hi = f3(PENALTY_MAX, PENALTY_MAX_T, PENALTY_MAX_T);
+            penalty = clamp3(penalty * P.gamma, lo, hi);
+            outM.contacts[i].rA = f4(rA_, bitsf(contacts[i].feature));
+            outM.contacts[i].rB = f4(rB_, stick);
+            outM.contacts[i].C0 = f4(C0, 0);
+            outM.contacts[i].lambda = f4(lambda, 0);
+            outM.contacts[i].penalty = f4(penalty, 0);
+        }
+        return;
+    }
+
+    // box - box SAT (30_narrowphase.metal:1138-1321)
+    AxisBest bestFace{0, 0, 0, -FLT_MAX, f3s(0), false};
+    AxisBest bestEdge{0, 0, 0, -FLT_MAX, f3s(0), false};
+    float cap = spec_cap(colShape[ia].w, colShape[ib].w, P.collisionMargin);
+    bool separated = false;
+    for (int i = 0; i < 3 && !separated; i++)
+        if (!test_axis(A, B, delta, A.ax[i], 0, i, -1, relVel, cap, P, bestFace)) separated = true;
+    for (int i = 0; i < 3 && !separated; i++)
+        if (!test_axis(A, B, delta, B.ax[i], 1, -1, i, relVel, cap, P, bestFace)) separated = true;
+    for (int i = 0; i < 3 && !separated; i++)
+        for (int j = 0; j < 3 && !separated; j++)
+            if (!test_axis(A, B, delta, cross(A.ax[i], B.ax[j]), 2, i, j, relVel, cap, P, bestEdge)) separated = true;
+    if (separated || !bestFace.valid) { outM.header = U4{ba, bb, 0, 0}; return; }
+    AxisBest best = bestFace;
+    if (bestEdge.valid && 0.95f * bestEdge.sep > bestFace.sep + 0.01f) best = bestEdge;
+    F3 mids[MAX_CONTACTS];
+    if (best.type == 2) {
+        F3 a0, a1, b0, b1, xA, xB;
+        support_edge(A, best.ia, best.n, a0, a1);
+        support_edge(B, best.ib, -best.n, b0, b1);
+        closest_seg_seg(a0, a1, b0, b1, xA, xB);
+        uint32_t feature = (2u << 24) | ((uint32_t)(best.ia & 0xFF) << 8) | (uint32_t)(best.ib & 0xFF);
+        add_contact(contacts, count, mids, xA, xB, feature);
+        if (count == 0) add_contact(contacts, count, mids, support(A, best.n), support(B, -best.n), feature);
+    } else {
+        bool refIsA = best.type == 0;
+        int refAxis = refIsA ? best.ia : best.ib;
+        const Box& ref = refIsA ? A : B;
+        const Box& inc = refIsA ? B : A;
+        F3 refOut = refIsA ? best.n : -best.n;
+        float signR = dot(refOut, ref.ax[refAxis]) >= 0.0f ? 1.0f : -1.0f;
+        F3 refN = ref.ax[refAxis] * signR;
+        F3 refC = ref.center + refN * box_half(ref, refAxis);
+        F3 refU, refV; float refEU, refEV;
+        face_axes(ref, refAxis, refU, refV, refEU, refEV);
+        int incAxis = 0;
+        float bestD = -FLT_MAX;
+        for (int i = 0; i < 3; i++) {
+            float d = std::fabs(dot(inc.ax[i], refN));
+            if (d > bestD) { bestD = d; incAxis = i; }
+        }
+        float signI = dot(inc.ax[incAxis], refN) > 0.0f ? -1.0f : 1.0f;
+        F3 incN = inc.ax[incAxis] * signI;
+        F3 incC = inc.center + incN * box_half(inc, incAxis);
+        F3 incU, incV; float incEU, incEV;
+        face_axes(inc, incAxis, incU, incV, incEU, incEV);
+        F3 p0[NP_MAX_POLY], p1[NP_MAX_POLY];
+        p0[0] = incC + incU * incEU + incV * incEV;
+        p0[1] = incC - incU * incEU + incV * incEV;
+        p0[2] = incC - incU * incEU - incV * incEV;
+        p0[3] = incC + incU * incEU - incV * incEV;
+        int n = 4;
+        n = clip_poly(p0, n, refU, dot(refU, refC) + refEU, p1);
+        n = clip_poly(p1, n, -refU, dot(-refU, refC) + refEU, p0);
+        n = clip_poly(p0, n, refV, dot(refV, refC) + refEV, p1);
+        n = clip_poly(p1, n, -refV, dot(-refV, refC) + refEV, p0);
+        uint32_t prefix = (refIsA ? 0u : 1u) << 24;
+        prefix |= (uint32_t)(refAxis & 0xFF) << 16;
+        prefix |= (uint32_t)(incAxis & 0xFF) << 8;
+        float slop = PLANE_EPS + fmax_(0.0f, best.sep);
+        for (int i = 0; i < n && count < MAX_CONTACTS; i++) {
+            F3 pInc = p0[i];
+            float d = dot(pInc - refC, refN);
+            if (d > slop) continue;
+            F3 pRef = pInc - refN * d;
+            add_contact(contacts, count, mids, refIsA ? pRef : pInc, refIsA ? pInc : pRef, prefix | (uint32_t)(i & 0xFF));
+        }
+        if (count == 0) add_contact(contacts, count, mids, support(A, best.n), support(B, -best.n), prefix);
+    }
+    nrm = -best.n;
+    F3 t1, t2;
+    orthonormal(nrm, t1, t2);
+    float sf = combine_friction(colFrictionS[ia], colFrictionS[ib], P.frictionCombineMode);
+    float df = combine_friction(colFrictionD[ia], colFrictionD[ib], P.frictionCombineMode);
+    int prev = map_find(ia, ib);
+    outM.header = U4{ba, bb, (uint32_t)count, 1u};
+    outM.basisN = f4(nrm, df);
+    outM.basisT1 = f4(t1, sf);
+    F4 qAc = q_conj(qBodyA), qBc = q_conj(qBodyB);
+    for (int i = 0; i < count; i++) {
+        F3 rA = q_rotate(qAc, contacts[i].xA - xyz(bodyPA));
+        F3 rB = q_rotate(qBc, contacts[i].xB - xyz(bodyPB));
+        F3 lambda = f3s(0), penalty = f3s(0);
+        float stick = 0.0f;
+        if (prev >= 0) {
+            const ManifoldGPU& pm = prevManifolds[prev];
+            for (uint32_t j = 0; j < pm.header.z; j++) {
+                if (fbits(pm.contacts[j].rA.w) == contacts[i].feature) {
+                    lambda = xyz(pm.contacts[j].lambda);
+                    penalty = xyz(pm.contacts[j].penalty);
+                    stick = pm.contacts[j].rB.w;
+                    if (stick != 0.0f) { rA = xyz(pm.contacts[j].rA); rB = xyz(pm.contacts[j].rB); }
+                    break;
+                }
+            }
+        }
+        F3 xAw = xform(xyz(bodyPA), qBodyA, rA);
+        F3 xBw = xform(xyz(bodyPB), qBodyB, rB);
+        F3 d = xAw - xBw;
+        F3 C0 = f3(dot(nrm, d) + P.collisionMargin, dot(t1, d), dot(t2, d));
+        float sx, sy;
+        spin_shift(spinVel[ba], spinVel[bb], xAw - xyz(bodyPA), xBw - xyz(bodyPB), t1, t2, P.dt, P.alpha, sx, sy);
+        C0.y -= sx; C0.z -= sy;
+        lambda *= warm;
+        penalty = clamp3(penalty * P.gamma, penalty_floor(*this, ba, bb), f3(PENALTY_MAX, PENALTY_MAX_T, PENALTY_MAX_T));
+        outM.contacts[i].rA = f4(rA, bitsf(contacts[i].feature));
+        outM.contacts[i].rB = f4(rB, stick);
+        outM.contacts[i].C0 = f4(C0, 0);
+        outM.contacts[i].lambda = f4(lambda, 0);
+        outM.contacts[i].penalty = f4(penalty, 0);
+    }
+}
+
+void Solver::narrowphase() {
+    for (uint32_t g = 0; g < numPairs; g++) narrow_one(g);
+}
+
+// Persistence map rebuilt from this frame's manifolds, queried next frame
+// (20_broadphase.metal:555-593).  Serial insertion in manifold order.
+void Solver::map_rebuild() {
+    std::fill(mapKeyA.begin(), mapKeyA.end(), 0u);
+    for (uint32_t g = 0; g < numPairs; g++) {
+        const ManifoldGPU& m = manifolds[g];
+        if (m.header.z == 0) continue;
+        uint32_t a = m.colliderPair.x, b = m.colliderPair.y;
+        uint32_t h = pair_map_hash(a, b, P.mapCapacity);
+        for (uint32_t probe = 0; probe < P.mapCapacity; probe++) {
+            if (mapKeyA[h] == 0) { mapKeyA[h] = a + 1; mapKeyB[h] = b; mapVal[h] = g; break; }
+            h = (h + 1) & (P.mapCapacity - 1u);
+        }
+    }
+}
+
+// ==========================================================================
+// Warm start (40_solver.metal:546-722)
+// ==========================================================================
+static float twist_angle(F4 qAr, F4 qB, F3 axis) {
+    F4 r = q_mul(q_inv(qAr), qB);
+    if (r.w < 0.0f) r = -r;
+    return 2.0f * std::atan2(dot(xyz(r), axis), r.w);
+}
+
+void Solver::warmstart_joints() {
+    for (uint32_t si = 0; si < springs.size(); si++) {
+        SpringGPU& sp = springs[si];
+        if (sp.header.z == 0) continue;
+        uint32_t a = sp.header.x, b = sp.header.y;
+        F3 pA = xform(xyz(posLin[a]), posAng[a], xyz(sp.rA));
+        F3 pB = xform(xyz(posLin[b]), posAng[b], xyz(sp.rB));
+        sp.dual.z = 0.5f * fmax_(length(pA - pB) - sp.rB.w, 0.0f);
+        float warm = P.alpha * P.gamma;
+        if (P.rodDecayPow > 0.0f) {
+            F3 d = pA - pB;
+            F3 dPrev = d - (xyz(velLin[a]) - xyz(velLin[b])) * P.dt;
+            float dl = length(d), dpl = length(dPrev);
+            if (dl > 1e-7f && dpl > 1e-7f) {
+                float ct = clampf_(dot(d / dl, dPrev / dpl), 0.0f, 1.0f);
+                warm *= std::pow(ct, P.rodDecayPow);
+            }
+        }
+        sp.dual.x *= warm;
+        sp.dual.y = fmin_(clampf_(sp.dual.y * P.gamma, PENALTY_MIN, PENALTY_MAX), sp.rA.w);
+    }
+    for (uint32_t gid = 0; gid < joints.size(); gid++) {
+        JointGPU& j = joints[gid];
+        if (j.header.z != 0) continue;
+        uint32_t a = j.header.x, b = j.header.y;
+        F3 pA = a == WORLD_BODY ? xyz(j.rA) : xform(xyz(posLin[a]), posAng[a], xyz(j.rA));
+        F3 pB = xform(xyz(posLin[b]), posAng[b], xyz(j.rB));
+        F4 qA = a == WORLD_BODY ? f4(0, 0, 0, 1) : posAng[a];
+        float torqueArm = j.C0Lin.w;
+        j.C0Lin = f4(pA - pB, torqueArm);
+        F3 c0a;
+        F3 axis = xyz(j.hingeAxis);
+        if (j.hingeAxis.w != 0.0f) {
+            F3 aB = q_rotate(posAng[b], axis);
+            F3 aA = q_rotate(q_mul(qA, j.restRel), axis);
+            c0a = cross(aA, aB) * torqueArm;
+            if (j.dynamics.x > 0.0f) {
+                float twist = twist_angle(q_mul(qA, j.restRel), posAng[b], axis);
+                F3 omegaA = a == WORLD_BODY ? f3s(0) : xyz(velAng[a]);
+                float twistRate = dot(xyz(velAng[b]) - omegaA, aB);
+                j.dynamics.y = twist + P.dt * twistRate;
+            }
+        } else {
+            c0a = q_sub(q_mul(qA, j.restRel), posAng[b]) * torqueArm;
+        }
+        j.C0Ang = f4(c0a, j.C0Ang.w);
+        if (j.motor.y > 0.0f) {
+            j.motor.z = 0.0f;
+            j.dynamics.z = 0.0f;
+            uint32_t mode = j.header.w & MOTOR_MODE_MASK;
+            if (mode == MOTOR_EXPLICIT || mode == MOTOR_VELOCITY) {
+                F4 qAr = a == WORLD_BODY ? j.restRel : q_mul(posAng[a], j.restRel);
+                float twist = twist_angle(qAr, posAng[b], axis);
+                F3 axisW = q_rotate(posAng[b], axis);
+                F3 omegaA = a == WORLD_BODY ? f3s(0) : xyz(velAng[a]);
+                float twistRate = dot(xyz(velAng[b]) - omegaA, axisW);
+                if (mode == MOTOR_VELOCITY)
+                    j.dynamics.z = clampf_(j.limits.z * (j.motor.x - twistRate), -j.motor.y, j.motor.y);
+                else
+                    j.dynamics.z = clampf_(j.motor.w * (j.motor.x - twist) - j.limits.z * twistRate,
+                                           -j.motor.y, j.motor.y);
+            }
+        }
+        float warm = P.alpha * P.gamma;
+        float stiffLin = j.rA.w, stiffAng = j.rB.w;
+        j.lambdaLin.x *= warm; j.lambdaLin.y *= warm; j.lambdaLin.z *= warm;
+        j.lambdaAng.x *= warm; j.lambdaAng.y *= warm; j.lambdaAng.z *= warm;
+        F3 pl = clamp3(xyz(j.penaltyLin) * P.gamma, f3s(PENALTY_MIN), f3s(PENALTY_MAX));
+        F3 pa = clamp3(xyz(j.penaltyAng) * P.gamma, f3s(PENALTY_MIN), f3s(PENALTY_MAX));
+        pl = fmin3(pl, f3s(stiffLin));
+        pa = fmin3(pa, f3s(stiffAng));
+        j.penaltyLin = f4(pl, j.penaltyLin.w);
+        j.penaltyAng = f4(pa, j.penaltyAng.w);
+    }
+}
+
+void Solver::warmstart_bodies() {
+    const float dt = P.dt;
+    for (uint32_t gid = 0; gid < nb; gid++) {
+        F4 pl = posLin[gid], pa = posAng[gid];
+        float mass = pl.w;
+        F3 vl = xyz(velLin[gid]), va = xyz(velAng[gid]);
+        F3 inertial = xyz(pl) + vl * dt;
+        float bodyGravity = P.gravity * gravityScale[gid];
+        if (mass > 0.0f) inertial += f3(0, 0, bodyGravity) * (dt * dt);
+        inertLin[gid] = f4(inertial, 0);
+        inertAng[gid] = q_addw(pa, va * dt);
+        F3 accel = (vl - xyz(prevVelLin[gid])) / dt;
+        float gsign = P.gravity < 0.0f ? -1.0f : (P.gravity > 0.0f ? 1.0f : 0.0f);
+        float w = clampf_(accel.z * gsign / std::fabs(P.gravity), 0.0f, 1.0f);
+        if (!std::isfinite(w)) w = 0.0f;
+        initLin[gid] = f4(xyz(pl), 0);
+        initAng[gid] = pa;
+        if (P.surfaceTruncationMode != 0u && shape[gid].w < 0.0f) ogcPrev[gid] = f4(xyz(pl), 0);
+        if (mass > 0.0f) {
+            F3 guess = xyz(pl) + vl * dt + f3(0, 0, bodyGravity) * (w * dt * dt);
+            if (P.surfaceTruncationMode == 1u && shape[gid].w < 0.0f) {
+                float d2 = bitsf(boundsBits[gid]);
+                if (d2 < 1e37f) {
+                    float bv = fmax_(0.45f * std::sqrt(d2), -0.2f * shape[gid].w);
+                    F3 tot = guess - xyz(pl);
+                    float t2 = dot(tot, tot);
+                    if (t2 > bv * bv) guess = xyz(pl) + tot * (bv * rsqrt_(t2));
+                }
+            }
+            posLin[gid] = f4(guess, mass);
+            posAng[gid] = q_addw(pa, va * dt);
+        }
+    }
+}
+
+// ==========================================================================
+// Adjacency (40_solver.metal:27-243): per body, sorted (kind<<28 | index).
+// ==========================================================================
+void Solver::adjacency() {
+    std::vector<std::vector<uint32_t>> lists(nb);
+    auto add = [&](uint32_t b, uint32_t entry) { if (body_dynamic(b)) lists[b].push_back(entry); };
+    for (uint32_t g = 0; g < joints.size(); g++) {
+        const JointGPU& j = joints[g];
+        if (j.header.z != 0) continue;
+        if (j.rA.w == 0.0f && j.rB.w == 0.0f && j.motor.y == 0.0f) continue;
+        uint32_t e = (FK_JOINT << ADJ_KIND_SHIFT) | g;
+        add(j.header.x, e); add(j.header.y, e);
+    }
+    for (uint32_t s = 0; s < springs.size(); s++) {
+        uint32_t e = (FK_SPRING << ADJ_KIND_SHIFT) | s;
+        add(springs[s].header.x, e); add(springs[s].header.y, e);
+    }
+    for (uint32_t m = 0; m < numPairs; m++) {
+        if (manifolds[m].header.z == 0) continue;
+        uint32_t e = (FK_MANIFOLD << ADJ_KIND_SHIFT) | m;
+        add(manifolds[m].header.x, e); add(manifolds[m].header.y, e);
+    }
+    for (uint32_t t = 0; t < tets.size(); t++) {
+        uint32_t e = (FK_TET << ADJ_KIND_SHIFT) | t;
+        add(tets[t].ids.x, e); add(tets[t].ids.y, e); add(tets[t].ids.z, e); add(tets[t].ids.w, e);
+    }
+    adjStart.assign(nb, 0); adjCount.assign(nb, 0); adjList.clear();
+    for (uint32_t b = 0; b < nb; b++) {
+        std::sort(lists[b].begin(), lists[b].end());
+        adjStart[b] = (uint32_t)adjList.size();
+        adjCount[b] = (uint32_t)lists[b].size();
+        adjList.insert(adjList.end(), lists[b].begin(), lists[b].end());
+    }
+}
+
+// ==========================================================================
+// Dynamic coloring (40_solver.metal:250-540), rigid-only scenes.
+// ==========================================================================
+void Solver::neighbor_colors(uint32_t entry, uint32_t self, uint32_t myColor,
+                             const std::vector<uint32_t>& colorsIn, uint32_t& maskLo,
+                             uint32_t& maskHi, uint32_t& allLo, uint32_t& allHi,
+                             bool& conflict) const {
+    uint32_t kind = entry >> ADJ_KIND_SHIFT, idx = entry & ADJ_INDEX_MASK;
+    uint32_t nbs[3];
+    uint32_t n = 0;
+    if (kind == FK_TET) {
+        const U4& ids = tets[idx].ids;
+        for (uint32_t v : {ids.x, ids.y, ids.z, ids.w}) if (v != self && n < 3) nbs[n++] = v;
+    } else {
+        uint32_t a, b;
+        if (kind == FK_JOINT) { a = joints[idx].header.x; b = joints[idx].header.y; }
+        else if (kind == FK_SPRING) { a = springs[idx].header.x; b = springs[idx].header.y; }
+        else { a = manifolds[idx].header.x; b = manifolds[idx].header.y; }
+        nbs[0] = a == self ? b : a;
+        n = 1;
+    }
+    for (uint32_t k = 0; k < n; k++) {
+        uint32_t nbb = nbs[k];
+        if (nbb == WORLD_BODY || posLin[nbb].w <= 0.0f) continue;
+        uint32_t nc_ = colorsIn[nbb];
+        uint32_t lo = nc_ < 32 ? (1u << nc_) : 0u;
+        uint32_t hi = (nc_ >= 32 && nc_ < 64) ? (1u << (nc_ - 32)) : 0u;
+        allLo |= lo; allHi |= hi;
+        if (nbb < self) { maskLo |= lo; maskHi |= hi; if (nc_ == myColor) conflict = true; }
+    }
+}
+
+static inline uint32_t ctz32(uint32_t x) { return (uint32_t)__builtin_ctz(x); }
+
+void Solver::dynamic_coloring() {
+    const int passes = 20;
+    uint32_t changed[passes] = {};
+    std::vector<uint32_t>* src = &colorsA;
+    std::vector<uint32_t>* dst = &colorsB;
+    for (int pass = 0; pass < passes; pass++) {
+        if (!(pass > 0 && changed[pass - 1] == 0u)) {
+            for (uint32_t gid = 0; gid < nb; gid++) {
+                if (posLin[gid].w <= 0.0f) { (*dst)[gid] = 0; continue; }
+                uint32_t my = (*src)[gid];
+                uint32_t mLo = 0, mHi = 0, aLo = 0, aHi = 0;
+                bool conflict = false;
+                for (uint32_t k = adjStart[gid]; k < adjStart[gid] + adjCount[gid]; k++)
+                    neighbor_colors(adjList[k], gid, my, *src, mLo, mHi, aLo, aHi, conflict);
+                if (conflict) {
+                    uint32_t freeLo = ~mLo, nc_;
+                    if (freeLo != 0) nc_ = ctz32(freeLo);
+                    else { uint32_t freeHi = ~mHi; nc_ = freeHi != 0 ? 32 + ctz32(freeHi) : (MAX_COLORS - 1); }
+                    (*dst)[gid] = std::min<uint32_t>(nc_, MAX_COLORS - 1);
+                    changed[pass] |= 1u;
+                } else {
+                    uint32_t freeLo = ~aLo;
+                    uint32_t best = freeLo != 0 ? ctz32(freeLo) : (~aHi != 0 ? 32 + ctz32(~aHi) : my);
+                    (*dst)[gid] = best < my ? best : my;
+                    if (best < my) changed[pass] |= 1u;
+                }
+            }
+        }
+        std::swap(src, dst);
+    }
+    std::vector<uint32_t>& fin = *src;
+    if (changed[passes - 1] != 0u) {
+        for (uint32_t self = 0; self < nb; self++) {
+            if (posLin[self].w <= 0.0f) { fin[self] = 0; continue; }
+            uint32_t mLo = 0, mHi = 0, aLo = 0, aHi = 0;
+            bool conflict = false;
+            for (uint32_t k = adjStart[self]; k < adjStart[self] + adjCount[self]; k++)
+                neighbor_colors(adjList[k], self, fin[self], fin, mLo, mHi, aLo, aHi, conflict);
+            uint32_t freeLo = ~mLo;
+            if (freeLo != 0) fin[self] = ctz32(freeLo);
+            else { uint32_t freeHi = ~mHi; fin[self] = freeHi != 0 ? 32 + ctz32(freeHi) : (MAX_COLORS - 1); }
+        }
+    }
+    colorConflicts = 0;
+    for (uint32_t gid = 0; gid < nb; gid++) {
+        if (posLin[gid].w <= 0.0f) continue;
+        uint32_t mLo = 0, mHi = 0, aLo = 0, aHi = 0;
+        bool conflict = false;
+        for (uint32_t k = adjStart[gid]; k < adjStart[gid] + adjCount[gid]; k++)
+            neighbor_colors(adjList[k], gid, fin[gid], fin, mLo, mHi, aLo, aHi, conflict);
+        if (conflict) colorConflicts++;
+    }
+    for (int c = 0; c < MAX_COLORS; c++) colorCounts[c] = 0;
+    for (uint32_t gid = 0; gid < nb; gid++) if (posLin[gid].w > 0.0f) colorCounts[fin[gid]]++;
+    uint32_t run = 0, used = 0;
+    for (int c = 0; c < MAX_COLORS; c++) { colorStart[c] = run; run += colorCounts[c]; if (colorCounts[c]) used = c + 1; }
+    colorStart[MAX_COLORS] = run;
+    colorStart[MAX_COLORS + 1] = used;
+    colorList.assign(run, 0);
+    std::vector<uint32_t> cur(colorStart.begin(), colorStart.begin() + MAX_COLORS);
+    for (uint32_t gid = 0; gid < nb; gid++) if (posLin[gid].w > 0.0f) colorList[cur[fin[gid]]++] = gid;
+    if (src != &colorsA) colorsA = fin;
+}
+
+// ==========================================================================
+// Primal (40_solver.metal:741-1684): force stamps + 8-lane split reduction.
+// ==========================================================================
+static M3 geom_stiff_ball_socket(int k, F3 v) {
+    M3 m = m3_diag(f3s(-comp(v, k)));
+    if (k == 0) { m.r0.x += v.x; m.r1.x += v.y; m.r2.x += v.z; }
+    else if (k == 1) { m.r0.y += v.x; m.r1.y += v.y; m.r2.y += v.z; }
+    else { m.r0.z += v.x; m.r1.z += v.y; m.r2.z += v.z; }
+    return m;
+}
+static inline float wrap_pi(float x) {
+    return x - 6.2831853f * std::floor((x + 3.14159265f) / 6.2831853f);
+}
+
+void Solver::stamp_joint(const JointGPU& j, uint32_t self, Accum& acc) const {
+    uint32_t a = j.header.x, b = j.header.y;
+    bool isA = self == a;
+    float torqueArm = j.C0Lin.w;
+    F3 penLin = xyz(j.penaltyLin);
+    if (dot(penLin, penLin) > 0.0f) {
+        F3 pA = a == WORLD_BODY ? xyz(j.rA) : xform(xyz(posLin[a]), posAng[a], xyz(j.rA));
+        F3 pB = xform(xyz(posLin[b]), posAng[b], xyz(j.rB));
+        F3 C = pA - pB;
+        if (j.header.w & 1) C -= xyz(j.C0Lin) * P.alpha;
+        F3 F = penLin * C + xyz(j.lambdaLin);
+        float jsign = isA ? 1.0f : -1.0f;
+        F3 rW = isA ? q_rotate(posAng[a], xyz(j.rA)) : q_rotate(posAng[b], xyz(j.rB));
+        M3 jAng = m3_skew(-jsign * rW);
+        M3 jAngT = m3_transpose(jAng);
+        M3 K = m3_diag(penLin);
+        M3 jAngTk = m3_mulm(jAngT, K);
+        acc.lhsLin = m3_add(acc.lhsLin, K);
+        acc.lhsAng = m3_add(acc.lhsAng, m3_mulm(jAngTk, jAng));
+        acc.lhsCross = m3_add(acc.lhsCross, m3_scale(jAngTk, jsign));
+        F3 r = jsign * rW;
+        M3 H = m3_add(m3_add(m3_scale(geom_stiff_ball_socket(0, r), F.x),
+                             m3_scale(geom_stiff_ball_socket(1, r), F.y)),
+                      m3_scale(geom_stiff_ball_socket(2, r), F.z));
+        acc.lhsAng = m3_add(acc.lhsAng, m3_diagonalize(H));
+        acc.rhsLin += jsign * F;
+        acc.rhsAng += m3_mul(jAngT, F);
+    }
+    F3 penAng = xyz(j.penaltyAng);
+    if (dot(penAng, penAng) > 0.0f) {
+        F4 qA = a == WORLD_BODY ? f4(0, 0, 0, 1) : posAng[a];
+        F3 C = q_sub(q_mul(qA, j.restRel), posAng[b]) * torqueArm;
+        float s = (isA ? 1.0f : -1.0f) * torqueArm;
+        if (j.hingeAxis.w != 0.0f) {
+            F3 axis = xyz(j.hingeAxis);
+            F3 aB = q_rotate(posAng[b], axis);
+            F3 aA = q_rotate(q_mul(qA, j.restRel), axis);
+            C = cross(aA, aB) * torqueArm;
+            if (j.header.w & 2) C -= xyz(j.C0Ang) * P.alpha;
+            F3 F = penAng * C + xyz(j.lambdaAng);
+            float alignment = dot(aA, aB);
+            M3 J = isA ? m3_add(m3_outer(aA, aB), m3_scale(m3_identity(), -alignment))
+                       : m3_add(m3_scale(m3_identity(), alignment), m3_scale(m3_outer(aB, aA), -1.0f));
+            J = m3_scale(J, torqueArm);
+            M3 JT = m3_transpose(J);
+            M3 K = m3_diag(penAng);
+            acc.lhsAng = m3_add(acc.lhsAng, m3_mulm(m3_mulm(JT, K), J));
+            acc.rhsAng += m3_mul(JT, F);
+            if (j.motor.y > 0.0f || j.limits.x < j.limits.y) {
+                float twist = twist_angle(q_mul(qA, j.restRel), posAng[b], axis);
+                if (j.dynamics.x > 0.0f) {
+                    float Ca = wrap_pi(twist - j.dynamics.y);
+                    float ka = j.dynamics.x / fmax_(P.dt * P.dt, 1e-12f);
+                    float sm = (self == a) ? -1.0f : 1.0f;
+                    acc.lhsAng = m3_add(acc.lhsAng, m3_scale(m3_outer(aB, aB), ka));
+                    acc.rhsAng += aB * (ka * Ca * sm);
+                }
+                if (j.limits.x < j.limits.y) {
+                    float over = fmax_(twist - j.limits.y, 0.0f) + fmin_(twist - j.limits.x, 0.0f);
+                    if (over != 0.0f) {
+                        float kL = 4.0e4f;
+                        float FL = clampf_(kL * over, -3000.0f, 3000.0f);
+                        float sm = (self == a) ? -1.0f : 1.0f;
+                        acc.lhsAng = m3_add(acc.lhsAng, m3_scale(m3_outer(aB, aB), kL));
+                        acc.rhsAng += aB * (FL * sm);
+                    }
+                }
+                if (j.motor.y > 0.0f) {
+                    float sm = (self == a) ? -1.0f : 1.0f;
+                    F3 axW = aB;
+                    uint32_t mode = j.header.w & MOTOR_MODE_MASK;
+                    if (mode == MOTOR_EXPLICIT || mode == MOTOR_VELOCITY) {
+                        acc.rhsAng += axW * (-j.dynamics.z * sm);
+                    } else {
+                        float Cm = wrap_pi(twist - j.motor.x);
+                        F4 qA0 = a == WORLD_BODY ? f4(0, 0, 0, 1) : initAng[a];
+                        float twist0 = twist_angle(q_mul(qA0, j.restRel), initAng[b], axis);
+                        float dTwist = wrap_pi(twist - twist0);
+                        float cD = j.limits.z / fmax_(P.dt, 1e-6f);
+                        float raw = j.motor.w * Cm + cD * dTwist;
+                        float effort = clampf_(raw, -j.motor.y, j.motor.y);
+                        if (std::fabs(raw) < j.motor.y)
+                            acc.lhsAng = m3_add(acc.lhsAng, m3_scale(m3_outer(axW, axW), j.motor.w + cD));
+                        acc.rhsAng += axW * (effort * sm);
+                    }
+                }
+            }
+        } else {
+            if (j.header.w & 2) C -= xyz(j.C0Ang) * P.alpha;
+            F3 F = penAng * C + xyz(j.lambdaAng);
+            acc.lhsAng = m3_add(acc.lhsAng, m3_diag(penAng * (s * s)));
+            acc.rhsAng += F * s;
+        }
+    }
+}
+
+void Solver::stamp_spring(const SpringGPU& sp, uint32_t self, Accum& acc) const {
+    uint32_t a = sp.header.x, b = sp.header.y;
+    float stiffness = sp.rA.w, rest = sp.rB.w;
+    F3 pA = xform(xyz(posLin[a]), posAng[a], xyz(sp.rA));
+    F3 pB = xform(xyz(posLin[b]), posAng[b], xyz(sp.rB));
+    F3 d = pA - pB;
+    float dLen = length(d);
+    if (dLen <= 1.0e-6f) return;
+    F3 n = d / dLen;
+    float f;
+    if (sp.header.z != 0) {
+        float C = dLen - rest - sp.dual.z * P.alpha;
+        stiffness = sp.dual.y;
+        f = stiffness * C + sp.dual.x;
+        if (f <= 0.0f) return;
+    } else {
+        f = stiffness * (dLen - rest);
+    }
+    bool isA = self == a;
+    F3 rW = isA ? q_rotate(posAng[a], xyz(sp.rA)) : q_rotate(posAng[b], xyz(sp.rB));
+    F3 jLin = isA ? n : -n;
+    F3 jAng = isA ? cross(rW, n) : -cross(rW, n);
+    acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(jLin, jLin), stiffness));
+    acc.lhsAng = m3_add(acc.lhsAng, m3_scale(m3_outer(jAng, jAng), stiffness));
+    acc.lhsCross = m3_add(acc.lhsCross, m3_scale(m3_outer(jAng, jLin), stiffness));
+    acc.rhsLin += jLin * f;
+    acc.rhsAng += jAng * f;
+    float ft = fmax_(f, 0.0f) / dLen;
+    if (ft > 0.0f)
+        acc.lhsLin = m3_add(acc.lhsLin, m3_add(m3_diag(f3s(ft)), m3_scale(m3_outer(n, n), -ft)));
+}
+
+void Solver::stamp_tet(const TetGPU& t, uint32_t self, Accum& acc) const {
+    F3 x0 = xyz(posLin[t.ids.x]), x1 = xyz(posLin[t.ids.y]), x2 = xyz(posLin[t.ids.z]), x3 = xyz(posLin[t.ids.w]);
+    float muV = t.r1.w, lamV = t.r2.w;
+    float alphaT = 1.0f + muV / fmax_(lamV, 1e-9f);
+    F3 d0 = x1 - x0, d1 = x2 - x0, d2 = x3 - x0;
+    F3 m0 = xyz(t.r0), m1 = xyz(t.r1), m2 = xyz(t.r2);
+    F3 f0 = d0 * m0.x + d1 * m1.x + d2 * m2.x;
+    F3 f1 = d0 * m0.y + d1 * m1.y + d2 * m2.y;
+    F3 f2 = d0 * m0.z + d1 * m1.z + d2 * m2.z;
+    float J = dot(f0, cross(f1, f2));
+    F3 j0 = cross(f1, f2), j1 = cross(f2, f0), j2 = cross(f0, f1);
+    float s2 = lamV * (J - alphaT);
+    F3 p0 = muV * f0 + s2 * j0;
+    F3 p1 = muV * f1 + s2 * j1;
+    F3 p2 = muV * f2 + s2 * j2;
+    F3 w;
+    if (self == t.ids.y) w = m0;
+    else if (self == t.ids.z) w = m1;
+    else if (self == t.ids.w) w = m2;
+    else w = -f3(m0.x + m1.x + m2.x, m0.y + m1.y + m2.y, m0.z + m1.z + m2.z);
+    F3 grad = p0 * w.x + p1 * w.y + p2 * w.z;
+    F3 g = j0 * w.x + j1 * w.y + j2 * w.z;
+    acc.rhsLin += grad;
+    acc.lhsLin = m3_add(acc.lhsLin, m3_diag(f3s(muV * dot(w, w))));
+    acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(g, g), lamV));
+}
+
+void Solver::stamp_manifold(const ManifoldGPU& m, uint32_t self, Accum& acc) const {
+    uint32_t a = m.header.x, b = m.header.y, n = m.header.z;
+    bool isA = self == a;
+    bool sphA = (m.header.w & 2u) != 0, sphB = (m.header.w & 4u) != 0;
+    F3 dqALin = xyz(posLin[a]) - xyz(initLin[a]);
+    F3 dqAAng = q_sub(posAng[a], initAng[a]);
+    F3 dqBLin = xyz(posLin[b]) - xyz(initLin[b]);
+    F3 dqBAng = q_sub(posAng[b], initAng[b]);
+    F3 nrm = xyz(m.basisN), t1 = xyz(m.basisT1), t2 = cross(nrm, t1);
+    float dynF = m.basisN.w, statF = m.basisT1.w;
+    for (uint32_t i = 0; i < n; i++) {
+        const ContactGPU& c = m.contacts[i];
+        F3 rAW = sphA ? xyz(c.rA) : q_rotate(posAng[a], xyz(c.rA));
+        F3 rBW = sphB ? xyz(c.rB) : q_rotate(posAng[b], xyz(c.rB));
+        F3 C = xyz(c.C0) * (1.0f - P.alpha);
+        C += f3(dot(nrm, dqALin), dot(t1, dqALin), dot(t2, dqALin));
+        C -= f3(dot(nrm, dqBLin), dot(t1, dqBLin), dot(t2, dqBLin));
+        C += f3(dot(cross(rAW, nrm), dqAAng), dot(cross(rAW, t1), dqAAng), dot(cross(rAW, t2), dqAAng));
+        C -= f3(dot(cross(rBW, nrm), dqBAng), dot(cross(rBW, t1), dqBAng), dot(cross(rBW, t2), dqBAng));
+        F3 F = xyz(c.penalty) * C + xyz(c.lambda);
+        F.x = fmin_(F.x, 0.0f);
+        float bounds = std::fabs(F.x) * statF;
+        float fs = std::sqrt(F.y * F.y + F.z * F.z);
+        if (fs > bounds && fs > 0.0f) {
+            float db = std::fabs(F.x) * dynF;
+            float sc = db / fs;
+            F.y *= sc; F.z *= sc;
+        }
+        float s = isA ? 1.0f : -1.0f;
+        M3 jLin = M3{nrm * s, t1 * s, t2 * s};
+        F3 rW = isA ? rAW : rBW;
+        M3 jAng = M3{cross(rW, jLin.r0), cross(rW, jLin.r1), cross(rW, jLin.r2)};
+        M3 K = m3_diag(xyz(c.penalty));
+        M3 jLinT = m3_transpose(jLin), jAngT = m3_transpose(jAng);
+        M3 jAngTk = m3_mulm(jAngT, K);
+        acc.lhsLin = m3_add(acc.lhsLin, m3_mulm(m3_mulm(jLinT, K), jLin));
+        acc.lhsAng = m3_add(acc.lhsAng, m3_mulm(jAngTk, jAng));
+        acc.lhsCross = m3_add(acc.lhsCross, m3_mulm(jAngTk, jLin));
+        acc.rhsLin += m3_mul(jLinT, F);
+        acc.rhsAng += m3_mul(jAngT, F);
+    }
+}
+
+void Solver::stamp_entry(uint32_t entry, uint32_t body, Accum& acc) const {
+    uint32_t kind = entry >> ADJ_KIND_SHIFT, idx = entry & ADJ_INDEX_MASK;
+    if (kind == FK_JOINT) stamp_joint(joints[idx], body, acc);
+    else if (kind == FK_SPRING) stamp_spring(springs[idx], body, acc);
+    else if (kind == FK_TET) stamp_tet(tets[idx], body, acc);
+    else if (kind == FK_MANIFOLD) stamp_manifold(manifolds[idx], body, acc);
+}
+
+void Solver::primal_body(uint32_t body) {
+    bool rigid = shape[body].w >= 0.0f;
+    Accum lane[8];
+    for (int l = 0; l < 8; l++) lane[l] = accum_zero();
+    uint32_t as = adjStart[body], cnt = adjCount[body];
+    for (uint32_t k = 0; k < cnt; k++) stamp_entry(adjList[as + k], body, lane[k & 7u]);
+    // xor-butterfly over the 8 lanes: offsets 4, 2, 1 (40_solver.metal:1616-1630)
+    for (int d = 4; d >= 1; d >>= 1) {
+        Accum nx[8];
+        for (int l = 0; l < 8; l++) {
+            nx[l] = lane[l];
+            nx[l].lhsLin = m3_add(lane[l].lhsLin, lane[l ^ d].lhsLin);
+            nx[l].rhsLin = lane[l].rhsLin + lane[l ^ d].rhsLin;
+            if (rigid) {
+                nx[l].lhsAng = m3_add(lane[l].lhsAng, lane[l ^ d].lhsAng);
+                nx[l].lhsCross = m3_add(lane[l].lhsCross, lane[l ^ d].lhsCross);
+                nx[l].rhsAng = lane[l].rhsAng + lane[l ^ d].rhsAng;
+            }
+        }
+        for (int l = 0; l < 8; l++) lane[l] = nx[l];
+    }
+    Accum acc = lane[0];
+    F4 pl = posLin[body];
+    float mass = pl.w;
+    float dt2 = P.dt * P.dt;
+    acc.lhsLin = m3_add(acc.lhsLin, m3_diag(f3s(mass / dt2)));
+    acc.rhsLin += (xyz(pl) - xyz(inertLin[body])) * (mass / dt2);
+    F3 dxLin = f3s(0), dxAng = f3s(0);
+    if (rigid) {
+        M3 inertia = m3_scale(world_inertia(posAng[body], xyz(props[body])), 1.0f / dt2);
+        acc.lhsAng = m3_add(acc.lhsAng, inertia);
+        acc.rhsAng += m3_mul(inertia, q_sub(posAng[body], inertAng[body]));
+        solve6x6(acc.lhsLin, acc.lhsAng, acc.lhsCross, -acc.rhsLin, -acc.rhsAng, dxLin, dxAng);
+        if (!finite3(dxLin) || !finite3(dxAng)) return;
+        float ang2 = dot(dxAng, dxAng);
+        const float maxAng = 0.5f;
+        if (ang2 > maxAng * maxAng) dxAng *= maxAng * rsqrt_(ang2);
+    } else {
+        solve6x6(acc.lhsLin, m3_identity(), m3_zero(), -acc.rhsLin, f3s(0), dxLin, dxAng);
+        if (!finite3(dxLin)) return;
+    }
+    float maxLin = 0.35f * std::fabs(shape[body].w);
+    float lin2 = dot(dxLin, dxLin);
+    if (lin2 > maxLin * maxLin) dxLin *= maxLin * rsqrt_(lin2);
+    if (!rigid && P.numTris > 0u && P.surfaceTruncationMode == 1u) {
+        // isotropic OGC bound (40_solver.metal:1361-1382)
+        float d2 = bitsf(boundsBits[body]);
+        if (d2 < 1e37f) {
+            float bv = fmax_(0.45f * std::sqrt(d2), 0.2f * -shape[body].w);
+            F3 x0 = xyz(ogcPrev[body]);
+            F3 tot = (xyz(pl) + dxLin) - x0;
+            float t2 = dot(tot, tot);
+            if (t2 > bv * bv) {
+                tot *= bv * rsqrt_(t2);
+                dxLin = (x0 + tot) - xyz(pl);
+                ogcExceeded++;
+            }
+        }
+    }
+    posLin[body] = f4(xyz(pl) + dxLin, mass);
+    if (rigid) posAng[body] = q_addw(posAng[body], dxAng);
+}
+
+void Solver::primal_color(uint32_t c) {
+    uint32_t s0 = colorStart[c], e0 = colorStart[c + 1];
+    int n = (int)(e0 - s0);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(threads) if (threads > 1 && n > 256)
+#endif
+    for (int i = 0; i < n; i++) primal_body(colorList[s0 + (uint32_t)i]);
+}
+
+// ==========================================================================
+// Dual (40_solver.metal:1729-1906)
+// ==========================================================================
+void Solver::dual_joint(uint32_t gid) {
+    JointGPU& j = joints[gid];
+    if (j.header.z != 0) return;
+    uint32_t a = j.header.x, b = j.header.y;
+    float torqueArm = j.C0Lin.w, stiffLin = j.rA.w, stiffAng = j.rB.w;
+    F3 penLin = xyz(j.penaltyLin);
+    if (dot(penLin, penLin) > 0.0f) {
+        F3 pA = a == WORLD_BODY ? xyz(j.rA) : xform(xyz(posLin[a]), posAng[a], xyz(j.rA));
+        F3 pB = xform(xyz(posLin[b]), posAng[b], xyz(j.rB));
+        F3 C = pA - pB;
+        if (j.header.w & 1) {
+            C -= xyz(j.C0Lin) * P.alpha;
+            F3 l = clamp3(penLin * C + xyz(j.lambdaLin), f3s(-P.lambdaMax), f3s(P.lambdaMax));
+            j.lambdaLin = f4(l, j.lambdaLin.w);
+        }
+        float cap = fmin_(stiffLin, PENALTY_MAX);
+        F3 p = fmin3(penLin + abs3(C) * P.betaLin, f3s(cap));
+        j.penaltyLin = f4(p, j.penaltyLin.w);
+    }
+    F3 penAng = xyz(j.penaltyAng);
+    if (dot(penAng, penAng) > 0.0f) {
+        F4 qA = a == WORLD_BODY ? f4(0, 0, 0, 1) : posAng[a];
+        F3 C;
+        if (j.hingeAxis.w != 0.0f) {
+            F3 axis = xyz(j.hingeAxis);
+            F3 aB = q_rotate(posAng[b], axis);
+            F3 aA = q_rotate(q_mul(qA, j.restRel), axis);
+            C = cross(aA, aB) * torqueArm;
+        } else {
+            C = q_sub(q_mul(qA, j.restRel), posAng[b]) * torqueArm;
+        }
+        if (j.header.w & 2) {
+            C -= xyz(j.C0Ang) * P.alpha;
+            F3 l = clamp3(penAng * C + xyz(j.lambdaAng), f3s(-P.lambdaMax), f3s(P.lambdaMax));
+            j.lambdaAng = f4(l, j.lambdaAng.w);
+        }
+        float cap = fmin_(stiffAng, PENALTY_MAX);
+        F3 p = fmin3(penAng + abs3(C) * P.betaAng, f3s(cap));
+        j.penaltyAng = f4(p, j.penaltyAng.w);
+    }
+    float fracture = j.C0Ang.w;
+    F3 la = xyz(j.lambdaAng);
+    float lin2 = (j.header.w & 8) ? dot(xyz(j.lambdaLin), xyz(j.lambdaLin)) : 0.0f;
+    if ((j.header.w & 4) && dot(la, la) + lin2 > fracture * fracture) {
+        j.penaltyLin = F4{}; j.penaltyAng = F4{}; j.lambdaLin = F4{}; j.lambdaAng = F4{};
+        j.header.z = 1;
+    }
+}
+
+void Solver::dual_spring(uint32_t si) {
+    SpringGPU& sp = springs[si];
+    if (sp.header.z == 0) return;
+    uint32_t a = sp.header.x, b = sp.header.y;
+    F3 pA = xform(xyz(posLin[a]), posAng[a], xyz(sp.rA));
+    F3 pB = xform(xyz(posLin[b]), posAng[b], xyz(sp.rB));
+    float C = length(pA - pB) - sp.rB.w - sp.dual.z * P.alpha;
+    float mA = posLin[a].w, mB = posLin[b].w;
+    float mMin = fmin_(mA > 0.0f ? mA : FLT_MAX, mB > 0.0f ? mB : FLT_MAX);
+    float cap = fmin_(P.lambdaMax, fmax_(2.0f, 5.0e3f * mMin));
+    sp.dual.x = clampf_(0.98f * sp.dual.x + sp.dual.y * C, 0.0f, cap);
+    if (C > 0.0f) sp.dual.y = fmin_(sp.dual.y + C * P.betaLin, fmin_(sp.rA.w, PENALTY_MAX));
+}
+
+void Solver::dual_manifold(uint32_t gid) {
+    ManifoldGPU& m = manifolds[gid];
+    uint32_t n = m.header.z;
+    if (n == 0) return;
+    uint32_t a = m.header.x, b = m.header.y;
+    bool sphA = (m.header.w & 2u) != 0, sphB = (m.header.w & 4u) != 0;
+    F3 dqALin = xyz(posLin[a]) - xyz(initLin[a]);
+    F3 dqAAng = q_sub(posAng[a], initAng[a]);
+    F3 dqBLin = xyz(posLin[b]) - xyz(initLin[b]);
+    F3 dqBAng = q_sub(posAng[b], initAng[b]);
+    float mA = posLin[a].w, mB = posLin[b].w;
+    float minMass = fmin_(mA > 0.0f ? mA : FLT_MAX, mB > 0.0f ? mB : FLT_MAX);
+    float lamCap = fmin_(P.lambdaMax, fmax_(10.0f, 1.0e5f * minMass));
+    F3 nrm = xyz(m.basisN), t1 = xyz(m.basisT1), t2 = cross(nrm, t1);
+    float dynF = m.basisN.w, statF = m.basisT1.w;
+    for (uint32_t i = 0; i < n; i++) {
+        ContactGPU& c = m.contacts[i];
+        F3 rAW = sphA ? xyz(c.rA) : q_rotate(posAng[a], xyz(c.rA));
+        F3 rBW = sphB ? xyz(c.rB) : q_rotate(posAng[b], xyz(c.rB));
+        F3 C = xyz(c.C0) * (1.0f - P.alpha);
+        C += f3(dot(nrm, dqALin), dot(t1, dqALin), dot(t2, dqALin));
+        C -= f3(dot(nrm, dqBLin), dot(t1, dqBLin), dot(t2, dqBLin));
+        C += f3(dot(cross(rAW, nrm), dqAAng), dot(cross(rAW, t1), dqAAng), dot(cross(rAW, t2), dqAAng));
+        C -= f3(dot(cross(rBW, nrm), dqBAng), dot(cross(rBW, t1), dqBAng), dot(cross(rBW, t2), dqBAng));
+        F3 F = xyz(c.penalty) * C + xyz(c.lambda);
+        F.x = fmin_(F.x, 0.0f);
+        float bounds = std::fabs(F.x) * statF;
+        float fs = std::sqrt(F.y * F.y + F.z * F.z);
+        if (fs > bounds && fs > 0.0f) {
+            float db = std::fabs(F.x) * dynF;
+            float sc = db / fs;
+            F.y *= sc; F.z *= sc;
+        }
+        F.x = fmax_(F.x, -lamCap);
+        c.lambda = f4(F, 0);
+        F3 pen = xyz(c.penalty);
+        if (F.x < 0.0f) pen.x = fmin_(pen.x + P.betaLin * std::fabs(C.x), PENALTY_MAX);
+        if (fs <= bounds) {
+            pen.y = fmin_(pen.y + P.betaLin * std::fabs(C.y), PENALTY_MAX_T);
+            pen.z = fmin_(pen.z + P.betaLin * std::fabs(C.z), PENALTY_MAX_T);
+            c.rB.w = std::sqrt(C.y * C.y + C.z * C.z) < STICK_THRESH ? 1.0f : 0.0f;
+        }
+        c.penalty = f4(pen, 0);
+    }
+}
+
+void Solver::dual_all() {
+    for (uint32_t g = 0; g < joints.size(); g++) dual_joint(g);
+    for (uint32_t s = 0; s < springs.size(); s++) dual_spring(s);
+    for (uint32_t m = 0; m < numPairs; m++) if (manifolds[m].header.z != 0) dual_manifold(m);
+}
+
+// ==========================================================================
+// Finalize (40_solver.metal:2108-2147)
+// ==========================================================================
+void Solver::finalize() {
+    for (uint32_t gid = 0; gid < nb; gid++) {
+        prevVelLin[gid] = velLin[gid];
+        if (posLin[gid].w <= 0.0f) continue;
+        F3 oldV = xyz(velLin[gid]);
+        F3 v = (xyz(posLin[gid]) - xyz(initLin[gid])) / P.dt;
+        float s2 = dot(v, v);
+        if (s2 > P.maxSpeed * P.maxSpeed) v *= P.maxSpeed * rsqrt_(s2);
+        if (shape[gid].w < 0.0f && P.particleDamping > 0.0f) {
+            F3 ballistic = oldV + f3(0, 0, P.gravity * gravityScale[gid]) * P.dt;
+            v = ballistic + (v - ballistic) / (1.0f + P.particleDamping * P.dt);
+        }
+        if (shape[gid].w >= 0.0f && P.rigidLinearDamping > 0.0f) v *= std::exp(-P.rigidLinearDamping * P.dt);
+        F3 omega = q_sub(posAng[gid], initAng[gid]) / P.dt;
+        if (shape[gid].w >= 0.0f && P.rigidAngularDamping > 0.0f) omega *= std::exp(-P.rigidAngularDamping * P.dt);
+        velLin[gid] = f4(v, 0);
+        velAng[gid] = f4(omega, 0);
+    }
+}
+
+void Solver::advance_spinners() {
+    const float TWO_PI = 6.28318530717958647692f;
+    for (auto& rm : rateMotors) {
+        float target = joints[rm.joint].motor.x + rm.rate * settings.dt;
+        target -= TWO_PI * std::round(target / TWO_PI);
+        joints[rm.joint].motor.x = target;
+    }
+    for (auto& sp : spinners) {
+        F4 q = posAng[sp.body];
+        float half = 0.5f * sp.omega * settings.dt;
+        float sn = std::sin(half);
+        F4 dq = f4(sp.axis[0] * sn, sp.axis[1] * sn, sp.axis[2] * sn, std::cos(half));
+        F4 nq = q_mul(dq, q);
+        posAng[sp.body] = nq / std::sqrt(dot4(nq, nq));
+    }
+}
+
+float Solver::max_constraint_error() const {
+    float err = 0.0f;
+    for (const JointGPU& j : joints) {
+        if (!(j.header.z == 0 && (j.rA.w > 0.0f || j.rB.w > 0.0f))) continue;
+        uint32_t a = j.header.x, b = j.header.y;
+        F3 pA = a == WORLD_BODY ? xyz(j.rA) : xform(xyz(posLin[a]), posAng[a], xyz(j.rA));
+        F3 pB = xform(xyz(posLin[b]), posAng[b], xyz(j.rB));
+        err = fmax_(err, length(pA - pB));
+    }
+    for (uint32_t g = 0; g < numPairs; g++) {
+        const ManifoldGPU& m = manifolds[g];
+        uint32_t a = m.header.x, b = m.header.y;
+        bool sphA = (m.header.w & 2u) != 0, sphB = (m.header.w & 4u) != 0;
+        for (uint32_t i = 0; i < m.header.z; i++) {
+            F3 xA = sphA ? xyz(posLin[a]) + xyz(m.contacts[i].rA) : xform(xyz(posLin[a]), posAng[a], xyz(m.contacts[i].rA));
+            F3 xB = sphB ? xyz(posLin[b]) + xyz(m.contacts[i].rB) : xform(xyz(posLin[b]), posAng[b], xyz(m.contacts[i].rB));
+            float pen = dot(xyz(m.basisN), xA - xB) + P.collisionMargin;
+            err = fmax_(err, fmax_(0.0f, -pen));
+        }
+    }
+    return err;
+}
+
+// ==========================================================================
+// One frame (GPUSolver.swift:3138-4375)
+// ==========================================================================
+void Solver::step() {
+    sync_params();
+    std::fill(boundsBits.begin(), boundsBits.end(), 0x7F7F7F7Fu);
+    ogcExceeded = 0;
+    colorConflicts = 0;
+    broadphase();
+    narrowphase();
+    map_rebuild();
+    warmstart_joints();
+    warmstart_bodies();
+    adjacency();
+    if (dynamicColoring) dynamic_coloring();
+    uint32_t colorBound = dynamicColoring ? (uint32_t)MAX_COLORS : staticUsedColors;
+    for (uint32_t it = 0; it < P.iterations; it++) {
+        for (uint32_t c = 0; c < colorBound; c++) primal_color(c);
+        dual_all();
+    }
+    finalize();
+    advance_spinners();
+    frameIndex++;
+    // the manifolds written this frame become next frame's warm-start source
+    std::swap(manifolds, prevManifolds);
+    if (pairCandidates > maxPairs && failure == AVBD_FAIL_NONE) {
+        failure = AVBD_FAIL_RIGID_PAIR_CAPACITY;
+        error = "rigid pair capacity exceeded";
+    }
+    if (colorConflicts > 0 && failure == AVBD_FAIL_NONE) {
+        failure = AVBD_FAIL_UNRESOLVED_COLORING;
+        error = "unresolved dynamic coloring";
+    }
+}
+
+}  // namespace oracle
+
+// ==========================================================================
+// C entry points used by the tests (ctypes) and bench.py's cpu_baseline.
+// ==========================================================================
+using oracle::Solver;
+extern "C" {
+
+int oracle_create(const avbd_scene_desc* scene, void** out) {
+    if (!out) return AVBD_ERR_INVALID_ARGUMENT;
+    Solver* s = new Solver();
+    int rc = s->create(scene);
+    if (rc != AVBD_OK) {
+        std::fprintf(stderr, "oracle_create: %s\n", s->error.c_str());
+        delete s;
+        *out = nullptr;
+        return rc;
+    }
+    *out = s;
+    return AVBD_OK;
+}
+void oracle_destroy(void* h) { delete static_cast<Solver*>(h); }
+int oracle_set_threads(void* h, int n) { static_cast<Solver*>(h)->threads = n < 1 ? 1 : n; return AVBD_OK; }
+int oracle_set_settings(void* h, const avbd_settings* st) { static_cast<Solver*>(h)->settings = *st; return AVBD_OK; }
+int oracle_step(void* h, uint32_t frames) {
+    Solver* s = static_cast<Solver*>(h);
+    for (uint32_t f = 0; f < frames; f++) {
+        if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
+        s->step();
+    }
+    return s->failure != AVBD_FAIL_NONE ? AVBD_ERR_RUNTIME_FAILURE : AVBD_OK;
+}
+int oracle_runtime_failure(void* h, int* kind) { *kind = static_cast<Solver*>(h)->failure; return AVBD_OK; }
+int oracle_get_positions(void* h, uint32_t n, float* pos, float* rot) {
+    Solver* s = static_cast<Solver*>(h);
+    if (n > s->nb) return AVBD_ERR_INVALID_ARGUMENT;
+    if (pos) std::memcpy(pos, s->posLin.data(), n * 16);
+    if (rot) std::memcpy(rot, s->posAng.data(), n * 16);
+    return AVBD_OK;
+}
+int oracle_get_body_states(void* h, uint32_t n, avbd_body_state* out) {
+    Solver* s = static_cast<Solver*>(h);
+    if (n > s->nb) return AVBD_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < n; i++) {
+        avbd_body_state& o = out[i];
+        o.position[0] = s->posLin[i].x; o.position[1] = s->posLin[i].y; o.position[2] = s->posLin[i].z;
+        o.rotation[0] = s->posAng[i].x; o.rotation[1] = s->posAng[i].y; o.rotation[2] = s->posAng[i].z; o.rotation[3] = s->posAng[i].w;
+        o.velocity[0] = s->velLin[i].x; o.velocity[1] = s->velLin[i].y; o.velocity[2] = s->velLin[i].z;
+        o.angular_velocity[0] = s->velAng[i].x; o.angular_velocity[1] = s->velAng[i].y; o.angular_velocity[2] = s->velAng[i].z;
+    }
+    return AVBD_OK;
+}
+int oracle_set_motor_targets(void* h, const uint32_t* ids, uint32_t n, const float* targets) {
+    Solver* s = static_cast<Solver*>(h);
+    for (uint32_t i = 0; i < n; i++) {
+        if (ids[i] >= s->joints.size()) return AVBD_ERR_INVALID_ARGUMENT;
+        oracle::JointGPU& j = s->joints[ids[i]];
+        if ((j.header.w & oracle::MOTOR_MODE_MASK) == 0) continue;
+        j.motor.x = targets[i];
+    }
+    return AVBD_OK;
+}
+int oracle_max_constraint_error(void* h, float* out) { *out = static_cast<Solver*>(h)->max_constraint_error(); return AVBD_OK; }
+int oracle_get_counters(void* h, avbd_counters* out) {
+    Solver* s = static_cast<Solver*>(h);
+    std::memset(out, 0, sizeof(*out));
+    out->frame = s->frameIndex;
+    out->num_pairs = s->numPairs;
+    out->pair_candidates = s->pairCandidates;
+    out->color_conflicts = s->colorConflicts;
+    out->ogc_exceeded = s->ogcExceeded;
+    out->used_colors = s->dynamicColoring ? s->colorStart[64 + 1] : s->staticUsedColors;
+    for (int c = 0; c < 64; c++) out->color_counts[c] = s->colorCounts[c];
+    return AVBD_OK;
+}
+static const void* oracle_buffer(Solver* s, int which, size_t& bytes) {
+    switch (which) {
+    case AVBD_BUF_POS_LIN: bytes = s->posLin.size() * 16; return s->posLin.data();
+    case AVBD_BUF_POS_ANG: bytes = s->posAng.size() * 16; return s->posAng.data();
+    case AVBD_BUF_VEL_LIN: bytes = s->velLin.size() * 16; return s->velLin.data();
+    case AVBD_BUF_VEL_ANG: bytes = s->velAng.size() * 16; return s->velAng.data();
+    case AVBD_BUF_PAIRS: bytes = (size_t)s->numPairs * 8; return s->pairs.data();
+    // manifolds were swapped at the end of the frame: the last frame's are in prevManifolds
+    case AVBD_BUF_MANIFOLDS: bytes = (size_t)s->numPairs * sizeof(oracle::ManifoldGPU); return s->prevManifolds.data();
+    case AVBD_BUF_ADJ_START: bytes = s->adjStart.size() * 4; return s->adjStart.data();
+    case AVBD_BUF_ADJ_COUNT: bytes = s->adjCount.size() * 4; return s->adjCount.data();
+    case AVBD_BUF_ADJ_LIST: bytes = s->adjList.size() * 4; return s->adjList.data();
+    case AVBD_BUF_COLORS: bytes = s->colorsA.size() * 4; return s->colorsA.data();
+    case AVBD_BUF_COLOR_START: bytes = s->colorStart.size() * 4; return s->colorStart.data();
+    case AVBD_BUF_COLOR_LIST: bytes = s->colorList.size() * 4; return s->colorList.data();
+    case AVBD_BUF_CELL_START: bytes = s->cellStart.size() * 4; return s->cellStart.data();
+    case AVBD_BUF_CELL_COUNT: bytes = s->cellCount.size() * 4; return s->cellCount.data();
+    case AVBD_BUF_CELL_BODIES: bytes = (size_t)s->P.numHashed * 4; return s->cellBodies.data();
+    case AVBD_BUF_MAP_KEY_A: bytes = s->mapKeyA.size() * 4; return s->mapKeyA.data();
+    case AVBD_BUF_MAP_KEY_B: bytes = s->mapKeyB.size() * 4; return s->mapKeyB.data();
+    case AVBD_BUF_MAP_VAL: bytes = s->mapVal.size() * 4; return s->mapVal.data();
+    case AVBD_BUF_JOINTS: bytes = s->joints.size() * sizeof(oracle::JointGPU); return s->joints.data();
+    case AVBD_BUF_SPRINGS: bytes = s->springs.size() * sizeof(oracle::SpringGPU); return s->springs.data();
+    case AVBD_BUF_TETS: bytes = s->tets.size() * sizeof(oracle::TetGPU); return s->tets.data();
+    case AVBD_BUF_INIT_LIN: bytes = s->initLin.size() * 16; return s->initLin.data();
+    case AVBD_BUF_INERT_LIN: bytes = s->inertLin.size() * 16; return s->inertLin.data();
+    case AVBD_BUF_EXCLUSIONS: bytes = s->exclusions.size() * 4; return s->exclusions.data();
+    case AVBD_BUF_HASHED_IDX: bytes = s->hashedIdx.size() * 4; return s->hashedIdx.data();
+    case AVBD_BUF_GLOBAL_IDX: bytes = s->globalIdx.size() * 4; return s->globalIdx.data();
+    default: bytes = 0; return nullptr;
+    }
+}
+size_t oracle_debug_buffer_size(void* h, int which) {
+    size_t bytes = 0;
+    oracle_buffer(static_cast<Solver*>(h), which, bytes);
+    return bytes;
+}
+int oracle_debug_read(void* h, int which, void* dst, size_t bytes) {
+    size_t have = 0;
+    const void* src = oracle_buffer(static_cast<Solver*>(h), which, have);
+    if (!src || bytes > have) return AVBD_ERR_INVALID_ARGUMENT;
+    std::memcpy(dst, src, bytes);
+    return AVBD_OK;
+}
+
+}  // extern "C"

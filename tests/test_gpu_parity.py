@@ -1,0 +1,194 @@
+"""Parity of the CUDA solver step with the CPU oracle, through the C ABI.
+
+Integer and index work (hash buckets, candidate pairs, adjacency lists, the
+static palette, the persistence map as a key->value set, upload records) must
+be bit-exact.  Positions, rotations and velocities must stay within 1e-4
+relative per step over the compared frames; the kernels and the oracle
+evaluate the same float32 expressions in the same order without FMA
+contraction, so in practice they agree bit for bit and the tests record that.
+"""
+import numpy as np
+import pytest
+
+from avbd_b200 import abi, demos
+from avbd_b200.scene import PhysicsScene, SceneJoint
+from avbd_b200.solver import GPUSolver, RuntimeFailure
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-4   # relative per-step tolerance on positions and velocities
+
+
+def pair(scene, oracle_lib, threads=8, **kw):
+    return GPUSolver(scene, **kw), oracle_lib.OracleSolver(scene, threads=threads, **kw)
+
+
+def assert_close(name, got, want, rel=REL_TOL):
+    got = np.asarray(got, np.float64)
+    want = np.asarray(want, np.float64)
+    scale = np.maximum(np.abs(want), 1.0)
+    err = np.max(np.abs(got - want) / scale) if got.size else 0.0
+    assert err <= rel, f"{name}: max relative error {err:.3e} > {rel:.1e}"
+    return err
+
+
+def compare_state(g, o, frame):
+    gp, gr = g.positions()
+    op, orr = o.positions()
+    assert_close(f"frame {frame} posLin", gp, op)
+    assert_close(f"frame {frame} posAng", gr, orr)
+    gv = np.array([list(s.velocity) for s in g.body_states()])
+    ov = np.array([list(s.velocity) for s in o.body_states()])
+    assert_close(f"frame {frame} velocity", gv, ov)
+    return bool(np.array_equal(gp.view(np.uint32), op.view(np.uint32))
+                and np.array_equal(gr.view(np.uint32), orr.view(np.uint32)))
+
+
+def run_parity(scene, oracle_lib, frames, **kw):
+    g, o = pair(scene, oracle_lib, **kw)
+    exact = 0
+    for f in range(frames):
+        g.step(1)
+        assert o.step(1) == 0
+        exact += compare_state(g, o, f + 1)
+    return g, o, exact
+
+
+def test_upload_records_bitwise(cuda_lib, oracle_lib):
+    s = demos.soft_cube_scene(seed=11, n=6)
+    g, o = pair(s, oracle_lib)
+    for name in ["TETS", "EXCLUSIONS", "HASHED_IDX", "GLOBAL_IDX", "COLOR_START", "COLOR_LIST"]:
+        a, b = g.debug_read(name), o.debug_read(name)
+        assert a.size == b.size and np.array_equal(a, b), name
+    gp, _ = g.positions()
+    op, _ = o.positions()
+    assert np.array_equal(gp.view(np.uint32), op.view(np.uint32))  # masses bit-exact
+
+
+@pytest.mark.parametrize("name,make,frames", [
+    ("single-tet", demos.single_tet_scene, 120),
+    ("rod-chain", demos.particle_rod_chain_scene, 120),
+    ("stack5", lambda: demos.stack(5), 120),
+    ("rigid-stack-20", lambda: demos.rigid_stack_scene(seed=1), 90),
+    ("soft-cube-6", lambda: demos.soft_cube_scene(seed=5, n=6), 90),
+])
+def test_trajectory_parity(cuda_lib, oracle_lib, name, make, frames):
+    g, o, exact = run_parity(make(), oracle_lib, frames)
+    print(f"{name}: {exact}/{frames} frames bit-identical")
+
+
+def test_soft_cube_full_size_parity(cuda_lib, oracle_lib):
+    # the benchmark scene itself: 24^3 lattice, 60,835 tets, 20 iterations
+    g, o, exact = run_parity(demos.soft_cube_scene(seed=2, n=24), oracle_lib, 24)
+    print(f"soft-cube-24: {exact}/24 frames bit-identical")
+
+
+def test_broadphase_and_adjacency_bitwise(cuda_lib, oracle_lib):
+    for scene, frames in [(demos.rigid_stack_scene(seed=3), 30),
+                          (demos.soft_cube_scene(seed=4, n=8), 30)]:
+        g, o = pair(scene, oracle_lib)
+        g.step(frames)
+        o.step(frames)
+        g.synchronize()
+        for name in ["CELL_COUNT", "CELL_START", "CELL_BODIES", "PAIRS", "ADJ_START", "ADJ_COUNT",
+                     "ADJ_LIST", "COLORS"]:
+            a, b = g.debug_read(name, np.uint32), o.debug_read(name, np.uint32)
+            assert a.size == b.size and np.array_equal(a, b), name
+        # manifolds: every active record bitwise, headers of the rest
+        gm = g.debug_read("MANIFOLDS", np.uint32).reshape(-1, 176)
+        om = o.debug_read("MANIFOLDS", np.uint32).reshape(-1, 176)
+        assert gm.shape == om.shape
+        assert np.array_equal(gm[:, :8], om[:, :8])
+        for r in range(gm.shape[0]):
+            n = gm[r, 2]
+            if n:
+                assert np.array_equal(gm[r, :16 + 20 * n], om[r, :16 + 20 * n]), f"manifold {r}"
+        # persistence map: same key -> value set (slot placement may differ)
+        def mapset(s):
+            ka, kb, v = (s.debug_read(k, np.uint32) for k in ("MAP_KEY_A", "MAP_KEY_B", "MAP_VAL"))
+            return {(int(a), int(b)): int(c) for a, b, c in zip(ka, kb, v) if a}
+        assert mapset(g) == mapset(o)
+        # dynamic palette: same per-color body sets
+        cs_g = g.debug_read("COLOR_START", np.uint32)
+        cs_o = o.debug_read("COLOR_START", np.uint32)
+        assert np.array_equal(cs_g, cs_o)
+        lg, lo = g.debug_read("COLOR_LIST", np.uint32), o.debug_read("COLOR_LIST", np.uint32)
+        for c in range(64):
+            a, b = cs_g[c], cs_g[c + 1]
+            assert sorted(lg[a:b]) == sorted(lo[a:b])
+
+
+def test_joint_motor_parity(cuda_lib, oracle_lib):
+    # hinge chain with implicit PD motors and targets changed every frame
+    s = PhysicsScene("hinge-chain")
+    demos.add_ground(s, friction=0.5)
+    prev = -1
+    for k in range(4):
+        b = s.add_body((0.3, 0.08, 0.08), 500.0, 0.5, (0.3 * k + 0.15, 0, 1.0))
+        s.add_joint(SceneJoint(prev, b, (0.3 * k, 0, 1.0) if prev < 0 else (0.15, 0, 0), (-0.15, 0, 0),
+                               stiffness_ang=float("inf"), hinge_axis=(0, 1, 0),
+                               motor_torque=50.0, motor_stiffness=200.0, motor_damping=2.0))
+        prev = b
+    g, o = pair(s, oracle_lib)
+    rng = demos.SplitMix64(9)
+    for f in range(60):
+        t = np.array([rng.uniform(-0.5, 0.5) for _ in range(4)], np.float32)
+        g.set_motor_targets(range(4), t)
+        o.set_motor_targets(range(4), t)
+        g.step(1)
+        o.step(1)
+        gp, gr = g.positions()
+        op, orr = o.positions()
+        # atan2f of the twist may differ in the last ulp between libm and CUDA
+        assert_close(f"frame {f} pos", gp, op, rel=1e-4)
+        assert_close(f"frame {f} rot", gr, orr, rel=1e-4)
+
+
+def test_pair_capacity_failure_is_sticky(cuda_lib):
+    s = PhysicsScene("crowd")
+    for i in range(120):
+        s.add_body((0.4, 0.4, 0.4), 1.0, 0.5, ((i % 10) * 0.05, (i // 10) * 0.05, 1.0), shape=abi.SHAPE_SPHERE)
+    g = GPUSolver(s, max_pairs_per_body=1)     # capacity floor 4096 < 7140 candidates
+    g.step(1)
+    with pytest.raises(RuntimeFailure) as e:
+        g.synchronize()
+    assert e.value.kind == abi.FAIL_RIGID_PAIR_CAPACITY
+    with pytest.raises(RuntimeFailure):       # latched: every later call rethrows
+        g.step(1)
+    assert g.runtime_failure() == abi.FAIL_RIGID_PAIR_CAPACITY
+
+
+def test_snapshot_restore_is_bitwise(cuda_lib):
+    g = GPUSolver(demos.soft_cube_scene(seed=6, n=6))
+    g.step(10)
+    snap = g.snapshot()
+    g.step(10)
+    a, ra = g.positions()
+    g.restore(snap)
+    g.step(10)
+    b, rb = g.positions()
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.array_equal(ra.view(np.uint32), rb.view(np.uint32))
+
+
+def test_set_body_states_teleports_and_clears_contacts(cuda_lib):
+    g = GPUSolver(demos.stack(3))
+    g.step(30)
+    st = g.body_states([3])[0]
+    st.position[:] = (5.0, 0.0, 3.0)
+    st.velocity[:] = (0.0, 0.0, 0.0)
+    g.set_body_states([3], [st])
+    assert abs(g.body_states([3])[0].position[0] - 5.0) < 1e-6
+    g.step(1)
+    p = g.body_states([3])[0].position
+    assert abs(p[0] - 5.0) < 1e-3 and p[2] < 3.0       # falls freely from the new pose
+
+
+def test_bitwise_determinism_across_instances(cuda_lib):
+    s = demos.rigid_stack_scene(seed=8, count=12)
+    a, b = GPUSolver(s), GPUSolver(s)
+    a.step(120)
+    b.step(120)
+    pa, _ = a.positions()
+    pb, _ = b.positions()
+    assert np.array_equal(pa.view(np.uint32), pb.view(np.uint32))
