@@ -163,5 +163,15 @@ EXPORTED = [
     "avbd_get_positions", "avbd_set_positions", "avbd_set_motor_targets",
     "avbd_max_constraint_error", "avbd_get_counters", "avbd_runtime_failure",
     "avbd_last_error", "avbd_snapshot_capture", "avbd_snapshot_restore",
-    "avbd_snapshot_free", "avbd_debug_buffer_size", "avbd_debug_read",
+    "avbd_snapshot_free", "avbd_debug_buffer_size", "avbd_debug_read", "avbd_set_stream",
+    "avbd_set_profiling", "avbd_get_profile",
 ]
+
+STAGES = ["broadphase", "narrowphase", "persistence_map", "warmstart", "adjacency",
+          "coloring", "primal", "dual", "finalize"]
+
+
+class Profile(C.Structure):
+    _fields_ = [("frames", C.c_uint64), ("kernels_per_frame", C.c_uint64),
+                ("stage_ms", C.c_double * 16),
+                ("stage_launches", C.c_uint64 * 16)]

@@ -70,6 +70,9 @@ def load_library() -> C.CDLL:
         "avbd_snapshot_free": ([vp], None),
         "avbd_debug_buffer_size": ([vp, i32], sz),
         "avbd_debug_read": ([vp, i32, vp, sz], i32),
+        "avbd_set_stream": ([vp, vp], i32),
+        "avbd_set_profiling": ([vp, i32], i32),
+        "avbd_get_profile": ([vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -208,6 +211,21 @@ class GPUSolver:
 
     def restore(self, snap):
         self._check(load_library().avbd_snapshot_restore(self._h, snap._h))
+
+    def set_stream(self, cuda_stream_handle):
+        """Launch on a caller-owned stream (an integer cudaStream_t handle, e.g.
+        torch.cuda.Stream().cuda_stream); None restores the solver's stream."""
+        self._check(load_library().avbd_set_stream(self._h, cuda_stream_handle or None))
+
+    def set_profiling(self, enabled: bool):
+        self._check(load_library().avbd_set_profiling(self._h, 1 if enabled else 0))
+
+    def profile(self) -> dict:
+        p = abi.Profile()
+        self._check(load_library().avbd_get_profile(self._h, C.byref(p)))
+        return {"frames": p.frames, "kernels_per_frame": p.kernels_per_frame,
+                "stage_ms": {n: p.stage_ms[i] for i, n in enumerate(abi.STAGES)},
+                "stage_launches": {n: p.stage_launches[i] for i, n in enumerate(abi.STAGES)}}
 
     def debug_read(self, name: str, dtype=np.uint8):
         lib = load_library()

@@ -66,7 +66,15 @@ struct avbd_solver {
     Params P{};
     avbd_settings settings{};
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;       // the solver's own stream (graph capture)
+    cudaStream_t launch = nullptr;       // where frames run: own or caller's stream
+    // per-stage profiling: events at stage boundaries inside the frame graph
+    bool profiling = false;
+    std::vector<cudaEvent_t> events;
+    std::vector<int> intervalStage;
+    int usedEvents = 0;
+    avbd_profile prof{};
+    uint64_t kernelsPerFrame = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphsValid = false;
     uint64_t frame = 0;
@@ -83,8 +91,10 @@ struct avbd_solver {
     Counters* hostCounters = nullptr;  // pinned copy of the last frame's counters
 
     ~avbd_solver() {
+        if (launch) cudaStreamSynchronize(launch);
         if (stream) cudaStreamSynchronize(stream);
         for (auto& g : graph) if (g) cudaGraphExecDestroy(g);
+        for (auto& e : events) cudaEventDestroy(e);
         for (void* p : allocations) cudaFree(p);
         if (stage) cudaFree(stage);
         if (hostLatch) cudaFreeHost(hostLatch);
@@ -144,32 +154,70 @@ struct avbd_solver {
 
     // One frame, in the reference's stage order.  `parity` selects which
     // manifold buffer is "current" (the buffers swap after every frame).
+    // With profiling on, an event is recorded at every stage boundary.
     void encode_frame(int parity) {
         DevPtrs f = d;
         if (parity) std::swap(f.manifolds, f.prevManifolds);
         cudaStream_t st = stream;
+        usedEvents = 0;
+        auto mark = [&](int stage) {
+            if (!profiling) return;
+            cudaEventRecordWithFlags(events[usedEvents], st, cudaEventRecordExternal);
+            intervalStage[usedEvents] = stage;
+            usedEvents++;
+        };
+        mark(AVBD_STAGE_BROADPHASE);
         cudaMemsetAsync(f.counters, 0, sizeof(Counters), st);
         launch_broadphase(P, f, z, st);
+        mark(AVBD_STAGE_NARROWPHASE);
         launch_narrowphase(P, f, z, st);
+        mark(AVBD_STAGE_PERSISTENCE_MAP);
         launch_map_rebuild(P, f, z, st);
+        mark(AVBD_STAGE_WARMSTART);
         launch_warmstart(P, f, z, st);
+        mark(AVBD_STAGE_ADJACENCY);
         launch_adjacency(P, f, z, st);
-        if (z.dynamicColoring) launch_dynamic_coloring(P, f, z, st);
+        if (z.dynamicColoring) {
+            mark(AVBD_STAGE_COLORING);
+            launch_dynamic_coloring(P, f, z, st);
+        }
         const uint32_t colorBound = z.dynamicColoring ? (uint32_t)MAX_COLORS : H.staticUsedColors;
         if (smallSolve) {
+            mark(AVBD_STAGE_PRIMAL);
             launch_solve_small(P, f, z, colorBound, st);
         } else {
             for (uint32_t it = 0; it < P.iterations; it++) {
-                for (uint32_t c = 0; c < colorBound; c++)
-                    launch_primal_color(P, f, z, c, z.dynamicColoring ? 0xFFFFFFFFu : H.colorCounts[c], st);
+                for (uint32_t c = 0; c < colorBound; c++) {
+                    const uint32_t count = z.dynamicColoring ? 0xFFFFFFFFu : H.colorCounts[c];
+                    if (count == 0) continue;
+                    mark(AVBD_STAGE_PRIMAL);
+                    launch_primal_color(P, f, z, c, count, st);
+                }
+                mark(AVBD_STAGE_DUAL);
                 launch_dual(P, f, z, st);
             }
         }
+        mark(AVBD_STAGE_FINALIZE);
         launch_finalize(P, f, z, st);
         launch_frame_end(P, f, z, st);
+        mark(-1);
+    }
+
+    int events_needed() const {
+        const uint32_t colorBound = z.dynamicColoring ? (uint32_t)MAX_COLORS : H.staticUsedColors;
+        return 16 + (int)(P.iterations * (colorBound + 1));
     }
 
     bool build_graphs() {
+        if (profiling) {
+            const int need = events_needed();
+            while ((int)events.size() < need) {
+                cudaEvent_t e;
+                if (!check(cudaEventCreate(&e), "event create")) return false;
+                events.push_back(e);
+            }
+            intervalStage.assign(events.size(), -1);
+        }
         for (int parity = 0; parity < 2; parity++) {
             if (graph[parity]) { cudaGraphExecDestroy(graph[parity]); graph[parity] = nullptr; }
             cudaGraph_t g = nullptr;
@@ -177,6 +225,16 @@ struct avbd_solver {
             encode_frame(parity);
             cudaError_t e = cudaStreamEndCapture(stream, &g);
             if (!check(e, "end capture")) return false;
+            size_t nodes = 0;
+            cudaGraphGetNodes(g, nullptr, &nodes);
+            std::vector<cudaGraphNode_t> list(nodes);
+            if (nodes) cudaGraphGetNodes(g, list.data(), &nodes);
+            uint64_t kernels = 0;
+            for (cudaGraphNode_t n : list) {
+                cudaGraphNodeType t;
+                if (cudaGraphNodeGetType(n, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) kernels++;
+            }
+            kernelsPerFrame = kernels;
             e = cudaGraphInstantiate(&graph[parity], g, 0);
             cudaGraphDestroy(g);
             if (!check(e, "graph instantiate")) return false;
@@ -194,6 +252,7 @@ struct avbd_solver {
         if (s->device < 0) cudaGetDevice(&device);
         if (device >= count || cudaSetDevice(device) != cudaSuccess) { error = "cannot select CUDA device"; return AVBD_ERR_NO_DEVICE; }
         if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) { error = "stream creation failed"; return AVBD_ERR_NO_DEVICE; }
+        launch = stream;
         settings = s->settings;
         P = H.P;
         sync_params();
@@ -296,7 +355,7 @@ struct avbd_solver {
     // Wait for the stream, then surface an execution error or a latched
     // capacity/coloring failure.
     int retire() {
-        if (!check(cudaStreamSynchronize(stream), "frame execution")) return AVBD_ERR_RUNTIME_FAILURE;
+        if (!check(cudaStreamSynchronize(launch), "frame execution")) return AVBD_ERR_RUNTIME_FAILURE;
         if (!check(cudaMemcpy(hostLatch, d.failureLatch, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost), "latch readback"))
             return AVBD_ERR_RUNTIME_FAILURE;
         if (hostLatch[0] != 0 && failure == AVBD_FAIL_NONE) {
@@ -317,8 +376,20 @@ struct avbd_solver {
         if (failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
         if (!graphsValid && !build_graphs()) return AVBD_ERR_RUNTIME_FAILURE;
         for (uint32_t f = 0; f < frames; f++) {
-            if (!check(cudaGraphLaunch(graph[frame & 1], stream), "graph launch")) return AVBD_ERR_RUNTIME_FAILURE;
+            if (!check(cudaGraphLaunch(graph[frame & 1], launch), "graph launch")) return AVBD_ERR_RUNTIME_FAILURE;
             frame++;
+            if (profiling) {
+                // profiled frames retire synchronously, as in the reference
+                int rc = retire();
+                if (rc != AVBD_OK) return rc;
+                for (int k = 0; k + 1 < usedEvents; k++) {
+                    float ms = 0.0f;
+                    if (!check(cudaEventElapsedTime(&ms, events[k], events[k + 1]), "event timing")) return AVBD_ERR_RUNTIME_FAILURE;
+                    const int stg = intervalStage[k];
+                    if (stg >= 0) { prof.stage_ms[stg] += ms; prof.stage_launches[stg] += 1; }
+                }
+                prof.frames++;
+            }
         }
         return AVBD_OK;
     }
@@ -435,11 +506,11 @@ int avbd_set_body_states(avbd_solver* s, const uint32_t* ids, uint32_t n, const 
     uint8_t* st = static_cast<uint8_t*>(s->staging(bytesStates + bytesIds + 16));
     if (!st) return AVBD_ERR_ALLOC_FAILED;
     uint32_t* dIds = ids ? reinterpret_cast<uint32_t*>(st + bytesStates) : nullptr;
-    if (!s->check(cudaMemcpyAsync(st, states, bytesStates, cudaMemcpyHostToDevice, s->stream), "state upload")) return AVBD_ERR_RUNTIME_FAILURE;
-    if (ids && !s->check(cudaMemcpyAsync(dIds, ids, bytesIds, cudaMemcpyHostToDevice, s->stream), "state upload")) return AVBD_ERR_RUNTIME_FAILURE;
-    cudaMemsetAsync(s->d.resetFlags, 0, 4 * (size_t)nb, s->stream);
-    k_set_states<<<(n + 127) / 128, 128, 0, s->stream>>>(s->d, dIds, reinterpret_cast<const avbd_body_state*>(st), n);
-    launch_reset_bodies(s->P, s->d, s->z, s->stream);
+    if (!s->check(cudaMemcpyAsync(st, states, bytesStates, cudaMemcpyHostToDevice, s->launch), "state upload")) return AVBD_ERR_RUNTIME_FAILURE;
+    if (ids && !s->check(cudaMemcpyAsync(dIds, ids, bytesIds, cudaMemcpyHostToDevice, s->launch), "state upload")) return AVBD_ERR_RUNTIME_FAILURE;
+    cudaMemsetAsync(s->d.resetFlags, 0, 4 * (size_t)nb, s->launch);
+    k_set_states<<<(n + 127) / 128, 128, 0, s->launch>>>(s->d, dIds, reinterpret_cast<const avbd_body_state*>(st), n);
+    launch_reset_bodies(s->P, s->d, s->z, s->launch);
     return s->retire();
 }
 
@@ -448,8 +519,8 @@ int avbd_set_positions(avbd_solver* s, uint32_t n, const float* xyz) {
     if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
     float* st = static_cast<float*>(s->staging((size_t)n * 12 + 16));
     if (!st) return AVBD_ERR_ALLOC_FAILED;
-    if (!s->check(cudaMemcpyAsync(st, xyz, (size_t)n * 12, cudaMemcpyHostToDevice, s->stream), "position upload")) return AVBD_ERR_RUNTIME_FAILURE;
-    k_set_positions<<<(n + 255) / 256, 256, 0, s->stream>>>(s->d.posLin, st, n);
+    if (!s->check(cudaMemcpyAsync(st, xyz, (size_t)n * 12, cudaMemcpyHostToDevice, s->launch), "position upload")) return AVBD_ERR_RUNTIME_FAILURE;
+    k_set_positions<<<(n + 255) / 256, 256, 0, s->launch>>>(s->d.posLin, st, n);
     return s->check(cudaGetLastError(), "position upload") ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
 }
 
@@ -464,9 +535,9 @@ int avbd_set_motor_targets(avbd_solver* s, const uint32_t* joints, uint32_t n, c
     if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
     uint8_t* st = static_cast<uint8_t*>(s->staging(8 * (size_t)n + 16));
     if (!st) return AVBD_ERR_ALLOC_FAILED;
-    cudaMemcpyAsync(st, joints, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream);
-    cudaMemcpyAsync(st + 4 * (size_t)n, targets, 4 * (size_t)n, cudaMemcpyHostToDevice, s->stream);
-    k_set_motor_targets<<<(n + 127) / 128, 128, 0, s->stream>>>(s->d.joints, reinterpret_cast<uint32_t*>(st),
+    cudaMemcpyAsync(st, joints, 4 * (size_t)n, cudaMemcpyHostToDevice, s->launch);
+    cudaMemcpyAsync(st + 4 * (size_t)n, targets, 4 * (size_t)n, cudaMemcpyHostToDevice, s->launch);
+    k_set_motor_targets<<<(n + 127) / 128, 128, 0, s->launch>>>(s->d.joints, reinterpret_cast<uint32_t*>(st),
                                                                  reinterpret_cast<float*>(st + 4 * (size_t)n), n);
     return s->check(cudaGetLastError(), "motor targets") ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
 }
@@ -477,8 +548,8 @@ int avbd_max_constraint_error(avbd_solver* s, float* out) {
     if (rc != AVBD_OK) return rc;
     DevPtrs f = s->d;
     if (s->frame & 1) std::swap(f.manifolds, f.prevManifolds);
-    launch_max_constraint_error(s->P, f, s->z, s->stream);
-    if (!s->check(cudaMemcpyAsync(out, s->d.diag, 4, cudaMemcpyDeviceToHost, s->stream), "diag readback")) return AVBD_ERR_RUNTIME_FAILURE;
+    launch_max_constraint_error(s->P, f, s->z, s->launch);
+    if (!s->check(cudaMemcpyAsync(out, s->d.diag, 4, cudaMemcpyDeviceToHost, s->launch), "diag readback")) return AVBD_ERR_RUNTIME_FAILURE;
     return s->retire();
 }
 
@@ -547,6 +618,33 @@ int avbd_snapshot_restore(avbd_solver* s, const avbd_snapshot* snap) {
 
 void avbd_snapshot_free(avbd_snapshot* snap) { delete snap; }
 
+int avbd_set_stream(avbd_solver* s, void* cuda_stream) {
+    if (!s) return AVBD_ERR_INVALID_ARGUMENT;
+    if (!s->check(cudaStreamSynchronize(s->launch), "stream switch")) return AVBD_ERR_RUNTIME_FAILURE;
+    s->launch = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : s->stream;
+    return AVBD_OK;
+}
+
+int avbd_set_profiling(avbd_solver* s, int enabled) {
+    if (!s) return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    if ((enabled != 0) != s->profiling) {
+        s->profiling = enabled != 0;
+        s->graphsValid = false;
+    }
+    std::memset(&s->prof, 0, sizeof(s->prof));
+    return AVBD_OK;
+}
+
+int avbd_get_profile(avbd_solver* s, avbd_profile* out) {
+    if (!s || !out) return AVBD_ERR_INVALID_ARGUMENT;
+    if (!s->graphsValid && !s->build_graphs()) return AVBD_ERR_RUNTIME_FAILURE;
+    *out = s->prof;
+    out->kernels_per_frame = s->kernelsPerFrame;
+    return AVBD_OK;
+}
+
 size_t avbd_debug_buffer_size(avbd_solver* s, int which) {
     if (!s) return 0;
     const HostScene& H = s->H;
@@ -556,7 +654,7 @@ size_t avbd_debug_buffer_size(avbd_solver* s, int which) {
     case AVBD_BUF_INIT_LIN: case AVBD_BUF_INERT_LIN: return nb * 16;
     case AVBD_BUF_PAIRS: case AVBD_BUF_MANIFOLDS: case AVBD_BUF_ADJ_LIST: {
         Counters c{};
-        cudaStreamSynchronize(s->stream);
+        cudaStreamSynchronize(s->launch);
         cudaMemcpy(&c, s->d.counters, sizeof(Counters), cudaMemcpyDeviceToHost);
         if (which == AVBD_BUF_PAIRS) return (size_t)c.numPairs * 8;
         if (which == AVBD_BUF_MANIFOLDS) return (size_t)c.numPairs * sizeof(ManifoldGPU);
@@ -585,7 +683,7 @@ size_t avbd_debug_buffer_size(avbd_solver* s, int which) {
 int avbd_debug_read(avbd_solver* s, int which, void* dst, size_t bytes) {
     if (!s || !dst) return AVBD_ERR_INVALID_ARGUMENT;
     if (bytes > avbd_debug_buffer_size(s, which)) return AVBD_ERR_INVALID_ARGUMENT;
-    if (!s->check(cudaStreamSynchronize(s->stream), "debug read")) return AVBD_ERR_RUNTIME_FAILURE;
+    if (!s->check(cudaStreamSynchronize(s->launch), "debug read")) return AVBD_ERR_RUNTIME_FAILURE;
     const DevPtrs& d = s->d;
     const HostScene& H = s->H;
     const size_t nb = H.numBodies;

@@ -305,6 +305,31 @@ int avbd_snapshot_capture(avbd_solver* solver, avbd_snapshot** out);
 int avbd_snapshot_restore(avbd_solver* solver, const avbd_snapshot* snap);
 void avbd_snapshot_free(avbd_snapshot* snap);
 
+/* Launch all subsequent solver work on a caller-owned CUDA stream (a
+ * cudaStream_t passed as void*, e.g. the stream an application or benchmark
+ * records its CUDA events on).  NULL restores the solver's own stream.  The
+ * solver synchronises its previous stream before switching.               */
+int avbd_set_stream(avbd_solver* solver, void* cuda_stream);
+
+/* Per-stage GPU timing (the reference's `profiling` mode with encoder
+ * timestamps, GPUSolver.swift:3081-3093, :3167-3216, :4377-4400): while
+ * enabled, every frame records CUDA events at its stage boundaries, is
+ * retired synchronously, and its stage durations are accumulated.        */
+enum {
+    AVBD_STAGE_BROADPHASE = 0, AVBD_STAGE_NARROWPHASE = 1, AVBD_STAGE_PERSISTENCE_MAP = 2,
+    AVBD_STAGE_WARMSTART = 3, AVBD_STAGE_ADJACENCY = 4, AVBD_STAGE_COLORING = 5,
+    AVBD_STAGE_PRIMAL = 6, AVBD_STAGE_DUAL = 7, AVBD_STAGE_FINALIZE = 8,
+    AVBD_STAGE_COUNT_ = 9
+};
+typedef struct avbd_profile {
+    uint64_t frames;
+    uint64_t kernels_per_frame;   /* kernel nodes in one frame's graph      */
+    double stage_ms[16];          /* summed GPU time per stage              */
+    uint64_t stage_launches[16];  /* kernel launches per stage              */
+} avbd_profile;
+int avbd_set_profiling(avbd_solver* solver, int enabled);
+int avbd_get_profile(avbd_solver* solver, avbd_profile* out);
+
 /* Read-only access to one internal buffer for parity checks and tools
  * (no counterpart in the reference's public API; its tests read the same
  * buffers through @testable imports).  `which` is an AVBD_BUF_* id; `bytes`
