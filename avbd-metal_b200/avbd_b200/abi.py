@@ -164,7 +164,7 @@ EXPORTED = [
     "avbd_max_constraint_error", "avbd_get_counters", "avbd_runtime_failure",
     "avbd_last_error", "avbd_snapshot_capture", "avbd_snapshot_restore",
     "avbd_snapshot_free", "avbd_debug_buffer_size", "avbd_debug_read", "avbd_set_stream",
-    "avbd_set_profiling", "avbd_get_profile",
+    "avbd_set_profiling", "avbd_get_profile", "avbd_exclusive_scan_noalloc",
 ]
 
 STAGES = ["broadphase", "narrowphase", "persistence_map", "warmstart", "adjacency",

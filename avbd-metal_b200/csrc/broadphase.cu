@@ -6,6 +6,9 @@
 // per-bucket sort by collider id); pairs are produced in two passes (count
 // per producer, scan, emit in producer/cell order) so the pair list — and
 // with it the manifold index of every pair — is the same on every run.
+#include <mutex>
+
+#include "../../include/avbd.h"
 #include "dmath.cuh"
 #include "kernels.h"
 
@@ -268,4 +271,74 @@ void launch_broadphase(const Params& P, const DevPtrs& d, const Sizes& z, cudaSt
     k_bp_finalize<<<1, 1, 0, st>>>(P, d, z.producers);
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free exclusive scan (avbd_exclusive_scan_noalloc).
+//
+// Some callers cannot call cudaMalloc: an arena or pool that must own every
+// device allocation, a real-time loop with an allocation ban, a host whose
+// allocator must see every device allocation.  For them the scan's block sums
+// live in this fixed device array instead of solver- or caller-allocated
+// memory.  The array is part of the library's device image, so every GPU that
+// loads the library holds these 4 KiB until the process exits.  Host code may
+// not use the array's name as a device address (it is a host-side stand-in);
+// the real address is looked up once per device with cudaGetSymbolAddress.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kNoAllocScratchWords = SCAN_BLOCK;                        // 1024 block sums
+constexpr uint32_t kNoAllocMaxElements = SCAN_BLOCK * kNoAllocScratchWords;  // 1,048,576 words
+
+static __device__ __align__(256) uint32_t g_noalloc_scan_block_sums[kNoAllocScratchWords];
+
+namespace {
+constexpr int kMaxDevices = 256;
+std::mutex g_noalloc_mutex;
+uint32_t* g_noalloc_scratch[kMaxDevices] = {};   // device address per device ordinal
+}  // namespace
+
+void set_thread_error(const char* msg);
+
 }  // namespace avbd
+
+extern "C" int avbd_exclusive_scan_noalloc(const uint32_t* d_in, uint32_t* d_out, uint32_t n,
+                                           void* cuda_stream) {
+    using namespace avbd;
+    if (n == 0) return AVBD_OK;
+    if (!d_in || !d_out) {
+        set_thread_error("avbd_exclusive_scan_noalloc: null device pointer");
+        return AVBD_ERR_INVALID_ARGUMENT;
+    }
+    if (n > kNoAllocMaxElements) {
+        set_thread_error("avbd_exclusive_scan_noalloc: n exceeds the 1,048,576-element limit "
+                         "of its fixed 4 KiB scratch");
+        return AVBD_ERR_INVALID_ARGUMENT;
+    }
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        set_thread_error("avbd_exclusive_scan_noalloc: no current CUDA device");
+        return AVBD_ERR_NO_DEVICE;
+    }
+    uint32_t* scratch = nullptr;
+    {
+        // once per device, with that device current: the device address of
+        // the fixed scratch array
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_scratch[dev]) {
+            void* addr = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scan_block_sums);
+            if (e != cudaSuccess || !addr) {
+                set_thread_error("avbd_exclusive_scan_noalloc: cudaGetSymbolAddress failed");
+                return AVBD_ERR_KERNEL_MISSING;
+            }
+            g_noalloc_scratch[dev] = static_cast<uint32_t*>(addr);
+        }
+        scratch = g_noalloc_scratch[dev];
+    }
+    // k_scan_blocks writes block sum b before k_scan_block_sums and k_scan_add
+    // read it, so the shared scratch needs no clearing between calls.
+    launch_exclusive_scan(d_in, d_out, n, scratch, static_cast<cudaStream_t>(cuda_stream));
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_thread_error(cudaGetErrorString(e));
+        return AVBD_ERR_RUNTIME_FAILURE;
+    }
+    return AVBD_OK;
+}

@@ -23,6 +23,14 @@ using namespace avbd;
 
 namespace {
 thread_local std::string g_last_error;
+}  // namespace
+
+namespace avbd {
+// Message for avbd_last_error(NULL, ...) from entry points without a solver.
+void set_thread_error(const char* msg) { g_last_error = msg; }
+}  // namespace avbd
+
+namespace {
 
 __global__ void k_set_positions(float4* posLin, const float* xyz, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

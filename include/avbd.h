@@ -349,6 +349,31 @@ enum {
 size_t avbd_debug_buffer_size(avbd_solver* solver, int which);
 int avbd_debug_read(avbd_solver* solver, int which, void* dst, size_t bytes);
 
+/* Allocation-free exclusive prefix sum of `n` uint32 words on the current
+ * device: d_out[i] = d_in[0] + ... + d_in[i-1] (the scan the solver uses for
+ * its hash grid, pair lists and adjacency).  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc: code that runs inside an arena or
+ * memory pool that must own every device allocation, a real-time loop with
+ * an allocation ban, or a host application whose allocator must see every
+ * device allocation.  This call makes no cudaMalloc, cudaFree or other
+ * allocating call.  Its only scratch, 4 KiB of block sums, is a fixed array
+ * in the library's device image: every GPU that loads the library holds it
+ * until the process exits.
+ *
+ * Limit: n <= 1,048,576; a larger n returns AVBD_ERR_INVALID_ARGUMENT and
+ * leaves the message for avbd_last_error(NULL, ...).  d_in and d_out are
+ * device pointers on the current device and may alias; `cuda_stream` is a
+ * cudaStream_t passed as void* (NULL = the default stream).  The first call
+ * on a device looks up the scratch array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one scratch array, so calls that overlap on the GPU
+ * (work on different streams running at the same time) race: serialise them.
+ * Each call writes every scratch word it reads before reading it, so nothing
+ * has to be cleared between calls.                                          */
+int avbd_exclusive_scan_noalloc(const uint32_t* d_in, uint32_t* d_out, uint32_t n,
+                                void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
