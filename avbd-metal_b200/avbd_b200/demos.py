@@ -195,6 +195,35 @@ def particle_rod_chain_scene() -> PhysicsScene:
     return s
 
 
+def pinned_soft_block_scene(n: int = 10) -> PhysicsScene:
+    """A soft block hanging from world joints at its four top corners: every
+    particle a 3-DOF body, some carrying joints (general primal path)."""
+    s = PhysicsScene("pinned-soft-block")
+    add_ground(s, friction=0.5)
+    ids = add_soft_block(s, (0.0, 0.0, 2.0), n, n, n, 0.08, mu=2e4, lam=8e4,
+                         mass_per_node=0.01, friction=0.5, exclusion_joints=False)
+    grid = np.array(ids).reshape(n, n, n)
+    for i in (0, n - 1):
+        for j in (0, n - 1):
+            b = int(grid[i, j, n - 1])
+            p = s.bodies[b].position
+            s.add_joint(SceneJoint(-1, b, p, (0, 0, 0)))
+    s.settings.iterations = 12
+    return s
+
+
+def box_field_scene(count: int = 700, seed: int = 4) -> PhysicsScene:
+    """`count` small boxes on the ground in a loose grid (rigid, dynamic coloring)."""
+    rng = SplitMix64(seed)
+    s = PhysicsScene("box-field")
+    add_ground(s, friction=0.6)
+    side = int(math.ceil(math.sqrt(count)))
+    for i in range(count):
+        x, y = (i % side) * 0.5, (i // side) * 0.5
+        s.add_body((0.3, 0.3, 0.3), 500.0, 0.6, (x, y, 0.16 + rng.uniform(0.0, 0.05)))
+    return s
+
+
 SCENES = {
     "rigid-stack": rigid_stack_scene,
     "soft-cube": soft_cube_scene,

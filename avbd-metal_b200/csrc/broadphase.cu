@@ -170,81 +170,112 @@ __device__ __forceinline__ bool domains_compatible(uint32_t ga, uint32_t gb, uin
     return true;
 }
 
-// One producer (a hashed or global collider) in collider/cell order.
+// Per-frame collider record: world center and |radius|, plus the metadata
+// the pair filters need, so a candidate test is two 16-byte loads.
+__global__ void k_bp_prep(const Params P, const DevPtrs d, uint32_t numColliders) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= numColliders) return;
+    const uint32_t owner = d.colOwner[c];
+    const float4 pl = d.posLin[owner];
+    const float3 center = xyz(pl) + q_rotate(d.posAng[owner], xyz(d.colLocalPos[c]));
+    d.colCenter[c] = mk4(center, fabsf(d.colShape[c].w));
+    d.colMeta[c] = make_uint4(owner, d.colGroup[c], d.colShared[c] | (pl.w > 0.0f ? 2u : 0u),
+                              d.clothGroup[owner]);
+}
+
+// Candidate pairs of one producer collider (20_broadphase.metal:287-424),
+// one warp per producer: lane s < 27 scans neighbour cell s in (dz, dy, dx)
+// order, lane 27 scans the global list.  A cell whose hash equals an earlier
+// lane's is skipped (the reference's visited-bucket check).  Lane counts are
+// prefix-summed, so pairs come out in exactly the serial order: cells in
+// order, each bucket in collider order, then globals.
 template <bool EMIT>
-__global__ void k_bp_pairs(const Params P, const DevPtrs d) {
-    const uint32_t producer = blockIdx.x * blockDim.x + threadIdx.x;
-    if (producer >= P.numHashed + P.numGlobals) return;
-    const uint32_t base = EMIT ? d.pairStart[producer] : 0u;
+__global__ void k_bp_pairs(const Params P, const DevPtrs d, uint32_t producers) {
+    const uint32_t producer = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (producer >= producers) return;                     // warp-uniform
     uint32_t count = 0;
-    auto consider = [&](uint32_t b, uint32_t ownerA, float3 pa, float ra, bool aDyn,
-                        uint32_t outA, uint32_t outB) {
-        const uint32_t ownerB = d.colOwner[b];
-        if (ownerA == ownerB) return;
-        if (!aDyn && d.posLin[ownerB].w <= 0.0f) return;
-        const float rb = fabsf(d.colShape[b].w);
-        const float3 dp = pa - collider_center(d, b);
-        const float r = ra + rb;
-        if (dot(dp, dp) > r * r) return;
-        if (pair_excluded(d.exclusions, P.numExclusions, min(ownerA, ownerB), max(ownerA, ownerB))) return;
-        const uint32_t slot = base + count;
-        if (EMIT && slot < P.maxPairs) d.pairs[slot] = make_uint2(outA, outB);
-        count++;
+    const bool hashedProducer = producer < P.numHashed;
+    const uint32_t a = hashedProducer ? d.hashedIdx[producer] : d.globalIdx[producer - P.numHashed];
+    const float4 ca = d.colCenter[a];
+    const uint4 ma = d.colMeta[a];
+    const float3 pa = xyz(ca);
+    const float ra = ca.w;
+    const uint32_t ownerA = ma.x, groupA = ma.y, sharedA = ma.z & 1u, ga = ma.w;
+    const bool aDyn = (ma.z & 2u) != 0;
+    // first output slot of this lane: producer start + counts of lower lanes
+    uint32_t slot = 0;
+    // --- lane work: count (and in EMIT mode write) this lane's candidates
+    auto visit = [&](uint32_t b, uint32_t outA, uint32_t outB, bool emit) -> bool {
+        const uint4 mb = d.colMeta[b];
+        if (!domains_compatible(groupA, mb.y, sharedA, mb.z & 1u)) return false;
+        const uint32_t ownerB = mb.x;
+        if (ownerA == ownerB) return false;
+        if (!aDyn && (mb.z & 2u) == 0) return false;
+        const float4 cb = d.colCenter[b];
+        const float3 dp = pa - xyz(cb);
+        const float r = ra + cb.w;
+        if (dot(dp, dp) > r * r) return false;
+        if (pair_excluded(d.exclusions, P.numExclusions, min(ownerA, ownerB), max(ownerA, ownerB))) return false;
+        if (emit && slot + count < P.maxPairs) d.pairs[slot + count] = make_uint2(outA, outB);
+        return true;
     };
-    if (producer < P.numHashed) {
-        const uint32_t a = d.hashedIdx[producer];
-        const uint32_t ownerA = d.colOwner[a], groupA = d.colGroup[a], sharedA = d.colShared[a];
-        const float3 pa = collider_center(d, a);
-        const float ra = fabsf(d.colShape[a].w);
-        const bool aDyn = d.posLin[ownerA].w > 0.0f;
-        const uint32_t ga = d.clothGroup[ownerA];
-        if (!(ga != 0 && P.numHashedRigid == 0)) {
-            int cx, cy, cz;
-            cell_coord(pa, P.cellSize, cx, cy, cz);
-            uint32_t visited[27];
-            uint32_t nv = 0;
-            for (int dz = -1; dz <= 1; dz++)
-                for (int dy = -1; dy <= 1; dy++)
-                    for (int dx = -1; dx <= 1; dx++) {
-                        const uint32_t h = cell_hash(cx + dx, cy + dy, cz + dz, groupA, P.gridHashSize);
-                        bool dup = false;
-                        for (uint32_t v = 0; v < nv; v++) dup = dup || visited[v] == h;
-                        if (dup) continue;
-                        visited[nv++] = h;
-                        if (ga != 0 && d.cellRigid[h] == 0) continue;
+    auto run_lane = [&](bool emit) {
+        count = 0;
+        if (hashedProducer) {
+            if (lane < 27) {
+                if (!(ga != 0 && P.numHashedRigid == 0)) {
+                    int cx, cy, cz;
+                    cell_coord(pa, P.cellSize, cx, cy, cz);
+                    const int dz = (int)(lane / 9) - 1, dy = (int)((lane / 3) % 3) - 1, dx = (int)(lane % 3) - 1;
+                    const uint32_t h = cell_hash(cx + dx, cy + dy, cz + dz, groupA, P.gridHashSize);
+                    const unsigned same = __match_any_sync(0x07FFFFFFu, h);
+                    const bool dup = (same & ((1u << lane) - 1u)) != 0u;
+                    if (!dup && !(ga != 0 && d.cellRigid[h] == 0)) {
                         const uint32_t s0 = d.cellStart[h], e0 = s0 + d.cellCount[h];
                         for (uint32_t k = s0; k < e0; k++) {
                             const uint32_t b = d.cellBodies[k];
                             if (b <= a) continue;
-                            if (!domains_compatible(groupA, d.colGroup[b], sharedA, d.colShared[b])) continue;
                             // soft surface vs soft surface belongs to element contacts
-                            if (ga != 0 && d.clothGroup[d.colOwner[b]] != 0) continue;
-                            consider(b, ownerA, pa, ra, aDyn, a, b);
+                            if (ga != 0 && d.colMeta[b].w != 0) continue;
+                            if (visit(b, a, b, emit)) count++;
                         }
                     }
+                }
+            } else if (lane == 27) {
+                for (uint32_t g = 0; g < P.numGlobals; g++) {
+                    const uint32_t b = d.globalIdx[g];
+                    if (ga != 0 && d.colMeta[b].w == ga) continue;
+                    if (visit(b, min(a, b), max(a, b), emit)) count++;
+                }
+            }
+        } else if (lane == 27) {
+            const uint32_t gp = producer - P.numHashed;
+            for (uint32_t g = gp + 1; g < P.numGlobals; g++) {
+                const uint32_t b = d.globalIdx[g];
+                if (ga != 0 && d.colMeta[b].w == ga) continue;
+                if (visit(b, min(a, b), max(a, b), emit)) count++;
+            }
         }
-        for (uint32_t g = 0; g < P.numGlobals; g++) {
-            const uint32_t b = d.globalIdx[g];
-            if (!domains_compatible(groupA, d.colGroup[b], sharedA, d.colShared[b])) continue;
-            if (ga != 0 && d.clothGroup[d.colOwner[b]] == ga) continue;
-            consider(b, ownerA, pa, ra, aDyn, min(a, b), max(a, b));
-        }
+    };
+    if (!EMIT) {
+        run_lane(false);
+        d.pairLaneCount[(size_t)producer * 32 + lane] = count;
+        uint32_t total = count;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+        if (lane == 0) d.pairCount[producer] = total;
     } else {
-        const uint32_t gp = producer - P.numHashed;
-        const uint32_t a = d.globalIdx[gp];
-        const uint32_t ownerA = d.colOwner[a], groupA = d.colGroup[a], sharedA = d.colShared[a];
-        const float3 pa = collider_center(d, a);
-        const float ra = fabsf(d.colShape[a].w);
-        const bool aDyn = d.posLin[ownerA].w > 0.0f;
-        const uint32_t ga = d.clothGroup[ownerA];
-        for (uint32_t g = gp + 1; g < P.numGlobals; g++) {
-            const uint32_t b = d.globalIdx[g];
-            if (!domains_compatible(groupA, d.colGroup[b], sharedA, d.colShared[b])) continue;
-            if (ga != 0 && d.clothGroup[d.colOwner[b]] == ga) continue;
-            consider(b, ownerA, pa, ra, aDyn, min(a, b), max(a, b));
+        const uint32_t mine = d.pairLaneCount[(size_t)producer * 32 + lane];
+        uint32_t x = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= (uint32_t)o) x += y;
         }
+        slot = d.pairStart[producer] + x - mine;
+        run_lane(true);
     }
-    if (!EMIT) d.pairCount[producer] = count;
 }
 
 __global__ void k_bp_finalize(const Params P, const DevPtrs d, uint32_t producers) {
@@ -264,9 +295,12 @@ void launch_broadphase(const Params& P, const DevPtrs& d, const Sizes& z, cudaSt
         k_bp_sort_cells<<<(P.gridHashSize + T - 1) / T, T, 0, st>>>(P, d);
     }
     if (z.producers > 0) {
-        k_bp_pairs<false><<<(z.producers + T - 1) / T, T, 0, st>>>(P, d);
+        k_bp_prep<<<(z.numColliders + T - 1) / T, T, 0, st>>>(P, d, z.numColliders);
+        const uint32_t warpsPerBlock = T / 32;
+        const uint32_t blocks = (z.producers + warpsPerBlock - 1) / warpsPerBlock;
+        k_bp_pairs<false><<<blocks, T, 0, st>>>(P, d, z.producers);
         launch_exclusive_scan(d.pairCount, d.pairStart, z.producers, d.scanScratch, st);
-        k_bp_pairs<true><<<(z.producers + T - 1) / T, T, 0, st>>>(P, d);
+        k_bp_pairs<true><<<blocks, T, 0, st>>>(P, d, z.producers);
     }
     k_bp_finalize<<<1, 1, 0, st>>>(P, d, z.producers);
 }

@@ -24,8 +24,10 @@ struct DevPtrs {
     // broadphase
     uint32_t *cellCount, *cellStart, *cellBodies, *cellRigid;
     uint2* bodyCellSlot;
-    uint32_t *pairCount, *pairStart;
+    uint32_t *pairCount, *pairStart, *pairLaneCount;
     uint2* pairs;
+    float4* colCenter;                    // per frame: world center xyz, |radius|
+    uint4* colMeta;                       // owner, group, shared | dynamic << 1, clothGroup(owner)
     // contacts (current frame and previous frame)
     ManifoldGPU *manifolds, *prevManifolds;
     uint32_t *mapKeyA, *mapKeyB, *mapVal;
@@ -63,6 +65,7 @@ struct Sizes {
     uint32_t maxPairs, producers, numDynamicBodies;
     uint32_t scanScratchWords;
     bool dynamicColoring;
+    bool particleFastPath;   // every dynamic body a particle with only tet/contact entries
 };
 
 // exclusive scan of n words (n <= 1024 * 1024); out may not alias in
@@ -78,7 +81,7 @@ void launch_dynamic_coloring(const Params& P, const DevPtrs& d, const Sizes& z, 
 // one color of the block-descent primal; `count` is the color's body count
 // when known on the host (static palette), else 0xFFFFFFFF (read on device)
 void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color,
-                         uint32_t count, cudaStream_t st);
+                         uint32_t count, uint32_t lanes, cudaStream_t st);
 // every iteration of a small scene in one thread block
 void launch_solve_small(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t colorBound,
                         cudaStream_t st);

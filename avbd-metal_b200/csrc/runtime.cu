@@ -199,7 +199,7 @@ struct avbd_solver {
                     const uint32_t count = z.dynamicColoring ? 0xFFFFFFFFu : H.colorCounts[c];
                     if (count == 0) continue;
                     mark(AVBD_STAGE_PRIMAL);
-                    launch_primal_color(P, f, z, c, count, st);
+                    launch_primal_color(P, f, z, c, count, H.colorLanes[c], st);
                 }
                 mark(AVBD_STAGE_DUAL);
                 launch_dual(P, f, z, st);
@@ -274,6 +274,7 @@ struct avbd_solver {
         z.producers = P.numHashed + P.numGlobals;
         z.numDynamicBodies = H.numDynamicBodies;
         z.dynamicColoring = H.dynamicColoring;
+        z.particleFastPath = H.particleFastPath;
         const uint32_t scanLimit = 1024u * 1024u;
         if (P.gridHashSize > scanLimit || z.producers > scanLimit || nb > scanLimit) {
             error = "scene exceeds the 1M-element scan limit of this build";
@@ -307,7 +308,9 @@ struct avbd_solver {
         ok = ok && alloc(d.cellRigid, P.gridHashSize, "cellRigid") && alloc(d.cellBodies, P.numHashed, "cellBodies");
         ok = ok && alloc(d.bodyCellSlot, P.numHashed, "bodyCellSlot");
         ok = ok && alloc(d.pairCount, z.producers, "pairCount") && alloc(d.pairStart, z.producers, "pairStart");
+        ok = ok && alloc(d.pairLaneCount, (size_t)z.producers * 32, "pairLaneCount");
         ok = ok && alloc(d.pairs, H.maxPairs, "pairs");
+        ok = ok && alloc(d.colCenter, nc, "colliderCenter") && alloc(d.colMeta, nc, "colliderMeta");
         ok = ok && alloc(d.manifolds, H.maxPairs, "manifolds", true) && alloc(d.prevManifolds, H.maxPairs, "prevManifolds", true);
         ok = ok && alloc(d.mapKeyA, H.mapCapacity, "mapKeyA", true) && alloc(d.mapKeyB, H.mapCapacity, "mapKeyB", true);
         ok = ok && alloc(d.mapVal, H.mapCapacity, "mapVal", true);

@@ -12,12 +12,39 @@
 // lanes then sum their 6x6 systems with an xor butterfly (offsets 4, 2, 1)
 // and lane 0 solves.  The static part of the adjacency (joints, springs,
 // tets) is built once at upload; only contact entries are rebuilt per frame.
+#include <utility>
+
 #include "dmath.cuh"
 #include "kernels.h"
 
 namespace avbd {
 
 constexpr float FLT_BIG = 3.402823466e38f;
+
+// Programmatic dependent launch: the iteration loop is a chain of ~120
+// dependent kernels per frame.  Each kernel lets the next one be scheduled as
+// soon as all of its own blocks are running, and waits for the previous grid
+// to complete (and its writes to be visible) before touching solver state.
+__device__ __forceinline__ void pdl_prologue() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+static void launch_pdl(void (*kernel)(KArgs...), uint32_t blocks, uint32_t threads, cudaStream_t st,
+                       Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 // failure kinds (mirrors AVBD_FAIL_* of include/avbd.h)
 constexpr uint32_t AVBD_FAIL_RIGID_PAIR_CAPACITY_ = 2;
 constexpr uint32_t AVBD_FAIL_UNRESOLVED_COLORING_ = 5;
@@ -656,12 +683,261 @@ __global__ void k_primal(const Params P, const DevPtrs d, uint32_t color, uint32
     primal_body(P, d, d.colorList[s + slot], lane, mask);
 }
 
+// ---------------------------------------------------------------------------
+// Warp-per-body primal for particles.  The 8-lane kernel above makes each
+// lane walk 2-3 tets as chains of dependent loads.  Here all 32 lanes of a
+// warp evaluate the force terms of 32 adjacency entries at once, and lanes
+// 0-7 then fold them in the 8-lane order — logical lane l takes entries
+// l, l+8, l+16, l+24 — applying exactly the additions the stamp would have
+// made, so every float is unchanged.  Entries whose terms do not fit the
+// shipped record (joints, springs, multi-contact manifolds) are stamped by
+// the logical lane itself during the fold.
+// ---------------------------------------------------------------------------
+struct ParticleTerms {
+    float3 rhs;          // tet: gradient; manifold: J^T F
+    float3 a, b, c;      // tet: (G00, G11, G22), (G01, G02, G12), (dd, -, -); manifold: rows of J^T K J
+    uint32_t kind;       // 0 none, 1 tet, 2 one-contact manifold, 3 stamp serially
+};
+
+__device__ __forceinline__ void particle_terms(const Params& P, const DevPtrs& d, uint32_t entry,
+                                               uint32_t self, ParticleTerms& t) {
+    const uint32_t kind = entry >> ADJ_KIND_SHIFT, idx = entry & ADJ_INDEX_MASK;
+    t.kind = 3;
+    if (kind == FK_TET) {
+        const TetGPU tt = d.tets[idx];
+        const float3 x0 = xyz(d.posLin[tt.ids.x]), x1 = xyz(d.posLin[tt.ids.y]);
+        const float3 x2 = xyz(d.posLin[tt.ids.z]), x3 = xyz(d.posLin[tt.ids.w]);
+        const float muV = tt.r1.w, lamV = tt.r2.w;
+        const float alphaT = 1.0f + muV / mx(lamV, 1e-9f);
+        const float3 d0 = x1 - x0, d1 = x2 - x0, d2 = x3 - x0;
+        const float3 m0 = xyz(tt.r0), m1 = xyz(tt.r1), m2 = xyz(tt.r2);
+        const float3 f0 = d0 * m0.x + d1 * m1.x + d2 * m2.x;
+        const float3 f1 = d0 * m0.y + d1 * m1.y + d2 * m2.y;
+        const float3 f2 = d0 * m0.z + d1 * m1.z + d2 * m2.z;
+        const float J = dot(f0, cross(f1, f2));
+        const float3 j0 = cross(f1, f2), j1 = cross(f2, f0), j2 = cross(f0, f1);
+        const float s2 = lamV * (J - alphaT);
+        const float3 p0 = muV * f0 + s2 * j0;
+        const float3 p1 = muV * f1 + s2 * j1;
+        const float3 p2 = muV * f2 + s2 * j2;
+        float3 w;
+        if (self == tt.ids.y) w = m0;
+        else if (self == tt.ids.z) w = m1;
+        else if (self == tt.ids.w) w = m2;
+        else w = -mk3(m0.x + m1.x + m2.x, m0.y + m1.y + m2.y, m0.z + m1.z + m2.z);
+        t.rhs = p0 * w.x + p1 * w.y + p2 * w.z;
+        const float3 g = j0 * w.x + j1 * w.y + j2 * w.z;
+        // lamV * outer(g, g) is exactly symmetric: g_i g_j == g_j g_i
+        t.a = mk3((g.x * g.x) * lamV, (g.y * g.y) * lamV, (g.z * g.z) * lamV);
+        t.b = mk3((g.y * g.x) * lamV, (g.z * g.x) * lamV, (g.z * g.y) * lamV);
+        t.c = mk3(muV * dot(w, w), 0.0f, 0.0f);
+        t.kind = 1;
+    } else if (kind == FK_MANIFOLD) {
+        const ManifoldGPU& m = d.manifolds[idx];
+        const u4 h = m.header;
+        if (h.z != 1u) return;
+        const uint32_t a = h.x, b = h.y;
+        const bool isA = self == a;
+        const bool sphA = (h.w & 2u) != 0, sphB = (h.w & 4u) != 0;
+        const float4 qa = d.posAng[a], qb = d.posAng[b];
+        const float3 dqALin = xyz(d.posLin[a]) - xyz(d.initLin[a]);
+        const float3 dqAAng = q_sub(qa, d.initAng[a]);
+        const float3 dqBLin = xyz(d.posLin[b]) - xyz(d.initLin[b]);
+        const float3 dqBAng = q_sub(qb, d.initAng[b]);
+        const float3 nrm = xyz(m.basisN), t1 = xyz(m.basisT1), t2 = cross(nrm, t1);
+        const ContactGPU c = m.contacts[0];
+        const float3 rAW = sphA ? xyz(c.rA) : q_rotate(qa, xyz(c.rA));
+        const float3 rBW = sphB ? xyz(c.rB) : q_rotate(qb, xyz(c.rB));
+        float3 C;
+        float fs, bnd;
+        const float3 F = contact_force(c, nrm, t1, t2, m.basisN.w, m.basisT1.w, P.alpha, dqALin, dqAAng, dqBLin,
+                                       dqBAng, rAW, rBW, C, fs, bnd);
+        const float sg = isA ? 1.0f : -1.0f;
+        const M3 jLin = M3{nrm * sg, t1 * sg, t2 * sg};
+        const M3 K = m3_diag(xyz(c.penalty));
+        const M3 jLinT = m3_transpose(jLin);
+        const M3 M = m3_mulm(m3_mulm(jLinT, K), jLin);
+        t.a = M.r0;
+        t.b = M.r1;
+        t.c = M.r2;
+        t.rhs = m3_mul(jLinT, F);
+        t.kind = 2;
+    }
+}
+
+__device__ __forceinline__ float3 shfl_idx3(float3 v, int src) {
+    return mk3(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
+               __shfl_sync(0xffffffffu, v.z, src));
+}
+
+// Linear block of a particle's system: the only part its solve reads.
+struct ParticleAccum { M3 lhs; float3 rhs; };
+
+// Rare entries (joints, springs, multi-contact manifolds) go through the
+// generic stamp, which changes lhsLin/rhsLin exactly as it would inside a
+// full accumulator.  Scenes that cannot produce them (every dynamic body a
+// particle whose adjacency holds only tets and sphere contacts — known at
+// upload) use the GENERAL = false instance, which drops these paths and
+// their registers.
+__device__ __forceinline__ void stamp_entry_particle(const Params& P, const DevPtrs& d, uint32_t entry,
+                                                     uint32_t body, ParticleAccum* acc) {
+    Accum full{acc->lhs, m3_zero(), m3_zero(), acc->rhs, s3(0)};
+    stamp_entry(P, d, entry, body, full);
+    acc->lhs = full.lhsLin;
+    acc->rhs = full.rhsLin;
+}
+
+// The particle system's angular block is the identity and its cross block
+// zero.  Every term of the 6x6 LDL^T that involves them is then an exact
+// "x - (+0)" (L4x..L6x, y4..y6, z4..z6 and xAng are all +0), so this 3x3
+// sequence returns bit for bit the linear part of solve6x6(lhs, I, 0, b, 0);
+// with non-finite input both produce a non-finite step and the update is
+// skipped.
+__device__ __forceinline__ float3 solve3x3_particle(const M3& a, float3 b) {
+    const float s1 = rsq(mx(a.r0.x, 1e-30f));
+    const float s2 = rsq(mx(a.r1.y, 1e-30f));
+    const float s3_ = rsq(mx(a.r2.z, 1e-30f));
+    const float A11 = 1.0f, A22 = 1.0f, A33 = 1.0f;
+    const float A21 = a.r1.x * s2 * s1;
+    const float A31 = a.r2.x * s3_ * s1, A32 = a.r2.y * s3_ * s2;
+    b = mk3(b.x * s1, b.y * s2, b.z * s3_);
+    const float L21 = A21 / A11, L31 = A31 / A11;
+    const float eps = 1e-6f;
+    const float D1 = mx(A11, eps);
+    const float D2 = mx(A22 - L21 * L21 * D1, eps);
+    const float L32 = (A32 - L21 * L31 * D1) / D2;
+    const float D3 = mx(A33 - (L31 * L31 * D1 + L32 * L32 * D2), eps);
+    const float y1 = b.x;
+    const float y2 = b.y - L21 * y1;
+    const float y3 = b.z - L31 * y1 - L32 * y2;
+    const float z1 = y1 / D1, z2 = y2 / D2, z3 = y3 / D3;
+    float3 x;
+    x.z = z3;
+    x.y = z2 - L32 * x.z;
+    x.x = z1 - L21 * x.y - L31 * x.z;
+    return mk3(x.x * s1, x.y * s2, x.z * s3_);
+}
+
+// Primal for one color with LANES consecutive lanes per body (8, 16 or 32,
+// chosen per color from its bodies' adjacency sizes).  Lane p of a group
+// evaluates entry base + p; logical lane l < 8 then folds entries
+// base + l, base + l + 8, ... in order.  Any LANES gives the same floats.
+template <int LANES, bool GENERAL>
+__global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevPtrs d, uint32_t color,
+                                                      uint32_t count) {
+    constexpr int GROUPS = 32 / LANES;
+    pdl_prologue();
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t slot = tid / LANES;
+    const uint32_t lane = tid & (LANES - 1);
+    const uint32_t s = d.colorStart[color];
+    const uint32_t n = count != 0xFFFFFFFFu ? count : d.colorStart[color + 1] - s;
+    if (slot >= n) return;                                   // uniform across the group
+    const unsigned mask = LANES == 32 ? 0xffffffffu
+                                      : (((1u << LANES) - 1u) << ((threadIdx.x & 31u) & ~(uint32_t)(LANES - 1)));
+    (void)GROUPS;
+    const uint32_t body = d.colorList[s + slot];
+    const float4 shp = d.shape[body];
+    if (GENERAL && shp.w >= 0.0f) {                          // rigid: the 8-lane path
+        if (lane < 8) primal_body(P, d, body, lane, mask & (0xFFu << ((threadIdx.x & 31u) & ~(uint32_t)(LANES - 1))));
+        return;
+    }
+    // lane 0 needs these after the reduction; issue the loads now
+    float4 pl = make_float4(0, 0, 0, 0), inert = make_float4(0, 0, 0, 0);
+    if (lane == 0) { pl = d.posLin[body]; inert = d.inertLin[body]; }
+    ParticleAccum acc{m3_zero(), s3(0)};
+    const AdjView v = adj_view(d, body);
+    const uint32_t cnt = v.count();
+    for (uint32_t base = 0; base < cnt; base += LANES) {
+        const uint32_t k = base + lane;
+        ParticleTerms t;
+        t.kind = 0;
+        uint32_t entry = 0;
+        if (k < cnt) {
+            entry = v.at(k);
+            particle_terms(P, d, entry, body, t);
+        }
+#pragma unroll
+        for (int j = 0; j < LANES / 8; j++) {
+            const int src = (int)(lane & 7u) + 8 * j;
+            ParticleTerms u;
+            uint32_t e;
+            if (j == 0) {
+                // logical lane l already holds entry base + l
+                u = t;
+                e = entry;
+            } else {
+            u.kind = __shfl_sync(mask, t.kind, src, LANES);
+            u.rhs = mk3(__shfl_sync(mask, t.rhs.x, src, LANES), __shfl_sync(mask, t.rhs.y, src, LANES),
+                        __shfl_sync(mask, t.rhs.z, src, LANES));
+            u.a = mk3(__shfl_sync(mask, t.a.x, src, LANES), __shfl_sync(mask, t.a.y, src, LANES),
+                      __shfl_sync(mask, t.a.z, src, LANES));
+            u.b = mk3(__shfl_sync(mask, t.b.x, src, LANES), __shfl_sync(mask, t.b.y, src, LANES),
+                      __shfl_sync(mask, t.b.z, src, LANES));
+            u.c = mk3(__shfl_sync(mask, t.c.x, src, LANES), __shfl_sync(mask, t.c.y, src, LANES),
+                      __shfl_sync(mask, t.c.z, src, LANES));
+            e = __shfl_sync(mask, entry, src, LANES);
+            }
+            if (lane < 8) {
+                if (u.kind == 1u) {
+                    acc.rhs += u.rhs;
+                    acc.lhs = m3_add(acc.lhs, m3_diag(s3(u.c.x)));
+                    acc.lhs = m3_add(acc.lhs, M3{mk3(u.a.x, u.b.x, u.b.y), mk3(u.b.x, u.a.y, u.b.z),
+                                                 mk3(u.b.y, u.b.z, u.a.z)});
+                } else if (u.kind == 2u) {
+                    acc.lhs = m3_add(acc.lhs, M3{u.a, u.b, u.c});
+                    acc.rhs += u.rhs;
+                } else if (GENERAL && u.kind == 3u) {
+                    stamp_entry_particle(P, d, e, body, &acc);
+                }
+            }
+        }
+    }
+    // xor butterfly over the 8 logical lanes (offsets 4, 2, 1)
+#pragma unroll
+    for (int o = 4; o >= 1; o >>= 1) {
+        acc.lhs.r0 = acc.lhs.r0 + mk3(__shfl_xor_sync(mask, acc.lhs.r0.x, o, LANES), __shfl_xor_sync(mask, acc.lhs.r0.y, o, LANES), __shfl_xor_sync(mask, acc.lhs.r0.z, o, LANES));
+        acc.lhs.r1 = acc.lhs.r1 + mk3(__shfl_xor_sync(mask, acc.lhs.r1.x, o, LANES), __shfl_xor_sync(mask, acc.lhs.r1.y, o, LANES), __shfl_xor_sync(mask, acc.lhs.r1.z, o, LANES));
+        acc.lhs.r2 = acc.lhs.r2 + mk3(__shfl_xor_sync(mask, acc.lhs.r2.x, o, LANES), __shfl_xor_sync(mask, acc.lhs.r2.y, o, LANES), __shfl_xor_sync(mask, acc.lhs.r2.z, o, LANES));
+        acc.rhs = acc.rhs + mk3(__shfl_xor_sync(mask, acc.rhs.x, o, LANES), __shfl_xor_sync(mask, acc.rhs.y, o, LANES), __shfl_xor_sync(mask, acc.rhs.z, o, LANES));
+    }
+    if (lane != 0) return;
+    const float mass = pl.w;
+    const float dt2 = P.dt * P.dt;
+    acc.lhs = m3_add(acc.lhs, m3_diag(s3(mass / dt2)));
+    acc.rhs += (xyz(pl) - xyz(inert)) * (mass / dt2);
+    float3 dxLin = solve3x3_particle(acc.lhs, -acc.rhs);
+    if (!finite3(dxLin)) return;
+    const float maxLin = 0.35f * fabsf(shp.w);
+    const float lin2 = dot(dxLin, dxLin);
+    if (lin2 > maxLin * maxLin) dxLin *= maxLin * rsq(lin2);
+    d.posLin[body] = mk4(xyz(pl) + dxLin, mass);
+}
+
+template <bool GENERAL>
+static void launch_primal_group(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count,
+                                uint32_t lanes, cudaStream_t st) {
+    const int T = 128;
+    const uint32_t blocks = (count * lanes + T - 1) / T;
+    if (lanes <= 8) launch_pdl(k_primal_group<8, GENERAL>, blocks, T, st, P, d, color, count);
+    else if (lanes <= 16) launch_pdl(k_primal_group<16, GENERAL>, blocks, T, st, P, d, color, count);
+    else launch_pdl(k_primal_group<32, GENERAL>, blocks, T, st, P, d, color, count);
+}
+
 void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color, uint32_t count,
-                         cudaStream_t st) {
+                         uint32_t lanes, cudaStream_t st) {
     const int T = 128;
     const uint32_t upper = count != 0xFFFFFFFFu ? count : z.numDynamicBodies;
     if (upper == 0) return;
-    k_primal<<<(upper * 8 + T - 1) / T, T, 0, st>>>(P, d, color, count);
+    if (z.dynamicColoring) {
+        k_primal<<<(upper * 8 + T - 1) / T, T, 0, st>>>(P, d, color, count);
+    } else {
+        // the grouped kernel needs the color's body count on the host
+        const uint32_t lanes_ = lanes < 8 ? 8 : (lanes > 32 ? 32 : lanes);
+        const uint32_t w = lanes_ <= 8 ? 8 : (lanes_ <= 16 ? 16 : 32);
+        if (z.particleFastPath) launch_primal_group<false>(P, d, color, upper, w, st);
+        else launch_primal_group<true>(P, d, color, upper, w, st);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -779,6 +1055,7 @@ __device__ __forceinline__ void dual_item(const Params& P, const DevPtrs& d, con
 }
 
 __global__ void k_dual(const Params P, const DevPtrs d, const Sizes z) {
+    pdl_prologue();
     const uint32_t total = z.numActiveJoints + z.numHardSprings + d.counters->numPairs;
     const uint32_t numPairs = d.counters->numPairs;
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x)
@@ -786,7 +1063,7 @@ __global__ void k_dual(const Params P, const DevPtrs d, const Sizes z) {
 }
 
 void launch_dual(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
-    k_dual<<<stride_blocks(z.numActiveJoints + z.numHardSprings + z.maxPairs, 128), 128, 0, st>>>(P, d, z);
+    launch_pdl(k_dual, stride_blocks(z.numActiveJoints + z.numHardSprings + z.maxPairs, 128), 128, st, P, d, z);
 }
 
 // ---------------------------------------------------------------------------

@@ -430,6 +430,27 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
         for (uint32_t v : {H.tets[t].ids.x, H.tets[t].ids.y, H.tets[t].ids.z, H.tets[t].ids.w})
             if (dyn(v)) post[v].push_back(e);
     }
+    // The warp-per-particle primal may drop its generic stamp path when no
+    // dynamic body is rigid and no particle carries a joint or spring entry
+    // (sphere contacts always have exactly one contact point).
+    H.particleFastPath = true;
+    for (uint32_t b = 0; b < nb; b++) {
+        if (!(H.posLin[b].w > 0.0f)) continue;
+        if (H.shape[b].w >= 0.0f || !pre[b].empty()) { H.particleFastPath = false; break; }
+    }
+    // lanes per body for each static color: enough for the largest static
+    // adjacency plus one contact entry in a single pass
+    H.colorLanes.assign(MAX_COLORS, 8);
+    if (!H.dynamicColoring) {
+        for (int c = 0; c < MAX_COLORS; c++) {
+            size_t mx = 0;
+            for (uint32_t i = H.colorStart[c]; i < H.colorStart[c + 1]; i++) {
+                const uint32_t b = H.colorList[i];
+                mx = std::max(mx, pre[b].size() + post[b].size() + 1);
+            }
+            H.colorLanes[c] = mx <= 8 ? 8u : (mx <= 16 ? 16u : 32u);
+        }
+    }
     H.staticSeg.assign(nb, u4{});
     for (uint32_t b = 0; b < nb; b++) {
         std::sort(pre[b].begin(), pre[b].end());

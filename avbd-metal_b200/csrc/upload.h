@@ -17,6 +17,7 @@ struct HostScene {
     bool dynamicColoring = true;
     uint32_t staticUsedColors = 1;
     uint32_t numDynamicBodies = 0;
+    bool particleFastPath = false;   // all dynamic bodies are particles without joints/springs
     Params P{};
 
     // bodies (SoA float4)
@@ -44,6 +45,7 @@ struct HostScene {
 
     // static palette (soft scenes) in final form
     std::vector<uint32_t> colors, colorStart, colorList, colorCounts;
+    std::vector<uint32_t> colorLanes;      // lanes per body for each static color
 
     // Static per-body adjacency, split around the per-frame contact entries:
     // pre = joints + springs (kinds 0, 1), post = tets (kind 3), each sorted.

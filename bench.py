@@ -296,7 +296,7 @@ def run_ours(args, world, rank, local):
                        "timing": "CUDA events on the solver stream per step, max over ranks"},
             "clocks": clock, "e2e": e2e,
             "gpu_launches": int(kernels_per_frame * K),
-            "roofline": {"bound": "hbm", "kernel": "k_primal (per-color 8-lane block-descent primal)",
+            "roofline": {"bound": "hbm", "kernel": "k_primal_group (per-color block-descent primal, 8/16/32 lanes per body)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                          else "fallback 6.65 TB/s",

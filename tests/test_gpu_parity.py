@@ -71,6 +71,8 @@ def test_upload_records_bitwise(cuda_lib, oracle_lib):
     ("stack5", lambda: demos.stack(5), 120),
     ("rigid-stack-20", lambda: demos.rigid_stack_scene(seed=1), 90),
     ("soft-cube-6", lambda: demos.soft_cube_scene(seed=5, n=6), 90),
+    ("pinned-soft-block-10", lambda: demos.pinned_soft_block_scene(10), 40),
+    ("box-field-700", lambda: demos.box_field_scene(700), 40),
 ])
 def test_trajectory_parity(cuda_lib, oracle_lib, name, make, frames):
     g, o, exact = run_parity(make(), oracle_lib, frames)
