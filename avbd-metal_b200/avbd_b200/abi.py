@@ -5,7 +5,7 @@ tests/test_abi.py checks the sizes against the compiled library.
 """
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 # status codes
 OK = 0
@@ -30,8 +30,8 @@ FAIL_SOFT_CONTACT_CAPACITY = 3
 FAIL_STATIC_COLOR_CAPACITY = 4
 FAIL_UNRESOLVED_COLORING = 5
 FAIL_PLANAR_DAT_PAIR_CAPACITY = 6
-FAIL_PLANAR_DAT_SOFT_CAPACITY = 7
-FAIL_PLANAR_DAT_INVALID = 8
+FAIL_PLANAR_DAT_GRID_SPAN = 7
+FAIL_PLANAR_DAT_INVALID_ANCHOR = 8
 FAIL_WAIT_TIMEOUT = 9
 
 SHAPE_BOX, SHAPE_SPHERE, SHAPE_TORUS, SHAPE_CAPSULE = 0, 1, 2, 3
@@ -44,7 +44,9 @@ BUF = dict(
     ADJ_COUNT=7, ADJ_LIST=8, COLORS=9, COLOR_START=10, COLOR_LIST=11, CELL_START=12,
     CELL_COUNT=13, CELL_BODIES=14, MAP_KEY_A=15, MAP_KEY_B=16, MAP_VAL=17, JOINTS=18,
     SPRINGS=19, TETS=20, INIT_LIN=21, INERT_LIN=22, EXCLUSIONS=23, HASHED_IDX=24,
-    GLOBAL_IDX=25,
+    GLOBAL_IDX=25, TRIS=26, EDGES=27, NBR_START=28, NBR_COUNT=29, NBR_LIST=30,
+    PARTICLE_IDX=31, MEMBRANES=32, BENDS=33, SOFT=34, DAT_PAIRS=35, CLOTH_GROUP=36,
+    OGC_PREV=37,
 )
 
 F3 = C.c_float * 3
@@ -153,6 +155,11 @@ class Counters(C.Structure):
         ("soft_candidates", C.c_uint32), ("used_colors", C.c_uint32),
         ("color_conflicts", C.c_uint32), ("ogc_exceeded", C.c_uint32),
         ("color_counts", C.c_uint32 * 64),
+        ("dat_pairs", C.c_uint32), ("dat_vt_pairs", C.c_uint32), ("dat_ee_pairs", C.c_uint32),
+        ("dat_grid_overflows", C.c_uint32), ("dat_invalid_anchors", C.c_uint32),
+        ("dat_truncations", C.c_uint32), ("dat_vt_degenerate", C.c_uint32),
+        ("dat_ee_degenerate", C.c_uint32), ("dat_nonfinite", C.c_uint32),
+        ("dat_tet_degenerate", C.c_uint32),
     ]
 
 
@@ -168,7 +175,7 @@ EXPORTED = [
 ]
 
 STAGES = ["broadphase", "narrowphase", "persistence_map", "warmstart", "adjacency",
-          "coloring", "primal", "dual", "finalize"]
+          "coloring", "primal", "dual", "finalize", "element_contacts", "truncation"]
 
 
 class Profile(C.Structure):

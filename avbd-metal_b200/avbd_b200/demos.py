@@ -12,7 +12,7 @@ import math
 import numpy as np
 
 from . import abi
-from .scene import PhysicsScene, SceneJoint, SceneSpring, SceneTet
+from .scene import PhysicsScene, SceneJoint, SceneSpring, SceneTet, SceneTri
 
 f32 = np.float32
 MASK64 = (1 << 64) - 1
@@ -118,6 +118,77 @@ def add_soft_block(s: PhysicsScene, center, nx: int, ny: int, nz: int, spacing: 
     return flat
 
 
+def add_cloth_grid(s: PhysicsScene, positions, thickness: float, mass_per_node: float,
+                   friction: float = 0.7, structural_k: float = 5000.0, hard_rods: bool = True,
+                   shear_k: float = 60.0, bend_k: float = 8.0, membrane_mu: float = 300.0,
+                   membrane_bend: float = 5e-4, pinned=()):
+    """Demos7.addClothGrid (Demos7.swift:17-84): a particle grid with
+    structural rods (hard AL rods by default: `structural_k` is their penalty
+    cap), StVK membranes with mu = lambda = `membrane_mu` and Bergou bending
+    on alternating diagonals.  `pinned` lists (i, j) nodes given zero mass."""
+    nu, nv = len(positions), len(positions[0])
+    pinned = set(pinned)
+    grid = []
+    for i in range(nu):
+        row = []
+        for j in range(nv):
+            m = 0.0 if (i, j) in pinned else mass_per_node
+            row.append(s.add_particle(thickness, m, friction, tuple(positions[i][j])))
+        grid.append(row)
+
+    def link(a, b, k, hard=False):
+        s.add_spring(SceneSpring(a, b, (0, 0, 0), (0, 0, 0), k, hard=hard))
+
+    for i in range(nu):
+        for j in range(nv):
+            if i + 1 < nu:
+                link(grid[i][j], grid[i + 1][j], structural_k, hard_rods)
+            if j + 1 < nv:
+                link(grid[i][j], grid[i][j + 1], structural_k, hard_rods)
+            if membrane_mu <= 0:
+                if i + 1 < nu and j + 1 < nv:
+                    link(grid[i][j], grid[i + 1][j + 1], shear_k)
+                    link(grid[i + 1][j], grid[i][j + 1], shear_k)
+                if i + 2 < nu:
+                    link(grid[i][j], grid[i + 2][j], bend_k)
+                if j + 2 < nv:
+                    link(grid[i][j], grid[i][j + 2], bend_k)
+    for i in range(nu - 1):
+        for j in range(nv - 1):
+            v00, v10 = grid[i][j], grid[i + 1][j]
+            v01, v11 = grid[i][j + 1], grid[i + 1][j + 1]
+
+            def tri(a, b, c):
+                s.add_tri(SceneTri((a, b, c), membrane_mu, membrane_mu, membrane_bend))
+
+            if (i + j) % 2 == 0:
+                tri(v00, v10, v11)
+                tri(v00, v11, v01)
+            else:
+                tri(v00, v10, v01)
+                tri(v10, v11, v01)
+    return grid
+
+
+def drape_scene(res: int = 28, friction: float = 0.6, membrane_mu: float = 300.0,
+                bend: float = 5e-4) -> PhysicsScene:
+    """Demos7.drape (Demos7.swift:270-301): a res x res sheet of 2.8 m falls
+    onto a static sphere of diameter 1.1 m above the ground."""
+    s = PhysicsScene("drape")
+    st = s.settings
+    st.iterations, st.beta_lin, st.particle_damping, st.cloth_viscosity = 10, 20000.0, 1.5, 0.25
+    add_ground(s, friction=friction)
+    s.add_sphere(1.1, 0.0, friction, (0.0, 0.0, 1.0))
+    n = max(20, res)
+    size = f32(2.8)
+    spacing = size / f32(n - 1)
+    r = min(f32(0.05), f32(0.3) * spacing)
+    pos = [[(float(f32(i) * spacing - size / f32(2)), float(f32(j) * spacing - size / f32(2)), 1.75)
+            for j in range(n)] for i in range(n)]
+    add_cloth_grid(s, pos, float(r), 0.008, friction, membrane_mu=membrane_mu, membrane_bend=bend)
+    return s
+
+
 # ---------------------------------------------------------------------------
 # Synthetic benchmark scenes (one per solver configuration)
 # ---------------------------------------------------------------------------
@@ -164,6 +235,38 @@ def soft_cube_scene(seed: int = 2, n: int = 24, iterations: int = 20,
                    exclusion_joints=exclusion_joints)
     st = s.settings
     st.dt, st.gravity, st.iterations = 1.0 / 60.0, -9.81, iterations
+    return s
+
+
+def cloth_sphere_scene(seed: int = 3, n: int = 256, iterations: int = 30,
+                       hard_rods: bool = True) -> PhysicsScene:
+    """Cloth with self-contact: an n x n sheet of 2 m side (spacing 2/(n-1)),
+    membrane mu = lambda = 1e4, Bergou bending 1e-3, particle (contact) radius
+    2e-3 m, areal density 0.1 kg/m^2, two corners of one edge pinned, held
+    0.1 m above a static sphere of radius 0.5 m (centre z = 1) over the ground;
+    in-plane noise U(+-1e-4 m) from the seed.  Hard structural rods
+    (penalty cap 5000) as in addClothGrid.  Planar-DAT is selected
+    automatically (shell-only scene); dt 1/120, `iterations` iterations."""
+    rng = SplitMix64(seed)
+    s = PhysicsScene("cloth-sphere")
+    st = s.settings
+    st.dt, st.iterations, st.beta_lin = 1.0 / 120.0, iterations, 20000.0
+    st.particle_damping, st.cloth_viscosity = 1.5, 0.25
+    add_ground(s, friction=0.5)
+    s.add_sphere(1.0, 0.0, 0.5, (0.0, 0.0, 1.0))
+    side = f32(2.0)
+    spacing = side / f32(n - 1)
+    pos = []
+    for i in range(n):
+        row = []
+        for j in range(n):
+            x = f32(i) * spacing - side / f32(2) + f32(rng.uniform(-1e-4, 1e-4))
+            y = f32(j) * spacing - side / f32(2) + f32(rng.uniform(-1e-4, 1e-4))
+            row.append((float(x), float(y), 1.6))
+        pos.append(row)
+    mass = float(f32(0.1) * side * side / f32(n * n))
+    add_cloth_grid(s, pos, 2e-3, mass, 0.5, hard_rods=hard_rods, membrane_mu=1e4,
+                   membrane_bend=1e-3, pinned=((0, 0), (0, n - 1)))
     return s
 
 
@@ -227,4 +330,5 @@ def box_field_scene(count: int = 700, seed: int = 4) -> PhysicsScene:
 SCENES = {
     "rigid-stack": rigid_stack_scene,
     "soft-cube": soft_cube_scene,
+    "cloth-sphere": cloth_sphere_scene,
 }

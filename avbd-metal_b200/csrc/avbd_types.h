@@ -67,6 +67,29 @@ static_assert(sizeof(SpringGPU) == 64, "SpringGPU layout");
 static_assert(sizeof(TetGPU) == 64, "TetGPU layout");
 static_assert(sizeof(ManifoldGPU) == 704, "ManifoldGPU layout");
 
+// Cloth element records (00_common.metal:387-421).
+struct MembraneGPU { u4 ids; f4 dm, mat; };   // StVK: DmInv (a, b, c, d); (mu A, lambda A, A)
+struct BendGPU { u4 ids; f4 K, mat; };        // Bergou hinge: cotangent K; 3 kappa / (A1 + A2)
+struct SoftContactGPU {                       // element contact on a 4-slot stencil
+    u4 ids;       // WORLD_BODY = unused slot
+    f4 normal;    // w = friction
+    f4 anchorA;   // rigid slot-0 local anchor, or (restT, 0, 0); w = flag bits
+    f4 weights;
+    f4 C0;        // x = normal gap at step start; w = lambda cap
+    f4 lambda;    // w = persistence key A (bits)
+    f4 penalty;   // w = persistence key B (bits)
+};
+static_assert(sizeof(MembraneGPU) == 48, "MembraneGPU layout");
+static_assert(sizeof(BendGPU) == 48, "BendGPU layout");
+static_assert(sizeof(SoftContactGPU) == 112, "SoftContactGPU layout");
+
+constexpr uint32_t SC_VT = 1, SC_RT = 2, SC_EE = 3;
+constexpr uint32_t SCF_RIGID_A = 1, SCF_SIDE_NEG = 2, SCF_KIND_SHIFT = 2, SCF_ROUND_A = 32;
+constexpr uint32_t DAT_PAIR_VT = 0, DAT_PAIR_EE = 1, DAT_PAIR_TRUNCATE = 1, DAT_PAIR_CONTACT = 2;
+constexpr uint32_t ELEM_EDGE_BIT = 0x80000000u;
+constexpr uint32_t RT_MAX_PER_TRI = 4;
+constexpr uint32_t FULL_PASS = 0xFFFFFFFFu;
+
 // Per-frame parameters (SimParams, 00_common.metal:233-288), passed by value.
 struct Params {
     float dt, gravity, alpha, betaLin, betaAng, gamma;
@@ -81,6 +104,12 @@ struct Params {
     uint32_t surfaceTruncationMode, tetInversionPreventionEnabled;
     float planarDATRelaxation;
     uint32_t numExclusions;
+    // cloth element pipeline (Planar-DAT)
+    uint32_t cloth;                   // authored triangles: element contacts + Planar-DAT
+    uint32_t colorJacobi;             // the primal writes posNext; a commit pass publishes it
+    uint32_t numEdges, numSurfaceEdges, elemHashSize;
+    uint32_t maxDatPairs, maxSoft, softMapCapacity, numMembranes, numBends;
+    float elemMargin, queryRadius, elemCellSize, surfaceCellSize, clothViscosity;
 };
 
 // Device counters of one frame (the reference's CTR_* layout, trimmed).
@@ -95,6 +124,14 @@ struct Counters {
     uint32_t colorCount[MAX_COLORS];
     uint32_t colorStart[MAX_COLORS + 2];
     uint32_t changed[32];
+    // element contacts and Planar-DAT (CTR_SOFT .. CTR_DAT_TET_DEGENERATE)
+    uint32_t numSoftRT;       // rigid-triangle records at the head of the soft list
+    uint32_t softRaw;         // soft demand before capacity clipping
+    uint32_t numSoft;         // stored soft records
+    uint32_t datRaw, datStored, datVT, datEE;   // current pair stream
+    uint32_t datPairsPeak, datVTPeak, datEEPeak;
+    uint32_t datGridOverflow, datInvalidAnchor, datTruncations;
+    uint32_t datVTDegenerate, datEEDegenerate, datNonfinite, datTetDegenerate;
 };
 
 }  // namespace avbd

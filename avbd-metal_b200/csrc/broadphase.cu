@@ -110,6 +110,28 @@ void launch_exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32
     }
 }
 
+// Any n < 2^30: scan blocks of 1024, scan the block sums recursively in
+// place (each thread reads its words before writing them), add back.
+void launch_exclusive_scan_large(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scratch,
+                                 cudaStream_t st) {
+    if (n == 0) return;
+    const uint32_t nblocks = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+    k_scan_blocks<<<nblocks, SCAN_THREADS, 0, st>>>(in, out, scratch, n);
+    if (nblocks > 1) {
+        launch_exclusive_scan_large(scratch, scratch, nblocks, scratch + nblocks, st);
+        k_scan_add<<<nblocks, SCAN_THREADS, 0, st>>>(out, scratch, n);
+    }
+}
+
+size_t scan_large_scratch_words(uint32_t n) {
+    size_t words = 64;
+    for (uint32_t m = n; m > 1;) {
+        m = (m + SCAN_BLOCK - 1) / SCAN_BLOCK;
+        words += m;
+    }
+    return words;
+}
+
 // ---------------------------------------------------------------------------
 // Spatial hash
 // ---------------------------------------------------------------------------

@@ -15,6 +15,7 @@ struct DevPtrs {
     float4 *velLin, *velAng, *prevVelLin, *props, *shape, *spinVel;
     float* gravityScale;
     uint32_t* clothGroup;
+    uint32_t* bodyShape;                  // AVBD_SHAPE_* of each body
     // colliders
     uint32_t *colOwner, *colShapeType, *colGroup, *colShared;
     float4 *colShape, *colLocalPos, *colLocalRot;
@@ -58,6 +59,24 @@ struct DevPtrs {
     uint32_t numSpinners, numRateMotors;
     uint32_t* failureLatch;               // [0] kind, [1] frame, [2] detail
     uint32_t* frameCounter;
+    // cloth: element topology (static)
+    uint4* tris;                          // collision triangles (authored, then tet faces)
+    uint2* edges;                         // unique edges, authored prefix first
+    uint32_t *nbrStart, *nbrCount, *nbrList;   // sorted one-ring per vertex
+    uint32_t *particleIdx, *selfCollision;
+    MembraneGPU* membranes;
+    BendGPU* bends;
+    // cloth: per frame
+    uint32_t *elemCellCount, *elemCellStart, *elemCursor, *elemCells;
+    uint32_t *datOwnerCount, *datOwnerStart;    // pairs per query owner (particles, edges)
+    uint4* datPairs;                            // (kind, owner, other, flags)
+    uint32_t *rtCount, *rtStart;                // rigid-triangle records per triangle
+    uint32_t *datEmit, *datEmitStart;           // element contacts per query owner
+    SoftContactGPU *soft, *prevSoft;
+    uint32_t *softKeyA, *softKeyB, *softVal;
+    uint32_t* truncBits;                        // Planar-DAT step fraction per body (float bits)
+    float4 *ogcPrev, *posNext, *angNext;
+    uint32_t* bigScanScratch;
 };
 
 struct Sizes {
@@ -66,6 +85,9 @@ struct Sizes {
     uint32_t scanScratchWords;
     bool dynamicColoring;
     bool particleFastPath;   // every dynamic body a particle with only tet/contact entries
+    // cloth
+    uint32_t numTris, numParticles, numEdges, numMembranes, numBends;
+    uint32_t maxDatPairs, maxSoft, elemHashSize;
 };
 
 // exclusive scan of n words (n <= 1024 * 1024); out may not alias in
@@ -92,5 +114,22 @@ void launch_max_constraint_error(const Params& P, const DevPtrs& d, const Sizes&
 void launch_reset_bodies(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 // spinners and legacy rate motors, then the end-of-frame failure check
 void launch_frame_end(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+
+// exclusive scan of any n < 2^30 words; scratch holds n/1024 + n/1024^2 + 64 words
+void launch_exclusive_scan_large(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* scratch,
+                                 cudaStream_t st);
+size_t scan_large_scratch_words(uint32_t n);
+
+// cloth element pipeline (cloth.cu)
+// step-start detection: element grid, pair stream, rigid-triangle contacts
+void launch_cloth_detect(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+// after the predictor: predictor truncation, accepted-pose pair stream,
+// element contacts, soft map, re-anchor
+void launch_cloth_accept(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+// per-color Planar-DAT pass that also publishes the color's solve
+void launch_dat_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color, uint32_t count,
+                      cudaStream_t st);
+void launch_cloth_restore(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_cloth_smoothing(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 
 }  // namespace avbd

@@ -165,7 +165,10 @@ struct avbd_solver {
     // With profiling on, an event is recorded at every stage boundary.
     void encode_frame(int parity) {
         DevPtrs f = d;
-        if (parity) std::swap(f.manifolds, f.prevManifolds);
+        if (parity) {
+            std::swap(f.manifolds, f.prevManifolds);
+            std::swap(f.soft, f.prevSoft);
+        }
         cudaStream_t st = stream;
         usedEvents = 0;
         auto mark = [&](int stage) {
@@ -181,8 +184,16 @@ struct avbd_solver {
         launch_narrowphase(P, f, z, st);
         mark(AVBD_STAGE_PERSISTENCE_MAP);
         launch_map_rebuild(P, f, z, st);
+        if (P.cloth) {
+            mark(AVBD_STAGE_ELEMENT_CONTACTS);
+            launch_cloth_detect(P, f, z, st);
+        }
         mark(AVBD_STAGE_WARMSTART);
         launch_warmstart(P, f, z, st);
+        if (P.cloth) {
+            mark(AVBD_STAGE_ELEMENT_CONTACTS);
+            launch_cloth_accept(P, f, z, st);
+        }
         mark(AVBD_STAGE_ADJACENCY);
         launch_adjacency(P, f, z, st);
         if (z.dynamicColoring) {
@@ -200,20 +211,26 @@ struct avbd_solver {
                     if (count == 0) continue;
                     mark(AVBD_STAGE_PRIMAL);
                     launch_primal_color(P, f, z, c, count, H.colorLanes[c], st);
+                    if (P.cloth) {
+                        mark(AVBD_STAGE_TRUNCATION);
+                        launch_dat_color(P, f, z, c, count, st);
+                    }
                 }
                 mark(AVBD_STAGE_DUAL);
                 launch_dual(P, f, z, st);
             }
         }
         mark(AVBD_STAGE_FINALIZE);
+        if (P.cloth) launch_cloth_restore(P, f, z, st);
         launch_finalize(P, f, z, st);
+        if (P.cloth) launch_cloth_smoothing(P, f, z, st);
         launch_frame_end(P, f, z, st);
         mark(-1);
     }
 
     int events_needed() const {
         const uint32_t colorBound = z.dynamicColoring ? (uint32_t)MAX_COLORS : H.staticUsedColors;
-        return 16 + (int)(P.iterations * (colorBound + 1));
+        return 20 + (int)(P.iterations * (2 * colorBound + 1));
     }
 
     bool build_graphs() {
@@ -275,6 +292,14 @@ struct avbd_solver {
         z.numDynamicBodies = H.numDynamicBodies;
         z.dynamicColoring = H.dynamicColoring;
         z.particleFastPath = H.particleFastPath;
+        z.numTris = H.numTris;
+        z.numParticles = P.numParticles;
+        z.numEdges = H.numEdges;
+        z.numMembranes = (uint32_t)H.membranes.size();
+        z.numBends = (uint32_t)H.bends.size();
+        z.maxDatPairs = H.maxDatPairs;
+        z.maxSoft = H.maxSoft;
+        z.elemHashSize = H.elemHashSize;
         const uint32_t scanLimit = 1024u * 1024u;
         if (P.gridHashSize > scanLimit || z.producers > scanLimit || nb > scanLimit) {
             error = "scene exceeds the 1M-element scan limit of this build";
@@ -294,6 +319,7 @@ struct avbd_solver {
         ok = ok && upload(reinterpret_cast<f4*&>(d.spinVel), H.spinVel, "spinVel");
         ok = ok && upload(d.gravityScale, H.gravityScale, "gravityScale");
         ok = ok && upload(d.clothGroup, H.clothGroup, "clothGroup");
+        ok = ok && upload(d.bodyShape, H.shapeType, "bodyShape");
         // colliders
         ok = ok && upload(d.colOwner, H.colOwner, "colliderOwner") && upload(d.colShapeType, H.colShapeType, "colliderShapeType");
         ok = ok && upload(d.colGroup, H.colGroup, "colliderGroup") && upload(d.colShared, H.colShared, "colliderShared");
@@ -324,7 +350,7 @@ struct avbd_solver {
         ok = ok && upload(reinterpret_cast<u4*&>(d.staticSeg), H.staticSeg, "staticSeg");
         ok = ok && upload(d.preList, H.preList, "preList") && upload(d.postList, H.postList, "postList");
         ok = ok && alloc(d.dynCount, nb, "dynCount") && alloc(d.dynStart, nb, "dynStart") && alloc(d.dynCursor, nb, "dynCursor");
-        ok = ok && alloc(d.dynList, 2 * (size_t)H.maxPairs, "dynList");
+        ok = ok && alloc(d.dynList, 2 * (size_t)H.maxPairs + (P.cloth ? 4 * (size_t)H.maxSoft : 0), "dynList");
         // coloring
         ok = ok && upload(d.colorsA, H.colors, "colorsA", true) && upload(d.colorsB, H.colors, "colorsB");
         ok = ok && alloc(d.bodySlot, nb, "bodySlot");
@@ -340,6 +366,32 @@ struct avbd_solver {
         ok = ok && alloc(d.failureLatch, 4, "failureLatch") && alloc(d.frameCounter, 1, "frameCounter", true);
         if (H.dynamicColoring)
             d.colorStart = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(d.counters) + offsetof(Counters, colorStart));
+        if (P.cloth) {
+            // element topology
+            ok = ok && upload(reinterpret_cast<u4*&>(d.tris), H.tris, "tris");
+            ok = ok && upload(reinterpret_cast<uint32_t*&>(d.edges), H.edges, "edges");
+            ok = ok && upload(d.nbrStart, H.nbrStart, "nbrStart") && upload(d.nbrCount, H.nbrCount, "nbrCount");
+            ok = ok && upload(d.nbrList, H.nbrList, "nbrList") && upload(d.particleIdx, H.particleIdx, "particleIdx");
+            ok = ok && upload(d.selfCollision, H.selfCollision, "softSelfCollision");
+            ok = ok && upload(d.membranes, H.membranes, "membranes") && upload(d.bends, H.bends, "bends");
+            // element grid, pair streams, element contacts
+            const size_t elems = (size_t)H.numTris + H.numEdges;
+            const uint32_t owners = P.numParticles + H.numEdges;
+            ok = ok && alloc(d.elemCellCount, H.elemHashSize, "elemCellCount") && alloc(d.elemCellStart, H.elemHashSize, "elemCellStart");
+            ok = ok && alloc(d.elemCursor, H.elemHashSize, "elemCursor") && alloc(d.elemCells, 64 * elems, "elemCells");
+            ok = ok && alloc(d.datOwnerCount, owners, "datOwnerCount") && alloc(d.datOwnerStart, owners, "datOwnerStart");
+            ok = ok && alloc(d.datEmit, owners, "datEmit") && alloc(d.datEmitStart, owners, "datEmitStart");
+            ok = ok && alloc(d.datPairs, H.maxDatPairs, "planarDATPairs");
+            ok = ok && alloc(d.rtCount, H.numTris, "rtCount") && alloc(d.rtStart, H.numTris, "rtStart");
+            ok = ok && alloc(d.soft, H.maxSoft, "softContacts", true) && alloc(d.prevSoft, H.maxSoft, "prevSoftContacts", true);
+            ok = ok && alloc(d.softKeyA, H.softMapCapacity, "softMapKeyA", true);
+            ok = ok && alloc(d.softKeyB, H.softMapCapacity, "softMapKeyB", true) && alloc(d.softVal, H.softMapCapacity, "softMapVal", true);
+            std::vector<uint32_t> ones(nb, 0x3F800000u);
+            ok = ok && upload(d.truncBits, ones, "planarDATT");
+            ok = ok && alloc(d.ogcPrev, nb, "ogcPrev", true) && alloc(d.posNext, nb, "posNext", true) && alloc(d.angNext, nb, "angNext", true);
+            const uint32_t scanMax = std::max(std::max(H.elemHashSize, owners), H.numTris);
+            ok = ok && alloc(d.bigScanScratch, scan_large_scratch_words(scanMax), "scanScratchLarge");
+        }
         std::vector<uint32_t> spB, rJ;
         std::vector<f4> spA;
         std::vector<float> rV;
@@ -358,7 +410,7 @@ struct avbd_solver {
         std::memset(hostLatch, 0, 4 * sizeof(uint32_t));
         std::memset(hostCounters, 0, sizeof(Counters));
         // Small scenes run their whole iteration loop in one thread block.
-        smallSolve = z.numDynamicBodies <= 512;
+        smallSolve = z.numDynamicBodies <= 512 && !P.cloth;
         if (cudaDeviceSynchronize() != cudaSuccess) { error = "device error during upload"; return AVBD_ERR_NO_DEVICE; }
         return AVBD_OK;
     }
@@ -375,6 +427,18 @@ struct avbd_solver {
             if (failure == AVBD_FAIL_RIGID_PAIR_CAPACITY)
                 std::snprintf(buf, sizeof buf, "rigid pair capacity exceeded at frame %u: %u candidates > %u",
                               hostLatch[1], hostLatch[2], H.maxPairs);
+            else if (failure == AVBD_FAIL_SOFT_CONTACT_CAPACITY)
+                std::snprintf(buf, sizeof buf, "soft contact capacity exceeded at frame %u: %u records > %u",
+                              hostLatch[1], hostLatch[2], H.maxSoft);
+            else if (failure == AVBD_FAIL_PLANAR_DAT_PAIR_CAPACITY)
+                std::snprintf(buf, sizeof buf, "Planar-DAT pair capacity exceeded at frame %u: %u pairs > %u",
+                              hostLatch[1], hostLatch[2], H.maxDatPairs);
+            else if (failure == AVBD_FAIL_PLANAR_DAT_GRID_SPAN)
+                std::snprintf(buf, sizeof buf, "Planar-DAT element grid span exceeded at frame %u: %u elements",
+                              hostLatch[1], hostLatch[2]);
+            else if (failure == AVBD_FAIL_PLANAR_DAT_INVALID_ANCHOR)
+                std::snprintf(buf, sizeof buf, "Planar-DAT invalid anchor at frame %u: %u pairs", hostLatch[1],
+                              hostLatch[2]);
             else
                 std::snprintf(buf, sizeof buf, "unresolved dynamic coloring at frame %u: %u conflicting bodies",
                               hostLatch[1], hostLatch[2]);
@@ -583,6 +647,18 @@ int avbd_get_counters(avbd_solver* s, avbd_counters* out) {
         out->used_colors = s->H.staticUsedColors;
         for (int i = 0; i < 64; i++) out->color_counts[i] = s->H.colorCounts[i];
     }
+    out->num_soft = c.numSoft;
+    out->soft_candidates = c.softRaw;
+    out->dat_pairs = c.datPairsPeak;
+    out->dat_vt_pairs = c.datVTPeak;
+    out->dat_ee_pairs = c.datEEPeak;
+    out->dat_grid_overflows = c.datGridOverflow;
+    out->dat_invalid_anchors = c.datInvalidAnchor;
+    out->dat_truncations = c.datTruncations;
+    out->dat_vt_degenerate = c.datVTDegenerate;
+    out->dat_ee_degenerate = c.datEEDegenerate;
+    out->dat_nonfinite = c.datNonfinite;
+    out->dat_tet_degenerate = c.datTetDegenerate;
     return AVBD_OK;
 }
 
@@ -687,6 +763,23 @@ size_t avbd_debug_buffer_size(avbd_solver* s, int which) {
     case AVBD_BUF_EXCLUSIONS: return H.exclusions.size() * 4;
     case AVBD_BUF_HASHED_IDX: return H.hashedIdx.size() * 4;
     case AVBD_BUF_GLOBAL_IDX: return H.globalIdx.size() * 4;
+    case AVBD_BUF_TRIS: return H.tris.size() * 16;
+    case AVBD_BUF_EDGES: return H.edges.size() * 4;
+    case AVBD_BUF_NBR_START: return H.nbrStart.size() * 4;
+    case AVBD_BUF_NBR_COUNT: return H.nbrCount.size() * 4;
+    case AVBD_BUF_NBR_LIST: return H.nbrList.size() * 4;
+    case AVBD_BUF_PARTICLE_IDX: return s->P.cloth ? (size_t)s->P.numParticles * 4 : 0;
+    case AVBD_BUF_MEMBRANES: return H.membranes.size() * sizeof(MembraneGPU);
+    case AVBD_BUF_BENDS: return H.bends.size() * sizeof(BendGPU);
+    case AVBD_BUF_CLOTH_GROUP: return nb * 4;
+    case AVBD_BUF_OGC_PREV: return s->P.cloth ? nb * 16 : 0;
+    case AVBD_BUF_SOFT: case AVBD_BUF_DAT_PAIRS: {
+        if (!s->P.cloth) return 0;
+        Counters c{};
+        cudaStreamSynchronize(s->launch);
+        cudaMemcpy(&c, s->d.counters, sizeof(Counters), cudaMemcpyDeviceToHost);
+        return which == AVBD_BUF_SOFT ? (size_t)c.numSoft * sizeof(SoftContactGPU) : (size_t)c.datStored * 16;
+    }
     default: return 0;
     }
 }
@@ -726,10 +819,23 @@ int avbd_debug_read(avbd_solver* s, int which, void* dst, size_t bytes) {
     case AVBD_BUF_EXCLUSIONS: src = d.exclusions; break;
     case AVBD_BUF_HASHED_IDX: src = d.hashedIdx; break;
     case AVBD_BUF_GLOBAL_IDX: src = d.globalIdx; break;
+    case AVBD_BUF_TRIS: src = d.tris; break;
+    case AVBD_BUF_EDGES: src = d.edges; break;
+    case AVBD_BUF_NBR_START: src = d.nbrStart; break;
+    case AVBD_BUF_NBR_COUNT: src = d.nbrCount; break;
+    case AVBD_BUF_NBR_LIST: src = d.nbrList; break;
+    case AVBD_BUF_PARTICLE_IDX: src = d.particleIdx; break;
+    case AVBD_BUF_MEMBRANES: src = d.membranes; break;
+    case AVBD_BUF_BENDS: src = d.bends; break;
+    case AVBD_BUF_CLOTH_GROUP: src = d.clothGroup; break;
+    case AVBD_BUF_OGC_PREV: src = d.ogcPrev; break;
+    // element contacts swap like the manifolds
+    case AVBD_BUF_SOFT: src = odd ? d.soft : d.prevSoft; break;
+    case AVBD_BUF_DAT_PAIRS: src = d.datPairs; break;
     case AVBD_BUF_ADJ_START: case AVBD_BUF_ADJ_COUNT: case AVBD_BUF_ADJ_LIST: {
         // materialise the merged (pre, contacts, post) lists
         std::vector<uint32_t> dc(nb), ds(nb);
-        std::vector<uint32_t> dl(2 * (size_t)H.maxPairs);
+        std::vector<uint32_t> dl(2 * (size_t)H.maxPairs + (s->P.cloth ? 4 * (size_t)H.maxSoft : 0));
         cudaMemcpy(dc.data(), d.dynCount, 4 * nb, cudaMemcpyDeviceToHost);
         cudaMemcpy(ds.data(), d.dynStart, 4 * nb, cudaMemcpyDeviceToHost);
         cudaMemcpy(dl.data(), d.dynList, 4 * dl.size(), cudaMemcpyDeviceToHost);

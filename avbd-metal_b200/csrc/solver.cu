@@ -161,6 +161,8 @@ __global__ void k_warmstart_bodies(const Params P, const DevPtrs d) {
     if (!isfinite(w)) w = 0.0f;
     d.initLin[gid] = mk4(xyz(pl), 0.0f);
     d.initAng[gid] = pa;
+    // the committed collision-query pose of every surface vertex, pins included
+    if (P.cloth && P.surfaceTruncationMode != 0u && d.shape[gid].w < 0.0f) d.ogcPrev[gid] = mk4(xyz(pl), 0.0f);
     if (mass > 0.0f) {
         // Isotropic-OGC warm-start truncation is a no-op while every bound is
         // "far" (no element contact emitted a bound), which holds for every
@@ -180,23 +182,32 @@ void launch_warmstart(const Params& P, const DevPtrs& d, const Sizes& z, cudaStr
 // ---------------------------------------------------------------------------
 // Per-frame contact adjacency: count, scan, scatter, sort per body.
 // ---------------------------------------------------------------------------
-__global__ void k_adj_dyn_count(const DevPtrs d) {
-    const uint32_t n = d.counters->numPairs;
-    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
-        const u4 h = d.manifolds[m].header;
-        if (h.z == 0) continue;
-        if (body_dynamic(d, h.x)) atomicAdd(&d.dynCount[h.x], 1u);
-        if (body_dynamic(d, h.y)) atomicAdd(&d.dynCount[h.y], 1u);
-    }
-}
-__global__ void k_adj_dyn_scatter(const DevPtrs d) {
-    const uint32_t n = d.counters->numPairs;
-    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < n; m += gridDim.x * blockDim.x) {
-        const u4 h = d.manifolds[m].header;
-        if (h.z == 0) continue;
-        const uint32_t e = (FK_MANIFOLD << ADJ_KIND_SHIFT) | m;
-        if (body_dynamic(d, h.x)) d.dynList[atomicAdd(&d.dynCursor[h.x], 1u)] = e;
-        if (body_dynamic(d, h.y)) d.dynList[atomicAdd(&d.dynCursor[h.y], 1u)] = e;
+// Items: this frame's manifolds, then (cloth scenes) its element contacts.
+template <bool SCATTER>
+__global__ void k_adj_dyn(const Params P, const DevPtrs d) {
+    const uint32_t nm = d.counters->numPairs;
+    const uint32_t ns = P.cloth ? d.counters->numSoft : 0u;
+    auto put = [&](uint32_t b, uint32_t e) {
+        if (!body_dynamic(d, b)) return;
+        if (SCATTER) d.dynList[atomicAdd(&d.dynCursor[b], 1u)] = e;
+        else atomicAdd(&d.dynCount[b], 1u);
+    };
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nm + ns; i += gridDim.x * blockDim.x) {
+        if (i < nm) {
+            const u4 h = d.manifolds[i].header;
+            if (h.z == 0) continue;
+            const uint32_t e = (FK_MANIFOLD << ADJ_KIND_SHIFT) | i;
+            put(h.x, e);
+            put(h.y, e);
+        } else {
+            const uint32_t k = i - nm;
+            const u4 ids = d.soft[k].ids;
+            const uint32_t e = (FK_SOFT << ADJ_KIND_SHIFT) | k;
+            put(ids.x, e);
+            put(ids.y, e);
+            put(ids.z, e);
+            put(ids.w, e);
+        }
     }
 }
 __global__ void k_adj_dyn_sort(const DevPtrs d, uint32_t nb) {
@@ -214,10 +225,11 @@ __global__ void k_adj_dyn_sort(const DevPtrs d, uint32_t nb) {
 
 void launch_adjacency(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     cudaMemsetAsync(d.dynCount, 0, sizeof(uint32_t) * P.numBodies, st);
-    k_adj_dyn_count<<<stride_blocks(z.maxPairs, 128), 128, 0, st>>>(d);
+    const uint32_t items = z.maxPairs + (P.cloth ? z.maxSoft : 0u);
+    k_adj_dyn<false><<<stride_blocks(items, 128), 128, 0, st>>>(P, d);
     launch_exclusive_scan(d.dynCount, d.dynStart, P.numBodies, d.scanScratch, st);
     cudaMemcpyAsync(d.dynCursor, d.dynStart, sizeof(uint32_t) * P.numBodies, cudaMemcpyDeviceToDevice, st);
-    k_adj_dyn_scatter<<<stride_blocks(z.maxPairs, 128), 128, 0, st>>>(d);
+    k_adj_dyn<true><<<stride_blocks(items, 128), 128, 0, st>>>(P, d);
     k_adj_dyn_sort<<<(P.numBodies + 127) / 128, 128, 0, st>>>(d, P.numBodies);
 }
 
@@ -605,6 +617,130 @@ __device__ void stamp_manifold(const Params& P, const DevPtrs& d, const Manifold
     }
 }
 
+// StVK membrane, Gauss-Newton Hessian (40_solver.metal:1088-1134).
+__device__ void stamp_membrane(const DevPtrs& d, const MembraneGPU& mb, uint32_t self, Accum& acc) {
+    const float3 x0 = xyz(d.posLin[mb.ids.x]), x1 = xyz(d.posLin[mb.ids.y]), x2 = xyz(d.posLin[mb.ids.z]);
+    const float muA = mb.mat.x, lamA = mb.mat.y;
+    const float3 d0 = x1 - x0, d1 = x2 - x0;
+    const float a = mb.dm.x, b = mb.dm.y, c = mb.dm.z, dd = mb.dm.w;
+    const float3 f1 = d0 * a + d1 * b;
+    const float3 f2 = d0 * c + d1 * dd;
+    const float E11 = 0.5f * (dot(f1, f1) - 1.0f);
+    const float E22 = 0.5f * (dot(f2, f2) - 1.0f);
+    const float E12 = 0.5f * dot(f1, f2);
+    const float trE = E11 + E22;
+    const float S11 = 2.0f * muA * E11 + lamA * trE;
+    const float S22 = 2.0f * muA * E22 + lamA * trE;
+    const float S12 = 2.0f * muA * E12;
+    const float3 p1 = f1 * S11 + f2 * S12;
+    const float3 p2 = f1 * S12 + f2 * S22;
+    float wx, wy;
+    if (self == mb.ids.y) { wx = a; wy = c; }
+    else if (self == mb.ids.z) { wx = b; wy = dd; }
+    else { wx = -a - b; wy = -c - dd; }
+    acc.rhsLin += p1 * wx + p2 * wy;
+    const float3 g11 = f1 * wx, g22 = f2 * wy;
+    const float3 g12 = (f2 * wx + f1 * wy) * 0.5f;
+    const float3 gtr = g11 + g22;
+    acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(g11, g11), 2.0f * muA));
+    acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(g22, g22), 2.0f * muA));
+    acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(g12, g12), 4.0f * muA));
+    acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(gtr, gtr), lamA));
+}
+
+// Quadratic (Bergou) bending, rank-1 isotropic Hessian (40_solver.metal:1136-1153).
+__device__ void stamp_bend(const DevPtrs& d, const BendGPU& bd, uint32_t self, Accum& acc) {
+    const float sc = bd.mat.x;
+    const float3 m = xyz(d.posLin[bd.ids.x]) * bd.K.x + xyz(d.posLin[bd.ids.y]) * bd.K.y +
+                     xyz(d.posLin[bd.ids.z]) * bd.K.z + xyz(d.posLin[bd.ids.w]) * bd.K.w;
+    float k;
+    if (self == bd.ids.x) k = bd.K.x;
+    else if (self == bd.ids.y) k = bd.K.y;
+    else if (self == bd.ids.z) k = bd.K.z;
+    else k = bd.K.w;
+    acc.rhsLin += m * (sc * k);
+    acc.lhsLin = m3_add(acc.lhsLin, m3_diag(s3(sc * k * k)));
+}
+
+// Element-contact constraint over the 4-slot stencil (40_solver.metal:1236-1263).
+__device__ float3 soft_c(const Params& P, const DevPtrs& d, const SoftContactGPU& sc, float3& n, float3& t1,
+                         float3& t2, float3& rAW, bool& rigidA) {
+    const uint32_t flags = __float_as_uint(sc.anchorA.w);
+    rigidA = (flags & SCF_RIGID_A) != 0;
+    const bool roundA = (flags & SCF_ROUND_A) != 0;
+    n = xyz(sc.normal);
+    orthonormal(n, t1, t2);
+    rAW = s3(0);
+    float3 C = xyz(sc.C0) * (1.0f - P.alpha);
+    const uint32_t ids[4] = {sc.ids.x, sc.ids.y, sc.ids.z, sc.ids.w};
+    const float ws[4] = {sc.weights.x, sc.weights.y, sc.weights.z, sc.weights.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const uint32_t b = ids[k];
+        if (b == WORLD_BODY) continue;
+        const float w = ws[k];
+        const float3 dq = xyz(d.posLin[b]) - xyz(d.initLin[b]);
+        C += mk3(dot(n, dq), dot(t1, dq), dot(t2, dq)) * w;
+        if (k == 0 && rigidA) {
+            const float4 q = d.posAng[b];
+            rAW = roundA ? xyz(sc.anchorA) : q_rotate(q, xyz(sc.anchorA));
+            const float3 dqa = q_sub(q, d.initAng[b]);
+            C += mk3(dot(cross(rAW, n), dqa), dot(cross(rAW, t1), dqa), dot(cross(rAW, t2), dqa)) * w;
+        }
+    }
+    return C;
+}
+
+// softContactForce with the two-stage barrier and stampSoft (40_solver.metal:1265-1359).
+__device__ void stamp_soft(const Params& P, const DevPtrs& d, const SoftContactGPU& sc, uint32_t self, Accum& acc) {
+    float3 n, t1, t2, rAW;
+    bool rigidA;
+    const float3 C = soft_c(P, d, sc, n, t1, t2, rAW, rigidA);
+    float3 F = xyz(sc.penalty) * C + xyz(sc.lambda);
+    float kN = sc.penalty.x;
+    const float rT = sc.anchorA.x;
+    const uint32_t kindB = (__float_as_uint(sc.anchorA.w) >> SCF_KIND_SHIFT) & 3u;
+    if (rT > 0.0f && kindB != SC_RT && C.x < -0.5f * rT) {
+        const float dsep = mx(C.x + rT, 0.02f * rT);
+        const float kp = 0.25f * rT * rT * sc.penalty.x;
+        F.x = -kp / dsep + sc.lambda.x;
+        kN = kp / (dsep * dsep);
+    }
+    F.x = mn(F.x, 0.0f);
+    const float bounds = fabsf(F.x) * sc.normal.w;
+    const float fs = sqrtf(F.y * F.y + F.z * F.z);
+    if (fs > bounds && fs > 0.0f) {
+        const float r = bounds / fs;
+        F.y *= r;
+        F.z *= r;
+    }
+    int slot = -1;
+    if (sc.ids.x == self) slot = 0;
+    else if (sc.ids.y == self) slot = 1;
+    else if (sc.ids.z == self) slot = 2;
+    else if (sc.ids.w == self) slot = 3;
+    if (slot < 0) return;
+    const float w = slot == 0 ? sc.weights.x : (slot == 1 ? sc.weights.y : (slot == 2 ? sc.weights.z : sc.weights.w));
+    if (slot == 0 && rigidA) {
+        const M3 jLin = M3{n * w, t1 * w, t2 * w};
+        const M3 jAng = M3{cross(rAW, jLin.r0), cross(rAW, jLin.r1), cross(rAW, jLin.r2)};
+        const M3 K = m3_diag(mk3(kN, sc.penalty.y, sc.penalty.z));
+        const M3 jLinT = m3_transpose(jLin), jAngT = m3_transpose(jAng);
+        const M3 jAngTk = m3_mulm(jAngT, K);
+        acc.lhsLin = m3_add(acc.lhsLin, m3_mulm(m3_mulm(jLinT, K), jLin));
+        acc.lhsAng = m3_add(acc.lhsAng, m3_mulm(jAngTk, jAng));
+        acc.lhsCross = m3_add(acc.lhsCross, m3_mulm(jAngTk, jLin));
+        acc.rhsLin += m3_mul(jLinT, F);
+        acc.rhsAng += m3_mul(jAngT, F);
+    } else {
+        const float w2 = w * w;
+        acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(n, n), kN * w2));
+        acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(t1, t1), sc.penalty.y * w2));
+        acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(t2, t2), sc.penalty.z * w2));
+        acc.rhsLin += (n * F.x + t1 * F.y + t2 * F.z) * w;
+    }
+}
+
 __device__ __forceinline__ void stamp_entry(const Params& P, const DevPtrs& d, uint32_t entry, uint32_t body,
                                             Accum& acc) {
     const uint32_t kind = entry >> ADJ_KIND_SHIFT, idx = entry & ADJ_INDEX_MASK;
@@ -612,12 +748,23 @@ __device__ __forceinline__ void stamp_entry(const Params& P, const DevPtrs& d, u
     else if (kind == FK_MANIFOLD) stamp_manifold(P, d, d.manifolds[idx], body, acc);
     else if (kind == FK_JOINT) stamp_joint(P, d, d.joints[idx], body, acc);
     else if (kind == FK_SPRING) stamp_spring(P, d, d.springs[idx], body, acc);
+    else if (kind == FK_SOFT) stamp_soft(P, d, d.soft[idx], body, acc);
+    else if (kind == FK_MEMBRANE) stamp_membrane(d, d.membranes[idx], body, acc);
+    else if (kind == FK_BEND) stamp_bend(d, d.bends[idx], body, acc);
 }
 
 __device__ __forceinline__ float3 shfl3(unsigned mask, float3 v, int o) {
     return mk3(__shfl_xor_sync(mask, v.x, o, 8), __shfl_xor_sync(mask, v.y, o, 8), __shfl_xor_sync(mask, v.z, o, 8));
 }
 __device__ __forceinline__ void add_shfl3(unsigned mask, float3& v, int o) { v = v + shfl3(mask, v, o); }
+
+// A skipped update (non-finite step) still publishes the unchanged pose
+// when the color commits through posNext.
+__device__ __forceinline__ void keep_body(const Params& P, const DevPtrs& d, uint32_t body, float4 pl, bool rigid) {
+    if (!P.colorJacobi) return;
+    d.posNext[body] = pl;
+    if (rigid) d.angNext[body] = d.posAng[body];
+}
 
 // One body on an 8-lane group; lane 0 writes the result.
 __device__ void primal_body(const Params& P, const DevPtrs& d, uint32_t body, uint32_t lane, unsigned mask) {
@@ -656,19 +803,24 @@ __device__ void primal_body(const Params& P, const DevPtrs& d, uint32_t body, ui
         acc.lhsAng = m3_add(acc.lhsAng, inertia);
         acc.rhsAng += m3_mul(inertia, q_sub(q, d.inertAng[body]));
         solve6x6(acc.lhsLin, acc.lhsAng, acc.lhsCross, -acc.rhsLin, -acc.rhsAng, dxLin, dxAng);
-        if (!finite3(dxLin) || !finite3(dxAng)) return;
+        if (!finite3(dxLin) || !finite3(dxAng)) { keep_body(P, d, body, pl, rigid); return; }
         const float ang2 = dot(dxAng, dxAng);
         const float maxAng = 0.5f;
         if (ang2 > maxAng * maxAng) dxAng *= maxAng * rsq(ang2);
     } else {
         solve6x6(acc.lhsLin, m3_identity(), m3_zero(), -acc.rhsLin, s3(0), dxLin, dxAng);
-        if (!finite3(dxLin)) return;
+        if (!finite3(dxLin)) { keep_body(P, d, body, pl, rigid); return; }
     }
     const float maxLin = 0.35f * fabsf(shp.w);
     const float lin2 = dot(dxLin, dxLin);
     if (lin2 > maxLin * maxLin) dxLin *= maxLin * rsq(lin2);
     // Isotropic OGC truncation needs an emitted conservative bound; with no
     // element contacts every bound is "far" and the step is unchanged.
+    if (P.colorJacobi) {
+        d.posNext[body] = mk4(xyz(pl) + dxLin, mass);
+        if (rigid) d.angNext[body] = q_addw(d.posAng[body], dxAng);
+        return;
+    }
     d.posLin[body] = mk4(xyz(pl) + dxLin, mass);
     if (rigid) d.posAng[body] = q_addw(d.posAng[body], dxAng);
 }
@@ -907,10 +1059,11 @@ __global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevP
     acc.lhs = m3_add(acc.lhs, m3_diag(s3(mass / dt2)));
     acc.rhs += (xyz(pl) - xyz(inert)) * (mass / dt2);
     float3 dxLin = solve3x3_particle(acc.lhs, -acc.rhs);
-    if (!finite3(dxLin)) return;
+    if (!finite3(dxLin)) { keep_body(P, d, body, pl, false); return; }
     const float maxLin = 0.35f * fabsf(shp.w);
     const float lin2 = dot(dxLin, dxLin);
     if (lin2 > maxLin * maxLin) dxLin *= maxLin * rsq(lin2);
+    if (P.colorJacobi) { d.posNext[body] = mk4(xyz(pl) + dxLin, mass); return; }
     d.posLin[body] = mk4(xyz(pl) + dxLin, mass);
 }
 
@@ -1045,25 +1198,54 @@ __device__ void dual_manifold(const Params& P, const DevPtrs& d, uint32_t gid) {
     }
 }
 
+// dual_soft_one (40_solver.metal:1689-1727): quadratic stage only.
+__device__ void dual_soft(const Params& P, const DevPtrs& d, uint32_t i) {
+    SoftContactGPU& sc = d.soft[i];
+    float3 n, t1, t2, rAW;
+    bool rigidA;
+    const float3 C = soft_c(P, d, sc, n, t1, t2, rAW, rigidA);
+    float3 F = xyz(sc.penalty) * C + xyz(sc.lambda);
+    F.x = mn(F.x, 0.0f);
+    const float bnd = fabsf(F.x) * sc.normal.w;
+    const float fs = sqrtf(F.y * F.y + F.z * F.z);
+    if (fs > bnd && fs > 0.0f) {
+        const float r = bnd / fs;
+        F.y *= r;
+        F.z *= r;
+    }
+    F.x = mx(F.x, -sc.C0.w);
+    sc.lambda = tof4(F, sc.lambda.w);
+    float3 pen = xyz(sc.penalty);
+    if (F.x < 0.0f) pen.x = mn(pen.x + P.betaLin * fabsf(C.x), PENALTY_MAX_T);
+    if (fs <= bnd) {
+        pen.y = mn(pen.y + P.betaLin * fabsf(C.y), PENALTY_MAX_T);
+        pen.z = mn(pen.z + P.betaLin * fabsf(C.z), PENALTY_MAX_T);
+    }
+    sc.penalty = tof4(pen, sc.penalty.w);
+}
+
 __device__ __forceinline__ void dual_item(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t g,
                                           uint32_t numPairs) {
     if (g < z.numActiveJoints) { dual_joint(P, d, d.activeJoints[g]); return; }
     g -= z.numActiveJoints;
     if (g < z.numHardSprings) { dual_spring(P, d, d.hardSprings[g]); return; }
     g -= z.numHardSprings;
-    if (g < numPairs) dual_manifold(P, d, g);
+    if (g < numPairs) { dual_manifold(P, d, g); return; }
+    dual_soft(P, d, g - numPairs);
 }
 
 __global__ void k_dual(const Params P, const DevPtrs d, const Sizes z) {
     pdl_prologue();
-    const uint32_t total = z.numActiveJoints + z.numHardSprings + d.counters->numPairs;
     const uint32_t numPairs = d.counters->numPairs;
+    const uint32_t numSoft = P.cloth ? d.counters->numSoft : 0u;
+    const uint32_t total = z.numActiveJoints + z.numHardSprings + numPairs + numSoft;
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x)
         dual_item(P, d, z, g, numPairs);
 }
 
 void launch_dual(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
-    launch_pdl(k_dual, stride_blocks(z.numActiveJoints + z.numHardSprings + z.maxPairs, 128), 128, st, P, d, z);
+    const uint32_t upper = z.numActiveJoints + z.numHardSprings + z.maxPairs + (P.cloth ? z.maxSoft : 0u);
+    launch_pdl(k_dual, stride_blocks(upper, 128), 128, st, P, d, z);
 }
 
 // ---------------------------------------------------------------------------
@@ -1234,8 +1416,13 @@ __global__ void k_frame_end(const Params P, const DevPtrs d, const Sizes z, floa
         const uint32_t frame = d.frameCounter[0] + 1u;
         d.frameCounter[0] = frame;
         uint32_t kind = 0, detail = 0;
-        if (d.counters->pairCandidates > P.maxPairs) { kind = AVBD_FAIL_RIGID_PAIR_CAPACITY_; detail = d.counters->pairCandidates; }
-        else if (z.dynamicColoring && d.counters->colorConflicts > 0) { kind = AVBD_FAIL_UNRESOLVED_COLORING_; detail = d.counters->colorConflicts; }
+        const Counters* c = d.counters;
+        if (c->pairCandidates > P.maxPairs) { kind = AVBD_FAIL_RIGID_PAIR_CAPACITY_; detail = c->pairCandidates; }
+        else if (P.cloth && c->softRaw > P.maxSoft) { kind = 3; detail = c->softRaw; }
+        else if (P.cloth && c->datPairsPeak > P.maxDatPairs) { kind = 6; detail = c->datPairsPeak; }
+        else if (P.cloth && c->datGridOverflow > 0) { kind = 7; detail = c->datGridOverflow; }
+        else if (P.cloth && c->datInvalidAnchor > 0) { kind = 8; detail = c->datInvalidAnchor; }
+        else if (z.dynamicColoring && c->colorConflicts > 0) { kind = AVBD_FAIL_UNRESOLVED_COLORING_; detail = c->colorConflicts; }
         if (kind != 0 && d.failureLatch[0] == 0u) {
             d.failureLatch[0] = kind;
             d.failureLatch[1] = frame;

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <map>
 #include <set>
+#include <unordered_set>
 
 namespace avbd {
 namespace {
@@ -90,6 +91,201 @@ std::vector<std::array<int, 3>> boundary_faces(const avbd_scene_desc* s) {
     return out;
 }
 
+inline float dist(V3 a, V3 b) { return length(sub(a, b)); }
+inline V3 unit(V3 a) { return mul(a, 1.0f / std::sqrt(dot(a, a))); }
+inline uint64_t edge_key(int a, int b) { return (uint64_t)std::min(a, b) << 32 | (uint64_t)std::max(a, b); }
+
+// Cloth topology, membranes, bends and element-contact parameters
+// (GPUSolver.swift:1289-1680).  Bends are numbered by ascending edge key.
+void upload_cloth(const avbd_scene_desc* s, const std::vector<std::array<int, 3>>& boundary, HostScene& H) {
+    const uint32_t nb = s->num_bodies;
+    const uint32_t authored = s->num_tris;
+    std::vector<std::array<int, 3>> coll;
+    coll.reserve(authored + boundary.size());
+    for (uint32_t i = 0; i < authored; i++) coll.push_back({s->tris[i].ids[0], s->tris[i].ids[1], s->tris[i].ids[2]});
+    coll.insert(coll.end(), boundary.begin(), boundary.end());
+    H.numTris = (uint32_t)coll.size();
+    auto P = [&](int i) { return from(s->bodies[i].position); };
+    auto SX = [&](int i) { return s->bodies[i].size[0]; };
+
+    std::unordered_set<uint64_t> topoSeen, contactSeen;
+    std::vector<uint64_t> topo, contact;
+    float maxElemR = 0.0f, maxCollR = 0.0f;
+    H.tris.resize(H.numTris);
+    for (uint32_t i = 0; i < H.numTris; i++) {
+        const int a = coll[i][0], b = coll[i][1], c = coll[i][2];
+        H.tris[i] = u4{(uint32_t)a, (uint32_t)b, (uint32_t)c, 0u};
+        const int ends[3][2] = {{a, b}, {b, c}, {a, c}};
+        for (const auto& e : ends) {
+            const uint64_t key = edge_key(e[0], e[1]);
+            if (topoSeen.insert(key).second) topo.push_back(key);
+            if (i < authored && contactSeen.insert(key).second) contact.push_back(key);
+        }
+        const V3 pa = P(a), pb = P(b), pc = P(c);
+        const V3 m = divs(add(add(pa, pb), pc), 3.0f);
+        const float thick = fmax_(SX(a), fmax_(SX(b), SX(c))) / 2.0f;
+        maxCollR = fmax_(maxCollR, thick);
+        maxElemR = fmax_(maxElemR, fmax_(dist(m, pa), fmax_(dist(m, pb), dist(m, pc))) + thick);
+    }
+    H.numSurfaceEdges = (uint32_t)contact.size();
+    for (uint64_t key : topo)
+        if (contactSeen.insert(key).second) contact.push_back(key);
+    H.numEdges = (uint32_t)contact.size();
+    std::vector<std::vector<uint32_t>> ring(nb);
+    for (uint64_t key : topo) {
+        const uint32_t a = (uint32_t)(key >> 32), b = (uint32_t)key;
+        ring[a].push_back(b);
+        ring[b].push_back(a);
+    }
+    H.edges.clear();
+    H.edges.reserve(2 * contact.size());
+    for (uint64_t key : contact) {
+        const int a = (int)(key >> 32), b = (int)(uint32_t)key;
+        H.edges.push_back((uint32_t)a);
+        H.edges.push_back((uint32_t)b);
+        maxElemR = fmax_(maxElemR, dist(P(a), P(b)) / 2.0f + fmax_(SX(a), SX(b)) / 2.0f);
+    }
+    H.nbrStart.assign(nb, 0);
+    H.nbrCount.assign(nb, 0);
+    H.nbrList.clear();
+    for (uint32_t i = 0; i < nb; i++) {
+        std::sort(ring[i].begin(), ring[i].end());
+        H.nbrStart[i] = (uint32_t)H.nbrList.size();
+        H.nbrCount[i] = (uint32_t)ring[i].size();
+        H.nbrList.insert(H.nbrList.end(), ring[i].begin(), ring[i].end());
+    }
+
+    // connected surface components and self-collision flags
+    H.selfCollision.assign(nb, 0);
+    std::vector<uint8_t> onSurface(nb, 0);
+    std::vector<int> parent(nb, -1);
+    auto root = [&](int x) {
+        int r = x;
+        while (parent[r] >= 0 && parent[r] != r) r = parent[r];
+        int c = x;
+        while (parent[c] >= 0 && parent[c] != r) { const int n = parent[c]; parent[c] = r; c = n; }
+        if (parent[r] < 0) parent[r] = r;
+        return r;
+    };
+    for (const auto& f : coll) { const int r = root(f[0]); parent[root(f[1])] = r; parent[root(f[2])] = r; }
+    std::set<int> selfRoots;
+    for (uint32_t i = 0; i < authored; i++) selfRoots.insert(root(s->tris[i].ids[0]));
+    for (uint32_t i = 0; i < s->num_tets; i++)
+        if (s->tets[i].self_collision)
+            for (int k = 0; k < 4; k++)
+                if (parent[s->tets[i].ids[k]] >= 0) selfRoots.insert(root(s->tets[i].ids[k]));
+    std::map<int, uint32_t> groupOf;
+    for (const auto& f : coll) {
+        const int r = root(f[0]);
+        auto it = groupOf.find(r);
+        const uint32_t g = it == groupOf.end() ? groupOf.emplace(r, (uint32_t)groupOf.size() + 1).first->second
+                                               : it->second;
+        const uint32_t self = selfRoots.count(r) ? 1u : 0u;
+        for (int k = 0; k < 3; k++)
+            if (s->bodies[f[k]].is_particle) { H.clothGroup[f[k]] = g; H.selfCollision[f[k]] = self; onSurface[f[k]] = 1; }
+    }
+    H.particleIdx.clear();
+    for (uint32_t i = 0; i < nb; i++) if (onSurface[i]) H.particleIdx.push_back(i);
+    H.numParticles = H.numTris == 0 ? 0u : (uint32_t)H.particleIdx.size();
+
+    // StVK membranes and Bergou hinges over interior edges
+    struct Flap { int opp; float k; };
+    std::map<uint64_t, std::vector<Flap>> hinge;
+    H.membranes.clear();
+    for (uint32_t ti = 0; ti < authored; ti++) {
+        const avbd_tri_desc& t = s->tris[ti];
+        if (!(t.mu > 0.0f)) continue;
+        const int i0 = t.ids[0], i1 = t.ids[1], i2 = t.ids[2];
+        const V3 x0 = P(i0), d1 = sub(P(i1), x0), d2 = sub(P(i2), x0);
+        const V3 nrm = cross(d1, d2);
+        const float area = length(nrm) / 2.0f;
+        if (!(area > 1e-10f)) continue;
+        const V3 e1 = unit(d1);
+        const V3 e2 = unit(cross(unit(nrm), e1));
+        const float a = dot(d1, e1), b = dot(d1, e2), c = dot(d2, e1), dd = dot(d2, e2);
+        const float det = a * dd - b * c;
+        if (!(std::fabs(det) > 1e-12f)) continue;
+        MembraneGPU m{};
+        m.ids = u4{(uint32_t)i0, (uint32_t)i1, (uint32_t)i2, 0u};
+        m.dm = f4{dd / det, -b / det, -c / det, a / det};
+        m.mat = f4{t.mu * area, t.lambda * area, area, 0.0f};
+        H.membranes.push_back(m);
+        if (t.bend > 0.0f) {
+            hinge[edge_key(i0, i1)].push_back(Flap{i2, t.bend});
+            hinge[edge_key(i1, i2)].push_back(Flap{i0, t.bend});
+            hinge[edge_key(i0, i2)].push_back(Flap{i1, t.bend});
+        }
+    }
+    H.bends.clear();
+    for (const auto& kv : hinge) {
+        if (kv.second.size() != 2) continue;
+        const int v0 = (int)(kv.first >> 32), v1 = (int)(uint32_t)kv.first;
+        const V3 p0 = P(v0), p1 = P(v1);
+        const float L = dist(p0, p1);
+        if (!(L > 1e-9f)) continue;
+        // unfold both flaps into the hinge plane from rest edge lengths
+        float qx[4] = {0.0f, L, 0.0f, 0.0f}, qy[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        bool ok = true;
+        for (int f = 0; f < 2 && ok; f++) {
+            const V3 po = P(kv.second[f].opp);
+            const float l0 = dist(po, p0), l1 = dist(po, p1);
+            const float ax = (L * L + l0 * l0 - l1 * l1) / (2.0f * L);
+            const float h2 = l0 * l0 - ax * ax;
+            if (!(h2 > 1e-12f)) { ok = false; break; }
+            qx[2 + f] = ax;
+            qy[2 + f] = (f == 0 ? 1.0f : -1.0f) * std::sqrt(h2);
+        }
+        if (!ok) continue;
+        // K spans the null space of {1, x, y} over the four stencil points
+        auto minor3 = [&](int c0, int c1, int c2) {
+            const V3 a = v3(1.0f, qx[c0], qy[c0]), b = v3(1.0f, qx[c1], qy[c1]), c = v3(1.0f, qx[c2], qy[c2]);
+            return dot(a, cross(b, c));
+        };
+        f4 K{minor3(1, 2, 3), -minor3(0, 2, 3), minor3(0, 1, 3), -minor3(0, 1, 2)};
+        auto cot = [&](int apex, int i, int j) {
+            const float ux = qx[i] - qx[apex], uy = qy[i] - qy[apex];
+            const float vx = qx[j] - qx[apex], vy = qy[j] - qy[apex];
+            const float cr = ux * vy - uy * vx;
+            return std::fabs(cr) > 1e-12f ? (ux * vx + uy * vy) / std::fabs(cr) : 0.0f;
+        };
+        const float want = cot(0, 1, 2) + cot(1, 0, 2);
+        if (!(std::fabs(K.z) > 1e-12f)) continue;
+        const float sc = want / K.z;
+        K = f4{K.x * sc, K.y * sc, K.z * sc, K.w * sc};
+        const float a1 = std::fabs((qx[1] - qx[0]) * qy[2]) / 2.0f;
+        const float a2 = std::fabs((qx[1] - qx[0]) * qy[3]) / 2.0f;
+        BendGPU bd{};
+        bd.ids = u4{(uint32_t)v0, (uint32_t)v1, (uint32_t)kv.second[0].opp, (uint32_t)kv.second[1].opp};
+        bd.K = K;
+        bd.mat = f4{3.0f * (kv.second[0].k + kv.second[1].k) / 2.0f / fmax_(a1 + a2, 1e-9f), 0.0f, 0.0f, 0.0f};
+        H.bends.push_back(bd);
+    }
+
+    // element-contact radii and cells
+    float maxPartR = maxCollR, edgeSum = 0.0f;
+    for (uint64_t key : topo) {
+        const int a = (int)(key >> 32), b = (int)(uint32_t)key;
+        maxPartR = fmax_(maxPartR, fmax_(SX(a), SX(b)) / 2.0f);
+        edgeSum += dist(P(a), P(b));
+    }
+    const float meanEdge = topo.empty() ? 0.2f : edgeSum / (float)topo.size();
+    H.elemMargin = fmin_(0.01f, fmax_(0.002f, 0.5f * maxPartR));
+    const float forceReach = 2.0f * maxPartR + H.elemMargin;
+    H.queryRadius = fmax_(1.5f * forceReach, 0.75f * meanEdge);
+    const float reach = (2.0f * maxPartR + H.elemMargin) / 0.7f;
+    H.surfaceCellSize = fmax_(0.02f, fmax_(fmax_(reach, meanEdge * 1.05f), maxElemR + maxPartR + H.elemMargin));
+    H.elemCellSize = fmax_(0.02f, fmax_(fmax_(reach, meanEdge * 1.05f), 2.0f * maxElemR + H.queryRadius));
+
+    // capacities (GPUSolver.swift:395-443)
+    const uint64_t surf = H.particleIdx.size();
+    const uint64_t pairsCap = std::max<uint64_t>(1, 64ull * surf + 128ull * topo.size());
+    const uint64_t budget = std::min<uint64_t>(pairsCap, 8ull * surf + 8ull * topo.size());
+    H.maxDatPairs = (uint32_t)std::min<uint64_t>(pairsCap, 0xFFFFFFFFull);
+    H.maxSoft = (uint32_t)std::max<uint64_t>(1, 4ull * H.numTris + budget);
+    H.softMapCapacity = next_pow2(std::max<uint32_t>(64u, 2u * H.maxSoft));
+    H.elemHashSize = next_pow2(std::max<uint32_t>(64u, 2u * 4u * H.numTris));
+}
+
 }  // namespace
 
 int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
@@ -105,7 +301,17 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
             return AVBD_ERR_UNSUPPORTED;
         }
     }
-    if (s->num_tris > 0) { err = "cloth triangles are not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+    if (s->num_tris > 0 && s->num_tets > 0) {
+        err = "scenes mixing cloth triangles and tets are not supported by this build";
+        return AVBD_ERR_UNSUPPORTED;
+    }
+    if (s->num_tris > 0 && s->truncation_selection == AVBD_TRUNCATION_ISOTROPIC) {
+        err = "isotropic OGC truncation of cloth is not supported by this build (Planar-DAT is)";
+        return AVBD_ERR_UNSUPPORTED;
+    }
+    for (uint32_t i = 0; i < s->num_tris; i++)
+        for (int k = 0; k < 3; k++)
+            if (s->tris[i].ids[k] < 0 || (uint32_t)s->tris[i].ids[k] >= nb) { err = "triangle vertex out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
     for (uint32_t i = 0; i < s->num_joints; i++) {
         const avbd_joint_desc& j = s->joints[i];
         if (j.body_b < 0 || (uint32_t)j.body_b >= nb || j.body_a >= (int32_t)nb || j.body_a < -1) { err = "joint body out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
@@ -128,7 +334,7 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
     H.mapCapacity = next_pow2(2 * H.maxPairs);
     H.gridHashSize = next_pow2(std::max<uint32_t>(64u, 2u * std::max<uint32_t>(1u, enabled)));
     std::vector<std::array<int, 3>> boundary = boundary_faces(s);
-    H.numTris = (uint32_t)boundary.size();
+    H.numTris = (uint32_t)boundary.size() + s->num_tris;
 
     // ---- bodies (GPUSolver.swift:915-969)
     H.posLin.assign(nb, f4{}); H.posAng.assign(nb, f4{}); H.velLin.assign(nb, f4{});
@@ -330,8 +536,12 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
     ex.erase(std::unique(ex.begin(), ex.end()), ex.end());
     for (uint64_t k : ex) { H.exclusions.push_back((uint32_t)(k >> 32)); H.exclusions.push_back((uint32_t)k); }
 
+    // ---- cloth topology and elements (GPUSolver.swift:1289-1680)
+    H.cloth = s->num_tris > 0;
+    if (H.cloth) upload_cloth(s, boundary, H);
+
     // ---- collision-surface groups of tet boundaries (GPUSolver.swift:1461-1535)
-    if (!boundary.empty()) {
+    if (!H.cloth && !boundary.empty()) {
         std::vector<int> parent(nb, -1);
         auto find = [&](int x) {
             int r = x;
@@ -430,11 +640,21 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
         for (uint32_t v : {H.tets[t].ids.x, H.tets[t].ids.y, H.tets[t].ids.z, H.tets[t].ids.w})
             if (dyn(v)) post[v].push_back(e);
     }
+    for (uint32_t m = 0; m < H.membranes.size(); m++) {
+        const uint32_t e = (FK_MEMBRANE << ADJ_KIND_SHIFT) | m;
+        for (uint32_t v : {H.membranes[m].ids.x, H.membranes[m].ids.y, H.membranes[m].ids.z})
+            if (dyn(v)) post[v].push_back(e);
+    }
+    for (uint32_t b = 0; b < H.bends.size(); b++) {
+        const uint32_t e = (FK_BEND << ADJ_KIND_SHIFT) | b;
+        for (uint32_t v : {H.bends[b].ids.x, H.bends[b].ids.y, H.bends[b].ids.z, H.bends[b].ids.w})
+            if (dyn(v)) post[v].push_back(e);
+    }
     // The warp-per-particle primal may drop its generic stamp path when no
     // dynamic body is rigid and no particle carries a joint or spring entry
     // (sphere contacts always have exactly one contact point).
-    H.particleFastPath = true;
-    for (uint32_t b = 0; b < nb; b++) {
+    H.particleFastPath = !H.cloth;
+    for (uint32_t b = 0; b < nb && H.particleFastPath; b++) {
         if (!(H.posLin[b].w > 0.0f)) continue;
         if (H.shape[b].w >= 0.0f || !pre[b].empty()) { H.particleFastPath = false; break; }
     }
@@ -482,10 +702,30 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
     P.numTris = H.numTris;
     P.numParticles = H.numTris == 0 ? 0 : H.numParticles;
     P.maxSpeed = fmax_(30.0f, 1.5f * P.cellSize / dt * 0.5f);
+    // effectiveSurfaceTruncationMode (GPUSolver.swift:93-101)
     P.surfaceTruncationMode = 0;
-    if (P.numParticles > 0)
-        P.surfaceTruncationMode = s->truncation_selection == AVBD_TRUNCATION_AUTOMATIC ? 1u : s->truncation_selection;
-    if (P.surfaceTruncationMode == 2u) { err = "Planar-DAT truncation is not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+    if (P.numParticles > 0) {
+        bool volumetricSelf = false;
+        for (uint32_t i = 0; i < s->num_tets; i++) volumetricSelf = volumetricSelf || s->tets[i].self_collision;
+        const uint32_t automatic = (volumetricSelf || (s->num_tris > 0 && s->num_tets == 0)) ? 2u : 1u;
+        P.surfaceTruncationMode = s->truncation_selection == AVBD_TRUNCATION_AUTOMATIC ? automatic : s->truncation_selection;
+    }
+    if (P.surfaceTruncationMode == 2u && !H.cloth) { err = "Planar-DAT truncation of tet surfaces is not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+    P.cloth = (H.cloth && P.surfaceTruncationMode == 2u) ? 1u : 0u;
+    P.colorJacobi = P.cloth;
+    P.numEdges = H.numEdges;
+    P.numSurfaceEdges = H.numSurfaceEdges;
+    P.elemHashSize = H.elemHashSize;
+    P.maxDatPairs = H.maxDatPairs;
+    P.maxSoft = H.maxSoft;
+    P.softMapCapacity = H.softMapCapacity;
+    P.numMembranes = (uint32_t)H.membranes.size();
+    P.numBends = (uint32_t)H.bends.size();
+    P.elemMargin = H.elemMargin;
+    P.queryRadius = H.queryRadius;
+    P.elemCellSize = H.elemCellSize;
+    P.surfaceCellSize = H.surfaceCellSize;
+    P.clothViscosity = s->settings.cloth_viscosity;
     P.tetInversionPreventionEnabled = 0;
     P.planarDATRelaxation = 0.85f;
     P.numExclusions = (uint32_t)(H.exclusions.size() / 2);

@@ -53,6 +53,20 @@ struct HostScene {
     // which is exactly the ascending (kind << 28 | index) order.
     std::vector<uint32_t> preList, postList;
     std::vector<u4> staticSeg;            // preStart, preCount, postStart, postCount
+
+    // cloth (authored triangles): element topology and elements.  In cloth
+    // scenes the post segment holds membranes and bends (kinds 5, 6) and the
+    // per-frame segment manifolds and element contacts (kinds 2, 4), which
+    // keeps the walk in ascending order.
+    bool cloth = false;
+    uint32_t numEdges = 0, numSurfaceEdges = 0, elemHashSize = 64;
+    uint32_t maxDatPairs = 1, maxSoft = 1, softMapCapacity = 64;
+    float elemMargin = 0.0f, queryRadius = 0.0f, elemCellSize = 1.0f, surfaceCellSize = 1.0f;
+    std::vector<u4> tris;
+    std::vector<uint32_t> edges;          // (a, b) per edge
+    std::vector<uint32_t> nbrStart, nbrCount, nbrList, particleIdx, selfCollision;
+    std::vector<MembraneGPU> membranes;
+    std::vector<BendGPU> bends;
 };
 
 // Returns an AVBD_* status; on failure `err` holds a message.

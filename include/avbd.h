@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define AVBD_ABI_VERSION 1u
+#define AVBD_ABI_VERSION 2u
 
 /* ------------------------------------------------------------------------ */
 /* Status codes.  Construction errors mirror `AVBDError`                     */
@@ -48,9 +48,10 @@ enum {
     AVBD_FAIL_SOFT_CONTACT_CAPACITY = 3,
     AVBD_FAIL_STATIC_COLOR_CAPACITY = 4,
     AVBD_FAIL_UNRESOLVED_COLORING = 5,
-    AVBD_FAIL_PLANAR_DAT_PAIR_CAPACITY = 6,
-    AVBD_FAIL_PLANAR_DAT_SOFT_CAPACITY = 7,
-    AVBD_FAIL_PLANAR_DAT_INVALID = 8,
+    /* Planar-DAT codes 1-3 (GPUSolver.swift:676-751) */
+    AVBD_FAIL_PLANAR_DAT_PAIR_CAPACITY = 6,  /* V-T/E-E pair demand > capacity */
+    AVBD_FAIL_PLANAR_DAT_GRID_SPAN = 7,      /* element AABB > 4 cells/axis   */
+    AVBD_FAIL_PLANAR_DAT_INVALID_ANCHOR = 8, /* coincident/non-finite anchor  */
     AVBD_FAIL_WAIT_TIMEOUT = 9         /* bounded device wait gave up        */
 };
 
@@ -230,6 +231,18 @@ typedef struct avbd_counters {
     uint32_t color_conflicts;
     uint32_t ogc_exceeded;
     uint32_t color_counts[64];
+    /* Planar-DAT statistics of the last retired frame (lastPlanarDAT*,
+     * GPUSolver.swift:318-325)                                             */
+    uint32_t dat_pairs;
+    uint32_t dat_vt_pairs;
+    uint32_t dat_ee_pairs;
+    uint32_t dat_grid_overflows;
+    uint32_t dat_invalid_anchors;
+    uint32_t dat_truncations;
+    uint32_t dat_vt_degenerate;
+    uint32_t dat_ee_degenerate;
+    uint32_t dat_nonfinite;
+    uint32_t dat_tet_degenerate;
 } avbd_counters;
 
 typedef struct avbd_solver avbd_solver;
@@ -319,7 +332,9 @@ enum {
     AVBD_STAGE_BROADPHASE = 0, AVBD_STAGE_NARROWPHASE = 1, AVBD_STAGE_PERSISTENCE_MAP = 2,
     AVBD_STAGE_WARMSTART = 3, AVBD_STAGE_ADJACENCY = 4, AVBD_STAGE_COLORING = 5,
     AVBD_STAGE_PRIMAL = 6, AVBD_STAGE_DUAL = 7, AVBD_STAGE_FINALIZE = 8,
-    AVBD_STAGE_COUNT_ = 9
+    AVBD_STAGE_ELEMENT_CONTACTS = 9,  /* element grid, pair streams, emission */
+    AVBD_STAGE_TRUNCATION = 10,       /* per-color Planar-DAT passes          */
+    AVBD_STAGE_COUNT_ = 11
 };
 typedef struct avbd_profile {
     uint64_t frames;
@@ -344,7 +359,12 @@ enum {
     AVBD_BUF_MAP_VAL = 17, AVBD_BUF_JOINTS = 18, AVBD_BUF_SPRINGS = 19,
     AVBD_BUF_TETS = 20, AVBD_BUF_INIT_LIN = 21, AVBD_BUF_INERT_LIN = 22,
     AVBD_BUF_EXCLUSIONS = 23, AVBD_BUF_HASHED_IDX = 24, AVBD_BUF_GLOBAL_IDX = 25,
-    AVBD_BUF_COUNT_ = 26
+    /* cloth: element topology, element contacts, Planar-DAT pair stream */
+    AVBD_BUF_TRIS = 26, AVBD_BUF_EDGES = 27, AVBD_BUF_NBR_START = 28,
+    AVBD_BUF_NBR_COUNT = 29, AVBD_BUF_NBR_LIST = 30, AVBD_BUF_PARTICLE_IDX = 31,
+    AVBD_BUF_MEMBRANES = 32, AVBD_BUF_BENDS = 33, AVBD_BUF_SOFT = 34,
+    AVBD_BUF_DAT_PAIRS = 35, AVBD_BUF_CLOTH_GROUP = 36, AVBD_BUF_OGC_PREV = 37,
+    AVBD_BUF_COUNT_ = 38
 };
 size_t avbd_debug_buffer_size(avbd_solver* solver, int which);
 int avbd_debug_read(avbd_solver* solver, int which, void* dst, size_t bytes);

@@ -13,7 +13,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "build", "liboracle.so")
-SRC = [os.path.join(HERE, "avbd_oracle.cpp"), os.path.join(HERE, "oracle_math.h"),
+SRC = [os.path.join(HERE, "avbd_oracle.cpp"), os.path.join(HERE, "oracle_cloth.cpp"),
+       os.path.join(HERE, "oracle_solver.h"), os.path.join(HERE, "oracle_math.h"),
        os.path.join(HERE, "..", "include", "avbd.h")]
 
 
@@ -24,7 +25,7 @@ def build(force: bool = False) -> str:
         return LIB
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
-           "-fPIC", "-shared", "-o", LIB, SRC[0]]
+           "-fPIC", "-shared", "-o", LIB, SRC[0], SRC[1]]
     subprocess.check_call(cmd)
     return LIB
 

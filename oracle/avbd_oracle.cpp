@@ -18,196 +18,10 @@
 //
 // Optional OpenMP: bodies of one color are independent, so the per-color loop
 // may run in parallel without changing any result (used for the CPU baseline).
-#include "oracle_math.h"
-#include "../include/avbd.h"
-
-#include <algorithm>
-#include <array>
-#include <cfloat>
-#include <cstdio>
-#include <cstdlib>
-#include <map>
-#include <set>
-#include <string>
-#include <vector>
-#ifdef _OPENMP
-#include <omp.h>
-#endif
+#include "oracle_solver.h"
 
 namespace oracle {
 
-static const float PENALTY_MIN = 1.0f;
-static const float PENALTY_MAX = 1.0e10f;
-static const float PENALTY_MAX_T = 1.0e6f;
-static const float STICK_THRESH = 0.00001f;
-static const int MAX_COLORS = 64;
-static const uint32_t WORLD_BODY = 0xFFFFFFFFu;
-static const uint32_t FK_JOINT = 0, FK_SPRING = 1, FK_MANIFOLD = 2, FK_TET = 3,
-                      FK_SOFT = 4, FK_MEMBRANE = 5, FK_BEND = 6;
-static const int ADJ_KIND_SHIFT = 28;
-static const uint32_t ADJ_INDEX_MASK = 0x0FFFFFFFu;
-static const int MAX_CONTACTS = 8;
-static const uint32_t MOTOR_MODE_MASK = 3u << 4, MOTOR_IMPLICIT = 1u << 4,
-                      MOTOR_EXPLICIT = 2u << 4, MOTOR_VELOCITY = 3u << 4;
-
-// ---- GPU record layouts (00_common.metal:330-431) ------------------------
-struct JointGPU {
-    U4 header;  // bodyA, bodyB, broken, flags
-    F4 rA, rB, C0Lin, C0Ang, lambdaLin, lambdaAng, penaltyLin, penaltyAng,
-        restRel, hingeAxis, motor, limits, dynamics;
-};
-struct SpringGPU { U4 header; F4 rA, rB, dual; };
-struct TetGPU { U4 ids; F4 r0, r1, r2; };
-struct ContactGPU { F4 rA, rB, C0, lambda, penalty; };
-struct ManifoldGPU {
-    U4 header;  // bodyA, bodyB, numContacts, flags (1 active, 2 roundA, 4 roundB)
-    U4 colliderPair;
-    F4 basisN, basisT1;
-    ContactGPU contacts[MAX_CONTACTS];
-};
-static_assert(sizeof(JointGPU) == 224, "JointGPU layout");
-static_assert(sizeof(SpringGPU) == 64, "SpringGPU layout");
-static_assert(sizeof(TetGPU) == 64, "TetGPU layout");
-static_assert(sizeof(ManifoldGPU) == 704, "ManifoldGPU layout");
-
-struct Params {
-    float dt, gravity, alpha, betaLin, betaAng, gamma;
-    uint32_t numBodies, numJoints, numSprings, mapCapacity, maxPairs;
-    float cellSize;
-    uint32_t gridHashSize, numHashed, numGlobals;
-    float maxSpeed, lambdaMax;
-    uint32_t iterations, numTets, numTris, numParticles;
-    float rodDecayPow, particleDamping;
-    uint32_t numHashedRigid, frame, frictionCombineMode;
-    float collisionMargin, rigidLinearDamping, rigidAngularDamping;
-    uint32_t surfaceTruncationMode, tetInversionPreventionEnabled;
-    float planarDATRelaxation;
-};
-
-static uint32_t next_pow2(uint32_t v) {
-    uint32_t p = 1;
-    while (p < v) p <<= 1;
-    return p;
-}
-
-// Hash of an integer cell (20_broadphase.metal:16-28).
-static inline uint32_t cell_hash(int cx, int cy, int cz, uint32_t group, uint32_t size) {
-    uint32_t h = ((uint32_t)cx * 92837111u) ^ ((uint32_t)cy * 689287499u)
-               ^ ((uint32_t)cz * 283923481u);
-    h ^= group * 0x9e3779b9u;
-    h ^= h >> 16;
-    h *= 0x7feb352du;
-    h ^= h >> 15;
-    return h & (size - 1u);
-}
-static inline void cell_coord(F3 p, float cs, int& x, int& y, int& z) {
-    x = (int)std::floor(p.x / cs);
-    y = (int)std::floor(p.y / cs);
-    z = (int)std::floor(p.z / cs);
-}
-// Manifold persistence-map hash (20_broadphase.metal:547-553).
-static inline uint32_t pair_map_hash(uint32_t a, uint32_t b, uint32_t cap) {
-    uint32_t h = (a * 73856093u) ^ (b * 19349663u);
-    h ^= h >> 16;
-    h *= 0x7feb352du;
-    h ^= h >> 15;
-    return h & (cap - 1u);
-}
-static inline bool groups_compatible(uint32_t a, uint32_t b) { return a == 0u || b == 0u || a == b; }
-static inline bool domains_compatible(uint32_t ga, uint32_t gb, uint32_t sa, uint32_t sb) {
-    if (!groups_compatible(ga, gb)) return false;
-    if (ga == 0u && gb != 0u) return sb != 0u;
-    if (gb == 0u && ga != 0u) return sa != 0u;
-    return true;
-}
-
-struct Accum { M3 lhsLin, lhsAng, lhsCross; F3 rhsLin, rhsAng; };
-static inline Accum accum_zero() { return Accum{m3_zero(), m3_zero(), m3_zero(), f3s(0), f3s(0)}; }
-static inline Accum accum_add(const Accum& a, const Accum& b) {
-    return Accum{m3_add(a.lhsLin, b.lhsLin), m3_add(a.lhsAng, b.lhsAng),
-                 m3_add(a.lhsCross, b.lhsCross), a.rhsLin + b.rhsLin, a.rhsAng + b.rhsAng};
-}
-
-struct Solver {
-    avbd_settings settings{};
-    Params P{};
-    uint32_t nb = 0, nc = 0;
-    uint64_t frameIndex = 0;
-    std::string error;
-    int failure = AVBD_FAIL_NONE;
-    int threads = 1;
-
-    // bodies
-    std::vector<F4> posLin, posAng, initLin, initAng, inertLin, inertAng, velLin, velAng,
-        prevVelLin, props, shape, spinVel, ogcPrev;
-    std::vector<float> gravityScale;
-    std::vector<uint32_t> shapeType, boundsBits, clothGroup, clothVert;
-    std::vector<uint8_t> isDynamic, isParticle;
-    // colliders
-    std::vector<uint32_t> colOwner, colShapeType, colGroup, colShared;
-    std::vector<F4> colShape, colLocalPos, colLocalRot;
-    std::vector<float> colFrictionS, colFrictionD;
-    std::vector<uint32_t> hashedIdx, globalIdx, hashedRigidIdx;
-    // constraints
-    std::vector<JointGPU> joints;
-    std::vector<F4> initPenLin, initPenAng;
-    std::vector<SpringGPU> springs;
-    std::vector<TetGPU> tets;
-    std::vector<uint32_t> exclusions;  // (a, b) pairs, sorted
-    std::vector<avbd_spinner_desc> spinners;
-    struct RateMotor { uint32_t joint; float rate; };
-    std::vector<RateMotor> rateMotors;
-    // capacities
-    uint32_t maxPairs = 0, mapCapacity = 0, gridHashSize = 0;
-    uint32_t numTris = 0, numParticles = 0;
-    bool dynamicColoring = true;
-    uint32_t staticUsedColors = 1;
-    // per-frame
-    std::vector<uint32_t> cellCount, cellStart, cellBodies, cellRigid, bodyCellSlot;
-    std::vector<uint32_t> pairCount, pairStart, pairs;
-    std::vector<ManifoldGPU> manifolds, prevManifolds;
-    std::vector<uint32_t> mapKeyA, mapKeyB, mapVal;
-    std::vector<uint32_t> adjStart, adjCount, adjList;
-    std::vector<uint32_t> colorsA, colorsB, colorStart, colorList;
-    uint32_t numPairs = 0, pairCandidates = 0, colorConflicts = 0, ogcExceeded = 0;
-    uint32_t colorCounts[MAX_COLORS] = {};
-
-    bool body_dynamic(uint32_t b) const { return b != WORLD_BODY && posLin[b].w > 0.0f; }
-
-    // ---------------------------------------------------------------- upload
-    int create(const avbd_scene_desc* s);
-    void sync_params();
-    void step();
-    // stages
-    void broadphase();
-    uint32_t process_producer(uint32_t producer, bool emit, uint32_t base);
-    void narrowphase();
-    void narrow_one(uint32_t gid);
-    void map_rebuild();
-    int map_find(uint32_t a, uint32_t b) const;
-    void warmstart_joints();
-    void warmstart_bodies();
-    void adjacency();
-    void dynamic_coloring();
-    void neighbor_colors(uint32_t entry, uint32_t self, uint32_t myColor,
-                         const std::vector<uint32_t>& colorsIn, uint32_t& maskLo,
-                         uint32_t& maskHi, uint32_t& allLo, uint32_t& allHi,
-                         bool& conflict) const;
-    void primal_color(uint32_t c);
-    void primal_body(uint32_t body);
-    void stamp_entry(uint32_t entry, uint32_t body, Accum& acc) const;
-    void stamp_joint(const JointGPU& j, uint32_t self, Accum& acc) const;
-    void stamp_spring(const SpringGPU& sp, uint32_t self, Accum& acc) const;
-    void stamp_tet(const TetGPU& t, uint32_t self, Accum& acc) const;
-    void stamp_manifold(const ManifoldGPU& m, uint32_t self, Accum& acc) const;
-    void dual_all();
-    void dual_joint(uint32_t gid);
-    void dual_spring(uint32_t si);
-    void dual_manifold(uint32_t mi);
-    void finalize();
-    void advance_spinners();
-    float max_constraint_error() const;
-};
 
 // ==========================================================================
 // Upload (GPUSolver.swift:338-638, :901-2081)
@@ -232,7 +46,14 @@ int Solver::create(const avbd_scene_desc* s) {
             return AVBD_ERR_UNSUPPORTED;
         }
     }
-    if (s->num_tris > 0) { error = "cloth triangles are not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+    if (s->num_tris > 0 && s->num_tets > 0) {
+        error = "scenes mixing cloth triangles and tets are not restated";
+        return AVBD_ERR_UNSUPPORTED;
+    }
+    if (s->num_tris > 0 && s->truncation_selection == AVBD_TRUNCATION_ISOTROPIC) {
+        error = "isotropic OGC truncation of cloth is not restated";
+        return AVBD_ERR_UNSUPPORTED;
+    }
 
     uint32_t enabled = 0;
     for (uint32_t i = 0; i < nc; i++) enabled += s->colliders[i].collision_enabled ? 1u : 0u;
@@ -242,7 +63,7 @@ int Solver::create(const avbd_scene_desc* s) {
     gridHashSize = next_pow2(std::max<uint32_t>(64u, 2u * std::max<uint32_t>(1u, enabled)));
 
     std::vector<std::array<int, 3>> boundary = tet_boundary_faces(s);
-    numTris = (uint32_t)boundary.size();
+    numTris = (uint32_t)boundary.size() + s->num_tris;
 
     posLin.assign(nb, F4{}); posAng.assign(nb, F4{}); initLin.assign(nb, F4{});
     initAng.assign(nb, F4{}); inertLin.assign(nb, F4{}); inertAng.assign(nb, F4{});
@@ -475,8 +296,14 @@ int Solver::create(const avbd_scene_desc* s) {
     exclusions.clear();
     for (uint64_t k : excl) { exclusions.push_back((uint32_t)(k >> 32)); exclusions.push_back((uint32_t)(k & 0xFFFFFFFFu)); }
 
+    if (s->num_tris > 0) {
+        int rc = cloth_upload(s, boundary);
+        if (rc != AVBD_OK) return rc;
+        colorJacobi = true;
+    }
+
     // collision-surface groups for tet boundary faces (GPUSolver.swift:1461-1535)
-    if (!boundary.empty()) {
+    if (s->num_tris == 0 && !boundary.empty()) {
         std::vector<int> parent(nb, -1);
         auto find = [&](int x) { int r = x; while (parent[r] >= 0 && parent[r] != r) r = parent[r];
             int c = x; while (parent[c] >= 0 && parent[c] != r) { int n = parent[c]; parent[c] = r; c = n; }
@@ -563,15 +390,20 @@ int Solver::create(const avbd_scene_desc* s) {
     P.numHashed = (uint32_t)hashedIdx.size(); P.numGlobals = (uint32_t)globalIdx.size();
     P.numHashedRigid = (uint32_t)hashedRigidIdx.size();
     P.numTris = numTris; P.numParticles = numTris == 0 ? 0 : numParticles;
+    clothViscosity = settings.cloth_viscosity;
     P.maxSpeed = fmax_(30.0f, 1.5f * P.cellSize / settings.dt * 0.5f);
 
     spinners.assign(s->spinners, s->spinners + s->num_spinners);
     for (auto& sp : spinners)
         spinVel[sp.body] = f4(sp.axis[0] * sp.omega, sp.axis[1] * sp.omega, sp.axis[2] * sp.omega, 1.0f);
+    // effectiveSurfaceTruncationMode (GPUSolver.swift:93-101)
     P.surfaceTruncationMode = 0;
     if (P.numParticles > 0) {
         uint32_t sel = s->truncation_selection;
-        P.surfaceTruncationMode = sel == AVBD_TRUNCATION_AUTOMATIC ? 1u : sel;
+        bool volumetricSelf = false;
+        for (uint32_t i = 0; i < s->num_tets; i++) volumetricSelf = volumetricSelf || s->tets[i].self_collision;
+        uint32_t automatic = (volumetricSelf || (s->num_tris > 0 && s->num_tets == 0)) ? 2u : 1u;
+        P.surfaceTruncationMode = sel == AVBD_TRUNCATION_AUTOMATIC ? automatic : sel;
     }
     P.tetInversionPreventionEnabled = (P.surfaceTruncationMode == 2u && s->tet_inversion_prevention) ? 1u : 0u;
     P.planarDATRelaxation = 0.85f;
@@ -622,6 +454,7 @@ void Solver::sync_params() {
     P.collisionMargin = fmax_(settings.collision_margin, 0.0f);
     P.rigidLinearDamping = fmax_(settings.rigid_linear_damping, 0.0f);
     P.rigidAngularDamping = fmax_(settings.rigid_angular_damping, 0.0f);
+    clothViscosity = settings.cloth_viscosity;
 }
 
 // ==========================================================================
@@ -1310,6 +1143,19 @@ void Solver::adjacency() {
         uint32_t e = (FK_TET << ADJ_KIND_SHIFT) | t;
         add(tets[t].ids.x, e); add(tets[t].ids.y, e); add(tets[t].ids.z, e); add(tets[t].ids.w, e);
     }
+    for (uint32_t i = 0; i < numSoft; i++) {
+        uint32_t e = (FK_SOFT << ADJ_KIND_SHIFT) | i;
+        const uint32_t ids[4] = {soft[i].ids.x, soft[i].ids.y, soft[i].ids.z, soft[i].ids.w};
+        for (uint32_t b : ids) add(b, e);
+    }
+    for (uint32_t i = 0; i < membranes.size(); i++) {
+        uint32_t e = (FK_MEMBRANE << ADJ_KIND_SHIFT) | i;
+        add(membranes[i].ids.x, e); add(membranes[i].ids.y, e); add(membranes[i].ids.z, e);
+    }
+    for (uint32_t i = 0; i < bends.size(); i++) {
+        uint32_t e = (FK_BEND << ADJ_KIND_SHIFT) | i;
+        add(bends[i].ids.x, e); add(bends[i].ids.y, e); add(bends[i].ids.z, e); add(bends[i].ids.w, e);
+    }
     adjStart.assign(nb, 0); adjCount.assign(nb, 0); adjList.clear();
     for (uint32_t b = 0; b < nb; b++) {
         std::sort(lists[b].begin(), lists[b].end());
@@ -1635,6 +1481,9 @@ void Solver::stamp_entry(uint32_t entry, uint32_t body, Accum& acc) const {
     else if (kind == FK_SPRING) stamp_spring(springs[idx], body, acc);
     else if (kind == FK_TET) stamp_tet(tets[idx], body, acc);
     else if (kind == FK_MANIFOLD) stamp_manifold(manifolds[idx], body, acc);
+    else if (kind == FK_SOFT) stamp_soft(soft[idx], body, acc);
+    else if (kind == FK_MEMBRANE) stamp_membrane(membranes[idx], body, acc);
+    else if (kind == FK_BEND) stamp_bend(bends[idx], body, acc);
 }
 
 void Solver::primal_body(uint32_t body) {
@@ -1696,6 +1545,11 @@ void Solver::primal_body(uint32_t body) {
             }
         }
     }
+    if (colorJacobi) {
+        posNext[body] = f4(xyz(pl) + dxLin, mass);
+        if (rigid) angNext[body] = q_addw(posAng[body], dxAng);
+        return;
+    }
     posLin[body] = f4(xyz(pl) + dxLin, mass);
     if (rigid) posAng[body] = q_addw(posAng[body], dxAng);
 }
@@ -1703,6 +1557,8 @@ void Solver::primal_body(uint32_t body) {
 void Solver::primal_color(uint32_t c) {
     uint32_t s0 = colorStart[c], e0 = colorStart[c + 1];
     int n = (int)(e0 - s0);
+    if (colorJacobi)
+        for (uint32_t i = s0; i < e0; i++) { posNext[colorList[i]] = posLin[colorList[i]]; angNext[colorList[i]] = posAng[colorList[i]]; }
 #ifdef _OPENMP
 #pragma omp parallel for schedule(static) num_threads(threads) if (threads > 1 && n > 256)
 #endif
@@ -1825,6 +1681,7 @@ void Solver::dual_all() {
     for (uint32_t g = 0; g < joints.size(); g++) dual_joint(g);
     for (uint32_t s = 0; s < springs.size(); s++) dual_spring(s);
     for (uint32_t m = 0; m < numPairs; m++) if (manifolds[m].header.z != 0) dual_manifold(m);
+    for (uint32_t i = 0; i < numSoft; i++) dual_soft(i);
 }
 
 // ==========================================================================
@@ -1898,26 +1755,59 @@ void Solver::step() {
     std::fill(boundsBits.begin(), boundsBits.end(), 0x7F7F7F7Fu);
     ogcExceeded = 0;
     colorConflicts = 0;
+    const bool planar = P.surfaceTruncationMode == 2u && numTris > 0;
+    dat = DatCounters{};
+    softRaw = 0;
+    numSoft = 0;
     broadphase();
     narrowphase();
     map_rebuild();
+    if (planar) {
+        elem_grid();
+        dat_build_pairs();                     // step-start pose
+        rt_emit();
+    }
     warmstart_joints();
     warmstart_bodies();
+    if (planar) {
+        dat_reduce(0xFFFFFFFFu);               // predictor pass
+        dat_apply_particles();
+        elem_grid();                           // accepted predictor pose
+        dat_build_pairs();
+        dat_emit_contacts();
+        soft_map_rebuild();
+        for (uint32_t v : particleIdx) ogcPrev[v] = f4(xyz(posLin[v]), 0.0f);
+    }
     adjacency();
     if (dynamicColoring) dynamic_coloring();
     uint32_t colorBound = dynamicColoring ? (uint32_t)MAX_COLORS : staticUsedColors;
     for (uint32_t it = 0; it < P.iterations; it++) {
-        for (uint32_t c = 0; c < colorBound; c++) primal_color(c);
+        for (uint32_t c = 0; c < colorBound; c++) {
+            primal_color(c);
+            if (planar) {
+                dat_reduce(c);
+                dat_apply_color(c);
+            }
+        }
         dual_all();
     }
+    if (planar) dat_restore_failed_surface();
     finalize();
+    if (numTris > 0 && cloth && clothViscosity > 0.0f) smooth_particle_velocities();
     advance_spinners();
     frameIndex++;
     // the manifolds written this frame become next frame's warm-start source
     std::swap(manifolds, prevManifolds);
+    if (cloth) std::swap(soft, prevSoft);
     if (pairCandidates > maxPairs && failure == AVBD_FAIL_NONE) {
         failure = AVBD_FAIL_RIGID_PAIR_CAPACITY;
         error = "rigid pair capacity exceeded";
+    }
+    if (planar && failure == AVBD_FAIL_NONE) {
+        if (dat.softCandidates > maxSoft) { failure = AVBD_FAIL_SOFT_CONTACT_CAPACITY; error = "soft contact capacity exceeded"; }
+        else if (dat.pairsPeak > maxDatPairs) { failure = AVBD_FAIL_PLANAR_DAT_PAIR_CAPACITY; error = "Planar-DAT pair capacity exceeded"; }
+        else if (dat.gridOverflow > 0) { failure = AVBD_FAIL_PLANAR_DAT_GRID_SPAN; error = "Planar-DAT element grid span exceeded"; }
+        else if (dat.invalidAnchor > 0) { failure = AVBD_FAIL_PLANAR_DAT_INVALID_ANCHOR; error = "Planar-DAT invalid anchor"; }
     }
     if (colorConflicts > 0 && failure == AVBD_FAIL_NONE) {
         failure = AVBD_FAIL_UNRESOLVED_COLORING;
@@ -1998,6 +1888,18 @@ int oracle_get_counters(void* h, avbd_counters* out) {
     out->ogc_exceeded = s->ogcExceeded;
     out->used_colors = s->dynamicColoring ? s->colorStart[64 + 1] : s->staticUsedColors;
     for (int c = 0; c < 64; c++) out->color_counts[c] = s->colorCounts[c];
+    out->num_soft = s->numSoft;
+    out->soft_candidates = s->dat.softCandidates;
+    out->dat_pairs = s->dat.pairsPeak;
+    out->dat_vt_pairs = s->dat.vtPeak;
+    out->dat_ee_pairs = s->dat.eePeak;
+    out->dat_grid_overflows = s->dat.gridOverflow;
+    out->dat_invalid_anchors = s->dat.invalidAnchor;
+    out->dat_truncations = s->dat.truncations;
+    out->dat_vt_degenerate = s->dat.vtDegenerate;
+    out->dat_ee_degenerate = s->dat.eeDegenerate;
+    out->dat_nonfinite = s->dat.nonfinite;
+    out->dat_tet_degenerate = s->dat.tetDegenerate;
     return AVBD_OK;
 }
 static const void* oracle_buffer(Solver* s, int which, size_t& bytes) {
@@ -2029,6 +1931,19 @@ static const void* oracle_buffer(Solver* s, int which, size_t& bytes) {
     case AVBD_BUF_EXCLUSIONS: bytes = s->exclusions.size() * 4; return s->exclusions.data();
     case AVBD_BUF_HASHED_IDX: bytes = s->hashedIdx.size() * 4; return s->hashedIdx.data();
     case AVBD_BUF_GLOBAL_IDX: bytes = s->globalIdx.size() * 4; return s->globalIdx.data();
+    case AVBD_BUF_TRIS: bytes = s->tris.size() * 16; return s->tris.data();
+    case AVBD_BUF_EDGES: bytes = s->edges.size() * 4; return s->edges.data();
+    case AVBD_BUF_NBR_START: bytes = s->nbrStart.size() * 4; return s->nbrStart.data();
+    case AVBD_BUF_NBR_COUNT: bytes = s->nbrCount.size() * 4; return s->nbrCount.data();
+    case AVBD_BUF_NBR_LIST: bytes = s->nbrList.size() * 4; return s->nbrList.data();
+    case AVBD_BUF_PARTICLE_IDX: bytes = (size_t)s->numParticles * 4; return s->particleIdx.data();
+    case AVBD_BUF_MEMBRANES: bytes = s->membranes.size() * sizeof(oracle::MembraneGPU); return s->membranes.data();
+    case AVBD_BUF_BENDS: bytes = s->bends.size() * sizeof(oracle::BendGPU); return s->bends.data();
+    // element contacts were swapped at the end of the frame like the manifolds
+    case AVBD_BUF_SOFT: bytes = (size_t)s->numSoft * sizeof(oracle::SoftContactGPU); return s->prevSoft.data();
+    case AVBD_BUF_DAT_PAIRS: bytes = s->datPairs.size() * 16; return s->datPairs.data();
+    case AVBD_BUF_CLOTH_GROUP: bytes = s->clothGroup.size() * 4; return s->clothGroup.data();
+    case AVBD_BUF_OGC_PREV: bytes = s->ogcPrev.size() * 16; return s->ogcPrev.data();
     default: bytes = 0; return nullptr;
     }
 }
