@@ -158,6 +158,7 @@ struct avbd_solver {
         P.collisionMargin = settings.collision_margin > 0.0f ? settings.collision_margin : 0.0f;
         P.rigidLinearDamping = settings.rigid_linear_damping > 0.0f ? settings.rigid_linear_damping : 0.0f;
         P.rigidAngularDamping = settings.rigid_angular_damping > 0.0f ? settings.rigid_angular_damping : 0.0f;
+        P.clothViscosity = settings.cloth_viscosity;
     }
 
     // One frame, in the reference's stage order.  `parity` selects which
