@@ -181,4 +181,5 @@ STAGES = ["broadphase", "narrowphase", "persistence_map", "warmstart", "adjacenc
 class Profile(C.Structure):
     _fields_ = [("frames", C.c_uint64), ("kernels_per_frame", C.c_uint64),
                 ("stage_ms", C.c_double * 16),
-                ("stage_launches", C.c_uint64 * 16)]
+                ("stage_launches", C.c_uint64 * 16),
+                ("color_lanes", C.c_uint32 * 64)]

@@ -225,7 +225,8 @@ class GPUSolver:
         self._check(load_library().avbd_get_profile(self._h, C.byref(p)))
         return {"frames": p.frames, "kernels_per_frame": p.kernels_per_frame,
                 "stage_ms": {n: p.stage_ms[i] for i, n in enumerate(abi.STAGES)},
-                "stage_launches": {n: p.stage_launches[i] for i, n in enumerate(abi.STAGES)}}
+                "stage_launches": {n: p.stage_launches[i] for i, n in enumerate(abi.STAGES)},
+                "color_lanes": list(p.color_lanes)}
 
     def debug_read(self, name: str, dtype=np.uint8):
         lib = load_library()

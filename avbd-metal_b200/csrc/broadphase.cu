@@ -156,20 +156,33 @@ __global__ void k_bp_scatter(const Params P, const DevPtrs d) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.numHashed) return;
     const uint2 cs = d.bodyCellSlot[i];
-    d.cellBodies[d.cellStart[cs.x] + cs.y] = d.hashedIdx[i];
+    d.cellTmp[d.cellStart[cs.x] + cs.y] = d.hashedIdx[i];
 }
 
-// Buckets are tiny: an insertion sort per bucket restores collider order.
+static uint32_t stride_blocks_bp(uint32_t threads, int T) {
+    const uint32_t need = (threads + T - 1) / T;
+    const uint32_t cap = 148u * 16u;
+    return need == 0 ? 1u : (need < cap ? need : cap);
+}
+
+// Collider order inside each bucket: one warp per bucket places every entry
+// at its rank (the number of smaller ids; ids are distinct).  Dense buckets —
+// a cloth sheet puts hundreds of particles in one cell — cost n^2/32 compares
+// per lane instead of a serial insertion sort.
 __global__ void k_bp_sort_cells(const Params P, const DevPtrs d) {
-    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= P.gridHashSize) return;
-    const uint32_t s = d.cellStart[h], n = d.cellCount[h];
-    uint32_t* b = d.cellBodies + s;
-    for (uint32_t i = 1; i < n; i++) {
-        const uint32_t v = b[i];
-        uint32_t j = i;
-        while (j > 0 && b[j - 1] > v) { b[j] = b[j - 1]; j--; }
-        b[j] = v;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < P.gridHashSize; h += warps) {
+        const uint32_t n = d.cellCount[h];
+        if (n == 0) continue;
+        const uint32_t s = d.cellStart[h];
+        const uint32_t* src = d.cellTmp + s;
+        for (uint32_t i = lane; i < n; i += 32) {
+            const uint32_t v = src[i];
+            uint32_t rank = 0;
+            for (uint32_t j = 0; j < n; j++) rank += src[j] < v ? 1u : 0u;
+            d.cellBodies[s + rank] = v;
+        }
     }
 }
 
@@ -314,7 +327,7 @@ void launch_broadphase(const Params& P, const DevPtrs& d, const Sizes& z, cudaSt
         k_bp_count<<<(P.numHashed + T - 1) / T, T, 0, st>>>(P, d);
         launch_exclusive_scan(d.cellCount, d.cellStart, P.gridHashSize, d.scanScratch, st);
         k_bp_scatter<<<(P.numHashed + T - 1) / T, T, 0, st>>>(P, d);
-        k_bp_sort_cells<<<(P.gridHashSize + T - 1) / T, T, 0, st>>>(P, d);
+        k_bp_sort_cells<<<stride_blocks_bp(P.gridHashSize * 32u, T), T, 0, st>>>(P, d);
     }
     if (z.producers > 0) {
         k_bp_prep<<<(z.numColliders + T - 1) / T, T, 0, st>>>(P, d, z.numColliders);

@@ -183,30 +183,50 @@ __device__ void soft_write(const Params& P, const DevPtrs& d, uint32_t slot, uin
     sc.penalty = tof4(pen, __uint_as_float(keyB));
 }
 
-// Element AABB padded by the Planar-DAT query radius (25_cloth.metal:147-180).
-__device__ void elem_bounds(const Params& P, const DevPtrs& d, uint32_t gid, float3& lo, float3& hi) {
-    const float pad = P.queryRadius;
+// Tight AABB of element gid (triangles, then edges).
+__device__ void elem_tight(const Params& P, const DevPtrs& d, uint32_t gid, float3& lo, float3& hi) {
     if (gid < P.numTris) {
         const uint4 t = d.tris[gid];
         const float3 a = xyz(d.posLin[t.x]), b = xyz(d.posLin[t.y]), c = xyz(d.posLin[t.z]);
-        lo = vmin(vmin(a, b), c) - s3(pad);
-        hi = vmax(vmax(a, b), c) + s3(pad);
+        lo = vmin(vmin(a, b), c);
+        hi = vmax(vmax(a, b), c);
     } else {
         const uint2 e = d.edges[gid - P.numTris];
         const float3 a = xyz(d.posLin[e.x]), b = xyz(d.posLin[e.y]);
-        lo = vmin(a, b) - s3(pad);
-        hi = vmax(a, b) + s3(pad);
+        lo = vmin(a, b);
+        hi = vmax(a, b);
     }
 }
 
+// Element AABB padded by the Planar-DAT query radius (25_cloth.metal:147-180),
+// from the tight box stored by the binning pass (min/max are exact, so the
+// padded bounds carry the same bits as when computed from the vertices).
+__device__ __forceinline__ void elem_bounds(const Params& P, const DevPtrs& d, uint32_t gid, float3& lo, float3& hi) {
+    const float4 l = d.elemBox[2 * gid], h = d.elemBox[2 * gid + 1];
+    lo = xyz(l) - s3(P.queryRadius);
+    hi = xyz(h) + s3(P.queryRadius);
+}
+
+// A conservative reach for box prefilters: anything within the query radius
+// by the exact float test also lies within this distance of the tight box.
+__device__ __forceinline__ float prefilter_reach(const Params& P) { return P.queryRadius * 1.001f + 1.0e-5f; }
+
 // ---------------------------------------------------------------------------
 // Element grid: every triangle and edge in each distinct bucket of its
-// (at most 4x4x4) cell cover.
+// (at most 4x4x4) cell cover.  Triangles and edges are binned into separate
+// halves of the count array ([0, H) triangles, [H, 2H) edges) so that a V-T
+// query scans only triangles and an E-E query only edges; the candidate
+// sets they accept are unchanged.
 // ---------------------------------------------------------------------------
 template <bool SCATTER>
 __global__ void k_elem_bin(const Params P, const DevPtrs d, uint32_t total) {
     for (uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x; gid < total; gid += gridDim.x * blockDim.x) {
         float3 lo, hi;
+        if (!SCATTER) {
+            elem_tight(P, d, gid, lo, hi);
+            d.elemBox[2 * gid] = mk4(lo, 0.0f);
+            d.elemBox[2 * gid + 1] = mk4(hi, 0.0f);
+        }
         elem_bounds(P, d, gid, lo, hi);
         if (!finite3(lo) || !finite3(hi)) {
             if (!SCATTER) {
@@ -219,7 +239,9 @@ __global__ void k_elem_bin(const Params P, const DevPtrs d, uint32_t total) {
         if (!SCATTER && (raw.x - c0.x > 3 || raw.y - c0.y > 3 || raw.z - c0.z > 3))
             atomicAdd(&d.counters->datGridOverflow, 1u);
         const I3 c1 = imin3(raw, iadd(c0, 3));
-        const uint32_t entry = gid < P.numTris ? gid : (ELEM_EDGE_BIT | (gid - P.numTris));
+        const bool tri = gid < P.numTris;
+        const uint32_t entry = tri ? gid : gid - P.numTris;
+        const uint32_t half = tri ? 0u : P.elemHashSize;
         uint32_t seen[64];
         uint32_t ns = 0;
         for (int z = c0.z; z <= c1.z; z++)
@@ -230,8 +252,8 @@ __global__ void k_elem_bin(const Params P, const DevPtrs d, uint32_t total) {
                     for (uint32_t i = 0; i < ns; i++) dup = dup || seen[i] == h;
                     if (dup) continue;
                     seen[ns++] = h;
-                    if (SCATTER) d.elemCells[atomicAdd(&d.elemCursor[h], 1u)] = entry;
-                    else atomicAdd(&d.elemCellCount[h], 1u);
+                    if (SCATTER) d.elemCells[atomicAdd(&d.elemCursor[half + h], 1u)] = entry;
+                    else atomicAdd(&d.elemCellCount[half + h], 1u);
                 }
     }
 }
@@ -241,11 +263,27 @@ __global__ void k_elem_bin(const Params P, const DevPtrs d, uint32_t total) {
 // owners [0, numParticles) are V-T queries of surface particles, the rest
 // E-E queries of edges.
 // ---------------------------------------------------------------------------
+// The reference's V-T acceptance is a conjunction of pure predicates
+// (27_planar_dat.metal:75-101); they are evaluated cheapest first, after a
+// conservative box test that every accepted pair passes.
 __device__ __forceinline__ bool vt_candidate(const Params& P, const DevPtrs& d, uint32_t v, float3 p, I3 cell,
                                              uint32_t ns, uint32_t ne, uint32_t entry, float query2) {
-    if ((entry & ELEM_EDGE_BIT) != 0u || entry >= P.numTris) return false;
+    if (entry >= P.numTris) return false;
+    const float4 bl = d.elemBox[2 * entry], bh = d.elemBox[2 * entry + 1];
+    const float r = prefilter_reach(P);
+    if (p.x < bl.x - r || p.y < bl.y - r || p.z < bl.z - r || p.x > bh.x + r || p.y > bh.y + r || p.z > bh.z + r)
+        return false;
+    const float3 lo = xyz(bl) - s3(P.queryRadius), hi = xyz(bh) + s3(P.queryRadius);
+    const I3 tc0 = cell_of(lo, P.elemCellSize);
+    const I3 tc1 = imin3(cell_of(hi, P.elemCellSize), iadd(tc0, 3));
+    if (cell.x < tc0.x || cell.y < tc0.y || cell.z < tc0.z || cell.x > tc1.x || cell.y > tc1.y || cell.z > tc1.z)
+        return false;
     const uint4 t = d.tris[entry];
     if (t.x == v || t.y == v || t.z == v) return false;
+    float3 bary;
+    const float3 q = closest_pt_triangle(p, xyz(d.posLin[t.x]), xyz(d.posLin[t.y]), xyz(d.posLin[t.z]), bary);
+    const float3 dd = p - q;
+    if (dot(dd, dd) > query2) return false;
     const uint32_t group = d.clothGroup[v];
     const bool same = group != 0u && d.clothGroup[t.x] == group && d.clothGroup[t.y] == group &&
                       d.clothGroup[t.z] == group;
@@ -253,26 +291,34 @@ __device__ __forceinline__ bool vt_candidate(const Params& P, const DevPtrs& d, 
     if (same && (nbr_contains(d.nbrList, ns, ne, t.x) || nbr_contains(d.nbrList, ns, ne, t.y) ||
                  nbr_contains(d.nbrList, ns, ne, t.z)))
         return false;
-    float3 lo, hi;
-    elem_bounds(P, d, entry, lo, hi);
-    const I3 tc0 = cell_of(lo, P.elemCellSize);
-    const I3 tc1 = imin3(cell_of(hi, P.elemCellSize), iadd(tc0, 3));
-    if (cell.x < tc0.x || cell.y < tc0.y || cell.z < tc0.z || cell.x > tc1.x || cell.y > tc1.y || cell.z > tc1.z)
-        return false;
-    float3 bary;
-    const float3 q = closest_pt_triangle(p, xyz(d.posLin[t.x]), xyz(d.posLin[t.y]), xyz(d.posLin[t.z]), bary);
-    const float3 dd = p - q;
-    return !(dot(dd, dd) > query2);
+    return true;
 }
 
+// E-E acceptance (27_planar_dat.metal:155-204), cheapest predicates first
+// after a conservative box-separation test.
 __device__ __forceinline__ bool ee_candidate(const Params& P, const DevPtrs& d, uint32_t gid, uint2 a, float3 a0,
-                                             float3 a1, I3 ac0, I3 ac1, I3 cell, uint32_t entry, float query2,
-                                             uint32_t& flags) {
-    if ((entry & ELEM_EDGE_BIT) == 0u) return false;
-    const uint32_t other = entry & ~ELEM_EDGE_BIT;
+                                             float3 a1, float3 alo, float3 ahi, I3 ac0, I3 ac1, I3 cell,
+                                             uint32_t other, float query2, uint32_t& flags) {
     if (other <= gid || other >= P.numEdges) return false;
+    const float4 bl = d.elemBox[2 * (P.numTris + other)], bh = d.elemBox[2 * (P.numTris + other) + 1];
+    const float r = prefilter_reach(P);
+    if (bl.x - ahi.x > r || bl.y - ahi.y > r || bl.z - ahi.z > r || alo.x - bh.x > r || alo.y - bh.y > r ||
+        alo.z - bh.z > r)
+        return false;
+    const float3 blo = xyz(bl) - s3(P.queryRadius), bhi = xyz(bh) + s3(P.queryRadius);
+    const I3 bc0 = cell_of(blo, P.elemCellSize);
+    const I3 bc1 = imin3(cell_of(bhi, P.elemCellSize), iadd(bc0, 3));
+    const I3 o0 = imax3(ac0, bc0), o1 = imin3(ac1, bc1);
+    if (o0.x > o1.x || o0.y > o1.y || o0.z > o1.z) return false;
+    if (cell.x != o0.x || cell.y != o0.y || cell.z != o0.z) return false;
     const uint2 b = d.edges[other];
     if (b.x == a.x || b.x == a.y || b.y == a.x || b.y == a.y) return false;
+    float sb, tb;
+    const float3 b0 = xyz(d.posLin[b.x]), b1 = xyz(d.posLin[b.y]);
+    closest_seg_seg(a0, a1, b0, b1, sb, tb);
+    const float3 ca = a0 + (a1 - a0) * sb, cb = b0 + (b1 - b0) * tb;
+    const float3 dd = ca - cb;
+    if (dot(dd, dd) > query2) return false;
     const uint32_t group = d.clothGroup[a.x];
     const bool same = group != 0u && d.clothGroup[a.y] == group && d.clothGroup[b.x] == group &&
                       d.clothGroup[b.y] == group;
@@ -284,19 +330,6 @@ __device__ __forceinline__ bool ee_candidate(const Params& P, const DevPtrs& d, 
             nbr_contains(d.nbrList, ns1, ne1, b.x) || nbr_contains(d.nbrList, ns1, ne1, b.y))
             return false;
     }
-    float3 blo, bhi;
-    elem_bounds(P, d, P.numTris + other, blo, bhi);
-    const I3 bc0 = cell_of(blo, P.elemCellSize);
-    const I3 bc1 = imin3(cell_of(bhi, P.elemCellSize), iadd(bc0, 3));
-    const I3 o0 = imax3(ac0, bc0), o1 = imin3(ac1, bc1);
-    if (o0.x > o1.x || o0.y > o1.y || o0.z > o1.z) return false;
-    if (cell.x != o0.x || cell.y != o0.y || cell.z != o0.z) return false;
-    float sb, tb;
-    const float3 b0 = xyz(d.posLin[b.x]), b1 = xyz(d.posLin[b.y]);
-    closest_seg_seg(a0, a1, b0, b1, sb, tb);
-    const float3 ca = a0 + (a1 - a0) * sb, cb = b0 + (b1 - b0) * tb;
-    const float3 dd = ca - cb;
-    if (dot(dd, dd) > query2) return false;
     flags = DAT_PAIR_TRUNCATE;
     if ((gid < P.numSurfaceEdges && other < P.numSurfaceEdges) || (same && d.selfCollision[a.x] != 0u))
         flags |= DAT_PAIR_CONTACT;
@@ -334,7 +367,7 @@ __global__ void __launch_bounds__(128) k_dat_pairs(const Params P, const DevPtrs
                 continue;
             }
             const I3 cell = cell_of(p, P.elemCellSize);
-            const uint32_t h = elem_hash(cell, P.elemHashSize);
+            const uint32_t h = elem_hash(cell, P.elemHashSize);           // triangle half
             const uint32_t s0 = d.elemCellStart[h], e0 = s0 + d.elemCellCount[h];
             const uint32_t ns = d.nbrStart[v], ne = ns + d.nbrCount[v];
             for (uint32_t k0 = s0; k0 < e0; k0 += 32) {
@@ -370,11 +403,12 @@ __global__ void __launch_bounds__(128) k_dat_pairs(const Params P, const DevPtrs
             if (!EMIT && lane == 0 && (raw.x - ac0.x > 3 || raw.y - ac0.y > 3 || raw.z - ac0.z > 3))
                 atomicAdd(&d.counters->datGridOverflow, 1u);
             const I3 ac1 = imin3(raw, iadd(ac0, 3));
+            const float3 alo = vmin(a0, a1), ahi = vmax(a0, a1);
             for (int z = ac0.z; z <= ac1.z; z++)
                 for (int y = ac0.y; y <= ac1.y; y++)
                     for (int x = ac0.x; x <= ac1.x; x++) {
                         const I3 cell{x, y, z};
-                        const uint32_t h = elem_hash(cell, P.elemHashSize);
+                        const uint32_t h = P.elemHashSize + elem_hash(cell, P.elemHashSize);   // edge half
                         const uint32_t s0 = d.elemCellStart[h], e0 = s0 + d.elemCellCount[h];
                         for (uint32_t k0 = s0; k0 < e0; k0 += 32) {
                             const uint32_t k = k0 + lane;
@@ -382,13 +416,13 @@ __global__ void __launch_bounds__(128) k_dat_pairs(const Params P, const DevPtrs
                             bool pass = false;
                             if (k < e0) {
                                 entry = d.elemCells[k];
-                                pass = ee_candidate(P, d, gid, a, a0, a1, ac0, ac1, cell, entry, query2, flags);
+                                pass = ee_candidate(P, d, gid, a, a0, a1, alo, ahi, ac0, ac1, cell, entry, query2, flags);
                             }
                             const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
                             if (EMIT && pass) {
                                 const uint32_t slot = base + count + __popc(ballot & below);
                                 if (slot < P.maxDatPairs)
-                                    d.datPairs[slot] = make_uint4(DAT_PAIR_EE, gid, entry & ~ELEM_EDGE_BIT, flags);
+                                    d.datPairs[slot] = make_uint4(DAT_PAIR_EE, gid, entry, flags);
                             }
                             count += __popc(ballot);
                         }
@@ -1023,10 +1057,11 @@ uint32_t blocks_for(uint32_t n, uint32_t threads, uint32_t cap = 148u * 16u) {
 
 void build_pairs(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     const uint32_t total = z.numTris + z.numEdges;
-    cudaMemsetAsync(d.elemCellCount, 0, sizeof(uint32_t) * z.elemHashSize, st);
+    const uint32_t buckets = 2 * z.elemHashSize;
+    cudaMemsetAsync(d.elemCellCount, 0, sizeof(uint32_t) * buckets, st);
     k_elem_bin<false><<<blocks_for(total, 128), 128, 0, st>>>(P, d, total);
-    launch_exclusive_scan_large(d.elemCellCount, d.elemCellStart, z.elemHashSize, d.bigScanScratch, st);
-    cudaMemcpyAsync(d.elemCursor, d.elemCellStart, sizeof(uint32_t) * z.elemHashSize, cudaMemcpyDeviceToDevice, st);
+    launch_exclusive_scan_large(d.elemCellCount, d.elemCellStart, buckets, d.bigScanScratch, st);
+    cudaMemcpyAsync(d.elemCursor, d.elemCellStart, sizeof(uint32_t) * buckets, cudaMemcpyDeviceToDevice, st);
     k_elem_bin<true><<<blocks_for(total, 128), 128, 0, st>>>(P, d, total);
     const uint32_t owners = z.numParticles + z.numEdges;
     if (owners == 0) return;

@@ -24,6 +24,7 @@ struct DevPtrs {
     uint32_t* exclusions;                 // uint2 pairs
     // broadphase
     uint32_t *cellCount, *cellStart, *cellBodies, *cellRigid;
+    uint32_t* cellTmp;                    // bucket contents before the per-bucket sort
     uint2* bodyCellSlot;
     uint32_t *pairCount, *pairStart, *pairLaneCount;
     uint2* pairs;
@@ -67,7 +68,8 @@ struct DevPtrs {
     MembraneGPU* membranes;
     BendGPU* bends;
     // cloth: per frame
-    uint32_t *elemCellCount, *elemCellStart, *elemCursor, *elemCells;
+    uint32_t *elemCellCount, *elemCellStart, *elemCursor, *elemCells;   // 2H buckets: triangles, edges
+    float4* elemBox;                            // tight AABB per element (lo, hi)
     uint32_t *datOwnerCount, *datOwnerStart;    // pairs per query owner (particles, edges)
     uint4* datPairs;                            // (kind, owner, other, flags)
     uint32_t *rtCount, *rtStart;                // rigid-triangle records per triangle

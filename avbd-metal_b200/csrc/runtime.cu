@@ -103,6 +103,7 @@ struct avbd_solver {
         if (stream) cudaStreamSynchronize(stream);
         for (auto& g : graph) if (g) cudaGraphExecDestroy(g);
         for (auto& e : events) cudaEventDestroy(e);
+        for (auto& e : tuneEvents) cudaEventDestroy(e);
         for (void* p : allocations) cudaFree(p);
         if (stage) cudaFree(stage);
         if (hostLatch) cudaFreeHost(hostLatch);
@@ -164,16 +165,21 @@ struct avbd_solver {
     // One frame, in the reference's stage order.  `parity` selects which
     // manifold buffer is "current" (the buffers swap after every frame).
     // With profiling on, an event is recorded at every stage boundary.
-    void encode_frame(int parity) {
+    void encode_frame(int parity) { encode_frame_on(parity, stream, nullptr, nullptr); }
+
+    // One frame on stream `st`.  `lanes` overrides the per-color lane width
+    // and `primalEvents` (2 per primal launch, in launch order) brackets every
+    // primal launch; both are used by the autotuner's eager frames.
+    void encode_frame_on(int parity, cudaStream_t st, const uint32_t* lanes, cudaEvent_t* primalEvents) {
         DevPtrs f = d;
         if (parity) {
             std::swap(f.manifolds, f.prevManifolds);
             std::swap(f.soft, f.prevSoft);
         }
-        cudaStream_t st = stream;
         usedEvents = 0;
+        uint32_t primalLaunch = 0;
         auto mark = [&](int stage) {
-            if (!profiling) return;
+            if (!profiling || primalEvents) return;
             cudaEventRecordWithFlags(events[usedEvents], st, cudaEventRecordExternal);
             intervalStage[usedEvents] = stage;
             usedEvents++;
@@ -211,7 +217,10 @@ struct avbd_solver {
                     const uint32_t count = z.dynamicColoring ? 0xFFFFFFFFu : H.colorCounts[c];
                     if (count == 0) continue;
                     mark(AVBD_STAGE_PRIMAL);
-                    launch_primal_color(P, f, z, c, count, H.colorLanes[c], st);
+                    if (primalEvents) cudaEventRecord(primalEvents[2 * primalLaunch], st);
+                    launch_primal_color(P, f, z, c, count, lanes ? lanes[c] : H.colorLanes[c], st);
+                    if (primalEvents) cudaEventRecord(primalEvents[2 * primalLaunch + 1], st);
+                    primalLaunch++;
                     if (P.cloth) {
                         mark(AVBD_STAGE_TRUNCATION);
                         launch_dat_color(P, f, z, c, count, st);
@@ -333,7 +342,7 @@ struct avbd_solver {
         // broadphase
         ok = ok && alloc(d.cellCount, P.gridHashSize, "cellCount") && alloc(d.cellStart, P.gridHashSize, "cellStart");
         ok = ok && alloc(d.cellRigid, P.gridHashSize, "cellRigid") && alloc(d.cellBodies, P.numHashed, "cellBodies");
-        ok = ok && alloc(d.bodyCellSlot, P.numHashed, "bodyCellSlot");
+        ok = ok && alloc(d.bodyCellSlot, P.numHashed, "bodyCellSlot") && alloc(d.cellTmp, P.numHashed, "cellBodiesUnsorted");
         ok = ok && alloc(d.pairCount, z.producers, "pairCount") && alloc(d.pairStart, z.producers, "pairStart");
         ok = ok && alloc(d.pairLaneCount, (size_t)z.producers * 32, "pairLaneCount");
         ok = ok && alloc(d.pairs, H.maxPairs, "pairs");
@@ -378,8 +387,10 @@ struct avbd_solver {
             // element grid, pair streams, element contacts
             const size_t elems = (size_t)H.numTris + H.numEdges;
             const uint32_t owners = P.numParticles + H.numEdges;
-            ok = ok && alloc(d.elemCellCount, H.elemHashSize, "elemCellCount") && alloc(d.elemCellStart, H.elemHashSize, "elemCellStart");
-            ok = ok && alloc(d.elemCursor, H.elemHashSize, "elemCursor") && alloc(d.elemCells, 64 * elems, "elemCells");
+            ok = ok && alloc(d.elemCellCount, 2 * (size_t)H.elemHashSize, "elemCellCount");
+            ok = ok && alloc(d.elemCellStart, 2 * (size_t)H.elemHashSize, "elemCellStart");
+            ok = ok && alloc(d.elemCursor, 2 * (size_t)H.elemHashSize, "elemCursor") && alloc(d.elemCells, 64 * elems, "elemCells");
+            ok = ok && alloc(d.elemBox, 2 * elems, "elemBox");
             ok = ok && alloc(d.datOwnerCount, owners, "datOwnerCount") && alloc(d.datOwnerStart, owners, "datOwnerStart");
             ok = ok && alloc(d.datEmit, owners, "datEmit") && alloc(d.datEmitStart, owners, "datEmitStart");
             ok = ok && alloc(d.datPairs, H.maxDatPairs, "planarDATPairs");
@@ -390,7 +401,7 @@ struct avbd_solver {
             std::vector<uint32_t> ones(nb, 0x3F800000u);
             ok = ok && upload(d.truncBits, ones, "planarDATT");
             ok = ok && alloc(d.ogcPrev, nb, "ogcPrev", true) && alloc(d.posNext, nb, "posNext", true) && alloc(d.angNext, nb, "angNext", true);
-            const uint32_t scanMax = std::max(std::max(H.elemHashSize, owners), H.numTris);
+            const uint32_t scanMax = std::max(std::max(2 * H.elemHashSize, owners), H.numTris);
             ok = ok && alloc(d.bigScanScratch, scan_large_scratch_words(scanMax), "scanScratchLarge");
         }
         std::vector<uint32_t> spB, rJ;
@@ -412,6 +423,7 @@ struct avbd_solver {
         std::memset(hostCounters, 0, sizeof(Counters));
         // Small scenes run their whole iteration loop in one thread block.
         smallSolve = z.numDynamicBodies <= 512 && !P.cloth;
+        tuneStage = tuning_applies() ? 0 : -1;
         if (cudaDeviceSynchronize() != cudaSuccess) { error = "device error during upload"; return AVBD_ERR_NO_DEVICE; }
         return AVBD_OK;
     }
@@ -448,10 +460,66 @@ struct avbd_solver {
         return failure == AVBD_FAIL_NONE ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
     }
 
+    // Lane-width autotuner.  Each static color's primal can run with 8, 16 or
+    // 32 lanes per body; the fold order is fixed, so every width computes the
+    // same floats and only speed differs (it depends on the color's body
+    // count and adjacency sizes).  The first three frames run eagerly, one
+    // width each, with events around every primal launch; each color then
+    // keeps its fastest width and the frame graphs are captured with it.
+    static constexpr uint32_t kTuneWidths[3] = {8, 16, 32};
+    int tuneStage = -1;                       // -1 off / done, 0..2 next width
+    double tuneMs[3][MAX_COLORS] = {};
+    std::vector<cudaEvent_t> tuneEvents;
+
+    bool tuning_applies() const { return !z.dynamicColoring && !smallSolve && H.staticUsedColors > 0; }
+
+    int tune_frame() {
+        const uint32_t colorBound = H.staticUsedColors;
+        const size_t need = 2 * (size_t)P.iterations * colorBound;
+        while (tuneEvents.size() < need) {
+            cudaEvent_t e;
+            if (!check(cudaEventCreate(&e), "event create")) return AVBD_ERR_RUNTIME_FAILURE;
+            tuneEvents.push_back(e);
+        }
+        uint32_t lanes[MAX_COLORS];
+        for (int c = 0; c < MAX_COLORS; c++) lanes[c] = kTuneWidths[tuneStage];
+        encode_frame_on((int)(frame & 1), launch, lanes, tuneEvents.data());
+        if (!check(cudaGetLastError(), "tuning frame")) return AVBD_ERR_RUNTIME_FAILURE;
+        frame++;
+        if (!check(cudaStreamSynchronize(launch), "tuning frame")) return AVBD_ERR_RUNTIME_FAILURE;
+        uint32_t k = 0;
+        for (uint32_t it = 0; it < P.iterations; it++)
+            for (uint32_t c = 0; c < colorBound; c++) {
+                if (H.colorCounts[c] == 0) continue;
+                float ms = 0.0f;
+                if (!check(cudaEventElapsedTime(&ms, tuneEvents[2 * k], tuneEvents[2 * k + 1]), "tuning timing"))
+                    return AVBD_ERR_RUNTIME_FAILURE;
+                tuneMs[tuneStage][c] += ms;
+                k++;
+            }
+        if (++tuneStage == 3) {
+            for (uint32_t c = 0; c < colorBound; c++) {
+                int best = 0;
+                for (int w = 1; w < 3; w++) if (tuneMs[w][c] < tuneMs[best][c]) best = w;
+                H.colorLanes[c] = kTuneWidths[best];
+            }
+            tuneStage = -1;
+            graphsValid = false;
+        }
+        return AVBD_OK;
+    }
+
     int step(uint32_t frames) {
         if (failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
+        uint32_t f = 0;
+        while (tuneStage >= 0 && f < frames) {
+            int rc = tune_frame();
+            if (rc != AVBD_OK) return rc;
+            f++;
+        }
+        if (f == frames) return AVBD_OK;
         if (!graphsValid && !build_graphs()) return AVBD_ERR_RUNTIME_FAILURE;
-        for (uint32_t f = 0; f < frames; f++) {
+        for (; f < frames; f++) {
             if (!check(cudaGraphLaunch(graph[frame & 1], launch), "graph launch")) return AVBD_ERR_RUNTIME_FAILURE;
             frame++;
             if (profiling) {
@@ -730,6 +798,7 @@ int avbd_get_profile(avbd_solver* s, avbd_profile* out) {
     if (!s->graphsValid && !s->build_graphs()) return AVBD_ERR_RUNTIME_FAILURE;
     *out = s->prof;
     out->kernels_per_frame = s->kernelsPerFrame;
+    for (int c = 0; c < 64; c++) out->color_lanes[c] = s->H.colorLanes[c];
     return AVBD_OK;
 }
 

@@ -842,15 +842,23 @@ __global__ void k_primal(const Params P, const DevPtrs d, uint32_t color, uint32
 // 0-7 then fold them in the 8-lane order — logical lane l takes entries
 // l, l+8, l+16, l+24 — applying exactly the additions the stamp would have
 // made, so every float is unchanged.  Entries whose terms do not fit the
-// shipped record (joints, springs, multi-contact manifolds) are stamped by
-// the logical lane itself during the fold.
+// shipped record (joints, multi-contact manifolds) are stamped by the
+// logical lane itself during the fold.
 // ---------------------------------------------------------------------------
+enum : uint32_t {
+    TERM_NONE = 0, TERM_TET = 1, TERM_MANIFOLD = 2, TERM_SERIAL = 3, TERM_SPRING = 4, TERM_MEMBRANE = 5,
+    TERM_BEND = 6, TERM_SOFT = 7
+};
 struct ParticleTerms {
-    float3 rhs;          // tet: gradient; manifold: J^T F
-    float3 a, b, c;      // tet: (G00, G11, G22), (G01, G02, G12), (dd, -, -); manifold: rows of J^T K J
-    uint32_t kind;       // 0 none, 1 tet, 2 one-contact manifold, 3 stamp serially
+    float3 rhs;          // the stamp's right-hand-side contribution
+    float3 a, b, c, e;   // tet: (G00, G11, G22), (G01, G02, G12), (dd, -, -); manifold: rows of J^T K J;
+                         // spring: n; membrane: g11, g22, g12, gtr; soft: n, t1, t2
+    float3 s;            // spring: (k, ft, -); membrane: (2 mu A, 4 mu A, lambda A); bend: (s k^2, -, -);
+                         // soft: (kN w^2, kT1 w^2, kT2 w^2)
+    uint32_t kind;       // TERM_*
 };
 
+template <bool CLOTH>
 __device__ __forceinline__ void particle_terms(const Params& P, const DevPtrs& d, uint32_t entry,
                                                uint32_t self, ParticleTerms& t) {
     const uint32_t kind = entry >> ADJ_KIND_SHIFT, idx = entry & ADJ_INDEX_MASK;
@@ -914,6 +922,114 @@ __device__ __forceinline__ void particle_terms(const Params& P, const DevPtrs& d
         t.c = M.r2;
         t.rhs = m3_mul(jLinT, F);
         t.kind = 2;
+    } else if (!CLOTH) {
+        return;
+    } else if (kind == FK_SPRING) {
+        // stamp_spring's linear block: outer(+-n, +-n) equals outer(n, n) bit for bit
+        const SpringGPU sp = d.springs[idx];
+        const uint32_t a = sp.header.x, b = sp.header.y;
+        float stiffness = sp.rA.w;
+        const float3 pA = xform(xyz(d.posLin[a]), d.posAng[a], xyz(sp.rA));
+        const float3 pB = xform(xyz(d.posLin[b]), d.posAng[b], xyz(sp.rB));
+        const float3 dd = pA - pB;
+        const float dLen = len3(dd);
+        t.kind = TERM_NONE;
+        if (dLen <= 1.0e-6f) return;
+        const float3 n = dd / dLen;
+        float f;
+        if (sp.header.z != 0) {
+            const float C = dLen - sp.rB.w - sp.dual.z * P.alpha;
+            stiffness = sp.dual.y;
+            f = stiffness * C + sp.dual.x;
+            if (f <= 0.0f) return;
+        } else {
+            f = stiffness * (dLen - sp.rB.w);
+        }
+        const float3 jLin = self == a ? n : -n;
+        t.rhs = jLin * f;
+        t.a = n;
+        t.s = mk3(stiffness, mx(f, 0.0f) / dLen, 0.0f);
+        t.kind = TERM_SPRING;
+    } else if (kind == FK_MEMBRANE) {
+        const MembraneGPU mb = d.membranes[idx];
+        const float3 x0 = xyz(d.posLin[mb.ids.x]), x1 = xyz(d.posLin[mb.ids.y]), x2 = xyz(d.posLin[mb.ids.z]);
+        const float muA = mb.mat.x, lamA = mb.mat.y;
+        const float3 d0 = x1 - x0, d1 = x2 - x0;
+        const float a = mb.dm.x, b = mb.dm.y, c = mb.dm.z, dm = mb.dm.w;
+        const float3 f1 = d0 * a + d1 * b;
+        const float3 f2 = d0 * c + d1 * dm;
+        const float E11 = 0.5f * (dot(f1, f1) - 1.0f);
+        const float E22 = 0.5f * (dot(f2, f2) - 1.0f);
+        const float E12 = 0.5f * dot(f1, f2);
+        const float trE = E11 + E22;
+        const float S11 = 2.0f * muA * E11 + lamA * trE;
+        const float S22 = 2.0f * muA * E22 + lamA * trE;
+        const float S12 = 2.0f * muA * E12;
+        const float3 p1 = f1 * S11 + f2 * S12;
+        const float3 p2 = f1 * S12 + f2 * S22;
+        float wx, wy;
+        if (self == mb.ids.y) { wx = a; wy = c; }
+        else if (self == mb.ids.z) { wx = b; wy = dm; }
+        else { wx = -a - b; wy = -c - dm; }
+        t.rhs = p1 * wx + p2 * wy;
+        t.a = f1 * wx;
+        t.b = f2 * wy;
+        t.c = (f2 * wx + f1 * wy) * 0.5f;
+        t.e = t.a + t.b;
+        t.s = mk3(2.0f * muA, 4.0f * muA, lamA);
+        t.kind = TERM_MEMBRANE;
+    } else if (kind == FK_BEND) {
+        const BendGPU bd = d.bends[idx];
+        const float sc = bd.mat.x;
+        const float3 m = xyz(d.posLin[bd.ids.x]) * bd.K.x + xyz(d.posLin[bd.ids.y]) * bd.K.y +
+                         xyz(d.posLin[bd.ids.z]) * bd.K.z + xyz(d.posLin[bd.ids.w]) * bd.K.w;
+        float k;
+        if (self == bd.ids.x) k = bd.K.x;
+        else if (self == bd.ids.y) k = bd.K.y;
+        else if (self == bd.ids.z) k = bd.K.z;
+        else k = bd.K.w;
+        t.rhs = m * (sc * k);
+        t.s = mk3(sc * k * k, 0.0f, 0.0f);
+        t.kind = TERM_BEND;
+    } else if (kind == FK_SOFT) {
+        const SoftContactGPU& sc = d.soft[idx];
+        float3 n, t1, t2, rAW;
+        bool rigidA;
+        const float3 C = soft_c(P, d, sc, n, t1, t2, rAW, rigidA);
+        float3 F = xyz(sc.penalty) * C + xyz(sc.lambda);
+        float kN = sc.penalty.x;
+        const float rT = sc.anchorA.x;
+        const uint32_t kindB = (__float_as_uint(sc.anchorA.w) >> SCF_KIND_SHIFT) & 3u;
+        if (rT > 0.0f && kindB != SC_RT && C.x < -0.5f * rT) {
+            const float dsep = mx(C.x + rT, 0.02f * rT);
+            const float kp = 0.25f * rT * rT * sc.penalty.x;
+            F.x = -kp / dsep + sc.lambda.x;
+            kN = kp / (dsep * dsep);
+        }
+        F.x = mn(F.x, 0.0f);
+        const float bounds = fabsf(F.x) * sc.normal.w;
+        const float fs = sqrtf(F.y * F.y + F.z * F.z);
+        if (fs > bounds && fs > 0.0f) {
+            const float r = bounds / fs;
+            F.y *= r;
+            F.z *= r;
+        }
+        int slot = -1;
+        if (sc.ids.x == self) slot = 0;
+        else if (sc.ids.y == self) slot = 1;
+        else if (sc.ids.z == self) slot = 2;
+        else if (sc.ids.w == self) slot = 3;
+        t.kind = TERM_NONE;
+        if (slot < 0) return;
+        if (slot == 0 && rigidA) { t.kind = TERM_SERIAL; return; }
+        const float w = slot == 0 ? sc.weights.x : (slot == 1 ? sc.weights.y : (slot == 2 ? sc.weights.z : sc.weights.w));
+        const float w2 = w * w;
+        t.a = n;
+        t.b = t1;
+        t.c = t2;
+        t.s = mk3(kN * w2, sc.penalty.y * w2, sc.penalty.z * w2);
+        t.rhs = (n * F.x + t1 * F.y + t2 * F.z) * w;
+        t.kind = TERM_SOFT;
     }
 }
 
@@ -974,7 +1090,7 @@ __device__ __forceinline__ float3 solve3x3_particle(const M3& a, float3 b) {
 // chosen per color from its bodies' adjacency sizes).  Lane p of a group
 // evaluates entry base + p; logical lane l < 8 then folds entries
 // base + l, base + l + 8, ... in order.  Any LANES gives the same floats.
-template <int LANES, bool GENERAL>
+template <int LANES, bool GENERAL, bool CLOTH>
 __global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevPtrs d, uint32_t color,
                                                       uint32_t count) {
     constexpr int GROUPS = 32 / LANES;
@@ -1007,7 +1123,7 @@ __global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevP
         uint32_t entry = 0;
         if (k < cnt) {
             entry = v.at(k);
-            particle_terms(P, d, entry, body, t);
+            particle_terms<CLOTH>(P, d, entry, body, t);
         }
 #pragma unroll
         for (int j = 0; j < LANES / 8; j++) {
@@ -1028,6 +1144,12 @@ __global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevP
                       __shfl_sync(mask, t.b.z, src, LANES));
             u.c = mk3(__shfl_sync(mask, t.c.x, src, LANES), __shfl_sync(mask, t.c.y, src, LANES),
                       __shfl_sync(mask, t.c.z, src, LANES));
+            if (CLOTH) {
+                u.e = mk3(__shfl_sync(mask, t.e.x, src, LANES), __shfl_sync(mask, t.e.y, src, LANES),
+                          __shfl_sync(mask, t.e.z, src, LANES));
+                u.s = mk3(__shfl_sync(mask, t.s.x, src, LANES), __shfl_sync(mask, t.s.y, src, LANES),
+                          __shfl_sync(mask, t.s.z, src, LANES));
+            }
             e = __shfl_sync(mask, entry, src, LANES);
             }
             if (lane < 8) {
@@ -1039,7 +1161,26 @@ __global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevP
                 } else if (u.kind == 2u) {
                     acc.lhs = m3_add(acc.lhs, M3{u.a, u.b, u.c});
                     acc.rhs += u.rhs;
-                } else if (GENERAL && u.kind == 3u) {
+                } else if (CLOTH && u.kind == TERM_MEMBRANE) {
+                    acc.rhs += u.rhs;
+                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.a, u.a), u.s.x));
+                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.b, u.b), u.s.x));
+                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.c, u.c), u.s.y));
+                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.e, u.e), u.s.z));
+                } else if (CLOTH && u.kind == TERM_BEND) {
+                    acc.rhs += u.rhs;
+                    acc.lhs = m3_add(acc.lhs, m3_diag(s3(u.s.x)));
+                } else if (CLOTH && u.kind == TERM_SPRING) {
+                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.a, u.a), u.s.x));
+                    acc.rhs += u.rhs;
+                    if (u.s.y > 0.0f)
+                        acc.lhs = m3_add(acc.lhs, m3_add(m3_diag(s3(u.s.y)), m3_scale(m3_outer(u.a, u.a), -u.s.y)));
+                } else if (CLOTH && u.kind == TERM_SOFT) {
+                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.a, u.a), u.s.x));
+                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.b, u.b), u.s.y));
+                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.c, u.c), u.s.z));
+                    acc.rhs += u.rhs;
+                } else if (GENERAL && u.kind != TERM_NONE) {
                     stamp_entry_particle(P, d, e, body, &acc);
                 }
             }
@@ -1067,14 +1208,14 @@ __global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevP
     d.posLin[body] = mk4(xyz(pl) + dxLin, mass);
 }
 
-template <bool GENERAL>
+template <bool GENERAL, bool CLOTH>
 static void launch_primal_group(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count,
                                 uint32_t lanes, cudaStream_t st) {
     const int T = 128;
     const uint32_t blocks = (count * lanes + T - 1) / T;
-    if (lanes <= 8) launch_pdl(k_primal_group<8, GENERAL>, blocks, T, st, P, d, color, count);
-    else if (lanes <= 16) launch_pdl(k_primal_group<16, GENERAL>, blocks, T, st, P, d, color, count);
-    else launch_pdl(k_primal_group<32, GENERAL>, blocks, T, st, P, d, color, count);
+    if (lanes <= 8) launch_pdl(k_primal_group<8, GENERAL, CLOTH>, blocks, T, st, P, d, color, count);
+    else if (lanes <= 16) launch_pdl(k_primal_group<16, GENERAL, CLOTH>, blocks, T, st, P, d, color, count);
+    else launch_pdl(k_primal_group<32, GENERAL, CLOTH>, blocks, T, st, P, d, color, count);
 }
 
 void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color, uint32_t count,
@@ -1088,8 +1229,9 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
         // the grouped kernel needs the color's body count on the host
         const uint32_t lanes_ = lanes < 8 ? 8 : (lanes > 32 ? 32 : lanes);
         const uint32_t w = lanes_ <= 8 ? 8 : (lanes_ <= 16 ? 16 : 32);
-        if (z.particleFastPath) launch_primal_group<false>(P, d, color, upper, w, st);
-        else launch_primal_group<true>(P, d, color, upper, w, st);
+        if (z.particleFastPath) launch_primal_group<false, false>(P, d, color, upper, w, st);
+        else if (P.cloth) launch_primal_group<true, true>(P, d, color, upper, w, st);
+        else launch_primal_group<true, false>(P, d, color, upper, w, st);
     }
 }
 

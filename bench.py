@@ -14,6 +14,12 @@ metric through the C ABI with host buffers (positions uploaded from pinned
 memory and read back every step).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload soft-cube|cloth-sphere]
+
+`--workload cloth-sphere` measures the cloth configuration instead: a
+256 x 256 sheet of 2 m (65,536 particles, 130,050 StVK membranes, Bergou
+bends, hard structural rods), two pinned corners, draped over a static
+sphere, Planar-DAT truncation, dt = 1/120, 30 iterations.
 
 Under torchrun (N > 1) every rank runs an independent replica of the scene
 ("replicas only": the coupled scene has no natural partition); time is the
@@ -35,11 +41,17 @@ for _p in (ROOT, os.path.join(ROOT, "avbd-metal_b200")):
         sys.path.insert(0, _p)
 
 METRIC = "vertex-steps/s at matched AL residual: plain vs learned warm-start, 1 B200"
-WORKLOAD = ("soft-cube-24: 24^3-vertex lattice of a 1 m cube, 13,824 particles, 60,835 "
-            "Stable Neo-Hookean tets, E=1e5 Pa, nu=0.4, rho=1000, friction 0.4, dt=1/60, "
-            "20 iterations, static palette, plain warm start")
-SCENE_SEED = 2
-N_LATTICE = 24
+WORKLOADS = {
+    "soft-cube": ("soft-cube-24: 24^3-vertex lattice of a 1 m cube, 13,824 particles, 60,835 "
+                  "Stable Neo-Hookean tets, E=1e5 Pa, nu=0.4, rho=1000, friction 0.4, dt=1/60, "
+                  "20 iterations, static palette, plain warm start"),
+    "cloth-sphere": ("cloth-sphere-256: 256^2-vertex sheet of 2 m (65,536 particles, 130,050 StVK "
+                     "membranes mu=lambda=1e4, Bergou bending 1e-3, hard structural rods), contact "
+                     "radius 2e-3 m, two pinned corners, static sphere r=0.5 m, Planar-DAT, dt=1/120, "
+                     "30 iterations, plain warm start"),
+}
+WORKLOAD_KEY = "soft-cube"
+WORKLOAD = WORKLOADS[WORKLOAD_KEY]
 
 
 def parse():
@@ -50,12 +62,18 @@ def parse():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="bound on the CPU baseline sample")
-    return ap.parse_args()
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="soft-cube")
+    args = ap.parse_args()
+    global WORKLOAD_KEY, WORKLOAD
+    WORKLOAD_KEY, WORKLOAD = args.workload, WORKLOADS[args.workload]
+    return args
 
 
 def make_scene():
     from avbd_b200 import demos
-    return demos.soft_cube_scene(seed=SCENE_SEED, n=N_LATTICE)
+    if WORKLOAD_KEY == "cloth-sphere":
+        return demos.cloth_sphere_scene(seed=3, n=256)
+    return demos.soft_cube_scene(seed=2, n=24)
 
 
 def dynamic_vertices(scene):
@@ -173,7 +191,8 @@ def measured_peaks():
 
 def ncu_traffic_per_launch():
     """DRAM bytes per primal launch from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "k_primal_soft_cube_24.md")
+    name = "k_primal_soft_cube_24.md" if WORKLOAD_KEY == "soft-cube" else "k_primal_cloth_sphere_256.md"
+    path = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(path):
         return None
     m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
@@ -185,14 +204,20 @@ def primal_bytes_per_iteration(solver, scene):
     per body 16 B position read + 16 B write + 16 B inertial target + 4 B
     color-list entry + 16 B static adjacency segment + 8 B contact segment,
     4 B per adjacency entry, one 64 B tet record per tet, 64 B manifold
-    header/basis + 80 B per active contact."""
+    header/basis + 80 B per active contact; cloth adds 48 B per membrane and
+    bend, 64 B per spring, 112 B per element contact."""
     import numpy as np
     nb = dynamic_vertices(scene) + sum(1 for b in scene.bodies if not b.is_particle and b.is_dynamic)
     adj = int(solver.debug_read("ADJ_COUNT", np.uint32).sum())
     man = solver.debug_read("MANIFOLDS", np.uint32).reshape(-1, 176)
     contacts = int(man[:, 2].sum()) if man.size else 0
     active = int((man[:, 2] > 0).sum()) if man.size else 0
-    return nb * (16 + 16 + 16 + 4 + 16 + 8) + 4 * adj + 64 * len(scene.tets) + 64 * active + 80 * contacts
+    cloth = 0
+    if scene.tris:
+        cloth = (48 * (solver.debug_read("MEMBRANES").size // 48 + solver.debug_read("BENDS").size // 48)
+                 + 64 * len(scene.springs) + solver.debug_read("SOFT").size)
+    return (nb * (16 + 16 + 16 + 4 + 16 + 8) + 4 * adj + 64 * len(scene.tets) + 64 * active + 80 * contacts
+            + cloth)
 
 
 # ---------------------------------------------------------------------------
@@ -279,7 +304,7 @@ def run_ours(args, world, rank, local):
         thr = host_threads()
         cv, frames, secs, _ = cpu_run(args.cpu_seconds, thr)
         cpu = {"value": cv, "unit": "vertex-steps/s", "cores": thr, "kind": "port",
-               "sample": f"soft-cube-24, frames 2-{frames + 1} after a 1-frame warm-up, "
+               "sample": f"{WORKLOAD.split(':')[0]}, frames 2-{frames + 1} after a 1-frame warm-up, "
                          f"{frames} frames in {secs:.1f} s, oracle with {thr} OpenMP threads"}
     if rank == 0:
         line = {
@@ -288,8 +313,11 @@ def run_ours(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded SplitMix64 scene)",
             "config": {"workload": WORKLOAD, "vertices_per_step": nv, "tets": len(scene.tets),
+                       "triangles": len(scene.tris),
                        "iterations": scene.settings.iterations,
                        "colors": int(counters.used_colors),
+                       "lanes_per_body": prof["color_lanes"][:int(counters.used_colors)],
+                       "lane_autotune": "fastest of 8/16/32 lanes per color, timed on the first 3 frames",
                        "warm_start": "plain (gamma warm start); learned warm start not in this build",
                        "parallelism": f"replicas x{world}",
                        "l2": "flushed between timed steps (256 MiB device write, untimed)",
@@ -330,7 +358,7 @@ def run_reference(args, world, rank):
             break
     secs = time.perf_counter() - t0
     value = nv * frames / secs
-    sample = (f"soft-cube-24, {frames} of {args.steps} requested frames after "
+    sample = (f"{WORKLOAD.split(':')[0]}, {frames} of {args.steps} requested frames after "
               f"{min(args.warmup, 3)} warm-up frames, bounded to {budget:.0f} s; the reference's "
               "solver restated in C++ (Swift/Metal cannot run here), OpenMP over bodies of a color")
     line = {

@@ -341,6 +341,8 @@ typedef struct avbd_profile {
     uint64_t kernels_per_frame;   /* kernel nodes in one frame's graph      */
     double stage_ms[16];          /* summed GPU time per stage              */
     uint64_t stage_launches[16];  /* kernel launches per stage              */
+    uint32_t color_lanes[64];     /* lanes per body of each static color's
+                                   * primal, as chosen by the autotuner      */
 } avbd_profile;
 int avbd_set_profiling(avbd_solver* solver, int enabled);
 int avbd_get_profile(avbd_solver* solver, avbd_profile* out);
