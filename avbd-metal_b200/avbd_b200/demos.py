@@ -270,6 +270,63 @@ def cloth_sphere_scene(seed: int = 3, n: int = 256, iterations: int = 30,
     return s
 
 
+def batched_worlds_scene(worlds: int = 4096, seed: int = 4, pitch: float = 1.6, first_world: int = 0):
+    """Batched articulated worlds packed into one scene, one collision group
+    per world (the reference's vector-environment layout,
+    RL/PushTEnv.swift:114-180): each world is a planar serial chain of 3-7
+    box links (0.25 x 0.06 x 0.06 m, density 500) lying on the ground plane,
+    joined by hinges about +z with implicit position-PD motors (effort 2 N m,
+    kp 50, kd 1), the first link hinged to the world, plus a welded T block
+    (bar 0.2 x 0.05 x 0.05 m, stem 0.05 x 0.15 x 0.05 m) at a seeded pose;
+    friction 0.5, dt 1/60, 8 iterations.  Returns (scene, motor joint ids,
+    world offsets): offsets[e] is the first body of world e (ragged).
+
+    World w draws from its own stream SplitMix64((seed << 32) + w), so a shard
+    [first_world, first_world + worlds) builds exactly the worlds that a
+    single scene of all worlds would contain."""
+    s = PhysicsScene("batched-worlds")
+    cols = int(math.ceil(math.sqrt(worlds)))
+    rows = int(math.ceil(worlds / cols))
+    hx, hy = 0.5 * (cols - 1) * pitch, 0.5 * (rows - 1) * pitch
+    s.add_body((2 * (hx + pitch), 2 * (hy + pitch), 2.0), 0.0, 0.5, (0.0, 0.0, -1.0))
+    motors, offsets = [], []
+    link = (0.25, 0.06, 0.06)
+    for e in range(worlds):
+        rng = SplitMix64((seed << 32) + first_world + e)
+        g = e + 1
+        cx, cy = (e % cols) * pitch - hx, (e // cols) * pitch - hy
+        offsets.append(len(s.bodies))
+        n = 3 + int(rng.next_float() * 5)
+        base = (cx - 0.6, cy - 0.3, 0.03)
+        prev = -1
+        for k in range(n):
+            pos = (base[0] + 0.25 * k + 0.125, base[1], base[2])
+            b = s.add_body(link, 500.0, 0.5, pos, collision_group=g)
+            anchor_a = (base[0], base[1], base[2]) if prev < 0 else (0.125, 0.0, 0.0)
+            motors.append(len(s.joints))
+            s.add_joint(SceneJoint(prev, b, anchor_a, (-0.125, 0.0, 0.0), stiffness_ang=float("inf"),
+                                   hinge_axis=(0.0, 0.0, 1.0), motor_torque=2.0, motor_stiffness=50.0,
+                                   motor_damping=1.0))
+            prev = b
+        yaw = (rng.next_float() - 0.5) * 2.0 * math.pi
+        qz = (0.0, 0.0, math.sin(0.5 * yaw), math.cos(0.5 * yaw))
+        cyaw, syaw = math.cos(yaw), math.sin(yaw)
+        bc = (cx + 0.25 + 0.2 * rng.next_float(), cy + 0.25 + 0.2 * rng.next_float(), 0.025)
+
+        def rot(v):
+            return (cyaw * v[0] - syaw * v[1], syaw * v[0] + cyaw * v[1], v[2])
+        ob, os_ = rot((0.0, 0.05, 0.0)), rot((0.0, -0.05, 0.0))
+        bar = s.add_body((0.2, 0.05, 0.05), 500.0, 0.5, (bc[0] + ob[0], bc[1] + ob[1], bc[2]), rotation=qz,
+                         collision_group=g)
+        stem = s.add_body((0.05, 0.15, 0.05), 500.0, 0.5, (bc[0] + os_[0], bc[1] + os_[1], bc[2]), rotation=qz,
+                          collision_group=g)
+        s.add_joint(SceneJoint(bar, stem, (0.0, -0.025, 0.0), (0.0, 0.075, 0.0), stiffness_ang=float("inf")))
+        s.add_joint(SceneJoint(bar, stem, (0.0, 0.0, 0.0), (0.0, 0.0, 0.0), 0.0, 0.0))
+    st = s.settings
+    st.dt, st.iterations, st.gravity = 1.0 / 60.0, 8, -9.81
+    return s, motors, offsets
+
+
 def single_tet_scene() -> PhysicsScene:
     """SoftBodyTests.testTetVolumePreservation (SoftBodyTests.swift:53-69)."""
     s = PhysicsScene("tet1")

@@ -106,6 +106,8 @@ void launch_dynamic_coloring(const Params& P, const DevPtrs& d, const Sizes& z, 
 // when known on the host (static palette), else 0xFFFFFFFF (read on device)
 void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color,
                          uint32_t count, uint32_t lanes, cudaStream_t st);
+// dynamic coloring: colors [first, 64) in one block, after the per-color launches
+void launch_primal_tail(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t first, cudaStream_t st);
 // every iteration of a small scene in one thread block
 void launch_solve_small(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t colorBound,
                         cudaStream_t st);

@@ -85,6 +85,11 @@ struct avbd_solver {
     uint64_t kernelsPerFrame = 0;
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graphsValid = false;
+    // Dynamic coloring: the frame graph launches this many colors one by one
+    // and a single-block tail kernel takes the rest.  It grows (and the graphs
+    // are re-captured) when a retired frame used more colors.
+    uint32_t colorLaunchBound = 8;
+    bool colorBoundFitted = false;
     uint64_t frame = 0;
     int failure = AVBD_FAIL_NONE;
     std::string error;
@@ -207,10 +212,10 @@ struct avbd_solver {
             mark(AVBD_STAGE_COLORING);
             launch_dynamic_coloring(P, f, z, st);
         }
-        const uint32_t colorBound = z.dynamicColoring ? (uint32_t)MAX_COLORS : H.staticUsedColors;
+        const uint32_t colorBound = z.dynamicColoring ? colorLaunchBound : H.staticUsedColors;
         if (smallSolve) {
             mark(AVBD_STAGE_PRIMAL);
-            launch_solve_small(P, f, z, colorBound, st);
+            launch_solve_small(P, f, z, z.dynamicColoring ? (uint32_t)MAX_COLORS : H.staticUsedColors, st);
         } else {
             for (uint32_t it = 0; it < P.iterations; it++) {
                 for (uint32_t c = 0; c < colorBound; c++) {
@@ -226,6 +231,7 @@ struct avbd_solver {
                         launch_dat_color(P, f, z, c, count, st);
                     }
                 }
+                if (z.dynamicColoring) launch_primal_tail(P, f, z, colorLaunchBound, st);
                 mark(AVBD_STAGE_DUAL);
                 launch_dual(P, f, z, st);
             }
@@ -239,7 +245,7 @@ struct avbd_solver {
     }
 
     int events_needed() const {
-        const uint32_t colorBound = z.dynamicColoring ? (uint32_t)MAX_COLORS : H.staticUsedColors;
+        const uint32_t colorBound = z.dynamicColoring ? colorLaunchBound : H.staticUsedColors;
         return 20 + (int)(P.iterations * (2 * colorBound + 1));
     }
 
@@ -434,6 +440,16 @@ struct avbd_solver {
         if (!check(cudaStreamSynchronize(launch), "frame execution")) return AVBD_ERR_RUNTIME_FAILURE;
         if (!check(cudaMemcpy(hostLatch, d.failureLatch, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost), "latch readback"))
             return AVBD_ERR_RUNTIME_FAILURE;
+        if (z.dynamicColoring && hostLatch[3] > 0) {
+            // first retirement: fit the bound to the palette seen so far
+            // (two colors of headroom); later frames only grow it
+            const uint32_t want = std::min<uint32_t>(MAX_COLORS, hostLatch[3] + 2);
+            if (want > colorLaunchBound || (!colorBoundFitted && want < colorLaunchBound)) {
+                colorLaunchBound = want;
+                graphsValid = false;
+            }
+            colorBoundFitted = true;
+        }
         if (hostLatch[0] != 0 && failure == AVBD_FAIL_NONE) {
             failure = (int)hostLatch[0];
             char buf[160];

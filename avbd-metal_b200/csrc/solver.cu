@@ -65,7 +65,7 @@ static uint32_t stride_blocks(uint32_t upper, int threads) {
 __device__ __forceinline__ float twist_angle(float4 qAr, float4 qB, float3 axis) {
     float4 r = q_mul(q_inv(qAr), qB);
     if (r.w < 0.0f) r = neg4(r);
-    return 2.0f * atan2f(dot(xyz(r), axis), r.w);
+    return 2.0f * atan2_series(dot(xyz(r), axis), r.w);
 }
 
 __global__ void k_warmstart_constraints(const Params P, const DevPtrs d, uint32_t nJ, uint32_t nS) {
@@ -1419,6 +1419,28 @@ void launch_solve_small(const Params& P, const DevPtrs& d, const Sizes& z, uint3
     k_solve_small<<<1, 256, 0, st>>>(P, d, z, colorBound);
 }
 
+// Dynamic coloring: the frame graph launches colors [0, first) one by one
+// and this single block handles any colors from `first` up (rare: a frame
+// that needs more colors than the graph was built for), color after color
+// with a block barrier between them — the same per-body solve in the same
+// color order.
+__global__ void __launch_bounds__(256) k_primal_tail(const Params P, const DevPtrs d, uint32_t first) {
+    const uint32_t groups = blockDim.x >> 3;
+    const uint32_t group = threadIdx.x >> 3, lane = threadIdx.x & 7u;
+    const unsigned mask = 0xFFu << (threadIdx.x & 24u);
+    for (uint32_t c = first; c < (uint32_t)MAX_COLORS; c++) {
+        const uint32_t s = d.colorStart[c], e = d.colorStart[c + 1];
+        if (s == e) continue;                    // block-uniform
+        for (uint32_t slot = group; s + slot < e; slot += groups)
+            primal_body(P, d, d.colorList[s + slot], lane, mask);
+        __syncthreads();
+    }
+}
+
+void launch_primal_tail(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t first, cudaStream_t st) {
+    if (first < (uint32_t)MAX_COLORS) k_primal_tail<<<1, 256, 0, st>>>(P, d, first);
+}
+
 // ---------------------------------------------------------------------------
 // BDF1 velocity finalize (40_solver.metal:2108-2147)
 // ---------------------------------------------------------------------------
@@ -1570,6 +1592,8 @@ __global__ void k_frame_end(const Params P, const DevPtrs d, const Sizes z, floa
             d.failureLatch[1] = frame;
             d.failureLatch[2] = detail;
         }
+        // peak dynamic palette size, read by the host to size the color launches
+        if (z.dynamicColoring && c->usedColors > d.failureLatch[3]) d.failureLatch[3] = c->usedColors;
     }
 }
 

@@ -20,6 +20,9 @@ memory and read back every step).
 256 x 256 sheet of 2 m (65,536 particles, 130,050 StVK membranes, Bergou
 bends, hard structural rods), two pinned corners, draped over a static
 sphere, Planar-DAT truncation, dt = 1/120, 30 iterations.
+`--workload batched-worlds` measures 4096 independent articulated worlds
+per GPU (body-steps/s; new motor targets every step); under torchrun each
+rank owns its own 4096 worlds (weak scaling, no data-path collective).
 
 Under torchrun (N > 1) every rank runs an independent replica of the scene
 ("replicas only": the coupled scene has no natural partition); time is the
@@ -49,7 +52,12 @@ WORKLOADS = {
                      "membranes mu=lambda=1e4, Bergou bending 1e-3, hard structural rods), contact "
                      "radius 2e-3 m, two pinned corners, static sphere r=0.5 m, Planar-DAT, dt=1/120, "
                      "30 iterations, plain warm start"),
+    "batched-worlds": ("batched-worlds-4096: 4096 worlds (one collision group each) of a planar 3-7 link "
+                       "hinge chain with implicit PD motors (targets U(+-0.5 rad) every step) and a welded "
+                       "T block on a plane, friction 0.5, dt=1/60, 8 iterations, dynamic coloring; "
+                       "worlds sharded across ranks"),
 }
+MOTORS = []
 WORKLOAD_KEY = "soft-cube"
 WORKLOAD = WORKLOADS[WORKLOAD_KEY]
 
@@ -69,15 +77,41 @@ def parse():
     return args
 
 
-def make_scene():
+def make_scene(rank=0):
     from avbd_b200 import demos
     if WORKLOAD_KEY == "cloth-sphere":
         return demos.cloth_sphere_scene(seed=3, n=256)
+    if WORKLOAD_KEY == "batched-worlds":
+        scene, motors, _ = demos.batched_worlds_scene(worlds=4096, seed=4, first_world=4096 * rank)
+        MOTORS[:] = motors
+        return scene
     return demos.soft_cube_scene(seed=2, n=24)
 
 
+class MotorTargets:
+    """Per-step joint targets U(+-0.5 rad) of the batched workload, drawn
+    ahead of the timed region (host arrays; uploaded by set_motor_targets)."""
+
+    def __init__(self, steps, seed=11):
+        import numpy as np
+        rng = np.random.default_rng(seed)
+        self.ids = np.array(MOTORS, np.uint32)
+        self.t = rng.uniform(-0.5, 0.5, size=(max(1, steps), len(MOTORS))).astype(np.float32) if MOTORS else None
+
+    def apply(self, solver, i):
+        if self.t is not None:
+            solver.set_motor_targets(self.ids, self.t[i % len(self.t)])
+
+
 def dynamic_vertices(scene):
-    return sum(1 for b in scene.bodies if b.is_particle and b.is_dynamic)
+    """Units of the metric: dynamic particles (vertex-steps), or dynamic
+    rigid bodies for a rigid-only scene (body-steps)."""
+    n = sum(1 for b in scene.bodies if b.is_particle and b.is_dynamic)
+    return n if n else sum(1 for b in scene.bodies if b.is_dynamic)
+
+
+def unit():
+    return "body-steps/s" if WORKLOAD_KEY == "batched-worlds" else "vertex-steps/s"
 
 
 def host_threads():
@@ -119,10 +153,13 @@ def cpu_run(seconds, threads, warmup=1, max_frames=200):
     scene = make_scene()
     nv = dynamic_vertices(scene)
     o = oracle.OracleSolver(scene, threads=threads)
-    if warmup:
-        o.step(warmup)
+    targets = MotorTargets(max_frames + warmup)
+    for i in range(warmup):
+        targets.apply(o, i)
+        o.step(1)
     frames, t0 = 0, time.perf_counter()
     while frames < max_frames:
+        targets.apply(o, warmup + frames)
         o.step(1)
         frames += 1
         if time.perf_counter() - t0 >= seconds:
@@ -216,8 +253,10 @@ def primal_bytes_per_iteration(solver, scene):
     if scene.tris:
         cloth = (48 * (solver.debug_read("MEMBRANES").size // 48 + solver.debug_read("BENDS").size // 48)
                  + 64 * len(scene.springs) + solver.debug_read("SOFT").size)
-    return (nb * (16 + 16 + 16 + 4 + 16 + 8) + 4 * adj + 64 * len(scene.tets) + 64 * active + 80 * contacts
-            + cloth)
+    rigid = sum(1 for b in scene.bodies if not b.is_particle and b.is_dynamic)
+    joints = sum(1 for j in scene.joints if j.stiffness_lin != 0 or j.stiffness_ang != 0 or j.motor_torque != 0)
+    return (nb * (16 + 16 + 16 + 4 + 16 + 8) + 48 * rigid + 4 * adj + 64 * len(scene.tets) + 64 * active
+            + 80 * contacts + 224 * joints + cloth)
 
 
 # ---------------------------------------------------------------------------
@@ -228,15 +267,18 @@ def run_ours(args, world, rank, local):
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    scene = make_scene()
+    scene = make_scene(rank)
     nv = dynamic_vertices(scene)
     solver = GPUSolver(scene, device=local)
+    targets = MotorTargets(args.steps + args.warmup + 400)
     stream = torch.cuda.Stream(device=dev)
     solver.set_stream(stream.cuda_stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
 
     with torch.cuda.stream(stream):
-        solver.step(args.warmup)
+        for i in range(args.warmup):
+            targets.apply(solver, i)
+            solver.step(1)
         solver.synchronize()
         K = args.steps
         starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
@@ -250,6 +292,7 @@ def run_ours(args, world, rank, local):
         time.sleep(0.2)
         for i in range(K):
             flush.zero_()
+            targets.apply(solver, args.warmup + i)    # input staging, before the timed step
             starts[i].record(stream)
             solver.step(1)
             ends[i].record(stream)
@@ -271,21 +314,25 @@ def run_ours(args, world, rank, local):
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for _ in range(E):
+        for i in range(E):
             solver.set_positions(xyz)            # H2D: n x 12 B from pinned memory
+            targets.apply(solver, args.warmup + K + i)
             solver.step(1)
             solver.read_positions_into(pos4)     # D2H: n x 16 B, synchronising read
             xyz[:] = pos4[:, :3]
         e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
-        e2e = {"value": world * nv * E / e2e_s, "unit": "vertex-steps/s",
-               "h2d_bytes_per_step": int(xyz.nbytes), "d2h_bytes_per_step": int(pos4.nbytes),
+        h2d = int(xyz.nbytes) + (targets.t.shape[1] * 8 if targets.t is not None else 0)
+        e2e = {"value": world * nv * E / e2e_s, "unit": unit(),
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(pos4.nbytes),
                "steps": E}
 
         # roofline of the dominant kernel (the per-color primal), from a
         # profiled pass with CUDA events around every primal launch
         prof_frames = 20
         solver.set_profiling(True)
-        solver.step(prof_frames)
+        for i in range(prof_frames):
+            targets.apply(solver, i)
+            solver.step(1)
         prof = solver.profile()
         solver.set_profiling(False)
         bytes_iter = primal_bytes_per_iteration(solver, scene)
@@ -303,12 +350,12 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1:
         thr = host_threads()
         cv, frames, secs, _ = cpu_run(args.cpu_seconds, thr)
-        cpu = {"value": cv, "unit": "vertex-steps/s", "cores": thr, "kind": "port",
+        cpu = {"value": cv, "unit": unit(), "cores": thr, "kind": "port",
                "sample": f"{WORKLOAD.split(':')[0]}, frames 2-{frames + 1} after a 1-frame warm-up, "
                          f"{frames} frames in {secs:.1f} s, oracle with {thr} OpenMP threads"}
     if rank == 0:
         line = {
-            "metric": METRIC, "value": value, "unit": "vertex-steps/s", "n_gpus": world,
+            "metric": METRIC, "value": value, "unit": unit(), "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": dev_ms / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded SplitMix64 scene)",
@@ -319,7 +366,8 @@ def run_ours(args, world, rank, local):
                        "lanes_per_body": prof["color_lanes"][:int(counters.used_colors)],
                        "lane_autotune": "fastest of 8/16/32 lanes per color, timed on the first 3 frames",
                        "warm_start": "plain (gamma warm start); learned warm start not in this build",
-                       "parallelism": f"replicas x{world}",
+                       "parallelism": (f"world shards x{world}" if WORKLOAD_KEY == "batched-worlds"
+                                       else f"replicas x{world}"),
                        "l2": "flushed between timed steps (256 MiB device write, untimed)",
                        "timing": "CUDA events on the solver stream per step, max over ranks"},
             "clocks": clock, "e2e": e2e,
@@ -349,9 +397,13 @@ def run_reference(args, world, rank):
     scene = make_scene()
     nv = dynamic_vertices(scene)
     o = oracle.OracleSolver(scene, threads=thr)
-    o.step(min(args.warmup, 3))
+    targets = MotorTargets(args.steps + 3)
+    for i in range(min(args.warmup, 3)):
+        targets.apply(o, i)
+        o.step(1)
     frames, t0 = 0, time.perf_counter()
     while frames < args.steps:
+        targets.apply(o, 3 + frames)
         o.step(1)
         frames += 1
         if time.perf_counter() - t0 >= budget:
@@ -362,14 +414,14 @@ def run_reference(args, world, rank):
               f"{min(args.warmup, 3)} warm-up frames, bounded to {budget:.0f} s; the reference's "
               "solver restated in C++ (Swift/Metal cannot run here), OpenMP over bodies of a color")
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "vertex-steps/s",
+        "impl": "reference", "metric": METRIC, "value": value, "unit": unit(),
         "n_gpus": world, "steps": frames, "warmup": min(args.warmup, 3),
         "ms_per_step": secs / frames * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64 scene)",
         "config": {"workload": WORKLOAD, "vertices_per_step": nv, "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": "vertex-steps/s", "cores": thr, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": unit(), "cores": thr, "kind": "port",
                          "sample": sample},
-        "e2e": {"value": value, "unit": "vertex-steps/s", "h2d_bytes_per_step": 0,
+        "e2e": {"value": value, "unit": unit(), "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

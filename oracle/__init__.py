@@ -53,6 +53,8 @@ def lib():
         _lib.oracle_debug_buffer_size.argtypes = [C.c_void_p, C.c_int]
         _lib.oracle_debug_buffer_size.restype = C.c_size_t
         _lib.oracle_debug_read.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
+        _lib.oracle_atan2.argtypes = [C.c_float, C.c_float]
+        _lib.oracle_atan2.restype = C.c_float
     return _lib
 
 

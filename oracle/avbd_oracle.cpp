@@ -1003,7 +1003,7 @@ void Solver::map_rebuild() {
 static float twist_angle(F4 qAr, F4 qB, F3 axis) {
     F4 r = q_mul(q_inv(qAr), qB);
     if (r.w < 0.0f) r = -r;
-    return 2.0f * std::atan2(dot(xyz(r), axis), r.w);
+    return 2.0f * atan2_series(dot(xyz(r), axis), r.w);
 }
 
 void Solver::warmstart_joints() {
@@ -1877,6 +1877,7 @@ int oracle_set_motor_targets(void* h, const uint32_t* ids, uint32_t n, const flo
     }
     return AVBD_OK;
 }
+float oracle_atan2(float y, float x) { return oracle::atan2_series(y, x); }
 int oracle_max_constraint_error(void* h, float* out) { *out = static_cast<Solver*>(h)->max_constraint_error(); return AVBD_OK; }
 int oracle_get_counters(void* h, avbd_counters* out) {
     Solver* s = static_cast<Solver*>(h);

@@ -189,6 +189,40 @@ static inline void orthonormal(F3 n, F3& t1, F3& t2) {
     t2 = cross(n, t1);
 }
 
+// atan2 evaluated with a fixed float32 operation sequence, so host and device
+// agree bit for bit (the libm and CUDA atan2f may differ in the last ulp).
+// Method: reduce to a = min/max in [0, 1]; for a > tan(pi/12) use
+// atan(a) = pi/6 + atan((sqrt(3) a - 1) / (sqrt(3) + a)) (Cody & Waite's
+// argument reduction), leaving |z| <= tan(pi/12) where the Maclaurin series
+// z - z^3/3 + ... + z^13/13 is exact to float32; then undo the octant and
+// quadrant symmetries.  Accuracy: a few ulp.
+static inline float atan2_series(float y, float x) {
+    if (y != y || x != x) return x + y;
+    const float ax = std::fabs(x), ay = std::fabs(y);
+    const float hi = ax > ay ? ax : ay, lo = ax > ay ? ay : ax;
+    float r;
+    if (hi == 0.0f) {
+        r = 0.0f;
+    } else {
+        const float a = lo / hi;
+        const bool big = a > 0.267949192431122706f;                  // tan(pi/12)
+        const float z = big ? (1.73205080756887729f * a - 1.0f) / (1.73205080756887729f + a) : a;
+        const float z2 = z * z;
+        float p = 1.0f / 13.0f;
+        p = p * z2 - 1.0f / 11.0f;
+        p = p * z2 + 1.0f / 9.0f;
+        p = p * z2 - 1.0f / 7.0f;
+        p = p * z2 + 1.0f / 5.0f;
+        p = p * z2 - 1.0f / 3.0f;
+        p = p * z2 + 1.0f;
+        r = z * p;
+        if (big) r = 0.523598775598298873f + r;                      // pi/6
+        if (ay > ax) r = 1.57079632679489662f - r;                   // pi/2
+    }
+    if (std::signbit(x)) r = 3.14159265358979324f - r;                    // pi
+    return std::signbit(y) ? -r : r;
+}
+
 static inline float combine_friction(float a, float b, uint32_t mode) {
     if (mode == 1u) return a * b;
     if (mode == 2u) return fmin_(a, b);

@@ -162,3 +162,24 @@ def test_unsupported_features_are_refused(oracle_lib):
     s.add_body((1, 0.2, 0), 1.0, 0.5, (0, 0, 1), shape=abi.SHAPE_CAPSULE)
     with pytest.raises(RuntimeError):
         oracle_lib.OracleSolver(s)
+
+
+def test_atan2_series_accuracy(oracle_lib):
+    """The fixed-sequence atan2 shared by the oracle and the kernels (hinge
+    twist angles) stays within a few ulp of the float64 value, keeps the
+    quadrant and signed-zero conventions of atan2."""
+    import math
+    lib = oracle_lib.lib()
+    rng = np.random.default_rng(3)
+    ys = np.concatenate([rng.normal(size=4000), rng.uniform(-1e-3, 1e-3, 500), [0.0, -0.0, 1.0, -1.0]])
+    xs = np.concatenate([rng.normal(size=4000), rng.uniform(-1e-3, 1e-3, 500), [1.0, 1.0, 0.0, 0.0]])
+    worst = 0.0
+    for y, x in zip(ys.astype(np.float32), xs.astype(np.float32)):
+        got = lib.oracle_atan2(float(y), float(x))
+        want = math.atan2(float(y), float(x))
+        ulp = np.spacing(np.float32(abs(want))) if want != 0 else np.float32(1e-45)
+        worst = max(worst, abs(got - want) / float(ulp))
+    assert worst <= 4.0, worst
+    assert lib.oracle_atan2(0.0, -0.0) == np.float32(math.pi)
+    assert math.copysign(1.0, lib.oracle_atan2(-0.0, 1.0)) < 0
+    assert lib.oracle_atan2(1.0, 0.0) == np.float32(math.pi / 2)
