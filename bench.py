@@ -77,12 +77,13 @@ def parse():
     return args
 
 
-def make_scene(rank=0):
+def make_scene(rank=0, worlds=4096):
     from avbd_b200 import demos
     if WORKLOAD_KEY == "cloth-sphere":
         return demos.cloth_sphere_scene(seed=3, n=256)
     if WORKLOAD_KEY == "batched-worlds":
-        scene, motors, _ = demos.batched_worlds_scene(worlds=4096, seed=4, first_world=4096 * rank)
+        # rank r owns worlds [r * worlds, (r + 1) * worlds)
+        scene, motors, _ = demos.batched_worlds_scene(worlds=worlds, seed=4, first_world=worlds * rank)
         MOTORS[:] = motors
         return scene
     return demos.soft_cube_scene(seed=2, n=24)
