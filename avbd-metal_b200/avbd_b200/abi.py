@@ -46,7 +46,7 @@ BUF = dict(
     SPRINGS=19, TETS=20, INIT_LIN=21, INERT_LIN=22, EXCLUSIONS=23, HASHED_IDX=24,
     GLOBAL_IDX=25, TRIS=26, EDGES=27, NBR_START=28, NBR_COUNT=29, NBR_LIST=30,
     PARTICLE_IDX=31, MEMBRANES=32, BENDS=33, SOFT=34, DAT_PAIRS=35, CLOTH_GROUP=36,
-    OGC_PREV=37,
+    OGC_PREV=37, LEARN_IDX=38, LEARN_FEATURES=39, LEARN_TARGETS=40, LEARN_PREDICTIONS=41,
 )
 
 F3 = C.c_float * 3
@@ -159,7 +159,7 @@ class Counters(C.Structure):
         ("dat_grid_overflows", C.c_uint32), ("dat_invalid_anchors", C.c_uint32),
         ("dat_truncations", C.c_uint32), ("dat_vt_degenerate", C.c_uint32),
         ("dat_ee_degenerate", C.c_uint32), ("dat_nonfinite", C.c_uint32),
-        ("dat_tet_degenerate", C.c_uint32),
+        ("dat_tet_degenerate", C.c_uint32), ("learn_accepted", C.c_uint32),
     ]
 
 
@@ -172,10 +172,14 @@ EXPORTED = [
     "avbd_last_error", "avbd_snapshot_capture", "avbd_snapshot_restore",
     "avbd_snapshot_free", "avbd_debug_buffer_size", "avbd_debug_read", "avbd_set_stream",
     "avbd_set_profiling", "avbd_get_profile", "avbd_exclusive_scan_noalloc",
+    "avbd_set_warm_start_model", "avbd_set_warm_start_mode", "avbd_set_learning_capture",
+    "avbd_set_residual_trace", "avbd_get_residual_trace", "avbd_mlp_param_count",
+    "avbd_mlp_workspace_bytes", "avbd_mlp_gradients", "avbd_mlp_train_step", "avbd_mlp_infer",
 ]
+WARM_START_PLAIN, WARM_START_LEARNED = 0, 1
 
 STAGES = ["broadphase", "narrowphase", "persistence_map", "warmstart", "adjacency",
-          "coloring", "primal", "dual", "finalize", "element_contacts", "truncation"]
+          "coloring", "primal", "dual", "finalize", "element_contacts", "truncation", "learned"]
 
 
 class Profile(C.Structure):

@@ -1,0 +1,254 @@
+"""Learned warm start: data collection from the solver's own rollouts,
+training with the library's BF16 tensor-core kernels, and evaluation in
+iterations-to-tolerance against the plain gamma warm start.
+
+The network (csrc/learned.cu) maps 16 per-vertex features to the correction
+the solve applies to the plain warm start.  Training runs on the GPU through
+avbd_mlp_train_step (forward, backward and Adam are the library's kernels;
+torch only owns the device buffers).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Sequence
+
+import numpy as np
+
+from . import abi
+from .solver import GPUSolver, load_library
+
+DIN, HID, DOUT, USED = 16, 128, 16, 3
+NPARAM = HID * DIN + HID + 2 * (HID * HID + HID) + DOUT * HID + DOUT
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-initialised weights, zero biases, small output layer."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(NPARAM, np.float32)
+    o = 0
+    for fan_out, fan_in, scale in ((HID, DIN, 1.0), (HID, HID, 1.0), (HID, HID, 1.0), (DOUT, HID, 0.1)):
+        w = rng.normal(0.0, scale * math.sqrt(2.0 / fan_in), size=(fan_out, fan_in))
+        p[o:o + fan_out * fan_in] = w.ravel()
+        o += fan_out * fan_in + fan_out
+    return p
+
+
+def fit_norm(features: np.ndarray, targets: np.ndarray) -> np.ndarray:
+    """Per-feature mean and 1/std, per-target mean and std (64 floats)."""
+    n = np.zeros(64, np.float32)
+    mu = features.mean(axis=0)
+    sd = features.std(axis=0)
+    n[:16] = mu
+    n[16:32] = np.where(sd > 1e-6, 1.0 / np.maximum(sd, 1e-6), 1.0)
+    n[16 + 15] = 1.0                                   # the constant feature
+    n[15] = 0.0
+    tm = targets.mean(axis=0)
+    ts = targets.std(axis=0)
+    n[32:32 + USED] = tm
+    n[48:48 + USED] = np.maximum(ts, 1e-6)
+    n[48 + USED:64] = 1.0
+    return n
+
+
+@dataclass
+class WarmStartModel:
+    params: np.ndarray
+    norm: np.ndarray
+    history: List[float] = field(default_factory=list)
+
+    def save(self, path: str) -> None:
+        np.savez(path, params=self.params, norm=self.norm, history=np.array(self.history, np.float32))
+
+    @staticmethod
+    def load(path: str) -> "WarmStartModel":
+        z = np.load(path)
+        return WarmStartModel(z["params"].astype(np.float32), z["norm"].astype(np.float32),
+                              list(z["history"]) if "history" in z else [])
+
+
+def collect(make_scene: Callable[[int], object], seeds: Sequence[int], frames: int, skip: int = 2,
+            every: int = 1, motor_targets: Optional[Callable] = None):
+    """Roll out the plain solver on seeded scene variants and record, per
+    frame, the features and the solve's correction of the plain warm start."""
+    feats, targs = [], []
+    for seed in seeds:
+        scene = make_scene(seed)
+        g = GPUSolver(scene)
+        g.set_learning_capture(True)
+        for f in range(frames):
+            g.step(1)
+            if f >= skip and (f - skip) % every == 0:
+                x, t = g.learning_sample()
+                feats.append(x.copy())
+                targs.append(t.copy())
+        g.close()
+    return np.concatenate(feats), np.concatenate(targs)
+
+
+def train(features: np.ndarray, targets: np.ndarray, steps: int = 2000, batch: int = 8192, lr: float = 1e-3,
+          seed: int = 0, norm: Optional[np.ndarray] = None, device: int = 0,
+          log_every: int = 100) -> WarmStartModel:
+    """Adam on the mean-squared error, on the GPU with the library's kernels."""
+    import torch
+    lib = load_library()
+    dev = torch.device("cuda", device)
+    norm = fit_norm(features, targets) if norm is None else norm
+    X = torch.from_numpy(np.ascontiguousarray(features, np.float32)).to(dev)
+    T = torch.from_numpy(np.ascontiguousarray(targets, np.float32)).to(dev)
+    prm = torch.from_numpy(init_params(seed)).to(dev)
+    nrm = torch.from_numpy(norm).to(dev)
+    m = torch.zeros_like(prm)
+    v = torch.zeros_like(prm)
+    ws = torch.empty(lib.avbd_mlp_workspace_bytes(batch), dtype=torch.uint8, device=dev)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+    hist = []
+    n = X.shape[0]
+    for step in range(1, steps + 1):
+        idx = torch.randint(0, n, (batch,), device=dev, generator=gen)
+        xb = X[idx].contiguous()
+        tb = T[idx].contiguous()
+        rc = lib.avbd_mlp_train_step(prm.data_ptr(), nrm.data_ptr(), xb.data_ptr(), tb.data_ptr(), batch,
+                                     m.data_ptr(), v.data_ptr(), step, C.c_float(lr), ws.data_ptr(),
+                                     loss.data_ptr(), stream)
+        if rc != 0:
+            raise RuntimeError(f"avbd_mlp_train_step failed: {rc}")
+        if step % log_every == 0 or step == steps:
+            hist.append(float(loss.item()) / USED)           # per-component mean squared error
+    return WarmStartModel(prm.cpu().numpy(), norm, hist)
+
+
+def gradients(params, norm, features, targets, device: int = 0):
+    """(loss, gradient) of one batch from the library's kernels."""
+    import torch
+    lib = load_library()
+    dev = torch.device("cuda", device)
+    B = features.shape[0]
+    prm = torch.from_numpy(np.ascontiguousarray(params, np.float32)).to(dev)
+    nrm = torch.from_numpy(np.ascontiguousarray(norm, np.float32)).to(dev)
+    X = torch.from_numpy(np.ascontiguousarray(features, np.float32)).to(dev)
+    T = torch.from_numpy(np.ascontiguousarray(targets, np.float32)).to(dev)
+    ws = torch.empty(lib.avbd_mlp_workspace_bytes(B), dtype=torch.uint8, device=dev)
+    g = torch.zeros(NPARAM, dtype=torch.float32, device=dev)
+    loss = torch.zeros(1, dtype=torch.float32, device=dev)
+    rc = lib.avbd_mlp_gradients(prm.data_ptr(), nrm.data_ptr(), X.data_ptr(), T.data_ptr(), B, ws.data_ptr(),
+                                g.data_ptr(), loss.data_ptr(), torch.cuda.current_stream(dev).cuda_stream)
+    if rc != 0:
+        raise RuntimeError(f"avbd_mlp_gradients failed: {rc}")
+    torch.cuda.synchronize(dev)
+    return float(loss.item()), g.cpu().numpy()
+
+
+def infer(params, norm, features, device: int = 0) -> np.ndarray:
+    """Predictions [n][3] from the fused inference kernel."""
+    import torch
+    lib = load_library()
+    dev = torch.device("cuda", device)
+    n = features.shape[0]
+    prm = torch.from_numpy(np.ascontiguousarray(params, np.float32)).to(dev)
+    nrm = torch.from_numpy(np.ascontiguousarray(norm, np.float32)).to(dev)
+    X = torch.from_numpy(np.ascontiguousarray(features, np.float32)).to(dev)
+    out = torch.zeros((n, USED), dtype=torch.float32, device=dev)
+    ws = torch.empty(1 << 17, dtype=torch.uint8, device=dev)
+    rc = lib.avbd_mlp_infer(prm.data_ptr(), nrm.data_ptr(), X.data_ptr(), n, out.data_ptr(), ws.data_ptr(),
+                            torch.cuda.current_stream(dev).cuda_stream)
+    if rc != 0:
+        raise RuntimeError(f"avbd_mlp_infer failed: {rc}")
+    torch.cuda.synchronize(dev)
+    return out.cpu().numpy()
+
+
+def iterations_to_tolerance(trace: np.ndarray, r0_plain: float, tol: float) -> int:
+    """First iteration k (1-based) with r_k / r0_plain <= tol, or -1."""
+    rel = trace[2:] / max(r0_plain, 1e-300)
+    hit = np.nonzero(rel <= tol)[0]
+    return int(hit[0]) + 1 if hit.size else -1
+
+
+def evaluate(make_scene: Callable[[int], object], seed: int, model: Optional[WarmStartModel], frames: int,
+             iterations: int, skip: int = 2, trial_sweeps: int = 1,
+             tolerances: Sequence[float] = (1e-1, 1e-2, 1e-3, 1e-6)) -> Dict[str, object]:
+    """Per-frame residual traces of one rollout with the plain (model=None)
+    or the learned warm start, at `iterations` iterations per frame."""
+    scene = make_scene(seed)
+    scene.settings.iterations = iterations
+    g = GPUSolver(scene)
+    if model is not None:
+        g.set_warm_start_model(model.params, model.norm, trial_sweeps)
+        g.set_warm_start_mode(abi.WARM_START_LEARNED)
+    g.set_residual_trace(True)
+    its = {t: [] for t in tolerances}
+    rel_final, rel_first = [], []
+    for f in range(frames):
+        g.step(1)
+        if f < skip:
+            continue
+        tr = g.residual_trace(2 + iterations)
+        r0 = tr[0]
+        rel_first.append(tr[2] / max(r0, 1e-300))
+        rel_final.append(tr[-1] / max(r0, 1e-300))
+        for t in tolerances:
+            its[t].append(iterations_to_tolerance(tr, r0, t))
+    c = g.counters()
+    g.close()
+    return {"iterations_to_tolerance": its, "rel_residual_after_1": float(np.median(rel_first)),
+            "rel_residual_final": float(np.median(rel_final)), "accepted": int(c.learn_accepted),
+            "frames": frames - skip}
+
+
+def matched_residual_iterations(make_scene: Callable[[int], object], seed: int, model: WarmStartModel,
+                                plain_iterations: int, frames: int = 60,
+                                candidates: Sequence[int] = (4, 6, 8, 10, 12, 14, 16, 18),
+                                trial_sweeps: int = 1):
+    """Smallest learned iteration count whose median relative residual
+    (r_final / r0 of the plain warm start) is no larger than the plain warm
+    start's at `plain_iterations`.  Returns (iterations, plain residual,
+    learned residual, accepted fraction)."""
+    plain = evaluate(make_scene, seed, None, frames, plain_iterations, trial_sweeps=trial_sweeps)
+    target = plain["rel_residual_final"]
+    for k in candidates:
+        if k >= plain_iterations:
+            break
+        r = evaluate(make_scene, seed, model, frames, k, trial_sweeps=trial_sweeps)
+        if r["rel_residual_final"] <= target:
+            return k, target, r["rel_residual_final"], r["accepted"] / max(1, r["frames"])
+    r = evaluate(make_scene, seed, model, frames, plain_iterations, trial_sweeps=trial_sweeps)
+    return plain_iterations, target, r["rel_residual_final"], r["accepted"] / max(1, r["frames"])
+
+
+def _main(argv=None):
+    """Train the soft-cube warm-start model from the solver's own rollouts:
+
+      PYTHONPATH=avbd-metal_b200 python -m avbd_b200.learned --out MODEL.npz
+    """
+    import argparse
+    from . import demos
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--n", type=int, default=24, help="soft-cube lattice size")
+    ap.add_argument("--seeds", type=int, nargs="+", default=[100, 101, 102, 103])
+    ap.add_argument("--frames", type=int, default=200)
+    ap.add_argument("--every", type=int, default=2)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--batch", type=int, default=8192)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--eval-seed", type=int, default=200)
+    a = ap.parse_args(argv)
+    scene = lambda s: demos.soft_cube_scene(seed=s, n=a.n)   # noqa: E731
+    X, T = collect(scene, a.seeds, a.frames, every=a.every)
+    model = train(X, T, steps=a.steps, batch=a.batch, lr=a.lr)
+    model.save(a.out)
+    print(f"samples {len(X)}, loss {model.history[0]:.4f} -> {model.history[-1]:.4f}")
+    for iters in (10, 20):
+        p = evaluate(scene, a.eval_seed, None, 120, iters)
+        q = evaluate(scene, a.eval_seed, model, 120, iters)
+        print(f"{iters} iterations: median r/r0 plain {p['rel_residual_final']:.4f}, learned "
+              f"{q['rel_residual_final']:.4f}, accepted {q['accepted']}/{q['frames']}")
+
+
+if __name__ == "__main__":
+    _main()

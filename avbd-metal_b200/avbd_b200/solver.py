@@ -73,6 +73,16 @@ def load_library() -> C.CDLL:
         "avbd_set_stream": ([vp, vp], i32),
         "avbd_set_profiling": ([vp, i32], i32),
         "avbd_get_profile": ([vp, vp], i32),
+        "avbd_set_warm_start_model": ([vp, vp, vp, u32], i32),
+        "avbd_set_warm_start_mode": ([vp, i32], i32),
+        "avbd_set_learning_capture": ([vp, i32], i32),
+        "avbd_set_residual_trace": ([vp, i32], i32),
+        "avbd_get_residual_trace": ([vp, vp, u32], i32),
+        "avbd_mlp_param_count": ([], u32),
+        "avbd_mlp_workspace_bytes": ([u32], sz),
+        "avbd_mlp_gradients": ([vp, vp, vp, vp, u32, vp, vp, vp, vp], i32),
+        "avbd_mlp_train_step": ([vp, vp, vp, vp, u32, vp, vp, u32, C.c_float, vp, vp, vp], i32),
+        "avbd_mlp_infer": ([vp, vp, vp, u32, vp, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -227,6 +237,35 @@ class GPUSolver:
                 "stage_ms": {n: p.stage_ms[i] for i, n in enumerate(abi.STAGES)},
                 "stage_launches": {n: p.stage_launches[i] for i, n in enumerate(abi.STAGES)},
                 "color_lanes": list(p.color_lanes)}
+
+    # ---- learned warm start ------------------------------------------------
+    def set_warm_start_model(self, params, norm, trial_sweeps: int = 1) -> None:
+        """Upload an MLP (fp32 parameter block and 64-float normalisation)."""
+        p = np.ascontiguousarray(params, np.float32)
+        n = np.ascontiguousarray(norm, np.float32)
+        self._check(load_library().avbd_set_warm_start_model(self._h, p.ctypes.data, n.ctypes.data,
+                                                             int(trial_sweeps)))
+
+    def set_warm_start_mode(self, mode: int) -> None:
+        self._check(load_library().avbd_set_warm_start_mode(self._h, int(mode)))
+
+    def set_learning_capture(self, enabled: bool) -> None:
+        self._check(load_library().avbd_set_learning_capture(self._h, 1 if enabled else 0))
+
+    def set_residual_trace(self, enabled: bool) -> None:
+        self._check(load_library().avbd_set_residual_trace(self._h, 1 if enabled else 0))
+
+    def residual_trace(self, n: int) -> np.ndarray:
+        """[r(plain warm start), r(warm start used), r after iteration 1..n-2]."""
+        out = np.zeros(n, np.float64)
+        self._check(load_library().avbd_get_residual_trace(self._h, out.ctypes.data, n))
+        return out
+
+    def learning_sample(self):
+        """(features [n][16], targets [n][3]) of the last captured frame."""
+        f = self.debug_read("LEARN_FEATURES", np.float32).reshape(-1, 16)
+        t = self.debug_read("LEARN_TARGETS", np.float32).reshape(-1, 3)
+        return f, t
 
     def debug_read(self, name: str, dtype=np.uint8):
         lib = load_library()

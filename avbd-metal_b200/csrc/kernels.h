@@ -79,6 +79,16 @@ struct DevPtrs {
     uint32_t* truncBits;                        // Planar-DAT step fraction per body (float bits)
     float4 *ogcPrev, *posNext, *angNext;
     uint32_t* bigScanScratch;
+    // learned warm start
+    uint32_t* learnIdx;                         // dynamic particles the model predicts
+    float *learnFeat, *learnPred, *learnTarget; // [n][16], [n][3], [n][3]
+    float4 *learnSaveLin, *learnSaveAng;        // the plain warm start
+    float4 *learnSweptLin, *learnSweptAng;      // the plain branch after its trial sweep
+    float *learnPrm, *learnNorm, *learnResidBodies;
+    void* learnHalf;                            // BF16 weight mirror
+    double* learnResid;                         // [0] plain, [1] predicted, [2] scratch
+    double* learnTrace;                         // residual trace of the last frame
+    uint32_t* learnAccepted;                    // frames whose prediction was kept (running)
 };
 
 struct Sizes {
@@ -90,6 +100,11 @@ struct Sizes {
     // cloth
     uint32_t numTris, numParticles, numEdges, numMembranes, numBends;
     uint32_t maxDatPairs, maxSoft, elemHashSize;
+    uint32_t numLearn;
+    uint32_t numDynamicRigid;
+    // static palette on the host (null with dynamic coloring)
+    const uint32_t* colorCounts;
+    const uint32_t* colorLanes;
 };
 
 // exclusive scan of n words (n <= 1024 * 1024); out may not alias in
@@ -106,6 +121,10 @@ void launch_dynamic_coloring(const Params& P, const DevPtrs& d, const Sizes& z, 
 // when known on the host (static palette), else 0xFFFFFFFF (read on device)
 void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color,
                          uint32_t count, uint32_t lanes, cudaStream_t st);
+// squared AL-gradient norm of every dynamic body (perBody[numDynamicBodies])
+// and their fixed-order sum (total)
+void launch_residual(const Params& P, const DevPtrs& d, const Sizes& z, float* perBody, double* total,
+                     cudaStream_t st);
 // dynamic coloring: colors [first, 64) in one block, after the per-color launches
 void launch_primal_tail(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t first, cudaStream_t st);
 // every iteration of a small scene in one thread block
@@ -135,5 +154,18 @@ void launch_dat_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_
                       cudaStream_t st);
 void launch_cloth_restore(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 void launch_cloth_smoothing(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+
+// learned warm start (learned.cu)
+void launch_learn_features(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_learn_apply(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_learn_select(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_learn_keep(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_learn_target(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_copy_double(const double* src, double* dst, cudaStream_t st);
+void launch_mlp_infer(const void* halfW, const float* prm, const float* norm, const float* X, uint32_t n, float* Y,
+                      cudaStream_t st);
+void launch_mlp_mirror(const float* prm, void* halfW, cudaStream_t st);
+uint32_t mlp_param_count();
+uint32_t mlp_half_count();
 
 }  // namespace avbd

@@ -1,0 +1,611 @@
+// learned.cu — learned warm start: per-vertex features, a 16-128-128-128-16
+// MLP (BF16 weights and activations, FP32 accumulation on the tensor cores)
+// for inference and training, and the acceptance test that keeps a predicted
+// warm start only when it is no worse than the plain gamma warm start.
+//
+// The MLP predicts the correction the solve applies to the plain warm start
+// of every dynamic particle, in units of s = max(|g|, 1) dt^2:
+//   x0 = x_plain + s * MLP(features).
+// Features (16, normalised by per-feature mean and 1/std stored with the
+// model): inertial offset (x~ - x_start)/s, plain warm-start offset
+// (x_plain - x_start)/s, previous-frame displacement v_prev dt / s, incident
+// contact count / 4, summed oriented contact normal, smallest contact gap / s
+// (clipped), log(1 + stiffness dt^2 / m) of the incident elements, and 1.
+//
+// Parameter block (fp32, also the layout of the gradients): W1[128][16], b1,
+// W2[128][128], b2, W3[128][128], b3, W4[16][128], b4[16].  The weights are
+// mirrored as BF16 for the tensor cores.
+#include <cuda_bf16.h>
+
+#include "../../include/avbd.h"
+#include "dmath.cuh"
+#include "kernels.h"
+
+namespace avbd {
+
+namespace mlp {
+constexpr int DIN = 16, HID = 128, DOUT = 16, USED_OUT = 3;
+constexpr uint32_t OW1 = 0, OB1 = OW1 + HID * DIN, OW2 = OB1 + HID, OB2 = OW2 + HID * HID, OW3 = OB2 + HID,
+                   OB3 = OW3 + HID * HID, OW4 = OB3 + HID, OB4 = OW4 + DOUT * HID, NPARAM = OB4 + DOUT;
+// bf16 weight mirror: W1 | W2 | W3 | W4
+constexpr uint32_t HW1 = 0, HW2 = HW1 + HID * DIN, HW3 = HW2 + HID * HID, HW4 = HW3 + HID * HID,
+                   NHALF = HW4 + DOUT * HID;
+// normalisation block: xmean[16], xinvstd[16], ymean[16], ystd[16]
+constexpr uint32_t NNORM = 64;
+}  // namespace mlp
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+// D = A * B + C for one m16n8k16 tile, BF16 inputs, FP32 accumulate.
+__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
+                                         uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t ld_pair(const bf16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
+// ---------------------------------------------------------------------------
+// Fused inference: one warp per 16 vertices, activations stay in registers
+// between layers (an m16n8 accumulator pair is exactly the next layer's
+// m16k16 operand), weights are read from L1/L2 (72 KB shared by all warps).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_mlp_infer(const bf16* __restrict__ W, const float* __restrict__ prm,
+                                                   const float* __restrict__ norm, const float* __restrict__ X,
+                                                   uint32_t n, float* __restrict__ Y) {
+    using namespace mlp;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, q = lane & 3u;
+    const uint32_t row0 = warp * 16u;
+    if (row0 >= n) return;
+    const uint32_t r0 = row0 + g, r1 = row0 + g + 8;
+    auto xin = [&](uint32_t r, uint32_t c) {
+        return r < n ? (X[r * DIN + c] - norm[c]) * norm[16 + c] : 0.0f;
+    };
+    uint32_t a[8][4];
+    a[0][0] = pack_bf16(xin(r0, 2 * q), xin(r0, 2 * q + 1));
+    a[0][1] = pack_bf16(xin(r1, 2 * q), xin(r1, 2 * q + 1));
+    a[0][2] = pack_bf16(xin(r0, 2 * q + 8), xin(r0, 2 * q + 9));
+    a[0][3] = pack_bf16(xin(r1, 2 * q + 8), xin(r1, 2 * q + 9));
+    float acc[16][4];
+    // layer 1: K = 16
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+        const bf16* w = W + HW1 + (8 * j + g) * DIN + 2 * q;
+        mma_bf16(acc[j], a[0][0], a[0][1], a[0][2], a[0][3], ld_pair(w), ld_pair(w + 8));
+    }
+    const float* bias = prm + OB1;
+    const bf16* Wl = W + HW2;
+#pragma unroll 1
+    for (int layer = 0; layer < 2; layer++) {
+        // epilogue: bias, ReLU, BF16 -> operand of the next layer
+#pragma unroll
+        for (int kb = 0; kb < 8; kb++) {
+            const float b00 = bias[16 * kb + 2 * q], b01 = bias[16 * kb + 2 * q + 1];
+            const float b10 = bias[16 * kb + 8 + 2 * q], b11 = bias[16 * kb + 8 + 2 * q + 1];
+            a[kb][0] = pack_bf16(fmaxf(acc[2 * kb][0] + b00, 0.0f), fmaxf(acc[2 * kb][1] + b01, 0.0f));
+            a[kb][1] = pack_bf16(fmaxf(acc[2 * kb][2] + b00, 0.0f), fmaxf(acc[2 * kb][3] + b01, 0.0f));
+            a[kb][2] = pack_bf16(fmaxf(acc[2 * kb + 1][0] + b10, 0.0f), fmaxf(acc[2 * kb + 1][1] + b11, 0.0f));
+            a[kb][3] = pack_bf16(fmaxf(acc[2 * kb + 1][2] + b10, 0.0f), fmaxf(acc[2 * kb + 1][3] + b11, 0.0f));
+        }
+#pragma unroll
+        for (int j = 0; j < 16; j++) {
+            acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+#pragma unroll
+            for (int kb = 0; kb < 8; kb++) {
+                const bf16* w = Wl + (8 * j + g) * HID + 16 * kb + 2 * q;
+                mma_bf16(acc[j], a[kb][0], a[kb][1], a[kb][2], a[kb][3], ld_pair(w), ld_pair(w + 8));
+            }
+        }
+        bias = layer == 0 ? prm + OB2 : prm + OB3;
+        Wl = W + HW3;
+    }
+#pragma unroll
+    for (int kb = 0; kb < 8; kb++) {
+        const float b00 = bias[16 * kb + 2 * q], b01 = bias[16 * kb + 2 * q + 1];
+        const float b10 = bias[16 * kb + 8 + 2 * q], b11 = bias[16 * kb + 8 + 2 * q + 1];
+        a[kb][0] = pack_bf16(fmaxf(acc[2 * kb][0] + b00, 0.0f), fmaxf(acc[2 * kb][1] + b01, 0.0f));
+        a[kb][1] = pack_bf16(fmaxf(acc[2 * kb][2] + b00, 0.0f), fmaxf(acc[2 * kb][3] + b01, 0.0f));
+        a[kb][2] = pack_bf16(fmaxf(acc[2 * kb + 1][0] + b10, 0.0f), fmaxf(acc[2 * kb + 1][1] + b11, 0.0f));
+        a[kb][3] = pack_bf16(fmaxf(acc[2 * kb + 1][2] + b10, 0.0f), fmaxf(acc[2 * kb + 1][3] + b11, 0.0f));
+    }
+    // layer 4: N = 16 (two tiles), only columns 0..2 are read
+    float o[2][4];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        o[j][0] = o[j][1] = o[j][2] = o[j][3] = 0.0f;
+#pragma unroll
+        for (int kb = 0; kb < 8; kb++) {
+            const bf16* w = W + HW4 + (8 * j + g) * HID + 16 * kb + 2 * q;
+            mma_bf16(o[j], a[kb][0], a[kb][1], a[kb][2], a[kb][3], ld_pair(w), ld_pair(w + 8));
+        }
+    }
+    // columns 2q, 2q+1 of tile 0 live in lane q; denormalise and store
+    if (q < 2) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const uint32_t r = h == 0 ? r0 : r1;
+            if (r >= n) continue;
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const uint32_t c = 2 * q + e;
+                if (c >= (uint32_t)USED_OUT) continue;
+                const float v = o[0][2 * h + e] + prm[OB4 + c];
+                Y[r * USED_OUT + c] = v * norm[48 + c] + norm[32 + c];
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Training GEMM: C[M][N] (fp32) = op(A) op(B) with BF16 operands, FP32
+// accumulation.  A is [M][K] (lda = K) or, with TA, stored [K][M]; B is
+// [N][K] or, with TB, stored [K][N].  64 x 64 tiles, 4 warps of 32 x 32,
+// K in steps of 32 staged through shared memory; split-K writes one partial
+// per z-slice (reduced in a fixed order by k_split_sum).
+// ---------------------------------------------------------------------------
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(128) k_gemm(const bf16* __restrict__ A, const bf16* __restrict__ B,
+                                              float* __restrict__ C, uint32_t M, uint32_t N, uint32_t K,
+                                              uint32_t kPerSplit) {
+    __shared__ __align__(16) bf16 As[64][40];
+    __shared__ __align__(16) bf16 Bs[64][40];
+    const uint32_t m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    const uint32_t kBeg = blockIdx.z * kPerSplit, kEnd = min(K, kBeg + kPerSplit);
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, g = lane >> 2, q = lane & 3u;
+    const uint32_t wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    float acc[2][4][4] = {};
+    for (uint32_t k0 = kBeg; k0 < kEnd; k0 += 32) {
+        for (uint32_t i = threadIdx.x; i < 64 * 32; i += 128) {
+            const uint32_t r = i >> 5, c = i & 31u;          // tile row (m or n), tile column (k)
+            const uint32_t gm = m0 + r, gn = n0 + r, gk = k0 + c;
+            bf16 av = __float2bfloat16(0.0f), bv = __float2bfloat16(0.0f);
+            if (gm < M && gk < kEnd) av = TA ? A[(size_t)gk * M + gm] : A[(size_t)gm * K + gk];
+            if (gn < N && gk < kEnd) bv = TB ? B[(size_t)gk * N + gn] : B[(size_t)gn * K + gk];
+            As[r][c] = av;
+            Bs[r][c] = bv;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 32; kk += 16) {
+            uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; i++) {
+                const uint32_t r = wm + 16 * i + g;
+                af[i][0] = ld_pair(&As[r][kk + 2 * q]);
+                af[i][1] = ld_pair(&As[r + 8][kk + 2 * q]);
+                af[i][2] = ld_pair(&As[r][kk + 8 + 2 * q]);
+                af[i][3] = ld_pair(&As[r + 8][kk + 8 + 2 * q]);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const uint32_t c = wn + 8 * j + g;
+                bfr[j][0] = ld_pair(&Bs[c][kk + 2 * q]);
+                bfr[j][1] = ld_pair(&Bs[c][kk + 8 + 2 * q]);
+            }
+#pragma unroll
+            for (int i = 0; i < 2; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++)
+                    mma_bf16(acc[i][j], af[i][0], af[i][1], af[i][2], af[i][3], bfr[j][0], bfr[j][1]);
+        }
+        __syncthreads();
+    }
+    float* Cz = C + (size_t)blockIdx.z * M * N;
+#pragma unroll
+    for (int i = 0; i < 2; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            const uint32_t r = m0 + wm + 16 * i + g, c = n0 + wn + 8 * j + 2 * q;
+            if (r < M && c < N) Cz[(size_t)r * N + c] = acc[i][j][0];
+            if (r < M && c + 1 < N) Cz[(size_t)r * N + c + 1] = acc[i][j][1];
+            if (r + 8 < M && c < N) Cz[(size_t)(r + 8) * N + c] = acc[i][j][2];
+            if (r + 8 < M && c + 1 < N) Cz[(size_t)(r + 8) * N + c + 1] = acc[i][j][3];
+        }
+}
+
+__global__ void k_split_sum(const float* part, uint32_t splits, uint32_t count, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    float s = 0.0f;
+    for (uint32_t z = 0; z < splits; z++) s += part[(size_t)z * count + i];
+    out[i] = s;
+}
+
+// H = bf16(relu(Z + b)) for Z [rows][cols]
+__global__ void k_bias_relu(const float* Z, const float* b, uint32_t rows, uint32_t cols, bf16* H) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows * cols) return;
+    H[i] = __float2bfloat16(fmaxf(Z[i] + b[i % cols], 0.0f));
+}
+
+// normalised inputs as BF16 [rows][16]
+__global__ void k_norm_input(const float* X, const float* norm, uint32_t rows, bf16* Xb) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows * mlp::DIN) return;
+    const uint32_t c = i % mlp::DIN;
+    Xb[i] = __float2bfloat16((X[i] - norm[c]) * norm[16 + c]);
+}
+
+// Output layer and loss: Y = Z + b4; dY = 2 (Y - Tn) / rows on the used
+// columns (Tn: targets normalised by ymean, ystd), 0 elsewhere; loss sums.
+__global__ void k_loss_grad(const float* Z, const float* b4, const float* T, const float* norm, uint32_t rows,
+                            float* dY, bf16* dYb, float* lossPart) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float l = 0.0f;
+    if (i < rows * mlp::DOUT) {
+        const uint32_t r = i / mlp::DOUT, c = i % mlp::DOUT;
+        float g = 0.0f;
+        if (c < (uint32_t)mlp::USED_OUT) {
+            const float y = Z[i] + b4[c];
+            const float t = (T[r * mlp::USED_OUT + c] - norm[32 + c]) / norm[48 + c];
+            const float e = y - t;
+            l = e * e;
+            g = 2.0f * e / (float)rows;
+        }
+        dY[i] = g;
+        dYb[i] = __float2bfloat16(g);
+    }
+    // block sum of the squared errors (fixed order)
+    __shared__ float red[256];
+    red[threadIdx.x] = l;
+    __syncthreads();
+    for (uint32_t w = blockDim.x >> 1; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) lossPart[blockIdx.x] = red[0];
+}
+
+// dH = bf16(G * (H > 0)), G fp32 [rows][cols]; also keeps fp32 for bias sums
+__global__ void k_relu_back(const float* G, const bf16* H, uint32_t n, float* dH, bf16* dHb) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v = __bfloat162float(H[i]) > 0.0f ? G[i] : 0.0f;
+    dH[i] = v;
+    dHb[i] = __float2bfloat16(v);
+}
+
+// column sums of G [rows][cols] in a fixed order (one thread per column)
+__global__ void k_col_sum(const float* G, uint32_t rows, uint32_t cols, float* out) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    float s = 0.0f;
+    for (uint32_t r = 0; r < rows; r++) s += G[(size_t)r * cols + c];
+    out[c] = s;
+}
+
+// fixed-order sum of n values, times `scale`
+__global__ void k_fixed_sum(const float* v, uint32_t n, float scale, float* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    float s = 0.0f;
+    for (uint32_t i = 0; i < n; i++) s += v[i];
+    *out = s * scale;
+}
+
+// Adam on the fp32 parameters; refreshes the BF16 weight mirror.
+__global__ void k_adam(float* prm, const float* grad, float* m, float* v, uint32_t step, float lr, float b1,
+                       float b2, float eps, bf16* half) {
+    using namespace mlp;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= NPARAM) return;
+    const float gi = grad[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float mh = mi / (1.0f - powf(b1, (float)step));
+    const float vh = vi / (1.0f - powf(b2, (float)step));
+    const float p = prm[i] - lr * mh / (sqrtf(vh) + eps);
+    prm[i] = p;
+    int h = -1;
+    if (i < OB1) h = (int)(HW1 + i);
+    else if (i >= OW2 && i < OB2) h = (int)(HW2 + i - OW2);
+    else if (i >= OW3 && i < OB3) h = (int)(HW3 + i - OW3);
+    else if (i >= OW4 && i < OB4) h = (int)(HW4 + i - OW4);
+    if (h >= 0) half[h] = __float2bfloat16(p);
+}
+
+__global__ void k_mirror(const float* prm, bf16* half) {
+    using namespace mlp;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= NPARAM) return;
+    int h = -1;
+    if (i < OB1) h = (int)(HW1 + i);
+    else if (i >= OW2 && i < OB2) h = (int)(HW2 + i - OW2);
+    else if (i >= OW3 && i < OB3) h = (int)(HW3 + i - OW3);
+    else if (i >= OW4 && i < OB4) h = (int)(HW4 + i - OW4);
+    if (h >= 0) half[h] = __float2bfloat16(prm[i]);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host side of training (forward with saved activations, backward, Adam).
+// Workspace layout for a batch of B rows (all offsets 256-byte aligned).
+// ---------------------------------------------------------------------------
+namespace {
+constexpr uint32_t kSplits = 16;
+struct Work {
+    bf16 *Xb, *H1, *H2, *H3, *dYb, *dH3b, *dH2b, *dH1b, *half;
+    float *Z, *dY, *dH, *part, *grad, *lossPart;
+};
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+size_t work_layout(uint32_t B, char* base, Work* w) {
+    using namespace mlp;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { char* p = base ? base + off : nullptr; off += align256(bytes); return p; };
+    const size_t Bp = (size_t)B;
+    char* p;
+    p = take(Bp * DIN * 2); if (w) w->Xb = (bf16*)p;
+    p = take(Bp * HID * 2); if (w) w->H1 = (bf16*)p;
+    p = take(Bp * HID * 2); if (w) w->H2 = (bf16*)p;
+    p = take(Bp * HID * 2); if (w) w->H3 = (bf16*)p;
+    p = take(Bp * DOUT * 2); if (w) w->dYb = (bf16*)p;
+    p = take(Bp * HID * 2); if (w) w->dH3b = (bf16*)p;
+    p = take(Bp * HID * 2); if (w) w->dH2b = (bf16*)p;
+    p = take(Bp * HID * 2); if (w) w->dH1b = (bf16*)p;
+    p = take((size_t)NHALF * 2); if (w) w->half = (bf16*)p;
+    p = take(Bp * HID * 4); if (w) w->Z = (float*)p;
+    p = take(Bp * DOUT * 4); if (w) w->dY = (float*)p;
+    p = take(Bp * HID * 4); if (w) w->dH = (float*)p;
+    p = take((size_t)kSplits * HID * HID * 4); if (w) w->part = (float*)p;
+    p = take((size_t)NPARAM * 4); if (w) w->grad = (float*)p;
+    p = take(((Bp * DOUT + 255) / 256) * 4 + 4); if (w) w->lossPart = (float*)p;
+    return off;
+}
+
+void gemm(const bf16* A, bool ta, const bf16* B, bool tb, float* C, uint32_t M, uint32_t N, uint32_t K,
+          uint32_t splits, float* part, cudaStream_t st) {
+    const uint32_t kPer = ((K + splits - 1) / splits + 31) / 32 * 32;
+    splits = (K + kPer - 1) / kPer;
+    dim3 grid((N + 63) / 64, (M + 63) / 64, splits);
+    float* dst = splits > 1 ? part : C;
+    if (!ta && !tb) k_gemm<false, false><<<grid, 128, 0, st>>>(A, B, dst, M, N, K, kPer);
+    else if (!ta && tb) k_gemm<false, true><<<grid, 128, 0, st>>>(A, B, dst, M, N, K, kPer);
+    else if (ta && !tb) k_gemm<true, false><<<grid, 128, 0, st>>>(A, B, dst, M, N, K, kPer);
+    else k_gemm<true, true><<<grid, 128, 0, st>>>(A, B, dst, M, N, K, kPer);
+    if (splits > 1) k_split_sum<<<(M * N + 255) / 256, 256, 0, st>>>(part, splits, M * N, C);
+}
+
+inline uint32_t blocks(size_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
+
+// Forward with saved activations, loss and full gradient into w.grad.
+void forward_backward(const float* prm, const float* norm, const float* X, const float* T, uint32_t B, Work& w,
+                      cudaStream_t st) {
+    using namespace mlp;
+    k_mirror<<<blocks(NPARAM, 256), 256, 0, st>>>(prm, w.half);
+    k_norm_input<<<blocks((size_t)B * DIN, 256), 256, 0, st>>>(X, norm, B, w.Xb);
+    // forward: Z = Hprev W^T (W stored [out][in] = [N][K])
+    gemm(w.Xb, false, w.half + HW1, false, w.Z, B, HID, DIN, 1, w.part, st);
+    k_bias_relu<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, prm + OB1, B, HID, w.H1);
+    gemm(w.H1, false, w.half + HW2, false, w.Z, B, HID, HID, 1, w.part, st);
+    k_bias_relu<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, prm + OB2, B, HID, w.H2);
+    gemm(w.H2, false, w.half + HW3, false, w.Z, B, HID, HID, 1, w.part, st);
+    k_bias_relu<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, prm + OB3, B, HID, w.H3);
+    gemm(w.H3, false, w.half + HW4, false, w.Z, B, DOUT, HID, 1, w.part, st);
+    const uint32_t lb = blocks((size_t)B * DOUT, 256);
+    k_loss_grad<<<lb, 256, 0, st>>>(w.Z, prm + OB4, T, norm, B, w.dY, w.dYb, w.lossPart);
+    k_fixed_sum<<<1, 32, 0, st>>>(w.lossPart, lb, 1.0f / (float)B, w.lossPart + lb);   // mean over the batch
+    // backward.  dW = dH^T Hprev: A = dH stored [B][out] = [K][M] (TA),
+    // B-operand = Hprev stored [B][in] = [K][N] (TB).  dHprev = dH W:
+    // A = dH [B][out] = [M][K], B-operand W stored [out][in] = [K][N] (TB).
+    gemm(w.dYb, true, w.H3, true, w.grad + OW4, DOUT, HID, B, kSplits, w.part, st);
+    k_col_sum<<<1, DOUT, 0, st>>>(w.dY, B, DOUT, w.grad + OB4);
+    gemm(w.dYb, false, w.half + HW4, true, w.Z, B, HID, DOUT, 1, w.part, st);
+    k_relu_back<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, w.H3, B * HID, w.dH, w.dH3b);
+    k_col_sum<<<1, HID, 0, st>>>(w.dH, B, HID, w.grad + OB3);
+    gemm(w.dH3b, true, w.H2, true, w.grad + OW3, HID, HID, B, kSplits, w.part, st);
+    gemm(w.dH3b, false, w.half + HW3, true, w.Z, B, HID, HID, 1, w.part, st);
+    k_relu_back<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, w.H2, B * HID, w.dH, w.dH2b);
+    k_col_sum<<<1, HID, 0, st>>>(w.dH, B, HID, w.grad + OB2);
+    gemm(w.dH2b, true, w.H1, true, w.grad + OW2, HID, HID, B, kSplits, w.part, st);
+    gemm(w.dH2b, false, w.half + HW2, true, w.Z, B, HID, HID, 1, w.part, st);
+    k_relu_back<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, w.H1, B * HID, w.dH, w.dH1b);
+    k_col_sum<<<1, HID, 0, st>>>(w.dH, B, HID, w.grad + OB1);
+    gemm(w.dH1b, true, w.Xb, true, w.grad + OW1, HID, DIN, B, kSplits, w.part, st);
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Solver integration
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ float step_scale(const Params& P) { return fmaxf(fabsf(P.gravity), 1.0f) * P.dt * P.dt; }
+
+// Per-vertex features at the plain warm start (see the file comment).  The
+// contact features walk the body's per-frame segment (manifolds), the
+// stiffness feature its static segments (springs; tets, membranes, bends).
+__global__ void k_learn_features(const Params P, const DevPtrs d, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t v = d.learnIdx[i];
+    const float s = step_scale(P);
+    const float4 pl = d.posLin[v];
+    const float3 x0 = xyz(d.initLin[v]);
+    const float3 fi = (xyz(d.inertLin[v]) - x0) / s;
+    const float3 fp = (xyz(pl) - x0) / s;
+    const float3 fv = xyz(d.prevVelLin[v]) * (P.dt / s);
+    float count = 0.0f, gap = 1e30f;
+    float3 nsum = s3(0);
+    const uint32_t ds = d.dynStart[v], dc = d.dynCount[v];
+    for (uint32_t k = 0; k < dc; k++) {
+        const uint32_t e = d.dynList[ds + k];
+        if ((e >> ADJ_KIND_SHIFT) != FK_MANIFOLD) continue;
+        const ManifoldGPU& m = d.manifolds[e & ADJ_INDEX_MASK];
+        const float sg = m.header.x == v ? 1.0f : -1.0f;
+        nsum += xyz(m.basisN) * sg;
+        for (uint32_t c = 0; c < m.header.z; c++) {
+            count += 1.0f;
+            gap = fminf(gap, m.contacts[c].C0.x);
+        }
+    }
+    float stiff = 0.0f;
+    const uint4 sg = d.staticSeg[v];
+    for (uint32_t k = 0; k < sg.y; k++) {
+        const uint32_t e = d.preList[sg.x + k];
+        if ((e >> ADJ_KIND_SHIFT) == FK_SPRING) stiff += d.springs[e & ADJ_INDEX_MASK].rA.w;
+    }
+    for (uint32_t k = 0; k < sg.w; k++) {
+        const uint32_t e = d.postList[sg.z + k], kind = e >> ADJ_KIND_SHIFT, idx = e & ADJ_INDEX_MASK;
+        if (kind == FK_TET) stiff += d.tets[idx].r1.w + d.tets[idx].r2.w;
+        else if (kind == FK_MEMBRANE) stiff += d.membranes[idx].mat.x + d.membranes[idx].mat.y;
+        else if (kind == FK_BEND) stiff += d.bends[idx].mat.x;
+    }
+    float* f = d.learnFeat + (size_t)i * mlp::DIN;
+    f[0] = fi.x; f[1] = fi.y; f[2] = fi.z;
+    f[3] = fp.x; f[4] = fp.y; f[5] = fp.z;
+    f[6] = fv.x; f[7] = fv.y; f[8] = fv.z;
+    f[9] = count * 0.25f;
+    f[10] = nsum.x; f[11] = nsum.y; f[12] = nsum.z;
+    f[13] = count > 0.0f ? fminf(fmaxf(gap / s, -10.0f), 10.0f) : 10.0f;
+    f[14] = log1pf(stiff * P.dt * P.dt / fmaxf(pl.w, 1e-12f));
+    f[15] = 1.0f;
+}
+
+// x0 = x_plain + s * prediction for every learned vertex
+__global__ void k_learn_apply(const Params P, const DevPtrs d, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t v = d.learnIdx[i];
+    const float s = step_scale(P);
+    const float4 xp = d.learnSaveLin[v];
+    const float* y = d.learnPred + (size_t)i * mlp::USED_OUT;
+    d.posLin[v] = mk4(xyz(xp) + mk3(y[0], y[1], y[2]) * s, xp.w);
+}
+
+// keep the prediction when its residual after the trial sweeps is no worse
+__global__ void k_learn_select(const Params P, const DevPtrs d, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool accept = d.learnResid[1] <= d.learnResid[0];
+    if (i == 0 && accept) atomicAdd(d.learnAccepted, 1u);
+    if (i >= n || !accept) return;
+    const uint32_t v = d.learnIdx[i];
+    const float s = step_scale(P);
+    const float4 xp = d.learnSaveLin[v];
+    const float* y = d.learnPred + (size_t)i * mlp::USED_OUT;
+    d.posLin[v] = mk4(xyz(xp) + mk3(y[0], y[1], y[2]) * s, xp.w);
+}
+
+// after both trial sweeps: keep the predicted branch's swept pose when its
+// residual is no worse, else the plain branch's (saved in learnSwept*)
+__global__ void k_learn_keep(const Params P, const DevPtrs d, uint32_t nb) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool accept = d.learnResid[1] <= d.learnResid[0];
+    if (b == 0 && accept) atomicAdd(d.learnAccepted, 1u);
+    if (b >= nb || accept) return;
+    d.posLin[b] = d.learnSweptLin[b];
+    d.posAng[b] = d.learnSweptAng[b];
+}
+
+// training target: the solve's correction of the plain warm start
+__global__ void k_learn_target(const Params P, const DevPtrs d, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t v = d.learnIdx[i];
+    const float s = step_scale(P);
+    const float3 t = (xyz(d.posLin[v]) - xyz(d.learnSaveLin[v])) / s;
+    float* y = d.learnTarget + (size_t)i * mlp::USED_OUT;
+    y[0] = t.x; y[1] = t.y; y[2] = t.z;
+}
+
+__global__ void k_copy_double(const double* src, double* dst) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *dst = *src;
+}
+
+}  // namespace
+
+void launch_learn_features(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    if (z.numLearn) k_learn_features<<<(z.numLearn + 127) / 128, 128, 0, st>>>(P, d, z.numLearn);
+}
+void launch_learn_apply(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    if (z.numLearn) k_learn_apply<<<(z.numLearn + 127) / 128, 128, 0, st>>>(P, d, z.numLearn);
+}
+void launch_learn_select(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    k_learn_select<<<(z.numLearn + 128) / 128, 128, 0, st>>>(P, d, z.numLearn);
+}
+void launch_learn_keep(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    k_learn_keep<<<(z.numBodies + 127) / 128, 128, 0, st>>>(P, d, z.numBodies);
+}
+void launch_learn_target(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    if (z.numLearn) k_learn_target<<<(z.numLearn + 127) / 128, 128, 0, st>>>(P, d, z.numLearn);
+}
+void launch_copy_double(const double* src, double* dst, cudaStream_t st) { k_copy_double<<<1, 32, 0, st>>>(src, dst); }
+
+void launch_mlp_infer(const void* halfW, const float* prm, const float* norm, const float* X, uint32_t n, float* Y,
+                      cudaStream_t st) {
+    if (n == 0) return;
+    const uint32_t warps = (n + 15) / 16;
+    k_mlp_infer<<<(warps + 3) / 4, 128, 0, st>>>(static_cast<const bf16*>(halfW), prm, norm, X, n, Y);
+}
+
+void launch_mlp_mirror(const float* prm, void* halfW, cudaStream_t st) {
+    k_mirror<<<blocks(mlp::NPARAM, 256), 256, 0, st>>>(prm, static_cast<bf16*>(halfW));
+}
+
+uint32_t mlp_param_count() { return mlp::NPARAM; }
+uint32_t mlp_half_count() { return mlp::NHALF; }
+
+}  // namespace avbd
+
+// ---------------------------------------------------------------------------
+// C ABI of the training kernels (no counterpart in the reference: the learned
+// warm start is new).  Every pointer is device memory; `stream` is a
+// cudaStream_t or null.
+// ---------------------------------------------------------------------------
+using namespace avbd;
+extern "C" {
+
+uint32_t avbd_mlp_param_count(void) { return mlp::NPARAM; }
+
+size_t avbd_mlp_workspace_bytes(uint32_t batch) { return work_layout(batch, nullptr, nullptr); }
+
+int avbd_mlp_gradients(const float* params, const float* norm, const float* features, const float* targets,
+                       uint32_t batch, void* workspace, float* grad_out, float* loss_out, void* stream) {
+    if (!params || !norm || !features || !targets || !workspace || batch == 0) return AVBD_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Work w{};
+    work_layout(batch, static_cast<char*>(workspace), &w);
+    forward_backward(params, norm, features, targets, batch, w, st);
+    const uint32_t lb = blocks((size_t)batch * mlp::DOUT, 256);
+    if (grad_out) cudaMemcpyAsync(grad_out, w.grad, sizeof(float) * mlp::NPARAM, cudaMemcpyDeviceToDevice, st);
+    if (loss_out) cudaMemcpyAsync(loss_out, w.lossPart + lb, sizeof(float), cudaMemcpyDeviceToDevice, st);
+    return cudaGetLastError() == cudaSuccess ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+}
+
+int avbd_mlp_train_step(float* params, const float* norm, const float* features, const float* targets,
+                        uint32_t batch, float* adam_m, float* adam_v, uint32_t step, float lr, void* workspace,
+                        float* loss_out, void* stream) {
+    if (!params || !adam_m || !adam_v || step == 0) return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = avbd_mlp_gradients(params, norm, features, targets, batch, workspace, nullptr, loss_out, stream);
+    if (rc != AVBD_OK) return rc;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    Work w{};
+    work_layout(batch, static_cast<char*>(workspace), &w);
+    k_adam<<<blocks(mlp::NPARAM, 256), 256, 0, st>>>(params, w.grad, adam_m, adam_v, step, lr, 0.9f, 0.999f, 1e-8f,
+                                                     w.half);
+    return cudaGetLastError() == cudaSuccess ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+}
+
+int avbd_mlp_infer(const float* params, const float* norm, const float* features, uint32_t n, float* out,
+                   void* workspace, void* stream) {
+    if (!params || !norm || !features || !out || !workspace) return AVBD_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    launch_mlp_mirror(params, workspace, st);
+    launch_mlp_infer(workspace, params, norm, features, n, out, st);
+    return cudaGetLastError() == cudaSuccess ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+}
+
+}  // extern "C"

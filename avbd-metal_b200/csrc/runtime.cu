@@ -90,6 +90,19 @@ struct avbd_solver {
     // are re-captured) when a retired frame used more colors.
     uint32_t colorLaunchBound = 8;
     bool colorBoundFitted = false;
+    // learned warm start
+    static constexpr uint32_t kTraceLength = 2 + 256;
+    int learnMode = AVBD_WARM_START_PLAIN;
+    bool modelSet = false, learnCapture = false, residualTrace = false;
+    uint32_t learnTrials = 1;
+
+    // per-color launches are needed by the learned warm start's trial sweeps
+    // and by the per-iteration residual trace
+    void update_small_solve() {
+        smallSolve = z.numDynamicBodies <= 512 && !P.cloth && learnMode == AVBD_WARM_START_PLAIN && !learnCapture &&
+                     !residualTrace;
+        if (smallSolve) tuneStage = -1;
+    }
     uint64_t frame = 0;
     int failure = AVBD_FAIL_NONE;
     std::string error;
@@ -213,12 +226,63 @@ struct avbd_solver {
             launch_dynamic_coloring(P, f, z, st);
         }
         const uint32_t colorBound = z.dynamicColoring ? colorLaunchBound : H.staticUsedColors;
+        // One primal sweep over every color (trial sweeps of the learned
+        // warm start; the iteration loop below inlines the same sequence).
+        auto sweep = [&]() {
+            for (uint32_t c = 0; c < colorBound; c++) {
+                const uint32_t count = z.dynamicColoring ? 0xFFFFFFFFu : H.colorCounts[c];
+                if (count == 0) continue;
+                launch_primal_color(P, f, z, c, count, H.colorLanes[c], st);
+            }
+            if (z.dynamicColoring) launch_primal_tail(P, f, z, colorLaunchBound, st);
+        };
+        const bool tuningFrame = primalEvents != nullptr;
+        const bool learned = !tuningFrame && learnMode == AVBD_WARM_START_LEARNED && modelSet && z.numLearn;
+        const bool capture = !tuningFrame && learnCapture && z.numLearn;
+        const bool trace = !tuningFrame && residualTrace;
+        const size_t poseBytes = sizeof(float4) * z.numBodies;
+        if (learned || capture || trace) {
+            mark(AVBD_STAGE_LEARNED);
+            if (learned || capture) launch_learn_features(P, f, z, st);
+            cudaMemcpyAsync(f.learnSaveLin, f.posLin, poseBytes, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(f.learnSaveAng, f.posAng, poseBytes, cudaMemcpyDeviceToDevice, st);
+            if (trace) launch_residual(P, f, z, f.learnResidBodies, f.learnTrace + 0, st);
+        }
+        // With one trial sweep the winner's swept pose is kept as the primal
+        // half of the first iteration (the dual follows as usual); with more
+        // trial sweeps both branches are undone and the solve restarts from
+        // the chosen warm start.
+        const bool reuseTrial = learned && learnTrials == 1 && P.iterations > 0;
+        if (learned) {
+            launch_mlp_infer(f.learnHalf, f.learnPrm, f.learnNorm, f.learnFeat, z.numLearn, f.learnPred, st);
+            for (uint32_t t = 0; t < learnTrials; t++) sweep();
+            launch_residual(P, f, z, f.learnResidBodies, f.learnResid + 0, st);
+            if (reuseTrial) {
+                cudaMemcpyAsync(f.learnSweptLin, f.posLin, poseBytes, cudaMemcpyDeviceToDevice, st);
+                cudaMemcpyAsync(f.learnSweptAng, f.posAng, poseBytes, cudaMemcpyDeviceToDevice, st);
+            }
+            cudaMemcpyAsync(f.posLin, f.learnSaveLin, poseBytes, cudaMemcpyDeviceToDevice, st);
+            cudaMemcpyAsync(f.posAng, f.learnSaveAng, poseBytes, cudaMemcpyDeviceToDevice, st);
+            launch_learn_apply(P, f, z, st);
+            if (trace) launch_residual(P, f, z, f.learnResidBodies, f.learnTrace + 1, st);
+            for (uint32_t t = 0; t < learnTrials; t++) sweep();
+            launch_residual(P, f, z, f.learnResidBodies, f.learnResid + 1, st);
+            if (reuseTrial) {
+                launch_learn_keep(P, f, z, st);
+            } else {
+                cudaMemcpyAsync(f.posLin, f.learnSaveLin, poseBytes, cudaMemcpyDeviceToDevice, st);
+                cudaMemcpyAsync(f.posAng, f.learnSaveAng, poseBytes, cudaMemcpyDeviceToDevice, st);
+                launch_learn_select(P, f, z, st);
+            }
+        } else if (trace) {
+            launch_copy_double(f.learnTrace + 0, f.learnTrace + 1, st);
+        }
         if (smallSolve) {
             mark(AVBD_STAGE_PRIMAL);
             launch_solve_small(P, f, z, z.dynamicColoring ? (uint32_t)MAX_COLORS : H.staticUsedColors, st);
         } else {
             for (uint32_t it = 0; it < P.iterations; it++) {
-                for (uint32_t c = 0; c < colorBound; c++) {
+                for (uint32_t c = 0; c < colorBound && !(reuseTrial && it == 0); c++) {
                     const uint32_t count = z.dynamicColoring ? 0xFFFFFFFFu : H.colorCounts[c];
                     if (count == 0) continue;
                     mark(AVBD_STAGE_PRIMAL);
@@ -231,11 +295,14 @@ struct avbd_solver {
                         launch_dat_color(P, f, z, c, count, st);
                     }
                 }
-                if (z.dynamicColoring) launch_primal_tail(P, f, z, colorLaunchBound, st);
+                if (z.dynamicColoring && !(reuseTrial && it == 0)) launch_primal_tail(P, f, z, colorLaunchBound, st);
                 mark(AVBD_STAGE_DUAL);
                 launch_dual(P, f, z, st);
+                if (trace && it + 2 < kTraceLength)
+                    launch_residual(P, f, z, f.learnResidBodies, f.learnTrace + 2 + it, st);
             }
         }
+        if (capture) launch_learn_target(P, f, z, st);
         mark(AVBD_STAGE_FINALIZE);
         if (P.cloth) launch_cloth_restore(P, f, z, st);
         launch_finalize(P, f, z, st);
@@ -316,6 +383,11 @@ struct avbd_solver {
         z.maxDatPairs = H.maxDatPairs;
         z.maxSoft = H.maxSoft;
         z.elemHashSize = H.elemHashSize;
+        z.numLearn = P.cloth ? 0u : (uint32_t)H.learnIdx.size();
+        z.colorCounts = H.dynamicColoring ? nullptr : H.colorCounts.data();
+        z.colorLanes = H.colorLanes.data();
+        z.numDynamicRigid = 0;
+        for (uint32_t b = 0; b < nb; b++) z.numDynamicRigid += (H.posLin[b].w > 0.0f && H.shape[b].w >= 0.0f) ? 1u : 0u;
         const uint32_t scanLimit = 1024u * 1024u;
         if (P.gridHashSize > scanLimit || z.producers > scanLimit || nb > scanLimit) {
             error = "scene exceeds the 1M-element scan limit of this build";
@@ -382,6 +454,21 @@ struct avbd_solver {
         ok = ok && alloc(d.failureLatch, 4, "failureLatch") && alloc(d.frameCounter, 1, "frameCounter", true);
         if (H.dynamicColoring)
             d.colorStart = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(d.counters) + offsetof(Counters, colorStart));
+        if (z.numLearn) {
+            const uint32_t nl = z.numLearn;
+            ok = ok && upload(d.learnIdx, H.learnIdx, "learnIdx");
+            ok = ok && alloc(d.learnFeat, 16 * (size_t)nl, "learnFeatures") && alloc(d.learnPred, 3 * (size_t)nl, "learnPrediction");
+            ok = ok && alloc(d.learnTarget, 3 * (size_t)nl, "learnTarget");
+            ok = ok && alloc(d.learnPrm, mlp_param_count(), "mlpParams") && alloc(d.learnNorm, 64, "mlpNorm");
+            uint16_t* half = nullptr;
+            ok = ok && alloc(half, mlp_half_count(), "mlpWeightsBF16");
+            d.learnHalf = half;
+        }
+        ok = ok && alloc(d.learnSaveLin, nb, "plainWarmStartLin") && alloc(d.learnSaveAng, nb, "plainWarmStartAng");
+        ok = ok && alloc(d.learnSweptLin, nb, "plainTrialLin") && alloc(d.learnSweptAng, nb, "plainTrialAng");
+        ok = ok && alloc(d.learnResidBodies, std::max<uint32_t>(1, H.numDynamicBodies), "residualBodies");
+        ok = ok && alloc(d.learnResid, 4, "residual") && alloc(d.learnTrace, kTraceLength, "residualTrace");
+        ok = ok && alloc(d.learnAccepted, 1, "learnAccepted", true);
         if (P.cloth) {
             // element topology
             ok = ok && upload(reinterpret_cast<u4*&>(d.tris), H.tris, "tris");
@@ -428,7 +515,7 @@ struct avbd_solver {
         std::memset(hostLatch, 0, 4 * sizeof(uint32_t));
         std::memset(hostCounters, 0, sizeof(Counters));
         // Small scenes run their whole iteration loop in one thread block.
-        smallSolve = z.numDynamicBodies <= 512 && !P.cloth;
+        update_small_solve();
         tuneStage = tuning_applies() ? 0 : -1;
         if (cudaDeviceSynchronize() != cudaSuccess) { error = "device error during upload"; return AVBD_ERR_NO_DEVICE; }
         return AVBD_OK;
@@ -744,6 +831,73 @@ int avbd_get_counters(avbd_solver* s, avbd_counters* out) {
     out->dat_ee_degenerate = c.datEEDegenerate;
     out->dat_nonfinite = c.datNonfinite;
     out->dat_tet_degenerate = c.datTetDegenerate;
+    uint32_t accepted = 0;
+    if (s->d.learnAccepted) cudaMemcpy(&accepted, s->d.learnAccepted, 4, cudaMemcpyDeviceToHost);
+    out->learn_accepted = accepted;
+    return AVBD_OK;
+}
+
+int avbd_set_warm_start_model(avbd_solver* s, const float* params, const float* norm, uint32_t trial_sweeps) {
+    if (!s || !params || !norm || trial_sweeps == 0) return AVBD_ERR_INVALID_ARGUMENT;
+    if (s->z.numLearn == 0) {
+        s->error = "the scene has no dynamic particles for the learned warm start (cloth is not supported)";
+        return AVBD_ERR_UNSUPPORTED;
+    }
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    const DevPtrs& d = s->d;
+    if (!s->check(cudaMemcpy(d.learnPrm, params, sizeof(float) * mlp_param_count(), cudaMemcpyHostToDevice), "model upload") ||
+        !s->check(cudaMemcpy(d.learnNorm, norm, sizeof(float) * 64, cudaMemcpyHostToDevice), "model upload"))
+        return AVBD_ERR_RUNTIME_FAILURE;
+    launch_mlp_mirror(d.learnPrm, d.learnHalf, s->launch);
+    if (!s->check(cudaStreamSynchronize(s->launch), "model upload")) return AVBD_ERR_RUNTIME_FAILURE;
+    s->modelSet = true;
+    s->learnTrials = trial_sweeps;
+    s->graphsValid = false;
+    return AVBD_OK;
+}
+
+int avbd_set_warm_start_mode(avbd_solver* s, int mode) {
+    if (!s || (mode != AVBD_WARM_START_PLAIN && mode != AVBD_WARM_START_LEARNED)) return AVBD_ERR_INVALID_ARGUMENT;
+    if (mode == AVBD_WARM_START_LEARNED && !s->modelSet) {
+        s->error = "no warm-start model: call avbd_set_warm_start_model first";
+        return AVBD_ERR_INVALID_ARGUMENT;
+    }
+    s->learnMode = mode;
+    s->update_small_solve();
+    s->graphsValid = false;
+    return AVBD_OK;
+}
+
+int avbd_set_learning_capture(avbd_solver* s, int enabled) {
+    if (!s) return AVBD_ERR_INVALID_ARGUMENT;
+    if (enabled && s->z.numLearn == 0) {
+        s->error = "the scene has no dynamic particles to learn from";
+        return AVBD_ERR_UNSUPPORTED;
+    }
+    s->learnCapture = enabled != 0;
+    s->update_small_solve();
+    s->graphsValid = false;
+    return AVBD_OK;
+}
+
+int avbd_set_residual_trace(avbd_solver* s, int enabled) {
+    if (!s) return AVBD_ERR_INVALID_ARGUMENT;
+    s->residualTrace = enabled != 0;
+    s->update_small_solve();
+    s->graphsValid = false;
+    return AVBD_OK;
+}
+
+int avbd_get_residual_trace(avbd_solver* s, double* out, uint32_t n) {
+    if (!s || !out) return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    const uint32_t len = std::min<uint32_t>(n, avbd_solver::kTraceLength);
+    std::vector<double> sq(len);
+    if (!s->check(cudaMemcpy(sq.data(), s->d.learnTrace, sizeof(double) * len, cudaMemcpyDeviceToHost), "trace readback"))
+        return AVBD_ERR_RUNTIME_FAILURE;
+    for (uint32_t i = 0; i < len; i++) out[i] = std::sqrt(sq[i]);
     return AVBD_OK;
 }
 
@@ -859,6 +1013,9 @@ size_t avbd_debug_buffer_size(avbd_solver* s, int which) {
     case AVBD_BUF_BENDS: return H.bends.size() * sizeof(BendGPU);
     case AVBD_BUF_CLOTH_GROUP: return nb * 4;
     case AVBD_BUF_OGC_PREV: return s->P.cloth ? nb * 16 : 0;
+    case AVBD_BUF_LEARN_IDX: return (size_t)s->z.numLearn * 4;
+    case AVBD_BUF_LEARN_FEATURES: return (size_t)s->z.numLearn * 64;
+    case AVBD_BUF_LEARN_TARGETS: case AVBD_BUF_LEARN_PREDICTIONS: return (size_t)s->z.numLearn * 12;
     case AVBD_BUF_SOFT: case AVBD_BUF_DAT_PAIRS: {
         if (!s->P.cloth) return 0;
         Counters c{};
@@ -918,6 +1075,10 @@ int avbd_debug_read(avbd_solver* s, int which, void* dst, size_t bytes) {
     // element contacts swap like the manifolds
     case AVBD_BUF_SOFT: src = odd ? d.soft : d.prevSoft; break;
     case AVBD_BUF_DAT_PAIRS: src = d.datPairs; break;
+    case AVBD_BUF_LEARN_IDX: src = d.learnIdx; break;
+    case AVBD_BUF_LEARN_FEATURES: src = d.learnFeat; break;
+    case AVBD_BUF_LEARN_TARGETS: src = d.learnTarget; break;
+    case AVBD_BUF_LEARN_PREDICTIONS: src = d.learnPred; break;
     case AVBD_BUF_ADJ_START: case AVBD_BUF_ADJ_COUNT: case AVBD_BUF_ADJ_LIST: {
         // materialise the merged (pre, contacts, post) lists
         std::vector<uint32_t> dc(nb), ds(nb);

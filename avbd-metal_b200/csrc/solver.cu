@@ -836,6 +836,57 @@ __global__ void k_primal(const Params P, const DevPtrs d, uint32_t color, uint32
 }
 
 // ---------------------------------------------------------------------------
+// Residual of the augmented-Lagrangian objective: the primal right-hand side
+// of every dynamic body (inertia + every stamped force) at the current pose,
+// squared and summed.  The square root is r_k of the iterations-to-tolerance
+// measurement.  Bodies come from the color lists (every dynamic body once).
+// ---------------------------------------------------------------------------
+__global__ void k_residual_bodies(const Params P, const DevPtrs d, uint32_t n, float* out) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t slot = tid >> 3, lane = tid & 7u;
+    if (slot >= n) return;
+    const unsigned mask = 0xFFu << (threadIdx.x & 24u);
+    const uint32_t body = d.colorList[slot];
+    const bool rigid = d.shape[body].w >= 0.0f;
+    Accum acc{m3_zero(), m3_zero(), m3_zero(), s3(0), s3(0)};
+    const AdjView v = adj_view(d, body);
+    const uint32_t cnt = v.count();
+    for (uint32_t k = lane; k < cnt; k += 8) stamp_entry(P, d, v.at(k), body, acc);
+#pragma unroll
+    for (int o = 4; o >= 1; o >>= 1) {
+        add_shfl3(mask, acc.rhsLin, o);
+        add_shfl3(mask, acc.rhsAng, o);
+    }
+    if (lane != 0) return;
+    const float4 pl = d.posLin[body];
+    const float dt2 = P.dt * P.dt;
+    float3 rl = acc.rhsLin + (xyz(pl) - xyz(d.inertLin[body])) * (pl.w / dt2);
+    float r2 = dot(rl, rl);
+    if (rigid) {
+        const float4 q = d.posAng[body];
+        const M3 inertia = m3_scale(world_inertia(q, xyz(d.props[body])), 1.0f / dt2);
+        const float3 ra = acc.rhsAng + m3_mul(inertia, q_sub(q, d.inertAng[body]));
+        r2 += dot(ra, ra);
+    }
+    out[slot] = r2;
+}
+
+// Fixed-order sum of n values in one block (double accumulation).
+__global__ void __launch_bounds__(1024) k_sum_fixed(const float* v, uint32_t n, double* out) {
+    __shared__ double part[1024];
+    double s = 0.0;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) s += (double)v[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (uint32_t w = blockDim.x >> 1; w > 0; w >>= 1) {
+        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = part[0];
+}
+
+
+// ---------------------------------------------------------------------------
 // Warp-per-body primal for particles.  The 8-lane kernel above makes each
 // lane walk 2-3 tets as chains of dependent loads.  Here all 32 lanes of a
 // warp evaluate the force terms of 32 adjacency entries at once, and lanes
@@ -1090,7 +1141,10 @@ __device__ __forceinline__ float3 solve3x3_particle(const M3& a, float3 b) {
 // chosen per color from its bodies' adjacency sizes).  Lane p of a group
 // evaluates entry base + p; logical lane l < 8 then folds entries
 // base + l, base + l + 8, ... in order.  Any LANES gives the same floats.
-template <int LANES, bool GENERAL, bool CLOTH>
+// RESID: evaluate instead of solve — lane 0 stores the body's squared
+// right-hand side (the AL gradient) in d.learnResidBodies[slot] and leaves
+// the pose alone (particle-only scenes; called over all colors at once).
+template <int LANES, bool GENERAL, bool CLOTH, bool RESID = false>
 __global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevPtrs d, uint32_t color,
                                                       uint32_t count) {
     constexpr int GROUPS = 32 / LANES;
@@ -1197,6 +1251,11 @@ __global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevP
     if (lane != 0) return;
     const float mass = pl.w;
     const float dt2 = P.dt * P.dt;
+    if (RESID) {
+        const float3 r = acc.rhs + (xyz(pl) - xyz(inert)) * (mass / dt2);
+        d.learnResidBodies[s + slot] = dot(r, r);
+        return;
+    }
     acc.lhs = m3_add(acc.lhs, m3_diag(s3(mass / dt2)));
     acc.rhs += (xyz(pl) - xyz(inert)) * (mass / dt2);
     float3 dxLin = solve3x3_particle(acc.lhs, -acc.rhs);
@@ -1233,6 +1292,37 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
         else if (P.cloth) launch_primal_group<true, true>(P, d, color, upper, w, st);
         else launch_primal_group<true, false>(P, d, color, upper, w, st);
     }
+}
+
+void launch_residual(const Params& P, const DevPtrs& d, const Sizes& z, float* perBody, double* total,
+                     cudaStream_t st) {
+    const uint32_t n = z.numDynamicBodies;
+    if (n && z.numDynamicRigid == 0 && perBody == d.learnResidBodies) {
+        // particle-only: the group stamping of the primal, one launch per
+        // static color at its lane width (or all bodies at 32 lanes)
+        auto run = [&](uint32_t color, uint32_t count, uint32_t lanes) {
+            const uint32_t w = lanes <= 8 ? 8u : (lanes <= 16 ? 16u : 32u);
+            const uint32_t blocks = (count * w + 127) / 128;
+            if (z.particleFastPath) {
+                if (w == 8) k_primal_group<8, false, false, true><<<blocks, 128, 0, st>>>(P, d, color, count);
+                else if (w == 16) k_primal_group<16, false, false, true><<<blocks, 128, 0, st>>>(P, d, color, count);
+                else k_primal_group<32, false, false, true><<<blocks, 128, 0, st>>>(P, d, color, count);
+            } else if (P.cloth) {
+                k_primal_group<32, true, true, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, d, color, count);
+            } else {
+                k_primal_group<32, true, false, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, d, color, count);
+            }
+        };
+        if (z.dynamicColoring || !z.colorCounts) {
+            run(0u, n, 32u);
+        } else {
+            for (uint32_t c = 0; c < MAX_COLORS; c++)
+                if (z.colorCounts[c]) run(c, z.colorCounts[c], z.colorLanes[c]);
+        }
+    } else if (n) {
+        k_residual_bodies<<<(n * 8 + 127) / 128, 128, 0, st>>>(P, d, n, perBody);
+    }
+    k_sum_fixed<<<1, 1024, 0, st>>>(perBody, n, total);
 }
 
 // ---------------------------------------------------------------------------

@@ -681,6 +681,10 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
         H.postList.insert(H.postList.end(), post[b].begin(), post[b].end());
     }
 
+    H.learnIdx.clear();
+    for (uint32_t b = 0; b < nb; b++)
+        if (s->bodies[b].is_particle && H.posLin[b].w > 0.0f) H.learnIdx.push_back(b);
+
     // ---- spinners and parameters (GPUSolver.swift:630-637, :2052-2080)
     H.spinners.assign(s->spinners, s->spinners + s->num_spinners);
     for (const auto& sp : H.spinners) {

@@ -67,6 +67,9 @@ struct HostScene {
     std::vector<uint32_t> nbrStart, nbrCount, nbrList, particleIdx, selfCollision;
     std::vector<MembraneGPU> membranes;
     std::vector<BendGPU> bends;
+
+    // dynamic particles whose warm start the learned model may predict
+    std::vector<uint32_t> learnIdx;
 };
 
 // Returns an AVBD_* status; on failure `err` holds a message.

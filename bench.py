@@ -261,6 +261,60 @@ def primal_bytes_per_iteration(solver, scene):
 
 
 # ---------------------------------------------------------------------------
+MODEL = os.path.join(ROOT, "avbd-metal_b200", "avbd_b200", "models", "soft_cube_24_warm_start.npz")
+
+
+def timed_steps(solver, targets, first, K, stream, flush):
+    """K frames, one CUDA-event pair per frame on the solver stream, with an
+    untimed L2 flush before each; returns the summed device milliseconds."""
+    import torch
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+    for i in range(K):
+        flush.zero_()
+        targets.apply(solver, first + i)
+        starts[i].record(stream)
+        solver.step(1)
+        ends[i].record(stream)
+    torch.cuda.synchronize()
+    return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+
+
+def learned_comparison(args, world, dev, stream, flush, plain_value):
+    """The same workload with the learned warm start, at the iteration count
+    whose median AL residual matches the plain warm start's."""
+    from avbd_b200 import GPUSolver, abi, demos, learned
+    model = learned.WarmStartModel.load(MODEL)
+    plain_iters = make_scene().settings.iterations
+    make = lambda seed: demos.soft_cube_scene(seed=seed, n=24)   # noqa: E731
+    k, r_plain, r_learned, acc = learned.matched_residual_iterations(make, 200, model, plain_iters, frames=120)
+    scene = make_scene()
+    scene.settings.iterations = k
+    solver = GPUSolver(scene, device=dev.index)
+    solver.set_stream(stream.cuda_stream)
+    solver.set_warm_start_model(model.params, model.norm, 1)
+    solver.set_warm_start_mode(abi.WARM_START_LEARNED)
+    targets = MotorTargets(1)
+    solver.step(args.warmup)
+    solver.synchronize()
+    ms = max_over_ranks(timed_steps(solver, targets, 0, args.steps, stream, flush), world, dev)
+    nv = dynamic_vertices(scene)
+    accepted = solver.counters().learn_accepted
+    solver.close()
+    value = world * nv * args.steps / (ms / 1e3)
+    return {"warm_start": "learned: 16-128-128-128-3 MLP, BF16 tensor-core inference, kept only when its "
+                          "residual after 1 trial sweep is no worse than the plain warm start's",
+            "iterations": k, "plain_iterations": plain_iters,
+            "matched_median_rel_residual": {"plain": r_plain, "learned": r_learned,
+                                            "definition": "r_final / r0(plain warm start), r = ||AL gradient||_2 "
+                                                          "over all dynamic DOFs, median over frames 3-120 of seed 200"},
+            "value": value, "unit": unit(), "ms_per_step": ms / args.steps,
+            "speedup_vs_plain": value / plain_value,
+            "accepted_frames": accepted / float(args.warmup + args.steps),
+            "model": "avbd_b200/models/soft_cube_24_warm_start.npz (trained on the GPU by avbd_mlp_train_step "
+                     "from plain rollouts of seeds 100-103)"}
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -347,6 +401,11 @@ def run_ours(args, world, rank, local):
         stage_share = {k: round(v / total_ms, 4) for k, v in prof["stage_ms"].items() if v > 0}
         kernels_per_frame = prof["kernels_per_frame"]
 
+    learned_line = None
+    if WORKLOAD_KEY == "soft-cube" and os.path.exists(MODEL):
+        with torch.cuda.stream(stream):
+            learned_line = learned_comparison(args, world, dev, stream, flush, value)
+
     cpu = None
     if rank == 0 and world == 1:
         thr = host_threads()
@@ -366,7 +425,7 @@ def run_ours(args, world, rank, local):
                        "colors": int(counters.used_colors),
                        "lanes_per_body": prof["color_lanes"][:int(counters.used_colors)],
                        "lane_autotune": "fastest of 8/16/32 lanes per color, timed on the first 3 frames",
-                       "warm_start": "plain (gamma warm start); learned warm start not in this build",
+                       "warm_start": "plain gamma warm start (value); learned warm start in learned_warm_start",
                        "parallelism": (f"world shards x{world}" if WORKLOAD_KEY == "batched-worlds"
                                        else f"replicas x{world}"),
                        "l2": "flushed between timed steps (256 MiB device write, untimed)",
@@ -382,6 +441,7 @@ def run_ours(args, world, rank, local):
                          "avg_launch_us": avg_ms * 1e3, "launches_per_iteration": launches_iter,
                          "measured": f"profiled pass of {prof_frames} frames, CUDA events around every launch"},
             "stage_share": stage_share,
+            "learned_warm_start": learned_line,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

@@ -243,6 +243,7 @@ typedef struct avbd_counters {
     uint32_t dat_ee_degenerate;
     uint32_t dat_nonfinite;
     uint32_t dat_tet_degenerate;
+    uint32_t learn_accepted;      /* frames whose predicted warm start was kept */
 } avbd_counters;
 
 typedef struct avbd_solver avbd_solver;
@@ -334,7 +335,8 @@ enum {
     AVBD_STAGE_PRIMAL = 6, AVBD_STAGE_DUAL = 7, AVBD_STAGE_FINALIZE = 8,
     AVBD_STAGE_ELEMENT_CONTACTS = 9,  /* element grid, pair streams, emission */
     AVBD_STAGE_TRUNCATION = 10,       /* per-color Planar-DAT passes          */
-    AVBD_STAGE_COUNT_ = 11
+    AVBD_STAGE_LEARNED = 11,          /* features, MLP, trial sweeps          */
+    AVBD_STAGE_COUNT_ = 12
 };
 typedef struct avbd_profile {
     uint64_t frames;
@@ -346,6 +348,44 @@ typedef struct avbd_profile {
 } avbd_profile;
 int avbd_set_profiling(avbd_solver* solver, int enabled);
 int avbd_get_profile(avbd_solver* solver, avbd_profile* out);
+
+/* ---- Learned warm start (no counterpart in the reference) -------------
+ * A 16-128-128-128-16 MLP (BF16 weights/activations, FP32 accumulation)
+ * predicts each dynamic particle's correction of the plain gamma warm start
+ * from local features.  In AVBD_WARM_START_LEARNED mode every frame races
+ * the plain and the predicted warm start for `trial_sweeps` primal sweeps and
+ * keeps the prediction only when its augmented-Lagrangian residual is no
+ * larger; plain AVBD stays the fallback.  Parameters are the fp32 block of
+ * avbd_mlp_param_count() floats (W1[128][16], b1, W2[128][128], b2,
+ * W3[128][128], b3, W4[16][128], b4[16]); `norm` holds 64 floats: feature
+ * mean[16], feature 1/std[16], target mean[16], target std[16].          */
+enum { AVBD_WARM_START_PLAIN = 0, AVBD_WARM_START_LEARNED = 1 };
+int avbd_set_warm_start_model(avbd_solver* solver, const float* params, const float* norm,
+                              uint32_t trial_sweeps);
+int avbd_set_warm_start_mode(avbd_solver* solver, int mode);
+/* Record every frame's features and training targets (the solve's
+ * correction of the plain warm start) in the LEARN_* debug buffers.       */
+int avbd_set_learning_capture(avbd_solver* solver, int enabled);
+/* Per-frame residual trace: out[0] at the plain warm start, out[1] at the
+ * warm start used, out[2 + k] after iteration k (sqrt of the summed squared
+ * AL gradient over all dynamic DOFs).  Read after avbd_sync.              */
+int avbd_set_residual_trace(avbd_solver* solver, int enabled);
+int avbd_get_residual_trace(avbd_solver* solver, double* out, uint32_t n);
+
+/* Training kernels (device pointers; stream may be null).  A batch is
+ * features[batch][16] and targets[batch][3] (raw, normalised with `norm`);
+ * the workspace holds avbd_mlp_workspace_bytes(batch) bytes.             */
+uint32_t avbd_mlp_param_count(void);
+size_t avbd_mlp_workspace_bytes(uint32_t batch);
+int avbd_mlp_gradients(const float* params, const float* norm, const float* features,
+                       const float* targets, uint32_t batch, void* workspace, float* grad_out,
+                       float* loss_out, void* stream);
+int avbd_mlp_train_step(float* params, const float* norm, const float* features,
+                        const float* targets, uint32_t batch, float* adam_m, float* adam_v,
+                        uint32_t step, float lr, void* workspace, float* loss_out, void* stream);
+/* Inference over n feature rows into out[n][3] (workspace >= 80 KiB).     */
+int avbd_mlp_infer(const float* params, const float* norm, const float* features, uint32_t n,
+                   float* out, void* workspace, void* stream);
 
 /* Read-only access to one internal buffer for parity checks and tools
  * (no counterpart in the reference's public API; its tests read the same
@@ -366,7 +406,11 @@ enum {
     AVBD_BUF_NBR_COUNT = 29, AVBD_BUF_NBR_LIST = 30, AVBD_BUF_PARTICLE_IDX = 31,
     AVBD_BUF_MEMBRANES = 32, AVBD_BUF_BENDS = 33, AVBD_BUF_SOFT = 34,
     AVBD_BUF_DAT_PAIRS = 35, AVBD_BUF_CLOTH_GROUP = 36, AVBD_BUF_OGC_PREV = 37,
-    AVBD_BUF_COUNT_ = 38
+    /* learned warm start: vertex ids, features [n][16], targets and
+     * predictions [n][3] of the last frame                                  */
+    AVBD_BUF_LEARN_IDX = 38, AVBD_BUF_LEARN_FEATURES = 39, AVBD_BUF_LEARN_TARGETS = 40,
+    AVBD_BUF_LEARN_PREDICTIONS = 41,
+    AVBD_BUF_COUNT_ = 42
 };
 size_t avbd_debug_buffer_size(avbd_solver* solver, int which);
 int avbd_debug_read(avbd_solver* solver, int which, void* dst, size_t bytes);

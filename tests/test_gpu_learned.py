@@ -1,0 +1,107 @@
+"""Learned warm start on the GPU: the BF16 tensor-core training kernels'
+gradients against the float64 oracle, fused inference against the oracle,
+the solver integration (a model that predicts no correction reproduces the
+plain trajectory bit for bit) and that training lowers the loss."""
+import numpy as np
+import pytest
+
+from avbd_b200 import abi, demos, learned
+from avbd_b200.solver import GPUSolver
+
+pytestmark = pytest.mark.gpu
+
+
+def _random_batch(rng, B):
+    X = rng.normal(size=(B, 16)).astype(np.float32)
+    X[:, 15] = 1.0
+    T = rng.normal(size=(B, 3)).astype(np.float32)
+    return X, T
+
+
+def _norm(rng):
+    n = np.zeros(64, np.float32)
+    n[:16] = rng.normal(0, 0.1, 16)
+    n[16:32] = rng.uniform(0.5, 2.0, 16)
+    n[32:48] = 0.0
+    n[32:35] = rng.normal(0, 0.1, 3)
+    n[48:64] = 1.0
+    n[48:51] = rng.uniform(0.5, 2.0, 3)
+    return n
+
+
+@pytest.mark.parametrize("B", [192, 4096])
+def test_gradients_match_float64_oracle(cuda_lib, oracle_lib, B):
+    from oracle import mlp_oracle as M
+    rng = np.random.default_rng(B)
+    p = learned.init_params(seed=B)
+    p[M.OB1:M.OW2] = rng.normal(0, 0.1, M.HID)       # nonzero biases exercise every term
+    p[M.OB3:M.OW4] = rng.normal(0, 0.1, M.HID)
+    norm = _norm(rng)
+    X, T = _random_batch(rng, B)
+    loss, g = learned.gradients(p, norm, X, T)
+    wl, wg = M.forward_backward(p, norm, X, T, rounded=True)
+    assert abs(loss - wl) <= 1e-4 * max(1.0, abs(wl)), (loss, wl)
+    for name, (a, b) in {"W1": (M.OW1, M.OB1), "b1": (M.OB1, M.OW2), "W2": (M.OW2, M.OB2),
+                         "b2": (M.OB2, M.OW3), "W3": (M.OW3, M.OB3), "b3": (M.OB3, M.OW4),
+                         "W4": (M.OW4, M.OB4), "b4": (M.OB4, M.NPARAM)}.items():
+        err = np.linalg.norm(g[a:b] - wg[a:b]) / max(np.linalg.norm(wg[a:b]), 1e-12)
+        assert err <= 5e-3, (name, err)
+
+
+def test_inference_matches_oracle(cuda_lib, oracle_lib):
+    from oracle import mlp_oracle as M
+    rng = np.random.default_rng(7)
+    p = learned.init_params(seed=3)
+    p[M.OB4:M.OB4 + 3] = [0.1, -0.2, 0.3]
+    norm = _norm(rng)
+    X, _ = _random_batch(rng, 1000)
+    y = learned.infer(p, norm, X)
+    want = M.predict(p, norm, X, rounded=True)
+    scale = np.abs(want).max()
+    assert np.abs(y - want).max() <= 1e-3 * scale + 1e-6
+
+
+def test_zero_correction_model_reproduces_plain_frames(cuda_lib):
+    """A model whose every prediction is zero: x_learned == x_plain, the
+    trial sweeps are undone, every frame accepts, and the trajectory is the
+    plain one bit for bit."""
+    s = demos.soft_cube_scene(seed=3, n=6)
+    plain, learn = GPUSolver(s), GPUSolver(s)
+    norm = np.zeros(64, np.float32)
+    norm[16:32] = 1.0
+    norm[48:64] = 1.0
+    learn.set_warm_start_model(np.zeros(learned.NPARAM, np.float32), norm, 2)
+    learn.set_warm_start_mode(abi.WARM_START_LEARNED)
+    for f in range(40):
+        plain.step(1)
+        learn.step(1)
+        a, _ = plain.positions()
+        b, _ = learn.positions()
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f
+    assert learn.counters().learn_accepted == 40
+
+
+def test_training_learns_the_correction(cuda_lib):
+    """Trained on the solver's own rollouts, the network explains most of the
+    variance of the solve's correction of the plain warm start."""
+    X, T = learned.collect(lambda seed: demos.soft_cube_scene(seed=seed, n=10), seeds=[1, 2], frames=60)
+    assert X.shape[1] == 16 and T.shape[1] == 3 and X.shape[0] == T.shape[0] > 1000
+    m = learned.train(X, T, steps=800, batch=4096, lr=1e-3, log_every=100)
+    pred = learned.infer(m.params, m.norm, X)
+    explained = 1.0 - ((pred - T) ** 2).mean(axis=0) / T.var(axis=0)
+    print("loss history", [round(h, 4) for h in m.history], "explained variance", np.round(explained, 3))
+    assert explained[2] > 0.5 and np.mean(m.history[-3:]) < np.mean(m.history[:2])
+
+
+def test_learned_warm_start_lowers_the_residual(cuda_lib):
+    """The committed soft-cube model, on a held-out seed: at equal iteration
+    counts the learned warm start leaves a smaller median AL residual."""
+    import os
+    path = os.path.join(os.path.dirname(learned.__file__), "models", "soft_cube_24_warm_start.npz")
+    model = learned.WarmStartModel.load(path)
+    make = lambda seed: demos.soft_cube_scene(seed=seed, n=24)   # noqa: E731
+    p = learned.evaluate(make, 201, None, 50, 10)
+    q = learned.evaluate(make, 201, model, 50, 10)
+    print(f"10 iterations: r/r0 plain {p['rel_residual_final']:.4f} learned {q['rel_residual_final']:.4f}, "
+          f"accepted {q['accepted']}/{q['frames']}")
+    assert q["accepted"] > 0 and q["rel_residual_final"] < p["rel_residual_final"]
