@@ -5,7 +5,7 @@ tests/test_abi.py checks the sizes against the compiled library.
 """
 import ctypes as C
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 # status codes
 OK = 0
@@ -160,6 +160,7 @@ class Counters(C.Structure):
         ("dat_truncations", C.c_uint32), ("dat_vt_degenerate", C.c_uint32),
         ("dat_ee_degenerate", C.c_uint32), ("dat_nonfinite", C.c_uint32),
         ("dat_tet_degenerate", C.c_uint32), ("learn_accepted", C.c_uint32),
+        ("soft_rt", C.c_uint32), ("soft_vt", C.c_uint32), ("soft_ee", C.c_uint32),
     ]
 
 

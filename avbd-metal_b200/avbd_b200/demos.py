@@ -384,8 +384,68 @@ def box_field_scene(count: int = 700, seed: int = 4) -> PhysicsScene:
     return s
 
 
+def mixed_scene(seed: int = 5, cubes: int = 64, cube_n: int = 10, boxes: int = 256, cloth_n: int = 128,
+                iterations: int = 20, cube_size: float = 0.3, pitch: float = 0.5) -> PhysicsScene:
+    """Mixed scene: `cubes` soft cubes of cube_n^3 vertices (Stable
+    Neo-Hookean E=5e4 Pa, nu=0.45, density 1000, side `cube_size`) on a
+    square grid of pitch `pitch`, `boxes` rigid boxes with edges U(0.1, 0.4) m
+    above them, and a cloth_n x cloth_n sheet (membrane mu = lambda = 1e4,
+    Bergou bending 1e-3, contact radius 5e-3 m, areal density 0.1 kg/m^2)
+    covering the field from above, all falling together onto the ground;
+    dt 1/60.  Tets and cloth together select isotropic OGC truncation; every
+    soft surface, the cloth and the boxes meet through vertex-triangle,
+    edge-edge and rigid-triangle contacts.  Positions and box sizes come
+    from the seed."""
+    rng = SplitMix64(seed)
+    s = PhysicsScene("mixed")
+    st = s.settings
+    st.dt, st.gravity, st.iterations = 1.0 / 60.0, -9.81, iterations
+    add_ground(s, friction=0.5)
+    E, nu, rho = 5.0e4, 0.45, 1000.0
+    mu = E / (2.0 * (1.0 + nu))
+    lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+    g = int(math.ceil(math.sqrt(cubes)))
+    extent = g * pitch
+    node_mass = rho * cube_size ** 3 / cube_n ** 3
+    for c in range(cubes):
+        cx = (c % g) * pitch - extent / 2 + pitch / 2 + rng.uniform(-0.02, 0.02)
+        cy = (c // g) * pitch - extent / 2 + pitch / 2 + rng.uniform(-0.02, 0.02)
+        cz = cube_size / 2 + 0.05 + rng.uniform(0.0, 0.1)
+        add_soft_block(s, (cx, cy, cz), cube_n, cube_n, cube_n, cube_size / (cube_n - 1), mu=mu, lam=lam,
+                       mass_per_node=node_mass, friction=0.5, exclusion_joints=False)
+    bg = int(math.ceil(math.sqrt(boxes)))
+    bpitch = extent / bg
+    for b in range(boxes):
+        size = (rng.uniform(0.1, 0.4), rng.uniform(0.1, 0.4), rng.uniform(0.1, 0.4))
+        bx = (b % bg) * bpitch - extent / 2 + bpitch / 2
+        by = (b // bg) * bpitch - extent / 2 + bpitch / 2
+        s.add_body(size, 500.0, 0.5, (bx, by, cube_size + 0.45 + rng.uniform(0.0, 0.2)))
+    if cloth_n >= 2:
+        side = f32(extent)
+        spacing = side / f32(cloth_n - 1)
+        z = cube_size + 1.2
+        pos = [[(float(f32(i) * spacing - side / f32(2)), float(f32(j) * spacing - side / f32(2)), z)
+                for j in range(cloth_n)] for i in range(cloth_n)]
+        mass = float(f32(0.1) * side * side / f32(cloth_n * cloth_n))
+        add_cloth_grid(s, pos, 5e-3, mass, 0.5, hard_rods=True, membrane_mu=1e4, membrane_bend=1e-3)
+    return s
+
+
+def two_cubes_scene(n: int = 5, iterations: int = 10) -> PhysicsScene:
+    """Two soft cubes, one dropped onto the other: vertex-triangle contacts
+    between separate soft surfaces (isotropic OGC)."""
+    s = PhysicsScene("two-cubes")
+    add_ground(s, friction=0.5)
+    for z in (0.16, 0.52):
+        add_soft_block(s, (0.03 * (z > 0.3), 0.0, z), n, n, n, 0.3 / (n - 1), mu=3000.0, lam=30000.0,
+                       mass_per_node=0.05, friction=0.5, exclusion_joints=False)
+    s.settings.iterations = iterations
+    return s
+
+
 SCENES = {
     "rigid-stack": rigid_stack_scene,
     "soft-cube": soft_cube_scene,
     "cloth-sphere": cloth_sphere_scene,
+    "mixed": mixed_scene,
 }

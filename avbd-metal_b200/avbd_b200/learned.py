@@ -2,7 +2,7 @@
 training with the library's BF16 tensor-core kernels, and evaluation in
 iterations-to-tolerance against the plain gamma warm start.
 
-The network (csrc/learned.cu) maps 16 per-vertex features to the correction
+The network (csrc/learned.cu) maps 32 per-vertex features to the correction
 the solve applies to the plain warm start.  Training runs on the GPU through
 avbd_mlp_train_step (forward, backward and Adam are the library's kernels;
 torch only owns the device buffers).
@@ -19,7 +19,8 @@ import numpy as np
 from . import abi
 from .solver import GPUSolver, load_library
 
-DIN, HID, DOUT, USED = 16, 128, 16, 3
+DIN, HID, DOUT, USED = 32, 128, 16, 3
+NNORM, XM, XI, YM, YS = 96, 0, 32, 64, 80
 NPARAM = HID * DIN + HID + 2 * (HID * HID + HID) + DOUT * HID + DOUT
 
 
@@ -36,19 +37,16 @@ def init_params(seed: int = 0) -> np.ndarray:
 
 
 def fit_norm(features: np.ndarray, targets: np.ndarray) -> np.ndarray:
-    """Per-feature mean and 1/std, per-target mean and std (64 floats)."""
-    n = np.zeros(64, np.float32)
+    """Per-feature mean and 1/std, per-target mean and std (96 floats)."""
+    n = np.zeros(NNORM, np.float32)
     mu = features.mean(axis=0)
     sd = features.std(axis=0)
-    n[:16] = mu
-    n[16:32] = np.where(sd > 1e-6, 1.0 / np.maximum(sd, 1e-6), 1.0)
-    n[16 + 15] = 1.0                                   # the constant feature
-    n[15] = 0.0
-    tm = targets.mean(axis=0)
-    ts = targets.std(axis=0)
-    n[32:32 + USED] = tm
-    n[48:48 + USED] = np.maximum(ts, 1e-6)
-    n[48 + USED:64] = 1.0
+    const = sd <= 1e-6                                  # constant features pass through
+    n[XM:XM + DIN] = np.where(const, 0.0, mu)
+    n[XI:XI + DIN] = np.where(const, 1.0, 1.0 / np.maximum(sd, 1e-6))
+    n[YM:YM + USED] = targets.mean(axis=0)
+    n[YS:YS + USED] = np.maximum(targets.std(axis=0), 1e-6)
+    n[YS + USED:NNORM] = 1.0
     return n
 
 
@@ -233,13 +231,22 @@ def _main(argv=None):
     ap.add_argument("--seeds", type=int, nargs="+", default=[100, 101, 102, 103])
     ap.add_argument("--frames", type=int, default=200)
     ap.add_argument("--every", type=int, default=2)
-    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--target-iterations", type=int, default=80,
+                    help="iterations of the rollouts that give the targets (a more converged solve than the "
+                         "iteration counts the model is used at)")
+    ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval-seed", type=int, default=200)
     a = ap.parse_args(argv)
     scene = lambda s: demos.soft_cube_scene(seed=s, n=a.n)   # noqa: E731
-    X, T = collect(scene, a.seeds, a.frames, every=a.every)
+
+    def rollout_scene(s):
+        sc = scene(s)
+        sc.settings.iterations = a.target_iterations
+        return sc
+
+    X, T = collect(rollout_scene, a.seeds, a.frames, every=a.every)
     model = train(X, T, steps=a.steps, batch=a.batch, lr=a.lr)
     model.save(a.out)
     print(f"samples {len(X)}, loss {model.history[0]:.4f} -> {model.history[-1]:.4f}")

@@ -240,7 +240,7 @@ class GPUSolver:
 
     # ---- learned warm start ------------------------------------------------
     def set_warm_start_model(self, params, norm, trial_sweeps: int = 1) -> None:
-        """Upload an MLP (fp32 parameter block and 64-float normalisation)."""
+        """Upload an MLP (fp32 parameter block and 96-float normalisation)."""
         p = np.ascontiguousarray(params, np.float32)
         n = np.ascontiguousarray(norm, np.float32)
         self._check(load_library().avbd_set_warm_start_model(self._h, p.ctypes.data, n.ctypes.data,
@@ -262,8 +262,8 @@ class GPUSolver:
         return out
 
     def learning_sample(self):
-        """(features [n][16], targets [n][3]) of the last captured frame."""
-        f = self.debug_read("LEARN_FEATURES", np.float32).reshape(-1, 16)
+        """(features [n][32], targets [n][3]) of the last captured frame."""
+        f = self.debug_read("LEARN_FEATURES", np.float32).reshape(-1, 32)
         t = self.debug_read("LEARN_TARGETS", np.float32).reshape(-1, 3)
         return f, t
 

@@ -110,6 +110,8 @@ struct Params {
     uint32_t numEdges, numSurfaceEdges, elemHashSize;
     uint32_t maxDatPairs, maxSoft, softMapCapacity, numMembranes, numBends;
     float elemMargin, queryRadius, elemCellSize, surfaceCellSize, clothViscosity;
+    // isotropic OGC element contacts (tet surfaces, mixed scenes)
+    uint32_t ogc;
 };
 
 // Device counters of one frame (the reference's CTR_* layout, trimmed).
@@ -132,6 +134,12 @@ struct Counters {
     uint32_t datPairsPeak, datVTPeak, datEEPeak;
     uint32_t datGridOverflow, datInvalidAnchor, datTruncations;
     uint32_t datVTDegenerate, datEEDegenerate, datNonfinite, datTetDegenerate;
+    // isotropic OGC bound exceeders: [0], [1] alternate over the iterations
+    // (the refresh after iteration k reads slot k & 1 and clears the other);
+    // [2], [3] count the plain and predicted trial sweeps of the learned warm
+    // start
+    uint32_t ogcSlots[4];
+    uint32_t numSoftVT, numSoftEE;   // isotropic element contacts of this frame
 };
 
 }  // namespace avbd

@@ -79,11 +79,24 @@ struct DevPtrs {
     uint32_t* truncBits;                        // Planar-DAT step fraction per body (float bits)
     float4 *ogcPrev, *posNext, *angNext;
     uint32_t* bigScanScratch;
+    // isotropic OGC (tet surfaces, mixed scenes): tracker topology (static),
+    // tracked closest elements (this frame / previous frame), conservative
+    // bounds (squared distances as float bits), the bound-exceeder count the
+    // primal of this pass adds to
+    uint4 *triAdj;
+    uint32_t *nbr2Start, *nbr2Count, *nbr2List;
+    uint32_t *vertEdgeStart, *vertEdgeCount, *vertEdgeList;
+    uint32_t* clothVert;
+    uint4 *vtTrack, *vtTrackPrev, *eeTrack, *eeTrackPrev;
+    uint32_t* ogcBounds;
+    uint32_t* ogcExceed;                        // one of counters->ogcSlots
+    uint32_t* elemCellsTmp;                     // bucket contents before the per-bucket sort
     // learned warm start
     uint32_t* learnIdx;                         // dynamic particles the model predicts
-    float *learnFeat, *learnPred, *learnTarget; // [n][16], [n][3], [n][3]
+    float *learnFeat, *learnPred, *learnTarget; // [n][32], [n][3], [n][3]
     float4 *learnSaveLin, *learnSaveAng;        // the plain warm start
-    float4 *learnSweptLin, *learnSweptAng;      // the plain branch after its trial sweep
+    float4 *learnSweptLin, *learnSweptAng;      // pose buffers of the predicted trial branch
+    uint32_t* learnSlot;                        // body -> index in learnIdx (or 0xFFFFFFFF)
     float *learnPrm, *learnNorm, *learnResidBodies;
     void* learnHalf;                            // BF16 weight mirror
     double* learnResid;                         // [0] plain, [1] predicted, [2] scratch
@@ -153,13 +166,27 @@ void launch_cloth_accept(const Params& P, const DevPtrs& d, const Sizes& z, cuda
 void launch_dat_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color, uint32_t count,
                       cudaStream_t st);
 void launch_cloth_restore(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+// rigid-feature-vs-triangle records at the head of the soft list
+void launch_rt_emit(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+// soft totals over `owners` query owners, then the soft persistence map
+void launch_soft_map(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t owners, cudaStream_t st);
+// isotropic OGC: element grid, V-T / E-E trackers and bounds, rigid-triangle
+// and element contact records, soft map (once per frame, before warm start)
+void launch_ogc_detect(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+// publish one color's solve (posNext -> posLin) in color-Jacobi scenes
+void launch_publish_color(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count, cudaStream_t st);
+// mid-solve OGC bound refresh when more than 1% of surface vertices hit their
+// bound in the pass counted by `readSlot`; zeroes `zeroSlot` for the next pass
+void launch_ogc_refresh(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t* readSlot, uint32_t* zeroSlot,
+                        cudaStream_t st);
 void launch_cloth_smoothing(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 
 // learned warm start (learned.cu)
 void launch_learn_features(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 void launch_learn_apply(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 void launch_learn_select(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
-void launch_learn_keep(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_learn_branch(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+void launch_learn_adopt(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 void launch_learn_target(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 void launch_copy_double(const double* src, double* dst, cudaStream_t st);
 void launch_mlp_infer(const void* halfW, const float* prm, const float* norm, const float* X, uint32_t n, float* Y,
@@ -167,5 +194,6 @@ void launch_mlp_infer(const void* halfW, const float* prm, const float* norm, co
 void launch_mlp_mirror(const float* prm, void* halfW, cudaStream_t st);
 uint32_t mlp_param_count();
 uint32_t mlp_half_count();
+uint32_t mlp_norm_count();
 
 }  // namespace avbd

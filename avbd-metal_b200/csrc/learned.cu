@@ -1,4 +1,4 @@
-// learned.cu — learned warm start: per-vertex features, a 16-128-128-128-16
+// learned.cu — learned warm start: per-vertex features, a 32-128-128-128-16
 // MLP (BF16 weights and activations, FP32 accumulation on the tensor cores)
 // for inference and training, and the acceptance test that keeps a predicted
 // warm start only when it is no worse than the plain gamma warm start.
@@ -6,13 +6,18 @@
 // The MLP predicts the correction the solve applies to the plain warm start
 // of every dynamic particle, in units of s = max(|g|, 1) dt^2:
 //   x0 = x_plain + s * MLP(features).
-// Features (16, normalised by per-feature mean and 1/std stored with the
-// model): inertial offset (x~ - x_start)/s, plain warm-start offset
-// (x_plain - x_start)/s, previous-frame displacement v_prev dt / s, incident
-// contact count / 4, summed oriented contact normal, smallest contact gap / s
-// (clipped), log(1 + stiffness dt^2 / m) of the incident elements, and 1.
+// Features (32, normalised by per-feature mean and 1/std stored with the
+// model): [0-2] inertial offset (x~ - x_start)/s, [3-5] plain warm-start
+// offset (x_plain - x_start)/s, [6-8] previous-frame displacement
+// v_prev dt / s, [9] incident contact count / 4, [10-12] summed oriented
+// contact normal, [13] smallest contact gap / s (clipped), [14] log(1 +
+// stiffness dt^2 / m) of the incident elements, [15] 1; [16-24] reserved
+// zeros; 1-ring aggregates over the vertices sharing a tet or spring: [25]
+// ring size / 10, [26] mean neighbour contact count / 4, [27] smallest
+// neighbour contact gap / s (clipped); [28-31] reserved zeros.  Contacts are
+// rigid manifolds and element contacts alike.
 //
-// Parameter block (fp32, also the layout of the gradients): W1[128][16], b1,
+// Parameter block (fp32, also the layout of the gradients): W1[128][32], b1,
 // W2[128][128], b2, W3[128][128], b3, W4[16][128], b4[16].  The weights are
 // mirrored as BF16 for the tensor cores.
 #include <cuda_bf16.h>
@@ -24,14 +29,14 @@
 namespace avbd {
 
 namespace mlp {
-constexpr int DIN = 16, HID = 128, DOUT = 16, USED_OUT = 3;
+constexpr int DIN = 32, HID = 128, DOUT = 16, USED_OUT = 3;
 constexpr uint32_t OW1 = 0, OB1 = OW1 + HID * DIN, OW2 = OB1 + HID, OB2 = OW2 + HID * HID, OW3 = OB2 + HID,
                    OB3 = OW3 + HID * HID, OW4 = OB3 + HID, OB4 = OW4 + DOUT * HID, NPARAM = OB4 + DOUT;
 // bf16 weight mirror: W1 | W2 | W3 | W4
 constexpr uint32_t HW1 = 0, HW2 = HW1 + HID * DIN, HW3 = HW2 + HID * HID, HW4 = HW3 + HID * HID,
                    NHALF = HW4 + DOUT * HID;
-// normalisation block: xmean[16], xinvstd[16], ymean[16], ystd[16]
-constexpr uint32_t NNORM = 64;
+// normalisation block: xmean[32], xinvstd[32], ymean[16], ystd[16]
+constexpr uint32_t NNORM = 96, NX_MEAN = 0, NX_INV = 32, NY_MEAN = 64, NY_STD = 80;
 }  // namespace mlp
 
 namespace {
@@ -70,20 +75,27 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const bf16* __restrict__ W, c
     if (row0 >= n) return;
     const uint32_t r0 = row0 + g, r1 = row0 + g + 8;
     auto xin = [&](uint32_t r, uint32_t c) {
-        return r < n ? (X[r * DIN + c] - norm[c]) * norm[16 + c] : 0.0f;
+        return r < n ? (X[r * DIN + c] - norm[NX_MEAN + c]) * norm[NX_INV + c] : 0.0f;
     };
     uint32_t a[8][4];
-    a[0][0] = pack_bf16(xin(r0, 2 * q), xin(r0, 2 * q + 1));
-    a[0][1] = pack_bf16(xin(r1, 2 * q), xin(r1, 2 * q + 1));
-    a[0][2] = pack_bf16(xin(r0, 2 * q + 8), xin(r0, 2 * q + 9));
-    a[0][3] = pack_bf16(xin(r1, 2 * q + 8), xin(r1, 2 * q + 9));
+#pragma unroll
+    for (int kb = 0; kb < DIN / 16; kb++) {
+        const uint32_t c0 = 16 * kb + 2 * q;
+        a[kb][0] = pack_bf16(xin(r0, c0), xin(r0, c0 + 1));
+        a[kb][1] = pack_bf16(xin(r1, c0), xin(r1, c0 + 1));
+        a[kb][2] = pack_bf16(xin(r0, c0 + 8), xin(r0, c0 + 9));
+        a[kb][3] = pack_bf16(xin(r1, c0 + 8), xin(r1, c0 + 9));
+    }
     float acc[16][4];
-    // layer 1: K = 16
+    // layer 1: K = DIN
 #pragma unroll
     for (int j = 0; j < 16; j++) {
         acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-        const bf16* w = W + HW1 + (8 * j + g) * DIN + 2 * q;
-        mma_bf16(acc[j], a[0][0], a[0][1], a[0][2], a[0][3], ld_pair(w), ld_pair(w + 8));
+#pragma unroll
+        for (int kb = 0; kb < DIN / 16; kb++) {
+            const bf16* w = W + HW1 + (8 * j + g) * DIN + 16 * kb + 2 * q;
+            mma_bf16(acc[j], a[kb][0], a[kb][1], a[kb][2], a[kb][3], ld_pair(w), ld_pair(w + 8));
+        }
     }
     const float* bias = prm + OB1;
     const bf16* Wl = W + HW2;
@@ -142,7 +154,7 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const bf16* __restrict__ W, c
                 const uint32_t c = 2 * q + e;
                 if (c >= (uint32_t)USED_OUT) continue;
                 const float v = o[0][2 * h + e] + prm[OB4 + c];
-                Y[r * USED_OUT + c] = v * norm[48 + c] + norm[32 + c];
+                Y[r * USED_OUT + c] = v * norm[NY_STD + c] + norm[NY_MEAN + c];
             }
         }
     }
@@ -235,7 +247,7 @@ __global__ void k_norm_input(const float* X, const float* norm, uint32_t rows, b
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows * mlp::DIN) return;
     const uint32_t c = i % mlp::DIN;
-    Xb[i] = __float2bfloat16((X[i] - norm[c]) * norm[16 + c]);
+    Xb[i] = __float2bfloat16((X[i] - norm[mlp::NX_MEAN + c]) * norm[mlp::NX_INV + c]);
 }
 
 // Output layer and loss: Y = Z + b4; dY = 2 (Y - Tn) / rows on the used
@@ -249,7 +261,7 @@ __global__ void k_loss_grad(const float* Z, const float* b4, const float* T, con
         float g = 0.0f;
         if (c < (uint32_t)mlp::USED_OUT) {
             const float y = Z[i] + b4[c];
-            const float t = (T[r * mlp::USED_OUT + c] - norm[32 + c]) / norm[48 + c];
+            const float t = (T[r * mlp::USED_OUT + c] - norm[mlp::NY_MEAN + c]) / norm[mlp::NY_STD + c];
             const float e = y - t;
             l = e * e;
             g = 2.0f * e / (float)rows;
@@ -426,8 +438,9 @@ namespace {
 __device__ __forceinline__ float step_scale(const Params& P) { return fmaxf(fabsf(P.gravity), 1.0f) * P.dt * P.dt; }
 
 // Per-vertex features at the plain warm start (see the file comment).  The
-// contact features walk the body's per-frame segment (manifolds), the
-// stiffness feature its static segments (springs; tets, membranes, bends).
+// contact features walk the body's per-frame segment (manifolds, element
+// contacts), the stiffness feature its static segments (springs; tets,
+// membranes, bends).
 __global__ void k_learn_features(const Params P, const DevPtrs d, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -443,13 +456,23 @@ __global__ void k_learn_features(const Params P, const DevPtrs d, uint32_t n) {
     const uint32_t ds = d.dynStart[v], dc = d.dynCount[v];
     for (uint32_t k = 0; k < dc; k++) {
         const uint32_t e = d.dynList[ds + k];
-        if ((e >> ADJ_KIND_SHIFT) != FK_MANIFOLD) continue;
-        const ManifoldGPU& m = d.manifolds[e & ADJ_INDEX_MASK];
-        const float sg = m.header.x == v ? 1.0f : -1.0f;
-        nsum += xyz(m.basisN) * sg;
-        for (uint32_t c = 0; c < m.header.z; c++) {
+        const uint32_t kind = e >> ADJ_KIND_SHIFT;
+        if (kind == FK_MANIFOLD) {
+            const ManifoldGPU& m = d.manifolds[e & ADJ_INDEX_MASK];
+            const float sg = m.header.x == v ? 1.0f : -1.0f;
+            nsum += xyz(m.basisN) * sg;
+            for (uint32_t c = 0; c < m.header.z; c++) {
+                count += 1.0f;
+                gap = fminf(gap, m.contacts[c].C0.x);
+            }
+        } else if (kind == FK_SOFT) {
+            // element contact: the vertex's side of the stencil gives the sign
+            const SoftContactGPU& sc = d.soft[e & ADJ_INDEX_MASK];
+            const float w = sc.ids.x == v ? sc.weights.x : (sc.ids.y == v ? sc.weights.y
+                                                            : (sc.ids.z == v ? sc.weights.z : sc.weights.w));
+            nsum += xyz(sc.normal) * (w >= 0.0f ? 1.0f : -1.0f);
             count += 1.0f;
-            gap = fminf(gap, m.contacts[c].C0.x);
+            gap = fminf(gap, sc.C0.x);
         }
     }
     float stiff = 0.0f;
@@ -464,7 +487,48 @@ __global__ void k_learn_features(const Params P, const DevPtrs d, uint32_t n) {
         else if (kind == FK_MEMBRANE) stiff += d.membranes[idx].mat.x + d.membranes[idx].mat.y;
         else if (kind == FK_BEND) stiff += d.bends[idx].mat.x;
     }
+    // 1-ring contact state: vertices sharing a tet (post segment) or a
+    // spring (pre segment); their contact count and closest gap
+    float ringN = 0.0f, ringContacts = 0.0f, ringGap = 1e30f;
+    auto visit = [&](uint32_t u) {
+        if (u == v || u == WORLD_BODY) return;
+        ringN += 1.0f;
+        if (d.posLin[u].w <= 0.0f) return;
+        const uint32_t us = d.dynStart[u], uc = d.dynCount[u];
+        for (uint32_t k = 0; k < uc; k++) {
+            const uint32_t e = d.dynList[us + k];
+            const uint32_t kind = e >> ADJ_KIND_SHIFT;
+            if (kind == FK_MANIFOLD) {
+                const ManifoldGPU& m = d.manifolds[e & ADJ_INDEX_MASK];
+                for (uint32_t c = 0; c < m.header.z; c++) {
+                    ringContacts += 1.0f;
+                    ringGap = fminf(ringGap, m.contacts[c].C0.x);
+                }
+            } else if (kind == FK_SOFT) {
+                ringContacts += 1.0f;
+                ringGap = fminf(ringGap, d.soft[e & ADJ_INDEX_MASK].C0.x);
+            }
+        }
+    };
+    for (uint32_t k = 0; k < sg.y; k++) {
+        const uint32_t e = d.preList[sg.x + k];
+        if ((e >> ADJ_KIND_SHIFT) != FK_SPRING) continue;
+        const SpringGPU& sp = d.springs[e & ADJ_INDEX_MASK];
+        visit(sp.header.x == v ? sp.header.y : sp.header.x);
+    }
+    for (uint32_t k = 0; k < sg.w; k++) {
+        const uint32_t e = d.postList[sg.z + k];
+        if ((e >> ADJ_KIND_SHIFT) != FK_TET) continue;
+        const auto t = d.tets[e & ADJ_INDEX_MASK].ids;
+        visit(t.x); visit(t.y); visit(t.z); visit(t.w);
+    }
+    const float inv = ringN > 0.0f ? 1.0f / ringN : 0.0f;
     float* f = d.learnFeat + (size_t)i * mlp::DIN;
+    for (int k = 16; k < 25; k++) f[k] = 0.0f;          // reserved
+    f[25] = ringN * 0.1f;
+    f[26] = ringContacts * inv * 0.25f;
+    f[27] = ringContacts > 0.0f ? fminf(fmaxf(ringGap / s, -10.0f), 10.0f) : 10.0f;
+    f[28] = 0.0f; f[29] = 0.0f; f[30] = 0.0f; f[31] = 0.0f;
     f[0] = fi.x; f[1] = fi.y; f[2] = fi.z;
     f[3] = fp.x; f[4] = fp.y; f[5] = fp.z;
     f[6] = fv.x; f[7] = fv.y; f[8] = fv.z;
@@ -499,13 +563,32 @@ __global__ void k_learn_select(const Params P, const DevPtrs d, uint32_t n) {
     d.posLin[v] = mk4(xyz(xp) + mk3(y[0], y[1], y[2]) * s, xp.w);
 }
 
-// after both trial sweeps: keep the predicted branch's swept pose when its
-// residual is no worse, else the plain branch's (saved in learnSwept*)
-__global__ void k_learn_keep(const Params P, const DevPtrs d, uint32_t nb) {
+// Pose buffers of the predicted branch: the solver's pose with every
+// learned vertex moved to x_plain + s * prediction.
+__global__ void k_learn_branch(const Params P, const DevPtrs d, uint32_t nb) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= nb) return;
+    const float4 x = d.posLin[b];
+    const uint32_t slot = d.learnSlot[b];
+    if (slot != 0xFFFFFFFFu) {
+        const float* y = d.learnPred + (size_t)slot * mlp::USED_OUT;
+        d.learnSweptLin[b] = mk4(xyz(x) + mk3(y[0], y[1], y[2]) * step_scale(P), x.w);
+    } else {
+        d.learnSweptLin[b] = x;
+    }
+    d.learnSweptAng[b] = d.posAng[b];
+}
+
+// After both trial sweeps: adopt the predicted branch's swept pose when its
+// residual is no worse; otherwise the plain branch's pose stays.
+__global__ void k_learn_adopt(const Params P, const DevPtrs d, uint32_t nb) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     const bool accept = d.learnResid[1] <= d.learnResid[0];
     if (b == 0 && accept) atomicAdd(d.learnAccepted, 1u);
-    if (b >= nb || accept) return;
+    // the kept trial sweep is the first pass: its OGC bound-exceeder count
+    // moves to the first pass's slot
+    if (b == 0 && P.ogc) d.counters->ogcSlots[0] = d.counters->ogcSlots[accept ? 3 : 2];
+    if (b >= nb || !accept) return;
     d.posLin[b] = d.learnSweptLin[b];
     d.posAng[b] = d.learnSweptAng[b];
 }
@@ -536,8 +619,11 @@ void launch_learn_apply(const Params& P, const DevPtrs& d, const Sizes& z, cudaS
 void launch_learn_select(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     k_learn_select<<<(z.numLearn + 128) / 128, 128, 0, st>>>(P, d, z.numLearn);
 }
-void launch_learn_keep(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
-    k_learn_keep<<<(z.numBodies + 127) / 128, 128, 0, st>>>(P, d, z.numBodies);
+void launch_learn_branch(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    k_learn_branch<<<(z.numBodies + 127) / 128, 128, 0, st>>>(P, d, z.numBodies);
+}
+void launch_learn_adopt(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    k_learn_adopt<<<(z.numBodies + 127) / 128, 128, 0, st>>>(P, d, z.numBodies);
 }
 void launch_learn_target(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     if (z.numLearn) k_learn_target<<<(z.numLearn + 127) / 128, 128, 0, st>>>(P, d, z.numLearn);
@@ -557,6 +643,7 @@ void launch_mlp_mirror(const float* prm, void* halfW, cudaStream_t st) {
 
 uint32_t mlp_param_count() { return mlp::NPARAM; }
 uint32_t mlp_half_count() { return mlp::NHALF; }
+uint32_t mlp_norm_count() { return mlp::NNORM; }
 
 }  // namespace avbd
 

@@ -1,0 +1,558 @@
+// ogc.cu — isotropic-OGC element contacts: tet boundary surfaces, cloth
+// under isotropic truncation, and mixed scenes of soft bodies, rigid bodies
+// and cloth.
+//
+// Follows Shaders/25_cloth.metal: the element grid at detection-radius
+// cells (:147-267, isotropic cover), vertex-triangle tracking and emission
+// (vt_emit :347-614), edge-edge tracking and emission (ee_emit :616-855),
+// the conservative bounds and their mid-solve refresh (:857-931); the
+// bound truncation itself lives in the primal (solver.cu, 40_solver.metal
+// :1361-1382, :1677-1681) and the warm start (40_solver.metal:700-717).
+// Stage order: GPUSolver.swift:3683-3790 (detection) and :4236-4276 (refresh).
+//
+// Everything here is deterministic:
+//   * element grid buckets are sorted by element index after the scatter;
+//   * every tracker reads the tracked sets of the previous frame (its own and
+//     its neighbours') and writes this frame's into the other buffer;
+//   * bounds are minima of non-negative squared distances (order-free
+//     atomics on float bits);
+//   * contact records are counted per query owner, scanned and written in
+//     owner order: rigid-triangle records, then V-T by particle, then E-E by
+//     edge.
+#include "elements.cuh"
+
+namespace avbd {
+
+namespace {
+
+constexpr uint32_t NONE = 0xFFFFFFFFu;
+
+// The four closest elements seen, ascending by squared distance; an equal
+// distance goes after the ones already held.
+struct Best4 {
+    uint32_t id[4];
+    float d2[4];
+};
+
+__device__ __forceinline__ void best4_init(Best4& b) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) { b.id[i] = NONE; b.d2[i] = FLT_BIG_; }
+}
+__device__ __forceinline__ bool best4_has(const Best4& b, uint32_t t) {
+    return b.id[0] == t || b.id[1] == t || b.id[2] == t || b.id[3] == t;
+}
+__device__ __forceinline__ void best4_insert(Best4& b, uint32_t t, float d2) {
+    if (d2 >= b.d2[3]) return;
+    int i = 3;
+    for (; i > 0 && b.d2[i - 1] > d2; i--) { b.id[i] = b.id[i - 1]; b.d2[i] = b.d2[i - 1]; }
+    b.id[i] = t;
+    b.d2[i] = d2;
+}
+__device__ __forceinline__ uint32_t u4_at(uint4 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w)); }
+
+__device__ __forceinline__ void bound_min(const DevPtrs& d, uint32_t b, uint32_t bits) { atomicMin(&d.ogcBounds[b], bits); }
+
+// ---------------------------------------------------------------------------
+// Element grid with the isotropic cover: every triangle and authored contact
+// edge, its box padded by its largest skin radius plus the element margin,
+// in each distinct bucket of at most 3x3x3 cells.  Triangles fill the first
+// half of the buckets, edges the second.
+// ---------------------------------------------------------------------------
+__device__ bool iso_bounds(const Params& P, const DevPtrs& d, uint32_t gid, float3& lo, float3& hi) {
+    if (gid < P.numTris) {
+        const uint4 t = d.tris[gid];
+        const float3 a = xyz(d.posLin[t.x]), b = xyz(d.posLin[t.y]), c = xyz(d.posLin[t.z]);
+        const float pad = mx(fabsf(d.shape[t.x].w), mx(fabsf(d.shape[t.y].w), fabsf(d.shape[t.z].w))) + P.elemMargin;
+        lo = vmin(vmin(a, b), c) - s3(pad);
+        hi = vmax(vmax(a, b), c) + s3(pad);
+    } else {
+        const uint2 e = d.edges[gid - P.numTris];
+        const float3 a = xyz(d.posLin[e.x]), b = xyz(d.posLin[e.y]);
+        const float pad = mx(fabsf(d.shape[e.x].w), fabsf(d.shape[e.y].w)) + P.elemMargin;
+        lo = vmin(a, b) - s3(pad);
+        hi = vmax(a, b) + s3(pad);
+    }
+    // a non-finite element has no cell (the reference leaves the cast of a
+    // non-finite coordinate undefined); it is left out of the grid
+    return finite3(lo) && finite3(hi);
+}
+
+template <bool SCATTER>
+__global__ void k_ogc_bin(const Params P, const DevPtrs d, uint32_t total) {
+    for (uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x; gid < total; gid += gridDim.x * blockDim.x) {
+        float3 lo, hi;
+        if (!iso_bounds(P, d, gid, lo, hi)) continue;
+        const I3 c0 = cell_of(lo, P.elemCellSize);
+        const I3 c1 = imin3(cell_of(hi, P.elemCellSize), iadd(c0, 2));
+        const bool tri = gid < P.numTris;
+        const uint32_t entry = tri ? gid : gid - P.numTris;
+        const uint32_t half = tri ? 0u : P.elemHashSize;
+        uint32_t seen[27];
+        uint32_t ns = 0;
+        for (int z = c0.z; z <= c1.z; z++)
+            for (int y = c0.y; y <= c1.y; y++)
+                for (int x = c0.x; x <= c1.x; x++) {
+                    const uint32_t h = elem_hash(I3{x, y, z}, P.elemHashSize);
+                    bool dup = false;
+                    for (uint32_t i = 0; i < ns; i++) dup = dup || seen[i] == h;
+                    if (dup) continue;
+                    seen[ns++] = h;
+                    if (SCATTER) d.elemCellsTmp[atomicAdd(&d.elemCursor[half + h], 1u)] = entry;
+                    else atomicAdd(&d.elemCellCount[half + h], 1u);
+                }
+    }
+}
+
+// One warp per bucket places every entry at its rank (entries of a bucket
+// are distinct element indices).
+__global__ void k_ogc_sort_cells(const DevPtrs d, uint32_t buckets) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < buckets; h += warps) {
+        const uint32_t n = d.elemCellCount[h];
+        if (n == 0) continue;
+        const uint32_t s = d.elemCellStart[h];
+        const uint32_t* src = d.elemCellsTmp + s;
+        for (uint32_t i = lane; i < n; i += 32) {
+            const uint32_t v = src[i];
+            uint32_t rank = 0;
+            for (uint32_t j = 0; j < n; j++) rank += src[j] < v ? 1u : 0u;
+            d.elemCells[s + rank] = v;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Vertex-triangle tracking (vt_emit, 25_cloth.metal:347-522)
+// ---------------------------------------------------------------------------
+struct VtQuery {
+    uint32_t v;
+    float3 pv;
+    uint32_t ns, ne, n2s, n2e, gv;
+    bool solidV;
+    float boundsCap2;
+};
+
+// One candidate triangle: topological exclusion (own and 1-ring triangles,
+// triangles of the same closed solid), the tracked-set update and the
+// conservative-bound contributions (2-ring excluded).
+__device__ void vt_consider(const Params& P, const DevPtrs& d, const VtQuery& q, Best4& best, float& ownB2,
+                            uint32_t t) {
+    if (t >= P.numTris || best4_has(best, t)) return;
+    const uint4 tid = d.tris[t];
+    if (tid.x == q.v || tid.y == q.v || tid.z == q.v) return;
+    if (q.solidV && d.clothGroup[tid.x] == q.gv && d.clothGroup[tid.y] == q.gv && d.clothGroup[tid.z] == q.gv &&
+        d.clothVert[tid.x] == 0u && d.clothVert[tid.y] == 0u && d.clothVert[tid.z] == 0u)
+        return;
+    float3 bary;
+    const float3 cp = closest_pt_triangle(q.pv, xyz(d.posLin[tid.x]), xyz(d.posLin[tid.y]), xyz(d.posLin[tid.z]), bary);
+    const float3 dd = q.pv - cp;
+    const float d2 = dot(dd, dd);
+    if (d2 < best.d2[3] && !nbr_contains(d.nbrList, q.ns, q.ne, tid.x) && !nbr_contains(d.nbrList, q.ns, q.ne, tid.y) &&
+        !nbr_contains(d.nbrList, q.ns, q.ne, tid.z))
+        best4_insert(best, t, d2);
+    if (d2 < q.boundsCap2 && !nbr_contains(d.nbr2List, q.n2s, q.n2e, tid.x) &&
+        !nbr_contains(d.nbr2List, q.n2s, q.n2e, tid.y) && !nbr_contains(d.nbr2List, q.n2s, q.n2e, tid.z)) {
+        const uint32_t db = __float_as_uint(d2);
+        ownB2 = fminf(ownB2, d2);
+        bound_min(d, tid.x, db);
+        bound_min(d, tid.y, db);
+        bound_min(d, tid.z, db);
+    }
+}
+
+// The contact of vertex v against tracked triangle t (emission loop of
+// vt_emit, 25_cloth.metal:531-613).  Returns whether a record is made; with
+// EMIT it is written to `slot`.
+template <bool EMIT>
+__device__ bool vt_contact(const Params& P, const DevPtrs& d, uint32_t v, uint32_t t, uint32_t slot) {
+    const float4 plv = d.posLin[v];
+    const float3 pv = xyz(plv);
+    const float massV = plv.w;
+    const float rv = fabsf(d.shape[v].w);
+    const float3 velV = xyz(d.velLin[v]);
+    const uint4 tid = d.tris[t];
+    const float3 a = xyz(d.posLin[tid.x]), b = xyz(d.posLin[tid.y]), c = xyz(d.posLin[tid.z]);
+    float3 bary;
+    const float3 q = closest_pt_triangle(pv, a, b, c, bary);
+    const float3 dv = pv - q;
+    const float dist2 = dot(dv, dv);
+    const float rt = mx(fabsf(d.shape[tid.x].w), mx(fabsf(d.shape[tid.y].w), fabsf(d.shape[tid.z].w)));
+    const float hSum = rv + rt;
+    const float3 velT = (xyz(d.velLin[tid.x]) + xyz(d.velLin[tid.y]) + xyz(d.velLin[tid.z])) / 3.0f;
+    const float inflate = mn(len3(velV - velT) * P.dt, 0.3f * P.surfaceCellSize);
+    const float detect = hSum + P.elemMargin + inflate;
+    if (dist2 > detect * detect) return false;
+    const float dist = sqrtf(dist2);
+    float3 triN = cross(b - a, c - a);
+    const float tnLen = len3(triN);
+    if (tnLen < 1e-12f) return false;
+    triN = triN / tnLen;
+    float minMass = massV > 0.0f ? massV : FLT_BIG_;
+    const uint32_t others[3] = {tid.x, tid.y, tid.z};
+    for (int k = 0; k < 3; k++) {
+        if (others[k] == WORLD_BODY) continue;
+        const float m = d.posLin[others[k]].w;
+        if (m > 0.0f) minMass = mn(minMass, m);
+    }
+    if (minMass == FLT_BIG_) return false;
+    if (EMIT) {
+        const uint32_t keyB = t, keyA = (SC_VT << 28) | v;
+        const float side = dot(dv, triN) >= 0.0f ? 1.0f : -1.0f;
+        const bool deepInterior = bary.x > 0.02f && bary.y > 0.02f && bary.z > 0.02f;
+        const float sMem = deepInterior ? soft_prev_side(P, d, keyA, keyB, side) : side;
+        float3 n;
+        float g;
+        if (dist > 1e-7f && side == sMem) { n = dv / dist; g = dist; }
+        else { n = triN * sMem; g = -dist; }
+        const float fricT = d.props[tid.x].w * bary.x + d.props[tid.y].w * bary.y + d.props[tid.z].w * bary.z;
+        const float friction = sqrtf(mx(d.props[v].w * fricT, 0.0f));
+        soft_write(P, d, slot, make_uint4(v, tid.x, tid.y, tid.z), make_float4(1.0f, -bary.x, -bary.y, -bary.z), n,
+                   friction, s3(0), g - hSum + P.elemMargin, hSum - P.elemMargin, soft_lambda_cap(P, minMass), minMass,
+                   SC_VT, false, false, sMem < 0.0f, keyA, keyB);
+    }
+    return true;
+}
+
+__device__ uint32_t vt_track(const Params& P, const DevPtrs& d, uint32_t gid, uint32_t frame) {
+    VtQuery q;
+    q.v = d.particleIdx[gid];
+    q.pv = xyz(d.posLin[q.v]);
+    const float3 velV = xyz(d.velLin[q.v]);
+    q.ns = d.nbrStart[q.v];
+    q.ne = q.ns + d.nbrCount[q.v];
+    q.gv = d.clothGroup[q.v];
+    q.solidV = q.gv != 0u && d.clothVert[q.v] == 0u;
+    q.n2s = d.nbr2Start[q.v];
+    q.n2e = q.n2s + d.nbr2Count[q.v];
+    q.boundsCap2 = P.elemCellSize * P.elemCellSize;
+    float ownB2 = FLT_BIG_;
+    Best4 best;
+    best4_init(best);
+    const uint4 tracked = d.vtTrackPrev[q.v];
+    for (int i = 0; i < 4; i++) vt_consider(P, d, q, best, ownB2, u4_at(tracked, i));
+    if (tracked.x < P.numTris) {
+        const uint4 adj = d.triAdj[tracked.x];
+        for (int i = 0; i < 3; i++) vt_consider(P, d, q, best, ownB2, u4_at(adj, i));
+    }
+    for (uint32_t k = q.ns; k < q.ne && k < q.ns + 8; k++) vt_consider(P, d, q, best, ownB2, d.vtTrackPrev[d.nbrList[k]].x);
+    // staggered reseed, faster where the motion relative to the tracked
+    // surface is large
+    float3 relV = velV;
+    if (best.id[0] < P.numTris) {
+        const uint4 bt = d.tris[best.id[0]];
+        relV = relV - (xyz(d.velLin[bt.x]) + xyz(d.velLin[bt.y]) + xyz(d.velLin[bt.z])) / 3.0f;
+    }
+    const float vThresh = 0.25f * P.elemCellSize / mx(P.dt, 1e-6f);
+    const uint32_t period = dot(relV, relV) > vThresh * vThresh ? 1u : 7u;
+    const bool missing = best.id[0] == NONE;
+    const bool reseed = ((q.v + frame) & period) == 0u || (missing && !q.solidV) ||
+                        (missing && q.solidV && ((q.v + frame) & 3u) == 0u);
+    if (reseed) {
+        const I3 cc = cell_of(q.pv, P.elemCellSize);
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const uint32_t h = elem_hash(I3{cc.x + dx, cc.y + dy, cc.z + dz}, P.elemHashSize);
+                    const uint32_t s0 = d.elemCellStart[h], e0 = s0 + d.elemCellCount[h];
+                    for (uint32_t k = s0; k < e0; k++) vt_consider(P, d, q, best, ownB2, d.elemCells[k]);
+                }
+    }
+    d.vtTrack[q.v] = make_uint4(best.id[0], best.id[1], best.id[2], best.id[3]);
+    if (ownB2 < FLT_BIG_) bound_min(d, q.v, __float_as_uint(ownB2));
+    uint32_t count = 0;
+    for (int bi = 0; bi < 4; bi++) {
+        if (best.id[bi] >= P.numTris) break;
+        if (vt_contact<false>(P, d, q.v, best.id[bi], 0u)) count++;
+    }
+    return count;
+}
+
+// ---------------------------------------------------------------------------
+// Edge-edge tracking (ee_emit, 25_cloth.metal:654-784), authored contact
+// edges only
+// ---------------------------------------------------------------------------
+struct EeQuery {
+    uint32_t gid;
+    uint2 eA;
+    float3 a0, a1;
+    uint32_t nsx, nex, nsy, ney, n2sx, n2ex, gA;
+    bool solidA;
+    float boundsCap2;
+};
+
+__device__ void ee_consider(const Params& P, const DevPtrs& d, const EeQuery& q, Best4& best, float& ownB2,
+                            uint32_t e) {
+    if (e >= P.numEdges || e == q.gid || best4_has(best, e)) return;
+    const uint2 eB = d.edges[e];
+    if (eB.x == q.eA.x || eB.x == q.eA.y || eB.y == q.eA.x || eB.y == q.eA.y) return;
+    if (q.solidA && d.clothGroup[eB.x] == q.gA && d.clothGroup[eB.y] == q.gA && d.clothVert[eB.x] == 0u &&
+        d.clothVert[eB.y] == 0u)
+        return;
+    float s, t;
+    const float3 b0 = xyz(d.posLin[eB.x]), b1 = xyz(d.posLin[eB.y]);
+    closest_seg_seg(q.a0, q.a1, b0, b1, s, t);
+    const float3 cA = q.a0 + (q.a1 - q.a0) * s;
+    const float3 cB = b0 + (b1 - b0) * t;
+    const float3 dd = cA - cB;
+    const float d2 = dot(dd, dd);
+    if (d2 < best.d2[3] && !nbr_contains(d.nbrList, q.nsx, q.nex, eB.x) &&
+        !nbr_contains(d.nbrList, q.nsx, q.nex, eB.y) && !nbr_contains(d.nbrList, q.nsy, q.ney, eB.x) &&
+        !nbr_contains(d.nbrList, q.nsy, q.ney, eB.y))
+        best4_insert(best, e, d2);
+    if (d2 < q.boundsCap2 && !nbr_contains(d.nbr2List, q.n2sx, q.n2ex, eB.x) &&
+        !nbr_contains(d.nbr2List, q.n2sx, q.n2ex, eB.y)) {
+        const uint32_t db = __float_as_uint(d2);
+        ownB2 = fminf(ownB2, d2);
+        bound_min(d, eB.x, db);
+        bound_min(d, eB.y, db);
+    }
+}
+
+// Emission loop of ee_emit (25_cloth.metal:792-854): interior closest points,
+// each pair once (owned by the smaller edge index).
+template <bool EMIT>
+__device__ bool ee_contact(const Params& P, const DevPtrs& d, uint32_t gid, uint32_t eBi, uint32_t slot) {
+    const uint2 eA = d.edges[gid], eB = d.edges[eBi];
+    const float3 a0 = xyz(d.posLin[eA.x]), a1 = xyz(d.posLin[eA.y]);
+    const float3 b0 = xyz(d.posLin[eB.x]), b1 = xyz(d.posLin[eB.y]);
+    float s, t;
+    closest_seg_seg(a0, a1, b0, b1, s, t);
+    if (s < EE_INTERIOR_EPS || s > 1.0f - EE_INTERIOR_EPS || t < EE_INTERIOR_EPS || t > 1.0f - EE_INTERIOR_EPS)
+        return false;
+    const float3 cA = a0 + (a1 - a0) * s;
+    const float3 cB = b0 + (b1 - b0) * t;
+    const float3 dv = cA - cB;
+    const float dist = len3(dv);
+    const float rA = mx(fabsf(d.shape[eA.x].w), fabsf(d.shape[eA.y].w));
+    const float rB = mx(fabsf(d.shape[eB.x].w), fabsf(d.shape[eB.y].w));
+    const float hSum = rA + rB;
+    const float3 velA = (xyz(d.velLin[eA.x]) + xyz(d.velLin[eA.y])) * 0.5f;
+    const float3 velB = (xyz(d.velLin[eB.x]) + xyz(d.velLin[eB.y])) * 0.5f;
+    const float inflate = mn(len3(velA - velB) * P.dt, 0.3f * P.surfaceCellSize);
+    if (dist - hSum > P.elemMargin + inflate) return false;
+    if (dist < 1e-7f) return false;
+    float minMass = FLT_BIG_;
+    const uint32_t ids[4] = {eA.x, eA.y, eB.x, eB.y};
+    for (int j = 0; j < 4; j++) {
+        const float m = d.posLin[ids[j]].w;
+        if (m > 0.0f) minMass = mn(minMass, m);
+    }
+    if (minMass == FLT_BIG_) return false;
+    if (EMIT) {
+        const float3 nGeo = dv / dist;
+        const uint32_t keyA = (SC_EE << 28) | gid, keyB = eBi;
+        float3 n = nGeo;
+        float g = dist;
+        const int prev = soft_map_find(P, d, keyA, keyB);
+        if (prev >= 0 && dot(nGeo, xyz(d.prevSoft[prev].normal)) < 0.0f) {
+            n = -nGeo;
+            g = -dist;
+        }
+        const float fric = sqrtf(mx((d.props[eA.x].w + d.props[eA.y].w) * 0.5f * (d.props[eB.x].w + d.props[eB.y].w) * 0.5f,
+                                    0.0f));
+        soft_write(P, d, slot, make_uint4(eA.x, eA.y, eB.x, eB.y), make_float4(1.0f - s, s, -(1.0f - t), -t), n, fric,
+                   s3(0), g - hSum + P.elemMargin, hSum - P.elemMargin, soft_lambda_cap(P, minMass), minMass, SC_EE,
+                   false, false, false, keyA, keyB);
+    }
+    return true;
+}
+
+__device__ uint32_t ee_track(const Params& P, const DevPtrs& d, uint32_t gid, uint32_t frame) {
+    EeQuery q;
+    q.gid = gid;
+    q.eA = d.edges[gid];
+    q.a0 = xyz(d.posLin[q.eA.x]);
+    q.a1 = xyz(d.posLin[q.eA.y]);
+    const float3 velA = (xyz(d.velLin[q.eA.x]) + xyz(d.velLin[q.eA.y])) * 0.5f;
+    q.nsx = d.nbrStart[q.eA.x];
+    q.nex = q.nsx + d.nbrCount[q.eA.x];
+    q.nsy = d.nbrStart[q.eA.y];
+    q.ney = q.nsy + d.nbrCount[q.eA.y];
+    q.gA = d.clothGroup[q.eA.x];
+    q.solidA = q.gA != 0u && d.clothGroup[q.eA.y] == q.gA && d.clothVert[q.eA.x] == 0u && d.clothVert[q.eA.y] == 0u;
+    q.n2sx = d.nbr2Start[q.eA.x];
+    q.n2ex = q.n2sx + d.nbr2Count[q.eA.x];
+    q.boundsCap2 = P.elemCellSize * P.elemCellSize;
+    float ownB2 = FLT_BIG_;
+    Best4 best;
+    best4_init(best);
+    const uint4 tracked = d.eeTrackPrev[gid];
+    for (int i = 0; i < 4; i++) ee_consider(P, d, q, best, ownB2, u4_at(tracked, i));
+    for (int side = 0; side < 2; side++) {
+        const uint32_t vv = side == 0 ? q.eA.x : q.eA.y;
+        const uint32_t es = d.vertEdgeStart[vv], ec = min(d.vertEdgeCount[vv], 6u);
+        for (uint32_t k = es; k < es + ec; k++) ee_consider(P, d, q, best, ownB2, d.eeTrackPrev[d.vertEdgeList[k]].x);
+    }
+    float3 relV = velA;
+    if (best.id[0] < P.numEdges) {
+        const uint2 bt = d.edges[best.id[0]];
+        relV = relV - (xyz(d.velLin[bt.x]) + xyz(d.velLin[bt.y])) * 0.5f;
+    }
+    const float vThresh = 0.25f * P.elemCellSize / mx(P.dt, 1e-6f);
+    const uint32_t period = dot(relV, relV) > vThresh * vThresh ? 1u : 7u;
+    const bool missing = best.id[0] == NONE;
+    const bool reseed = ((gid + frame) & period) == 0u || (missing && !q.solidA) ||
+                        (missing && q.solidA && ((gid + frame) & 3u) == 0u);
+    if (reseed) {
+        const I3 cc = cell_of((q.a0 + q.a1) * 0.5f, P.elemCellSize);
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const uint32_t h = P.elemHashSize + elem_hash(I3{cc.x + dx, cc.y + dy, cc.z + dz}, P.elemHashSize);
+                    const uint32_t s0 = d.elemCellStart[h], e0 = s0 + d.elemCellCount[h];
+                    for (uint32_t k = s0; k < e0; k++) ee_consider(P, d, q, best, ownB2, d.elemCells[k]);
+                }
+    }
+    d.eeTrack[gid] = make_uint4(best.id[0], best.id[1], best.id[2], best.id[3]);
+    if (ownB2 < FLT_BIG_) {
+        bound_min(d, q.eA.x, __float_as_uint(ownB2));
+        bound_min(d, q.eA.y, __float_as_uint(ownB2));
+    }
+    uint32_t count = 0;
+    for (int bi = 0; bi < 4; bi++) {
+        const uint32_t e = best.id[bi];
+        if (e >= P.numEdges) break;
+        if (e <= gid) continue;
+        if (ee_contact<false>(P, d, gid, e, 0u)) count++;
+    }
+    return count;
+}
+
+// Owners [0, numParticles) are V-T queries, the rest E-E queries.
+__global__ void k_ogc_track(const Params P, const DevPtrs d, uint32_t owners) {
+    const uint32_t frame = d.frameCounter[0];
+    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < owners; o += gridDim.x * blockDim.x)
+        d.datEmit[o] = o < P.numParticles ? vt_track(P, d, o, frame) : ee_track(P, d, o - P.numParticles, frame);
+}
+
+__global__ void k_ogc_emit(const Params P, const DevPtrs d, uint32_t owners) {
+    const uint32_t head = d.counters->numSoftRT;
+    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < owners; o += gridDim.x * blockDim.x) {
+        uint32_t slot = head + d.datEmitStart[o];
+        if (o < P.numParticles) {
+            const uint32_t v = d.particleIdx[o];
+            const uint4 best = d.vtTrack[v];
+            for (int bi = 0; bi < 4; bi++) {
+                const uint32_t t = u4_at(best, bi);
+                if (t >= P.numTris) break;
+                if (vt_contact<false>(P, d, v, t, 0u)) { vt_contact<true>(P, d, v, t, slot); slot++; }
+            }
+        } else {
+            const uint32_t gid = o - P.numParticles;
+            const uint4 best = d.eeTrack[gid];
+            for (int bi = 0; bi < 4; bi++) {
+                const uint32_t e = u4_at(best, bi);
+                if (e >= P.numEdges) break;
+                if (e <= gid) continue;
+                if (ee_contact<false>(P, d, gid, e, 0u)) { ee_contact<true>(P, d, gid, e, slot); slot++; }
+            }
+        }
+    }
+}
+
+__global__ void k_ogc_totals(const Params P, const DevPtrs d, uint32_t owners) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t vt = P.numParticles < owners ? d.datEmitStart[P.numParticles]
+                                                : (owners ? d.datEmitStart[owners - 1] + d.datEmit[owners - 1] : 0u);
+    const uint32_t all = owners ? d.datEmitStart[owners - 1] + d.datEmit[owners - 1] : 0u;
+    d.counters->numSoftVT = vt;
+    d.counters->numSoftEE = all - vt;
+}
+
+// ---------------------------------------------------------------------------
+// Mid-solve bound refresh (ogc_refresh_args + ogc_bounds_refresh,
+// 25_cloth.metal:857-931): when more than 1% of the surface vertices were
+// bound-limited in the last pass, re-anchor at the live pose and recompute
+// every bound from the tracked sets.
+// ---------------------------------------------------------------------------
+__global__ void k_ogc_refresh(const Params P, const DevPtrs d, const uint32_t* readSlot, uint32_t* zeroSlot) {
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid == 0) *zeroSlot = 0u;
+    if (!(*readSlot * 100u > P.numParticles) || gid >= P.numParticles) return;
+    const uint32_t v = d.particleIdx[gid];
+    const float3 pv = xyz(d.posLin[v]);
+    const uint32_t n2s = d.nbr2Start[v], n2e = n2s + d.nbr2Count[v];
+    float dmin2 = 3.0e38f;
+    const uint4 tracked = d.vtTrack[v];
+    for (int i = 0; i < 4; i++) {
+        const uint32_t t = u4_at(tracked, i);
+        if (t >= P.numTris) break;
+        const uint4 tid = d.tris[t];
+        if (nbr_contains(d.nbr2List, n2s, n2e, tid.x) || nbr_contains(d.nbr2List, n2s, n2e, tid.y) ||
+            nbr_contains(d.nbr2List, n2s, n2e, tid.z))
+            continue;
+        float3 bary;
+        const float3 q = closest_pt_triangle(pv, xyz(d.posLin[tid.x]), xyz(d.posLin[tid.y]), xyz(d.posLin[tid.z]), bary);
+        const float3 dd = pv - q;
+        dmin2 = fminf(dmin2, dot(dd, dd));
+    }
+    const uint32_t es = d.vertEdgeStart[v], ec = min(d.vertEdgeCount[v], 6u);
+    for (uint32_t k = es; k < es + ec; k++) {
+        const uint32_t myE = d.vertEdgeList[k];
+        const uint32_t other = d.eeTrack[myE].x;
+        if (other >= P.numEdges) continue;
+        const uint2 eo = d.edges[other];
+        if (nbr_contains(d.nbr2List, n2s, n2e, eo.x) || nbr_contains(d.nbr2List, n2s, n2e, eo.y)) continue;
+        const uint2 em = d.edges[myE];
+        const float3 a0 = xyz(d.posLin[em.x]), a1 = xyz(d.posLin[em.y]);
+        const float3 b0 = xyz(d.posLin[eo.x]), b1 = xyz(d.posLin[eo.y]);
+        float s, t;
+        closest_seg_seg(a0, a1, b0, b1, s, t);
+        const float3 dd = (a0 + (a1 - a0) * s) - (b0 + (b1 - b0) * t);
+        dmin2 = fminf(dmin2, dot(dd, dd));
+    }
+    d.ogcBounds[v] = __float_as_uint(dmin2);
+    d.ogcPrev[v] = d.posLin[v];
+}
+
+// Color-Jacobi commit of one color (the primal of the color wrote posNext).
+__global__ void k_publish_color(const DevPtrs d, uint32_t color, uint32_t count) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const uint32_t v = d.colorList[d.colorStart[color] + i];
+    d.posLin[v] = mk4(xyz(d.posNext[v]), d.posLin[v].w);
+    if (d.shape[v].w >= 0.0f) d.posAng[v] = d.angNext[v];
+}
+
+uint32_t grid_for(uint32_t n, uint32_t threads, uint32_t cap = 148u * 16u) {
+    const uint32_t need = (n + threads - 1) / threads;
+    return need == 0 ? 1u : (need < cap ? need : cap);
+}
+
+}  // namespace
+
+void launch_ogc_detect(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
+    // bounds start "far" (0x7F7F7F7F ~ 3.4e38) every frame
+    cudaMemsetAsync(d.ogcBounds, 0x7F, sizeof(uint32_t) * z.numBodies, st);
+    const uint32_t total = z.numTris + P.numEdges;
+    const uint32_t buckets = 2 * z.elemHashSize;
+    cudaMemsetAsync(d.elemCellCount, 0, sizeof(uint32_t) * buckets, st);
+    k_ogc_bin<false><<<grid_for(total, 128), 128, 0, st>>>(P, d, total);
+    launch_exclusive_scan_large(d.elemCellCount, d.elemCellStart, buckets, d.bigScanScratch, st);
+    cudaMemcpyAsync(d.elemCursor, d.elemCellStart, sizeof(uint32_t) * buckets, cudaMemcpyDeviceToDevice, st);
+    k_ogc_bin<true><<<grid_for(total, 128), 128, 0, st>>>(P, d, total);
+    k_ogc_sort_cells<<<grid_for(buckets * 32u, 128), 128, 0, st>>>(d, buckets);
+    const uint32_t owners = z.numParticles + P.numEdges;
+    if (owners) k_ogc_track<<<grid_for(owners, 128), 128, 0, st>>>(P, d, owners);
+    launch_rt_emit(P, d, z, st);
+    if (owners) {
+        launch_exclusive_scan_large(d.datEmit, d.datEmitStart, owners, d.bigScanScratch, st);
+        k_ogc_emit<<<grid_for(owners, 128), 128, 0, st>>>(P, d, owners);
+        k_ogc_totals<<<1, 32, 0, st>>>(P, d, owners);
+    }
+    launch_soft_map(P, d, z, owners, st);
+}
+
+void launch_publish_color(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count, cudaStream_t st) {
+    (void)P;
+    if (count == 0) return;
+    k_publish_color<<<(count + 127) / 128, 128, 0, st>>>(d, color, count);
+}
+
+void launch_ogc_refresh(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t* readSlot, uint32_t* zeroSlot,
+                        cudaStream_t st) {
+    k_ogc_refresh<<<(z.numParticles + 127) / 128, 128, 0, st>>>(P, d, readSlot, zeroSlot);
+}
+
+}  // namespace avbd

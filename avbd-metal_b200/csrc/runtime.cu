@@ -99,7 +99,7 @@ struct avbd_solver {
     // per-color launches are needed by the learned warm start's trial sweeps
     // and by the per-iteration residual trace
     void update_small_solve() {
-        smallSolve = z.numDynamicBodies <= 512 && !P.cloth && learnMode == AVBD_WARM_START_PLAIN && !learnCapture &&
+        smallSolve = z.numDynamicBodies <= 512 && !P.cloth && !P.ogc && learnMode == AVBD_WARM_START_PLAIN && !learnCapture &&
                      !residualTrace;
         if (smallSolve) tuneStage = -1;
     }
@@ -193,7 +193,13 @@ struct avbd_solver {
         if (parity) {
             std::swap(f.manifolds, f.prevManifolds);
             std::swap(f.soft, f.prevSoft);
+            std::swap(f.vtTrack, f.vtTrackPrev);
+            std::swap(f.eeTrack, f.eeTrackPrev);
         }
+        uint32_t* ogcSlots = d.counters ? reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(d.counters) +
+                                                                      offsetof(Counters, ogcSlots))
+                                        : nullptr;
+        f.ogcExceed = ogcSlots;
         usedEvents = 0;
         uint32_t primalLaunch = 0;
         auto mark = [&](int stage) {
@@ -212,6 +218,9 @@ struct avbd_solver {
         if (P.cloth) {
             mark(AVBD_STAGE_ELEMENT_CONTACTS);
             launch_cloth_detect(P, f, z, st);
+        } else if (P.ogc) {
+            mark(AVBD_STAGE_ELEMENT_CONTACTS);
+            launch_ogc_detect(P, f, z, st);
         }
         mark(AVBD_STAGE_WARMSTART);
         launch_warmstart(P, f, z, st);
@@ -226,49 +235,53 @@ struct avbd_solver {
             launch_dynamic_coloring(P, f, z, st);
         }
         const uint32_t colorBound = z.dynamicColoring ? colorLaunchBound : H.staticUsedColors;
-        // One primal sweep over every color (trial sweeps of the learned
-        // warm start; the iteration loop below inlines the same sequence).
-        auto sweep = [&]() {
+        // One primal sweep over every color of pose buffers `g` (trial sweeps of
+        // the learned warm start; the iteration loop inlines the same sequence).
+        auto sweep = [&](const DevPtrs& g) {
             for (uint32_t c = 0; c < colorBound; c++) {
                 const uint32_t count = z.dynamicColoring ? 0xFFFFFFFFu : H.colorCounts[c];
                 if (count == 0) continue;
-                launch_primal_color(P, f, z, c, count, H.colorLanes[c], st);
+                launch_primal_color(P, g, z, c, count, H.colorLanes[c], st);
+                if (P.ogc) launch_publish_color(P, g, c, count, st);
             }
-            if (z.dynamicColoring) launch_primal_tail(P, f, z, colorLaunchBound, st);
+            if (z.dynamicColoring) launch_primal_tail(P, g, z, colorLaunchBound, st);
         };
         const bool tuningFrame = primalEvents != nullptr;
         const bool learned = !tuningFrame && learnMode == AVBD_WARM_START_LEARNED && modelSet && z.numLearn;
         const bool capture = !tuningFrame && learnCapture && z.numLearn;
         const bool trace = !tuningFrame && residualTrace;
-        const size_t poseBytes = sizeof(float4) * z.numBodies;
-        if (learned || capture || trace) {
-            mark(AVBD_STAGE_LEARNED);
-            if (learned || capture) launch_learn_features(P, f, z, st);
-            cudaMemcpyAsync(f.learnSaveLin, f.posLin, poseBytes, cudaMemcpyDeviceToDevice, st);
-            cudaMemcpyAsync(f.learnSaveAng, f.posAng, poseBytes, cudaMemcpyDeviceToDevice, st);
-            if (trace) launch_residual(P, f, z, f.learnResidBodies, f.learnTrace + 0, st);
-        }
         // With one trial sweep the winner's swept pose is kept as the primal
         // half of the first iteration (the dual follows as usual); with more
         // trial sweeps both branches are undone and the solve restarts from
         // the chosen warm start.
         const bool reuseTrial = learned && learnTrials == 1 && P.iterations > 0;
-        if (learned) {
-            launch_mlp_infer(f.learnHalf, f.learnPrm, f.learnNorm, f.learnFeat, z.numLearn, f.learnPred, st);
-            for (uint32_t t = 0; t < learnTrials; t++) sweep();
-            launch_residual(P, f, z, f.learnResidBodies, f.learnResid + 0, st);
-            if (reuseTrial) {
-                cudaMemcpyAsync(f.learnSweptLin, f.posLin, poseBytes, cudaMemcpyDeviceToDevice, st);
-                cudaMemcpyAsync(f.learnSweptAng, f.posAng, poseBytes, cudaMemcpyDeviceToDevice, st);
+        const size_t poseBytes = sizeof(float4) * z.numBodies;
+        if (learned || capture || trace) {
+            mark(AVBD_STAGE_LEARNED);
+            if (learned || capture) launch_learn_features(P, f, z, st);
+            if (capture || (learned && !reuseTrial)) {
+                cudaMemcpyAsync(f.learnSaveLin, f.posLin, poseBytes, cudaMemcpyDeviceToDevice, st);
+                cudaMemcpyAsync(f.learnSaveAng, f.posAng, poseBytes, cudaMemcpyDeviceToDevice, st);
             }
-            cudaMemcpyAsync(f.posLin, f.learnSaveLin, poseBytes, cudaMemcpyDeviceToDevice, st);
-            cudaMemcpyAsync(f.posAng, f.learnSaveAng, poseBytes, cudaMemcpyDeviceToDevice, st);
-            launch_learn_apply(P, f, z, st);
-            if (trace) launch_residual(P, f, z, f.learnResidBodies, f.learnTrace + 1, st);
-            for (uint32_t t = 0; t < learnTrials; t++) sweep();
-            launch_residual(P, f, z, f.learnResidBodies, f.learnResid + 1, st);
+            if (trace) launch_residual(P, f, z, f.learnResidBodies, f.learnTrace + 0, st);
+        }
+        if (learned) {
+            // The predicted branch runs in its own pose buffers (fb); the
+            // plain branch sweeps the solver's pose in place.
+            DevPtrs fb = f, fp = f;
+            fb.posLin = f.learnSweptLin;
+            fb.posAng = f.learnSweptAng;
+            // the trial sweeps count OGC bound exceeders in slots 2 (plain) and 3 (predicted)
+            if (ogcSlots) { fp.ogcExceed = ogcSlots + 2; fb.ogcExceed = ogcSlots + 3; }
+            launch_mlp_infer(f.learnHalf, f.learnPrm, f.learnNorm, f.learnFeat, z.numLearn, f.learnPred, st);
+            launch_learn_branch(P, f, z, st);
+            if (trace) launch_residual(P, fb, z, f.learnResidBodies, f.learnTrace + 1, st);
+            for (uint32_t t = 0; t < learnTrials; t++) sweep(fp);
+            launch_residual(P, f, z, f.learnResidBodies, f.learnResid + 0, st);
+            for (uint32_t t = 0; t < learnTrials; t++) sweep(fb);
+            launch_residual(P, fb, z, f.learnResidBodies, f.learnResid + 1, st);
             if (reuseTrial) {
-                launch_learn_keep(P, f, z, st);
+                launch_learn_adopt(P, f, z, st);
             } else {
                 cudaMemcpyAsync(f.posLin, f.learnSaveLin, poseBytes, cudaMemcpyDeviceToDevice, st);
                 cudaMemcpyAsync(f.posAng, f.learnSaveAng, poseBytes, cudaMemcpyDeviceToDevice, st);
@@ -282,22 +295,31 @@ struct avbd_solver {
             launch_solve_small(P, f, z, z.dynamicColoring ? (uint32_t)MAX_COLORS : H.staticUsedColors, st);
         } else {
             for (uint32_t it = 0; it < P.iterations; it++) {
+                // OGC bound exceeders of this pass alternate between slots 0 and 1
+                DevPtrs g = f;
+                if (ogcSlots) g.ogcExceed = ogcSlots + (it & 1u);
                 for (uint32_t c = 0; c < colorBound && !(reuseTrial && it == 0); c++) {
                     const uint32_t count = z.dynamicColoring ? 0xFFFFFFFFu : H.colorCounts[c];
                     if (count == 0) continue;
                     mark(AVBD_STAGE_PRIMAL);
                     if (primalEvents) cudaEventRecord(primalEvents[2 * primalLaunch], st);
-                    launch_primal_color(P, f, z, c, count, lanes ? lanes[c] : H.colorLanes[c], st);
+                    launch_primal_color(P, g, z, c, count, lanes ? lanes[c] : H.colorLanes[c], st);
                     if (primalEvents) cudaEventRecord(primalEvents[2 * primalLaunch + 1], st);
                     primalLaunch++;
                     if (P.cloth) {
                         mark(AVBD_STAGE_TRUNCATION);
                         launch_dat_color(P, f, z, c, count, st);
+                    } else if (P.ogc) {
+                        launch_publish_color(P, f, c, count, st);
                     }
                 }
-                if (z.dynamicColoring && !(reuseTrial && it == 0)) launch_primal_tail(P, f, z, colorLaunchBound, st);
+                if (z.dynamicColoring && !(reuseTrial && it == 0)) launch_primal_tail(P, g, z, colorLaunchBound, st);
                 mark(AVBD_STAGE_DUAL);
                 launch_dual(P, f, z, st);
+                if (P.ogc && it + 1 < P.iterations) {
+                    mark(AVBD_STAGE_TRUNCATION);
+                    launch_ogc_refresh(P, f, z, ogcSlots + (it & 1u), ogcSlots + ((it + 1u) & 1u), st);
+                }
                 if (trace && it + 2 < kTraceLength)
                     launch_residual(P, f, z, f.learnResidBodies, f.learnTrace + 2 + it, st);
             }
@@ -306,7 +328,7 @@ struct avbd_solver {
         mark(AVBD_STAGE_FINALIZE);
         if (P.cloth) launch_cloth_restore(P, f, z, st);
         launch_finalize(P, f, z, st);
-        if (P.cloth) launch_cloth_smoothing(P, f, z, st);
+        if (z.numTris) launch_cloth_smoothing(P, f, z, st);
         launch_frame_end(P, f, z, st);
         mark(-1);
     }
@@ -377,11 +399,11 @@ struct avbd_solver {
         z.particleFastPath = H.particleFastPath;
         z.numTris = H.numTris;
         z.numParticles = P.numParticles;
-        z.numEdges = H.numEdges;
+        z.numEdges = P.numEdges;
         z.numMembranes = (uint32_t)H.membranes.size();
         z.numBends = (uint32_t)H.bends.size();
         z.maxDatPairs = H.maxDatPairs;
-        z.maxSoft = H.maxSoft;
+        z.maxSoft = P.maxSoft;
         z.elemHashSize = H.elemHashSize;
         z.numLearn = P.cloth ? 0u : (uint32_t)H.learnIdx.size();
         z.colorCounts = H.dynamicColoring ? nullptr : H.colorCounts.data();
@@ -438,7 +460,7 @@ struct avbd_solver {
         ok = ok && upload(reinterpret_cast<u4*&>(d.staticSeg), H.staticSeg, "staticSeg");
         ok = ok && upload(d.preList, H.preList, "preList") && upload(d.postList, H.postList, "postList");
         ok = ok && alloc(d.dynCount, nb, "dynCount") && alloc(d.dynStart, nb, "dynStart") && alloc(d.dynCursor, nb, "dynCursor");
-        ok = ok && alloc(d.dynList, 2 * (size_t)H.maxPairs + (P.cloth ? 4 * (size_t)H.maxSoft : 0), "dynList");
+        ok = ok && alloc(d.dynList, 2 * (size_t)H.maxPairs + ((P.cloth || P.ogc) ? 4 * (size_t)P.maxSoft : 0), "dynList");
         // coloring
         ok = ok && upload(d.colorsA, H.colors, "colorsA", true) && upload(d.colorsB, H.colors, "colorsB");
         ok = ok && alloc(d.bodySlot, nb, "bodySlot");
@@ -454,12 +476,16 @@ struct avbd_solver {
         ok = ok && alloc(d.failureLatch, 4, "failureLatch") && alloc(d.frameCounter, 1, "frameCounter", true);
         if (H.dynamicColoring)
             d.colorStart = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(d.counters) + offsetof(Counters, colorStart));
+        if (ok) d.ogcExceed = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(d.counters) + offsetof(Counters, ogcSlots));
         if (z.numLearn) {
             const uint32_t nl = z.numLearn;
             ok = ok && upload(d.learnIdx, H.learnIdx, "learnIdx");
-            ok = ok && alloc(d.learnFeat, 16 * (size_t)nl, "learnFeatures") && alloc(d.learnPred, 3 * (size_t)nl, "learnPrediction");
+            std::vector<uint32_t> slot(nb, 0xFFFFFFFFu);
+            for (uint32_t i = 0; i < nl; i++) slot[H.learnIdx[i]] = i;
+            ok = ok && upload(d.learnSlot, slot, "learnSlot");
+            ok = ok && alloc(d.learnFeat, 32 * (size_t)nl, "learnFeatures") && alloc(d.learnPred, 3 * (size_t)nl, "learnPrediction");
             ok = ok && alloc(d.learnTarget, 3 * (size_t)nl, "learnTarget");
-            ok = ok && alloc(d.learnPrm, mlp_param_count(), "mlpParams") && alloc(d.learnNorm, 64, "mlpNorm");
+            ok = ok && alloc(d.learnPrm, mlp_param_count(), "mlpParams") && alloc(d.learnNorm, mlp_norm_count(), "mlpNorm");
             uint16_t* half = nullptr;
             ok = ok && alloc(half, mlp_half_count(), "mlpWeightsBF16");
             d.learnHalf = half;
@@ -469,7 +495,7 @@ struct avbd_solver {
         ok = ok && alloc(d.learnResidBodies, std::max<uint32_t>(1, H.numDynamicBodies), "residualBodies");
         ok = ok && alloc(d.learnResid, 4, "residual") && alloc(d.learnTrace, kTraceLength, "residualTrace");
         ok = ok && alloc(d.learnAccepted, 1, "learnAccepted", true);
-        if (P.cloth) {
+        if (H.numTris > 0) {
             // element topology
             ok = ok && upload(reinterpret_cast<u4*&>(d.tris), H.tris, "tris");
             ok = ok && upload(reinterpret_cast<uint32_t*&>(d.edges), H.edges, "edges");
@@ -477,25 +503,48 @@ struct avbd_solver {
             ok = ok && upload(d.nbrList, H.nbrList, "nbrList") && upload(d.particleIdx, H.particleIdx, "particleIdx");
             ok = ok && upload(d.selfCollision, H.selfCollision, "softSelfCollision");
             ok = ok && upload(d.membranes, H.membranes, "membranes") && upload(d.bends, H.bends, "bends");
+        }
+        if (P.cloth || P.ogc) {
             // element grid, pair streams, element contacts
             const size_t elems = (size_t)H.numTris + H.numEdges;
             const uint32_t owners = P.numParticles + H.numEdges;
             ok = ok && alloc(d.elemCellCount, 2 * (size_t)H.elemHashSize, "elemCellCount");
             ok = ok && alloc(d.elemCellStart, 2 * (size_t)H.elemHashSize, "elemCellStart");
-            ok = ok && alloc(d.elemCursor, 2 * (size_t)H.elemHashSize, "elemCursor") && alloc(d.elemCells, 64 * elems, "elemCells");
-            ok = ok && alloc(d.elemBox, 2 * elems, "elemBox");
+            ok = ok && alloc(d.elemCursor, 2 * (size_t)H.elemHashSize, "elemCursor");
+            ok = ok && alloc(d.elemCells, (P.ogc ? 27 : 64) * elems, "elemCells");
             ok = ok && alloc(d.datOwnerCount, owners, "datOwnerCount") && alloc(d.datOwnerStart, owners, "datOwnerStart");
             ok = ok && alloc(d.datEmit, owners, "datEmit") && alloc(d.datEmitStart, owners, "datEmitStart");
-            ok = ok && alloc(d.datPairs, H.maxDatPairs, "planarDATPairs");
             ok = ok && alloc(d.rtCount, H.numTris, "rtCount") && alloc(d.rtStart, H.numTris, "rtStart");
-            ok = ok && alloc(d.soft, H.maxSoft, "softContacts", true) && alloc(d.prevSoft, H.maxSoft, "prevSoftContacts", true);
-            ok = ok && alloc(d.softKeyA, H.softMapCapacity, "softMapKeyA", true);
-            ok = ok && alloc(d.softKeyB, H.softMapCapacity, "softMapKeyB", true) && alloc(d.softVal, H.softMapCapacity, "softMapVal", true);
-            std::vector<uint32_t> ones(nb, 0x3F800000u);
-            ok = ok && upload(d.truncBits, ones, "planarDATT");
+            ok = ok && alloc(d.soft, P.maxSoft, "softContacts", true) && alloc(d.prevSoft, P.maxSoft, "prevSoftContacts", true);
+            ok = ok && alloc(d.softKeyA, P.softMapCapacity, "softMapKeyA", true);
+            ok = ok && alloc(d.softKeyB, P.softMapCapacity, "softMapKeyB", true) &&
+                 alloc(d.softVal, P.softMapCapacity, "softMapVal", true);
             ok = ok && alloc(d.ogcPrev, nb, "ogcPrev", true) && alloc(d.posNext, nb, "posNext", true) && alloc(d.angNext, nb, "angNext", true);
             const uint32_t scanMax = std::max(std::max(2 * H.elemHashSize, owners), H.numTris);
             ok = ok && alloc(d.bigScanScratch, scan_large_scratch_words(scanMax), "scanScratchLarge");
+        }
+        if (P.cloth) {
+            const size_t elems = (size_t)H.numTris + H.numEdges;
+            ok = ok && alloc(d.elemBox, 2 * elems, "elemBox");
+            ok = ok && alloc(d.datPairs, H.maxDatPairs, "planarDATPairs");
+            std::vector<uint32_t> ones(nb, 0x3F800000u);
+            ok = ok && upload(d.truncBits, ones, "planarDATT");
+        }
+        if (P.ogc) {
+            const size_t elems = (size_t)H.numTris + P.numEdges;
+            ok = ok && upload(reinterpret_cast<u4*&>(d.triAdj), H.triAdj, "triAdj");
+            ok = ok && upload(d.nbr2Start, H.nbr2Start, "nbr2Start") && upload(d.nbr2Count, H.nbr2Count, "nbr2Count");
+            ok = ok && upload(d.nbr2List, H.nbr2List, "nbr2List");
+            ok = ok && upload(d.vertEdgeStart, H.vertEdgeStart, "vertEdgeStart") &&
+                 upload(d.vertEdgeCount, H.vertEdgeCount, "vertEdgeCount");
+            ok = ok && upload(d.vertEdgeList, H.vertEdgeList, "vertEdgeList") && upload(d.clothVert, H.clothVert, "clothVertFlag");
+            std::vector<u4> none(nb, u4{0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu});
+            ok = ok && upload(reinterpret_cast<u4*&>(d.vtTrack), none, "vtTrack", true) &&
+                 upload(reinterpret_cast<u4*&>(d.vtTrackPrev), none, "vtTrackPrev", true);
+            none.assign(std::max<uint32_t>(1, H.numEdges), u4{0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu});
+            ok = ok && upload(reinterpret_cast<u4*&>(d.eeTrack), none, "eeTrack", true) &&
+                 upload(reinterpret_cast<u4*&>(d.eeTrackPrev), none, "eeTrackPrev", true);
+            ok = ok && alloc(d.ogcBounds, nb, "ogcBounds") && alloc(d.elemCellsTmp, 27 * elems, "elemCellsUnsorted");
         }
         std::vector<uint32_t> spB, rJ;
         std::vector<f4> spA;
@@ -834,6 +883,11 @@ int avbd_get_counters(avbd_solver* s, avbd_counters* out) {
     uint32_t accepted = 0;
     if (s->d.learnAccepted) cudaMemcpy(&accepted, s->d.learnAccepted, 4, cudaMemcpyDeviceToHost);
     out->learn_accepted = accepted;
+    if (s->P.ogc) {
+        out->soft_rt = c.numSoftRT;
+        out->soft_vt = c.numSoftVT;
+        out->soft_ee = c.numSoftEE;
+    }
     return AVBD_OK;
 }
 
@@ -847,7 +901,7 @@ int avbd_set_warm_start_model(avbd_solver* s, const float* params, const float* 
     if (rc != AVBD_OK) return rc;
     const DevPtrs& d = s->d;
     if (!s->check(cudaMemcpy(d.learnPrm, params, sizeof(float) * mlp_param_count(), cudaMemcpyHostToDevice), "model upload") ||
-        !s->check(cudaMemcpy(d.learnNorm, norm, sizeof(float) * 64, cudaMemcpyHostToDevice), "model upload"))
+        !s->check(cudaMemcpy(d.learnNorm, norm, sizeof(float) * mlp_norm_count(), cudaMemcpyHostToDevice), "model upload"))
         return AVBD_ERR_RUNTIME_FAILURE;
     launch_mlp_mirror(d.learnPrm, d.learnHalf, s->launch);
     if (!s->check(cudaStreamSynchronize(s->launch), "model upload")) return AVBD_ERR_RUNTIME_FAILURE;
@@ -1008,16 +1062,16 @@ size_t avbd_debug_buffer_size(avbd_solver* s, int which) {
     case AVBD_BUF_NBR_START: return H.nbrStart.size() * 4;
     case AVBD_BUF_NBR_COUNT: return H.nbrCount.size() * 4;
     case AVBD_BUF_NBR_LIST: return H.nbrList.size() * 4;
-    case AVBD_BUF_PARTICLE_IDX: return s->P.cloth ? (size_t)s->P.numParticles * 4 : 0;
+    case AVBD_BUF_PARTICLE_IDX: return H.numTris ? (size_t)s->P.numParticles * 4 : 0;
     case AVBD_BUF_MEMBRANES: return H.membranes.size() * sizeof(MembraneGPU);
     case AVBD_BUF_BENDS: return H.bends.size() * sizeof(BendGPU);
     case AVBD_BUF_CLOTH_GROUP: return nb * 4;
-    case AVBD_BUF_OGC_PREV: return s->P.cloth ? nb * 16 : 0;
+    case AVBD_BUF_OGC_PREV: return (s->P.cloth || s->P.ogc) ? nb * 16 : 0;
     case AVBD_BUF_LEARN_IDX: return (size_t)s->z.numLearn * 4;
-    case AVBD_BUF_LEARN_FEATURES: return (size_t)s->z.numLearn * 64;
+    case AVBD_BUF_LEARN_FEATURES: return (size_t)s->z.numLearn * 128;
     case AVBD_BUF_LEARN_TARGETS: case AVBD_BUF_LEARN_PREDICTIONS: return (size_t)s->z.numLearn * 12;
     case AVBD_BUF_SOFT: case AVBD_BUF_DAT_PAIRS: {
-        if (!s->P.cloth) return 0;
+        if (!s->P.cloth && !(s->P.ogc && which == AVBD_BUF_SOFT)) return 0;
         Counters c{};
         cudaStreamSynchronize(s->launch);
         cudaMemcpy(&c, s->d.counters, sizeof(Counters), cudaMemcpyDeviceToHost);
@@ -1082,7 +1136,7 @@ int avbd_debug_read(avbd_solver* s, int which, void* dst, size_t bytes) {
     case AVBD_BUF_ADJ_START: case AVBD_BUF_ADJ_COUNT: case AVBD_BUF_ADJ_LIST: {
         // materialise the merged (pre, contacts, post) lists
         std::vector<uint32_t> dc(nb), ds(nb);
-        std::vector<uint32_t> dl(2 * (size_t)H.maxPairs + (s->P.cloth ? 4 * (size_t)H.maxSoft : 0));
+        std::vector<uint32_t> dl(2 * (size_t)H.maxPairs + ((s->P.cloth || s->P.ogc) ? 4 * (size_t)s->P.maxSoft : 0));
         cudaMemcpy(dc.data(), d.dynCount, 4 * nb, cudaMemcpyDeviceToHost);
         cudaMemcpy(ds.data(), d.dynStart, 4 * nb, cudaMemcpyDeviceToHost);
         cudaMemcpy(dl.data(), d.dynList, 4 * dl.size(), cudaMemcpyDeviceToHost);

@@ -162,12 +162,22 @@ __global__ void k_warmstart_bodies(const Params P, const DevPtrs d) {
     d.initLin[gid] = mk4(xyz(pl), 0.0f);
     d.initAng[gid] = pa;
     // the committed collision-query pose of every surface vertex, pins included
-    if (P.cloth && P.surfaceTruncationMode != 0u && d.shape[gid].w < 0.0f) d.ogcPrev[gid] = mk4(xyz(pl), 0.0f);
+    if ((P.cloth || P.ogc) && P.surfaceTruncationMode != 0u && d.shape[gid].w < 0.0f)
+        d.ogcPrev[gid] = mk4(xyz(pl), 0.0f);
     if (mass > 0.0f) {
-        // Isotropic-OGC warm-start truncation is a no-op while every bound is
-        // "far" (no element contact emitted a bound), which holds for every
-        // scene this build accepts.
-        const float3 guess = xyz(pl) + vl * dt + mk3(0, 0, bodyGravity) * (w * dt * dt);
+        float3 guess = xyz(pl) + vl * dt + mk3(0, 0, bodyGravity) * (w * dt * dt);
+        // Isotropic OGC: the warm start stays within the particle's bound
+        // (40_solver.metal:700-717).  Without element contacts (P.ogc == 0)
+        // every bound is "far" and this is a no-op.
+        if (P.ogc && d.shape[gid].w < 0.0f) {
+            const float d2 = __uint_as_float(d.ogcBounds[gid]);
+            if (d2 < 1e37f) {
+                const float bv = mx(0.45f * sqrtf(d2), -0.2f * d.shape[gid].w);
+                const float3 tot = guess - xyz(pl);
+                const float t2 = dot(tot, tot);
+                if (t2 > bv * bv) guess = xyz(pl) + tot * (bv * rsq(t2));
+            }
+        }
         d.posLin[gid] = mk4(guess, mass);
         d.posAng[gid] = q_addw(pa, va * dt);
     }
@@ -186,7 +196,7 @@ void launch_warmstart(const Params& P, const DevPtrs& d, const Sizes& z, cudaStr
 template <bool SCATTER>
 __global__ void k_adj_dyn(const Params P, const DevPtrs d) {
     const uint32_t nm = d.counters->numPairs;
-    const uint32_t ns = P.cloth ? d.counters->numSoft : 0u;
+    const uint32_t ns = (P.cloth || P.ogc) ? d.counters->numSoft : 0u;
     auto put = [&](uint32_t b, uint32_t e) {
         if (!body_dynamic(d, b)) return;
         if (SCATTER) d.dynList[atomicAdd(&d.dynCursor[b], 1u)] = e;
@@ -225,7 +235,7 @@ __global__ void k_adj_dyn_sort(const DevPtrs d, uint32_t nb) {
 
 void launch_adjacency(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     cudaMemsetAsync(d.dynCount, 0, sizeof(uint32_t) * P.numBodies, st);
-    const uint32_t items = z.maxPairs + (P.cloth ? z.maxSoft : 0u);
+    const uint32_t items = z.maxPairs + ((P.cloth || P.ogc) ? z.maxSoft : 0u);
     k_adj_dyn<false><<<stride_blocks(items, 128), 128, 0, st>>>(P, d);
     launch_exclusive_scan(d.dynCount, d.dynStart, P.numBodies, d.scanScratch, st);
     cudaMemcpyAsync(d.dynCursor, d.dynStart, sizeof(uint32_t) * P.numBodies, cudaMemcpyDeviceToDevice, st);
@@ -758,6 +768,25 @@ __device__ __forceinline__ float3 shfl3(unsigned mask, float3 v, int o) {
 }
 __device__ __forceinline__ void add_shfl3(unsigned mask, float3& v, int o) { v = v + shfl3(mask, v, o); }
 
+// Isotropic-OGC conservative-bound truncation (ogcTruncate,
+// 40_solver.metal:1361-1382): the displacement since the bound's anchor stays
+// within max(0.45 * bound distance, 0.2 * radius); every clamped step is
+// counted for the mid-solve refresh.
+__device__ __forceinline__ float3 ogc_truncate(const DevPtrs& d, uint32_t body, float3 dxLin, float3 cur, float partR) {
+    const float d2 = __uint_as_float(d.ogcBounds[body]);
+    if (d2 >= 1e37f) return dxLin;
+    const float bv = mx(0.45f * sqrtf(d2), 0.2f * partR);
+    const float3 x0 = xyz(d.ogcPrev[body]);
+    float3 tot = (cur + dxLin) - x0;
+    const float t2 = dot(tot, tot);
+    if (t2 > bv * bv) {
+        tot *= bv * rsq(t2);
+        dxLin = (x0 + tot) - cur;
+        atomicAdd(d.ogcExceed, 1u);
+    }
+    return dxLin;
+}
+
 // A skipped update (non-finite step) still publishes the unchanged pose
 // when the color commits through posNext.
 __device__ __forceinline__ void keep_body(const Params& P, const DevPtrs& d, uint32_t body, float4 pl, bool rigid) {
@@ -814,8 +843,7 @@ __device__ void primal_body(const Params& P, const DevPtrs& d, uint32_t body, ui
     const float maxLin = 0.35f * fabsf(shp.w);
     const float lin2 = dot(dxLin, dxLin);
     if (lin2 > maxLin * maxLin) dxLin *= maxLin * rsq(lin2);
-    // Isotropic OGC truncation needs an emitted conservative bound; with no
-    // element contacts every bound is "far" and the step is unchanged.
+    if (!rigid && P.ogc) dxLin = ogc_truncate(d, body, dxLin, xyz(pl), -shp.w);
     if (P.colorJacobi) {
         d.posNext[body] = mk4(xyz(pl) + dxLin, mass);
         if (rigid) d.angNext[body] = q_addw(d.posAng[body], dxAng);
@@ -1263,6 +1291,7 @@ __global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevP
     const float maxLin = 0.35f * fabsf(shp.w);
     const float lin2 = dot(dxLin, dxLin);
     if (lin2 > maxLin * maxLin) dxLin *= maxLin * rsq(lin2);
+    if (P.ogc) dxLin = ogc_truncate(d, body, dxLin, xyz(pl), -shp.w);
     if (P.colorJacobi) { d.posNext[body] = mk4(xyz(pl) + dxLin, mass); return; }
     d.posLin[body] = mk4(xyz(pl) + dxLin, mass);
 }
@@ -1289,7 +1318,7 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
         const uint32_t lanes_ = lanes < 8 ? 8 : (lanes > 32 ? 32 : lanes);
         const uint32_t w = lanes_ <= 8 ? 8 : (lanes_ <= 16 ? 16 : 32);
         if (z.particleFastPath) launch_primal_group<false, false>(P, d, color, upper, w, st);
-        else if (P.cloth) launch_primal_group<true, true>(P, d, color, upper, w, st);
+        else if (P.cloth || P.ogc) launch_primal_group<true, true>(P, d, color, upper, w, st);
         else launch_primal_group<true, false>(P, d, color, upper, w, st);
     }
 }
@@ -1298,8 +1327,7 @@ void launch_residual(const Params& P, const DevPtrs& d, const Sizes& z, float* p
                      cudaStream_t st) {
     const uint32_t n = z.numDynamicBodies;
     if (n && z.numDynamicRigid == 0 && perBody == d.learnResidBodies) {
-        // particle-only: the group stamping of the primal, one launch per
-        // static color at its lane width (or all bodies at 32 lanes)
+        // particle-only: the group stamping of the primal over all colors at once
         auto run = [&](uint32_t color, uint32_t count, uint32_t lanes) {
             const uint32_t w = lanes <= 8 ? 8u : (lanes <= 16 ? 16u : 32u);
             const uint32_t blocks = (count * w + 127) / 128;
@@ -1307,18 +1335,13 @@ void launch_residual(const Params& P, const DevPtrs& d, const Sizes& z, float* p
                 if (w == 8) k_primal_group<8, false, false, true><<<blocks, 128, 0, st>>>(P, d, color, count);
                 else if (w == 16) k_primal_group<16, false, false, true><<<blocks, 128, 0, st>>>(P, d, color, count);
                 else k_primal_group<32, false, false, true><<<blocks, 128, 0, st>>>(P, d, color, count);
-            } else if (P.cloth) {
+            } else if (P.cloth || P.ogc) {
                 k_primal_group<32, true, true, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, d, color, count);
             } else {
                 k_primal_group<32, true, false, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, d, color, count);
             }
         };
-        if (z.dynamicColoring || !z.colorCounts) {
-            run(0u, n, 32u);
-        } else {
-            for (uint32_t c = 0; c < MAX_COLORS; c++)
-                if (z.colorCounts[c]) run(c, z.colorCounts[c], z.colorLanes[c]);
-        }
+        run(0u, n, 32u);
     } else if (n) {
         k_residual_bodies<<<(n * 8 + 127) / 128, 128, 0, st>>>(P, d, n, perBody);
     }
@@ -1469,14 +1492,14 @@ __device__ __forceinline__ void dual_item(const Params& P, const DevPtrs& d, con
 __global__ void k_dual(const Params P, const DevPtrs d, const Sizes z) {
     pdl_prologue();
     const uint32_t numPairs = d.counters->numPairs;
-    const uint32_t numSoft = P.cloth ? d.counters->numSoft : 0u;
+    const uint32_t numSoft = (P.cloth || P.ogc) ? d.counters->numSoft : 0u;
     const uint32_t total = z.numActiveJoints + z.numHardSprings + numPairs + numSoft;
     for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x)
         dual_item(P, d, z, g, numPairs);
 }
 
 void launch_dual(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
-    const uint32_t upper = z.numActiveJoints + z.numHardSprings + z.maxPairs + (P.cloth ? z.maxSoft : 0u);
+    const uint32_t upper = z.numActiveJoints + z.numHardSprings + z.maxPairs + ((P.cloth || P.ogc) ? z.maxSoft : 0u);
     launch_pdl(k_dual, stride_blocks(upper, 128), 128, st, P, d, z);
 }
 
@@ -1672,7 +1695,7 @@ __global__ void k_frame_end(const Params P, const DevPtrs d, const Sizes z, floa
         uint32_t kind = 0, detail = 0;
         const Counters* c = d.counters;
         if (c->pairCandidates > P.maxPairs) { kind = AVBD_FAIL_RIGID_PAIR_CAPACITY_; detail = c->pairCandidates; }
-        else if (P.cloth && c->softRaw > P.maxSoft) { kind = 3; detail = c->softRaw; }
+        else if ((P.cloth || P.ogc) && c->softRaw > P.maxSoft) { kind = 3; detail = c->softRaw; }
         else if (P.cloth && c->datPairsPeak > P.maxDatPairs) { kind = 6; detail = c->datPairsPeak; }
         else if (P.cloth && c->datGridOverflow > 0) { kind = 7; detail = c->datGridOverflow; }
         else if (P.cloth && c->datInvalidAnchor > 0) { kind = 8; detail = c->datInvalidAnchor; }
@@ -1684,6 +1707,9 @@ __global__ void k_frame_end(const Params P, const DevPtrs d, const Sizes z, floa
         }
         // peak dynamic palette size, read by the host to size the color launches
         if (z.dynamicColoring && c->usedColors > d.failureLatch[3]) d.failureLatch[3] = c->usedColors;
+        // OGC bound exceeders of the last pass (the counter the reference
+        // leaves at frame end: every earlier pass is consumed by a refresh)
+        if (P.ogc) d.counters->ogcExceeded = P.iterations ? c->ogcSlots[(P.iterations - 1u) & 1u] : 0u;
     }
 }
 

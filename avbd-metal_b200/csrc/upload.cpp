@@ -276,6 +276,66 @@ void upload_cloth(const avbd_scene_desc* s, const std::vector<std::array<int, 3>
     H.surfaceCellSize = fmax_(0.02f, fmax_(fmax_(reach, meanEdge * 1.05f), maxElemR + maxPartR + H.elemMargin));
     H.elemCellSize = fmax_(0.02f, fmax_(fmax_(reach, meanEdge * 1.05f), 2.0f * maxElemR + H.queryRadius));
 
+    // isotropic-OGC topology (GPUSolver.swift:1338-1460): edge-adjacent
+    // triangles (edges visited in ascending key order), the incident contact
+    // edges of every vertex, and the sorted 1-ring-plus-2-ring sets.
+    std::map<uint64_t, std::pair<int, int>> edgeTris;
+    for (uint32_t ti = 0; ti < H.numTris; ti++) {
+        const int a = coll[ti][0], b = coll[ti][1], c = coll[ti][2];
+        const int ends[3][2] = {{a, b}, {b, c}, {a, c}};
+        for (const auto& e : ends) {
+            auto it = edgeTris.find(edge_key(e[0], e[1]));
+            if (it == edgeTris.end()) edgeTris.emplace(edge_key(e[0], e[1]), std::make_pair((int)ti, -1));
+            else it->second.second = (int)ti;
+        }
+    }
+    H.triAdj.assign(std::max<uint32_t>(1, H.numTris), u4{0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu});
+    std::vector<int> fill(std::max<uint32_t>(1, H.numTris), 0);
+    auto put = [&](int t, int other) {
+        if (fill[t] >= 3) return;
+        uint32_t* slots = &H.triAdj[t].x;
+        slots[fill[t]++] = (uint32_t)other;
+    };
+    for (const auto& kv : edgeTris) {
+        if (kv.second.second < 0) continue;
+        put(kv.second.first, kv.second.second);
+        put(kv.second.second, kv.second.first);
+    }
+    std::vector<std::vector<uint32_t>> vertEdges(nb);
+    for (uint32_t i = 0; i < H.numEdges; i++) {
+        vertEdges[H.edges[2 * i]].push_back(i);
+        vertEdges[H.edges[2 * i + 1]].push_back(i);
+    }
+    H.vertEdgeStart.assign(nb, 0);
+    H.vertEdgeCount.assign(nb, 0);
+    H.vertEdgeList.clear();
+    for (uint32_t i = 0; i < nb; i++) {
+        H.vertEdgeStart[i] = (uint32_t)H.vertEdgeList.size();
+        H.vertEdgeCount[i] = (uint32_t)vertEdges[i].size();
+        H.vertEdgeList.insert(H.vertEdgeList.end(), vertEdges[i].begin(), vertEdges[i].end());
+    }
+    H.nbr2Start.assign(nb, 0);
+    H.nbr2Count.assign(nb, 0);
+    H.nbr2List.clear();
+    std::vector<uint32_t> mark(nb, 0xFFFFFFFFu), two;
+    for (uint32_t i = 0; i < nb; i++) {
+        H.nbr2Start[i] = (uint32_t)H.nbr2List.size();
+        if (ring[i].empty()) continue;
+        two.clear();
+        mark[i] = i;
+        for (uint32_t n1 : ring[i]) {
+            if (mark[n1] != i) { mark[n1] = i; two.push_back(n1); }
+            for (uint32_t n2 : ring[n1])
+                if (mark[n2] != i) { mark[n2] = i; two.push_back(n2); }
+        }
+        std::sort(two.begin(), two.end());
+        H.nbr2Count[i] = (uint32_t)two.size();
+        H.nbr2List.insert(H.nbr2List.end(), two.begin(), two.end());
+    }
+    H.clothVert.assign(nb, 0);
+    for (uint32_t i = 0; i < authored; i++)
+        for (int k = 0; k < 3; k++) H.clothVert[s->tris[i].ids[k]] = 1;
+
     // capacities (GPUSolver.swift:395-443)
     const uint64_t surf = H.particleIdx.size();
     const uint64_t pairsCap = std::max<uint64_t>(1, 64ull * surf + 128ull * topo.size());
@@ -284,6 +344,9 @@ void upload_cloth(const avbd_scene_desc* s, const std::vector<std::array<int, 3>
     H.maxSoft = (uint32_t)std::max<uint64_t>(1, 4ull * H.numTris + budget);
     H.softMapCapacity = next_pow2(std::max<uint32_t>(64u, 2u * H.maxSoft));
     H.elemHashSize = next_pow2(std::max<uint32_t>(64u, 2u * 4u * H.numTris));
+    const uint64_t iso = std::max<uint64_t>(1, 4ull * surf + 4ull * H.numTris + 4ull * H.numSurfaceEdges);
+    H.maxSoftIso = (uint32_t)std::min<uint64_t>(iso, 0x7FFFFFFFull);
+    H.softMapCapacityIso = next_pow2(std::max<uint32_t>(64u, 2u * H.maxSoftIso));
 }
 
 }  // namespace
@@ -300,14 +363,6 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
             err = "torus, capsule and convex-hull colliders are not supported by this build";
             return AVBD_ERR_UNSUPPORTED;
         }
-    }
-    if (s->num_tris > 0 && s->num_tets > 0) {
-        err = "scenes mixing cloth triangles and tets are not supported by this build";
-        return AVBD_ERR_UNSUPPORTED;
-    }
-    if (s->num_tris > 0 && s->truncation_selection == AVBD_TRUNCATION_ISOTROPIC) {
-        err = "isotropic OGC truncation of cloth is not supported by this build (Planar-DAT is)";
-        return AVBD_ERR_UNSUPPORTED;
     }
     for (uint32_t i = 0; i < s->num_tris; i++)
         for (int k = 0; k < 3; k++)
@@ -538,44 +593,24 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
 
     // ---- cloth topology and elements (GPUSolver.swift:1289-1680)
     H.cloth = s->num_tris > 0;
-    if (H.cloth) upload_cloth(s, boundary, H);
-
-    // ---- collision-surface groups of tet boundaries (GPUSolver.swift:1461-1535)
-    if (!H.cloth && !boundary.empty()) {
-        std::vector<int> parent(nb, -1);
-        auto find = [&](int x) {
-            int r = x;
-            while (parent[r] >= 0 && parent[r] != r) r = parent[r];
-            int c = x;
-            while (parent[c] >= 0 && parent[c] != r) { int n = parent[c]; parent[c] = r; c = n; }
-            if (parent[r] < 0) parent[r] = r;
-            return r;
-        };
-        for (const auto& f : boundary) { int r = find(f[0]); parent[find(f[1])] = r; parent[find(f[2])] = r; }
-        std::map<int, uint32_t> groupIndex;
-        std::vector<uint8_t> surf(nb, 0);
-        for (const auto& f : boundary) {
-            int root = find(f[0]);
-            auto it = groupIndex.find(root);
-            uint32_t g;
-            if (it == groupIndex.end()) { g = (uint32_t)groupIndex.size() + 1; groupIndex.emplace(root, g); }
-            else g = it->second;
-            for (int k = 0; k < 3; k++) if (s->bodies[f[k]].is_particle) { H.clothGroup[f[k]] = g; surf[f[k]] = 1; }
-        }
-        for (uint32_t i = 0; i < nb; i++) H.numParticles += surf[i];
-        // Element contacts (V-T, E-E, rigid feature vs triangle) are not in
-        // this build: accept only scenes where they cannot arise — one soft
-        // surface without self-collision and no rigid collider other than
-        // large static ground slabs whose corners lie far outside the scene.
-        if (groupIndex.size() > 1) { err = "contacts between separate soft surfaces (V-T/E-E) are not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
-        for (uint32_t i = 0; i < s->num_tets; i++)
-            if (s->tets[i].self_collision) { err = "volumetric self-collision is not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+    if (H.numTris > 0) {
+        upload_cloth(s, boundary, H);
+        // Element contacts (V-T, E-E, rigid feature vs triangle) can arise
+        // unless the scene has a single closed soft surface, no authored
+        // triangles, no self-collision and no rigid collider other than
+        // large static ground slabs whose corners lie far outside the scene:
+        // then the isotropic-OGC stages would produce nothing and are skipped.
+        std::set<uint32_t> groups;
+        bool self = false;
+        for (uint32_t v : H.particleIdx) { groups.insert(H.clothGroup[v]); self = self || H.selfCollision[v] != 0; }
+        bool rigidReach = false;
         for (uint32_t i = 0; i < nc; i++) {
             const avbd_collider_desc& c = s->colliders[i];
             if (!c.collision_enabled || s->bodies[c.body].is_particle) continue;
-            bool slab = !H.isDynamic[c.body] && c.shape == AVBD_SHAPE_BOX && c.size[0] >= 20.0f && c.size[1] >= 20.0f;
-            if (!slab) { err = "rigid-vs-soft-surface contacts are not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+            const bool slab = !H.isDynamic[c.body] && c.shape == AVBD_SHAPE_BOX && c.size[0] >= 20.0f && c.size[1] >= 20.0f;
+            rigidReach = rigidReach || !slab;
         }
+        H.ogc = H.cloth || groups.size() > 1 || self || rigidReach;
     }
 
     // ---- static palette for soft scenes (GPUSolver.swift:1956-2049)
@@ -653,7 +688,7 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
     // The warp-per-particle primal may drop its generic stamp path when no
     // dynamic body is rigid and no particle carries a joint or spring entry
     // (sphere contacts always have exactly one contact point).
-    H.particleFastPath = !H.cloth;
+    H.particleFastPath = !H.cloth && !H.ogc;
     for (uint32_t b = 0; b < nb && H.particleFastPath; b++) {
         if (!(H.posLin[b].w > 0.0f)) continue;
         if (H.shape[b].w >= 0.0f || !pre[b].empty()) { H.particleFastPath = false; break; }
@@ -714,9 +749,13 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
         const uint32_t automatic = (volumetricSelf || (s->num_tris > 0 && s->num_tets == 0)) ? 2u : 1u;
         P.surfaceTruncationMode = s->truncation_selection == AVBD_TRUNCATION_AUTOMATIC ? automatic : s->truncation_selection;
     }
-    if (P.surfaceTruncationMode == 2u && !H.cloth) { err = "Planar-DAT truncation of tet surfaces is not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+    if (P.surfaceTruncationMode == 2u && s->num_tets > 0) { err = "Planar-DAT truncation of tet surfaces is not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
     P.cloth = (H.cloth && P.surfaceTruncationMode == 2u) ? 1u : 0u;
-    P.colorJacobi = P.cloth;
+    H.ogc = H.ogc && P.surfaceTruncationMode == 1u;
+    P.ogc = H.ogc ? 1u : 0u;
+    // Element contacts couple bodies that share a static color: those scenes
+    // solve a color against its pre-color pose and publish it afterwards.
+    P.colorJacobi = (P.cloth || P.ogc) ? 1u : 0u;
     P.numEdges = H.numEdges;
     P.numSurfaceEdges = H.numSurfaceEdges;
     P.elemHashSize = H.elemHashSize;
@@ -733,6 +772,15 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
     P.tetInversionPreventionEnabled = 0;
     P.planarDATRelaxation = 0.85f;
     P.numExclusions = (uint32_t)(H.exclusions.size() / 2);
+    if (P.ogc) {
+        // isotropic element contacts: detection-radius cells, authored
+        // contact edges only, the isotropic soft-contact budget
+        // (GPUSolver.swift:2117-2133)
+        P.elemCellSize = H.surfaceCellSize;
+        P.numEdges = H.numSurfaceEdges;
+        P.maxSoft = H.maxSoftIso;
+        P.softMapCapacity = H.softMapCapacityIso;
+    }
     return AVBD_OK;
 }
 

@@ -68,6 +68,17 @@ struct HostScene {
     std::vector<MembraneGPU> membranes;
     std::vector<BendGPU> bends;
 
+    // isotropic OGC (25_cloth.metal:347-931): tracker propagation topology
+    // and the 2-ring exclusion sets of the conservative bounds.  `ogc` is set
+    // when element contacts can arise (several surfaces, authored triangles,
+    // self-collision or rigid colliders that may reach a surface).
+    bool ogc = false;
+    std::vector<u4> triAdj;               // up to 3 edge-adjacent triangles per triangle
+    std::vector<uint32_t> nbr2Start, nbr2Count, nbr2List;
+    std::vector<uint32_t> vertEdgeStart, vertEdgeCount, vertEdgeList;
+    std::vector<uint32_t> clothVert;      // 1 for vertices of authored triangles
+    uint32_t maxSoftIso = 1, softMapCapacityIso = 64;
+
     // dynamic particles whose warm start the learned model may predict
     std::vector<uint32_t> learnIdx;
 };

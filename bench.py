@@ -302,7 +302,7 @@ def learned_comparison(args, world, dev, stream, flush, plain_value):
     accepted = solver.counters().learn_accepted
     solver.close()
     value = world * nv * args.steps / (ms / 1e3)
-    return {"warm_start": "learned: 16-128-128-128-3 MLP, BF16 tensor-core inference, kept only when its "
+    return {"warm_start": "learned: 32-128-128-128-3 MLP, BF16 tensor-core inference, kept only when its "
                           "residual after 1 trial sweep is no worse than the plain warm start's",
             "iterations": k, "plain_iterations": plain_iters,
             "matched_median_rel_residual": {"plain": r_plain, "learned": r_learned,

@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define AVBD_ABI_VERSION 2u
+#define AVBD_ABI_VERSION 3u
 
 /* ------------------------------------------------------------------------ */
 /* Status codes.  Construction errors mirror `AVBDError`                     */
@@ -244,6 +244,12 @@ typedef struct avbd_counters {
     uint32_t dat_nonfinite;
     uint32_t dat_tet_degenerate;
     uint32_t learn_accepted;      /* frames whose predicted warm start was kept */
+    /* isotropic-OGC element contacts of the last retired frame: rigid-
+     * triangle, vertex-triangle and edge-edge records (rt_emit, vt_emit,
+     * ee_emit, 25_cloth.metal:347-1142)                                    */
+    uint32_t soft_rt;
+    uint32_t soft_vt;
+    uint32_t soft_ee;
 } avbd_counters;
 
 typedef struct avbd_solver avbd_solver;
@@ -350,20 +356,20 @@ int avbd_set_profiling(avbd_solver* solver, int enabled);
 int avbd_get_profile(avbd_solver* solver, avbd_profile* out);
 
 /* ---- Learned warm start (no counterpart in the reference) -------------
- * A 16-128-128-128-16 MLP (BF16 weights/activations, FP32 accumulation)
+ * A 32-128-128-128-16 MLP (BF16 weights/activations, FP32 accumulation)
  * predicts each dynamic particle's correction of the plain gamma warm start
  * from local features.  In AVBD_WARM_START_LEARNED mode every frame races
  * the plain and the predicted warm start for `trial_sweeps` primal sweeps and
  * keeps the prediction only when its augmented-Lagrangian residual is no
  * larger; plain AVBD stays the fallback.  Parameters are the fp32 block of
- * avbd_mlp_param_count() floats (W1[128][16], b1, W2[128][128], b2,
- * W3[128][128], b3, W4[16][128], b4[16]); `norm` holds 64 floats: feature
- * mean[16], feature 1/std[16], target mean[16], target std[16].          */
+ * avbd_mlp_param_count() floats (W1[128][32], b1, W2[128][128], b2,
+ * W3[128][128], b3, W4[16][128], b4[16]); `norm` holds 96 floats: feature
+ * mean[32], feature 1/std[32], target mean[16], target std[16].          */
 enum { AVBD_WARM_START_PLAIN = 0, AVBD_WARM_START_LEARNED = 1 };
 int avbd_set_warm_start_model(avbd_solver* solver, const float* params, const float* norm,
                               uint32_t trial_sweeps);
 int avbd_set_warm_start_mode(avbd_solver* solver, int mode);
-/* Record every frame's features and training targets (the solve's
+/* Record every frame's features [n][32] and training targets (the solve's
  * correction of the plain warm start) in the LEARN_* debug buffers.       */
 int avbd_set_learning_capture(avbd_solver* solver, int enabled);
 /* Per-frame residual trace: out[0] at the plain warm start, out[1] at the
@@ -373,7 +379,7 @@ int avbd_set_residual_trace(avbd_solver* solver, int enabled);
 int avbd_get_residual_trace(avbd_solver* solver, double* out, uint32_t n);
 
 /* Training kernels (device pointers; stream may be null).  A batch is
- * features[batch][16] and targets[batch][3] (raw, normalised with `norm`);
+ * features[batch][32] and targets[batch][3] (raw, normalised with `norm`);
  * the workspace holds avbd_mlp_workspace_bytes(batch) bytes.             */
 uint32_t avbd_mlp_param_count(void);
 size_t avbd_mlp_workspace_bytes(uint32_t batch);
@@ -406,7 +412,7 @@ enum {
     AVBD_BUF_NBR_COUNT = 29, AVBD_BUF_NBR_LIST = 30, AVBD_BUF_PARTICLE_IDX = 31,
     AVBD_BUF_MEMBRANES = 32, AVBD_BUF_BENDS = 33, AVBD_BUF_SOFT = 34,
     AVBD_BUF_DAT_PAIRS = 35, AVBD_BUF_CLOTH_GROUP = 36, AVBD_BUF_OGC_PREV = 37,
-    /* learned warm start: vertex ids, features [n][16], targets and
+    /* learned warm start: vertex ids, features [n][32], targets and
      * predictions [n][3] of the last frame                                  */
     AVBD_BUF_LEARN_IDX = 38, AVBD_BUF_LEARN_FEATURES = 39, AVBD_BUF_LEARN_TARGETS = 40,
     AVBD_BUF_LEARN_PREDICTIONS = 41,

@@ -46,14 +46,6 @@ int Solver::create(const avbd_scene_desc* s) {
             return AVBD_ERR_UNSUPPORTED;
         }
     }
-    if (s->num_tris > 0 && s->num_tets > 0) {
-        error = "scenes mixing cloth triangles and tets are not restated";
-        return AVBD_ERR_UNSUPPORTED;
-    }
-    if (s->num_tris > 0 && s->truncation_selection == AVBD_TRUNCATION_ISOTROPIC) {
-        error = "isotropic OGC truncation of cloth is not restated";
-        return AVBD_ERR_UNSUPPORTED;
-    }
 
     uint32_t enabled = 0;
     for (uint32_t i = 0; i < nc; i++) enabled += s->colliders[i].collision_enabled ? 1u : 0u;
@@ -296,40 +288,25 @@ int Solver::create(const avbd_scene_desc* s) {
     exclusions.clear();
     for (uint64_t k : excl) { exclusions.push_back((uint32_t)(k >> 32)); exclusions.push_back((uint32_t)(k & 0xFFFFFFFFu)); }
 
-    if (s->num_tris > 0) {
+    bool ogcCandidate = false;
+    if (numTris > 0) {
         int rc = cloth_upload(s, boundary);
         if (rc != AVBD_OK) return rc;
-        colorJacobi = true;
-    }
-
-    // collision-surface groups for tet boundary faces (GPUSolver.swift:1461-1535)
-    if (s->num_tris == 0 && !boundary.empty()) {
-        std::vector<int> parent(nb, -1);
-        auto find = [&](int x) { int r = x; while (parent[r] >= 0 && parent[r] != r) r = parent[r];
-            int c = x; while (parent[c] >= 0 && parent[c] != r) { int n = parent[c]; parent[c] = r; c = n; }
-            if (parent[r] < 0) parent[r] = r;
-            return r; };
-        for (auto& f : boundary) { int r = find(f[0]); parent[find(f[1])] = r; parent[find(f[2])] = r; }
-        std::map<int, uint32_t> groupIndex;
-        std::vector<uint8_t> surf(nb, 0);
-        for (auto& f : boundary) {
-            int root = find(f[0]);
-            if (!groupIndex.count(root)) { uint32_t g = (uint32_t)groupIndex.size() + 1; groupIndex[root] = g; }
-            uint32_t g = groupIndex[root];
-            for (int k = 0; k < 3; k++) if (isParticle[f[k]]) { clothGroup[f[k]] = g; surf[f[k]] = 1; }
-        }
-        numParticles = 0;
-        for (uint32_t i = 0; i < nb; i++) numParticles += surf[i];
-        // element contacts are not restated yet: refuse scenes that need them
-        if (groupIndex.size() > 1) { error = "soft-soft element contacts are not restated"; return AVBD_ERR_UNSUPPORTED; }
-        for (uint32_t i = 0; i < s->num_tets; i++)
-            if (s->tets[i].self_collision) { error = "volumetric self-collision is not restated"; return AVBD_ERR_UNSUPPORTED; }
+        // element contacts can arise unless the scene is one closed soft
+        // surface without authored triangles or self-collision whose only
+        // rigid colliders are far-reaching static ground slabs (then the
+        // isotropic stages produce nothing and are skipped)
+        std::set<uint32_t> groups;
+        bool self = false;
+        for (uint32_t v : particleIdx) { groups.insert(clothGroup[v]); self = self || selfCollision[v] != 0; }
+        bool rigidReach = false;
         for (uint32_t i = 0; i < nc; i++) {
             const avbd_collider_desc& c = s->colliders[i];
             if (!c.collision_enabled || isParticle[c.body]) continue;
             bool slab = !isDynamic[c.body] && c.shape == AVBD_SHAPE_BOX && c.size[0] >= 20.0f && c.size[1] >= 20.0f;
-            if (!slab) { error = "rigid-vs-soft-surface contacts are not restated"; return AVBD_ERR_UNSUPPORTED; }
+            rigidReach = rigidReach || !slab;
         }
+        ogcCandidate = cloth || groups.size() > 1 || self || rigidReach;
     }
 
     // static coloring (GPUSolver.swift:1956-2049)
@@ -407,6 +384,19 @@ int Solver::create(const avbd_scene_desc* s) {
     }
     P.tetInversionPreventionEnabled = (P.surfaceTruncationMode == 2u && s->tet_inversion_prevention) ? 1u : 0u;
     P.planarDATRelaxation = 0.85f;
+    if (P.surfaceTruncationMode == 2u && s->num_tets > 0) {
+        error = "Planar-DAT truncation of tet surfaces is not restated";
+        return AVBD_ERR_UNSUPPORTED;
+    }
+    ogc = ogcCandidate && P.surfaceTruncationMode == 1u;
+    colorJacobi = (cloth && P.surfaceTruncationMode == 2u) || ogc;
+    if (ogc) {
+        maxSoft = maxSoftIso;
+        softMapCapacity = softMapCapacityIso;
+        soft.assign(maxSoft, SoftContactGPU{});
+        prevSoft.assign(maxSoft, SoftContactGPU{});
+        softKeyA.assign(softMapCapacity, 0); softKeyB.assign(softMapCapacity, 0); softVal.assign(softMapCapacity, 0);
+    }
     return AVBD_OK;
 }
 
@@ -1541,7 +1531,10 @@ void Solver::primal_body(uint32_t body) {
             if (t2 > bv * bv) {
                 tot *= bv * rsqrt_(t2);
                 dxLin = (x0 + tot) - xyz(pl);
-                ogcExceeded++;
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+                ogcPass++;
             }
         }
     }
@@ -1754,6 +1747,7 @@ void Solver::step() {
     sync_params();
     std::fill(boundsBits.begin(), boundsBits.end(), 0x7F7F7F7Fu);
     ogcExceeded = 0;
+    ogcPass = 0;
     colorConflicts = 0;
     const bool planar = P.surfaceTruncationMode == 2u && numTris > 0;
     dat = DatCounters{};
@@ -1766,6 +1760,8 @@ void Solver::step() {
         elem_grid();
         dat_build_pairs();                     // step-start pose
         rt_emit();
+    } else if (ogc) {
+        ogc_detect();
     }
     warmstart_joints();
     warmstart_bodies();
@@ -1782,26 +1778,38 @@ void Solver::step() {
     if (dynamicColoring) dynamic_coloring();
     uint32_t colorBound = dynamicColoring ? (uint32_t)MAX_COLORS : staticUsedColors;
     for (uint32_t it = 0; it < P.iterations; it++) {
+        ogcPass = 0;
         for (uint32_t c = 0; c < colorBound; c++) {
             primal_color(c);
             if (planar) {
                 dat_reduce(c);
                 dat_apply_color(c);
+            } else if (ogc) {
+                publish_color(c);
             }
         }
         dual_all();
+        // mid-solve bound refresh when more than 1% of the surface vertices
+        // were bound-limited (ogc_refresh_args, 25_cloth.metal:857-870)
+        if (ogc && it + 1 < P.iterations && ogcPass * 100u > P.numParticles) ogc_refresh();
+        ogcExceeded = ogcPass;
     }
     if (planar) dat_restore_failed_surface();
     finalize();
-    if (numTris > 0 && cloth && clothViscosity > 0.0f) smooth_particle_velocities();
+    if (numTris > 0 && clothViscosity > 0.0f) smooth_particle_velocities();
     advance_spinners();
     frameIndex++;
     // the manifolds written this frame become next frame's warm-start source
     std::swap(manifolds, prevManifolds);
-    if (cloth) std::swap(soft, prevSoft);
+    if (cloth || ogc) std::swap(soft, prevSoft);
+    if (ogc) { std::swap(vtTrack, vtTrackPrev); std::swap(eeTrack, eeTrackPrev); }
     if (pairCandidates > maxPairs && failure == AVBD_FAIL_NONE) {
         failure = AVBD_FAIL_RIGID_PAIR_CAPACITY;
         error = "rigid pair capacity exceeded";
+    }
+    if (ogc && failure == AVBD_FAIL_NONE && dat.softCandidates > maxSoft) {
+        failure = AVBD_FAIL_SOFT_CONTACT_CAPACITY;
+        error = "soft contact capacity exceeded";
     }
     if (planar && failure == AVBD_FAIL_NONE) {
         if (dat.softCandidates > maxSoft) { failure = AVBD_FAIL_SOFT_CONTACT_CAPACITY; error = "soft contact capacity exceeded"; }
@@ -1901,6 +1909,11 @@ int oracle_get_counters(void* h, avbd_counters* out) {
     out->dat_ee_degenerate = s->dat.eeDegenerate;
     out->dat_nonfinite = s->dat.nonfinite;
     out->dat_tet_degenerate = s->dat.tetDegenerate;
+    if (s->ogc) {
+        out->soft_rt = s->numSoftRT;
+        out->soft_vt = s->numSoftVT;
+        out->soft_ee = s->numSoftEE;
+    }
     return AVBD_OK;
 }
 static const void* oracle_buffer(Solver* s, int which, size_t& bytes) {

@@ -1,6 +1,6 @@
 """Float64 forward/backward of the warm-start MLP — TEST INFRASTRUCTURE.
 
-The network is the one of avbd-metal_b200/csrc/learned.cu: 16 -> 128 -> 128
+The network is the one of avbd-metal_b200/csrc/learned.cu: 32 -> 128 -> 128
 -> 128 -> 16 with ReLU, the first 3 outputs used, mean-squared-error loss on
 targets normalised by (ymean, ystd).  With `rounded=True` the oracle rounds
 exactly where the kernels store BF16 (normalised inputs, weights, hidden
@@ -13,7 +13,8 @@ Only tests/ may import this module.
 """
 import numpy as np
 
-DIN, HID, DOUT, USED = 16, 128, 16, 3
+DIN, HID, DOUT, USED = 32, 128, 16, 3
+XM, XI, YM, YS = 0, 32, 64, 80          # offsets in the 96-float normalisation block
 OW1 = 0
 OB1 = OW1 + HID * DIN
 OW2 = OB1 + HID
@@ -54,12 +55,12 @@ def forward_backward(params, norm, X, T, rounded=True):
     T = np.asarray(T, np.float64)
     B = X.shape[0]
     W1b, W2b, W3b, W4b = R(W1), R(W2), R(W3), R(W4)
-    Xb = R(F((X - norm[:16]) * norm[16:32]))
+    Xb = R(F((X - norm[XM:XM + DIN]) * norm[XI:XI + DIN]))
     H1 = R(np.maximum(Xb @ W1b.T + b1, 0.0))
     H2 = R(np.maximum(H1 @ W2b.T + b2, 0.0))
     H3 = R(np.maximum(H2 @ W3b.T + b3, 0.0))
     Y = H3 @ W4b.T + b4
-    t = (T - norm[32:32 + USED]) / norm[48:48 + USED]
+    t = (T - norm[YM:YM + USED]) / norm[YS:YS + USED]
     e = Y[:, :USED] - t
     loss = float(np.sum(e * e)) / B                     # mean over the batch
     dY = np.zeros((B, DOUT))
@@ -90,9 +91,9 @@ def predict(params, norm, X, rounded=True):
     F = f32 if rounded else (lambda a: np.asarray(a, np.float64))
     W1, b1, W2, b2, W3, b3, W4, b4 = unpack(params)
     norm = np.asarray(norm, np.float64)
-    Xb = R(F((np.asarray(X, np.float64) - norm[:16]) * norm[16:32]))
+    Xb = R(F((np.asarray(X, np.float64) - norm[XM:XM + DIN]) * norm[XI:XI + DIN]))
     H1 = R(np.maximum(Xb @ R(W1).T + b1, 0.0))
     H2 = R(np.maximum(H1 @ R(W2).T + b2, 0.0))
     H3 = R(np.maximum(H2 @ R(W3).T + b3, 0.0))
     Y = H3 @ R(W4).T + b4
-    return Y[:, :USED] * norm[48:48 + USED] + norm[32:32 + USED]
+    return Y[:, :USED] * norm[YS:YS + USED] + norm[YM:YM + USED]

@@ -11,6 +11,9 @@
 //   DAT passes       27_planar_dat.metal:525-561, :752-946, :1179-1310
 //   stamps / dual    40_solver.metal:1088-1153, :1236-1359, :1689-1727
 //   smoothing        40_solver.metal:2150-2180
+//   isotropic OGC    25_cloth.metal:147-267 (isotropic cover), :347-931
+//                    (V-T / E-E trackers, bounds, refresh), topology
+//                    GPUSolver.swift:1338-1460
 //
 // Deterministic where the reference is scheduling-dependent (each choice is
 // one of the orders the reference can produce):
@@ -20,6 +23,10 @@
 //     pair order; the reference takes slots with atomics;
 //   * bends are numbered by ascending edge key; the reference walks a Swift
 //     dictionary whose order is seeded per process;
+//   * isotropic trackers read the tracked sets of the previous frame (own and
+//     neighbours'); the reference reads neighbours' sets while they are
+//     being rewritten; element grid buckets hold elements in index order;
+//     triangle adjacency is filled in ascending edge-key order;
 //   * a body's solve reads the pre-color pose of bodies in its own color
 //     (a Jacobi step inside the color); the reference's reads race with the
 //     writes of same-color neighbours (membrane diagonals, bend stencils,
@@ -311,6 +318,10 @@ int Solver::cloth_upload(const avbd_scene_desc* s, const std::vector<std::array<
     maxSoft = (uint32_t)std::max<uint64_t>(1, 4ull * numTris + budget);
     softMapCapacity = next_pow2(std::max<uint32_t>(64u, 2u * maxSoft));
     elemHashSize = next_pow2(std::max<uint32_t>(64u, 2u * 4u * numTris));
+
+    maxSoftIso = (uint32_t)std::max<uint64_t>(1, 4ull * surfaceParticles + 4ull * numTris + 4ull * numSurfaceEdges);
+    softMapCapacityIso = next_pow2(std::max<uint32_t>(64u, 2u * maxSoftIso));
+    ogc_topology(coll, nbr);
 
     soft.assign(maxSoft, SoftContactGPU{});
     prevSoft.assign(maxSoft, SoftContactGPU{});
@@ -1167,6 +1178,437 @@ void Solver::dual_soft(uint32_t i) {
         pen.z = fmin_(pen.z + P.betaLin * std::fabs(C.z), PENALTY_MAX_T);
     }
     sc.penalty = f4(pen, sc.penalty.w);
+}
+
+}  // namespace oracle
+
+// ==========================================================================
+// Isotropic OGC (25_cloth.metal:147-267 isotropic cover, :347-931)
+// ==========================================================================
+namespace oracle {
+
+static const uint32_t NONE = 0xFFFFFFFFu;
+static const float FBIG = 3.402823466e38f;
+
+struct Best4 {
+    uint32_t id[4] = {NONE, NONE, NONE, NONE};
+    float d2[4] = {FBIG, FBIG, FBIG, FBIG};
+    bool has(uint32_t t) const { return id[0] == t || id[1] == t || id[2] == t || id[3] == t; }
+    void insert(uint32_t t, float d) {
+        if (d >= d2[3]) return;
+        int i = 3;
+        for (; i > 0 && d2[i - 1] > d; i--) { id[i] = id[i - 1]; d2[i] = d2[i - 1]; }
+        id[i] = t;
+        d2[i] = d;
+    }
+};
+static inline uint32_t u4_at(U4 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : (i == 2 ? v.z : v.w)); }
+
+// Tracker topology (GPUSolver.swift:1338-1460): edge-adjacent triangles
+// (edges in ascending key order), incident contact edges per vertex, sorted
+// 1-ring-plus-2-ring sets, cloth-vertex flags.
+void Solver::ogc_topology(const std::vector<std::array<int, 3>>& coll, const std::vector<std::vector<uint32_t>>& ring) {
+    std::map<uint64_t, std::pair<int, int>> et;
+    for (uint32_t ti = 0; ti < numTris; ti++) {
+        const int a = coll[ti][0], b = coll[ti][1], c = coll[ti][2];
+        const int pr[3][2] = {{a, b}, {b, c}, {a, c}};
+        for (auto& e : pr) {
+            uint64_t key = (uint64_t)std::min(e[0], e[1]) << 32 | (uint64_t)std::max(e[0], e[1]);
+            auto it = et.find(key);
+            if (it == et.end()) et.emplace(key, std::make_pair((int)ti, -1));
+            else it->second.second = (int)ti;
+        }
+    }
+    triAdj.assign(std::max<uint32_t>(1, numTris), U4{NONE, NONE, NONE, NONE});
+    std::vector<int> fill(std::max<uint32_t>(1, numTris), 0);
+    auto put = [&](int t, int o) {
+        if (fill[t] >= 3) return;
+        uint32_t* sl = &triAdj[t].x;
+        sl[fill[t]++] = (uint32_t)o;
+    };
+    for (auto& kv : et) {
+        if (kv.second.second < 0) continue;
+        put(kv.second.first, kv.second.second);
+        put(kv.second.second, kv.second.first);
+    }
+    std::vector<std::vector<uint32_t>> ve(nb);
+    for (uint32_t i = 0; i < numEdges; i++) { ve[edges[2 * i]].push_back(i); ve[edges[2 * i + 1]].push_back(i); }
+    vertEdgeStart.assign(nb, 0); vertEdgeCount.assign(nb, 0); vertEdgeList.clear();
+    for (uint32_t i = 0; i < nb; i++) {
+        vertEdgeStart[i] = (uint32_t)vertEdgeList.size();
+        vertEdgeCount[i] = (uint32_t)ve[i].size();
+        vertEdgeList.insert(vertEdgeList.end(), ve[i].begin(), ve[i].end());
+    }
+    nbr2Start.assign(nb, 0); nbr2Count.assign(nb, 0); nbr2List.clear();
+    std::vector<uint32_t> mark(nb, NONE), two;
+    for (uint32_t i = 0; i < nb; i++) {
+        nbr2Start[i] = (uint32_t)nbr2List.size();
+        if (ring[i].empty()) continue;
+        two.clear();
+        mark[i] = i;
+        for (uint32_t n1 : ring[i]) {
+            if (mark[n1] != i) { mark[n1] = i; two.push_back(n1); }
+            for (uint32_t n2 : ring[n1]) if (mark[n2] != i) { mark[n2] = i; two.push_back(n2); }
+        }
+        std::sort(two.begin(), two.end());
+        nbr2Count[i] = (uint32_t)two.size();
+        nbr2List.insert(nbr2List.end(), two.begin(), two.end());
+    }
+    clothVert.assign(nb, 0);
+    for (uint32_t i = 0; i < numAuthoredTris; i++) {
+        clothVert[tris[i].x] = 1; clothVert[tris[i].y] = 1; clothVert[tris[i].z] = 1;
+    }
+    vtTrack.assign(nb, U4{NONE, NONE, NONE, NONE});
+    vtTrackPrev = vtTrack;
+    eeTrack.assign(std::max<uint32_t>(1, numEdges), U4{NONE, NONE, NONE, NONE});
+    eeTrackPrev = eeTrack;
+}
+
+// Element grid, isotropic cover: skin radius + margin padding, at most
+// 3x3x3 cells; triangles and authored contact edges in separate buckets.
+void Solver::ogc_grid() {
+    isoTriCells.assign(elemHashSize, {});
+    isoEdgeCells.assign(elemHashSize, {});
+    const float cs = surfaceCellSize;
+    const uint32_t total = numTris + numSurfaceEdges;
+    for (uint32_t gid = 0; gid < total; gid++) {
+        F3 lo, hi;
+        if (gid < numTris) {
+            U4 t = tris[gid];
+            F3 a = xyz(posLin[t.x]), b = xyz(posLin[t.y]), c = xyz(posLin[t.z]);
+            float pad = fmax_(std::fabs(shape[t.x].w), fmax_(std::fabs(shape[t.y].w), std::fabs(shape[t.z].w))) + elemMargin;
+            lo = vmin3(vmin3(a, b), c) - f3s(pad);
+            hi = vmax3(vmax3(a, b), c) + f3s(pad);
+        } else {
+            uint32_t e = gid - numTris;
+            F3 a = xyz(posLin[edges[2 * e]]), b = xyz(posLin[edges[2 * e + 1]]);
+            float pad = fmax_(std::fabs(shape[edges[2 * e]].w), std::fabs(shape[edges[2 * e + 1]].w)) + elemMargin;
+            lo = vmin3(a, b) - f3s(pad);
+            hi = vmax3(a, b) + f3s(pad);
+        }
+        if (!finite3(lo) || !finite3(hi)) continue;
+        I3 c0 = cell_of(lo, cs), r1 = cell_of(hi, cs);
+        I3 c1{std::min(r1.x, c0.x + 2), std::min(r1.y, c0.y + 2), std::min(r1.z, c0.z + 2)};
+        uint32_t seen[27];
+        uint32_t ns = 0;
+        for (int z = c0.z; z <= c1.z; z++)
+            for (int y = c0.y; y <= c1.y; y++)
+                for (int x = c0.x; x <= c1.x; x++) {
+                    uint32_t h = elem_hash(I3{x, y, z}, elemHashSize);
+                    bool dup = false;
+                    for (uint32_t i = 0; i < ns; i++) dup = dup || seen[i] == h;
+                    if (dup) continue;
+                    seen[ns++] = h;
+                    if (gid < numTris) isoTriCells[h].push_back(gid);
+                    else isoEdgeCells[h].push_back(gid - numTris);
+                }
+    }
+}
+
+static inline void bound_min(std::vector<uint32_t>& b, uint32_t i, uint32_t bits) { if (bits < b[i]) b[i] = bits; }
+
+// vt_emit tracking half (25_cloth.metal:391-529)
+void Solver::ogc_track_vt(uint32_t gid) {
+    const uint32_t v = particleIdx[gid];
+    const F3 pv = xyz(posLin[v]);
+    const F3 velV = xyz(velLin[v]);
+    const uint32_t ns = nbrStart[v], ne = ns + nbrCount[v];
+    const uint32_t gv = clothGroup[v];
+    const bool solidV = gv != 0u && clothVert[v] == 0u;
+    const uint32_t n2s = nbr2Start[v], n2e = n2s + nbr2Count[v];
+    const float cap2 = surfaceCellSize * surfaceCellSize;
+    float ownB2 = FBIG;
+    Best4 best;
+    auto consider = [&](uint32_t t) {
+        if (t >= numTris || best.has(t)) return;
+        U4 tid = tris[t];
+        if (tid.x == v || tid.y == v || tid.z == v) return;
+        if (solidV && clothGroup[tid.x] == gv && clothGroup[tid.y] == gv && clothGroup[tid.z] == gv &&
+            clothVert[tid.x] == 0u && clothVert[tid.y] == 0u && clothVert[tid.z] == 0u)
+            return;
+        F3 bary;
+        F3 q = closest_pt_triangle(pv, xyz(posLin[tid.x]), xyz(posLin[tid.y]), xyz(posLin[tid.z]), bary);
+        F3 dd = pv - q;
+        float d2 = dot(dd, dd);
+        if (d2 < best.d2[3] && !nbr_contains(nbrList, ns, ne, tid.x) && !nbr_contains(nbrList, ns, ne, tid.y) &&
+            !nbr_contains(nbrList, ns, ne, tid.z))
+            best.insert(t, d2);
+        if (d2 < cap2 && !nbr_contains(nbr2List, n2s, n2e, tid.x) && !nbr_contains(nbr2List, n2s, n2e, tid.y) &&
+            !nbr_contains(nbr2List, n2s, n2e, tid.z)) {
+            uint32_t db = fbits(d2);
+            ownB2 = std::fmin(ownB2, d2);
+            bound_min(boundsBits, tid.x, db);
+            bound_min(boundsBits, tid.y, db);
+            bound_min(boundsBits, tid.z, db);
+        }
+    };
+    const U4 tracked = vtTrackPrev[v];
+    for (int i = 0; i < 4; i++) consider(u4_at(tracked, i));
+    if (tracked.x < numTris) {
+        U4 adj = triAdj[tracked.x];
+        for (int i = 0; i < 3; i++) consider(u4_at(adj, i));
+    }
+    for (uint32_t k = ns; k < ne && k < ns + 8; k++) consider(vtTrackPrev[nbrList[k]].x);
+    F3 relV = velV;
+    if (best.id[0] < numTris) {
+        U4 bt = tris[best.id[0]];
+        relV = relV - (xyz(velLin[bt.x]) + xyz(velLin[bt.y]) + xyz(velLin[bt.z])) / 3.0f;
+    }
+    const float vThresh = 0.25f * surfaceCellSize / fmax_(P.dt, 1e-6f);
+    const uint32_t period = dot(relV, relV) > vThresh * vThresh ? 1u : 7u;
+    const bool missing = best.id[0] == NONE;
+    const bool reseed = ((v + P.frame) & period) == 0u || (missing && !solidV) ||
+                        (missing && solidV && ((v + P.frame) & 3u) == 0u);
+    if (reseed) {
+        I3 cc = cell_of(pv, surfaceCellSize);
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    uint32_t h = elem_hash(I3{cc.x + dx, cc.y + dy, cc.z + dz}, elemHashSize);
+                    for (uint32_t t : isoTriCells[h]) consider(t);
+                }
+    }
+    vtTrack[v] = U4{best.id[0], best.id[1], best.id[2], best.id[3]};
+    if (ownB2 < FBIG) bound_min(boundsBits, v, fbits(ownB2));
+}
+
+// vt_emit emission half (25_cloth.metal:531-613)
+bool Solver::vt_contact(uint32_t v, uint32_t t, bool emit) {
+    const F4 plv = posLin[v];
+    const F3 pv = xyz(plv);
+    const float massV = plv.w;
+    const float rv = std::fabs(shape[v].w);
+    const F3 velV = xyz(velLin[v]);
+    const U4 tid = tris[t];
+    const F3 a = xyz(posLin[tid.x]), b = xyz(posLin[tid.y]), c = xyz(posLin[tid.z]);
+    F3 bary;
+    const F3 q = closest_pt_triangle(pv, a, b, c, bary);
+    const F3 dv = pv - q;
+    const float dist2 = dot(dv, dv);
+    const float rt = fmax_(std::fabs(shape[tid.x].w), fmax_(std::fabs(shape[tid.y].w), std::fabs(shape[tid.z].w)));
+    const float hSum = rv + rt;
+    const F3 velT = (xyz(velLin[tid.x]) + xyz(velLin[tid.y]) + xyz(velLin[tid.z])) / 3.0f;
+    const float inflate = fmin_(length(velV - velT) * P.dt, 0.3f * surfaceCellSize);
+    const float detect = hSum + elemMargin + inflate;
+    if (dist2 > detect * detect) return false;
+    const float dist = std::sqrt(dist2);
+    F3 triN = cross(b - a, c - a);
+    const float tnLen = length(triN);
+    if (tnLen < 1e-12f) return false;
+    triN = triN / tnLen;
+    float minMass = massV > 0.0f ? massV : FBIG;
+    const uint32_t others[3] = {tid.x, tid.y, tid.z};
+    for (int k = 0; k < 3; k++) {
+        if (others[k] == WORLD_BODY) continue;
+        float m = posLin[others[k]].w;
+        if (m > 0.0f) minMass = fmin_(minMass, m);
+    }
+    if (minMass == FBIG) return false;
+    if (emit) {
+        const uint32_t keyB = t, keyA = (SC_VT << 28) | v;
+        const float side = dot(dv, triN) >= 0.0f ? 1.0f : -1.0f;
+        const bool deep = bary.x > 0.02f && bary.y > 0.02f && bary.z > 0.02f;
+        const float sMem = deep ? soft_prev_side(keyA, keyB, side) : side;
+        F3 n;
+        float g;
+        if (dist > 1e-7f && side == sMem) { n = dv / dist; g = dist; }
+        else { n = triN * sMem; g = -dist; }
+        const float fricT = props[tid.x].w * bary.x + props[tid.y].w * bary.y + props[tid.z].w * bary.z;
+        const float friction = std::sqrt(fmax_(props[v].w * fricT, 0.0f));
+        soft_emit(U4{v, tid.x, tid.y, tid.z}, f4(1.0f, -bary.x, -bary.y, -bary.z), n, friction, f3s(0),
+                  g - hSum + elemMargin, hSum - elemMargin, soft_lambda_cap(P, minMass), minMass, SC_VT, false, false,
+                  sMem < 0.0f, keyA, keyB);
+    }
+    return true;
+}
+
+// ee_emit tracking half (25_cloth.metal:654-790)
+void Solver::ogc_track_ee(uint32_t gid) {
+    const uint32_t ax = edges[2 * gid], ay = edges[2 * gid + 1];
+    const F3 a0 = xyz(posLin[ax]), a1 = xyz(posLin[ay]);
+    const F3 velA = (xyz(velLin[ax]) + xyz(velLin[ay])) * 0.5f;
+    const uint32_t nsx = nbrStart[ax], nex = nsx + nbrCount[ax];
+    const uint32_t nsy = nbrStart[ay], ney = nsy + nbrCount[ay];
+    const uint32_t gA = clothGroup[ax];
+    const bool solidA = gA != 0u && clothGroup[ay] == gA && clothVert[ax] == 0u && clothVert[ay] == 0u;
+    const uint32_t n2sx = nbr2Start[ax], n2ex = n2sx + nbr2Count[ax];
+    const float cap2 = surfaceCellSize * surfaceCellSize;
+    float ownB2 = FBIG;
+    Best4 best;
+    auto consider = [&](uint32_t e) {
+        if (e >= numSurfaceEdges || e == gid || best.has(e)) return;
+        const uint32_t bx = edges[2 * e], by = edges[2 * e + 1];
+        if (bx == ax || bx == ay || by == ax || by == ay) return;
+        if (solidA && clothGroup[bx] == gA && clothGroup[by] == gA && clothVert[bx] == 0u && clothVert[by] == 0u) return;
+        float s, t;
+        const F3 b0 = xyz(posLin[bx]), b1 = xyz(posLin[by]);
+        closest_seg_seg_st(a0, a1, b0, b1, s, t);
+        const F3 cA = a0 + (a1 - a0) * s;
+        const F3 cB = b0 + (b1 - b0) * t;
+        const F3 dd = cA - cB;
+        const float d2 = dot(dd, dd);
+        if (d2 < best.d2[3] && !nbr_contains(nbrList, nsx, nex, bx) && !nbr_contains(nbrList, nsx, nex, by) &&
+            !nbr_contains(nbrList, nsy, ney, bx) && !nbr_contains(nbrList, nsy, ney, by))
+            best.insert(e, d2);
+        if (d2 < cap2 && !nbr_contains(nbr2List, n2sx, n2ex, bx) && !nbr_contains(nbr2List, n2sx, n2ex, by)) {
+            uint32_t db = fbits(d2);
+            ownB2 = std::fmin(ownB2, d2);
+            bound_min(boundsBits, bx, db);
+            bound_min(boundsBits, by, db);
+        }
+    };
+    const U4 tracked = eeTrackPrev[gid];
+    for (int i = 0; i < 4; i++) consider(u4_at(tracked, i));
+    for (int side = 0; side < 2; side++) {
+        const uint32_t vv = side == 0 ? ax : ay;
+        const uint32_t es = vertEdgeStart[vv], ec = std::min(vertEdgeCount[vv], 6u);
+        for (uint32_t k = es; k < es + ec; k++) consider(eeTrackPrev[vertEdgeList[k]].x);
+    }
+    F3 relV = velA;
+    if (best.id[0] < numSurfaceEdges) {
+        const uint32_t bx = edges[2 * best.id[0]], by = edges[2 * best.id[0] + 1];
+        relV = relV - (xyz(velLin[bx]) + xyz(velLin[by])) * 0.5f;
+    }
+    const float vThresh = 0.25f * surfaceCellSize / fmax_(P.dt, 1e-6f);
+    const uint32_t period = dot(relV, relV) > vThresh * vThresh ? 1u : 7u;
+    const bool missing = best.id[0] == NONE;
+    const bool reseed = ((gid + P.frame) & period) == 0u || (missing && !solidA) ||
+                        (missing && solidA && ((gid + P.frame) & 3u) == 0u);
+    if (reseed) {
+        I3 cc = cell_of((a0 + a1) * 0.5f, surfaceCellSize);
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    uint32_t h = elem_hash(I3{cc.x + dx, cc.y + dy, cc.z + dz}, elemHashSize);
+                    for (uint32_t e : isoEdgeCells[h]) consider(e);
+                }
+    }
+    eeTrack[gid] = U4{best.id[0], best.id[1], best.id[2], best.id[3]};
+    if (ownB2 < FBIG) {
+        bound_min(boundsBits, ax, fbits(ownB2));
+        bound_min(boundsBits, ay, fbits(ownB2));
+    }
+}
+
+// ee_emit emission half (25_cloth.metal:792-854)
+bool Solver::ee_contact(uint32_t gid, uint32_t eBi, bool emit) {
+    const uint32_t ax = edges[2 * gid], ay = edges[2 * gid + 1], bx = edges[2 * eBi], by = edges[2 * eBi + 1];
+    const F3 a0 = xyz(posLin[ax]), a1 = xyz(posLin[ay]);
+    const F3 b0 = xyz(posLin[bx]), b1 = xyz(posLin[by]);
+    float s, t;
+    closest_seg_seg_st(a0, a1, b0, b1, s, t);
+    const float EPS = 0.02f;
+    if (s < EPS || s > 1.0f - EPS || t < EPS || t > 1.0f - EPS) return false;
+    const F3 cA = a0 + (a1 - a0) * s;
+    const F3 cB = b0 + (b1 - b0) * t;
+    const F3 dv = cA - cB;
+    const float dist = length(dv);
+    const float rA = fmax_(std::fabs(shape[ax].w), std::fabs(shape[ay].w));
+    const float rB = fmax_(std::fabs(shape[bx].w), std::fabs(shape[by].w));
+    const float hSum = rA + rB;
+    const F3 velA = (xyz(velLin[ax]) + xyz(velLin[ay])) * 0.5f;
+    const F3 velB = (xyz(velLin[bx]) + xyz(velLin[by])) * 0.5f;
+    const float inflate = fmin_(length(velA - velB) * P.dt, 0.3f * surfaceCellSize);
+    if (dist - hSum > elemMargin + inflate) return false;
+    if (dist < 1e-7f) return false;
+    float minMass = FBIG;
+    const uint32_t ids[4] = {ax, ay, bx, by};
+    for (int j = 0; j < 4; j++) {
+        float m = posLin[ids[j]].w;
+        if (m > 0.0f) minMass = fmin_(minMass, m);
+    }
+    if (minMass == FBIG) return false;
+    if (emit) {
+        const F3 nGeo = dv / dist;
+        const uint32_t keyA = (SC_EE << 28) | gid, keyB = eBi;
+        F3 n = nGeo;
+        float g = dist;
+        int prev = soft_map_find(keyA, keyB);
+        if (prev >= 0 && dot(nGeo, xyz(prevSoft[prev].normal)) < 0.0f) { n = nGeo * -1.0f; g = -dist; }
+        const float fric = std::sqrt(fmax_((props[ax].w + props[ay].w) * 0.5f * (props[bx].w + props[by].w) * 0.5f, 0.0f));
+        soft_emit(U4{ax, ay, bx, by}, f4(1.0f - s, s, -(1.0f - t), -t), n, fric, f3s(0), g - hSum + elemMargin,
+                  hSum - elemMargin, soft_lambda_cap(P, minMass), minMass, SC_EE, false, false, false, keyA, keyB);
+    }
+    return true;
+}
+
+// Detection of one frame: grid, trackers and bounds, rigid-triangle records,
+// then V-T records by particle and E-E records by edge, then the soft map.
+void Solver::ogc_detect() {
+    ogc_grid();
+    for (uint32_t g = 0; g < numParticles; g++) ogc_track_vt(g);
+    for (uint32_t g = 0; g < numSurfaceEdges; g++) ogc_track_ee(g);
+    rt_emit();
+    numSoftRT = softRaw;
+    for (uint32_t g = 0; g < numParticles; g++) {
+        const uint32_t v = particleIdx[g];
+        const U4 best = vtTrack[v];
+        for (int bi = 0; bi < 4; bi++) {
+            const uint32_t t = u4_at(best, bi);
+            if (t >= numTris) break;
+            vt_contact(v, t, true);
+        }
+    }
+    numSoftVT = softRaw - numSoftRT;
+    for (uint32_t g = 0; g < numSurfaceEdges; g++) {
+        const U4 best = eeTrack[g];
+        for (int bi = 0; bi < 4; bi++) {
+            const uint32_t e = u4_at(best, bi);
+            if (e >= numSurfaceEdges) break;
+            if (e <= g) continue;
+            ee_contact(g, e, true);
+        }
+    }
+    numSoftEE = softRaw - numSoftRT - numSoftVT;
+    soft_map_rebuild();
+}
+
+// ogc_bounds_refresh (25_cloth.metal:879-931)
+void Solver::ogc_refresh() {
+    for (uint32_t g = 0; g < numParticles; g++) {
+        const uint32_t v = particleIdx[g];
+        const F3 pv = xyz(posLin[v]);
+        const uint32_t n2s = nbr2Start[v], n2e = n2s + nbr2Count[v];
+        float dmin2 = 3.0e38f;
+        const U4 tracked = vtTrack[v];
+        for (int i = 0; i < 4; i++) {
+            const uint32_t t = u4_at(tracked, i);
+            if (t >= numTris) break;
+            U4 tid = tris[t];
+            if (nbr_contains(nbr2List, n2s, n2e, tid.x) || nbr_contains(nbr2List, n2s, n2e, tid.y) ||
+                nbr_contains(nbr2List, n2s, n2e, tid.z))
+                continue;
+            F3 bary;
+            F3 q = closest_pt_triangle(pv, xyz(posLin[tid.x]), xyz(posLin[tid.y]), xyz(posLin[tid.z]), bary);
+            F3 dd = pv - q;
+            dmin2 = std::fmin(dmin2, dot(dd, dd));
+        }
+        const uint32_t es = vertEdgeStart[v], ec = std::min(vertEdgeCount[v], 6u);
+        for (uint32_t k = es; k < es + ec; k++) {
+            const uint32_t myE = vertEdgeList[k];
+            const uint32_t other = eeTrack[myE].x;
+            if (other >= numSurfaceEdges) continue;
+            const uint32_t ox = edges[2 * other], oy = edges[2 * other + 1];
+            if (nbr_contains(nbr2List, n2s, n2e, ox) || nbr_contains(nbr2List, n2s, n2e, oy)) continue;
+            const F3 a0 = xyz(posLin[edges[2 * myE]]), a1 = xyz(posLin[edges[2 * myE + 1]]);
+            const F3 b0 = xyz(posLin[ox]), b1 = xyz(posLin[oy]);
+            float s, t;
+            closest_seg_seg_st(a0, a1, b0, b1, s, t);
+            const F3 dd = (a0 + (a1 - a0) * s) - (b0 + (b1 - b0) * t);
+            dmin2 = std::fmin(dmin2, dot(dd, dd));
+        }
+        boundsBits[v] = fbits(dmin2);
+        ogcPrev[v] = posLin[v];
+    }
+}
+
+// Color-Jacobi commit of one color
+void Solver::publish_color(uint32_t c) {
+    for (uint32_t i = colorStart[c]; i < colorStart[c + 1]; i++) {
+        const uint32_t v = colorList[i];
+        posLin[v] = f4(xyz(posNext[v]), posLin[v].w);
+        if (shape[v].w >= 0.0f) posAng[v] = angNext[v];
+    }
 }
 
 }  // namespace oracle

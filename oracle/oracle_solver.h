@@ -197,6 +197,15 @@ struct Solver {
     std::vector<uint32_t> softKeyA, softKeyB, softVal;
     std::vector<uint32_t> truncBits;
     std::vector<F4> posNext, angNext;
+    // isotropic OGC (25_cloth.metal:347-931): tracker topology, tracked sets
+    // of this frame and the previous one, the exceeder count of the pass
+    bool ogc = false;
+    uint32_t maxSoftIso = 1, softMapCapacityIso = 64;
+    std::vector<U4> triAdj, vtTrack, vtTrackPrev, eeTrack, eeTrackPrev;
+    std::vector<uint32_t> nbr2Start, nbr2Count, nbr2List, vertEdgeStart, vertEdgeCount, vertEdgeList;
+    std::vector<std::vector<uint32_t>> isoTriCells, isoEdgeCells;   // per bucket, ascending element index
+    uint32_t ogcPass = 0;
+    uint32_t numSoftRT = 0, numSoftVT = 0, numSoftEE = 0;
     struct DatCounters {
         uint32_t pairsPeak, vtPeak, eePeak, gridOverflow, invalidAnchor, truncations,
             vtDegenerate, eeDegenerate, nonfinite, tetDegenerate, softCandidates;
@@ -265,6 +274,16 @@ struct Solver {
     void dat_apply_color(uint32_t c);
     void dat_restore_failed_surface();
     void smooth_particle_velocities();
+    // isotropic OGC stages
+    void ogc_topology(const std::vector<std::array<int, 3>>& coll, const std::vector<std::vector<uint32_t>>& ring);
+    void ogc_grid();
+    void ogc_detect();
+    void ogc_track_vt(uint32_t gid);
+    void ogc_track_ee(uint32_t gid);
+    bool vt_contact(uint32_t v, uint32_t t, bool emit);
+    bool ee_contact(uint32_t gid, uint32_t e, bool emit);
+    void ogc_refresh();
+    void publish_color(uint32_t c);
     void dual_all();
     void dual_joint(uint32_t gid);
     void dual_spring(uint32_t si);

@@ -12,20 +12,19 @@ pytestmark = pytest.mark.gpu
 
 
 def _random_batch(rng, B):
-    X = rng.normal(size=(B, 16)).astype(np.float32)
+    X = rng.normal(size=(B, learned.DIN)).astype(np.float32)
     X[:, 15] = 1.0
     T = rng.normal(size=(B, 3)).astype(np.float32)
     return X, T
 
 
 def _norm(rng):
-    n = np.zeros(64, np.float32)
-    n[:16] = rng.normal(0, 0.1, 16)
-    n[16:32] = rng.uniform(0.5, 2.0, 16)
-    n[32:48] = 0.0
-    n[32:35] = rng.normal(0, 0.1, 3)
-    n[48:64] = 1.0
-    n[48:51] = rng.uniform(0.5, 2.0, 3)
+    n = np.zeros(learned.NNORM, np.float32)
+    n[learned.XM:learned.XM + learned.DIN] = rng.normal(0, 0.1, learned.DIN)
+    n[learned.XI:learned.XI + learned.DIN] = rng.uniform(0.5, 2.0, learned.DIN)
+    n[learned.YM:learned.YM + 3] = rng.normal(0, 0.1, 3)
+    n[learned.YS:learned.NNORM] = 1.0
+    n[learned.YS:learned.YS + 3] = rng.uniform(0.5, 2.0, 3)
     return n
 
 
@@ -67,9 +66,9 @@ def test_zero_correction_model_reproduces_plain_frames(cuda_lib):
     plain one bit for bit."""
     s = demos.soft_cube_scene(seed=3, n=6)
     plain, learn = GPUSolver(s), GPUSolver(s)
-    norm = np.zeros(64, np.float32)
-    norm[16:32] = 1.0
-    norm[48:64] = 1.0
+    norm = np.zeros(learned.NNORM, np.float32)
+    norm[learned.XI:learned.XI + learned.DIN] = 1.0
+    norm[learned.YS:learned.NNORM] = 1.0
     learn.set_warm_start_model(np.zeros(learned.NPARAM, np.float32), norm, 2)
     learn.set_warm_start_mode(abi.WARM_START_LEARNED)
     for f in range(40):
@@ -85,7 +84,7 @@ def test_training_learns_the_correction(cuda_lib):
     """Trained on the solver's own rollouts, the network explains most of the
     variance of the solve's correction of the plain warm start."""
     X, T = learned.collect(lambda seed: demos.soft_cube_scene(seed=seed, n=10), seeds=[1, 2], frames=60)
-    assert X.shape[1] == 16 and T.shape[1] == 3 and X.shape[0] == T.shape[0] > 1000
+    assert X.shape[1] == learned.DIN and T.shape[1] == 3 and X.shape[0] == T.shape[0] > 1000
     m = learned.train(X, T, steps=800, batch=4096, lr=1e-3, log_every=100)
     pred = learned.infer(m.params, m.norm, X)
     explained = 1.0 - ((pred - T) ** 2).mean(axis=0) / T.var(axis=0)

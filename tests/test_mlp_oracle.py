@@ -8,10 +8,10 @@ from oracle import mlp_oracle as M
 def test_oracle_backward_matches_finite_differences():
     rng = np.random.default_rng(0)
     p = rng.normal(0, 0.2, size=M.NPARAM)
-    norm = np.zeros(64)
-    norm[16:32] = 1.0
-    norm[48:64] = 1.0
-    X = rng.normal(size=(7, 16))
+    norm = np.zeros(96)
+    norm[M.XI:M.XI + M.DIN] = 1.0
+    norm[M.YS:96] = 1.0
+    X = rng.normal(size=(7, M.DIN))
     T = rng.normal(size=(7, 3))
     loss, g = M.forward_backward(p, norm, X, T, rounded=False)
     h = 1e-6
