@@ -43,6 +43,8 @@ struct DevPtrs {
     uint4* staticSeg;
     uint32_t *preList, *postList;
     uint32_t *dynCount, *dynStart, *dynCursor, *dynList;
+    uint32_t* dynSplit;                   // manifold entries at the head of each sorted dyn segment
+    uint32_t* postTets;                   // tet entries at the head of each static post segment
     // coloring
     uint32_t *colorsA, *colorsB, *colorList, *bodySlot;
     // control

@@ -460,6 +460,7 @@ struct avbd_solver {
         ok = ok && upload(reinterpret_cast<u4*&>(d.staticSeg), H.staticSeg, "staticSeg");
         ok = ok && upload(d.preList, H.preList, "preList") && upload(d.postList, H.postList, "postList");
         ok = ok && alloc(d.dynCount, nb, "dynCount") && alloc(d.dynStart, nb, "dynStart") && alloc(d.dynCursor, nb, "dynCursor");
+        ok = ok && alloc(d.dynSplit, nb, "dynSplit") && upload(d.postTets, H.postTets, "postTets");
         ok = ok && alloc(d.dynList, 2 * (size_t)H.maxPairs + ((P.cloth || P.ogc) ? 4 * (size_t)P.maxSoft : 0), "dynList");
         // coloring
         ok = ok && upload(d.colorsA, H.colors, "colorsA", true) && upload(d.colorsB, H.colors, "colorsB");
@@ -1140,14 +1141,20 @@ int avbd_debug_read(avbd_solver* s, int which, void* dst, size_t bytes) {
         cudaMemcpy(dc.data(), d.dynCount, 4 * nb, cudaMemcpyDeviceToHost);
         cudaMemcpy(ds.data(), d.dynStart, 4 * nb, cudaMemcpyDeviceToHost);
         cudaMemcpy(dl.data(), d.dynList, 4 * dl.size(), cudaMemcpyDeviceToHost);
+        std::vector<uint32_t> dsp(nb);
+        cudaMemcpy(dsp.data(), d.dynSplit, 4 * nb, cudaMemcpyDeviceToHost);
         std::vector<uint32_t> start(nb), count(nb), list;
         for (size_t b = 0; b < nb; b++) {
+            // pre, manifolds, tets, element contacts, membranes and bends
             const u4 sg = H.staticSeg[b];
+            const uint32_t pt = H.postTets[b];
             start[b] = (uint32_t)list.size();
             count[b] = sg.y + dc[b] + sg.w;
             list.insert(list.end(), H.preList.begin() + sg.x, H.preList.begin() + sg.x + sg.y);
-            list.insert(list.end(), dl.begin() + ds[b], dl.begin() + ds[b] + dc[b]);
-            list.insert(list.end(), H.postList.begin() + sg.z, H.postList.begin() + sg.z + sg.w);
+            list.insert(list.end(), dl.begin() + ds[b], dl.begin() + ds[b] + dsp[b]);
+            list.insert(list.end(), H.postList.begin() + sg.z, H.postList.begin() + sg.z + pt);
+            list.insert(list.end(), dl.begin() + ds[b] + dsp[b], dl.begin() + ds[b] + dc[b]);
+            list.insert(list.end(), H.postList.begin() + sg.z + pt, H.postList.begin() + sg.z + sg.w);
         }
         const std::vector<uint32_t>& v = which == AVBD_BUF_ADJ_START ? start : (which == AVBD_BUF_ADJ_COUNT ? count : list);
         std::memcpy(dst, v.data(), bytes);

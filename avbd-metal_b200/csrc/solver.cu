@@ -231,6 +231,9 @@ __global__ void k_adj_dyn_sort(const DevPtrs d, uint32_t nb) {
         while (j > 0 && l[j - 1] > v) { l[j] = l[j - 1]; j--; }
         l[j] = v;
     }
+    uint32_t m = 0;
+    while (m < n && (l[m] >> ADJ_KIND_SHIFT) == FK_MANIFOLD) m++;
+    d.dynSplit[b] = m;
 }
 
 void launch_adjacency(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
@@ -243,26 +246,31 @@ void launch_adjacency(const Params& P, const DevPtrs& d, const Sizes& z, cudaStr
     k_adj_dyn_sort<<<(P.numBodies + 127) / 128, 128, 0, st>>>(d, P.numBodies);
 }
 
-// Adjacency entry k of a body in ascending order: static pre (joints,
-// springs), this frame's manifolds, static post (tets).
+// The five runs in ascending (kind << 28 | index) order: static pre
+// (joints, springs), this frame's manifolds, static tets, this frame's
+// element contacts, static membranes and bends.
 struct AdjView {
     const uint32_t* pre; uint32_t nPre;
-    const uint32_t* dyn; uint32_t nDyn;
-    const uint32_t* post; uint32_t nPost;
+    const uint32_t* dyn; uint32_t nMan, nDyn;
+    const uint32_t* post; uint32_t nTet, nPost;
     __device__ __forceinline__ uint32_t count() const { return nPre + nDyn + nPost; }
     __device__ __forceinline__ uint32_t at(uint32_t k) const {
         if (k < nPre) return pre[k];
         k -= nPre;
-        if (k < nDyn) return dyn[k];
-        return post[k - nDyn];
+        if (k < nMan) return dyn[k];
+        k -= nMan;
+        if (k < nTet) return post[k];
+        k -= nTet;
+        if (k < nDyn - nMan) return dyn[nMan + k];
+        return post[nTet + k - (nDyn - nMan)];
     }
 };
 __device__ __forceinline__ AdjView adj_view(const DevPtrs& d, uint32_t b) {
     const uint4 s = d.staticSeg[b];
     AdjView v;
     v.pre = d.preList + s.x; v.nPre = s.y;
-    v.dyn = d.dynList + d.dynStart[b]; v.nDyn = d.dynCount[b];
-    v.post = d.postList + s.z; v.nPost = s.w;
+    v.dyn = d.dynList + d.dynStart[b]; v.nDyn = d.dynCount[b]; v.nMan = d.dynSplit[b];
+    v.post = d.postList + s.z; v.nPost = s.w; v.nTet = d.postTets[b];
     return v;
 }
 

@@ -707,9 +707,11 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
         }
     }
     H.staticSeg.assign(nb, u4{});
+    H.postTets.assign(nb, 0);
     for (uint32_t b = 0; b < nb; b++) {
         std::sort(pre[b].begin(), pre[b].end());
         std::sort(post[b].begin(), post[b].end());
+        for (uint32_t e : post[b]) H.postTets[b] += (e >> ADJ_KIND_SHIFT) == FK_TET ? 1u : 0u;
         H.staticSeg[b] = u4{(uint32_t)H.preList.size(), (uint32_t)pre[b].size(),
                             (uint32_t)H.postList.size(), (uint32_t)post[b].size()};
         H.preList.insert(H.preList.end(), pre[b].begin(), pre[b].end());

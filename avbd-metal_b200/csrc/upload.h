@@ -53,6 +53,9 @@ struct HostScene {
     // which is exactly the ascending (kind << 28 | index) order.
     std::vector<uint32_t> preList, postList;
     std::vector<u4> staticSeg;            // preStart, preCount, postStart, postCount
+    // tets (kind 3) at the head of each post segment: element contacts
+    // (kind 4) go between them and the membranes / bends (kinds 5, 6)
+    std::vector<uint32_t> postTets;
 
     // cloth (authored triangles): element topology and elements.  In cloth
     // scenes the post segment holds membranes and bends (kinds 5, 6) and the
