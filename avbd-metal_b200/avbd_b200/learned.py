@@ -218,16 +218,29 @@ def matched_residual_iterations(make_scene: Callable[[int], object], seed: int, 
     return plain_iterations, target, r["rel_residual_final"], r["accepted"] / max(1, r["frames"])
 
 
-def _main(argv=None):
-    """Train the soft-cube warm-start model from the solver's own rollouts:
+def _soft_cube(seed):
+    from . import demos
+    return demos.soft_cube_scene(seed=seed, n=24)
 
-      PYTHONPATH=avbd-metal_b200 python -m avbd_b200.learned --out MODEL.npz
+
+def _mixed(seed):
+    from . import demos
+    return demos.mixed_scene(seed=seed)
+
+
+# scene families with a trained model (avbd_b200/models)
+SCENES = {"soft-cube": _soft_cube, "mixed": _mixed}
+
+
+def _main(argv=None):
+    """Train a warm-start model from the solver's own rollouts:
+
+      PYTHONPATH=avbd-metal_b200 python -m avbd_b200.learned [--scene soft-cube|mixed] --out MODEL.npz
     """
     import argparse
-    from . import demos
     ap = argparse.ArgumentParser(description=_main.__doc__)
     ap.add_argument("--out", required=True)
-    ap.add_argument("--n", type=int, default=24, help="soft-cube lattice size")
+    ap.add_argument("--scene", choices=sorted(SCENES), default="soft-cube")
     ap.add_argument("--seeds", type=int, nargs="+", default=[100, 101, 102, 103])
     ap.add_argument("--frames", type=int, default=200)
     ap.add_argument("--every", type=int, default=2)
@@ -239,7 +252,7 @@ def _main(argv=None):
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval-seed", type=int, default=200)
     a = ap.parse_args(argv)
-    scene = lambda s: demos.soft_cube_scene(seed=s, n=a.n)   # noqa: E731
+    scene = SCENES[a.scene]
 
     def rollout_scene(s):
         sc = scene(s)

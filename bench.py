@@ -14,12 +14,15 @@ metric through the C ABI with host buffers (positions uploaded from pinned
 memory and read back every step).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload soft-cube|cloth-sphere]
+                  [--workload soft-cube|cloth-sphere|mixed|batched-worlds]
 
 `--workload cloth-sphere` measures the cloth configuration instead: a
 256 x 256 sheet of 2 m (65,536 particles, 130,050 StVK membranes, Bergou
 bends, hard structural rods), two pinned corners, draped over a static
 sphere, Planar-DAT truncation, dt = 1/120, 30 iterations.
+`--workload mixed` measures the mixed configuration: 64 soft cubes of 10^3
+vertices, 256 rigid boxes and a 128 x 128 cloth falling together, with
+isotropic-OGC vertex-triangle, edge-edge and rigid-triangle contacts.
 `--workload batched-worlds` measures 4096 independent articulated worlds
 per GPU (body-steps/s; new motor targets every step); under torchrun each
 rank owns its own 4096 worlds (weak scaling, no data-path collective).
@@ -52,6 +55,10 @@ WORKLOADS = {
                      "membranes mu=lambda=1e4, Bergou bending 1e-3, hard structural rods), contact "
                      "radius 2e-3 m, two pinned corners, static sphere r=0.5 m, Planar-DAT, dt=1/120, "
                      "30 iterations, plain warm start"),
+    "mixed": ("mixed-64: 64 soft cubes of 10^3 vertices (Stable Neo-Hookean E=5e4 Pa, nu=0.45, side 0.3 m), "
+              "256 rigid boxes with edges U(0.1, 0.4) m and a 128^2 cloth (mu=lambda=1e4, bending 1e-3) falling "
+              "together onto the ground (80,384 particles + 256 boxes, 233,280 tets, 32,258 triangles), "
+              "isotropic OGC element contacts, dt=1/60, 20 iterations, plain warm start"),
     "batched-worlds": ("batched-worlds-4096: 4096 worlds (one collision group each) of a planar 3-7 link "
                        "hinge chain with implicit PD motors (targets U(+-0.5 rad) every step) and a welded "
                        "T block on a plane, friction 0.5, dt=1/60, 8 iterations, dynamic coloring; "
@@ -81,6 +88,8 @@ def make_scene(rank=0, worlds=4096):
     from avbd_b200 import demos
     if WORKLOAD_KEY == "cloth-sphere":
         return demos.cloth_sphere_scene(seed=3, n=256)
+    if WORKLOAD_KEY == "mixed":
+        return demos.mixed_scene(seed=5)
     if WORKLOAD_KEY == "batched-worlds":
         # rank r owns worlds [r * worlds, (r + 1) * worlds)
         scene, motors, _ = demos.batched_worlds_scene(worlds=worlds, seed=4, first_world=worlds * rank)
@@ -105,10 +114,9 @@ class MotorTargets:
 
 
 def dynamic_vertices(scene):
-    """Units of the metric: dynamic particles (vertex-steps), or dynamic
-    rigid bodies for a rigid-only scene (body-steps)."""
-    n = sum(1 for b in scene.bodies if b.is_particle and b.is_dynamic)
-    return n if n else sum(1 for b in scene.bodies if b.is_dynamic)
+    """Units of the metric: dynamic particles plus dynamic rigid bodies
+    (vertex-steps; body-steps for a rigid-only scene)."""
+    return sum(1 for b in scene.bodies if b.is_dynamic)
 
 
 def unit():
@@ -261,7 +269,12 @@ def primal_bytes_per_iteration(solver, scene):
 
 
 # ---------------------------------------------------------------------------
-MODEL = os.path.join(ROOT, "avbd-metal_b200", "avbd_b200", "models", "soft_cube_24_warm_start.npz")
+MODELS = {"soft-cube": "soft_cube_24_warm_start.npz", "mixed": "mixed_warm_start.npz"}
+
+
+def model_path():
+    name = MODELS.get(WORKLOAD_KEY)
+    return os.path.join(ROOT, "avbd-metal_b200", "avbd_b200", "models", name) if name else None
 
 
 def timed_steps(solver, targets, first, K, stream, flush):
@@ -284,9 +297,9 @@ def learned_comparison(args, world, dev, stream, flush, plain_value):
     """The same workload with the learned warm start, at the iteration count
     whose median AL residual matches the plain warm start's."""
     from avbd_b200 import GPUSolver, abi, demos, learned
-    model = learned.WarmStartModel.load(MODEL)
+    model = learned.WarmStartModel.load(model_path())
     plain_iters = make_scene().settings.iterations
-    make = lambda seed: demos.soft_cube_scene(seed=seed, n=24)   # noqa: E731
+    make = learned.SCENES[WORKLOAD_KEY]
     k, r_plain, r_learned, acc = learned.matched_residual_iterations(make, 200, model, plain_iters, frames=120)
     scene = make_scene()
     scene.settings.iterations = k
@@ -311,8 +324,8 @@ def learned_comparison(args, world, dev, stream, flush, plain_value):
             "value": value, "unit": unit(), "ms_per_step": ms / args.steps,
             "speedup_vs_plain": value / plain_value,
             "accepted_frames": accepted / float(args.warmup + args.steps),
-            "model": "avbd_b200/models/soft_cube_24_warm_start.npz (trained on the GPU by avbd_mlp_train_step "
-                     "from plain rollouts of seeds 100-103)"}
+            "model": f"avbd_b200/models/{MODELS[WORKLOAD_KEY]} (trained on the GPU by avbd_mlp_train_step "
+                     "from plain rollouts of held-out seeds at a higher iteration count)"}
 
 
 def run_ours(args, world, rank, local):
@@ -402,7 +415,7 @@ def run_ours(args, world, rank, local):
         kernels_per_frame = prof["kernels_per_frame"]
 
     learned_line = None
-    if WORKLOAD_KEY == "soft-cube" and os.path.exists(MODEL):
+    if model_path() and os.path.exists(model_path()):
         with torch.cuda.stream(stream):
             learned_line = learned_comparison(args, world, dev, stream, flush, value)
 
