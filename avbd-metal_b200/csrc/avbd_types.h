@@ -112,6 +112,10 @@ struct Params {
     float elemMargin, queryRadius, elemCellSize, surfaceCellSize, clothViscosity;
     // isotropic OGC element contacts (tet surfaces, mixed scenes)
     uint32_t ogc;
+    // particle grid of the broadphase (rigid colliders much larger than the
+    // particles): cell size and hash size
+    uint32_t fineBP, fineHashSize;
+    float fineCellSize;
 };
 
 // Device counters of one frame (the reference's CTR_* layout, trimmed).
@@ -140,6 +144,7 @@ struct Counters {
     // start
     uint32_t ogcSlots[4];
     uint32_t numSoftVT, numSoftEE;   // isotropic element contacts of this frame
+    uint32_t ogcQueue;               // trackers that reseed from the grid this frame
 };
 
 }  // namespace avbd

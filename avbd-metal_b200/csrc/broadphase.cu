@@ -140,23 +140,40 @@ __device__ __forceinline__ float3 collider_center(const DevPtrs& d, uint32_t c) 
     return xyz(d.posLin[b]) + q_rotate(d.posAng[b], xyz(d.colLocalPos[c]));
 }
 
+// Every hashed collider into its bucket (cell hash with its collision group);
+// cellRigid counts the rigid colliders of a bucket.  With the particle grid
+// on (P.fineBP), particle colliders are also binned into fine cells of twice
+// the largest particle radius (hash without group).
 __global__ void k_bp_count(const Params P, const DevPtrs d) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.numHashed) return;
     const uint32_t c = d.hashedIdx[i];
     int x, y, z;
-    cell_coord(collider_center(d, c), P.cellSize, x, y, z);
+    const float3 p = collider_center(d, c);
+    cell_coord(p, P.cellSize, x, y, z);
     const uint32_t h = cell_hash(x, y, z, d.colGroup[c], P.gridHashSize);
     const uint32_t slot = atomicAdd(&d.cellCount[h], 1u);
     d.bodyCellSlot[i] = make_uint2(h, slot);
-    if (d.colShape[c].w >= 0.0f) d.cellRigid[h] = 1u;
+    d.colBucket[c] = h;
+    if (d.colShape[c].w >= 0.0f) {
+        atomicAdd(&d.cellRigid[h], 1u);
+    } else if (P.fineBP) {
+        cell_coord(p, P.fineCellSize, x, y, z);
+        const uint32_t hf = cell_hash(x, y, z, 0u, P.fineHashSize);
+        d.fineSlot[i] = make_uint2(hf, atomicAdd(&d.fineCount[hf], 1u));
+    }
 }
 
 __global__ void k_bp_scatter(const Params P, const DevPtrs d) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.numHashed) return;
     const uint2 cs = d.bodyCellSlot[i];
-    d.cellTmp[d.cellStart[cs.x] + cs.y] = d.hashedIdx[i];
+    const uint32_t c = d.hashedIdx[i];
+    d.cellTmp[d.cellStart[cs.x] + cs.y] = c;
+    if (P.fineBP && d.colShape[c].w < 0.0f) {
+        const uint2 fs = d.fineSlot[i];
+        d.fineTmp[d.fineStart[fs.x] + fs.y] = c;
+    }
 }
 
 static uint32_t stride_blocks_bp(uint32_t threads, int T) {
@@ -169,19 +186,44 @@ static uint32_t stride_blocks_bp(uint32_t threads, int T) {
 // at its rank (the number of smaller ids; ids are distinct).  Dense buckets —
 // a cloth sheet puts hundreds of particles in one cell — cost n^2/32 compares
 // per lane instead of a serial insertion sort.
-__global__ void k_bp_sort_cells(const Params P, const DevPtrs d) {
+__global__ void k_bp_sort_cells(const uint32_t* count, const uint32_t* start, const uint32_t* tmp, uint32_t* out,
+                                uint32_t buckets) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < P.gridHashSize; h += warps) {
-        const uint32_t n = d.cellCount[h];
+    for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < buckets; h += warps) {
+        const uint32_t n = count[h];
         if (n == 0) continue;
-        const uint32_t s = d.cellStart[h];
-        const uint32_t* src = d.cellTmp + s;
+        const uint32_t s = start[h];
+        const uint32_t* src = tmp + s;
         for (uint32_t i = lane; i < n; i += 32) {
             const uint32_t v = src[i];
             uint32_t rank = 0;
             for (uint32_t j = 0; j < n; j++) rank += src[j] < v ? 1u : 0u;
-            d.cellBodies[s + rank] = v;
+            out[s + rank] = v;
+        }
+    }
+}
+
+// The rigid colliders of every bucket, in bucket (collider) order: one warp
+// per bucket compacts the sorted bucket.
+__global__ void k_bp_rigid_compact(const Params P, const DevPtrs d) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < P.gridHashSize; h += warps) {
+        if (d.cellRigid[h] == 0) continue;
+        const uint32_t s = d.cellStart[h], n = d.cellCount[h];
+        uint32_t out = d.rigidStart[h];
+        for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+            const uint32_t k = k0 + lane;
+            uint32_t c = 0;
+            bool rigid = false;
+            if (k < n) {
+                c = d.cellBodies[s + k];
+                rigid = d.colShape[c].w >= 0.0f;
+            }
+            const uint32_t ballot = __ballot_sync(0xffffffffu, rigid);
+            if (rigid) d.rigidCells[out + __popc(ballot & ((1u << lane) - 1u))] = c;
+            out += __popc(ballot);
         }
     }
 }
@@ -224,10 +266,20 @@ __global__ void k_bp_prep(const Params P, const DevPtrs d, uint32_t numColliders
 // lane's is skipped (the reference's visited-bucket check).  Lane counts are
 // prefix-summed, so pairs come out in exactly the serial order: cells in
 // order, each bucket in collider order, then globals.
+//
+// With the particle grid on (P.fineBP: large rigid colliders make the cells
+// far coarser than the particles), a particle producer takes its rigid
+// candidates from the rigid sublists of its buckets and its particle
+// candidates from the 27 fine cells around it, keeps exactly the candidates
+// the bucket scan would accept (bucket in its visit list, the same filters)
+// and sorts them into the serial order: by the visit rank of the candidate's
+// bucket, then by collider index.
 template <bool EMIT>
-__global__ void k_bp_pairs(const Params P, const DevPtrs d, uint32_t producers) {
+__global__ void __launch_bounds__(128) k_bp_pairs(const Params P, const DevPtrs d, uint32_t producers) {
+    __shared__ uint32_t visitH[4][27];
     const uint32_t producer = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = threadIdx.x >> 5;
     if (producer >= producers) return;                     // warp-uniform
     uint32_t count = 0;
     const bool hashedProducer = producer < P.numHashed;
@@ -238,6 +290,44 @@ __global__ void k_bp_pairs(const Params P, const DevPtrs d, uint32_t producers) 
     const float ra = ca.w;
     const uint32_t ownerA = ma.x, groupA = ma.y, sharedA = ma.z & 1u, ga = ma.w;
     const bool aDyn = (ma.z & 2u) != 0;
+    const bool fine = P.fineBP && hashedProducer && d.colShape[a].w < 0.0f;
+    // rigid producers next to the particle grid scan their (large) buckets
+    // with a warp per bucket in k_bp_heavy; here they only total the counts
+    const bool heavy = P.fineBP && hashedProducer && !fine;
+    if (heavy) {
+        if (!EMIT) {
+            const uint32_t c = lane < 28 ? d.pairLaneCount[(size_t)producer * 32 + lane] : 0u;
+            if (lane >= 28) d.pairLaneCount[(size_t)producer * 32 + lane] = 0u;
+            uint32_t total = c;
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+            if (lane == 0) d.pairCount[producer] = total;
+        }
+        return;
+    }
+    // this lane's bucket (NONE when an earlier lane visits the same bucket)
+    uint32_t h = 0xFFFFFFFFu, hf = 0xFFFFFFFFu;
+    if (hashedProducer) {
+        int cx = 0, cy = 0, cz = 0;
+        cell_coord(pa, P.cellSize, cx, cy, cz);
+        const int dz = (int)(lane / 9) - 1, dy = (int)((lane / 3) % 3) - 1, dx = (int)(lane % 3) - 1;
+        const uint32_t hh = cell_hash(cx + dx, cy + dy, cz + dz, groupA, P.gridHashSize);
+        const unsigned same = __match_any_sync(0xffffffffu, lane < 27 ? hh : 0xFFFFFFFFu);
+        if (lane < 27 && (same & ((1u << lane) - 1u)) == 0u) h = hh;
+        if (fine) {
+            cell_coord(pa, P.fineCellSize, cx, cy, cz);
+            const uint32_t hfh = cell_hash(cx + dx, cy + dy, cz + dz, 0u, P.fineHashSize);
+            const unsigned sameF = __match_any_sync(0xffffffffu, lane < 27 ? hfh : 0xFFFFFFFFu);
+            if (lane < 27 && (sameF & ((1u << lane) - 1u)) == 0u) hf = hfh;
+            if (lane < 27) visitH[warp][lane] = h;
+            __syncwarp();
+        }
+    }
+    auto visit_rank = [&](uint32_t hb) -> uint32_t {
+        for (uint32_t s = 0; s < 27; s++)
+            if (visitH[warp][s] == hb) return s;
+        return 0xFFFFFFFFu;
+    };
     // first output slot of this lane: producer start + counts of lower lanes
     uint32_t slot = 0;
     // --- lane work: count (and in EMIT mode write) this lane's candidates
@@ -260,38 +350,56 @@ __global__ void k_bp_pairs(const Params P, const DevPtrs d, uint32_t producers) 
         if (hashedProducer) {
             if (lane < 27) {
                 if (!(ga != 0 && P.numHashedRigid == 0)) {
-                    int cx, cy, cz;
-                    cell_coord(pa, P.cellSize, cx, cy, cz);
-                    const int dz = (int)(lane / 9) - 1, dy = (int)((lane / 3) % 3) - 1, dx = (int)(lane % 3) - 1;
-                    const uint32_t h = cell_hash(cx + dx, cy + dy, cz + dz, groupA, P.gridHashSize);
-                    const unsigned same = __match_any_sync(0x07FFFFFFu, h);
-                    const bool dup = (same & ((1u << lane) - 1u)) != 0u;
-                    if (!dup && !(ga != 0 && d.cellRigid[h] == 0)) {
-                        const uint32_t s0 = d.cellStart[h], e0 = s0 + d.cellCount[h];
-                        for (uint32_t k = s0; k < e0; k++) {
-                            const uint32_t b = d.cellBodies[k];
+                    if (h != 0xFFFFFFFFu && !(ga != 0 && d.cellRigid[h] == 0)) {
+                        // the whole bucket, or only its rigid colliders when
+                        // the particle grid supplies the particles
+                        const uint32_t* list = fine ? d.rigidCells + d.rigidStart[h] : d.cellBodies + d.cellStart[h];
+                        const uint32_t n = fine ? d.cellRigid[h] : d.cellCount[h];
+                        for (uint32_t k = 0; k < n; k++) {
+                            const uint32_t b = list[k];
                             if (b <= a) continue;
                             // soft surface vs soft surface belongs to element contacts
                             if (ga != 0 && d.colMeta[b].w != 0) continue;
                             if (visit(b, a, b, emit)) count++;
                         }
                     }
+                    if (fine && hf != 0xFFFFFFFFu) {
+                        const uint32_t s0 = d.fineStart[hf], e0 = s0 + d.fineCount[hf];
+                        for (uint32_t k = s0; k < e0; k++) {
+                            const uint32_t b = d.fineCells[k];
+                            if (b <= a) continue;
+                            if (ga != 0 && d.colMeta[b].w != 0) continue;
+                            const uint32_t hb = d.colBucket[b];
+                            if (ga != 0 && d.cellRigid[hb] == 0) continue;
+                            if (visit_rank(hb) == 0xFFFFFFFFu) continue;
+                            if (visit(b, a, b, emit)) count++;
+                        }
+                    }
                 }
-            } else if (lane == 27) {
-                for (uint32_t g = 0; g < P.numGlobals; g++) {
-                    const uint32_t b = d.globalIdx[g];
-                    if (ga != 0 && d.colMeta[b].w == ga) continue;
-                    if (visit(b, min(a, b), max(a, b), emit)) count++;
-                }
-            }
-        } else if (lane == 27) {
-            const uint32_t gp = producer - P.numHashed;
-            for (uint32_t g = gp + 1; g < P.numGlobals; g++) {
-                const uint32_t b = d.globalIdx[g];
-                if (ga != 0 && d.colMeta[b].w == ga) continue;
-                if (visit(b, min(a, b), max(a, b), emit)) count++;
             }
         }
+        // the global list, counted for lane 27: the whole warp tests 32
+        // globals at a time and ranks the accepted ones by ballot
+        const uint32_t g0 = hashedProducer ? 0u : producer - P.numHashed + 1u;
+        const uint32_t gslot = __shfl_sync(0xffffffffu, slot, 27);
+        const uint32_t below = (1u << lane) - 1u;
+        uint32_t gcount = 0;
+        for (uint32_t gb = g0; gb < P.numGlobals; gb += 32) {
+            const uint32_t g = gb + lane;
+            uint32_t b = 0;
+            bool pass = false;
+            if (g < P.numGlobals) {
+                b = d.globalIdx[g];
+                if (!(ga != 0 && d.colMeta[b].w == ga)) pass = visit(b, 0u, 0u, false);
+            }
+            const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
+            if (emit && pass) {
+                const uint32_t o = gslot + gcount + __popc(ballot & below);
+                if (o < P.maxPairs) d.pairs[o] = make_uint2(min(a, b), max(a, b));
+            }
+            gcount += __popc(ballot);
+        }
+        if (lane == 27) count = gcount;
     };
     if (!EMIT) {
         run_lane(false);
@@ -310,7 +418,108 @@ __global__ void k_bp_pairs(const Params P, const DevPtrs d, uint32_t producers) 
         }
         slot = d.pairStart[producer] + x - mine;
         run_lane(true);
+        if (fine) {
+            // bucket pairs (lanes 0-26) into the serial order; the global
+            // pairs of lane 27 already follow them in order
+            const uint32_t first = __shfl_sync(0xffffffffu, slot, 0);
+            const uint32_t end = min(__shfl_sync(0xffffffffu, slot, 27), P.maxPairs);
+            __syncwarp();
+            if (lane == 0 && end > first + 1) {
+                auto key = [&](uint2 p) { return (visit_rank(d.colBucket[p.y]) << 24) | p.y; };
+                for (uint32_t i = first + 1; i < end; i++) {
+                    const uint2 v = d.pairs[i];
+                    const uint32_t kv = key(v);
+                    uint32_t j = i;
+                    while (j > first && key(d.pairs[j - 1]) > kv) { d.pairs[j] = d.pairs[j - 1]; j--; }
+                    d.pairs[j] = v;
+                }
+            }
+        }
     }
+}
+
+// One rigid producer's bucket s (s < 27) or its global list (s == 27) with a
+// whole warp: entries in chunks of 32, emitted in order by ballot rank.
+template <bool EMIT>
+__global__ void __launch_bounds__(128) k_bp_heavy(const Params P, const DevPtrs d, const uint32_t* list, uint32_t n) {
+    const uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (w >= n * 28u) return;                               // warp-uniform
+    const uint32_t producer = list[w / 28u], s = w % 28u;
+    const uint32_t a = d.hashedIdx[producer];
+    const float4 ca = d.colCenter[a];
+    const uint4 ma = d.colMeta[a];
+    const float3 pa = xyz(ca);
+    const float ra = ca.w;
+    const uint32_t ownerA = ma.x, groupA = ma.y, sharedA = ma.z & 1u, ga = ma.w;
+    const bool aDyn = (ma.z & 2u) != 0;
+    const uint32_t below = (1u << lane) - 1u;
+    uint32_t slot = 0;
+    if (EMIT) {
+        const uint32_t c = lane < s ? d.pairLaneCount[(size_t)producer * 32 + lane] : 0u;
+        uint32_t x = c;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        slot = d.pairStart[producer] + x;
+    }
+    auto accept = [&](uint32_t b) -> bool {
+        const uint4 mb = d.colMeta[b];
+        if (!domains_compatible(groupA, mb.y, sharedA, mb.z & 1u)) return false;
+        const uint32_t ownerB = mb.x;
+        if (ownerA == ownerB) return false;
+        if (!aDyn && (mb.z & 2u) == 0) return false;
+        const float4 cb = d.colCenter[b];
+        const float3 dp = pa - xyz(cb);
+        const float r = ra + cb.w;
+        if (dot(dp, dp) > r * r) return false;
+        return !pair_excluded(d.exclusions, P.numExclusions, min(ownerA, ownerB), max(ownerA, ownerB));
+    };
+    uint32_t count = 0;
+    if (s < 27) {
+        int cx, cy, cz;
+        cell_coord(pa, P.cellSize, cx, cy, cz);
+        const int dz = (int)(lane / 9) - 1, dy = (int)((lane / 3) % 3) - 1, dx = (int)(lane % 3) - 1;
+        const uint32_t hh = cell_hash(cx + dx, cy + dy, cz + dz, groupA, P.gridHashSize);
+        const unsigned same = __match_any_sync(0xffffffffu, lane < 27 ? hh : 0xFFFFFFFFu);
+        const bool dupMine = lane < 27 && (same & below) != 0u;
+        const uint32_t h = __shfl_sync(0xffffffffu, hh, s);
+        const bool dup = __shfl_sync(0xffffffffu, dupMine ? 1u : 0u, s) != 0u;
+        if (!(ga != 0 && P.numHashedRigid == 0) && !dup && !(ga != 0 && d.cellRigid[h] == 0)) {
+            const uint32_t s0 = d.cellStart[h], nb = d.cellCount[h];
+            for (uint32_t k0 = 0; k0 < nb; k0 += 32) {
+                const uint32_t k = k0 + lane;
+                uint32_t b = 0;
+                bool pass = false;
+                if (k < nb) {
+                    b = d.cellBodies[s0 + k];
+                    pass = b > a && !(ga != 0 && d.colMeta[b].w != 0) && accept(b);
+                }
+                const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
+                if (EMIT && pass) {
+                    const uint32_t o = slot + count + __popc(ballot & below);
+                    if (o < P.maxPairs) d.pairs[o] = make_uint2(a, b);
+                }
+                count += __popc(ballot);
+            }
+        }
+    } else {
+        for (uint32_t g0 = 0; g0 < P.numGlobals; g0 += 32) {
+            const uint32_t g = g0 + lane;
+            uint32_t b = 0;
+            bool pass = false;
+            if (g < P.numGlobals) {
+                b = d.globalIdx[g];
+                pass = !(ga != 0 && d.colMeta[b].w == ga) && accept(b);
+            }
+            const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
+            if (EMIT && pass) {
+                const uint32_t o = slot + count + __popc(ballot & below);
+                if (o < P.maxPairs) d.pairs[o] = make_uint2(min(a, b), max(a, b));
+            }
+            count += __popc(ballot);
+        }
+    }
+    if (!EMIT && lane == 0) d.pairLaneCount[(size_t)producer * 32 + s] = count;
 }
 
 __global__ void k_bp_finalize(const Params P, const DevPtrs d, uint32_t producers) {
@@ -322,19 +531,33 @@ __global__ void k_bp_finalize(const Params P, const DevPtrs d, uint32_t producer
 void launch_broadphase(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     cudaMemsetAsync(d.cellCount, 0, sizeof(uint32_t) * P.gridHashSize, st);
     cudaMemsetAsync(d.cellRigid, 0, sizeof(uint32_t) * P.gridHashSize, st);
+    if (P.fineBP) cudaMemsetAsync(d.fineCount, 0, sizeof(uint32_t) * P.fineHashSize, st);
     const int T = 128;
     if (P.numHashed > 0) {
         k_bp_count<<<(P.numHashed + T - 1) / T, T, 0, st>>>(P, d);
         launch_exclusive_scan(d.cellCount, d.cellStart, P.gridHashSize, d.scanScratch, st);
+        if (P.fineBP) launch_exclusive_scan(d.fineCount, d.fineStart, P.fineHashSize, d.scanScratch, st);
         k_bp_scatter<<<(P.numHashed + T - 1) / T, T, 0, st>>>(P, d);
-        k_bp_sort_cells<<<stride_blocks_bp(P.gridHashSize * 32u, T), T, 0, st>>>(P, d);
+        k_bp_sort_cells<<<stride_blocks_bp(P.gridHashSize * 32u, T), T, 0, st>>>(d.cellCount, d.cellStart, d.cellTmp,
+                                                                                   d.cellBodies, P.gridHashSize);
+        if (P.numHashedRigid > 0) {
+            launch_exclusive_scan(d.cellRigid, d.rigidStart, P.gridHashSize, d.scanScratch, st);
+            k_bp_rigid_compact<<<stride_blocks_bp(P.gridHashSize * 32u, T), T, 0, st>>>(P, d);
+        }
+        if (P.fineBP)
+            k_bp_sort_cells<<<stride_blocks_bp(P.fineHashSize * 32u, T), T, 0, st>>>(d.fineCount, d.fineStart, d.fineTmp,
+                                                                                       d.fineCells, P.fineHashSize);
     }
     if (z.producers > 0) {
         k_bp_prep<<<(z.numColliders + T - 1) / T, T, 0, st>>>(P, d, z.numColliders);
         const uint32_t warpsPerBlock = T / 32;
         const uint32_t blocks = (z.producers + warpsPerBlock - 1) / warpsPerBlock;
+        const uint32_t nh = z.numHeavyProducers;
+        const uint32_t hblocks = (nh * 28u + warpsPerBlock - 1) / warpsPerBlock;
+        if (nh) k_bp_heavy<false><<<hblocks, T, 0, st>>>(P, d, d.heavyProducers, nh);
         k_bp_pairs<false><<<blocks, T, 0, st>>>(P, d, z.producers);
         launch_exclusive_scan(d.pairCount, d.pairStart, z.producers, d.scanScratch, st);
+        if (nh) k_bp_heavy<true><<<hblocks, T, 0, st>>>(P, d, d.heavyProducers, nh);
         k_bp_pairs<true><<<blocks, T, 0, st>>>(P, d, z.producers);
     }
     k_bp_finalize<<<1, 1, 0, st>>>(P, d, z.producers);

@@ -307,8 +307,13 @@ __global__ void k_dat_pair_totals(const Params P, const DevPtrs d, uint32_t owne
 // collider's owner; the grid sweep visits each distinct bucket once.
 // ---------------------------------------------------------------------------
 template <bool EMIT>
-__global__ void k_rt_emit(const Params P, const DevPtrs d) {
-    for (uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x; gid < P.numTris; gid += gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(128) k_rt_emit(const Params P, const DevPtrs d) {
+    // one warp per triangle: lane 0 emits in the serial order; the warp
+    // pre-tests 32 global colliders at a time with the reach test that opens
+    // the body test, so lane 0 visits only globals that can pass it
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t gid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gid < P.numTris; gid += warps) {
         const uint4 tid = d.tris[gid];
         const float3 a = xyz(d.posLin[tid.x]), b = xyz(d.posLin[tid.y]), c = xyz(d.posLin[tid.z]);
         const float3 m = (a + b + c) / 3.0f;
@@ -391,6 +396,18 @@ __global__ void k_rt_emit(const Params P, const DevPtrs d) {
                     emitted++;
                 }
             };
+            auto near_body = [&](uint32_t o) {
+                const float4 sh = d.shape[o];
+                const float3 po = xyz(d.posLin[o]);
+                bool nearO = dist3(po, m) <= rT + fabsf(sh.w) + P.collisionMargin;
+                if (nearO && d.bodyShape[o] == AVBD_SHAPE_BOX) {
+                    const float3 lm = q_rotate(q_conj(d.posAng[o]), m - po);
+                    const float3 dq2 = mx3(abs3(lm) - xyz(sh) * 0.5f, s3(0.0f));
+                    nearO = len3(dq2) <= rT + P.collisionMargin + 0.05f;
+                }
+                return nearO;
+            };
+            if (lane == 0) {
             if (P.numHashedRigid > 0 && P.numHashedRigid <= 8) {
                 for (uint32_t ri = 0; ri < P.numHashed && emitted < RT_MAX_PER_TRI; ri++) {
                     const uint32_t col = d.hashedIdx[ri];
@@ -411,21 +428,36 @@ __global__ void k_rt_emit(const Params P, const DevPtrs d) {
                             for (uint32_t i = 0; i < ns; i++) dup = dup || seen[i] == h;
                             if (dup) continue;
                             seen[ns++] = h;
-                            const uint32_t s0 = d.cellStart[h], e0 = s0 + d.cellCount[h];
+                            // the bucket's rigid colliders, in bucket order
+                            const uint32_t s0 = d.rigidStart[h], e0 = s0 + d.cellRigid[h];
                             for (uint32_t k = s0; k < e0 && emitted < RT_MAX_PER_TRI; k++) {
-                                const uint32_t o = d.colOwner[d.cellBodies[k]];
+                                const uint32_t o = d.colOwner[d.rigidCells[k]];
                                 if (d.shape[o].w < 0.0f) continue;
                                 test_body(o);
                             }
                         }
             }
-            for (uint32_t g = 0; g < P.numGlobals && emitted < RT_MAX_PER_TRI; g++) {
-                const uint32_t o = d.colOwner[d.globalIdx[g]];
-                if (d.shape[o].w < 0.0f) continue;
-                test_body(o);
+            }
+            emitted = __shfl_sync(0xffffffffu, emitted, 0);
+            for (uint32_t gb = 0; gb < P.numGlobals && emitted < RT_MAX_PER_TRI; gb += 32) {
+                const uint32_t g = gb + lane;
+                bool cand = false;
+                if (g < P.numGlobals) {
+                    const uint32_t o = d.colOwner[d.globalIdx[g]];
+                    cand = d.shape[o].w >= 0.0f && near_body(o);
+                }
+                uint32_t ballot = __ballot_sync(0xffffffffu, cand);
+                if (lane == 0) {
+                    while (ballot && emitted < RT_MAX_PER_TRI) {
+                        const uint32_t j = __ffs(ballot) - 1;
+                        ballot &= ballot - 1;
+                        test_body(d.colOwner[d.globalIdx[gb + j]]);
+                    }
+                }
+                emitted = __shfl_sync(0xffffffffu, emitted, 0);
             }
         }
-        if (!EMIT) d.rtCount[gid] = emitted;
+        if (!EMIT && lane == 0) d.rtCount[gid] = emitted;
     }
 }
 
@@ -922,9 +954,9 @@ void build_pairs(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t
 
 void launch_rt_emit(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     if (z.numTris == 0) return;
-    k_rt_emit<false><<<blocks_for(z.numTris, 128), 128, 0, st>>>(P, d);
+    k_rt_emit<false><<<blocks_for(z.numTris * 32u, 128), 128, 0, st>>>(P, d);
     launch_exclusive_scan_large(d.rtCount, d.rtStart, z.numTris, d.bigScanScratch, st);
-    k_rt_emit<true><<<blocks_for(z.numTris, 128), 128, 0, st>>>(P, d);
+    k_rt_emit<true><<<blocks_for(z.numTris * 32u, 128), 128, 0, st>>>(P, d);
     k_rt_totals<<<1, 32, 0, st>>>(P, d);
 }
 

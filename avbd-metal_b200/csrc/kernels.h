@@ -25,6 +25,13 @@ struct DevPtrs {
     // broadphase
     uint32_t *cellCount, *cellStart, *cellBodies, *cellRigid;
     uint32_t* cellTmp;                    // bucket contents before the per-bucket sort
+    uint32_t* colBucket;                  // bucket of every hashed collider this frame
+    uint32_t *rigidStart, *rigidCells;    // rigid colliders of each bucket, in bucket order
+    // particle grid (P.fineBP): particle colliders in cells of twice the
+    // largest particle radius
+    uint32_t *fineCount, *fineStart, *fineTmp, *fineCells;
+    uint2* fineSlot;
+    uint32_t* heavyProducers;             // producer indices of hashed rigid colliders (particle grid on)
     uint2* bodyCellSlot;
     uint32_t *pairCount, *pairStart, *pairLaneCount;
     uint2* pairs;
@@ -93,6 +100,7 @@ struct DevPtrs {
     uint32_t* ogcBounds;
     uint32_t* ogcExceed;                        // one of counters->ogcSlots
     uint32_t* elemCellsTmp;                     // bucket contents before the per-bucket sort
+    float4* ogcPartial;                         // per query owner: tracked set so far, its distances, own bound
     // learned warm start
     uint32_t* learnIdx;                         // dynamic particles the model predicts
     float *learnFeat, *learnPred, *learnTarget; // [n][32], [n][3], [n][3]
@@ -117,6 +125,7 @@ struct Sizes {
     uint32_t maxDatPairs, maxSoft, elemHashSize;
     uint32_t numLearn;
     uint32_t numDynamicRigid;
+    uint32_t numHeavyProducers;
     // static palette on the host (null with dynamic coloring)
     const uint32_t* colorCounts;
     const uint32_t* colorLanes;

@@ -214,11 +214,9 @@ __device__ bool vt_contact(const Params& P, const DevPtrs& d, uint32_t v, uint32
     return true;
 }
 
-__device__ uint32_t vt_track(const Params& P, const DevPtrs& d, uint32_t gid, uint32_t frame) {
-    VtQuery q;
+__device__ void vt_query(const Params& P, const DevPtrs& d, uint32_t gid, VtQuery& q) {
     q.v = d.particleIdx[gid];
     q.pv = xyz(d.posLin[q.v]);
-    const float3 velV = xyz(d.velLin[q.v]);
     q.ns = d.nbrStart[q.v];
     q.ne = q.ns + d.nbrCount[q.v];
     q.gv = d.clothGroup[q.v];
@@ -226,9 +224,13 @@ __device__ uint32_t vt_track(const Params& P, const DevPtrs& d, uint32_t gid, ui
     q.n2s = d.nbr2Start[q.v];
     q.n2e = q.n2s + d.nbr2Count[q.v];
     q.boundsCap2 = P.elemCellSize * P.elemCellSize;
-    float ownB2 = FLT_BIG_;
-    Best4 best;
-    best4_init(best);
+}
+
+// Tracked set, triangle adjacency of the best, neighbours' best; returns
+// whether this vertex reseeds from the grid this frame.
+__device__ bool vt_begin(const Params& P, const DevPtrs& d, const VtQuery& q, uint32_t frame, Best4& best,
+                         float& ownB2) {
+    const float3 velV = xyz(d.velLin[q.v]);
     const uint4 tracked = d.vtTrackPrev[q.v];
     for (int i = 0; i < 4; i++) vt_consider(P, d, q, best, ownB2, u4_at(tracked, i));
     if (tracked.x < P.numTris) {
@@ -246,18 +248,11 @@ __device__ uint32_t vt_track(const Params& P, const DevPtrs& d, uint32_t gid, ui
     const float vThresh = 0.25f * P.elemCellSize / mx(P.dt, 1e-6f);
     const uint32_t period = dot(relV, relV) > vThresh * vThresh ? 1u : 7u;
     const bool missing = best.id[0] == NONE;
-    const bool reseed = ((q.v + frame) & period) == 0u || (missing && !q.solidV) ||
-                        (missing && q.solidV && ((q.v + frame) & 3u) == 0u);
-    if (reseed) {
-        const I3 cc = cell_of(q.pv, P.elemCellSize);
-        for (int dz = -1; dz <= 1; dz++)
-            for (int dy = -1; dy <= 1; dy++)
-                for (int dx = -1; dx <= 1; dx++) {
-                    const uint32_t h = elem_hash(I3{cc.x + dx, cc.y + dy, cc.z + dz}, P.elemHashSize);
-                    const uint32_t s0 = d.elemCellStart[h], e0 = s0 + d.elemCellCount[h];
-                    for (uint32_t k = s0; k < e0; k++) vt_consider(P, d, q, best, ownB2, d.elemCells[k]);
-                }
-    }
+    return ((q.v + frame) & period) == 0u || (missing && !q.solidV) || (missing && q.solidV && ((q.v + frame) & 3u) == 0u);
+}
+
+// Store the tracked set and the vertex's own bound; returns its contact count.
+__device__ uint32_t vt_finish(const Params& P, const DevPtrs& d, const VtQuery& q, const Best4& best, float ownB2) {
     d.vtTrack[q.v] = make_uint4(best.id[0], best.id[1], best.id[2], best.id[3]);
     if (ownB2 < FLT_BIG_) bound_min(d, q.v, __float_as_uint(ownB2));
     uint32_t count = 0;
@@ -358,13 +353,11 @@ __device__ bool ee_contact(const Params& P, const DevPtrs& d, uint32_t gid, uint
     return true;
 }
 
-__device__ uint32_t ee_track(const Params& P, const DevPtrs& d, uint32_t gid, uint32_t frame) {
-    EeQuery q;
+__device__ void ee_query(const Params& P, const DevPtrs& d, uint32_t gid, EeQuery& q) {
     q.gid = gid;
     q.eA = d.edges[gid];
     q.a0 = xyz(d.posLin[q.eA.x]);
     q.a1 = xyz(d.posLin[q.eA.y]);
-    const float3 velA = (xyz(d.velLin[q.eA.x]) + xyz(d.velLin[q.eA.y])) * 0.5f;
     q.nsx = d.nbrStart[q.eA.x];
     q.nex = q.nsx + d.nbrCount[q.eA.x];
     q.nsy = d.nbrStart[q.eA.y];
@@ -374,10 +367,12 @@ __device__ uint32_t ee_track(const Params& P, const DevPtrs& d, uint32_t gid, ui
     q.n2sx = d.nbr2Start[q.eA.x];
     q.n2ex = q.n2sx + d.nbr2Count[q.eA.x];
     q.boundsCap2 = P.elemCellSize * P.elemCellSize;
-    float ownB2 = FLT_BIG_;
-    Best4 best;
-    best4_init(best);
-    const uint4 tracked = d.eeTrackPrev[gid];
+}
+
+__device__ bool ee_begin(const Params& P, const DevPtrs& d, const EeQuery& q, uint32_t frame, Best4& best,
+                         float& ownB2) {
+    const float3 velA = (xyz(d.velLin[q.eA.x]) + xyz(d.velLin[q.eA.y])) * 0.5f;
+    const uint4 tracked = d.eeTrackPrev[q.gid];
     for (int i = 0; i < 4; i++) ee_consider(P, d, q, best, ownB2, u4_at(tracked, i));
     for (int side = 0; side < 2; side++) {
         const uint32_t vv = side == 0 ? q.eA.x : q.eA.y;
@@ -392,19 +387,12 @@ __device__ uint32_t ee_track(const Params& P, const DevPtrs& d, uint32_t gid, ui
     const float vThresh = 0.25f * P.elemCellSize / mx(P.dt, 1e-6f);
     const uint32_t period = dot(relV, relV) > vThresh * vThresh ? 1u : 7u;
     const bool missing = best.id[0] == NONE;
-    const bool reseed = ((gid + frame) & period) == 0u || (missing && !q.solidA) ||
-                        (missing && q.solidA && ((gid + frame) & 3u) == 0u);
-    if (reseed) {
-        const I3 cc = cell_of((q.a0 + q.a1) * 0.5f, P.elemCellSize);
-        for (int dz = -1; dz <= 1; dz++)
-            for (int dy = -1; dy <= 1; dy++)
-                for (int dx = -1; dx <= 1; dx++) {
-                    const uint32_t h = P.elemHashSize + elem_hash(I3{cc.x + dx, cc.y + dy, cc.z + dz}, P.elemHashSize);
-                    const uint32_t s0 = d.elemCellStart[h], e0 = s0 + d.elemCellCount[h];
-                    for (uint32_t k = s0; k < e0; k++) ee_consider(P, d, q, best, ownB2, d.elemCells[k]);
-                }
-    }
-    d.eeTrack[gid] = make_uint4(best.id[0], best.id[1], best.id[2], best.id[3]);
+    return ((q.gid + frame) & period) == 0u || (missing && !q.solidA) ||
+           (missing && q.solidA && ((q.gid + frame) & 3u) == 0u);
+}
+
+__device__ uint32_t ee_finish(const Params& P, const DevPtrs& d, const EeQuery& q, const Best4& best, float ownB2) {
+    d.eeTrack[q.gid] = make_uint4(best.id[0], best.id[1], best.id[2], best.id[3]);
     if (ownB2 < FLT_BIG_) {
         bound_min(d, q.eA.x, __float_as_uint(ownB2));
         bound_min(d, q.eA.y, __float_as_uint(ownB2));
@@ -413,17 +401,223 @@ __device__ uint32_t ee_track(const Params& P, const DevPtrs& d, uint32_t gid, ui
     for (int bi = 0; bi < 4; bi++) {
         const uint32_t e = best.id[bi];
         if (e >= P.numEdges) break;
-        if (e <= gid) continue;
-        if (ee_contact<false>(P, d, gid, e, 0u)) count++;
+        if (e <= q.gid) continue;
+        if (ee_contact<false>(P, d, q.gid, e, 0u)) count++;
     }
     return count;
 }
 
-// Owners [0, numParticles) are V-T queries, the rest E-E queries.
+__device__ __forceinline__ void save_partial(const DevPtrs& d, uint32_t o, const Best4& b, float ownB2) {
+    float4* p = d.ogcPartial + 3 * (size_t)o;
+    p[0] = make_float4(__uint_as_float(b.id[0]), __uint_as_float(b.id[1]), __uint_as_float(b.id[2]),
+                       __uint_as_float(b.id[3]));
+    p[1] = make_float4(b.d2[0], b.d2[1], b.d2[2], b.d2[3]);
+    p[2] = make_float4(ownB2, 0.0f, 0.0f, 0.0f);
+}
+__device__ __forceinline__ void load_partial(const DevPtrs& d, uint32_t o, Best4& b, float& ownB2) {
+    const float4* p = d.ogcPartial + 3 * (size_t)o;
+    const float4 ids = p[0], d2 = p[1];
+    b.id[0] = __float_as_uint(ids.x); b.id[1] = __float_as_uint(ids.y);
+    b.id[2] = __float_as_uint(ids.z); b.id[3] = __float_as_uint(ids.w);
+    b.d2[0] = d2.x; b.d2[1] = d2.y; b.d2[2] = d2.z; b.d2[3] = d2.w;
+    ownB2 = p[2].x;
+}
+
+// Owners [0, numParticles) are V-T queries, the rest E-E queries.  The
+// first pass evaluates the cheap candidates (tracked sets, adjacency,
+// neighbours) and finishes every owner that does not reseed this frame; the
+// reseeding owners (a quarter to an eighth of them) are queued so that the
+// grid scans run without idle lanes.  Each owner's result is independent of
+// the queue order.
 __global__ void k_ogc_track(const Params P, const DevPtrs d, uint32_t owners) {
     const uint32_t frame = d.frameCounter[0];
-    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < owners; o += gridDim.x * blockDim.x)
-        d.datEmit[o] = o < P.numParticles ? vt_track(P, d, o, frame) : ee_track(P, d, o - P.numParticles, frame);
+    for (uint32_t o = blockIdx.x * blockDim.x + threadIdx.x; o < owners; o += gridDim.x * blockDim.x) {
+        Best4 best;
+        best4_init(best);
+        float ownB2 = FLT_BIG_;
+        bool reseed;
+        uint32_t count = 0;
+        if (o < P.numParticles) {
+            VtQuery q;
+            vt_query(P, d, o, q);
+            reseed = vt_begin(P, d, q, frame, best, ownB2);
+            if (!reseed) count = vt_finish(P, d, q, best, ownB2);
+        } else {
+            EeQuery q;
+            ee_query(P, d, o - P.numParticles, q);
+            reseed = ee_begin(P, d, q, frame, best, ownB2);
+            if (!reseed) count = ee_finish(P, d, q, best, ownB2);
+        }
+        if (reseed) {
+            save_partial(d, o, best, ownB2);
+            d.datOwnerCount[atomicAdd(&d.counters->ogcQueue, 1u)] = o;
+        } else {
+            d.datEmit[o] = count;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Grid reseed of the queued owners, one warp per owner.  The serial tracker
+// keeps the four closest distinct candidates by (distance, arrival order):
+// an equal distance never displaces an earlier arrival, and a candidate that
+// is already held is skipped.  So the warp splits the candidate stream
+// (buckets in (dz, dy, dx) order, each bucket in element order) over its
+// lanes, every lane keeps its own four by (distance, arrival) — lane 0
+// starting from the tracked set found before the reseed — and four rounds of
+// a warp-wide minimum pick the result, each winner removed from every lane.
+// Bound contributions are minima and need no order.
+// ---------------------------------------------------------------------------
+struct Best4A {
+    uint32_t id[4], arr[4];
+    float d2[4];
+};
+
+__device__ __forceinline__ void best4a_init(Best4A& b) {
+#pragma unroll
+    for (int i = 0; i < 4; i++) { b.id[i] = NONE; b.arr[i] = NONE; b.d2[i] = FLT_BIG_; }
+}
+// arrivals of one lane increase, so (d2, arrival) order is the serial rule
+__device__ __forceinline__ void best4a_insert(Best4A& b, uint32_t t, float d2, uint32_t arr) {
+    if (b.id[0] == t || b.id[1] == t || b.id[2] == t || b.id[3] == t) return;
+    if (d2 >= b.d2[3]) return;
+    int i = 3;
+    for (; i > 0 && b.d2[i - 1] > d2; i--) { b.id[i] = b.id[i - 1]; b.d2[i] = b.d2[i - 1]; b.arr[i] = b.arr[i - 1]; }
+    b.id[i] = t;
+    b.d2[i] = d2;
+    b.arr[i] = arr;
+}
+
+__device__ void warp_merge(Best4A& loc, Best4& out, uint32_t lane) {
+    for (int r = 0; r < 4; r++) {
+        float d2 = loc.d2[0];
+        uint32_t arr = loc.arr[0], id = loc.id[0];
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) {
+            const float od = __shfl_xor_sync(0xffffffffu, d2, o);
+            const uint32_t oa = __shfl_xor_sync(0xffffffffu, arr, o);
+            const uint32_t oi = __shfl_xor_sync(0xffffffffu, id, o);
+            if (od < d2 || (od == d2 && oa < arr)) { d2 = od; arr = oa; id = oi; }
+        }
+        out.id[r] = id;
+        out.d2[r] = d2;
+        if (id == NONE) continue;
+        // drop the winner from every lane, keeping each list in order
+        int w = 0;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            if (loc.id[i] == id) continue;
+            loc.id[w] = loc.id[i]; loc.d2[w] = loc.d2[i]; loc.arr[w] = loc.arr[i];
+            w++;
+        }
+        for (; w < 4; w++) { loc.id[w] = NONE; loc.d2[w] = FLT_BIG_; loc.arr[w] = NONE; }
+    }
+    (void)lane;
+}
+
+// The serial tracked-set update of vt_consider without the held-set test
+// (duplicates are removed by the merge; their bound contributions repeat).
+__device__ void vt_consider_lane(const Params& P, const DevPtrs& d, const VtQuery& q, Best4A& loc, float& ownB2,
+                                 uint32_t t, uint32_t arr) {
+    if (t >= P.numTris) return;
+    const uint4 tid = d.tris[t];
+    if (tid.x == q.v || tid.y == q.v || tid.z == q.v) return;
+    if (q.solidV && d.clothGroup[tid.x] == q.gv && d.clothGroup[tid.y] == q.gv && d.clothGroup[tid.z] == q.gv &&
+        d.clothVert[tid.x] == 0u && d.clothVert[tid.y] == 0u && d.clothVert[tid.z] == 0u)
+        return;
+    float3 bary;
+    const float3 cp = closest_pt_triangle(q.pv, xyz(d.posLin[tid.x]), xyz(d.posLin[tid.y]), xyz(d.posLin[tid.z]), bary);
+    const float3 dd = q.pv - cp;
+    const float d2 = dot(dd, dd);
+    if (d2 < loc.d2[3] && !nbr_contains(d.nbrList, q.ns, q.ne, tid.x) && !nbr_contains(d.nbrList, q.ns, q.ne, tid.y) &&
+        !nbr_contains(d.nbrList, q.ns, q.ne, tid.z))
+        best4a_insert(loc, t, d2, arr);
+    if (d2 < q.boundsCap2 && !nbr_contains(d.nbr2List, q.n2s, q.n2e, tid.x) &&
+        !nbr_contains(d.nbr2List, q.n2s, q.n2e, tid.y) && !nbr_contains(d.nbr2List, q.n2s, q.n2e, tid.z)) {
+        const uint32_t db = __float_as_uint(d2);
+        ownB2 = fminf(ownB2, d2);
+        bound_min(d, tid.x, db);
+        bound_min(d, tid.y, db);
+        bound_min(d, tid.z, db);
+    }
+}
+
+__device__ void ee_consider_lane(const Params& P, const DevPtrs& d, const EeQuery& q, Best4A& loc, float& ownB2,
+                                 uint32_t e, uint32_t arr) {
+    if (e >= P.numEdges || e == q.gid) return;
+    const uint2 eB = d.edges[e];
+    if (eB.x == q.eA.x || eB.x == q.eA.y || eB.y == q.eA.x || eB.y == q.eA.y) return;
+    if (q.solidA && d.clothGroup[eB.x] == q.gA && d.clothGroup[eB.y] == q.gA && d.clothVert[eB.x] == 0u &&
+        d.clothVert[eB.y] == 0u)
+        return;
+    float s, t;
+    const float3 b0 = xyz(d.posLin[eB.x]), b1 = xyz(d.posLin[eB.y]);
+    closest_seg_seg(q.a0, q.a1, b0, b1, s, t);
+    const float3 cA = q.a0 + (q.a1 - q.a0) * s;
+    const float3 cB = b0 + (b1 - b0) * t;
+    const float3 dd = cA - cB;
+    const float d2 = dot(dd, dd);
+    if (d2 < loc.d2[3] && !nbr_contains(d.nbrList, q.nsx, q.nex, eB.x) &&
+        !nbr_contains(d.nbrList, q.nsx, q.nex, eB.y) && !nbr_contains(d.nbrList, q.nsy, q.ney, eB.x) &&
+        !nbr_contains(d.nbrList, q.nsy, q.ney, eB.y))
+        best4a_insert(loc, e, d2, arr);
+    if (d2 < q.boundsCap2 && !nbr_contains(d.nbr2List, q.n2sx, q.n2ex, eB.x) &&
+        !nbr_contains(d.nbr2List, q.n2sx, q.n2ex, eB.y)) {
+        const uint32_t db = __float_as_uint(d2);
+        ownB2 = fminf(ownB2, d2);
+        bound_min(d, eB.x, db);
+        bound_min(d, eB.y, db);
+    }
+}
+
+__global__ void __launch_bounds__(128) k_ogc_reseed(const Params P, const DevPtrs d) {
+    const uint32_t n = d.counters->ogcQueue;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+        const uint32_t o = d.datOwnerCount[i];
+        Best4 start;
+        float ownB2;
+        load_partial(d, o, start, ownB2);
+        if (lane != 0) ownB2 = FLT_BIG_;
+        Best4A loc;
+        best4a_init(loc);
+        if (lane == 0)
+            for (int k = 0; k < 4; k++) { loc.id[k] = start.id[k]; loc.d2[k] = start.d2[k]; loc.arr[k] = (uint32_t)k; }
+        const bool vt = o < P.numParticles;
+        VtQuery qv;
+        EeQuery qe;
+        I3 cc;
+        uint32_t half = 0;
+        if (vt) {
+            vt_query(P, d, o, qv);
+            cc = cell_of(qv.pv, P.elemCellSize);
+        } else {
+            ee_query(P, d, o - P.numParticles, qe);
+            cc = cell_of((qe.a0 + qe.a1) * 0.5f, P.elemCellSize);
+            half = P.elemHashSize;
+        }
+        // candidate j of the stream arrives as 4 + j; lane l takes j = l mod 32
+        uint32_t base = 0;
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const uint32_t h = half + elem_hash(I3{cc.x + dx, cc.y + dy, cc.z + dz}, P.elemHashSize);
+                    const uint32_t s0 = d.elemCellStart[h], cnt = d.elemCellCount[h];
+                    for (uint32_t k = (lane - base) & 31u; k < cnt; k += 32) {
+                        const uint32_t arr = 4u + base + k;
+                        if (vt) vt_consider_lane(P, d, qv, loc, ownB2, d.elemCells[s0 + k], arr);
+                        else ee_consider_lane(P, d, qe, loc, ownB2, d.elemCells[s0 + k], arr);
+                    }
+                    base += cnt;
+                }
+        Best4 best;
+        warp_merge(loc, best, lane);
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) ownB2 = fminf(ownB2, __shfl_xor_sync(0xffffffffu, ownB2, off));
+        if (lane == 0) d.datEmit[o] = vt ? vt_finish(P, d, qv, best, ownB2) : ee_finish(P, d, qe, best, ownB2);
+        __syncwarp();
+    }
 }
 
 __global__ void k_ogc_emit(const Params P, const DevPtrs d, uint32_t owners) {
@@ -534,7 +728,10 @@ void launch_ogc_detect(const Params& P, const DevPtrs& d, const Sizes& z, cudaSt
     k_ogc_bin<true><<<grid_for(total, 128), 128, 0, st>>>(P, d, total);
     k_ogc_sort_cells<<<grid_for(buckets * 32u, 128), 128, 0, st>>>(d, buckets);
     const uint32_t owners = z.numParticles + P.numEdges;
-    if (owners) k_ogc_track<<<grid_for(owners, 128), 128, 0, st>>>(P, d, owners);
+    if (owners) {
+        k_ogc_track<<<grid_for(owners, 128), 128, 0, st>>>(P, d, owners);
+        k_ogc_reseed<<<grid_for(owners * 32u, 128), 128, 0, st>>>(P, d);
+    }
     launch_rt_emit(P, d, z, st);
     if (owners) {
         launch_exclusive_scan_large(d.datEmit, d.datEmitStart, owners, d.bigScanScratch, st);

@@ -443,6 +443,19 @@ struct avbd_solver {
         ok = ok && alloc(d.cellCount, P.gridHashSize, "cellCount") && alloc(d.cellStart, P.gridHashSize, "cellStart");
         ok = ok && alloc(d.cellRigid, P.gridHashSize, "cellRigid") && alloc(d.cellBodies, P.numHashed, "cellBodies");
         ok = ok && alloc(d.bodyCellSlot, P.numHashed, "bodyCellSlot") && alloc(d.cellTmp, P.numHashed, "cellBodiesUnsorted");
+        ok = ok && alloc(d.colBucket, nc, "colliderBucket") && alloc(d.rigidStart, P.gridHashSize, "rigidStart");
+        ok = ok && alloc(d.rigidCells, P.numHashed, "rigidCells");
+        z.numHeavyProducers = 0;
+        if (P.fineBP) {
+            std::vector<uint32_t> heavy;
+            for (uint32_t i = 0; i < P.numHashed; i++)
+                if (H.colShape[H.hashedIdx[i]].w >= 0.0f) heavy.push_back(i);
+            z.numHeavyProducers = (uint32_t)heavy.size();
+            ok = ok && upload(d.heavyProducers, heavy, "heavyProducers");
+            ok = ok && alloc(d.fineCount, P.fineHashSize, "fineCount") && alloc(d.fineStart, P.fineHashSize, "fineStart");
+            ok = ok && alloc(d.fineTmp, P.numHashed, "fineCellsUnsorted") && alloc(d.fineCells, P.numHashed, "fineCells");
+            ok = ok && alloc(d.fineSlot, P.numHashed, "fineSlot");
+        }
         ok = ok && alloc(d.pairCount, z.producers, "pairCount") && alloc(d.pairStart, z.producers, "pairStart");
         ok = ok && alloc(d.pairLaneCount, (size_t)z.producers * 32, "pairLaneCount");
         ok = ok && alloc(d.pairs, H.maxPairs, "pairs");
@@ -546,6 +559,7 @@ struct avbd_solver {
             ok = ok && upload(reinterpret_cast<u4*&>(d.eeTrack), none, "eeTrack", true) &&
                  upload(reinterpret_cast<u4*&>(d.eeTrackPrev), none, "eeTrackPrev", true);
             ok = ok && alloc(d.ogcBounds, nb, "ogcBounds") && alloc(d.elemCellsTmp, 27 * elems, "elemCellsUnsorted");
+            ok = ok && alloc(d.ogcPartial, 3 * ((size_t)P.numParticles + P.numEdges), "ogcPartialTrack");
         }
         std::vector<uint32_t> spB, rJ;
         std::vector<f4> spA;

@@ -480,11 +480,12 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
         if (collider_radius(c) > threshold || (isolated && c.collision_group == 0)) H.globalIdx.push_back(i);
         else H.hashedIdx.push_back(i);
     }
-    float maxHashedRadius = 0.05f;
-    uint32_t numHashedRigid = 0;
+    float maxHashedRadius = 0.05f, maxParticleRadius = 0.0f;
+    uint32_t numHashedRigid = 0, numHashedParticles = 0;
     for (uint32_t i : H.hashedIdx) {
         maxHashedRadius = fmax_(maxHashedRadius, std::fabs(H.colShape[i].w));
-        if (!s->bodies[s->colliders[i].body].is_particle) numHashedRigid++;
+        if (H.colShape[i].w >= 0.0f) numHashedRigid++;
+        else { numHashedParticles++; maxParticleRadius = fmax_(maxParticleRadius, std::fabs(H.colShape[i].w)); }
     }
 
     // ---- joints (GPUSolver.swift:1092-1195)
@@ -740,6 +741,13 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
     P.numHashed = (uint32_t)H.hashedIdx.size();
     P.numGlobals = (uint32_t)H.globalIdx.size();
     P.numHashedRigid = numHashedRigid;
+    // Particle grid: when the largest hashed collider is far bigger than the
+    // particles, particle candidates come from cells just above twice the
+    // largest particle radius (two overlapping particles always lie in
+    // neighbouring fine cells) instead of the coarse buckets.
+    P.fineCellSize = 2.02f * maxParticleRadius;
+    P.fineBP = (numHashedRigid > 0 && numHashedParticles > 0 && P.cellSize >= 4.0f * P.fineCellSize) ? 1u : 0u;
+    P.fineHashSize = std::min<uint32_t>(next_pow2(std::max<uint32_t>(64u, 2u * numHashedParticles)), 1u << 20);
     P.numTris = H.numTris;
     P.numParticles = H.numTris == 0 ? 0 : H.numParticles;
     P.maxSpeed = fmax_(30.0f, 1.5f * P.cellSize / dt * 0.5f);
