@@ -306,14 +306,16 @@ __global__ void k_dat_pair_totals(const Params P, const DevPtrs d, uint32_t owne
 // triangle, at most four records.  Bodies are reached through their
 // collider's owner; the grid sweep visits each distinct bucket once.
 // ---------------------------------------------------------------------------
-template <bool EMIT>
+// WARP (many global colliders): one warp per triangle, lane 0 emits in the
+// serial order and the warp pre-tests 32 globals at a time with the reach
+// test that opens the body test, so lane 0 visits only globals that can pass
+// it.  Otherwise one thread per triangle.
+template <bool EMIT, bool WARP>
 __global__ void __launch_bounds__(128) k_rt_emit(const Params P, const DevPtrs d) {
-    // one warp per triangle: lane 0 emits in the serial order; the warp
-    // pre-tests 32 global colliders at a time with the reach test that opens
-    // the body test, so lane 0 visits only globals that can pass it
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t gid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gid < P.numTris; gid += warps) {
+    const uint32_t lane = WARP ? (threadIdx.x & 31u) : 0u;
+    const uint32_t step = WARP ? (gridDim.x * blockDim.x) >> 5 : gridDim.x * blockDim.x;
+    const uint32_t first = WARP ? (blockIdx.x * blockDim.x + threadIdx.x) >> 5 : blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint32_t gid = first; gid < P.numTris; gid += step) {
         const uint4 tid = d.tris[gid];
         const float3 a = xyz(d.posLin[tid.x]), b = xyz(d.posLin[tid.y]), c = xyz(d.posLin[tid.z]);
         const float3 m = (a + b + c) / 3.0f;
@@ -438,23 +440,31 @@ __global__ void __launch_bounds__(128) k_rt_emit(const Params P, const DevPtrs d
                         }
             }
             }
-            emitted = __shfl_sync(0xffffffffu, emitted, 0);
-            for (uint32_t gb = 0; gb < P.numGlobals && emitted < RT_MAX_PER_TRI; gb += 32) {
-                const uint32_t g = gb + lane;
-                bool cand = false;
-                if (g < P.numGlobals) {
-                    const uint32_t o = d.colOwner[d.globalIdx[g]];
-                    cand = d.shape[o].w >= 0.0f && near_body(o);
-                }
-                uint32_t ballot = __ballot_sync(0xffffffffu, cand);
-                if (lane == 0) {
-                    while (ballot && emitted < RT_MAX_PER_TRI) {
-                        const uint32_t j = __ffs(ballot) - 1;
-                        ballot &= ballot - 1;
-                        test_body(d.colOwner[d.globalIdx[gb + j]]);
-                    }
-                }
+            if (WARP) {
                 emitted = __shfl_sync(0xffffffffu, emitted, 0);
+                for (uint32_t gb = 0; gb < P.numGlobals && emitted < RT_MAX_PER_TRI; gb += 32) {
+                    const uint32_t g = gb + lane;
+                    bool cand = false;
+                    if (g < P.numGlobals) {
+                        const uint32_t o = d.colOwner[d.globalIdx[g]];
+                        cand = d.shape[o].w >= 0.0f && near_body(o);
+                    }
+                    uint32_t ballot = __ballot_sync(0xffffffffu, cand);
+                    if (lane == 0) {
+                        while (ballot && emitted < RT_MAX_PER_TRI) {
+                            const uint32_t j = __ffs(ballot) - 1;
+                            ballot &= ballot - 1;
+                            test_body(d.colOwner[d.globalIdx[gb + j]]);
+                        }
+                    }
+                    emitted = __shfl_sync(0xffffffffu, emitted, 0);
+                }
+            } else {
+                for (uint32_t g = 0; g < P.numGlobals && emitted < RT_MAX_PER_TRI; g++) {
+                    const uint32_t o = d.colOwner[d.globalIdx[g]];
+                    if (d.shape[o].w < 0.0f) continue;
+                    test_body(o);
+                }
             }
         }
         if (!EMIT && lane == 0) d.rtCount[gid] = emitted;
@@ -954,9 +964,12 @@ void build_pairs(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t
 
 void launch_rt_emit(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     if (z.numTris == 0) return;
-    k_rt_emit<false><<<blocks_for(z.numTris * 32u, 128), 128, 0, st>>>(P, d);
+    const bool warp = P.numGlobals > 32;
+    if (warp) k_rt_emit<false, true><<<blocks_for(z.numTris * 32u, 128), 128, 0, st>>>(P, d);
+    else k_rt_emit<false, false><<<blocks_for(z.numTris, 128), 128, 0, st>>>(P, d);
     launch_exclusive_scan_large(d.rtCount, d.rtStart, z.numTris, d.bigScanScratch, st);
-    k_rt_emit<true><<<blocks_for(z.numTris * 32u, 128), 128, 0, st>>>(P, d);
+    if (warp) k_rt_emit<true, true><<<blocks_for(z.numTris * 32u, 128), 128, 0, st>>>(P, d);
+    else k_rt_emit<true, false><<<blocks_for(z.numTris, 128), 128, 0, st>>>(P, d);
     k_rt_totals<<<1, 32, 0, st>>>(P, d);
 }
 

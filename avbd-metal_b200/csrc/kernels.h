@@ -107,7 +107,12 @@ struct DevPtrs {
     float4 *learnSaveLin, *learnSaveAng;        // the plain warm start
     float4 *learnSweptLin, *learnSweptAng;      // pose buffers of the predicted trial branch
     uint32_t* learnSlot;                        // body -> index in learnIdx (or 0xFFFFFFFF)
+    float4* learnStat;                          // per learned vertex: summed contact normal, contact count
+    float *learnGap, *learnStiff, *learnRingN;  // closest contact gap; static stiffness sum and ring size
+    uint32_t* learnRingStart;                   // 1-ring CSR over learned vertices: (slot, multiplicity)
+    uint2* learnRing;
     float *learnPrm, *learnNorm, *learnResidBodies;
+    float* learnResidBodies2;                   // per-body residual scratch of the predicted branch
     void* learnHalf;                            // BF16 weight mirror
     double* learnResid;                         // [0] plain, [1] predicted, [2] scratch
     double* learnTrace;                         // residual trace of the last frame

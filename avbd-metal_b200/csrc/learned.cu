@@ -22,6 +22,8 @@
 // mirrored as BF16 for the tensor cores.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+
 #include "../../include/avbd.h"
 #include "dmath.cuh"
 #include "kernels.h"
@@ -65,14 +67,40 @@ __device__ __forceinline__ uint32_t ld_pair(const bf16* p) { return *reinterpret
 // between layers (an m16n8 accumulator pair is exactly the next layer's
 // m16k16 operand), weights are read from L1/L2 (72 KB shared by all warps).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(128) k_mlp_infer(const bf16* __restrict__ W, const float* __restrict__ prm,
+// Shared-memory copy of the BF16 weights: rows padded by 8 halves so that the
+// eight rows a fragment load touches fall in distinct banks.
+constexpr int kS1 = mlp::DIN + 8, kSH = mlp::HID + 8;
+constexpr uint32_t kSW1 = 0, kSW2 = kSW1 + mlp::HID * kS1, kSW3 = kSW2 + mlp::HID * kSH, kSW4 = kSW3 + mlp::HID * kSH,
+                   kSWN = kSW4 + mlp::DOUT * kSH;
+constexpr uint32_t kInferWarps = 8;
+constexpr size_t kInferSmem = sizeof(bf16) * kSWN;
+
+// Fused 4-layer inference: every block stages the weights once and its warps
+// take 16-row tiles until the batch is done (m16n8k16 BF16 MMA, FP32
+// accumulation, bias / ReLU / BF16 conversion between layers in registers).
+__global__ void __launch_bounds__(256) k_mlp_infer(const bf16* __restrict__ W, const float* __restrict__ prm,
                                                    const float* __restrict__ norm, const float* __restrict__ X,
                                                    uint32_t n, float* __restrict__ Y) {
     using namespace mlp;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    bf16* sw = reinterpret_cast<bf16*>(smem_raw);
+    // stage the weights: 16-byte chunks, 8 halves each
+    auto stage = [&](uint32_t dst, uint32_t src, int rows, int cols, int stride) {
+        const int chunks = rows * (cols / 8);
+        for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
+            const int r = c / (cols / 8), k = (c % (cols / 8)) * 8;
+            *reinterpret_cast<uint4*>(sw + dst + r * stride + k) = *reinterpret_cast<const uint4*>(W + src + r * cols + k);
+        }
+    };
+    stage(kSW1, HW1, HID, DIN, kS1);
+    stage(kSW2, HW2, HID, HID, kSH);
+    stage(kSW3, HW3, HID, HID, kSH);
+    stage(kSW4, HW4, DOUT, HID, kSH);
+    __syncthreads();
     const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, q = lane & 3u;
-    const uint32_t row0 = warp * 16u;
-    if (row0 >= n) return;
+    const uint32_t tiles = (n + 15) / 16;
+    for (uint32_t tile = blockIdx.x * kInferWarps + (threadIdx.x >> 5); tile < tiles; tile += gridDim.x * kInferWarps) {
+    const uint32_t row0 = tile * 16u;
     const uint32_t r0 = row0 + g, r1 = row0 + g + 8;
     auto xin = [&](uint32_t r, uint32_t c) {
         return r < n ? (X[r * DIN + c] - norm[NX_MEAN + c]) * norm[NX_INV + c] : 0.0f;
@@ -93,12 +121,12 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const bf16* __restrict__ W, c
         acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
 #pragma unroll
         for (int kb = 0; kb < DIN / 16; kb++) {
-            const bf16* w = W + HW1 + (8 * j + g) * DIN + 16 * kb + 2 * q;
+            const bf16* w = sw + kSW1 + (8 * j + g) * kS1 + 16 * kb + 2 * q;
             mma_bf16(acc[j], a[kb][0], a[kb][1], a[kb][2], a[kb][3], ld_pair(w), ld_pair(w + 8));
         }
     }
     const float* bias = prm + OB1;
-    const bf16* Wl = W + HW2;
+    const bf16* Wl = sw + kSW2;
 #pragma unroll 1
     for (int layer = 0; layer < 2; layer++) {
         // epilogue: bias, ReLU, BF16 -> operand of the next layer
@@ -116,12 +144,12 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const bf16* __restrict__ W, c
             acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
 #pragma unroll
             for (int kb = 0; kb < 8; kb++) {
-                const bf16* w = Wl + (8 * j + g) * HID + 16 * kb + 2 * q;
+                const bf16* w = Wl + (8 * j + g) * kSH + 16 * kb + 2 * q;
                 mma_bf16(acc[j], a[kb][0], a[kb][1], a[kb][2], a[kb][3], ld_pair(w), ld_pair(w + 8));
             }
         }
         bias = layer == 0 ? prm + OB2 : prm + OB3;
-        Wl = W + HW3;
+        Wl = sw + kSW3;
     }
 #pragma unroll
     for (int kb = 0; kb < 8; kb++) {
@@ -139,7 +167,7 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const bf16* __restrict__ W, c
         o[j][0] = o[j][1] = o[j][2] = o[j][3] = 0.0f;
 #pragma unroll
         for (int kb = 0; kb < 8; kb++) {
-            const bf16* w = W + HW4 + (8 * j + g) * HID + 16 * kb + 2 * q;
+            const bf16* w = sw + kSW4 + (8 * j + g) * kSH + 16 * kb + 2 * q;
             mma_bf16(o[j], a[kb][0], a[kb][1], a[kb][2], a[kb][3], ld_pair(w), ld_pair(w + 8));
         }
     }
@@ -157,6 +185,7 @@ __global__ void __launch_bounds__(128) k_mlp_infer(const bf16* __restrict__ W, c
                 Y[r * USED_OUT + c] = v * norm[NY_STD + c] + norm[NY_MEAN + c];
             }
         }
+    }
     }
 }
 
@@ -441,16 +470,12 @@ __device__ __forceinline__ float step_scale(const Params& P) { return fmaxf(fabs
 // contact features walk the body's per-frame segment (manifolds, element
 // contacts), the stiffness feature its static segments (springs; tets,
 // membranes, bends).
-__global__ void k_learn_features(const Params P, const DevPtrs d, uint32_t n) {
+// Contact state of every learned vertex: count of contact points, closest
+// gap and summed oriented normal of its manifolds and element contacts.
+__global__ void k_learn_contacts(const Params P, const DevPtrs d, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t v = d.learnIdx[i];
-    const float s = step_scale(P);
-    const float4 pl = d.posLin[v];
-    const float3 x0 = xyz(d.initLin[v]);
-    const float3 fi = (xyz(d.inertLin[v]) - x0) / s;
-    const float3 fp = (xyz(pl) - x0) / s;
-    const float3 fv = xyz(d.prevVelLin[v]) * (P.dt / s);
     float count = 0.0f, gap = 1e30f;
     float3 nsum = s3(0);
     const uint32_t ds = d.dynStart[v], dc = d.dynCount[v];
@@ -475,52 +500,35 @@ __global__ void k_learn_features(const Params P, const DevPtrs d, uint32_t n) {
             gap = fminf(gap, sc.C0.x);
         }
     }
-    float stiff = 0.0f;
-    const uint4 sg = d.staticSeg[v];
-    for (uint32_t k = 0; k < sg.y; k++) {
-        const uint32_t e = d.preList[sg.x + k];
-        if ((e >> ADJ_KIND_SHIFT) == FK_SPRING) stiff += d.springs[e & ADJ_INDEX_MASK].rA.w;
-    }
-    for (uint32_t k = 0; k < sg.w; k++) {
-        const uint32_t e = d.postList[sg.z + k], kind = e >> ADJ_KIND_SHIFT, idx = e & ADJ_INDEX_MASK;
-        if (kind == FK_TET) stiff += d.tets[idx].r1.w + d.tets[idx].r2.w;
-        else if (kind == FK_MEMBRANE) stiff += d.membranes[idx].mat.x + d.membranes[idx].mat.y;
-        else if (kind == FK_BEND) stiff += d.bends[idx].mat.x;
-    }
-    // 1-ring contact state: vertices sharing a tet (post segment) or a
-    // spring (pre segment); their contact count and closest gap
-    float ringN = 0.0f, ringContacts = 0.0f, ringGap = 1e30f;
-    auto visit = [&](uint32_t u) {
-        if (u == v || u == WORLD_BODY) return;
-        ringN += 1.0f;
-        if (d.posLin[u].w <= 0.0f) return;
-        const uint32_t us = d.dynStart[u], uc = d.dynCount[u];
-        for (uint32_t k = 0; k < uc; k++) {
-            const uint32_t e = d.dynList[us + k];
-            const uint32_t kind = e >> ADJ_KIND_SHIFT;
-            if (kind == FK_MANIFOLD) {
-                const ManifoldGPU& m = d.manifolds[e & ADJ_INDEX_MASK];
-                for (uint32_t c = 0; c < m.header.z; c++) {
-                    ringContacts += 1.0f;
-                    ringGap = fminf(ringGap, m.contacts[c].C0.x);
-                }
-            } else if (kind == FK_SOFT) {
-                ringContacts += 1.0f;
-                ringGap = fminf(ringGap, d.soft[e & ADJ_INDEX_MASK].C0.x);
-            }
-        }
-    };
-    for (uint32_t k = 0; k < sg.y; k++) {
-        const uint32_t e = d.preList[sg.x + k];
-        if ((e >> ADJ_KIND_SHIFT) != FK_SPRING) continue;
-        const SpringGPU& sp = d.springs[e & ADJ_INDEX_MASK];
-        visit(sp.header.x == v ? sp.header.y : sp.header.x);
-    }
-    for (uint32_t k = 0; k < sg.w; k++) {
-        const uint32_t e = d.postList[sg.z + k];
-        if ((e >> ADJ_KIND_SHIFT) != FK_TET) continue;
-        const auto t = d.tets[e & ADJ_INDEX_MASK].ids;
-        visit(t.x); visit(t.y); visit(t.z); visit(t.w);
+    d.learnStat[i] = mk4(nsum, count);
+    d.learnGap[i] = gap;
+}
+
+// Features of every learned vertex.  The static parts (incident stiffness,
+// the 1-ring of vertices sharing a tet or spring with its multiplicities)
+// are precomputed at upload; the ring's contact state sums the neighbours'
+// contact counts (times their multiplicity) and takes their closest gap.
+__global__ void k_learn_features(const Params P, const DevPtrs d, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t v = d.learnIdx[i];
+    const float s = step_scale(P);
+    const float4 pl = d.posLin[v];
+    const float3 x0 = xyz(d.initLin[v]);
+    const float3 fi = (xyz(d.inertLin[v]) - x0) / s;
+    const float3 fp = (xyz(pl) - x0) / s;
+    const float3 fv = xyz(d.prevVelLin[v]) * (P.dt / s);
+    const float4 st = d.learnStat[i];
+    const float3 nsum = xyz(st);
+    const float count = st.w, gap = d.learnGap[i];
+    const float stiff = d.learnStiff[i];
+    const float ringN = d.learnRingN[i];
+    float ringContacts = 0.0f, ringGap = 1e30f;
+    const uint32_t r1 = d.learnRingStart[i + 1];
+    for (uint32_t k = d.learnRingStart[i]; k < r1; k++) {
+        const uint2 e = d.learnRing[k];
+        ringContacts += d.learnStat[e.x].w * (float)e.y;
+        ringGap = fminf(ringGap, d.learnGap[e.x]);
     }
     const float inv = ringN > 0.0f ? 1.0f / ringN : 0.0f;
     float* f = d.learnFeat + (size_t)i * mlp::DIN;
@@ -611,7 +619,9 @@ __global__ void k_copy_double(const double* src, double* dst) {
 }  // namespace
 
 void launch_learn_features(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
-    if (z.numLearn) k_learn_features<<<(z.numLearn + 127) / 128, 128, 0, st>>>(P, d, z.numLearn);
+    if (!z.numLearn) return;
+    k_learn_contacts<<<(z.numLearn + 127) / 128, 128, 0, st>>>(P, d, z.numLearn);
+    k_learn_features<<<(z.numLearn + 127) / 128, 128, 0, st>>>(P, d, z.numLearn);
 }
 void launch_learn_apply(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     if (z.numLearn) k_learn_apply<<<(z.numLearn + 127) / 128, 128, 0, st>>>(P, d, z.numLearn);
@@ -633,8 +643,14 @@ void launch_copy_double(const double* src, double* dst, cudaStream_t st) { k_cop
 void launch_mlp_infer(const void* halfW, const float* prm, const float* norm, const float* X, uint32_t n, float* Y,
                       cudaStream_t st) {
     if (n == 0) return;
-    const uint32_t warps = (n + 15) / 16;
-    k_mlp_infer<<<(warps + 3) / 4, 128, 0, st>>>(static_cast<const bf16*>(halfW), prm, norm, X, n, Y);
+    static bool attr = false;     // the weights need more than the default 48 KiB of shared memory
+    if (!attr) {
+        cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInferSmem);
+        attr = true;
+    }
+    const uint32_t tiles = (n + 15) / 16;
+    const uint32_t blocks = std::min<uint32_t>((tiles + kInferWarps - 1) / kInferWarps, 2u * 148u);
+    k_mlp_infer<<<blocks, 32 * kInferWarps, kInferSmem, st>>>(static_cast<const bf16*>(halfW), prm, norm, X, n, Y);
 }
 
 void launch_mlp_mirror(const float* prm, void* halfW, cudaStream_t st) {

@@ -76,6 +76,10 @@ struct avbd_solver {
     int device = 0;
     cudaStream_t stream = nullptr;       // the solver's own stream (graph capture)
     cudaStream_t launch = nullptr;       // where frames run: own or caller's stream
+    // the learned warm start's predicted trial branch runs beside the plain
+    // one on this stream (fork / join by events inside the frame)
+    cudaStream_t branchStream = nullptr;
+    cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
     // per-stage profiling: events at stage boundaries inside the frame graph
     bool profiling = false;
     std::vector<cudaEvent_t> events;
@@ -126,6 +130,9 @@ struct avbd_solver {
         if (stage) cudaFree(stage);
         if (hostLatch) cudaFreeHost(hostLatch);
         if (hostCounters) cudaFreeHost(hostCounters);
+        if (forkEvent) cudaEventDestroy(forkEvent);
+        if (joinEvent) cudaEventDestroy(joinEvent);
+        if (branchStream) cudaStreamDestroy(branchStream);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -237,14 +244,14 @@ struct avbd_solver {
         const uint32_t colorBound = z.dynamicColoring ? colorLaunchBound : H.staticUsedColors;
         // One primal sweep over every color of pose buffers `g` (trial sweeps of
         // the learned warm start; the iteration loop inlines the same sequence).
-        auto sweep = [&](const DevPtrs& g) {
+        auto sweep = [&](const DevPtrs& g, cudaStream_t sst) {
             for (uint32_t c = 0; c < colorBound; c++) {
                 const uint32_t count = z.dynamicColoring ? 0xFFFFFFFFu : H.colorCounts[c];
                 if (count == 0) continue;
-                launch_primal_color(P, g, z, c, count, H.colorLanes[c], st);
-                if (P.ogc) launch_publish_color(P, g, c, count, st);
+                launch_primal_color(P, g, z, c, count, H.colorLanes[c], sst);
+                if (P.ogc) launch_publish_color(P, g, c, count, sst);
             }
-            if (z.dynamicColoring) launch_primal_tail(P, g, z, colorLaunchBound, st);
+            if (z.dynamicColoring) launch_primal_tail(P, g, z, colorLaunchBound, sst);
         };
         const bool tuningFrame = primalEvents != nullptr;
         const bool learned = !tuningFrame && learnMode == AVBD_WARM_START_LEARNED && modelSet && z.numLearn;
@@ -276,10 +283,23 @@ struct avbd_solver {
             launch_mlp_infer(f.learnHalf, f.learnPrm, f.learnNorm, f.learnFeat, z.numLearn, f.learnPred, st);
             launch_learn_branch(P, f, z, st);
             if (trace) launch_residual(P, fb, z, f.learnResidBodies, f.learnTrace + 1, st);
-            for (uint32_t t = 0; t < learnTrials; t++) sweep(fp);
+            // The two trial branches touch disjoint pose buffers, so the
+            // predicted one runs on a second stream beside the plain one
+            // (color-Jacobi scenes share posNext and run them in turn).
+            const bool fork = !P.colorJacobi;
+            cudaStream_t bst = fork ? branchStream : st;
+            if (fork) {
+                cudaEventRecord(forkEvent, st);
+                cudaStreamWaitEvent(bst, forkEvent, 0);
+            }
+            for (uint32_t t = 0; t < learnTrials; t++) sweep(fb, bst);
+            launch_residual(P, fb, z, f.learnResidBodies2, f.learnResid + 1, bst);
+            for (uint32_t t = 0; t < learnTrials; t++) sweep(fp, st);
             launch_residual(P, f, z, f.learnResidBodies, f.learnResid + 0, st);
-            for (uint32_t t = 0; t < learnTrials; t++) sweep(fb);
-            launch_residual(P, fb, z, f.learnResidBodies, f.learnResid + 1, st);
+            if (fork) {
+                cudaEventRecord(joinEvent, bst);
+                cudaStreamWaitEvent(st, joinEvent, 0);
+            }
             if (reuseTrial) {
                 launch_learn_adopt(P, f, z, st);
             } else {
@@ -381,7 +401,13 @@ struct avbd_solver {
         device = s->device >= 0 ? s->device : 0;
         if (s->device < 0) cudaGetDevice(&device);
         if (device >= count || cudaSetDevice(device) != cudaSuccess) { error = "cannot select CUDA device"; return AVBD_ERR_NO_DEVICE; }
-        if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess) { error = "stream creation failed"; return AVBD_ERR_NO_DEVICE; }
+        if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaStreamCreateWithFlags(&branchStream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&joinEvent, cudaEventDisableTiming) != cudaSuccess) {
+            error = "stream creation failed";
+            return AVBD_ERR_NO_DEVICE;
+        }
         launch = stream;
         settings = s->settings;
         P = H.P;
@@ -497,6 +523,50 @@ struct avbd_solver {
             std::vector<uint32_t> slot(nb, 0xFFFFFFFFu);
             for (uint32_t i = 0; i < nl; i++) slot[H.learnIdx[i]] = i;
             ok = ok && upload(d.learnSlot, slot, "learnSlot");
+            // static feature parts: incident stiffness (springs, then tets /
+            // membranes / bends, in adjacency order) and the 1-ring of
+            // vertices sharing a spring or tet, with multiplicities
+            std::vector<float> stiff(nl, 0.0f), ringN(nl, 0.0f);
+            std::vector<uint32_t> ringStart(nl + 1, 0);
+            std::vector<uint2> ring;
+            for (uint32_t i = 0; i < nl; i++) {
+                const uint32_t v = H.learnIdx[i];
+                const u4 sg = H.staticSeg[v];
+                float k = 0.0f;
+                std::vector<std::pair<uint32_t, uint32_t>> nbr;   // (slot, multiplicity) in first-visit order
+                auto visit = [&](uint32_t u) {
+                    if (u == v || u == WORLD_BODY) return;
+                    ringN[i] += 1.0f;
+                    if (!(H.posLin[u].w > 0.0f) || slot[u] == 0xFFFFFFFFu) return;
+                    for (auto& e : nbr) if (e.first == slot[u]) { e.second++; return; }
+                    nbr.push_back({slot[u], 1u});
+                };
+                for (uint32_t q = 0; q < sg.y; q++) {
+                    const uint32_t e = H.preList[sg.x + q];
+                    if ((e >> ADJ_KIND_SHIFT) != FK_SPRING) continue;
+                    const SpringGPU& sp = H.springs[e & ADJ_INDEX_MASK];
+                    k += sp.rA.w;
+                    visit(sp.header.x == v ? sp.header.y : sp.header.x);
+                }
+                for (uint32_t q = 0; q < sg.w; q++) {
+                    const uint32_t e = H.postList[sg.z + q], kind = e >> ADJ_KIND_SHIFT, idx = e & ADJ_INDEX_MASK;
+                    if (kind == FK_TET) {
+                        k += H.tets[idx].r1.w + H.tets[idx].r2.w;
+                        visit(H.tets[idx].ids.x); visit(H.tets[idx].ids.y);
+                        visit(H.tets[idx].ids.z); visit(H.tets[idx].ids.w);
+                    } else if (kind == FK_MEMBRANE) {
+                        k += H.membranes[idx].mat.x + H.membranes[idx].mat.y;
+                    } else if (kind == FK_BEND) {
+                        k += H.bends[idx].mat.x;
+                    }
+                }
+                stiff[i] = k;
+                for (auto& e : nbr) ring.push_back(make_uint2(e.first, e.second));
+                ringStart[i + 1] = (uint32_t)ring.size();
+            }
+            ok = ok && upload(d.learnStiff, stiff, "learnStiffness") && upload(d.learnRingN, ringN, "learnRingSize");
+            ok = ok && upload(d.learnRingStart, ringStart, "learnRingStart") && upload(d.learnRing, ring, "learnRing");
+            ok = ok && alloc(d.learnStat, nl, "learnContactState") && alloc(d.learnGap, nl, "learnContactGap");
             ok = ok && alloc(d.learnFeat, 32 * (size_t)nl, "learnFeatures") && alloc(d.learnPred, 3 * (size_t)nl, "learnPrediction");
             ok = ok && alloc(d.learnTarget, 3 * (size_t)nl, "learnTarget");
             ok = ok && alloc(d.learnPrm, mlp_param_count(), "mlpParams") && alloc(d.learnNorm, mlp_norm_count(), "mlpNorm");
@@ -507,6 +577,7 @@ struct avbd_solver {
         ok = ok && alloc(d.learnSaveLin, nb, "plainWarmStartLin") && alloc(d.learnSaveAng, nb, "plainWarmStartAng");
         ok = ok && alloc(d.learnSweptLin, nb, "plainTrialLin") && alloc(d.learnSweptAng, nb, "plainTrialAng");
         ok = ok && alloc(d.learnResidBodies, std::max<uint32_t>(1, H.numDynamicBodies), "residualBodies");
+        ok = ok && alloc(d.learnResidBodies2, std::max<uint32_t>(1, H.numDynamicBodies), "residualBodiesBranch");
         ok = ok && alloc(d.learnResid, 4, "residual") && alloc(d.learnTrace, kTraceLength, "residualTrace");
         ok = ok && alloc(d.learnAccepted, 1, "learnAccepted", true);
         if (H.numTris > 0) {

@@ -225,11 +225,30 @@ __global__ void k_adj_dyn_sort(const DevPtrs d, uint32_t nb) {
     if (b >= nb) return;
     uint32_t* l = d.dynList + d.dynStart[b];
     const uint32_t n = d.dynCount[b];
-    for (uint32_t i = 1; i < n; i++) {
-        const uint32_t v = l[i];
-        uint32_t j = i;
-        while (j > 0 && l[j - 1] > v) { l[j] = l[j - 1]; j--; }
-        l[j] = v;
+    if (n <= 32) {
+        for (uint32_t i = 1; i < n; i++) {
+            const uint32_t v = l[i];
+            uint32_t j = i;
+            while (j > 0 && l[j - 1] > v) { l[j] = l[j - 1]; j--; }
+            l[j] = v;
+        }
+    } else {
+        // heapsort: bodies under a pile (a box on a cloth) carry hundreds of
+        // entries; the entries are distinct, so the order is unique
+        auto sift = [&](uint32_t root, uint32_t end) {
+            while (2 * root + 1 < end) {
+                uint32_t c = 2 * root + 1;
+                if (c + 1 < end && l[c] < l[c + 1]) c++;
+                if (l[root] >= l[c]) return;
+                const uint32_t t = l[root]; l[root] = l[c]; l[c] = t;
+                root = c;
+            }
+        };
+        for (uint32_t i = n / 2; i-- > 0;) sift(i, n);
+        for (uint32_t end = n - 1; end > 0; end--) {
+            const uint32_t t = l[0]; l[0] = l[end]; l[end] = t;
+            sift(0, end);
+        }
     }
     uint32_t m = 0;
     while (m < n && (l[m] >> ADJ_KIND_SHIFT) == FK_MANIFOLD) m++;
@@ -907,18 +926,25 @@ __global__ void k_residual_bodies(const Params P, const DevPtrs d, uint32_t n, f
     out[slot] = r2;
 }
 
-// Fixed-order sum of n values in one block (double accumulation).
+// Fixed-order sum of n values in one block (double accumulation): thread t
+// sums a contiguous run, a warp shuffle tree and a second tree over the
+// warps combine them, always in the same order.
 __global__ void __launch_bounds__(1024) k_sum_fixed(const float* v, uint32_t n, double* out) {
-    __shared__ double part[1024];
+    __shared__ double part[32];
+    const uint32_t t = threadIdx.x, per = (n + blockDim.x - 1) / blockDim.x;
     double s = 0.0;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) s += (double)v[i];
-    part[threadIdx.x] = s;
+    const uint32_t b0 = t * per, b1 = min(n, b0 + per);
+    for (uint32_t i = b0; i < b1; i++) s += (double)v[i];
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if ((t & 31u) == 0) part[t >> 5] = s;
     __syncthreads();
-    for (uint32_t w = blockDim.x >> 1; w > 0; w >>= 1) {
-        if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
-        __syncthreads();
+    if (t < 32) {
+        s = t < (blockDim.x >> 5) ? part[t] : 0.0;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (t == 0) *out = s;
     }
-    if (threadIdx.x == 0) *out = part[0];
 }
 
 
@@ -1334,19 +1360,22 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
 void launch_residual(const Params& P, const DevPtrs& d, const Sizes& z, float* perBody, double* total,
                      cudaStream_t st) {
     const uint32_t n = z.numDynamicBodies;
-    if (n && z.numDynamicRigid == 0 && perBody == d.learnResidBodies) {
-        // particle-only: the group stamping of the primal over all colors at once
+    if (n && z.numDynamicRigid == 0) {
+        // particle-only: the group stamping of the primal over all colors at
+        // once, writing the per-body values to perBody
+        DevPtrs g = d;
+        g.learnResidBodies = perBody;
         auto run = [&](uint32_t color, uint32_t count, uint32_t lanes) {
             const uint32_t w = lanes <= 8 ? 8u : (lanes <= 16 ? 16u : 32u);
             const uint32_t blocks = (count * w + 127) / 128;
             if (z.particleFastPath) {
-                if (w == 8) k_primal_group<8, false, false, true><<<blocks, 128, 0, st>>>(P, d, color, count);
-                else if (w == 16) k_primal_group<16, false, false, true><<<blocks, 128, 0, st>>>(P, d, color, count);
-                else k_primal_group<32, false, false, true><<<blocks, 128, 0, st>>>(P, d, color, count);
+                if (w == 8) k_primal_group<8, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count);
+                else if (w == 16) k_primal_group<16, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count);
+                else k_primal_group<32, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count);
             } else if (P.cloth || P.ogc) {
-                k_primal_group<32, true, true, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, d, color, count);
+                k_primal_group<32, true, true, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, g, color, count);
             } else {
-                k_primal_group<32, true, false, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, d, color, count);
+                k_primal_group<32, true, false, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, g, color, count);
             }
         };
         run(0u, n, 32u);

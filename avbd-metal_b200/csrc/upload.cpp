@@ -741,12 +741,14 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
     P.numHashed = (uint32_t)H.hashedIdx.size();
     P.numGlobals = (uint32_t)H.globalIdx.size();
     P.numHashedRigid = numHashedRigid;
-    // Particle grid: when the largest hashed collider is far bigger than the
-    // particles, particle candidates come from cells just above twice the
-    // largest particle radius (two overlapping particles always lie in
-    // neighbouring fine cells) instead of the coarse buckets.
+    // Particle grid: when the coarse cells (twice the largest hashed radius,
+    // at least 0.1 m) are well above the particles, particle candidates come
+    // from cells just above twice the largest particle radius (two
+    // overlapping particles always lie in neighbouring fine cells) instead of
+    // the coarse buckets; the pair kernel keeps exactly the candidates the
+    // coarse scan accepts.
     P.fineCellSize = 2.02f * maxParticleRadius;
-    P.fineBP = (numHashedRigid > 0 && numHashedParticles > 0 && P.cellSize >= 4.0f * P.fineCellSize) ? 1u : 0u;
+    P.fineBP = (numHashedParticles > 0 && P.fineCellSize > 0.0f && P.cellSize >= 2.0f * P.fineCellSize) ? 1u : 0u;
     P.fineHashSize = std::min<uint32_t>(next_pow2(std::max<uint32_t>(64u, 2u * numHashedParticles)), 1u << 20);
     P.numTris = H.numTris;
     P.numParticles = H.numTris == 0 ? 0 : H.numParticles;

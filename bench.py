@@ -78,6 +78,12 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="bound on the CPU baseline sample")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="soft-cube")
+    ap.add_argument("--frames-only", action="store_true",
+                    help="profiling runs: warm-up and timed frames of the workload only (no e2e, stage "
+                         "profile, learned comparison or CPU baseline); prints ms per frame")
+    ap.add_argument("--warm-start", choices=["plain", "learned"], default="plain",
+                    help="with --frames-only: the warm start of the frames")
+    ap.add_argument("--iterations", type=int, default=0, help="with --frames-only: override the iterations")
     args = ap.parse_args()
     global WORKLOAD_KEY, WORKLOAD
     WORKLOAD_KEY, WORKLOAD = args.workload, WORKLOADS[args.workload]
@@ -328,6 +334,37 @@ def learned_comparison(args, world, dev, stream, flush, plain_value):
                      "from plain rollouts of held-out seeds at a higher iteration count)"}
 
 
+def run_frames(args, local):
+    """Warm-up and timed frames only: the command the committed ncu launch
+    lists were taken with."""
+    import torch
+    from avbd_b200 import GPUSolver, abi, learned
+    torch.cuda.set_device(local)
+    scene = make_scene()
+    if args.iterations:
+        scene.settings.iterations = args.iterations
+    solver = GPUSolver(scene, device=local)
+    if args.warm_start == "learned":
+        model = learned.WarmStartModel.load(model_path())
+        solver.set_warm_start_model(model.params, model.norm, 1)
+        solver.set_warm_start_mode(abi.WARM_START_LEARNED)
+    targets = MotorTargets(args.warmup + args.steps)
+    for i in range(args.warmup):
+        targets.apply(solver, i)
+        solver.step(1)
+    solver.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        targets.apply(solver, args.warmup + i)
+        solver.step(1)
+    solver.synchronize()
+    print(json.dumps({"workload": WORKLOAD_KEY, "frames": args.steps, "warm_start": args.warm_start,
+                      "iterations": scene.settings.iterations,
+                      "wall_ms_per_frame": (time.perf_counter() - t0) / max(1, args.steps) * 1e3,
+                      "runtime_failure": solver.runtime_failure()}), flush=True)
+    solver.close()
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -507,6 +544,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.frames_only:
+            run_frames(args, local)
         else:
             run_ours(args, world, rank, local)
     finally:
