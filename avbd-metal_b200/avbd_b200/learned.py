@@ -67,10 +67,12 @@ class WarmStartModel:
 
 
 def collect(make_scene: Callable[[int], object], seeds: Sequence[int], frames: int, skip: int = 2,
-            every: int = 1, motor_targets: Optional[Callable] = None):
+            every: int = 1, motor_targets: Optional[Callable] = None, fraction: float = 1.0):
     """Roll out the plain solver on seeded scene variants and record, per
-    frame, the features and the solve's correction of the plain warm start."""
+    frame, the features and the solve's correction of the plain warm start
+    (of a seeded random `fraction` of the vertices, for large scenes)."""
     feats, targs = [], []
+    rng = np.random.default_rng(12345)
     for seed in seeds:
         scene = make_scene(seed)
         g = GPUSolver(scene)
@@ -79,6 +81,9 @@ def collect(make_scene: Callable[[int], object], seeds: Sequence[int], frames: i
             g.step(1)
             if f >= skip and (f - skip) % every == 0:
                 x, t = g.learning_sample()
+                if fraction < 1.0:
+                    keep = rng.random(len(x)) < fraction
+                    x, t = x[keep], t[keep]
                 feats.append(x.copy())
                 targs.append(t.copy())
         g.close()
@@ -244,6 +249,7 @@ def _main(argv=None):
     ap.add_argument("--seeds", type=int, nargs="+", default=[100, 101, 102, 103])
     ap.add_argument("--frames", type=int, default=200)
     ap.add_argument("--every", type=int, default=2)
+    ap.add_argument("--fraction", type=float, default=1.0, help="share of the vertices sampled per frame")
     ap.add_argument("--target-iterations", type=int, default=80,
                     help="iterations of the rollouts that give the targets (a more converged solve than the "
                          "iteration counts the model is used at)")
@@ -259,7 +265,7 @@ def _main(argv=None):
         sc.settings.iterations = a.target_iterations
         return sc
 
-    X, T = collect(rollout_scene, a.seeds, a.frames, every=a.every)
+    X, T = collect(rollout_scene, a.seeds, a.frames, every=a.every, fraction=a.fraction)
     model = train(X, T, steps=a.steps, batch=a.batch, lr=a.lr)
     model.save(a.out)
     print(f"samples {len(X)}, loss {model.history[0]:.4f} -> {model.history[-1]:.4f}")
