@@ -145,6 +145,7 @@ struct Counters {
     uint32_t ogcSlots[4];
     uint32_t numSoftVT, numSoftEE;   // isotropic element contacts of this frame
     uint32_t ogcQueue;               // trackers that reseed from the grid this frame
+    uint32_t adjLong;                // bodies whose contact segment is sorted by a block
 };
 
 }  // namespace avbd

@@ -260,6 +260,51 @@ __global__ void k_bp_prep(const Params P, const DevPtrs d, uint32_t numColliders
                               d.clothGroup[owner]);
 }
 
+// Boxes of every chunk of 32 global colliders: collider spheres (pair
+// kernels) and owner bounding spheres (rigid-triangle emission).  A chunk
+// that a query ball misses cannot hold a candidate, so the global scans skip
+// it; the candidates they keep, and their order, are unchanged.
+__global__ void k_global_chunks(const Params P, const DevPtrs d) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t chunk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t g = chunk * 32u + lane;
+    if (chunk * 32u >= P.numGlobals) return;                // warp-uniform
+    const float big = 3.0e38f;
+    float3 clo = s3(big), chi = s3(-big), blo = s3(big), bhi = s3(-big);
+    if (g < P.numGlobals) {
+        const uint32_t c = d.globalIdx[g];
+        const float4 cc = d.colCenter[c];
+        clo = xyz(cc) - s3(cc.w);
+        chi = xyz(cc) + s3(cc.w);
+        const uint32_t o = d.colOwner[c];
+        const float3 po = xyz(d.posLin[o]);
+        const float rb = fabsf(d.shape[o].w);
+        blo = po - s3(rb);
+        bhi = po + s3(rb);
+        // a non-finite member makes the chunk unbounded (never skipped)
+        if (!(finite3(clo) && finite3(chi))) { clo = s3(-big); chi = s3(big); }
+        if (!(finite3(blo) && finite3(bhi))) { blo = s3(-big); bhi = s3(big); }
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        clo = mk3(fminf(clo.x, __shfl_xor_sync(0xffffffffu, clo.x, off)), fminf(clo.y, __shfl_xor_sync(0xffffffffu, clo.y, off)),
+                  fminf(clo.z, __shfl_xor_sync(0xffffffffu, clo.z, off)));
+        chi = mk3(fmaxf(chi.x, __shfl_xor_sync(0xffffffffu, chi.x, off)), fmaxf(chi.y, __shfl_xor_sync(0xffffffffu, chi.y, off)),
+                  fmaxf(chi.z, __shfl_xor_sync(0xffffffffu, chi.z, off)));
+        blo = mk3(fminf(blo.x, __shfl_xor_sync(0xffffffffu, blo.x, off)), fminf(blo.y, __shfl_xor_sync(0xffffffffu, blo.y, off)),
+                  fminf(blo.z, __shfl_xor_sync(0xffffffffu, blo.z, off)));
+        bhi = mk3(fmaxf(bhi.x, __shfl_xor_sync(0xffffffffu, bhi.x, off)), fmaxf(bhi.y, __shfl_xor_sync(0xffffffffu, bhi.y, off)),
+                  fmaxf(bhi.z, __shfl_xor_sync(0xffffffffu, bhi.z, off)));
+    }
+    if (lane == 0) {
+        float4* out = d.globalChunk + 4 * (size_t)chunk;
+        out[0] = mk4(clo, 0.0f);
+        out[1] = mk4(chi, 0.0f);
+        out[2] = mk4(blo, 0.0f);
+        out[3] = mk4(bhi, 0.0f);
+    }
+}
+
 // Candidate pairs of one producer collider (20_broadphase.metal:287-424),
 // one warp per producer: lane s < 27 scans neighbour cell s in (dz, dy, dx)
 // order, lane 27 scans the global list.  A cell whose hash equals an earlier
@@ -384,11 +429,15 @@ __global__ void __launch_bounds__(128) k_bp_pairs(const Params P, const DevPtrs 
         const uint32_t gslot = __shfl_sync(0xffffffffu, slot, 27);
         const uint32_t below = (1u << lane) - 1u;
         uint32_t gcount = 0;
-        for (uint32_t gb = g0; gb < P.numGlobals; gb += 32) {
+        for (uint32_t gb = g0 & ~31u; gb < P.numGlobals; gb += 32) {
+            if (P.numGlobals > 32) {
+                const float4* box = d.globalChunk + 4 * (size_t)(gb >> 5);
+                if (ball_misses_box(pa, ra, box[0], box[1])) continue;
+            }
             const uint32_t g = gb + lane;
             uint32_t b = 0;
             bool pass = false;
-            if (g < P.numGlobals) {
+            if (g >= g0 && g < P.numGlobals) {
                 b = d.globalIdx[g];
                 if (!(ga != 0 && d.colMeta[b].w == ga)) pass = visit(b, 0u, 0u, false);
             }
@@ -504,6 +553,10 @@ __global__ void __launch_bounds__(128) k_bp_heavy(const Params P, const DevPtrs 
         }
     } else {
         for (uint32_t g0 = 0; g0 < P.numGlobals; g0 += 32) {
+            if (P.numGlobals > 32) {
+                const float4* box = d.globalChunk + 4 * (size_t)(g0 >> 5);
+                if (ball_misses_box(pa, ra, box[0], box[1])) continue;
+            }
             const uint32_t g = g0 + lane;
             uint32_t b = 0;
             bool pass = false;
@@ -550,6 +603,10 @@ void launch_broadphase(const Params& P, const DevPtrs& d, const Sizes& z, cudaSt
     }
     if (z.producers > 0) {
         k_bp_prep<<<(z.numColliders + T - 1) / T, T, 0, st>>>(P, d, z.numColliders);
+        if (P.numGlobals > 32) {
+            const uint32_t chunks = (P.numGlobals + 31) / 32;
+            k_global_chunks<<<(chunks + 3) / 4, 128, 0, st>>>(P, d);
+        }
         const uint32_t warpsPerBlock = T / 32;
         const uint32_t blocks = (z.producers + warpsPerBlock - 1) / warpsPerBlock;
         const uint32_t nh = z.numHeavyProducers;

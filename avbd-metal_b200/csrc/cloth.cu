@@ -342,10 +342,18 @@ __global__ void __launch_bounds__(128) k_rt_emit(const Params P, const DevPtrs d
                     nearO = len3(dq2) <= rT + P.collisionMargin + 0.05f;
                 }
                 if (!nearO) return;
-                if (pair_excluded(d, P.numExclusions, min(o, tid.x), max(o, tid.x)) ||
-                    pair_excluded(d, P.numExclusions, min(o, tid.y), max(o, tid.y)) ||
-                    pair_excluded(d, P.numExclusions, min(o, tid.z), max(o, tid.z)))
-                    return;
+                // excluded pairs emit nothing: the test runs before the first
+                // record it would prevent (cheaper than before the features)
+                int excluded = -1;
+                auto is_excluded = [&]() {
+                    if (excluded < 0)
+                        excluded = (pair_excluded(d, P.numExclusions, min(o, tid.x), max(o, tid.x)) ||
+                                    pair_excluded(d, P.numExclusions, min(o, tid.y), max(o, tid.y)) ||
+                                    pair_excluded(d, P.numExclusions, min(o, tid.z), max(o, tid.z)))
+                                       ? 1
+                                       : 0;
+                    return excluded == 1;
+                };
                 float3 fw[4];
                 float fr[4];
                 uint32_t fid[4];
@@ -375,6 +383,7 @@ __global__ void __launch_bounds__(128) k_rt_emit(const Params P, const DevPtrs d
                     if (mB > 0.0f) minMass = mn(minMass, mB);
                     if (mC > 0.0f) minMass = mn(minMass, mC);
                     if (minMass == FLT_BIG_) continue;
+                    if (is_excluded()) return;
                     if (EMIT) {
                         const float side = dot(dv, triN) >= 0.0f ? 1.0f : -1.0f;
                         const uint32_t keyA = (SC_RT << 28) | o;
@@ -443,6 +452,9 @@ __global__ void __launch_bounds__(128) k_rt_emit(const Params P, const DevPtrs d
             if (WARP) {
                 emitted = __shfl_sync(0xffffffffu, emitted, 0);
                 for (uint32_t gb = 0; gb < P.numGlobals && emitted < RT_MAX_PER_TRI; gb += 32) {
+                    // a chunk whose bodies all lie beyond the reach test is skipped
+                    const float4* box = d.globalChunk + 4 * (size_t)(gb >> 5);
+                    if (ball_misses_box(m, rT + P.collisionMargin, box[2], box[3])) continue;
                     const uint32_t g = gb + lane;
                     bool cand = false;
                     if (g < P.numGlobals) {

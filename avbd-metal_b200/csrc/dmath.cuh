@@ -243,4 +243,15 @@ __device__ __forceinline__ uint32_t pair_map_hash(uint32_t a, uint32_t b, uint32
     return h & (cap - 1u);
 }
 
+// Conservative test that a ball (p, reach) misses the box [lo, hi]: true
+// only when it lies farther than reach plus a rounding allowance.
+__device__ __forceinline__ bool ball_misses_box(float3 p, float reach, float4 lo, float4 hi) {
+    const float dx = fmaxf(fmaxf(lo.x - p.x, p.x - hi.x), 0.0f);
+    const float dy = fmaxf(fmaxf(lo.y - p.y, p.y - hi.y), 0.0f);
+    const float dz = fmaxf(fmaxf(lo.z - p.z, p.z - hi.z), 0.0f);
+    const float scale = fmaxf(fmaxf(fabsf(p.x), fabsf(p.y)), fmaxf(fabsf(p.z), reach));
+    const float r = reach * 1.0001f + scale * 1.0e-5f + 1.0e-6f;
+    return dx * dx + dy * dy + dz * dz > r * r;
+}
+
 }  // namespace avbd

@@ -32,6 +32,10 @@ struct DevPtrs {
     uint32_t *fineCount, *fineStart, *fineTmp, *fineCells;
     uint2* fineSlot;
     uint32_t* heavyProducers;             // producer indices of hashed rigid colliders (particle grid on)
+    // per chunk of 32 consecutive global colliders (more than 32 globals):
+    // box of their collider spheres (lo, hi) and of their bodies' bounding
+    // spheres (lo, hi), this frame
+    float4* globalChunk;
     uint2* bodyCellSlot;
     uint32_t *pairCount, *pairStart, *pairLaneCount;
     uint2* pairs;
@@ -51,6 +55,7 @@ struct DevPtrs {
     uint32_t *preList, *postList;
     uint32_t *dynCount, *dynStart, *dynCursor, *dynList;
     uint32_t* dynSplit;                   // manifold entries at the head of each sorted dyn segment
+    uint32_t* adjLongQueue;               // bodies with long contact segments this frame
     uint32_t* postTets;                   // tet entries at the head of each static post segment
     // coloring
     uint32_t *colorsA, *colorsB, *colorList, *bodySlot;

@@ -486,6 +486,7 @@ struct avbd_solver {
         ok = ok && alloc(d.pairLaneCount, (size_t)z.producers * 32, "pairLaneCount");
         ok = ok && alloc(d.pairs, H.maxPairs, "pairs");
         ok = ok && alloc(d.colCenter, nc, "colliderCenter") && alloc(d.colMeta, nc, "colliderMeta");
+        ok = ok && alloc(d.globalChunk, 4 * (size_t)std::max<uint32_t>(1, (P.numGlobals + 31) / 32), "globalChunkBoxes");
         ok = ok && alloc(d.manifolds, H.maxPairs, "manifolds", true) && alloc(d.prevManifolds, H.maxPairs, "prevManifolds", true);
         ok = ok && alloc(d.mapKeyA, H.mapCapacity, "mapKeyA", true) && alloc(d.mapKeyB, H.mapCapacity, "mapKeyB", true);
         ok = ok && alloc(d.mapVal, H.mapCapacity, "mapVal", true);
@@ -500,6 +501,7 @@ struct avbd_solver {
         ok = ok && upload(d.preList, H.preList, "preList") && upload(d.postList, H.postList, "postList");
         ok = ok && alloc(d.dynCount, nb, "dynCount") && alloc(d.dynStart, nb, "dynStart") && alloc(d.dynCursor, nb, "dynCursor");
         ok = ok && alloc(d.dynSplit, nb, "dynSplit") && upload(d.postTets, H.postTets, "postTets");
+        ok = ok && alloc(d.adjLongQueue, nb, "adjLongQueue");
         ok = ok && alloc(d.dynList, 2 * (size_t)H.maxPairs + ((P.cloth || P.ogc) ? 4 * (size_t)P.maxSoft : 0), "dynList");
         // coloring
         ok = ok && upload(d.colorsA, H.colors, "colorsA", true) && upload(d.colorsB, H.colors, "colorsB");

@@ -220,6 +220,8 @@ __global__ void k_adj_dyn(const Params P, const DevPtrs d) {
         }
     }
 }
+constexpr uint32_t kLongSegment = 2048;   // entries a block sorts in shared memory
+
 __global__ void k_adj_dyn_sort(const DevPtrs d, uint32_t nb) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
@@ -232,6 +234,11 @@ __global__ void k_adj_dyn_sort(const DevPtrs d, uint32_t nb) {
             while (j > 0 && l[j - 1] > v) { l[j] = l[j - 1]; j--; }
             l[j] = v;
         }
+    } else if (n <= kLongSegment) {
+        // left to k_adj_long_sort (one block per segment)
+        d.dynSplit[b] = 0xFFFFFFFFu;
+        d.adjLongQueue[atomicAdd(&d.counters->adjLong, 1u)] = b;
+        return;
     } else {
         // heapsort: bodies under a pile (a box on a cloth) carry hundreds of
         // entries; the entries are distinct, so the order is unique
@@ -255,6 +262,51 @@ __global__ void k_adj_dyn_sort(const DevPtrs d, uint32_t nb) {
     d.dynSplit[b] = m;
 }
 
+// Segments of 33..2048 entries: one block loads the segment into shared
+// memory, sorts it with a bitonic network (padded with 0xFFFFFFFF), writes
+// it back and marks the manifold run.  Entries are distinct, so the result
+// equals the serial sort.
+__global__ void __launch_bounds__(256) k_adj_long_sort(const DevPtrs d) {
+    __shared__ uint32_t buf[kLongSegment];
+    const uint32_t count = d.counters->adjLong;
+    for (uint32_t q = blockIdx.x; q < count; q += gridDim.x) {
+        const uint32_t b = d.adjLongQueue[q];
+        uint32_t* l = d.dynList + d.dynStart[b];
+        const uint32_t n = d.dynCount[b];
+        uint32_t m = 64;
+        while (m < n) m <<= 1;
+        for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) buf[i] = i < n ? l[i] : 0xFFFFFFFFu;
+        __syncthreads();
+        for (uint32_t k = 2; k <= m; k <<= 1)
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t i = threadIdx.x; i < m; i += blockDim.x) {
+                    const uint32_t p = i ^ j;
+                    if (p > i) {
+                        const uint32_t x = buf[i], y = buf[p];
+                        const bool up = (i & k) == 0;
+                        if ((x > y) == up) { buf[i] = y; buf[p] = x; }
+                    }
+                }
+                __syncthreads();
+            }
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) l[i] = buf[i];
+        // manifold entries lead the sorted segment
+        uint32_t man = 0;
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) man += (buf[i] >> ADJ_KIND_SHIFT) == FK_MANIFOLD ? 1u : 0u;
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1) man += __shfl_xor_sync(0xffffffffu, man, o);
+        __shared__ uint32_t warpMan[8];
+        if ((threadIdx.x & 31u) == 0) warpMan[threadIdx.x >> 5] = man;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            uint32_t t = 0;
+            for (uint32_t w = 0; w < (blockDim.x >> 5); w++) t += warpMan[w];
+            d.dynSplit[b] = t;
+        }
+        __syncthreads();
+    }
+}
+
 void launch_adjacency(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     cudaMemsetAsync(d.dynCount, 0, sizeof(uint32_t) * P.numBodies, st);
     const uint32_t items = z.maxPairs + ((P.cloth || P.ogc) ? z.maxSoft : 0u);
@@ -263,6 +315,7 @@ void launch_adjacency(const Params& P, const DevPtrs& d, const Sizes& z, cudaStr
     cudaMemcpyAsync(d.dynCursor, d.dynStart, sizeof(uint32_t) * P.numBodies, cudaMemcpyDeviceToDevice, st);
     k_adj_dyn<true><<<stride_blocks(items, 128), 128, 0, st>>>(P, d);
     k_adj_dyn_sort<<<(P.numBodies + 127) / 128, 128, 0, st>>>(d, P.numBodies);
+    k_adj_long_sort<<<148, 256, 0, st>>>(d);
 }
 
 // The five runs in ascending (kind << 28 | index) order: static pre
