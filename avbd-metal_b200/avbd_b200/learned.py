@@ -253,6 +253,8 @@ def _main(argv=None):
     ap.add_argument("--target-iterations", type=int, default=80,
                     help="iterations of the rollouts that give the targets (a more converged solve than the "
                          "iteration counts the model is used at)")
+    ap.add_argument("--drop-ring", action="store_true",
+                    help="train without the 1-ring features (16-31): their inputs and first-layer weights are zero")
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=1e-3)
@@ -266,7 +268,11 @@ def _main(argv=None):
         return sc
 
     X, T = collect(rollout_scene, a.seeds, a.frames, every=a.every, fraction=a.fraction)
+    if a.drop_ring:
+        X[:, 16:] = 0.0
     model = train(X, T, steps=a.steps, batch=a.batch, lr=a.lr)
+    if a.drop_ring:
+        model.params[:HID * DIN].reshape(HID, DIN)[:, 16:] = 0.0
     model.save(a.out)
     print(f"samples {len(X)}, loss {model.history[0]:.4f} -> {model.history[-1]:.4f}")
     for iters in (10, 20):

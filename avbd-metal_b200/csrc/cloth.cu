@@ -192,6 +192,10 @@ __device__ void sort_segment(uint4* seg, uint32_t n) {
     }
 }
 
+// Pairs per owner kept from the counting pass (other, flags): an owner with
+// at most this many is written from them instead of a second grid scan.
+constexpr uint32_t kDatCache = 16;
+
 template <bool EMIT>
 __global__ void __launch_bounds__(128) k_dat_pairs(const Params P, const DevPtrs d, uint32_t owners) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -201,6 +205,24 @@ __global__ void __launch_bounds__(128) k_dat_pairs(const Params P, const DevPtrs
     for (uint32_t owner = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; owner < owners; owner += warps) {
         uint32_t count = 0;
         const uint32_t base = EMIT ? d.datOwnerStart[owner] : 0u;
+        uint2* cache = d.datCache + (size_t)owner * kDatCache;
+        if (EMIT) {
+            const uint32_t n = d.datOwnerCount[owner];
+            if (n <= kDatCache) {
+                const bool vt = owner < P.numParticles;
+                const uint32_t id = vt ? d.particleIdx[owner] : owner - P.numParticles;
+                if (lane < n && base + lane < P.maxDatPairs) {
+                    const uint2 c = cache[lane];
+                    d.datPairs[base + lane] = make_uint4(vt ? DAT_PAIR_VT : DAT_PAIR_EE, id, c.x, c.y);
+                }
+                __syncwarp();
+                if (lane == 0 && n > 1) {
+                    const uint32_t end = min(base + n, P.maxDatPairs);
+                    if (end > base) sort_segment(d.datPairs + base, end - base);
+                }
+                continue;
+            }
+        }
         if (owner < P.numParticles) {
             const uint32_t v = d.particleIdx[owner];
             const float3 p = xyz(d.posLin[v]);
@@ -230,6 +252,8 @@ __global__ void __launch_bounds__(128) k_dat_pairs(const Params P, const DevPtrs
                     if (slot < P.maxDatPairs)
                         d.datPairs[slot] = make_uint4(DAT_PAIR_VT, v, entry, DAT_PAIR_TRUNCATE | DAT_PAIR_CONTACT);
                 }
+                if (!EMIT && pass && count + __popc(ballot & below) < kDatCache)
+                    cache[count + __popc(ballot & below)] = make_uint2(entry, DAT_PAIR_TRUNCATE | DAT_PAIR_CONTACT);
                 count += __popc(ballot);
             }
         } else {
@@ -270,6 +294,8 @@ __global__ void __launch_bounds__(128) k_dat_pairs(const Params P, const DevPtrs
                                 if (slot < P.maxDatPairs)
                                     d.datPairs[slot] = make_uint4(DAT_PAIR_EE, gid, entry, flags);
                             }
+                            if (!EMIT && pass && count + __popc(ballot & below) < kDatCache)
+                                cache[count + __popc(ballot & below)] = make_uint2(entry, flags);
                             count += __popc(ballot);
                         }
                     }

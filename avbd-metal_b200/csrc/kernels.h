@@ -86,6 +86,7 @@ struct DevPtrs {
     float4* elemBox;                            // tight AABB per element (lo, hi)
     uint32_t *datOwnerCount, *datOwnerStart;    // pairs per query owner (particles, edges)
     uint4* datPairs;                            // (kind, owner, other, flags)
+    uint2* datCache;                            // first pairs of each owner from the counting pass (other, flags)
     uint32_t *rtCount, *rtStart;                // rigid-triangle records per triangle
     uint32_t *datEmit, *datEmitStart;           // element contacts per query owner
     SoftContactGPU *soft, *prevSoft;
