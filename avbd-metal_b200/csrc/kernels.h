@@ -119,6 +119,7 @@ struct DevPtrs {
     uint2* learnRing;
     float *learnPrm, *learnNorm, *learnResidBodies;
     float* learnResidBodies2;                   // per-body residual scratch of the predicted branch
+    float4 *learnNextLin, *learnNextAng;        // pending solves of the predicted branch (color-Jacobi scenes)
     void* learnHalf;                            // BF16 weight mirror
     double* learnResid;                         // [0] plain, [1] predicted, [2] scratch
     double* learnTrace;                         // residual trace of the last frame

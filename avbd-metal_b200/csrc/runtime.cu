@@ -283,10 +283,12 @@ struct avbd_solver {
             launch_mlp_infer(f.learnHalf, f.learnPrm, f.learnNorm, f.learnFeat, z.numLearn, f.learnPred, st);
             launch_learn_branch(P, f, z, st);
             if (trace) launch_residual(P, fb, z, f.learnResidBodies, f.learnTrace + 1, st);
-            // The two trial branches touch disjoint pose buffers, so the
-            // predicted one runs on a second stream beside the plain one
-            // (color-Jacobi scenes share posNext and run them in turn).
-            const bool fork = !P.colorJacobi;
+            // The two trial branches touch disjoint pose buffers (in
+            // color-Jacobi scenes the predicted branch also has its own
+            // pending-solve buffers), so the predicted one runs on a second
+            // stream beside the plain one.
+            if (P.colorJacobi) { fb.posNext = f.learnNextLin; fb.angNext = f.learnNextAng; }
+            const bool fork = !P.colorJacobi || f.learnNextLin != nullptr;
             cudaStream_t bst = fork ? branchStream : st;
             if (fork) {
                 cudaEventRecord(forkEvent, st);
@@ -580,6 +582,8 @@ struct avbd_solver {
         ok = ok && alloc(d.learnSweptLin, nb, "plainTrialLin") && alloc(d.learnSweptAng, nb, "plainTrialAng");
         ok = ok && alloc(d.learnResidBodies, std::max<uint32_t>(1, H.numDynamicBodies), "residualBodies");
         ok = ok && alloc(d.learnResidBodies2, std::max<uint32_t>(1, H.numDynamicBodies), "residualBodiesBranch");
+        if (z.numLearn && P.colorJacobi)
+            ok = ok && alloc(d.learnNextLin, nb, "branchNextLin") && alloc(d.learnNextAng, nb, "branchNextAng");
         ok = ok && alloc(d.learnResid, 4, "residual") && alloc(d.learnTrace, kTraceLength, "residualTrace");
         ok = ok && alloc(d.learnAccepted, 1, "learnAccepted", true);
         if (H.numTris > 0) {
