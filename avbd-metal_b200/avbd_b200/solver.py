@@ -72,6 +72,7 @@ def load_library() -> C.CDLL:
         "avbd_debug_read": ([vp, i32, vp, sz], i32),
         "avbd_set_stream": ([vp, vp], i32),
         "avbd_set_profiling": ([vp, i32], i32),
+        "avbd_set_capacity_for_testing": ([vp, i32, u32], i32),
         "avbd_get_profile": ([vp, vp], i32),
         "avbd_set_warm_start_model": ([vp, vp, vp, u32], i32),
         "avbd_set_warm_start_mode": ([vp, i32], i32),
@@ -226,6 +227,11 @@ class GPUSolver:
         """Launch on a caller-owned stream (an integer cudaStream_t handle, e.g.
         torch.cuda.Stream().cuda_stream); None restores the solver's stream."""
         self._check(load_library().avbd_set_stream(self._h, cuda_stream_handle or None))
+
+    def set_capacity_for_testing(self, which: int, value: int):
+        """Lower the soft-contact or Planar-DAT pair capacity (abi.CAPACITY_*)
+        to provoke its capacity failure on a small scene."""
+        self._check(load_library().avbd_set_capacity_for_testing(self._h, int(which), int(value)))
 
     def set_profiling(self, enabled: bool):
         self._check(load_library().avbd_set_profiling(self._h, 1 if enabled else 0))

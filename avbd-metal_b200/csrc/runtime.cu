@@ -687,10 +687,10 @@ struct avbd_solver {
                               hostLatch[1], hostLatch[2], H.maxPairs);
             else if (failure == AVBD_FAIL_SOFT_CONTACT_CAPACITY)
                 std::snprintf(buf, sizeof buf, "soft contact capacity exceeded at frame %u: %u records > %u",
-                              hostLatch[1], hostLatch[2], H.maxSoft);
+                              hostLatch[1], hostLatch[2], P.maxSoft);
             else if (failure == AVBD_FAIL_PLANAR_DAT_PAIR_CAPACITY)
                 std::snprintf(buf, sizeof buf, "Planar-DAT pair capacity exceeded at frame %u: %u pairs > %u",
-                              hostLatch[1], hostLatch[2], H.maxDatPairs);
+                              hostLatch[1], hostLatch[2], P.maxDatPairs);
             else if (failure == AVBD_FAIL_PLANAR_DAT_GRID_SPAN)
                 std::snprintf(buf, sizeof buf, "Planar-DAT element grid span exceeded at frame %u: %u elements",
                               hostLatch[1], hostLatch[2]);
@@ -1095,6 +1095,17 @@ int avbd_set_stream(avbd_solver* s, void* cuda_stream) {
     if (!s) return AVBD_ERR_INVALID_ARGUMENT;
     if (!s->check(cudaStreamSynchronize(s->launch), "stream switch")) return AVBD_ERR_RUNTIME_FAILURE;
     s->launch = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : s->stream;
+    return AVBD_OK;
+}
+
+int avbd_set_capacity_for_testing(avbd_solver* s, int which, uint32_t value) {
+    if (!s) return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    if (which == AVBD_CAPACITY_SOFT_CONTACTS) s->P.maxSoft = std::min(value, s->z.maxSoft);
+    else if (which == AVBD_CAPACITY_PLANAR_DAT_PAIRS) s->P.maxDatPairs = std::min(value, s->H.maxDatPairs);
+    else return AVBD_ERR_INVALID_ARGUMENT;
+    s->graphsValid = false;   // capacities are baked into the frame graphs
     return AVBD_OK;
 }
 

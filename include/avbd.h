@@ -355,6 +355,14 @@ typedef struct avbd_profile {
 int avbd_set_profiling(avbd_solver* solver, int enabled);
 int avbd_get_profile(avbd_solver* solver, avbd_profile* out);
 
+/* Lower a contact capacity below the one sized at upload, to provoke the
+ * capacity failures on small scenes (`planarDATSoftCapacityForTesting`,
+ * `planarDATPairCapacityForTesting`, GPUSolver.swift:2117-2133, :2235-2236).
+ * The value is clamped to the allocated capacity; takes effect from the next
+ * frame.                                                                    */
+enum { AVBD_CAPACITY_SOFT_CONTACTS = 0, AVBD_CAPACITY_PLANAR_DAT_PAIRS = 1 };
+int avbd_set_capacity_for_testing(avbd_solver* solver, int which, uint32_t value);
+
 /* ---- Learned warm start (no counterpart in the reference) -------------
  * A 32-128-128-128-16 MLP (BF16 weights/activations, FP32 accumulation)
  * predicts each dynamic particle's correction of the plain gamma warm start

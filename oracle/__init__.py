@@ -54,6 +54,7 @@ def lib():
         _lib.oracle_debug_buffer_size.restype = C.c_size_t
         _lib.oracle_debug_read.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_size_t]
         _lib.oracle_atan2.argtypes = [C.c_float, C.c_float]
+        _lib.oracle_set_capacity_for_testing.argtypes = [C.c_void_p, C.c_int, C.c_uint32]
         _lib.oracle_atan2.restype = C.c_float
     return _lib
 
@@ -106,6 +107,9 @@ class OracleSolver:
         out = (self._abi.BodyState * n)()
         lib().oracle_get_body_states(self._h, n, out)
         return out
+
+    def set_capacity_for_testing(self, which: int, value: int):
+        return lib().oracle_set_capacity_for_testing(self._h, which, value)
 
     def set_motor_targets(self, joints, targets):
         ids = np.ascontiguousarray(joints, dtype=np.uint32)

@@ -1847,6 +1847,13 @@ int oracle_create(const avbd_scene_desc* scene, void** out) {
 void oracle_destroy(void* h) { delete static_cast<Solver*>(h); }
 int oracle_set_threads(void* h, int n) { static_cast<Solver*>(h)->threads = n < 1 ? 1 : n; return AVBD_OK; }
 int oracle_set_settings(void* h, const avbd_settings* st) { static_cast<Solver*>(h)->settings = *st; return AVBD_OK; }
+int oracle_set_capacity_for_testing(void* h, int which, uint32_t value) {
+    Solver* s = static_cast<Solver*>(h);
+    if (which == AVBD_CAPACITY_SOFT_CONTACTS) s->maxSoft = std::min<uint32_t>(value, (uint32_t)s->soft.size());
+    else if (which == AVBD_CAPACITY_PLANAR_DAT_PAIRS) s->maxDatPairs = std::min(value, s->maxDatPairs);
+    else return AVBD_ERR_INVALID_ARGUMENT;
+    return AVBD_OK;
+}
 int oracle_step(void* h, uint32_t frames) {
     Solver* s = static_cast<Solver*>(h);
     for (uint32_t f = 0; f < frames; f++) {
