@@ -72,13 +72,13 @@ __device__ __forceinline__ uint32_t ld_pair(const bf16* p) { return *reinterpret
 constexpr int kS1 = mlp::DIN + 8, kSH = mlp::HID + 8;
 constexpr uint32_t kSW1 = 0, kSW2 = kSW1 + mlp::HID * kS1, kSW3 = kSW2 + mlp::HID * kSH, kSW4 = kSW3 + mlp::HID * kSH,
                    kSWN = kSW4 + mlp::DOUT * kSH;
-constexpr uint32_t kInferWarps = 8;
+constexpr uint32_t kInferWarps = 4;
 constexpr size_t kInferSmem = sizeof(bf16) * kSWN;
 
 // Fused 4-layer inference: every block stages the weights once and its warps
 // take 16-row tiles until the batch is done (m16n8k16 BF16 MMA, FP32
 // accumulation, bias / ReLU / BF16 conversion between layers in registers).
-__global__ void __launch_bounds__(256) k_mlp_infer(const bf16* __restrict__ W, const float* __restrict__ prm,
+__global__ void __launch_bounds__(128) k_mlp_infer(const bf16* __restrict__ W, const float* __restrict__ prm,
                                                    const float* __restrict__ norm, const float* __restrict__ X,
                                                    uint32_t n, float* __restrict__ Y) {
     using namespace mlp;

@@ -94,3 +94,18 @@ def test_cloth_full_size_runs(cuda_lib):
     assert np.isfinite(pos).all()
     c = g.counters()
     print(f"cloth-256: soft {c.num_soft} dat pairs {c.dat_pairs} truncations {c.dat_truncations}")
+
+
+def test_snapshot_restore_drape_bitwise(cuda_lib):
+    """Snapshots of a Planar-DAT cloth: replaying from one repeats the frames
+    bit for bit."""
+    from avbd_b200.solver import GPUSolver
+    g = GPUSolver(demos.drape_scene(res=16))
+    g.step(40)
+    snap = g.snapshot()
+    g.step(15)
+    a, _ = g.positions()
+    g.restore(snap)
+    g.step(15)
+    b, _ = g.positions()
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))

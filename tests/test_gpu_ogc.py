@@ -95,3 +95,24 @@ def test_mixed_full_size_runs(cuda_lib):
     print(f"mixed: soft {c.num_soft} (rt {c.soft_rt}, vt {c.soft_vt}, ee {c.soft_ee}), ogc {c.ogc_exceeded}")
     assert g.runtime_failure() == 0 and np.isfinite(pos).all()
     assert c.soft_vt > 0
+
+
+def test_snapshot_restore_mixed_bitwise(cuda_lib):
+    """Snapshots cover the element-contact state (soft contacts and their map,
+    tracked sets, bound anchors): replaying from one repeats the frames bit
+    for bit (the reference's snapshots refuse soft scenes,
+    GPUSolver.swift:2985-2986)."""
+    from avbd_b200.solver import GPUSolver
+    g = GPUSolver(small_mixed())
+    g.step(70)
+    snap = g.snapshot()
+    g.step(20)
+    a, ra = g.positions()
+    ca = g.counters()
+    g.restore(snap)
+    g.step(20)
+    b, rb = g.positions()
+    cb = g.counters()
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    assert np.array_equal(ra.view(np.uint32), rb.view(np.uint32))
+    assert (ca.num_soft, ca.soft_vt, ca.soft_ee, ca.soft_rt) == (cb.num_soft, cb.soft_vt, cb.soft_ee, cb.soft_rt)
