@@ -170,6 +170,8 @@ EXPORTED = [
     "avbd_create", "avbd_destroy", "avbd_set_settings", "avbd_get_settings",
     "avbd_step", "avbd_sync", "avbd_get_body_states", "avbd_set_body_states",
     "avbd_get_positions", "avbd_set_positions", "avbd_set_motor_targets",
+    "avbd_set_joint_world_anchors", "avbd_set_motor_velocities", "avbd_set_motor_torques",
+    "avbd_get_motor_states",
     "avbd_max_constraint_error", "avbd_get_counters", "avbd_runtime_failure",
     "avbd_last_error", "avbd_snapshot_capture", "avbd_snapshot_restore",
     "avbd_snapshot_free", "avbd_debug_buffer_size", "avbd_debug_read", "avbd_set_stream",

@@ -171,14 +171,24 @@ def add_cloth_grid(s: PhysicsScene, positions, thickness: float, mass_per_node: 
 
 
 def drape_scene(res: int = 28, friction: float = 0.6, membrane_mu: float = 300.0,
-                bend: float = 5e-4) -> PhysicsScene:
+                bend: float = 5e-4, obstacle: str = "sphere") -> PhysicsScene:
     """Demos7.drape (Demos7.swift:270-301): a res x res sheet of 2.8 m falls
-    onto a static sphere of diameter 1.1 m above the ground."""
+    onto a static sphere of diameter 1.1 m above the ground.  `obstacle`
+    "capsule" (a horizontal static capsule, met by the capsule's three
+    feature spheres) or "torus" (a flat static ring, met only by
+    particle-torus contacts) replaces the sphere."""
     s = PhysicsScene("drape")
     st = s.settings
     st.iterations, st.beta_lin, st.particle_damping, st.cloth_viscosity = 10, 20000.0, 1.5, 0.25
     add_ground(s, friction=friction)
-    s.add_sphere(1.1, 0.0, friction, (0.0, 0.0, 1.0))
+    if obstacle == "sphere":
+        s.add_sphere(1.1, 0.0, friction, (0.0, 0.0, 1.0))
+    elif obstacle == "capsule":
+        s.add_capsule(1.2, 0.4, 0.0, friction, (0.0, 0.0, 1.0), rotation=quat_axis_angle(math.pi / 2, (0, 1, 0)))
+    elif obstacle == "torus":
+        s.add_torus(0.5, 0.2, 0.0, friction, (0.0, 0.0, 1.2))
+    else:
+        raise ValueError(f"unknown obstacle {obstacle!r}")
     n = max(20, res)
     size = f32(2.8)
     spacing = size / f32(n - 1)
@@ -440,6 +450,215 @@ def two_cubes_scene(n: int = 5, iterations: int = 10) -> PhysicsScene:
         add_soft_block(s, (0.03 * (z > 0.3), 0.0, z), n, n, n, 0.3 / (n - 1), mu=3000.0, lam=30000.0,
                        mass_per_node=0.05, friction=0.5, exclusion_joints=False)
     s.settings.iterations = iterations
+    return s
+
+
+# ---------------------------------------------------------------------------
+# Tori, capsules and convex hulls
+# ---------------------------------------------------------------------------
+
+def quat_axis_angle(angle: float, axis) -> tuple:
+    """Unit quaternion (x, y, z, w) of a rotation by `angle` about `axis`."""
+    a = np.asarray(axis, dtype=np.float64)
+    a = a / np.linalg.norm(a)
+    h = 0.5 * angle
+    return tuple(float(f32(x)) for x in (*(a * math.sin(h)), math.cos(h)))
+
+
+def quat_mul(a, b) -> tuple:
+    """Hamilton product a * b of (x, y, z, w) quaternions, normalised."""
+    ax, ay, az, aw = a
+    bx, by, bz, bw = b
+    q = np.array([aw * bx + ax * bw + ay * bz - az * by,
+                  aw * by - ax * bz + ay * bw + az * bx,
+                  aw * bz + ax * by - ay * bx + az * bw,
+                  aw * bw - ax * bx - ay * by - az * bz])
+    q /= np.linalg.norm(q)
+    return tuple(float(f32(x)) for x in q)
+
+
+Q_X90 = quat_axis_angle(math.pi / 2, (1, 0, 0))
+
+
+def torus_rest_scene() -> PhysicsScene:
+    """A torus dropped flat onto a static slab comes to rest lying flat, its
+    centre one tube radius up (TorusAndMachineTests.swift:7-15)."""
+    s = PhysicsScene("torus-rest")
+    s.add_body((100, 100, 2), 0.0, 0.5, (0, 0, -1))
+    s.add_torus(0.45, 0.12, 1.0, 0.5, (0, 0, 2))
+    return s
+
+
+def linked_tori_scene() -> PhysicsScene:
+    """Two interlocked rings, the upper one pinned to the world, carrying a
+    1 kg box on the lower one (TorusAndMachineTests.swift:17-30).  The box is
+    the last body."""
+    s = PhysicsScene("linked-tori")
+    t1 = s.add_torus(0.45, 0.12, 1.0, 0.4, (0, 0, 6), rotation=Q_X90)
+    t2 = s.add_torus(0.45, 0.12, 1.0, 0.4, (0, 0, 5.34),
+                     rotation=quat_mul(quat_axis_angle(math.pi / 2, (0, 0, 1)), Q_X90))
+    s.add_joint(SceneJoint(-1, t1, (0, 0, 6.4), (0.45, 0, 0)))
+    w = s.add_body((0.5, 0.5, 0.5), 8.0, 0.5, (0, 0, 4.4))
+    s.add_joint(SceneJoint(t2, w, (0.45, 0, 0), (0, 0, 0.45)))
+    return s
+
+
+def ring_catch_scene() -> PhysicsScene:
+    """A ball dropped into a static upright ring stays in it
+    (TorusAndMachineTests.swift:32-41)."""
+    s = PhysicsScene("ring-catch")
+    s.add_body((100, 100, 2), 0.0, 0.5, (0, 0, -1))
+    s.add_torus(0.6, 0.15, 0.0, 0.5, (0, 0, 1.5), rotation=Q_X90)
+    s.add_sphere(0.7, 1.0, 0.5, (0, 0, 1.52))
+    return s
+
+
+def bearing_scene() -> PhysicsScene:
+    """A torus hub hanging on a static capsule axle settles at the analytic
+    offset (major - minor) - axle radius below it
+    (TorusAndMachineTests.swift:88-102)."""
+    s = PhysicsScene("bearing")
+    s.settings.iterations = 20
+    s.settings.beta_lin = 20000.0
+    s.add_capsule(2.0, 0.11, 0.0, 0.02, (0, 0, 3), rotation=Q_X90)
+    s.add_torus(0.27, 0.115, 1.5, 0.02, (0, 0, 3), rotation=Q_X90)
+    return s
+
+
+def hull_box_scene() -> PhysicsScene:
+    """A body whose only collider is an 8-vertex convex hull (a unit cube)
+    rests on box terrain (GPUSolverTests.swift:537-571).  Body 1 is the hull
+    body."""
+    s = PhysicsScene("hull-box")
+    s.settings.dt = 1.0 / 120.0
+    s.settings.gravity = -9.81
+    s.settings.iterations = 20
+    s.add_body((20, 20, 0.2), 0.0, 1.0, (0, 0, -0.1))
+    body = s.add_body((1, 1, 1), 0.0, 1.0, (0, 0, 2), mass=1.0, diagonal_inertia=(1 / 6, 1 / 6, 1 / 6),
+                      collision_enabled=False)
+    hull = [(x, y, z) for z in (-0.5, 0.5) for y in (-0.5, 0.5) for x in (-0.5, 0.5)]
+    s.add_convex_collider(body, hull, friction=1.0)
+    return s
+
+
+def capsule_foot_scene() -> PhysicsScene:
+    """A foot of three capsule colliders with material anchors, held by a
+    500 N/m spring to a world point (GPUSolverTests.swift:577-620): under a
+    load below the Coulomb limit it must not creep.  Joint 0 is the spring;
+    body 1 the foot."""
+    s = PhysicsScene("capsule-foot")
+    s.settings.dt = 1.0 / 120.0
+    s.settings.iterations = 20
+    s.add_body((20, 8, 0.2), 0.0, 1.1, (0, 0, -0.1))
+    foot = s.add_body((0.35, 0.2, 0.2), 0.0, 1.1, (0, 0, 0.36), mass=5.0, diagonal_inertia=(0.08, 0.12, 0.08),
+                      collision_enabled=False)
+    along_x = quat_axis_angle(math.pi / 2, (0, 1, 0))
+    for y in (-0.07, 0.07):
+        s.add_collider(foot, (0.24, 0.035, 0), friction=1.1, local_position=(0, y, -0.31),
+                       local_rotation=along_x, shape=abi.SHAPE_CAPSULE)
+    s.add_collider(foot, (0.14, 0.035, 0), friction=1.1, local_position=(0.14, 0, -0.31),
+                   local_rotation=Q_X90, shape=abi.SHAPE_CAPSULE)
+    s.add_joint(SceneJoint(-1, foot, (0, 0, 0.36), (0, 0, 0), stiffness_lin=500.0, stiffness_ang=0.0))
+    return s
+
+
+def chainmail_scene(rings: int = 6, drops: int = 3) -> PhysicsScene:
+    """Demos2.chainmail (Demos2.swift:318-430): a sheet of interlinked tori
+    hung on welded peg posts, with spheres and boxes dropped on it."""
+    s = PhysicsScene("chainmail")
+    st = s.settings
+    st.iterations, st.beta_lin, st.lambda_max = 15, 20000.0, 1500.0
+    add_ground(s, friction=0.6)
+    R, r, sheet_z, pitch = 0.45, 0.15, 8.0, 1.15
+    n = rings
+    extent = float(f32(n - 1) * f32(pitch) / f32(2))
+    mid = (n - 1) // 2
+    inf = float("inf")
+
+    def add_post(x, y):
+        seg_h, cross = 1.6, 0.22
+        peg_z, top_z = sheet_z - 0.3, sheet_z + 1.0
+        prev = s.add_body((cross, cross, seg_h), 0.0, 0.4, (x, y, seg_h / 2))
+        z = seg_h
+        while z < top_z:
+            h = min(seg_h, top_z - z)
+            seg = s.add_body((cross, cross, h), 4.0, 0.4, (x, y, z + h / 2))
+            s.add_joint(SceneJoint(prev, seg, (0, 0, s.bodies[prev].size[2] / 2), (0, 0, -h / 2),
+                                   stiffness_lin=inf, stiffness_ang=inf))
+            prev = seg
+            z += h
+        host = prev
+        for axis in range(2):
+            size = (1.1, 0.14, 0.14) if axis == 0 else (0.14, 1.1, 0.14)
+            peg = s.add_body(size, 2.0, 0.5, (x, y, peg_z))
+            seg_c = s.bodies[host].position[2]
+            s.add_joint(SceneJoint(host, peg, (0, 0, peg_z - seg_c), (0, 0, 0), stiffness_lin=inf,
+                                   stiffness_ang=inf))
+            off = (0.4, 0, 0) if axis == 0 else (0, 0.4, 0)
+            s.add_joint(SceneJoint(host, peg, (off[0], off[1], peg_z - seg_c), off, stiffness_lin=inf,
+                                   stiffness_ang=inf))
+
+    cells = set()
+    for j in range(n):
+        for i in range(n):
+            corner = (i in (0, n - 1)) and (j in (0, n - 1))
+            edge_mid = (i == mid and j in (0, n - 1)) or (j == mid and i in (0, n - 1))
+            if corner or edge_mid:
+                cells.add(j * n + i)
+    for cell in sorted(cells):
+        i, j = cell % n, cell // n
+        add_post(i * pitch - extent, j * pitch - extent)
+    q_y = quat_mul(quat_axis_angle(math.pi / 2, (0, 0, 1)), Q_X90)
+    for j in range(n):
+        for i in range(n):
+            cx, cy = i * pitch - extent, j * pitch - extent
+            s.add_torus(R, r, 1.0, 0.3, (cx, cy, sheet_z))
+            if i + 1 < n:
+                s.add_torus(R, r, 1.0, 0.3, (cx + pitch / 2, cy, sheet_z), rotation=Q_X90)
+            if j + 1 < n:
+                s.add_torus(R, r, 1.0, 0.3, (cx, cy + pitch / 2, sheet_z), rotation=q_y)
+    rng = SplitMix64(11)
+    for k in range(drops):
+        sz = 0.9 + rng.next_float() * 0.7
+        pos = ((rng.next_float() - 0.5) * n * pitch * 0.4, (rng.next_float() - 0.5) * n * pitch * 0.4,
+               sheet_z + 4 + k * 2)
+        if k % 2 == 0:
+            s.add_sphere(sz, 1.0, 0.5, pos)
+        else:
+            s.add_body((sz, sz, sz), 1.0, 0.5, pos)
+    return s
+
+
+def shapes_scene(seed: int = 6, count: int = 512, pitch: float = 1.3) -> PhysicsScene:
+    """A seeded pile of capsules, tori, spheres, boxes and convex-hull
+    bodies (octahedra) dropped onto the ground in a square grid of columns:
+    every narrowphase shape pair except hull/round (which produces no
+    contact) occurs."""
+    s = PhysicsScene("shapes")
+    add_ground(s, friction=0.6)
+    rng = SplitMix64(seed)
+    side = max(1, int(math.ceil(math.sqrt(count / 4))))
+    octa = [(0.35, 0, 0), (-0.35, 0, 0), (0, 0.35, 0), (0, -0.35, 0), (0, 0, 0.35), (0, 0, -0.35)]
+    for k in range(count):
+        col, layer = k % (side * side), k // (side * side)
+        x = (col % side - 0.5 * (side - 1)) * pitch + rng.uniform(-0.1, 0.1)
+        y = (col // side - 0.5 * (side - 1)) * pitch + rng.uniform(-0.1, 0.1)
+        z = 0.6 + 1.1 * layer
+        q = quat_axis_angle(rng.uniform(0.0, math.pi), (rng.uniform(-1, 1), rng.uniform(-1, 1), 1.0))
+        kind = rng.next() % 5
+        if kind == 0:
+            s.add_capsule(rng.uniform(0.3, 0.7), rng.uniform(0.12, 0.2), 1.0, 0.5, (x, y, z), rotation=q)
+        elif kind == 1:
+            s.add_torus(rng.uniform(0.25, 0.4), rng.uniform(0.08, 0.12), 1.0, 0.5, (x, y, z), rotation=q)
+        elif kind == 2:
+            s.add_sphere(rng.uniform(0.3, 0.6), 1.0, 0.5, (x, y, z))
+        elif kind == 3:
+            s.add_body((rng.uniform(0.3, 0.6), rng.uniform(0.3, 0.6), rng.uniform(0.3, 0.6)), 1.0, 0.5, (x, y, z),
+                       rotation=q)
+        else:
+            b = s.add_body((0.7, 0.7, 0.7), 0.0, 0.5, (x, y, z), rotation=q, mass=0.3,
+                           diagonal_inertia=(0.02, 0.02, 0.02), collision_enabled=False)
+            s.add_convex_collider(b, octa, friction=0.5)
     return s
 
 

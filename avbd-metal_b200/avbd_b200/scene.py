@@ -60,6 +60,15 @@ class SimSettings:
         return s
 
 
+def _qrot32(q, v):
+    """Rotate v by the unit quaternion q = (x, y, z, w), in float32."""
+    u = np.asarray(q[:3], dtype=np.float32)
+    w = np.float32(q[3])
+    v = np.asarray(v, dtype=np.float32)
+    t = np.float32(2) * np.cross(u, v)
+    return (v + w * t + np.cross(u, t)).astype(np.float32)
+
+
 def _vec(v, n=3):
     return tuple(float(f32(x)) for x in v)[:n]
 
@@ -99,6 +108,7 @@ class SceneCollider:
     collides_with_shared: bool = True
     collision_enabled: bool = True
     world_round_anchor: bool = False
+    hull_vertices: Optional[List[Tuple[float, float, float]]] = None  # centred, collider frame
 
 
 @dataclass
@@ -217,9 +227,50 @@ class PhysicsScene:
             collision_enabled=collision_enabled, world_round_anchor=False))
         return len(self.colliders) - 1
 
+    def add_convex_collider(self, body, vertices, friction=None, dynamic_friction=None,
+                            local_position=(0, 0, 0), local_rotation=(0, 0, 0, 1),
+                            collision_group=0, collides_with_shared=True,
+                            collision_enabled=True) -> int:
+        """addConvexCollider (Scene.swift:645-676): 4...64 cooked hull
+        vertices in the collider frame; the collider becomes the vertices'
+        tight box, its origin moved to the box centre without changing the
+        geometry.  The narrowphase contacts hulls against boxes only."""
+        v = np.asarray(vertices, dtype=np.float32).reshape(-1, 3)
+        if not 4 <= len(v) <= 64:
+            raise ValueError("convex collider requires 4...64 cooked hull vertices")
+        if not np.isfinite(v).all():
+            raise ValueError("convex collider vertices must be finite")
+        lo, hi = v.min(axis=0), v.max(axis=0)
+        center = (lo + hi) * np.float32(0.5)
+        centered = v - center
+        q = np.asarray(local_rotation, dtype=np.float32)
+        shift = _qrot32(q, center)
+        lp = np.asarray(local_position, dtype=np.float32) + shift
+        c = self.add_collider(body, tuple(float(x) for x in hi - lo), friction=friction,
+                              dynamic_friction=dynamic_friction, local_position=tuple(float(x) for x in lp),
+                              local_rotation=local_rotation, shape=abi.SHAPE_BOX,
+                              collision_group=collision_group, collides_with_shared=collides_with_shared,
+                              collision_enabled=collision_enabled)
+        self.colliders[c].hull_vertices = [tuple(float(x) for x in row) for row in centered]
+        return c
+
     def add_sphere(self, diameter, density, friction, position, velocity=(0, 0, 0)) -> int:
         return self.add_body((diameter, diameter, diameter), density, friction, position,
                              velocity=velocity, shape=abi.SHAPE_SPHERE)
+
+    def add_capsule(self, length, radius, density, friction, position, rotation=(0, 0, 0, 1),
+                    velocity=(0, 0, 0)) -> int:
+        """addCapsule (Scene.swift:687-694): axis along local z, size
+        (length, radius, 0)."""
+        return self.add_body((length, radius, 0.0), density, friction, position, rotation=rotation,
+                             velocity=velocity, shape=abi.SHAPE_CAPSULE)
+
+    def add_torus(self, major, minor, density, friction, position, rotation=(0, 0, 0, 1),
+                  velocity=(0, 0, 0)) -> int:
+        """addTorus (Scene.swift:696-703): axis along local z, size
+        (major, minor, 0)."""
+        return self.add_body((major, minor, 0.0), density, friction, position, rotation=rotation,
+                             velocity=velocity, shape=abi.SHAPE_TORUS)
 
     def add_particle(self, radius, mass, friction=0.5, position=(0, 0, 0),
                      velocity=(0, 0, 0)) -> int:
@@ -285,10 +336,17 @@ class PhysicsScene:
                    0 if b.mass is None else 1, 0.0 if b.mass is None else b.mass,
                    (0.0, 0.0, 0.0) if b.diagonal_inertia is None else tuple(b.diagonal_inertia),
                    b.gravity_scale) for b in self.bodies]
-        colliders = [(c.body, c.size, c.friction, dyn(c.friction, c.dynamic_friction),
-                      c.local_position, c.local_rotation, c.shape, c.collision_group,
-                      1 if c.collides_with_shared else 0, 1 if c.collision_enabled else 0,
-                      1 if c.world_round_anchor else 0, 0, 0) for c in self.colliders]
+        hull_rows = []
+        colliders = []
+        for c in self.colliders:
+            first, count = 0, 0
+            if c.hull_vertices:
+                first, count = len(hull_rows), len(c.hull_vertices)
+                hull_rows.extend(c.hull_vertices)
+            colliders.append((c.body, c.size, c.friction, dyn(c.friction, c.dynamic_friction),
+                              c.local_position, c.local_rotation, c.shape, c.collision_group,
+                              1 if c.collides_with_shared else 0, 1 if c.collision_enabled else 0,
+                              1 if c.world_round_anchor else 0, first, count))
         joints = [(j.body_a, j.body_b, _vec(j.r_a), _vec(j.r_b), j.stiffness_lin,
                    j.stiffness_ang, j.fracture, 1 if j.fracture_linear else 0,
                    0 if j.hinge_axis is None else 1,
@@ -307,7 +365,11 @@ class PhysicsScene:
         desc.abi_version = abi.ABI_VERSION
         desc.num_bodies, desc.bodies = pack(abi.BodyDesc, bodies)
         desc.num_colliders, desc.colliders = pack(abi.ColliderDesc, colliders)
-        desc.num_hull_vertices = 0
+        hv = np.ascontiguousarray(np.asarray(hull_rows if hull_rows else [(0.0, 0.0, 0.0)],
+                                             dtype=np.float32).reshape(-1))
+        keep.append(hv)
+        desc.num_hull_vertices = len(hull_rows)
+        desc.hull_vertices = hv.ctypes.data_as(C.POINTER(C.c_float))
         desc.num_joints, desc.joints = pack(abi.JointDesc, joints)
         desc.num_springs, desc.springs = pack(abi.SpringDesc, springs)
         desc.num_tets, desc.tets = pack(abi.TetDesc, tets)

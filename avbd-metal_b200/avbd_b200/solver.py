@@ -61,6 +61,10 @@ def load_library() -> C.CDLL:
         "avbd_get_positions": ([vp, u32, vp, vp], i32),
         "avbd_set_positions": ([vp, u32, vp], i32),
         "avbd_set_motor_targets": ([vp, vp, u32, vp], i32),
+        "avbd_set_joint_world_anchors": ([vp, vp, u32, vp], i32),
+        "avbd_set_motor_velocities": ([vp, vp, u32, vp], i32),
+        "avbd_set_motor_torques": ([vp, vp, u32, vp], i32),
+        "avbd_get_motor_states": ([vp, vp, u32, vp, vp], i32),
         "avbd_max_constraint_error": ([vp, C.POINTER(C.c_float)], i32),
         "avbd_get_counters": ([vp, vp], i32),
         "avbd_runtime_failure": ([vp, C.POINTER(i32)], i32),
@@ -195,6 +199,35 @@ class GPUSolver:
         ids = np.ascontiguousarray(joints, dtype=np.uint32)
         t = np.ascontiguousarray(targets, dtype=np.float32)
         self._check(load_library().avbd_set_motor_targets(self._h, ids.ctypes.data, len(ids), t.ctypes.data))
+
+    def set_joint_world_anchors(self, joints, points):
+        """setJointWorldAnchors (GPUSolver.swift:2481-2494)."""
+        ids = np.ascontiguousarray(joints, dtype=np.uint32)
+        p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1)
+        if p.size != 3 * ids.size:
+            raise ValueError("one xyz point per joint")
+        self._check(load_library().avbd_set_joint_world_anchors(self._h, ids.ctypes.data, len(ids), p.ctypes.data))
+
+    def set_motor_velocities(self, joints, rad_per_s):
+        """setMotorVelocities (GPUSolver.swift:2534-2551)."""
+        ids = np.ascontiguousarray(joints, dtype=np.uint32)
+        v = np.ascontiguousarray(rad_per_s, dtype=np.float32)
+        self._check(load_library().avbd_set_motor_velocities(self._h, ids.ctypes.data, len(ids), v.ctypes.data))
+
+    def set_motor_torques(self, joints, torques):
+        """setMotorTorques (GPUSolver.swift:2564-2578)."""
+        ids = np.ascontiguousarray(joints, dtype=np.uint32)
+        t = np.ascontiguousarray(torques, dtype=np.float32)
+        self._check(load_library().avbd_set_motor_torques(self._h, ids.ctypes.data, len(ids), t.ctypes.data))
+
+    def motor_states(self, joints):
+        """motorStates (GPUSolver.swift:2606-2637): (angles, velocities)."""
+        ids = np.ascontiguousarray(joints, dtype=np.uint32)
+        a = np.zeros(len(ids), np.float32)
+        v = np.zeros(len(ids), np.float32)
+        self._check(load_library().avbd_get_motor_states(self._h, ids.ctypes.data, len(ids), a.ctypes.data,
+                                                         v.ctypes.data))
+        return a, v
 
     # -- diagnostics -----------------------------------------------------------
     def max_constraint_error(self) -> float:

@@ -116,6 +116,9 @@ struct Params {
     // particles): cell size and hash size
     uint32_t fineBP, fineHashSize;
     float fineCellSize;
+    // the scene has torus, capsule or convex-hull colliders (second
+    // narrowphase pass)
+    uint32_t roundShapes;
 };
 
 // Device counters of one frame (the reference's CTR_* layout, trimmed).

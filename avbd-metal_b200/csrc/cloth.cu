@@ -386,6 +386,16 @@ __global__ void __launch_bounds__(128) k_rt_emit(const Params P, const DevPtrs d
                 int nf = 0;
                 if (sk == AVBD_SHAPE_SPHERE) {
                     fw[0] = po; fr[0] = sh.x * 0.5f; fid[0] = 8; nf = 1;
+                } else if (sk == AVBD_SHAPE_CAPSULE) {
+                    // three spheres along the axis (a torus has no feature
+                    // points: 25_cloth.metal:957-971)
+                    const float half_ = sh.x * 0.5f, r = sh.y;
+                    const float3 ax = q_rotate(qo, mk3(0, 0, 1));
+                    for (int i = -1; i <= 1; i++) {
+                        const float3 w = po + ax * (half_ * (float)i);
+                        if (dist3(w, m) > rT + r + 4.0f * P.collisionMargin) continue;
+                        fw[nf] = w; fr[nf] = r; fid[nf] = (uint32_t)(9 + i + 1); nf++;
+                    }
                 } else if (sk == AVBD_SHAPE_BOX) {
                     const float3 h3 = xyz(sh) * 0.5f;
                     for (uint32_t i = 0; i < 8; i++) {

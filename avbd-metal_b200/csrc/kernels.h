@@ -20,6 +20,8 @@ struct DevPtrs {
     uint32_t *colOwner, *colShapeType, *colGroup, *colShared;
     float4 *colShape, *colLocalPos, *colLocalRot;
     float2* colFriction;
+    uint2* colHullRange;                  // (first vertex, vertex count); count 0 = analytic shape
+    float4* hullVerts;                    // convex hull vertices in the collider frame
     uint32_t *hashedIdx, *globalIdx;
     uint32_t* exclusions;                 // uint2 pairs
     // broadphase

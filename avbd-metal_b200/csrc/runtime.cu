@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/avbd.h"
+#include "dmath.cuh"
 #include "kernels.h"
 #include "upload.h"
 
@@ -59,6 +60,43 @@ __global__ void k_set_motor_targets(JointGPU* joints, const uint32_t* ids, const
     JointGPU& j = joints[ids[i]];
     if ((j.header.w & MOTOR_MODE_MASK) == 0u) return;   // welded/disabled: a no-op
     j.motor.x = targets[i];
+}
+
+// World anchors (rA.xyz), velocity commands (motor.x) and effort limits
+// (motor.y) of listed joints; the host has validated every entry.
+__global__ void k_set_joint_anchors(JointGPU* joints, const uint32_t* ids, const float* xyz, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    JointGPU& j = joints[ids[i]];
+    j.rA.x = xyz[3 * i];
+    j.rA.y = xyz[3 * i + 1];
+    j.rA.z = xyz[3 * i + 2];
+}
+__global__ void k_set_motor_field(JointGPU* joints, const uint32_t* ids, const float* v, uint32_t n, int torque) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    JointGPU& j = joints[ids[i]];
+    if (torque) j.motor.y = v[i];
+    else j.motor.x = v[i];
+}
+
+// Hinge twist angle of child against parent and the twist rate about the
+// child's hinge axis (GPUSolver.swift:2606-2637).
+__global__ void k_motor_states(const JointGPU* joints, const float4* posAng, const float4* velAng,
+                               const uint32_t* ids, uint32_t n, float* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const JointGPU& j = joints[ids[i]];
+    const uint32_t a = j.header.x, b = j.header.y;
+    const float4 qB = posAng[b];
+    const float4 qA = a == WORLD_BODY ? make_float4(0, 0, 0, 1) : posAng[a];
+    float4 r = q_mul(q_inv(q_mul(qA, tof(j.restRel))), qB);
+    if (r.w < 0.0f) r = neg4(r);
+    const float3 axis = xyz(tof(j.hingeAxis));
+    out[2 * i] = 2.0f * atan2_series(dot(xyz(r), axis), r.w);
+    const float3 wB = xyz(velAng[b]);
+    const float3 wA = a == WORLD_BODY ? s3(0) : xyz(velAng[a]);
+    out[2 * i + 1] = dot(wB - wA, q_rotate(qB, axis));
 }
 }  // namespace
 
@@ -465,6 +503,8 @@ struct avbd_solver {
         ok = ok && upload(reinterpret_cast<f4*&>(d.colLocalPos), H.colLocalPos, "colliderLocalPosition");
         ok = ok && upload(reinterpret_cast<f4*&>(d.colLocalRot), H.colLocalRot, "colliderLocalRotation");
         ok = ok && upload(reinterpret_cast<float*&>(d.colFriction), H.colFriction, "colliderFriction");
+        ok = ok && upload(reinterpret_cast<uint32_t*&>(d.colHullRange), H.colHullRange, "colliderHullRange");
+        ok = ok && upload(reinterpret_cast<f4*&>(d.hullVerts), H.hullVerts, "convexHullVertices");
         ok = ok && upload(d.hashedIdx, H.hashedIdx, "hashedIdx") && upload(d.globalIdx, H.globalIdx, "globalIdx");
         ok = ok && upload(d.exclusions, H.exclusions, "exclusions");
         // broadphase
@@ -929,6 +969,81 @@ int avbd_set_motor_targets(avbd_solver* s, const uint32_t* joints, uint32_t n, c
     k_set_motor_targets<<<(n + 127) / 128, 128, 0, s->launch>>>(s->d.joints, reinterpret_cast<uint32_t*>(st),
                                                                  reinterpret_cast<float*>(st + 4 * (size_t)n), n);
     return s->check(cudaGetLastError(), "motor targets") ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+}
+
+namespace {
+// Copies ids and n * width floats into staging and launches one setter.
+int joint_update(avbd_solver* s, const uint32_t* joints, uint32_t n, const float* vals, int width, int which,
+                 const char* label) {
+    if (n == 0) return AVBD_OK;
+    if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
+    const size_t idBytes = 4 * (size_t)n, valBytes = 4 * (size_t)n * width;
+    const size_t valOff = (idBytes + 15) & ~(size_t)15;
+    uint8_t* st = static_cast<uint8_t*>(s->staging(valOff + valBytes + 16));
+    if (!st) return AVBD_ERR_ALLOC_FAILED;
+    cudaMemcpyAsync(st, joints, idBytes, cudaMemcpyHostToDevice, s->launch);
+    cudaMemcpyAsync(st + valOff, vals, valBytes, cudaMemcpyHostToDevice, s->launch);
+    const uint32_t* ids = reinterpret_cast<uint32_t*>(st);
+    const float* v = reinterpret_cast<float*>(st + valOff);
+    if (which == 0) k_set_joint_anchors<<<(n + 127) / 128, 128, 0, s->launch>>>(s->d.joints, ids, v, n);
+    else k_set_motor_field<<<(n + 127) / 128, 128, 0, s->launch>>>(s->d.joints, ids, v, n, which == 2 ? 1 : 0);
+    return s->check(cudaGetLastError(), label) ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+}
+}  // namespace
+
+int avbd_set_joint_world_anchors(avbd_solver* s, const uint32_t* joints, uint32_t n, const float* points_xyz) {
+    if (!s || (n && (!joints || !points_xyz))) return AVBD_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < n; i++) {
+        if (joints[i] >= s->H.joints.size()) return AVBD_ERR_INVALID_ARGUMENT;
+        for (int k = 0; k < 3; k++)
+            if (!std::isfinite(points_xyz[3 * i + k])) return AVBD_ERR_INVALID_ARGUMENT;
+    }
+    return joint_update(s, joints, n, points_xyz, 3, 0, "joint anchors");
+}
+
+int avbd_set_motor_velocities(avbd_solver* s, const uint32_t* joints, uint32_t n, const float* rad_per_s) {
+    if (!s || (n && (!joints || !rad_per_s))) return AVBD_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < n; i++) {
+        if (joints[i] >= s->H.joints.size() || !std::isfinite(rad_per_s[i])) return AVBD_ERR_INVALID_ARGUMENT;
+        if ((s->H.joints[joints[i]].header.w & MOTOR_MODE_MASK) != MOTOR_VELOCITY) return AVBD_ERR_INVALID_ARGUMENT;
+    }
+    return joint_update(s, joints, n, rad_per_s, 1, 1, "motor velocities");
+}
+
+int avbd_set_motor_torques(avbd_solver* s, const uint32_t* joints, uint32_t n, const float* torques) {
+    if (!s || (n && (!joints || !torques))) return AVBD_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < n; i++) {
+        if (joints[i] >= s->H.joints.size() || !std::isfinite(torques[i]) || torques[i] < 0.0f) return AVBD_ERR_INVALID_ARGUMENT;
+        const JointGPU& j = s->H.joints[joints[i]];
+        if ((j.header.w & MOTOR_MODE_MASK) == 0) return AVBD_ERR_INVALID_ARGUMENT;  // no authored motor
+        // a joint authored with zero stiffness and zero effort is never
+        // solved (no stage reads it); raising its effort is not supported
+        if (j.rA.w == 0.0f && j.rB.w == 0.0f && j.motor.y == 0.0f && torques[i] > 0.0f) return AVBD_ERR_UNSUPPORTED;
+    }
+    return joint_update(s, joints, n, torques, 1, 2, "motor torques");
+}
+
+int avbd_get_motor_states(avbd_solver* s, const uint32_t* joints, uint32_t n, float* angles, float* velocities) {
+    if (!s || (n && (!joints || !angles || !velocities))) return AVBD_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < n; i++)
+        if (joints[i] >= s->H.joints.size()) return AVBD_ERR_INVALID_ARGUMENT;
+    if (n == 0) return AVBD_OK;
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    const size_t idBytes = ((4 * (size_t)n) + 15) & ~(size_t)15;
+    uint8_t* st = static_cast<uint8_t*>(s->staging(idBytes + 8 * (size_t)n + 16));
+    if (!st) return AVBD_ERR_ALLOC_FAILED;
+    float* dOut = reinterpret_cast<float*>(st + idBytes);
+    cudaMemcpyAsync(st, joints, 4 * (size_t)n, cudaMemcpyHostToDevice, s->launch);
+    k_motor_states<<<(n + 127) / 128, 128, 0, s->launch>>>(s->d.joints, s->d.posAng, s->d.velAng,
+                                                           reinterpret_cast<uint32_t*>(st), n, dOut);
+    std::vector<float> out(2 * (size_t)n);
+    if (!s->check(cudaGetLastError(), "motor states") ||
+        !s->check(cudaMemcpyAsync(out.data(), dOut, 8 * (size_t)n, cudaMemcpyDeviceToHost, s->launch), "motor states readback") ||
+        !s->check(cudaStreamSynchronize(s->launch), "motor states"))
+        return AVBD_ERR_RUNTIME_FAILURE;
+    for (uint32_t i = 0; i < n; i++) { angles[i] = out[2 * i]; velocities[i] = out[2 * i + 1]; }
+    return AVBD_OK;
 }
 
 int avbd_max_constraint_error(avbd_solver* s, float* out) {

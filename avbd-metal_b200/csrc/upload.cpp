@@ -52,7 +52,17 @@ bool desc_dynamic(const avbd_body_desc& b) {
     return b.has_explicit_mass ? b.mass > 0.0f : b.density > 0.0f;
 }
 
-float collider_radius(const avbd_collider_desc& c) {
+// Bounding radius of a collider about its origin (GPUSolver.swift:993-1002):
+// the farthest hull vertex for a convex hull.
+float collider_radius(const avbd_scene_desc* s, const avbd_collider_desc& c) {
+    if (c.hull_count > 0) {
+        float r = 0.0f;
+        for (uint32_t k = 0; k < c.hull_count; k++) {
+            const float* v = s->hull_vertices + 3 * (size_t)(c.hull_offset + k);
+            r = std::max(r, length(V3{v[0], v[1], v[2]}));
+        }
+        return r;
+    }
     V3 sz = from(c.size);
     if (c.shape == AVBD_SHAPE_SPHERE) return sz.x / 2.0f;
     if (c.shape == AVBD_SHAPE_TORUS) return sz.x + sz.y;
@@ -359,11 +369,17 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
     for (uint32_t i = 0; i < nc; i++) {
         const avbd_collider_desc& c = s->colliders[i];
         if (c.body < 0 || (uint32_t)c.body >= nb) { err = "collider owner out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
-        if (c.collision_enabled && (c.hull_count > 0 || c.shape == AVBD_SHAPE_TORUS || c.shape == AVBD_SHAPE_CAPSULE)) {
-            err = "torus, capsule and convex-hull colliders are not supported by this build";
-            return AVBD_ERR_UNSUPPORTED;
+        if (c.shape > AVBD_SHAPE_CAPSULE) { err = "unknown collider shape"; return AVBD_ERR_INVALID_ARGUMENT; }
+        if (c.hull_count > 0) {
+            // GPUSolver.swift:1023-1024 and Scene.swift:656-657
+            if (c.hull_count < 4 || c.hull_count > 64) { err = "a convex collider needs 4...64 hull vertices"; return AVBD_ERR_INVALID_ARGUMENT; }
+            if (!s->hull_vertices || (uint64_t)c.hull_offset + c.hull_count > s->num_hull_vertices) { err = "hull vertex range out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
+            for (uint32_t k = 0; k < 3 * c.hull_count; k++)
+                if (!std::isfinite(s->hull_vertices[3 * (size_t)c.hull_offset + k])) { err = "convex collider vertices must be finite"; return AVBD_ERR_INVALID_ARGUMENT; }
         }
     }
+    for (uint32_t i = 0; i < nb; i++)
+        if (s->bodies[i].shape > AVBD_SHAPE_CAPSULE) { err = "unknown body shape"; return AVBD_ERR_INVALID_ARGUMENT; }
     for (uint32_t i = 0; i < s->num_tris; i++)
         for (int k = 0; k < 3; k++)
             if (s->tris[i].ids[k] < 0 || (uint32_t)s->tris[i].ids[k] >= nb) { err = "triangle vertex out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
@@ -448,10 +464,12 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
     H.colOwner.assign(nc, 0); H.colShapeType.assign(nc, 0); H.colGroup.assign(nc, 0);
     H.colShared.assign(nc, 0); H.colShape.assign(nc, f4{}); H.colLocalPos.assign(nc, f4{});
     H.colLocalRot.assign(nc, f4{}); H.colFriction.assign(2 * nc, 0.0f);
+    H.colHullRange.assign(2 * nc, 0u);
+    H.hullVerts.clear();
     std::vector<float> radii;
     for (uint32_t i = 0; i < nc; i++) {
         const avbd_collider_desc& c = s->colliders[i];
-        float r = collider_radius(c);
+        float r = collider_radius(s, c);
         bool particle = s->bodies[c.body].is_particle != 0;
         H.colOwner[i] = (uint32_t)c.body;
         H.colGroup[i] = c.collision_group;
@@ -462,6 +480,16 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
         H.colFriction[2 * i] = c.friction;
         H.colFriction[2 * i + 1] = c.dynamic_friction;
         uint32_t flags = c.shape;
+        if (c.hull_count > 0) {
+            // hulls are packed in collider order (GPUSolver.swift:1020-1032)
+            H.colHullRange[2 * i] = (uint32_t)H.hullVerts.size();
+            H.colHullRange[2 * i + 1] = c.hull_count;
+            for (uint32_t k = 0; k < c.hull_count; k++) {
+                const float* v = s->hull_vertices + 3 * (size_t)(c.hull_offset + k);
+                H.hullVerts.push_back(f4{v[0], v[1], v[2], 0.0f});
+            }
+            flags = 4u;
+        }
         if (particle) flags |= SHAPE_PARTICLE;
         if (c.world_round_anchor) flags |= COLLIDER_WORLD_ROUND_ANCHOR;
         H.colShapeType[i] = flags;
@@ -477,7 +505,7 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
     for (uint32_t i = 0; i < nc; i++) {
         const avbd_collider_desc& c = s->colliders[i];
         if (!c.collision_enabled) continue;
-        if (collider_radius(c) > threshold || (isolated && c.collision_group == 0)) H.globalIdx.push_back(i);
+        if (collider_radius(s, c) > threshold || (isolated && c.collision_group == 0)) H.globalIdx.push_back(i);
         else H.hashedIdx.push_back(i);
     }
     float maxHashedRadius = 0.05f, maxParticleRadius = 0.0f;
@@ -608,7 +636,7 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
         for (uint32_t i = 0; i < nc; i++) {
             const avbd_collider_desc& c = s->colliders[i];
             if (!c.collision_enabled || s->bodies[c.body].is_particle) continue;
-            const bool slab = !H.isDynamic[c.body] && c.shape == AVBD_SHAPE_BOX && c.size[0] >= 20.0f && c.size[1] >= 20.0f;
+            const bool slab = !H.isDynamic[c.body] && c.shape == AVBD_SHAPE_BOX && c.hull_count == 0 && c.size[0] >= 20.0f && c.size[1] >= 20.0f;
             rigidReach = rigidReach || !slab;
         }
         H.ogc = H.cloth || groups.size() > 1 || self || rigidReach;
@@ -741,6 +769,9 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
     P.numHashed = (uint32_t)H.hashedIdx.size();
     P.numGlobals = (uint32_t)H.globalIdx.size();
     P.numHashedRigid = numHashedRigid;
+    P.roundShapes = 0u;
+    for (uint32_t i = 0; i < nc; i++)
+        if ((H.colShapeType[i] & SHAPE_KIND_MASK) >= 2u) P.roundShapes = 1u;
     // Particle grid: when the coarse cells (twice the largest hashed radius,
     // at least 0.1 m) are well above the particles, particle candidates come
     // from cells just above twice the largest particle radius (two

@@ -30,6 +30,8 @@ struct HostScene {
     std::vector<uint32_t> colOwner, colShapeType, colGroup, colShared;
     std::vector<f4> colShape, colLocalPos, colLocalRot;
     std::vector<float> colFriction;  // (static, dynamic) pairs
+    std::vector<uint32_t> colHullRange;  // (first vertex, vertex count) pairs
+    std::vector<f4> hullVerts;
     std::vector<uint32_t> hashedIdx, globalIdx;
 
     // constraints

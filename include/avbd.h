@@ -302,6 +302,30 @@ int avbd_set_positions(avbd_solver* solver, uint32_t n, const float* pos_xyz);
 int avbd_set_motor_targets(avbd_solver* solver, const uint32_t* joints,
                            uint32_t n, const float* targets);
 
+/* World anchor of each listed joint (its rA, the world point of a joint to
+ * the world) from xyz triples (`setJointWorldAnchors`,
+ * GPUSolver.swift:2481-2494).                                             */
+int avbd_set_joint_world_anchors(avbd_solver* solver, const uint32_t* joints,
+                                 uint32_t n, const float* points_xyz);
+
+/* Commands of velocity motors in rad/s (`setMotorVelocities`,
+ * GPUSolver.swift:2534-2551); every listed joint must carry a velocity
+ * motor.                                                                  */
+int avbd_set_motor_velocities(avbd_solver* solver, const uint32_t* joints,
+                              uint32_t n, const float* rad_per_s);
+
+/* Effort limits of authored motors (`setMotorTorques`,
+ * GPUSolver.swift:2564-2578): finite and non-negative.  Raising the limit
+ * of a joint authored with zero stiffness and zero effort (a joint no stage
+ * solves) returns AVBD_ERR_UNSUPPORTED.                                   */
+int avbd_set_motor_torques(avbd_solver* solver, const uint32_t* joints,
+                           uint32_t n, const float* torques);
+
+/* Hinge twist angle and twist rate of each listed joint (`motorStates`,
+ * GPUSolver.swift:2606-2637).                                             */
+int avbd_get_motor_states(avbd_solver* solver, const uint32_t* joints,
+                          uint32_t n, float* angles, float* velocities);
+
 /* Largest joint violation / contact penetration (`maxConstraintErrorChecked`,
  * GPUSolver.swift:4819-4865; kernel 40_solver.metal:2189-2229).            */
 int avbd_max_constraint_error(avbd_solver* solver, float* out);

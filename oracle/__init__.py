@@ -48,6 +48,9 @@ def lib():
         _lib.oracle_get_positions.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
         _lib.oracle_get_body_states.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
         _lib.oracle_set_motor_targets.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        for name in ("oracle_set_joint_world_anchors", "oracle_set_motor_velocities", "oracle_set_motor_torques"):
+            getattr(_lib, name).argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        _lib.oracle_get_motor_states.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
         _lib.oracle_max_constraint_error.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
         _lib.oracle_get_counters.argtypes = [C.c_void_p, C.c_void_p]
         _lib.oracle_debug_buffer_size.argtypes = [C.c_void_p, C.c_int]
@@ -115,6 +118,28 @@ class OracleSolver:
         ids = np.ascontiguousarray(joints, dtype=np.uint32)
         t = np.ascontiguousarray(targets, dtype=np.float32)
         lib().oracle_set_motor_targets(self._h, ids.ctypes.data, len(ids), t.ctypes.data)
+
+    def set_joint_world_anchors(self, joints, points):
+        ids = np.ascontiguousarray(joints, dtype=np.uint32)
+        p = np.ascontiguousarray(points, dtype=np.float32).reshape(-1)
+        lib().oracle_set_joint_world_anchors(self._h, ids.ctypes.data, len(ids), p.ctypes.data)
+
+    def set_motor_velocities(self, joints, rad_per_s):
+        ids = np.ascontiguousarray(joints, dtype=np.uint32)
+        v = np.ascontiguousarray(rad_per_s, dtype=np.float32)
+        lib().oracle_set_motor_velocities(self._h, ids.ctypes.data, len(ids), v.ctypes.data)
+
+    def set_motor_torques(self, joints, torques):
+        ids = np.ascontiguousarray(joints, dtype=np.uint32)
+        t = np.ascontiguousarray(torques, dtype=np.float32)
+        lib().oracle_set_motor_torques(self._h, ids.ctypes.data, len(ids), t.ctypes.data)
+
+    def motor_states(self, joints):
+        ids = np.ascontiguousarray(joints, dtype=np.uint32)
+        a = np.zeros(len(ids), np.float32)
+        v = np.zeros(len(ids), np.float32)
+        lib().oracle_get_motor_states(self._h, ids.ctypes.data, len(ids), a.ctypes.data, v.ctypes.data)
+        return a, v
 
     def max_constraint_error(self) -> float:
         v = C.c_float()

@@ -41,11 +41,16 @@ int Solver::create(const avbd_scene_desc* s) {
     for (uint32_t i = 0; i < nc; i++) {
         const avbd_collider_desc& c = s->colliders[i];
         if (c.body < 0 || (uint32_t)c.body >= nb) { error = "collider owner out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
-        if (c.collision_enabled && (c.hull_count > 0 || c.shape == AVBD_SHAPE_TORUS || c.shape == AVBD_SHAPE_CAPSULE)) {
-            error = "torus, capsule and convex-hull colliders are not supported by this build";
-            return AVBD_ERR_UNSUPPORTED;
+        if (c.shape > AVBD_SHAPE_CAPSULE) { error = "unknown collider shape"; return AVBD_ERR_INVALID_ARGUMENT; }
+        if (c.hull_count > 0) {
+            if (c.hull_count < 4 || c.hull_count > 64) { error = "a convex collider needs 4...64 hull vertices"; return AVBD_ERR_INVALID_ARGUMENT; }
+            if (!s->hull_vertices || (uint64_t)c.hull_offset + c.hull_count > s->num_hull_vertices) { error = "hull vertex range out of range"; return AVBD_ERR_INVALID_ARGUMENT; }
+            for (uint32_t k = 0; k < 3 * c.hull_count; k++)
+                if (!std::isfinite(s->hull_vertices[3 * (size_t)c.hull_offset + k])) { error = "convex collider vertices must be finite"; return AVBD_ERR_INVALID_ARGUMENT; }
         }
     }
+    for (uint32_t i = 0; i < nb; i++)
+        if (s->bodies[i].shape > AVBD_SHAPE_CAPSULE) { error = "unknown body shape"; return AVBD_ERR_INVALID_ARGUMENT; }
 
     uint32_t enabled = 0;
     for (uint32_t i = 0; i < nc; i++) enabled += s->colliders[i].collision_enabled ? 1u : 0u;
@@ -120,7 +125,18 @@ int Solver::create(const avbd_scene_desc* s) {
     colOwner.assign(nc, 0); colShapeType.assign(nc, 0); colGroup.assign(nc, 0); colShared.assign(nc, 0);
     colShape.assign(nc, F4{}); colLocalPos.assign(nc, F4{}); colLocalRot.assign(nc, F4{});
     colFrictionS.assign(nc, 0); colFrictionD.assign(nc, 0);
-    auto collider_radius = [](const avbd_collider_desc& c) -> float {
+    colHullFirst.assign(nc, 0); colHullCount.assign(nc, 0); hullVerts.clear();
+    // bounding radius about the collider origin; the farthest hull vertex
+    // for a convex hull (GPUSolver.swift:993-1002)
+    auto collider_radius = [s](const avbd_collider_desc& c) -> float {
+        if (c.hull_count > 0) {
+            float r = 0.0f;
+            for (uint32_t k = 0; k < c.hull_count; k++) {
+                const float* v = s->hull_vertices + 3 * (size_t)(c.hull_offset + k);
+                r = std::max(r, length(f3(v[0], v[1], v[2])));
+            }
+            return r;
+        }
         F3 sz = f3(c.size[0], c.size[1], c.size[2]);
         if (c.shape == AVBD_SHAPE_SPHERE) return sz.x / 2.0f;
         if (c.shape == AVBD_SHAPE_TORUS) return sz.x + sz.y;
@@ -141,6 +157,15 @@ int Solver::create(const avbd_scene_desc* s) {
         colFrictionS[i] = c.friction;
         colFrictionD[i] = c.dynamic_friction;
         uint32_t flags = c.shape;
+        if (c.hull_count > 0) {
+            colHullFirst[i] = (uint32_t)hullVerts.size();
+            colHullCount[i] = c.hull_count;
+            for (uint32_t k = 0; k < c.hull_count; k++) {
+                const float* v = s->hull_vertices + 3 * (size_t)(c.hull_offset + k);
+                hullVerts.push_back(f3(v[0], v[1], v[2]));
+            }
+            flags = 4u;
+        }
         if (particle) flags |= 0x10u;
         if (c.world_round_anchor) flags |= 0x20u;
         colShapeType[i] = flags;
@@ -303,7 +328,7 @@ int Solver::create(const avbd_scene_desc* s) {
         for (uint32_t i = 0; i < nc; i++) {
             const avbd_collider_desc& c = s->colliders[i];
             if (!c.collision_enabled || isParticle[c.body]) continue;
-            bool slab = !isDynamic[c.body] && c.shape == AVBD_SHAPE_BOX && c.size[0] >= 20.0f && c.size[1] >= 20.0f;
+            bool slab = !isDynamic[c.body] && c.shape == AVBD_SHAPE_BOX && c.hull_count == 0 && c.size[0] >= 20.0f && c.size[1] >= 20.0f;
             rigidReach = rigidReach || !slab;
         }
         ogcCandidate = cloth || groups.size() > 1 || self || rigidReach;
@@ -717,6 +742,481 @@ int Solver::map_find(uint32_t a, uint32_t b) const {
     return -1;
 }
 
+// --------------------------------------------------------------------------
+// Convex hull vs box, capsule and torus pairs (30_narrowphase.metal:189-340,
+// :430-975).  Same contact rules as the sphere and box paths: feature-keyed
+// warm start for hulls, proximity-matched for the round shapes.
+// --------------------------------------------------------------------------
+struct NPair {
+    uint32_t ia, ib, ba, bb;
+    F4 bodyPA, bodyPB, qBodyA, qBodyB, qA, qB;
+    F3 vA, vB;
+    Box A, B;
+};
+
+static void emit_feature_manifold(const Solver& S, const NPair& p, ManifoldGPU& outM,
+                                  const NPContact* contacts, int count, F3 nrm) {
+    const Params& P = S.P;
+    F3 t1, t2;
+    orthonormal(nrm, t1, t2);
+    float sf = combine_friction(S.colFrictionS[p.ia], S.colFrictionS[p.ib], P.frictionCombineMode);
+    float df = combine_friction(S.colFrictionD[p.ia], S.colFrictionD[p.ib], P.frictionCombineMode);
+    int prev = S.map_find(p.ia, p.ib);
+    outM.header = U4{p.ba, p.bb, (uint32_t)count, 1u};
+    outM.basisN = f4(nrm, df);
+    outM.basisT1 = f4(t1, sf);
+    float warm = P.alpha * P.gamma;
+    F4 qAc = q_conj(p.qBodyA), qBc = q_conj(p.qBodyB);
+    for (int i = 0; i < count; i++) {
+        F3 rA = q_rotate(qAc, contacts[i].xA - xyz(p.bodyPA));
+        F3 rB = q_rotate(qBc, contacts[i].xB - xyz(p.bodyPB));
+        F3 lambda = f3s(0), penalty = f3s(0);
+        float stick = 0.0f;
+        if (prev >= 0) {
+            const ManifoldGPU& pm = S.prevManifolds[prev];
+            for (uint32_t j = 0; j < pm.header.z; j++) {
+                if (fbits(pm.contacts[j].rA.w) == contacts[i].feature) {
+                    lambda = xyz(pm.contacts[j].lambda);
+                    penalty = xyz(pm.contacts[j].penalty);
+                    stick = pm.contacts[j].rB.w;
+                    if (stick != 0.0f) { rA = xyz(pm.contacts[j].rA); rB = xyz(pm.contacts[j].rB); }
+                    break;
+                }
+            }
+        }
+        F3 xAw = xform(xyz(p.bodyPA), p.qBodyA, rA);
+        F3 xBw = xform(xyz(p.bodyPB), p.qBodyB, rB);
+        F3 d = xAw - xBw;
+        F3 C0 = f3(dot(nrm, d) + P.collisionMargin, dot(t1, d), dot(t2, d));
+        float sx, sy;
+        spin_shift(S.spinVel[p.ba], S.spinVel[p.bb], xAw - xyz(p.bodyPA), xBw - xyz(p.bodyPB), t1, t2, P.dt, P.alpha, sx, sy);
+        C0.y -= sx; C0.z -= sy;
+        lambda *= warm;
+        penalty = clamp3(penalty * P.gamma, penalty_floor(S, p.ba, p.bb), f3(PENALTY_MAX, PENALTY_MAX_T, PENALTY_MAX_T));
+        outM.contacts[i].rA = f4(rA, bitsf(contacts[i].feature));
+        outM.contacts[i].rB = f4(rB, stick);
+        outM.contacts[i].C0 = f4(C0, 0);
+        outM.contacts[i].lambda = f4(lambda, 0);
+        outM.contacts[i].penalty = f4(penalty, 0);
+    }
+}
+
+// keepAnchors: capsules keep sticking anchors only between two
+// material-anchored colliders (:711-724); tori never (:944-962).
+static void emit_round_manifold(const Solver& S, const NPair& p, ManifoldGPU& outM, const NPContact* contacts,
+                                int count, F3 nrm, float matchDist, bool capsuleRule) {
+    const Params& P = S.P;
+    F3 t1, t2;
+    orthonormal(nrm, t1, t2);
+    float sf = combine_friction(S.colFrictionS[p.ia], S.colFrictionS[p.ib], P.frictionCombineMode);
+    float df = combine_friction(S.colFrictionD[p.ia], S.colFrictionD[p.ib], P.frictionCombineMode);
+    int prev = S.map_find(p.ia, p.ib);
+    bool roundA = (S.colShapeType[p.ia] & 0x20u) != 0, roundB = (S.colShapeType[p.ib] & 0x20u) != 0;
+    outM.header = U4{p.ba, p.bb, (uint32_t)count, 1u | (roundA ? 2u : 0u) | (roundB ? 4u : 0u)};
+    outM.basisN = f4(nrm, df);
+    outM.basisT1 = f4(t1, sf);
+    float warm = P.alpha * P.gamma;
+    bool keepAnchors = capsuleRule && !roundA && !roundB;
+    F4 qAc = q_conj(p.qBodyA), qBc = q_conj(p.qBodyB);
+    for (int i = 0; i < count; i++) {
+        F3 rA_ = roundA ? contacts[i].xA - xyz(p.bodyPA) : q_rotate(qAc, contacts[i].xA - xyz(p.bodyPA));
+        F3 rB_ = roundB ? contacts[i].xB - xyz(p.bodyPB) : q_rotate(qBc, contacts[i].xB - xyz(p.bodyPB));
+        F3 lambda = f3s(0), penalty = f3s(0);
+        float stick = 0.0f;
+        if (prev >= 0) {
+            const ManifoldGPU& pm = S.prevManifolds[prev];
+            float bestD = matchDist;
+            int bestJ = -1;
+            for (uint32_t j = 0; j < pm.header.z; j++) {
+                float dj = distance(xyz(pm.contacts[j].rA), rA_);
+                if (dj < bestD) { bestD = dj; bestJ = (int)j; }
+            }
+            if (bestJ >= 0) {
+                lambda = xyz(pm.contacts[bestJ].lambda);
+                penalty = xyz(pm.contacts[bestJ].penalty);
+                F3 t1o = xyz(pm.basisT1);
+                F3 t2o = cross(xyz(pm.basisN), t1o);
+                F3 lt = t1o * lambda.y + t2o * lambda.z;
+                lambda.y = dot(t1, lt);
+                lambda.z = dot(t2, lt);
+                if (keepAnchors) {
+                    stick = pm.contacts[bestJ].rB.w;
+                    if (stick != 0.0f) { rA_ = xyz(pm.contacts[bestJ].rA); rB_ = xyz(pm.contacts[bestJ].rB); }
+                }
+            }
+        }
+        F3 xAw = roundA ? xyz(p.bodyPA) + rA_ : xform(xyz(p.bodyPA), p.qBodyA, rA_);
+        F3 xBw = roundB ? xyz(p.bodyPB) + rB_ : xform(xyz(p.bodyPB), p.qBodyB, rB_);
+        F3 d = xAw - xBw;
+        F3 C0 = f3(dot(nrm, d) + P.collisionMargin, dot(t1, d), dot(t2, d));
+        float sx, sy;
+        spin_shift(S.spinVel[p.ba], S.spinVel[p.bb], xAw - xyz(p.bodyPA), xBw - xyz(p.bodyPB), t1, t2, P.dt, P.alpha, sx, sy);
+        C0.y -= sx; C0.z -= sy;
+        lambda *= warm;
+        penalty = clamp3(penalty * P.gamma, penalty_floor(S, p.ba, p.bb), f3(PENALTY_MAX, PENALTY_MAX_T, PENALTY_MAX_T));
+        outM.contacts[i].rA = f4(rA_, bitsf(contacts[i].feature));
+        outM.contacts[i].rB = f4(rB_, stick);
+        outM.contacts[i].C0 = f4(C0, 0);
+        outM.contacts[i].lambda = f4(lambda, 0);
+        outM.contacts[i].penalty = f4(penalty, 0);
+    }
+}
+
+static int min_axis(F3 v) {
+    int a = 0;
+    if (v.y < comp(v, a)) a = 1;
+    if (v.z < comp(v, a)) a = 2;
+    return a;
+}
+
+// 30_narrowphase.metal:286-290
+static F3 closest_on_segment(F3 p, F3 a, F3 b) {
+    F3 ab = b - a;
+    float t = clampf_(dot(p - a, ab) / fmax_(dot(ab, ab), 1e-12f), 0.0f, 1.0f);
+    return a + ab * t;
+}
+
+struct HullCand { F3 xHull, xBox, boxToHull; float sep; uint32_t feature; };
+
+// 30_narrowphase.metal:203-246
+static bool hull_vertex_box(F3 vw, uint32_t vid, const Box& box, F4 qBox, F3 rel, float hullR, float boxR,
+                            const Params& P, HullCand& out) {
+    F3 local = q_rotate(q_conj(qBox), vw - box.center);
+    F3 h = box.half;
+    F3 cl = clamp3(local, -h, h);
+    F3 nL, bL;
+    float sep;
+    bool inside = local.x >= -h.x && local.y >= -h.y && local.z >= -h.z &&
+                  local.x <= h.x && local.y <= h.y && local.z <= h.z;
+    if (inside) {
+        F3 clr = h - abs3(local);
+        int axis = min_axis(clr);
+        nL = f3s(0);
+        setcomp(nL, axis, comp(local, axis) >= 0.0f ? 1.0f : -1.0f);
+        bL = local;
+        setcomp(bL, axis, comp(nL, axis) * comp(h, axis));
+        sep = -comp(clr, axis);
+    } else {
+        F3 dl = local - cl;
+        float dist = length(dl);
+        if (dist < 1e-8f) return false;
+        nL = dl / dist;
+        float det = detect_margin(q_rotate(qBox, nL), rel, P, hullR, boxR);
+        if (dist > det) return false;
+        bL = cl;
+        sep = dist;
+    }
+    out.xHull = vw;
+    out.xBox = q_rotate(qBox, bL) + box.center;
+    out.boxToHull = q_rotate(qBox, nL);
+    out.sep = sep;
+    out.feature = (4u << 24) | (vid & 0x00FFFFFFu);
+    return true;
+}
+
+// 30_narrowphase.metal:430-545
+static void narrow_hull(const Solver& S, const NPair& p, ManifoldGPU& outM, uint32_t stA, uint32_t stB) {
+    const Params& P = S.P;
+    bool hIsA = stA == 4;
+    if ((stA == 4 && stB == 4) || (hIsA ? stB : stA) != 0) { outM.header = U4{p.ba, p.bb, 0, 0}; return; }
+    uint32_t ih = hIsA ? p.ia : p.ib;
+    F4 qH = hIsA ? p.qA : p.qB;
+    F3 pH = hIsA ? p.A.center : p.B.center;
+    const Box& box = hIsA ? p.B : p.A;
+    F4 qBox = hIsA ? p.qB : p.qA;
+    F3 rel = hIsA ? (p.vA - p.vB) : (p.vB - p.vA);
+    float hullR = std::fabs(S.colShape[ih].w);
+    float boxR = std::fabs(S.colShape[hIsA ? p.ib : p.ia].w);
+    uint32_t first = S.colHullFirst[ih], nv = S.colHullCount[ih];
+    auto candidate = [&](uint32_t v, HullCand& c) {
+        F3 vw = pH + q_rotate(qH, S.hullVerts[first + v]);
+        return hull_vertex_box(vw, v, box, qBox, rel, hullR, boxR, P, c);
+    };
+    HullCand best{};
+    bool have = false;
+    for (uint32_t v = 0; v < nv; v++) {
+        HullCand c;
+        if (!candidate(v, c)) continue;
+        if (!have || c.sep < best.sep - 1e-8f || (std::fabs(c.sep - best.sep) <= 1e-8f && c.feature < best.feature)) {
+            best = c;
+            have = true;
+        }
+    }
+    if (!have) { outM.header = U4{p.ba, p.bb, 0, 0}; return; }
+    HullCand chosen[MAX_CONTACTS];
+    int count = 1;
+    chosen[0] = best;
+    float band = 0.75f * P.collisionMargin;
+    while (count < MAX_CONTACTS) {
+        HullCand next{};
+        bool haveNext = false;
+        float bestSpread = -1.0f;
+        for (uint32_t v = 0; v < nv; v++) {
+            HullCand c;
+            if (!candidate(v, c)) continue;
+            if (c.sep > best.sep + band || dot(c.boxToHull, best.boxToHull) < 0.98f) continue;
+            bool dup = false;
+            float minSpread = FLT_MAX;
+            for (int j = 0; j < count; j++) {
+                if (c.feature == chosen[j].feature) { dup = true; break; }
+                F3 dd = c.xHull - chosen[j].xHull;
+                dd = dd - best.boxToHull * dot(best.boxToHull, dd);
+                minSpread = fmin_(minSpread, dot(dd, dd));
+            }
+            if (dup) continue;
+            if (!haveNext || minSpread > bestSpread + 1e-10f ||
+                (std::fabs(minSpread - bestSpread) <= 1e-10f && c.feature < next.feature)) {
+                next = c;
+                bestSpread = minSpread;
+                haveNext = true;
+            }
+        }
+        if (!haveNext || bestSpread < MERGE_DIST_SQ) break;
+        chosen[count++] = next;
+    }
+    NPContact contacts[MAX_CONTACTS];
+    for (int i = 0; i < count; i++)
+        contacts[i] = NPContact{hIsA ? chosen[i].xHull : chosen[i].xBox, hIsA ? chosen[i].xBox : chosen[i].xHull,
+                                chosen[i].feature};
+    emit_feature_manifold(S, p, outM, contacts, count, hIsA ? best.boxToHull : -best.boxToHull);
+}
+
+// 30_narrowphase.metal:547-745
+static void narrow_capsule(const Solver& S, const NPair& p, ManifoldGPU& outM, uint32_t stA, uint32_t stB) {
+    const Params& P = S.P;
+    bool cIsA = stA == 3;
+    uint32_t ic = cIsA ? p.ia : p.ib, io = cIsA ? p.ib : p.ia;
+    F4 qC = cIsA ? p.qA : p.qB, qO = cIsA ? p.qB : p.qA;
+    F3 pC = cIsA ? p.A.center : p.B.center, pO = cIsA ? p.B.center : p.A.center;
+    F4 shC = S.colShape[ic], shO = S.colShape[io];
+    float half_ = shC.x * 0.5f, rc = shC.y;
+    F3 axC = q_rotate(qC, f3(0, 0, 1));
+    F3 c0 = pC - axC * half_, c1 = pC + axC * half_;
+    uint32_t other = cIsA ? stB : stA;
+    F3 relCO = cIsA ? (p.vB - p.vA) : (p.vA - p.vB);
+    NPContact hits[3];
+    int nh = 0;
+    F3 nCO = f3(0, 0, 1);
+    if (other == 1) {
+        float rs = shO.x * 0.5f;
+        F3 q = closest_on_segment(pO, c0, c1);
+        F3 dd = pO - q;
+        float dist = length(dd);
+        F3 nT = dist > 1e-6f ? dd / dist : f3(0, 0, 1);
+        float dm = detect_margin(nT, relCO, P, shC.w, shO.w);
+        if (dist <= rc + rs + dm) {
+            nCO = nT;
+            hits[0] = NPContact{q + nCO * rc, pO - nCO * rs, 0};
+            nh = 1;
+        }
+    } else if (other == 3) {
+        float halfO = shO.x * 0.5f, ro = shO.y;
+        F3 axO = q_rotate(qO, f3(0, 0, 1));
+        F3 o0 = pO - axO * halfO, o1 = pO + axO * halfO;
+        F3 qa, qb;
+        closest_seg_seg(c0, c1, o0, o1, qa, qb);
+        F3 dd = qb - qa;
+        float dist = length(dd);
+        F3 nT = dist > 1e-6f ? dd / dist : f3(0, 0, 1);
+        float dm = detect_margin(nT, relCO, P, shC.w, shO.w);
+        if (dist <= rc + ro + dm) {
+            nCO = nT;
+            hits[0] = NPContact{qa + nCO * rc, qb - nCO * ro, 0};
+            nh = 1;
+        }
+    } else {
+        F4 qOc = q_conj(qO);
+        F3 halfO = xyz(shO) * 0.5f;
+        F3 nAccum = f3s(0);
+        for (int seed = 0; seed < 3 && nh < 3; seed++) {
+            float t = (float)seed * 0.5f;
+            F3 q = c0 + (c1 - c0) * t;
+            F3 bw = q;
+            for (int it = 0; it < 5; it++) {
+                F3 lb = clamp3(q_rotate(qOc, q - pO), -halfO, halfO);
+                bw = q_rotate(qO, lb) + pO;
+                q = closest_on_segment(bw, c0, c1);
+            }
+            F3 dd = bw - q;
+            float dist = length(dd);
+            F3 n;
+            if (dist < 1e-6f) {
+                F3 lb = q_rotate(qOc, q - pO);
+                F3 pen = halfO - abs3(lb);
+                int axis = min_axis(pen);
+                F3 nl = f3s(0);
+                setcomp(nl, axis, comp(lb, axis) >= 0.0f ? 1.0f : -1.0f);
+                n = -q_rotate(qO, nl);
+                bw = q - n * comp(pen, axis);
+            } else {
+                n = dd / dist;
+                float dm = detect_margin(n, relCO, P, shC.w, shO.w);
+                if (dist - rc > dm) continue;
+            }
+            bool dup = false;
+            for (int h = 0; h < nh; h++)
+                if (distance(hits[h].xA, q + n * rc) < 0.4f * rc + 0.05f) { dup = true; break; }
+            if (dup) continue;
+            hits[nh] = NPContact{q + n * rc, bw, (uint32_t)seed};
+            nAccum = nAccum + n;
+            nh++;
+        }
+        if (nh > 0) nCO = normalize(nAccum);
+    }
+    if (nh == 0) { outM.header = U4{p.ba, p.bb, 0, 0}; return; }
+    NPContact contacts[3];
+    for (int i = 0; i < nh; i++)
+        contacts[i] = NPContact{cIsA ? hits[i].xA : hits[i].xB, cIsA ? hits[i].xB : hits[i].xA, hits[i].feature};
+    emit_round_manifold(S, p, outM, contacts, nh, cIsA ? -nCO : nCO, 0.6f * (shC.y + 0.2f), true);
+}
+
+struct Torus { F3 center, axis, u, v; float R, r; };
+
+// 30_narrowphase.metal:300-332
+static Torus torus_frame(F3 pos, F4 q, float R, float r) {
+    Torus t;
+    t.center = pos;
+    t.axis = q_rotate(q, f3(0, 0, 1));
+    t.u = std::fabs(t.axis.x) > std::fabs(t.axis.z) ? f3(-t.axis.y, t.axis.x, 0.0f) : f3(0.0f, -t.axis.z, t.axis.y);
+    t.u = normalize(t.u);
+    t.v = cross(t.axis, t.u);
+    t.R = R;
+    t.r = r;
+    return t;
+}
+static F3 torus_spine(const Torus& t, F3 p) {
+    F3 d = p - t.center;
+    d = d - t.axis * dot(t.axis, d);
+    float l = length(d);
+    return l < 1e-6f ? t.center + t.u * t.R : t.center + d / l * t.R;
+}
+
+// cos and sin of the spine sample angles float(i) / 32 * 2 * pi, correctly
+// rounded at those float angles.
+static const float kSpineCos[32] = {
+    1.0f, 0.980785251f, 0.923879504f, 0.831469595f, 0.707106769f, 0.555570185f, 0.382683426f, 0.195090234f,
+    -4.37113883e-08f, -0.195090324f, -0.382683516f, -0.555570364f, -0.707106769f, -0.831469655f, -0.923879623f,
+    -0.98078531f, -1.0f, -0.980785251f, -0.923879504f, -0.831469536f, -0.70710665f, -0.555570006f, -0.382683128f,
+    -0.195090383f, 1.19248806e-08f, 0.195090413f, 0.382683605f, 0.555570424f, 0.707107008f, 0.831469595f,
+    0.923879564f, 0.98078531f};
+static const float kSpineSin[32] = {
+    0.0f, 0.195090324f, 0.382683456f, 0.555570245f, 0.707106769f, 0.831469655f, 0.923879504f, 0.98078531f,
+    1.0f, 0.980785251f, 0.923879504f, 0.831469536f, 0.707106769f, 0.555570185f, 0.382683277f, 0.195090309f,
+    -8.74227766e-08f, -0.195090488f, -0.382683426f, -0.555570304f, -0.707106888f, -0.831469774f, -0.923879683f,
+    -0.980785251f, -1.0f, -0.980785251f, -0.923879445f, -0.831469476f, -0.707106531f, -0.555570304f,
+    -0.382683426f, -0.195090234f};
+
+// 30_narrowphase.metal:747-975
+static void narrow_torus(const Solver& S, const NPair& p, ManifoldGPU& outM, uint32_t stA, uint32_t stB) {
+    const Params& P = S.P;
+    struct TorusHit { F3 xT, xO, n; float sep; uint32_t feature; };
+    bool tIsA = stA == 2;
+    uint32_t it = tIsA ? p.ia : p.ib, io = tIsA ? p.ib : p.ia;
+    F4 qT = tIsA ? p.qA : p.qB, qO = tIsA ? p.qB : p.qA;
+    F3 pT = tIsA ? p.A.center : p.B.center, pO = tIsA ? p.B.center : p.A.center;
+    F4 shT = S.colShape[it], shO = S.colShape[io];
+    Torus T = torus_frame(pT, qT, shT.x, shT.y);
+    uint32_t other = tIsA ? stB : stA;
+    float detectM = fmax_(P.collisionMargin, 0.8f * T.r);
+    TorusHit hits[4];
+    int nHits = 0;
+    if (other == 1) {
+        float rs = shO.x * 0.5f;
+        F3 spine = torus_spine(T, pO);
+        F3 dd = pO - spine;
+        float dist = length(dd);
+        if (dist <= T.r + rs + detectM) {
+            F3 n = dist > 1e-6f ? dd / dist : f3(0, 0, 1);
+            hits[0] = TorusHit{spine + n * T.r, pO - n * rs, -n, dist - T.r - rs, 0};
+            nHits = 1;
+        }
+    } else {
+        const int NSAMP = 32;
+        bool isBox = other == 0, isCap = other == 3;
+        Torus T2{};
+        F4 qOc = q_conj(qO);
+        F3 halfO = xyz(shO) * 0.5f;
+        float otherR = 0.0f;
+        F3 cs0 = f3s(0), cs1 = f3s(0);
+        if (isCap) {
+            float chalf = shO.x * 0.5f;
+            F3 axO = q_rotate(qO, f3(0, 0, 1));
+            cs0 = pO - axO * chalf;
+            cs1 = pO + axO * chalf;
+            otherR = shO.y;
+        } else if (!isBox) {
+            T2 = torus_frame(pO, qO, shO.x, shO.y);
+            otherR = T2.r;
+        }
+        auto closest_other = [&](F3 q) {
+            if (isBox) return q_rotate(qO, clamp3(q_rotate(qOc, q - pO), -halfO, halfO)) + pO;
+            if (isCap) return closest_on_segment(q, cs0, cs1);
+            return torus_spine(T2, q);
+        };
+        float dists[32];
+        F3 closest[32];
+        for (int i = 0; i < NSAMP; i++) {
+            F3 q = T.center + (T.u * kSpineCos[i] + T.v * kSpineSin[i]) * T.R;
+            F3 b = closest_other(q);
+            closest[i] = b;
+            dists[i] = distance(q, b);
+        }
+        bool used[32] = {};
+        for (int pick = 0; pick < 4; pick++) {
+            int best = -1;
+            float bd = FLT_MAX;
+            for (int i = 0; i < NSAMP; i++) {
+                if (used[i]) continue;
+                if (dists[i] < bd) { bd = dists[i]; best = i; }
+            }
+            if (best < 0) break;
+            if (bd - T.r - otherR > detectM) break;
+            for (int k = -3; k <= 3; k++) used[(best + k + NSAMP) % NSAMP] = true;
+            F3 q = T.center + (T.u * kSpineCos[best] + T.v * kSpineSin[best]) * T.R;
+            F3 b = closest[best];
+            for (int it2 = 0; it2 < 2; it2++) {
+                q = torus_spine(T, b);
+                b = closest_other(q);
+            }
+            F3 dd = q - b;
+            float dist = length(dd);
+            F3 n;
+            F3 xO_ = b;
+            if (dist < 1e-6f) {
+                if (isBox) {
+                    F3 lb = q_rotate(qOc, q - pO);
+                    F3 pen = halfO - abs3(lb);
+                    int axis = min_axis(pen);
+                    F3 nl = f3s(0);
+                    setcomp(nl, axis, comp(lb, axis) >= 0.0f ? 1.0f : -1.0f);
+                    n = q_rotate(qO, nl);
+                    xO_ = q + n * comp(pen, axis);
+                } else if (isCap) {
+                    n = normalize(cross(T.axis, normalize(cs1 - cs0)) + f3(1e-4f, 0, 0));
+                } else {
+                    n = normalize(cross(T.axis, T2.axis) + f3(1e-4f, 0, 0));
+                }
+            } else {
+                if (dist - T.r - otherR > detectM) continue;
+                n = dd / dist;
+            }
+            hits[nHits] = TorusHit{q - n * T.r, xO_ + (isBox ? f3s(0) : n * otherR), n, dist - T.r - otherR,
+                                   (uint32_t)best};
+            nHits++;
+        }
+    }
+    if (nHits == 0) { outM.header = U4{p.ba, p.bb, 0, 0}; return; }
+    int deep = 0;
+    float minSep = FLT_MAX;
+    for (int h = 0; h < nHits; h++)
+        if (hits[h].sep < minSep) { minSep = hits[h].sep; deep = h; }
+    F3 nT = hits[deep].n;
+    NPContact contacts[4];
+    for (int i = 0; i < nHits; i++)
+        contacts[i] = NPContact{tIsA ? hits[i].xT : hits[i].xO, tIsA ? hits[i].xO : hits[i].xT, hits[i].feature};
+    emit_round_manifold(S, p, outM, contacts, nHits, tIsA ? nT : -nT, 1.1f * shT.x, false);
+}
+
 void Solver::narrow_one(uint32_t gid) {
     uint32_t ia = pairs[2 * gid], ib = pairs[2 * gid + 1];
     uint32_t ba = colOwner[ia], bb = colOwner[ib];
@@ -739,7 +1239,13 @@ void Solver::narrow_one(uint32_t gid) {
     outM.colliderPair = U4{ia, ib, 0, 0};
     uint32_t stA = colShapeType[ia] & 0xFu, stB = colShapeType[ib] & 0xFu;
     bool sphA = stA == 1, sphB = stB == 1;
-    if (stA >= 2 || stB >= 2) { outM.header = U4{ba, bb, 0, 0}; return; }
+    if (stA >= 2 || stB >= 2) {
+        NPair p{ia, ib, ba, bb, bodyPA, bodyPB, qBodyA, qBodyB, qA, qB, vA, vB, A, B};
+        if (stA == 4 || stB == 4) narrow_hull(*this, p, outM, stA, stB);
+        else if ((stA == 3 || stB == 3) && stA != 2 && stB != 2) narrow_capsule(*this, p, outM, stA, stB);
+        else narrow_torus(*this, p, outM, stA, stB);
+        return;
+    }
 
     NPContact contacts[MAX_CONTACTS];
     int count = 0;
@@ -1889,6 +2395,52 @@ int oracle_set_motor_targets(void* h, const uint32_t* ids, uint32_t n, const flo
         oracle::JointGPU& j = s->joints[ids[i]];
         if ((j.header.w & oracle::MOTOR_MODE_MASK) == 0) continue;
         j.motor.x = targets[i];
+    }
+    return AVBD_OK;
+}
+// GPUSolver.swift:2481-2494, :2534-2551, :2564-2578
+int oracle_set_joint_world_anchors(void* h, const uint32_t* ids, uint32_t n, const float* xyz) {
+    Solver* s = static_cast<Solver*>(h);
+    for (uint32_t i = 0; i < n; i++) {
+        if (ids[i] >= s->joints.size()) return AVBD_ERR_INVALID_ARGUMENT;
+        oracle::JointGPU& j = s->joints[ids[i]];
+        j.rA.x = xyz[3 * i]; j.rA.y = xyz[3 * i + 1]; j.rA.z = xyz[3 * i + 2];
+    }
+    return AVBD_OK;
+}
+int oracle_set_motor_velocities(void* h, const uint32_t* ids, uint32_t n, const float* v) {
+    Solver* s = static_cast<Solver*>(h);
+    for (uint32_t i = 0; i < n; i++) {
+        if (ids[i] >= s->joints.size()) return AVBD_ERR_INVALID_ARGUMENT;
+        s->joints[ids[i]].motor.x = v[i];
+    }
+    return AVBD_OK;
+}
+int oracle_set_motor_torques(void* h, const uint32_t* ids, uint32_t n, const float* t) {
+    Solver* s = static_cast<Solver*>(h);
+    for (uint32_t i = 0; i < n; i++) {
+        if (ids[i] >= s->joints.size()) return AVBD_ERR_INVALID_ARGUMENT;
+        s->joints[ids[i]].motor.y = t[i];
+    }
+    return AVBD_OK;
+}
+// GPUSolver.swift:2606-2637
+int oracle_get_motor_states(void* h, const uint32_t* ids, uint32_t n, float* angles, float* velocities) {
+    using namespace oracle;
+    Solver* s = static_cast<Solver*>(h);
+    for (uint32_t i = 0; i < n; i++) {
+        if (ids[i] >= s->joints.size()) return AVBD_ERR_INVALID_ARGUMENT;
+        const JointGPU& j = s->joints[ids[i]];
+        uint32_t a = j.header.x, b = j.header.y;
+        F4 qB = s->posAng[b];
+        F4 qA = a == 0xFFFFFFFFu ? F4{0, 0, 0, 1} : s->posAng[a];
+        F4 r = q_mul(q_inv(q_mul(qA, j.restRel)), qB);
+        if (r.w < 0.0f) r = F4{-r.x, -r.y, -r.z, -r.w};
+        F3 axis = xyz(j.hingeAxis);
+        angles[i] = 2.0f * atan2_series(dot(xyz(r), axis), r.w);
+        F3 wB = xyz(s->velAng[b]);
+        F3 wA = a == 0xFFFFFFFFu ? f3s(0) : xyz(s->velAng[a]);
+        velocities[i] = dot(wB - wA, q_rotate(qB, axis));
     }
     return AVBD_OK;
 }

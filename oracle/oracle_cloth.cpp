@@ -585,6 +585,15 @@ void Solver::rt_emit() {
             if (st == AVBD_SHAPE_SPHERE) {
                 feats[0] = Feat{po, shape[o].x * 0.5f, 8};
                 nf = 1;
+            } else if (st == AVBD_SHAPE_CAPSULE) {
+                // three spheres along the axis; a torus has none (25_cloth.metal:957-971)
+                float half_ = shape[o].x * 0.5f, r = shape[o].y;
+                F3 ax = q_rotate(qo, f3(0, 0, 1));
+                for (int i = -1; i <= 1; i++) {
+                    F3 w = po + ax * (half_ * (float)i);
+                    if (distance(w, m) > rT + r + 4.0f * P.collisionMargin) continue;
+                    feats[nf++] = Feat{w, r, (uint32_t)(9 + i + 1)};
+                }
             } else if (st == AVBD_SHAPE_BOX) {
                 F3 h3 = xyz(shape[o]) * 0.5f;
                 for (uint32_t i = 0; i < 8; i++) {

@@ -151,6 +151,8 @@ struct Solver {
     std::vector<uint32_t> colOwner, colShapeType, colGroup, colShared;
     std::vector<F4> colShape, colLocalPos, colLocalRot;
     std::vector<float> colFrictionS, colFrictionD;
+    std::vector<uint32_t> colHullFirst, colHullCount;  // convex hull vertex range per collider
+    std::vector<F3> hullVerts;
     std::vector<uint32_t> hashedIdx, globalIdx, hashedRigidIdx;
     // constraints
     std::vector<JointGPU> joints;

@@ -158,10 +158,10 @@ def test_soft_cube_settles_on_ground(oracle_lib):
 
 
 def test_unsupported_features_are_refused(oracle_lib):
-    s = PhysicsScene("capsule")
-    s.add_body((1, 0.2, 0), 1.0, 0.5, (0, 0, 1), shape=abi.SHAPE_CAPSULE)
+    # Planar-DAT truncation of tet surfaces is refused, not approximated
+    s = demos.two_cubes_scene(n=3)
     with pytest.raises(RuntimeError):
-        oracle_lib.OracleSolver(s)
+        oracle_lib.OracleSolver(s, truncation=abi.TRUNCATION_PLANAR_DAT)
 
 
 def test_atan2_series_accuracy(oracle_lib):
