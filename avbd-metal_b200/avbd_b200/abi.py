@@ -165,6 +165,22 @@ class Counters(C.Structure):
     ]
 
 
+class RenderInstance(C.Structure):
+    """avbd_render_instance (RenderInstance, 50_render.metal:7-11)."""
+    _fields_ = [("model", C.c_float * 16), ("color", C.c_float * 4), ("params", C.c_float * 4)]
+
+
+class SkinBinding(C.Structure):
+    """avbd_skin_binding (SkinBindingGPU, GPUTypes.swift:104-111)."""
+    _fields_ = [("ids", C.c_uint32 * 4), ("weights", C.c_float * 4), ("rest_normal", C.c_float * 4),
+                ("inv0", C.c_float * 4), ("inv1", C.c_float * 4), ("inv2", C.c_float * 4)]
+
+
+class PushTEnv(C.Structure):
+    """avbd_pusht_env (PushTEnvGPU, RL/PushTEnv.swift:28-32)."""
+    _fields_ = [("ids", C.c_uint32 * 4), ("frame", C.c_float * 4), ("goal", C.c_float * 4)]
+
+
 # Exported symbols declared in include/avbd.h (checked by the CPU tests).
 EXPORTED = [
     "avbd_create", "avbd_destroy", "avbd_set_settings", "avbd_get_settings",
@@ -179,6 +195,8 @@ EXPORTED = [
     "avbd_set_warm_start_model", "avbd_set_warm_start_mode", "avbd_set_learning_capture",
     "avbd_set_residual_trace", "avbd_get_residual_trace", "avbd_mlp_param_count",
     "avbd_mlp_workspace_bytes", "avbd_mlp_gradients", "avbd_mlp_train_step", "avbd_mlp_infer",
+    "avbd_build_instances", "avbd_soft_normals", "avbd_set_skin_bindings", "avbd_skin_deform",
+    "avbd_render_pusht_obs",
 ]
 WARM_START_PLAIN, WARM_START_LEARNED = 0, 1
 

@@ -662,6 +662,111 @@ def shapes_scene(seed: int = 6, count: int = 512, pitch: float = 1.3) -> Physics
     return s
 
 
+# ---------------------------------------------------------------------------
+# Push-T vector environment (RL/PushTEnv.swift)
+# ---------------------------------------------------------------------------
+
+PUSHT_TIP_HEIGHT = 0.42
+PUSHT_PUSHER_FORCE = 60.0
+PUSHT_PITCH = 7.0
+
+
+def _qrot(q, v):
+    u = np.asarray(q[:3], np.float64)
+    t = 2.0 * np.cross(u, v)
+    return np.asarray(v, np.float64) + q[3] * t + np.cross(u, t)
+
+
+def pusht_scene(num_envs: int = 16, seed: int = 1):
+    """PushTEnv.init(numEnvs:seed:) with the grid layout
+    (RL/PushTEnv.swift:114-183, buildOne :194-246): one collision group per
+    environment, each with a vertical capsule pusher tip driven by a soft
+    world joint (the drag joint, moved with set_joint_world_anchors) plus an
+    angular weld, a T block of two welded boxes at a seeded pose, and a
+    fence.  Returns (scene, envs): envs[e] is a dict with the body ids
+    (tip, bar, stem), the drag joint, the centre and the goal."""
+    s = PhysicsScene("pusht")
+    st = s.settings
+    st.iterations, st.beta_lin, st.lambda_max = 16, 20000.0, 600.0
+    cols = int(math.ceil(math.sqrt(num_envs)))
+    rows = int(math.ceil(num_envs / cols))
+    hx, hy = 0.5 * (cols - 1) * PUSHT_PITCH, 0.5 * (rows - 1) * PUSHT_PITCH
+    s.add_body((2 * (hx + 3.5), 2 * (hy + 3.5), 2.0), 0.0, 1.3, (0.0, 0.0, -1.0))
+    rng = SplitMix64(seed)
+    inf = float("inf")
+    envs = []
+    for e in range(num_envs):
+        c = np.array([(e % cols) * PUSHT_PITCH - hx, (e // cols) * PUSHT_PITCH - hy, 0.0])
+        g = e + 1
+        tip = s.add_body((0.7, 0.09, 0.0), 1.2, 0.35, tuple(c + (1.4, 0.0, PUSHT_TIP_HEIGHT)),
+                         shape=abi.SHAPE_CAPSULE, collision_group=g)
+        drag = len(s.joints)
+        s.add_joint(SceneJoint(-1, tip, tuple(c + (1.4, 0.0, PUSHT_TIP_HEIGHT)), (0, 0, 0),
+                               stiffness_lin=PUSHT_PUSHER_FORCE / 0.08, stiffness_ang=0.0))
+        s.add_joint(SceneJoint(-1, tip, (0, 0, 0), (0, 0, 0), stiffness_lin=0.0, stiffness_ang=inf))
+        ang = rng.next_float() * 2.0 * math.pi
+        rad = 0.55 + rng.next_float() * 1.0
+        byaw = (rng.next_float() - 0.5) * 2.0 * math.pi
+        q = quat_axis_angle(byaw, (0, 0, 1))
+        block = c + (math.cos(ang) * rad, math.sin(ang) * rad, 0.0)
+        pbar = block + _qrot(q, (0.0, 0.125, 0.0)) + (0, 0, 0.09)
+        pstem = block + _qrot(q, (0.0, -0.325, 0.0)) + (0, 0, 0.09)
+        bar = s.add_body((1.0, 0.25, 0.18), 3.0, 1.1, tuple(pbar), rotation=q, collision_group=g)
+        stem = s.add_body((0.25, 0.65, 0.18), 3.0, 1.1, tuple(pstem), rotation=q, collision_group=g)
+        mid = (np.asarray(s.bodies[bar].position) + np.asarray(s.bodies[stem].position)) * 0.5
+        qi = (-q[0], -q[1], -q[2], q[3])
+        s.add_joint(SceneJoint(bar, stem, tuple(_qrot(qi, mid - np.asarray(s.bodies[bar].position))),
+                               tuple(_qrot(qi, mid - np.asarray(s.bodies[stem].position))),
+                               stiffness_lin=inf, stiffness_ang=inf))
+        s.add_joint(SceneJoint(bar, stem, (0, 0, 0), (0, 0, 0), stiffness_lin=0.0, stiffness_ang=0.0))
+        for sgn in (-1.0, 1.0):
+            s.add_body((6.4, 0.12, 0.45), 0.0, 0.4, tuple(c + (0.0, sgn * 3.2, 0.22)), collision_group=g)
+            s.add_body((0.12, 6.4, 0.45), 0.0, 0.4, tuple(c + (sgn * 3.2, 0.0, 0.22)), collision_group=g)
+        envs.append(dict(tip=tip, bar=bar, stem=stem, drag_joint=drag, center=(float(c[0]), float(c[1])),
+                         goal_pos=(0.85, 0.85), goal_yaw=0.0))
+    return s, envs
+
+
+def pusht_env_table(envs, half_window: float = 3.25):
+    """PushTEnvGPU records of a batch (RL/PushTEnv.swift:569-575): the
+    window covers the whole arena."""
+    out = []
+    for r in envs:
+        t = abi.PushTEnv()
+        t.ids[:] = [r["tip"], r["bar"], r["stem"], 0]
+        t.frame[:] = [r["center"][0], r["center"][1], r["goal_pos"][0], r["goal_pos"][1]]
+        t.goal[:] = [r["goal_yaw"], half_window, 0.0, 0.0]
+        out.append(t)
+    return out
+
+
+def pusht_tip_anchors(envs, targets):
+    """World anchor points of the drag joints for env-local tip targets
+    (setTipTarget, RL/PushTEnv.swift:258-262): targets clamped to +-3.02 m."""
+    t = np.clip(np.asarray(targets, np.float64).reshape(-1, 2), -3.02, 3.02)
+    pts = [(r["center"][0] + t[i, 0], r["center"][1] + t[i, 1], PUSHT_TIP_HEIGHT) for i, r in enumerate(envs)]
+    return [r["drag_joint"] for r in envs], np.asarray(pts, np.float32)
+
+
+def skin_bindings_for_tets(scene, per_tet: int = 1, seed: int = 9):
+    """Render-skin bindings for a tet scene: `per_tet` points inside each
+    tet (random barycentric weights), bound to its four vertices with a
+    seeded rest normal; zero inverses (computed from the rest pose on
+    upload)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for t in scene.tets:
+        for _ in range(per_tet):
+            w = rng.dirichlet(np.ones(4)).astype(np.float32)
+            b = abi.SkinBinding()
+            b.ids[:] = list(t.ids)
+            b.weights[:] = [float(x) for x in w]
+            n = rng.normal(size=3)
+            b.rest_normal[:] = [float(n[0]), float(n[1]), float(n[2]), 0.0]
+            out.append(b)
+    return out
+
+
 SCENES = {
     "rigid-stack": rigid_stack_scene,
     "soft-cube": soft_cube_scene,

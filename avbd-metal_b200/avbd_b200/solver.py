@@ -65,6 +65,11 @@ def load_library() -> C.CDLL:
         "avbd_set_motor_velocities": ([vp, vp, u32, vp], i32),
         "avbd_set_motor_torques": ([vp, vp, u32, vp], i32),
         "avbd_get_motor_states": ([vp, vp, u32, vp, vp], i32),
+        "avbd_build_instances": ([vp, vp, u32, vp, u32, vp, i32], i32),
+        "avbd_soft_normals": ([vp, C.c_float, vp, i32], i32),
+        "avbd_set_skin_bindings": ([vp, vp, u32], i32),
+        "avbd_skin_deform": ([vp, vp, i32], i32),
+        "avbd_render_pusht_obs": ([vp, vp, u32, u32, vp, i32], i32),
         "avbd_max_constraint_error": ([vp, C.POINTER(C.c_float)], i32),
         "avbd_get_counters": ([vp, vp], i32),
         "avbd_runtime_failure": ([vp, C.POINTER(i32)], i32),
@@ -219,6 +224,61 @@ class GPUSolver:
         ids = np.ascontiguousarray(joints, dtype=np.uint32)
         t = np.ascontiguousarray(torques, dtype=np.float32)
         self._check(load_library().avbd_set_motor_torques(self._h, ids.ctypes.data, len(ids), t.ctypes.data))
+
+    # -- headless render and observation compute -------------------------------
+    # Each call writes host arrays (returned) unless `device_out` gives a
+    # device address (an int, e.g. a torch tensor's data_ptr()): then it only
+    # enqueues the kernel on the solver's stream and returns None.
+    def build_instances(self, colliders, colors=None, color_mode: int = 0, device_out=None):
+        """encodeBuildInstancesChecked (GPUSolver.swift:4605-4646): (n, 24)
+        float32 records (4x4 model column-major, rgba-kind colour, params)."""
+        ids = np.ascontiguousarray(colliders, dtype=np.uint32)
+        col = None if colors is None else np.ascontiguousarray(colors, dtype=np.float32).reshape(-1, 4)
+        out = None if device_out is not None else np.zeros((len(ids), 24), np.float32)
+        self._check(load_library().avbd_build_instances(
+            self._h, ids.ctypes.data, len(ids), None if col is None else col.ctypes.data, color_mode,
+            device_out if device_out is not None else out.ctypes.data, 1 if device_out is not None else 0))
+        return out
+
+    def soft_normals(self, cloth_scale: float = 0.0, out=None, device_out=None):
+        """soft_face_normals + soft_normals (50_render.metal:104-180): one
+        float4 per body (normal, render thickness); entries off the surface
+        keep the values of `out` (zeros by default)."""
+        if device_out is not None:
+            self._check(load_library().avbd_soft_normals(self._h, cloth_scale, device_out, 1))
+            return None
+        res = np.zeros((self.num_bodies, 4), np.float32) if out is None else np.ascontiguousarray(out, np.float32)
+        self._check(load_library().avbd_soft_normals(self._h, cloth_scale, res.ctypes.data, 0))
+        return res
+
+    def set_skin_bindings(self, bindings):
+        """Skin bindings (GPUSolver.swift:1849-1907): a sequence of
+        abi.SkinBinding or a ctypes array of them."""
+        arr = (abi.SkinBinding * len(bindings))(*bindings)
+        self._num_skin = len(bindings)
+        self._check(load_library().avbd_set_skin_bindings(self._h, arr, len(bindings)))
+
+    def skin_deform(self, device_out=None):
+        """skin_deform (50_render.metal:182-212): (n, 8) float32 = position
+        (w 1) and normal (w 0) per binding."""
+        n = getattr(self, "_num_skin", 0)
+        if device_out is not None:
+            self._check(load_library().avbd_skin_deform(self._h, device_out, 1))
+            return None
+        out = np.zeros((n, 8), np.float32)
+        self._check(load_library().avbd_skin_deform(self._h, out.ctypes.data if n else out.ctypes.data, 0))
+        return out
+
+    def render_pusht_obs(self, envs, res: int = 64, device_out=None):
+        """renderPushTObsChecked (GPUSolver.swift:2296-2325): uint8 array
+        (num_envs, res, res, 3)."""
+        arr = (abi.PushTEnv * len(envs))(*envs)
+        if device_out is not None:
+            self._check(load_library().avbd_render_pusht_obs(self._h, arr, len(envs), res, device_out, 1))
+            return None
+        out = np.zeros((len(envs), res, res, 3), np.uint8)
+        self._check(load_library().avbd_render_pusht_obs(self._h, arr, len(envs), res, out.ctypes.data, 0))
+        return out
 
     def motor_states(self, joints):
         """motorStates (GPUSolver.swift:2606-2637): (angles, velocities)."""

@@ -173,6 +173,23 @@ void launch_finalize(const Params& P, const DevPtrs& d, const Sizes& z, cudaStre
 void launch_max_constraint_error(const Params& P, const DevPtrs& d, const Sizes& z,
                                  cudaStream_t st);
 void launch_reset_bodies(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
+
+// ---- headless render and observation compute (render.cu)
+// SkinBindingGPU (layout of avbd_skin_binding)
+struct SkinBinding { uint4 ids; float4 weights, restNormal, inv0, inv1, inv2; };
+// one Push-T environment with the goal heading's cos/sin
+struct PushTDev { uint4 ids; float4 frame; float goalYaw, halfWin, goalCos, goalSin; };
+static_assert(sizeof(SkinBinding) == 96, "SkinBinding layout");
+static_assert(sizeof(PushTDev) == 48, "PushTDev layout");
+// out: 24 floats per instance (avbd_render_instance)
+void launch_build_instances(const DevPtrs& d, const uint32_t* ids, const float4* colors, uint32_t n,
+                            uint32_t colorMode, float* out, cudaStream_t st);
+void launch_soft_normals(const DevPtrs& d, uint32_t numTris, const uint32_t* surfVerts, const uint32_t* vtStart,
+                         const uint32_t* vtCount, const uint32_t* vtList, uint32_t numSurf, float4* faceN,
+                         float clothScale, float4* out, cudaStream_t st);
+void launch_skin_deform(const float4* posLin, const SkinBinding* b, uint32_t n, float4* out, cudaStream_t st);
+void launch_pusht_obs(const float4* posLin, const float4* posAng, const PushTDev* envs, uint32_t numEnvs,
+                      uint32_t res, uint8_t* out, cudaStream_t st);
 // spinners and legacy rate motors, then the end-of-frame failure check
 void launch_frame_end(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 

@@ -7,6 +7,7 @@
 // serves state reads and writes.
 #include <cuda_runtime.h>
 
+#include <array>
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
@@ -157,6 +158,16 @@ struct avbd_solver {
     size_t stageBytes = 0;
     uint32_t* hostLatch = nullptr;     // pinned copy of the failure latch
     Counters* hostCounters = nullptr;  // pinned copy of the last frame's counters
+    // render surface (built on the first smooth-normals call): surface
+    // vertices, their incident triangles, face normals
+    bool renderSurfaceReady = false;
+    uint32_t numSurfVerts = 0;
+    uint32_t *surfVerts = nullptr, *surfVtStart = nullptr, *surfVtCount = nullptr, *surfVtList = nullptr;
+    uint32_t* surfClothVert = nullptr;
+    float4* faceNormals = nullptr;
+    // skin bindings (replaced by each upload)
+    SkinBinding* skin = nullptr;
+    uint32_t numSkin = 0;
 
     ~avbd_solver() {
         if (launch) cudaStreamSynchronize(launch);
@@ -166,6 +177,7 @@ struct avbd_solver {
         for (auto& e : tuneEvents) cudaEventDestroy(e);
         for (void* p : allocations) cudaFree(p);
         if (stage) cudaFree(stage);
+        if (skin) cudaFree(skin);
         if (hostLatch) cudaFreeHost(hostLatch);
         if (hostCounters) cudaFreeHost(hostCounters);
         if (forkEvent) cudaEventDestroy(forkEvent);
@@ -1044,6 +1056,204 @@ int avbd_get_motor_states(avbd_solver* s, const uint32_t* joints, uint32_t n, fl
         return AVBD_ERR_RUNTIME_FAILURE;
     for (uint32_t i = 0; i < n; i++) { angles[i] = out[2 * i]; velocities[i] = out[2 * i + 1]; }
     return AVBD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Headless render and observation compute (render.cu)
+// ---------------------------------------------------------------------------
+namespace {
+// Staging layout: `in` bytes of inputs, then (host output only) `out` bytes.
+uint8_t* render_staging(avbd_solver* s, size_t in, size_t out, size_t& outOff) {
+    outOff = (in + 255) & ~(size_t)255;
+    return static_cast<uint8_t*>(s->staging(outOff + out + 16));
+}
+// Goal heading of a Push-T environment: cos and sin of the yaw, evaluated in
+// double and rounded once.
+void goal_heading(float yaw, float& c, float& s) {
+    c = (float)std::cos((double)yaw);
+    s = (float)std::sin((double)yaw);
+}
+
+// Rest normal (unit, +z when zero) and rest inverse of a skin binding; a
+// zero inverse becomes the inverse of the four bodies' scene-pose edge
+// matrix [d0 d1 d2] (rows cross(d1,d2), cross(d2,d0), cross(d0,d1) over the
+// determinant; the identity when it is singular), GPUSolver.swift:1866-1896.
+void skin_rest_frame(const avbd_skin_binding& g, const std::vector<f4>& pos, SkinBinding& o) {
+    const float* rn = g.rest_normal;
+    const float l2 = rn[0] * rn[0] + rn[1] * rn[1] + rn[2] * rn[2];
+    if (l2 > 1e-12f) {
+        const float l = std::sqrt(l2);
+        o.restNormal = make_float4(rn[0] / l, rn[1] / l, rn[2] / l, 0.0f);
+    } else {
+        o.restNormal = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+    }
+    auto sq = [](const float* v) { return v[0] * v[0] + v[1] * v[1] + v[2] * v[2]; };
+    if (sq(g.inv0) + sq(g.inv1) + sq(g.inv2) > 1e-16f) {
+        o.inv0 = make_float4(g.inv0[0], g.inv0[1], g.inv0[2], 0.0f);
+        o.inv1 = make_float4(g.inv1[0], g.inv1[1], g.inv1[2], 0.0f);
+        o.inv2 = make_float4(g.inv2[0], g.inv2[1], g.inv2[2], 0.0f);
+        return;
+    }
+    auto P = [&](uint32_t i) { return std::array<float, 3>{pos[i].x, pos[i].y, pos[i].z}; };
+    auto sub3 = [](std::array<float, 3> a, std::array<float, 3> b) {
+        return std::array<float, 3>{a[0] - b[0], a[1] - b[1], a[2] - b[2]};
+    };
+    auto crs = [](std::array<float, 3> a, std::array<float, 3> b) {
+        return std::array<float, 3>{a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+    };
+    const auto x0 = P(g.ids[0]);
+    const auto d0 = sub3(P(g.ids[1]), x0), d1 = sub3(P(g.ids[2]), x0), d2 = sub3(P(g.ids[3]), x0);
+    const auto r0 = crs(d1, d2), r1 = crs(d2, d0), r2 = crs(d0, d1);
+    const float det = d0[0] * r0[0] + d0[1] * r0[1] + d0[2] * r0[2];
+    if (std::fabs(det) > 1e-12f) {
+        o.inv0 = make_float4(r0[0] / det, r0[1] / det, r0[2] / det, 0.0f);
+        o.inv1 = make_float4(r1[0] / det, r1[1] / det, r1[2] / det, 0.0f);
+        o.inv2 = make_float4(r2[0] / det, r2[1] / det, r2[2] / det, 0.0f);
+    } else {
+        o.inv0 = make_float4(1.0f, 0.0f, 0.0f, 0.0f);
+        o.inv1 = make_float4(0.0f, 1.0f, 0.0f, 0.0f);
+        o.inv2 = make_float4(0.0f, 0.0f, 1.0f, 0.0f);
+    }
+}
+
+// Host output: copy back and wait; device output: return at once.
+int render_finish(avbd_solver* s, void* hostOut, const void* devOut, size_t bytes, const char* label) {
+    if (!s->check(cudaGetLastError(), label)) return AVBD_ERR_RUNTIME_FAILURE;
+    if (hostOut) {
+        if (!s->check(cudaMemcpyAsync(hostOut, devOut, bytes, cudaMemcpyDeviceToHost, s->launch), label) ||
+            !s->check(cudaStreamSynchronize(s->launch), label))
+            return AVBD_ERR_RUNTIME_FAILURE;
+    }
+    return AVBD_OK;
+}
+}  // namespace
+
+int avbd_build_instances(avbd_solver* s, const uint32_t* colliders, uint32_t n, const float* colors_rgba,
+                         uint32_t color_mode, avbd_render_instance* out, int out_on_device) {
+    if (!s || (n && (!colliders || !out)) || color_mode > 1) return AVBD_ERR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < n; i++)
+        if (colliders[i] >= s->H.numColliders) return AVBD_ERR_INVALID_ARGUMENT;
+    if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
+    if (n == 0) return AVBD_OK;
+    const size_t idBytes = ((4 * (size_t)n) + 15) & ~(size_t)15, colBytes = colors_rgba ? 16 * (size_t)n : 0;
+    const size_t outBytes = sizeof(avbd_render_instance) * (size_t)n;
+    size_t outOff;
+    uint8_t* st = render_staging(s, idBytes + colBytes, out_on_device ? 0 : outBytes, outOff);
+    if (!st) return AVBD_ERR_ALLOC_FAILED;
+    cudaMemcpyAsync(st, colliders, 4 * (size_t)n, cudaMemcpyHostToDevice, s->launch);
+    if (colors_rgba) cudaMemcpyAsync(st + idBytes, colors_rgba, colBytes, cudaMemcpyHostToDevice, s->launch);
+    float* dOut = out_on_device ? reinterpret_cast<float*>(out) : reinterpret_cast<float*>(st + outOff);
+    launch_build_instances(s->d, reinterpret_cast<uint32_t*>(st),
+                           colors_rgba ? reinterpret_cast<float4*>(st + idBytes) : nullptr, n, color_mode, dOut,
+                           s->launch);
+    return render_finish(s, out_on_device ? nullptr : out, dOut, outBytes, "build instances");
+}
+
+int avbd_soft_normals(avbd_solver* s, float cloth_scale, float* out, int out_on_device) {
+    if (!s || !out || !std::isfinite(cloth_scale)) return AVBD_ERR_INVALID_ARGUMENT;
+    if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
+    const uint32_t nt = s->H.numTris, nb = s->H.numBodies;
+    if (nt == 0) return AVBD_OK;
+    if (!s->renderSurfaceReady) {
+        // vertex -> incident surface triangles, vertices ascending, triangles
+        // in surface order (GPUSolver.swift:1812-1842)
+        std::vector<uint32_t> cnt(nb, 0);
+        for (const u4& t : s->H.tris) { cnt[t.x]++; cnt[t.y]++; cnt[t.z]++; }
+        std::vector<uint32_t> verts, start, count, list, pos(nb, 0);
+        for (uint32_t v = 0; v < nb; v++)
+            if (cnt[v]) { verts.push_back(v); start.push_back((uint32_t)list.size()); count.push_back(cnt[v]); pos[v] = (uint32_t)list.size(); list.resize(list.size() + cnt[v]); }
+        for (uint32_t t = 0; t < nt; t++) {
+            const u4 tr = s->H.tris[t];
+            for (uint32_t v : {tr.x, tr.y, tr.z}) list[pos[v]++] = t;
+        }
+        std::vector<uint32_t> cloth = s->H.clothVert;
+        cloth.resize(nb, 0);
+        bool ok = s->upload(s->surfVerts, verts, "surfaceVertices") && s->upload(s->surfVtStart, start, "surfaceVtStart") &&
+                  s->upload(s->surfVtCount, count, "surfaceVtCount") && s->upload(s->surfVtList, list, "surfaceVtList") &&
+                  s->upload(s->surfClothVert, cloth, "surfaceClothVert") &&
+                  s->alloc(s->faceNormals, nt, "faceNormals");
+        if (!ok) return AVBD_ERR_ALLOC_FAILED;
+        s->numSurfVerts = (uint32_t)verts.size();
+        s->renderSurfaceReady = true;
+    }
+    const size_t outBytes = 16 * (size_t)nb;
+    size_t outOff;
+    uint8_t* st = render_staging(s, 0, out_on_device ? 0 : outBytes, outOff);
+    if (!st) return AVBD_ERR_ALLOC_FAILED;
+    float4* dOut = out_on_device ? reinterpret_cast<float4*>(out) : reinterpret_cast<float4*>(st + outOff);
+    if (!out_on_device) cudaMemcpyAsync(dOut, out, outBytes, cudaMemcpyHostToDevice, s->launch);  // untouched entries
+    DevPtrs d = s->d;
+    d.clothVert = s->surfClothVert;
+    launch_soft_normals(d, nt, s->surfVerts, s->surfVtStart, s->surfVtCount, s->surfVtList, s->numSurfVerts,
+                        s->faceNormals, cloth_scale, dOut, s->launch);
+    return render_finish(s, out_on_device ? nullptr : out, dOut, outBytes, "soft normals");
+}
+
+int avbd_set_skin_bindings(avbd_solver* s, const avbd_skin_binding* b, uint32_t n) {
+    if (!s || (n && !b)) return AVBD_ERR_INVALID_ARGUMENT;
+    const uint32_t nb = s->H.numBodies;
+    std::vector<SkinBinding> host(n);
+    for (uint32_t i = 0; i < n; i++) {
+        const avbd_skin_binding& g = b[i];
+        for (int k = 0; k < 4; k++)
+            if (g.ids[k] >= nb) return AVBD_ERR_INVALID_ARGUMENT;
+        SkinBinding& o = host[i];
+        o.ids = make_uint4(g.ids[0], g.ids[1], g.ids[2], g.ids[3]);
+        o.weights = make_float4(g.weights[0], g.weights[1], g.weights[2], g.weights[3]);
+        skin_rest_frame(g, s->H.posLin, o);
+    }
+    if (s->launch) cudaStreamSynchronize(s->launch);
+    if (s->skin) { cudaFree(s->skin); s->skin = nullptr; }
+    s->numSkin = 0;
+    if (n == 0) return AVBD_OK;
+    if (cudaMalloc(&s->skin, sizeof(SkinBinding) * (size_t)n) != cudaSuccess) return AVBD_ERR_ALLOC_FAILED;
+    if (cudaMemcpy(s->skin, host.data(), sizeof(SkinBinding) * (size_t)n, cudaMemcpyHostToDevice) != cudaSuccess)
+        return AVBD_ERR_ALLOC_FAILED;
+    s->numSkin = n;
+    return AVBD_OK;
+}
+
+int avbd_skin_deform(avbd_solver* s, float* out, int out_on_device) {
+    if (!s || !out) return AVBD_ERR_INVALID_ARGUMENT;
+    if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
+    if (s->numSkin == 0) return AVBD_OK;
+    const size_t outBytes = 32 * (size_t)s->numSkin;
+    size_t outOff;
+    uint8_t* st = render_staging(s, 0, out_on_device ? 0 : outBytes, outOff);
+    if (!st) return AVBD_ERR_ALLOC_FAILED;
+    float4* dOut = out_on_device ? reinterpret_cast<float4*>(out) : reinterpret_cast<float4*>(st + outOff);
+    launch_skin_deform(s->d.posLin, s->skin, s->numSkin, dOut, s->launch);
+    return render_finish(s, out_on_device ? nullptr : out, dOut, outBytes, "skin deform");
+}
+
+int avbd_render_pusht_obs(avbd_solver* s, const avbd_pusht_env* envs, uint32_t num_envs, uint32_t res,
+                          uint8_t* out, int out_on_device) {
+    if (!s || (num_envs && (!envs || !out)) || res < 2 || res > 4096) return AVBD_ERR_INVALID_ARGUMENT;
+    const uint32_t nb = s->H.numBodies;
+    std::vector<PushTDev> table(num_envs);
+    for (uint32_t e = 0; e < num_envs; e++) {
+        const avbd_pusht_env& v = envs[e];
+        for (int k = 0; k < 3; k++)
+            if (v.ids[k] >= nb) return AVBD_ERR_INVALID_ARGUMENT;
+        PushTDev& t = table[e];
+        t.ids = make_uint4(v.ids[0], v.ids[1], v.ids[2], v.ids[3]);
+        t.frame = make_float4(v.frame[0], v.frame[1], v.frame[2], v.frame[3]);
+        t.goalYaw = v.goal[0];
+        t.halfWin = v.goal[1];
+        goal_heading(v.goal[0], t.goalCos, t.goalSin);
+    }
+    if (out_on_device && (res % 4u == 0u) && (reinterpret_cast<uintptr_t>(out) & 3u)) return AVBD_ERR_INVALID_ARGUMENT;
+    if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
+    if (num_envs == 0) return AVBD_OK;
+    const size_t inBytes = sizeof(PushTDev) * (size_t)num_envs;
+    const size_t outBytes = (size_t)num_envs * res * res * 3;
+    size_t outOff;
+    uint8_t* st = render_staging(s, inBytes, out_on_device ? 0 : outBytes, outOff);
+    if (!st) return AVBD_ERR_ALLOC_FAILED;
+    cudaMemcpyAsync(st, table.data(), inBytes, cudaMemcpyHostToDevice, s->launch);
+    uint8_t* dOut = out_on_device ? out : st + outOff;
+    launch_pusht_obs(s->d.posLin, s->d.posAng, reinterpret_cast<PushTDev*>(st), num_envs, res, dOut, s->launch);
+    return render_finish(s, out_on_device ? nullptr : out, dOut, outBytes, "Push-T observation");
 }
 
 int avbd_max_constraint_error(avbd_solver* s, float* out) {

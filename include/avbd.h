@@ -478,6 +478,84 @@ int avbd_debug_read(avbd_solver* solver, int which, void* dst, size_t bytes);
 int avbd_exclusive_scan_noalloc(const uint32_t* d_in, uint32_t* d_out, uint32_t n,
                                 void* cuda_stream);
 
+/* ---- Headless render and observation compute ---------------------------
+ * The reference's render-side compute kernels (Shaders/50_render.metal,
+ * Shaders/60_robotics.metal) as CUDA kernels on the solver's stream, ordered
+ * after the frames already submitted.  No graphics API is involved: every
+ * call writes plain buffers.  `out_on_device` = 1: `out` is a device pointer
+ * on the solver's device and the call returns without waiting; 0: `out` is
+ * host memory and the call waits for the result.                          */
+
+/* One instance record per rendered collider (RenderInstance,
+ * 50_render.metal:7-11).                                                  */
+typedef struct avbd_render_instance {
+    float model[16];   /* column-major 4x4; sizes scale boxes and spheres,
+                        * tori, capsules and hulls keep unit scale         */
+    float color[4];    /* rgb; w = shape kind (0 box .. 4 convex hull)    */
+    float params[4];   /* size x, size y, signed bounding radius,
+                        * 1 for dynamic bodies (shadow strength)           */
+} avbd_render_instance;
+
+/* Instance transforms and colours from the current poses (`build_instances`,
+ * 50_render.metal:34-97; `encodeBuildInstancesChecked`,
+ * GPUSolver.swift:4605-4646).  `colliders`: n collider ids (the reference
+ * renders colliders with `isRendered` whose body is not part of a soft
+ * surface, GPUSolver.swift:1942-1949); `colors_rgba`: n render colours (w > 0
+ * overrides the palette) or NULL; `color_mode` 0: palette by body id, 1: by
+ * the body's graph colour.  A static ground slab wider than 150 m gets an
+ * all-zero record.                                                         */
+int avbd_build_instances(avbd_solver* solver, const uint32_t* colliders, uint32_t n,
+                         const float* colors_rgba, uint32_t color_mode,
+                         avbd_render_instance* out, int out_on_device);
+
+/* Smooth normals of the soft surface (tet boundary faces and authored
+ * triangles): face normals, then an angle x area weighted gather per vertex
+ * (`soft_face_normals`, `soft_normals`, 50_render.metal:104-180).  `out`
+ * holds one float4 per body (xyz unit normal, w render thickness =
+ * |radius| x (cloth_scale for cloth vertices) x a curvature factor); entries
+ * of bodies off the surface are left untouched.  `cloth_scale` is
+ * `clothRenderScale` (Scene.swift:542).                                   */
+int avbd_soft_normals(avbd_solver* solver, float cloth_scale, float* out_xyzw,
+                      int out_on_device);
+
+/* A render-mesh vertex bound to four bodies (SkinBindingGPU,
+ * GPUTypes.swift:104-111): position = sum of weights x body positions; the
+ * normal follows the cofactor of the deformation gradient Ds * Dm^-1.      */
+typedef struct avbd_skin_binding {
+    uint32_t ids[4];
+    float weights[4];
+    float rest_normal[4];  /* xyz; normalised on upload, +z if zero        */
+    float inv0[4], inv1[4], inv2[4];  /* rows of Dm^-1; all zero = the
+                                         rest-pose inverse of the four
+                                         bodies' scene positions          */
+} avbd_skin_binding;
+
+/* Uploads the skin bindings (GPUSolver.swift:1849-1907), replacing earlier
+ * ones.  n = 0 clears them.                                                */
+int avbd_set_skin_bindings(avbd_solver* solver, const avbd_skin_binding* bindings,
+                           uint32_t n);
+
+/* Deformed skin vertices (`skin_deform`, 50_render.metal:182-212): per
+ * binding 8 floats, position (w = 1) then unit normal (w = 0).             */
+int avbd_skin_deform(avbd_solver* solver, float* out, int out_on_device);
+
+/* One Push-T environment of an observation batch (PushTEnvGPU,
+ * RL/PushTEnv.swift:28-32).                                               */
+typedef struct avbd_pusht_env {
+    uint32_t ids[4];   /* pusher tip, block bar, block stem, unused        */
+    float frame[4];    /* environment centre xy, goal position xy (local)  */
+    float goal[4];     /* goal yaw, half window, unused, unused            */
+} avbd_pusht_env;
+
+/* Top-down RGB observations of a Push-T batch (`pusht_obs`,
+ * 60_robotics.metal:21-69; `renderPushTObsChecked`, GPUSolver.swift:
+ * 2296-2325): num_envs x res x res x 3 bytes, row-major per environment,
+ * goal T green under the block T red under the pusher disc blue on a dark
+ * background.  res >= 2.                                                   */
+int avbd_render_pusht_obs(avbd_solver* solver, const avbd_pusht_env* envs,
+                          uint32_t num_envs, uint32_t res, uint8_t* out,
+                          int out_on_device);
+
 #ifdef __cplusplus
 }
 #endif

@@ -14,6 +14,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "build", "liboracle.so")
 SRC = [os.path.join(HERE, "avbd_oracle.cpp"), os.path.join(HERE, "oracle_cloth.cpp"),
+       os.path.join(HERE, "oracle_render.cpp"),
        os.path.join(HERE, "oracle_solver.h"), os.path.join(HERE, "oracle_math.h"),
        os.path.join(HERE, "..", "include", "avbd.h")]
 
@@ -25,7 +26,7 @@ def build(force: bool = False) -> str:
         return LIB
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
     cmd = ["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
-           "-fPIC", "-shared", "-o", LIB, SRC[0], SRC[1]]
+           "-fPIC", "-shared", "-o", LIB, SRC[0], SRC[1], SRC[2]]
     subprocess.check_call(cmd)
     return LIB
 
@@ -51,6 +52,12 @@ def lib():
         for name in ("oracle_set_joint_world_anchors", "oracle_set_motor_velocities", "oracle_set_motor_torques"):
             getattr(_lib, name).argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
         _lib.oracle_get_motor_states.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        _lib.oracle_build_instances.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32,
+                                                C.c_void_p]
+        _lib.oracle_soft_normals.argtypes = [C.c_void_p, C.c_float, C.c_void_p]
+        _lib.oracle_set_skin_bindings.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        _lib.oracle_skin_deform.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.oracle_render_pusht_obs.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
         _lib.oracle_max_constraint_error.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
         _lib.oracle_get_counters.argtypes = [C.c_void_p, C.c_void_p]
         _lib.oracle_debug_buffer_size.argtypes = [C.c_void_p, C.c_int]
@@ -133,6 +140,37 @@ class OracleSolver:
         ids = np.ascontiguousarray(joints, dtype=np.uint32)
         t = np.ascontiguousarray(torques, dtype=np.float32)
         lib().oracle_set_motor_torques(self._h, ids.ctypes.data, len(ids), t.ctypes.data)
+
+    def build_instances(self, colliders, colors=None, color_mode: int = 0):
+        ids = np.ascontiguousarray(colliders, dtype=np.uint32)
+        col = None if colors is None else np.ascontiguousarray(colors, dtype=np.float32).reshape(-1, 4)
+        out = np.zeros((len(ids), 24), np.float32)
+        lib().oracle_build_instances(self._h, ids.ctypes.data, len(ids), None if col is None else col.ctypes.data,
+                                     color_mode, out.ctypes.data)
+        return out
+
+    def soft_normals(self, cloth_scale: float = 0.0, out=None):
+        res = np.zeros((self.num_bodies, 4), np.float32) if out is None else np.ascontiguousarray(out, np.float32)
+        lib().oracle_soft_normals(self._h, cloth_scale, res.ctypes.data)
+        return res
+
+    def set_skin_bindings(self, bindings):
+        arr = (self._abi.SkinBinding * len(bindings))(*bindings)
+        self._num_skin = len(bindings)
+        rc = lib().oracle_set_skin_bindings(self._h, arr, len(bindings))
+        if rc != 0:
+            raise RuntimeError(f"oracle_set_skin_bindings failed: {rc}")
+
+    def skin_deform(self):
+        out = np.zeros((getattr(self, "_num_skin", 0), 8), np.float32)
+        lib().oracle_skin_deform(self._h, out.ctypes.data)
+        return out
+
+    def render_pusht_obs(self, envs, res: int = 64):
+        arr = (self._abi.PushTEnv * len(envs))(*envs)
+        out = np.zeros((len(envs), res, res, 3), np.uint8)
+        lib().oracle_render_pusht_obs(self._h, arr, len(envs), res, out.ctypes.data)
+        return out
 
     def motor_states(self, joints):
         ids = np.ascontiguousarray(joints, dtype=np.uint32)

@@ -120,6 +120,7 @@ int Solver::create(const avbd_scene_desc* s) {
         isDynamic[i] = is_dynamic_desc(b) ? 1 : 0;
         isParticle[i] = b.is_particle ? 1 : 0;
     }
+    scenePos = posLin;
 
     // colliders
     colOwner.assign(nc, 0); colShapeType.assign(nc, 0); colGroup.assign(nc, 0); colShared.assign(nc, 0);

@@ -153,6 +153,10 @@ struct Solver {
     std::vector<float> colFrictionS, colFrictionD;
     std::vector<uint32_t> colHullFirst, colHullCount;  // convex hull vertex range per collider
     std::vector<F3> hullVerts;
+    std::vector<F4> scenePos;  // body positions of the scene description (skin rest poses)
+    // skin bindings: ids, weights, rest normal, rows of Dm^-1
+    struct Skin { U4 ids; F4 weights; F3 restNormal, inv0, inv1, inv2; };
+    std::vector<Skin> skins;
     std::vector<uint32_t> hashedIdx, globalIdx, hashedRigidIdx;
     // constraints
     std::vector<JointGPU> joints;
