@@ -728,15 +728,13 @@ def pusht_scene(num_envs: int = 16, seed: int = 1):
 
 
 def pusht_env_table(envs, half_window: float = 3.25):
-    """PushTEnvGPU records of a batch (RL/PushTEnv.swift:569-575): the
-    window covers the whole arena."""
-    out = []
-    for r in envs:
-        t = abi.PushTEnv()
+    """PushTEnvGPU records of a batch (RL/PushTEnv.swift:569-575) as a
+    ctypes array: the window covers the whole arena."""
+    out = (abi.PushTEnv * len(envs))()
+    for t, r in zip(out, envs):
         t.ids[:] = [r["tip"], r["bar"], r["stem"], 0]
         t.frame[:] = [r["center"][0], r["center"][1], r["goal_pos"][0], r["goal_pos"][1]]
         t.goal[:] = [r["goal_yaw"], half_window, 0.0, 0.0]
-        out.append(t)
     return out
 
 

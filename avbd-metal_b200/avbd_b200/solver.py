@@ -272,7 +272,7 @@ class GPUSolver:
     def render_pusht_obs(self, envs, res: int = 64, device_out=None):
         """renderPushTObsChecked (GPUSolver.swift:2296-2325): uint8 array
         (num_envs, res, res, 3)."""
-        arr = (abi.PushTEnv * len(envs))(*envs)
+        arr = envs if isinstance(envs, C.Array) else (abi.PushTEnv * len(envs))(*envs)
         if device_out is not None:
             self._check(load_library().avbd_render_pusht_obs(self._h, arr, len(envs), res, device_out, 1))
             return None

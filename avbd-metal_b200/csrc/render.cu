@@ -167,15 +167,23 @@ __device__ __forceinline__ void heading(float4 q, float& cs, float& sn) {
 
 }  // namespace
 
-// Push-T observations (60_robotics.metal:21-69): one block row per
-// environment slice; the environment's shapes are set up once per block.
-// QUADS: each thread classifies four consecutive pixels of a row (res a
-// multiple of 4) and stores them as three 32-bit words.
+// Push-T observations (60_robotics.metal:21-69): blockIdx.y walks the
+// environments; each block sets up its environment's shapes once.
+// QUADS (res a multiple of 4): each thread classifies four consecutive
+// pixels of a row into three 32-bit words, the block stages its 3 KB run in
+// shared memory and writes it out as 16-byte stores (the run starts on a
+// 16-byte boundary: 3 * res^2 and 3072 are multiples of 48).  Otherwise one
+// thread per pixel with byte stores.
+constexpr uint32_t kObsThreads = 256;
 template <bool QUADS>
-__global__ void __launch_bounds__(256) k_pusht_obs(const float4* posLin, const float4* posAng, const PushTDev* envs,
-                                                   uint32_t numEnvs, uint32_t res, uint8_t* out) {
+__global__ void __launch_bounds__(kObsThreads) k_pusht_obs(const float4* posLin, const float4* posAng,
+                                                           const PushTDev* envs, uint32_t numEnvs, uint32_t res,
+                                                           uint8_t* out) {
     __shared__ float sh[20];
+    __shared__ uint32_t words[3 * kObsThreads];
     const uint32_t perEnv = QUADS ? res * res / 4u : res * res;
+    const uint32_t blockFirst = blockIdx.x * kObsThreads;
+    const uint32_t valid = perEnv - blockFirst < kObsThreads ? perEnv - blockFirst : kObsThreads;
     for (uint32_t e = blockIdx.y; e < numEnvs; e += gridDim.y) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -196,25 +204,26 @@ __global__ void __launch_bounds__(256) k_pusht_obs(const float4* posLin, const f
             sh[19] = (float)(res - 1u);
         }
         __syncthreads();
-        const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= perEnv) continue;
-        const uint32_t first = QUADS ? 4u * i : i;
-        const uint32_t py = first / res, px0 = first % res;
-        const float wy = sh[17] + ((float)py / sh[19] - 0.5f) * sh[18];
+        const uint32_t i = blockFirst + threadIdx.x;
         uint32_t kinds = 0;  // 2 bits per pixel: 0 background, 1 goal, 2 block, 3 pusher
-        constexpr int N = QUADS ? 4 : 1;
+        const uint32_t first = QUADS ? 4u * i : i;
+        if (threadIdx.x < valid) {
+            const uint32_t py = first / res, px0 = first % res;
+            const float wy = sh[17] + ((float)py / sh[19] - 0.5f) * sh[18];
+            constexpr int N = QUADS ? 4 : 1;
 #pragma unroll
-        for (int k = 0; k < N; k++) {
-            const float wx = sh[16] + ((float)(px0 + k) / sh[19] - 0.5f) * sh[18];
-            uint32_t kind = 0;
-            if (in_box(wx, wy, sh[0], sh[1], sh[4], sh[5], 0.5f, 0.125f) ||
-                in_box(wx, wy, sh[2], sh[3], sh[4], sh[5], 0.125f, 0.325f))
-                kind = 1;
-            if (in_box(wx, wy, sh[6], sh[7], sh[8], sh[9], 0.5f, 0.125f)) kind = 2;
-            if (in_box(wx, wy, sh[10], sh[11], sh[12], sh[13], 0.125f, 0.325f)) kind = 2;
-            const float dx = wx - sh[14], dy = wy - sh[15];
-            if (sqrtf(dx * dx + dy * dy) < 0.13f) kind = 3;
-            kinds |= kind << (2 * k);
+            for (int k = 0; k < N; k++) {
+                const float wx = sh[16] + ((float)(px0 + k) / sh[19] - 0.5f) * sh[18];
+                uint32_t kind = 0;
+                if (in_box(wx, wy, sh[0], sh[1], sh[4], sh[5], 0.5f, 0.125f) ||
+                    in_box(wx, wy, sh[2], sh[3], sh[4], sh[5], 0.125f, 0.325f))
+                    kind = 1;
+                if (in_box(wx, wy, sh[6], sh[7], sh[8], sh[9], 0.5f, 0.125f)) kind = 2;
+                if (in_box(wx, wy, sh[10], sh[11], sh[12], sh[13], 0.125f, 0.325f)) kind = 2;
+                const float dx = wx - sh[14], dy = wy - sh[15];
+                if (sqrtf(dx * dx + dy * dy) < 0.13f) kind = 3;
+                kinds |= kind << (2 * k);
+            }
         }
         // the four palette entries as bytes
         const uint32_t pal[4][3] = {
@@ -222,7 +231,6 @@ __global__ void __launch_bounds__(256) k_pusht_obs(const float4* posLin, const f
             {to_byte(0.10f), to_byte(0.55f), to_byte(0.12f)},
             {to_byte(0.85f), to_byte(0.15f), to_byte(0.12f)},
             {to_byte(0.2f), to_byte(0.4f), to_byte(0.95f)}};
-        uint8_t* o = out + ((size_t)e * res * res + first) * 3u;
         if (QUADS) {
             uint32_t b[12];
 #pragma unroll
@@ -230,12 +238,20 @@ __global__ void __launch_bounds__(256) k_pusht_obs(const float4* posLin, const f
                 const uint32_t kind = (kinds >> (2 * k)) & 3u;
                 b[3 * k] = pal[kind][0]; b[3 * k + 1] = pal[kind][1]; b[3 * k + 2] = pal[kind][2];
             }
-            uint32_t* w = reinterpret_cast<uint32_t*>(o);
-            w[0] = b[0] | (b[1] << 8) | (b[2] << 16) | (b[3] << 24);
-            w[1] = b[4] | (b[5] << 8) | (b[6] << 16) | (b[7] << 24);
-            w[2] = b[8] | (b[9] << 8) | (b[10] << 16) | (b[11] << 24);
-        } else {
+            words[3 * threadIdx.x] = b[0] | (b[1] << 8) | (b[2] << 16) | (b[3] << 24);
+            words[3 * threadIdx.x + 1] = b[4] | (b[5] << 8) | (b[6] << 16) | (b[7] << 24);
+            words[3 * threadIdx.x + 2] = b[8] | (b[9] << 8) | (b[10] << 16) | (b[11] << 24);
+            __syncthreads();
+            // 3 * valid words from byte (e * res^2 + 4 * blockFirst) * 3
+            uint32_t* dst = reinterpret_cast<uint32_t*>(out + ((size_t)e * res * res + 4u * (size_t)blockFirst) * 3u);
+            const uint32_t nWords = 3u * valid, nVec = nWords / 4u;
+            for (uint32_t v = threadIdx.x; v < nVec; v += kObsThreads)
+                reinterpret_cast<uint4*>(dst)[v] =
+                    make_uint4(words[4 * v], words[4 * v + 1], words[4 * v + 2], words[4 * v + 3]);
+            for (uint32_t w = 4u * nVec + threadIdx.x; w < nWords; w += kObsThreads) dst[w] = words[w];
+        } else if (threadIdx.x < valid) {
             const uint32_t kind = kinds & 3u;
+            uint8_t* o = out + ((size_t)e * res * res + first) * 3u;
             o[0] = (uint8_t)pal[kind][0]; o[1] = (uint8_t)pal[kind][1]; o[2] = (uint8_t)pal[kind][2];
         }
     }
@@ -266,9 +282,9 @@ void launch_pusht_obs(const float4* posLin, const float4* posAng, const PushTDev
     if (!numEnvs) return;
     const bool quads = res % 4u == 0u;
     const uint32_t perEnv = quads ? res * res / 4u : res * res;
-    const dim3 grid(blocks_for(perEnv, 256), numEnvs < 65535u ? numEnvs : 65535u);
-    if (quads) k_pusht_obs<true><<<grid, 256, 0, st>>>(posLin, posAng, envs, numEnvs, res, out);
-    else k_pusht_obs<false><<<grid, 256, 0, st>>>(posLin, posAng, envs, numEnvs, res, out);
+    const dim3 grid(blocks_for(perEnv, kObsThreads), numEnvs < 65535u ? numEnvs : 65535u);
+    if (quads) k_pusht_obs<true><<<grid, kObsThreads, 0, st>>>(posLin, posAng, envs, numEnvs, res, out);
+    else k_pusht_obs<false><<<grid, kObsThreads, 0, st>>>(posLin, posAng, envs, numEnvs, res, out);
 }
 
 }  // namespace avbd

@@ -168,6 +168,11 @@ struct avbd_solver {
     // skin bindings (replaced by each upload)
     SkinBinding* skin = nullptr;
     uint32_t numSkin = 0;
+    // the last Push-T environment table, kept on the device while the
+    // caller passes the same records
+    std::vector<avbd_pusht_env> pushtHost;
+    PushTDev* pushtDev = nullptr;
+    size_t pushtCap = 0;
 
     ~avbd_solver() {
         if (launch) cudaStreamSynchronize(launch);
@@ -178,6 +183,7 @@ struct avbd_solver {
         for (void* p : allocations) cudaFree(p);
         if (stage) cudaFree(stage);
         if (skin) cudaFree(skin);
+        if (pushtDev) cudaFree(pushtDev);
         if (hostLatch) cudaFreeHost(hostLatch);
         if (hostCounters) cudaFreeHost(hostCounters);
         if (forkEvent) cudaEventDestroy(forkEvent);
@@ -1229,30 +1235,45 @@ int avbd_skin_deform(avbd_solver* s, float* out, int out_on_device) {
 int avbd_render_pusht_obs(avbd_solver* s, const avbd_pusht_env* envs, uint32_t num_envs, uint32_t res,
                           uint8_t* out, int out_on_device) {
     if (!s || (num_envs && (!envs || !out)) || res < 2 || res > 4096) return AVBD_ERR_INVALID_ARGUMENT;
-    const uint32_t nb = s->H.numBodies;
-    std::vector<PushTDev> table(num_envs);
-    for (uint32_t e = 0; e < num_envs; e++) {
-        const avbd_pusht_env& v = envs[e];
-        for (int k = 0; k < 3; k++)
-            if (v.ids[k] >= nb) return AVBD_ERR_INVALID_ARGUMENT;
-        PushTDev& t = table[e];
-        t.ids = make_uint4(v.ids[0], v.ids[1], v.ids[2], v.ids[3]);
-        t.frame = make_float4(v.frame[0], v.frame[1], v.frame[2], v.frame[3]);
-        t.goalYaw = v.goal[0];
-        t.halfWin = v.goal[1];
-        goal_heading(v.goal[0], t.goalCos, t.goalSin);
-    }
-    if (out_on_device && (res % 4u == 0u) && (reinterpret_cast<uintptr_t>(out) & 3u)) return AVBD_ERR_INVALID_ARGUMENT;
+    if (out_on_device && (res % 4u == 0u) && (reinterpret_cast<uintptr_t>(out) & 15u)) return AVBD_ERR_INVALID_ARGUMENT;
     if (s->failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
     if (num_envs == 0) return AVBD_OK;
-    const size_t inBytes = sizeof(PushTDev) * (size_t)num_envs;
+    const bool same = s->pushtHost.size() == num_envs &&
+                      std::memcmp(s->pushtHost.data(), envs, sizeof(avbd_pusht_env) * (size_t)num_envs) == 0;
+    if (!same) {
+        const uint32_t nb = s->H.numBodies;
+        std::vector<PushTDev> table(num_envs);
+        for (uint32_t e = 0; e < num_envs; e++) {
+            const avbd_pusht_env& v = envs[e];
+            for (int k = 0; k < 3; k++)
+                if (v.ids[k] >= nb) return AVBD_ERR_INVALID_ARGUMENT;
+            PushTDev& t = table[e];
+            t.ids = make_uint4(v.ids[0], v.ids[1], v.ids[2], v.ids[3]);
+            t.frame = make_float4(v.frame[0], v.frame[1], v.frame[2], v.frame[3]);
+            t.goalYaw = v.goal[0];
+            t.halfWin = v.goal[1];
+            goal_heading(v.goal[0], t.goalCos, t.goalSin);
+        }
+        // earlier observation launches may still read the old table
+        if (!s->check(cudaStreamSynchronize(s->launch), "Push-T table")) return AVBD_ERR_RUNTIME_FAILURE;
+        if (num_envs > s->pushtCap) {
+            if (s->pushtDev) cudaFree(s->pushtDev);
+            s->pushtDev = nullptr;
+            s->pushtCap = 0;
+            if (cudaMalloc(&s->pushtDev, sizeof(PushTDev) * (size_t)num_envs) != cudaSuccess) return AVBD_ERR_ALLOC_FAILED;
+            s->pushtCap = num_envs;
+        }
+        if (!s->check(cudaMemcpy(s->pushtDev, table.data(), sizeof(PushTDev) * (size_t)num_envs,
+                                 cudaMemcpyHostToDevice), "Push-T table"))
+            return AVBD_ERR_RUNTIME_FAILURE;
+        s->pushtHost.assign(envs, envs + num_envs);
+    }
     const size_t outBytes = (size_t)num_envs * res * res * 3;
-    size_t outOff;
-    uint8_t* st = render_staging(s, inBytes, out_on_device ? 0 : outBytes, outOff);
-    if (!st) return AVBD_ERR_ALLOC_FAILED;
-    cudaMemcpyAsync(st, table.data(), inBytes, cudaMemcpyHostToDevice, s->launch);
+    size_t outOff = 0;
+    uint8_t* st = out_on_device ? nullptr : render_staging(s, 0, outBytes, outOff);
+    if (!out_on_device && !st) return AVBD_ERR_ALLOC_FAILED;
     uint8_t* dOut = out_on_device ? out : st + outOff;
-    launch_pusht_obs(s->d.posLin, s->d.posAng, reinterpret_cast<PushTDev*>(st), num_envs, res, dOut, s->launch);
+    launch_pusht_obs(s->d.posLin, s->d.posAng, s->pushtDev, num_envs, res, dOut, s->launch);
     return render_finish(s, out_on_device ? nullptr : out, dOut, outBytes, "Push-T observation");
 }
 

@@ -551,7 +551,9 @@ typedef struct avbd_pusht_env {
  * 60_robotics.metal:21-69; `renderPushTObsChecked`, GPUSolver.swift:
  * 2296-2325): num_envs x res x res x 3 bytes, row-major per environment,
  * goal T green under the block T red under the pusher disc blue on a dark
- * background.  res >= 2.                                                   */
+ * background.  2 <= res <= 4096; a device `out` must be 16-byte aligned
+ * when res is a multiple of 4.  The table is kept on the device while later
+ * calls pass the same records.                                             */
 int avbd_render_pusht_obs(avbd_solver* solver, const avbd_pusht_env* envs,
                           uint32_t num_envs, uint32_t res, uint8_t* out,
                           int out_on_device);

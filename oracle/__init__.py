@@ -167,7 +167,7 @@ class OracleSolver:
         return out
 
     def render_pusht_obs(self, envs, res: int = 64):
-        arr = (self._abi.PushTEnv * len(envs))(*envs)
+        arr = envs if isinstance(envs, C.Array) else (self._abi.PushTEnv * len(envs))(*envs)
         out = np.zeros((len(envs), res, res, 3), np.uint8)
         lib().oracle_render_pusht_obs(self._h, arr, len(envs), res, out.ctypes.data)
         return out
