@@ -169,21 +169,35 @@ __device__ __forceinline__ void heading(float4 q, float& cs, float& sn) {
 
 // Push-T observations (60_robotics.metal:21-69): blockIdx.y walks the
 // environments; each block sets up its environment's shapes once.
+// The pixel-centre offsets (float)j / (res - 1) - 0.5 are a shared table
+// (the same division per pixel, done once per block).  A quad of pixels
+// whose centre is farther from a shape's centre than the shape's bounding
+// radius plus two pixel widths cannot touch it, so that shape's exact test
+// is skipped (most quads are background).
 // QUADS (res a multiple of 4): each thread classifies four consecutive
 // pixels of a row into three 32-bit words, the block stages its 3 KB run in
 // shared memory and writes it out as 16-byte stores (the run starts on a
 // 16-byte boundary: 3 * res^2 and 3072 are multiples of 48).  Otherwise one
 // thread per pixel with byte stores.
 constexpr uint32_t kObsThreads = 256;
+
+__device__ __forceinline__ bool near_(float x, float y, float cx, float cy, float r2) {
+    const float dx = x - cx, dy = y - cy;
+    return dx * dx + dy * dy <= r2;
+}
+
 template <bool QUADS>
 __global__ void __launch_bounds__(kObsThreads) k_pusht_obs(const float4* posLin, const float4* posAng,
                                                            const PushTDev* envs, uint32_t numEnvs, uint32_t res,
                                                            uint8_t* out) {
-    __shared__ float sh[20];
+    extern __shared__ float offs[];  // res entries
+    __shared__ float sh[24];
     __shared__ uint32_t words[3 * kObsThreads];
     const uint32_t perEnv = QUADS ? res * res / 4u : res * res;
     const uint32_t blockFirst = blockIdx.x * kObsThreads;
     const uint32_t valid = perEnv - blockFirst < kObsThreads ? perEnv - blockFirst : kObsThreads;
+    const float denom = (float)(res - 1u);
+    for (uint32_t j = threadIdx.x; j < res; j += kObsThreads) offs[j] = (float)j / denom - 0.5f;
     for (uint32_t e = blockIdx.y; e < numEnvs; e += gridDim.y) {
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -201,28 +215,42 @@ __global__ void __launch_bounds__(kObsThreads) k_pusht_obs(const float4* posLin,
             sh[14] = posLin[env.ids.x].x; sh[15] = posLin[env.ids.x].y;
             sh[16] = env.frame.x; sh[17] = env.frame.y;
             sh[18] = 2.0f * env.halfWin;
-            sh[19] = (float)(res - 1u);
+            // squared cull radii: bar (0.5 x 0.125 half extents), stem
+            // (0.125 x 0.325), pusher disc (0.13), each plus two pixels
+            const float pw = fabsf(sh[18]) / denom;
+            const float rb = 0.5154f + 2.0f * pw, rs = 0.3483f + 2.0f * pw, rt = 0.13f + 2.0f * pw;
+            sh[19] = rb * rb; sh[20] = rs * rs; sh[21] = rt * rt;
         }
         __syncthreads();
         const uint32_t i = blockFirst + threadIdx.x;
         uint32_t kinds = 0;  // 2 bits per pixel: 0 background, 1 goal, 2 block, 3 pusher
         const uint32_t first = QUADS ? 4u * i : i;
         if (threadIdx.x < valid) {
-            const uint32_t py = first / res, px0 = first % res;
-            const float wy = sh[17] + ((float)py / sh[19] - 0.5f) * sh[18];
             constexpr int N = QUADS ? 4 : 1;
+            const uint32_t py = first / res, px0 = first % res;
+            const float wy = sh[17] + offs[py] * sh[18];
+            float wx[N];
 #pragma unroll
-            for (int k = 0; k < N; k++) {
-                const float wx = sh[16] + ((float)(px0 + k) / sh[19] - 0.5f) * sh[18];
-                uint32_t kind = 0;
-                if (in_box(wx, wy, sh[0], sh[1], sh[4], sh[5], 0.5f, 0.125f) ||
-                    in_box(wx, wy, sh[2], sh[3], sh[4], sh[5], 0.125f, 0.325f))
-                    kind = 1;
-                if (in_box(wx, wy, sh[6], sh[7], sh[8], sh[9], 0.5f, 0.125f)) kind = 2;
-                if (in_box(wx, wy, sh[10], sh[11], sh[12], sh[13], 0.125f, 0.325f)) kind = 2;
-                const float dx = wx - sh[14], dy = wy - sh[15];
-                if (sqrtf(dx * dx + dy * dy) < 0.13f) kind = 3;
-                kinds |= kind << (2 * k);
+            for (int k = 0; k < N; k++) wx[k] = sh[16] + offs[px0 + k] * sh[18];
+            const float cx = 0.5f * (wx[0] + wx[N - 1]);
+            const bool gBar = near_(cx, wy, sh[0], sh[1], sh[19]), gStem = near_(cx, wy, sh[2], sh[3], sh[20]);
+            const bool bBar = near_(cx, wy, sh[6], sh[7], sh[19]), bStem = near_(cx, wy, sh[10], sh[11], sh[20]);
+            const bool tip = near_(cx, wy, sh[14], sh[15], sh[21]);
+            if (gBar || gStem || bBar || bStem || tip) {
+#pragma unroll
+                for (int k = 0; k < N; k++) {
+                    uint32_t kind = 0;
+                    if ((gBar && in_box(wx[k], wy, sh[0], sh[1], sh[4], sh[5], 0.5f, 0.125f)) ||
+                        (gStem && in_box(wx[k], wy, sh[2], sh[3], sh[4], sh[5], 0.125f, 0.325f)))
+                        kind = 1;
+                    if (bBar && in_box(wx[k], wy, sh[6], sh[7], sh[8], sh[9], 0.5f, 0.125f)) kind = 2;
+                    if (bStem && in_box(wx[k], wy, sh[10], sh[11], sh[12], sh[13], 0.125f, 0.325f)) kind = 2;
+                    if (tip) {
+                        const float dx = wx[k] - sh[14], dy = wy - sh[15];
+                        if (sqrtf(dx * dx + dy * dy) < 0.13f) kind = 3;
+                    }
+                    kinds |= kind << (2 * k);
+                }
             }
         }
         // the four palette entries as bytes
@@ -283,8 +311,9 @@ void launch_pusht_obs(const float4* posLin, const float4* posAng, const PushTDev
     const bool quads = res % 4u == 0u;
     const uint32_t perEnv = quads ? res * res / 4u : res * res;
     const dim3 grid(blocks_for(perEnv, kObsThreads), numEnvs < 65535u ? numEnvs : 65535u);
-    if (quads) k_pusht_obs<true><<<grid, kObsThreads, 0, st>>>(posLin, posAng, envs, numEnvs, res, out);
-    else k_pusht_obs<false><<<grid, kObsThreads, 0, st>>>(posLin, posAng, envs, numEnvs, res, out);
+    const size_t smem = sizeof(float) * res;  // res <= 4096: at most 16 KB
+    if (quads) k_pusht_obs<true><<<grid, kObsThreads, smem, st>>>(posLin, posAng, envs, numEnvs, res, out);
+    else k_pusht_obs<false><<<grid, kObsThreads, smem, st>>>(posLin, posAng, envs, numEnvs, res, out);
 }
 
 }  // namespace avbd

@@ -84,6 +84,11 @@ def parse():
     ap.add_argument("--warm-start", choices=["plain", "learned"], default="plain",
                     help="with --frames-only: the warm start of the frames")
     ap.add_argument("--iterations", type=int, default=0, help="with --frames-only: override the iterations")
+    ap.add_argument("--pusht-obs", action="store_true",
+                    help="time the Push-T pixel-observation kernel instead (--obs-envs x --obs-res^2 x 3 "
+                         "bytes per launch) and print its own JSON line")
+    ap.add_argument("--obs-envs", type=int, default=4096)
+    ap.add_argument("--obs-res", type=int, default=64)
     args = ap.parse_args()
     global WORKLOAD_KEY, WORKLOAD
     WORKLOAD_KEY, WORKLOAD = args.workload, WORKLOADS[args.workload]
@@ -365,6 +370,43 @@ def run_frames(args, local):
     solver.close()
 
 
+def run_pusht_obs(args, local):
+    """The Push-T observation kernel alone: a batch of --obs-envs
+    environments after a few frames, --steps back-to-back renders into one
+    device buffer timed with CUDA events on the solver stream (the output is
+    larger than nothing cached: each launch writes every byte once)."""
+    import numpy as np
+    import torch
+    from avbd_b200 import GPUSolver, demos
+    torch.cuda.set_device(local)
+    scene, envs = demos.pusht_scene(args.obs_envs, seed=1)
+    solver = GPUSolver(scene, device=local)
+    stream = torch.cuda.Stream()
+    solver.set_stream(stream.cuda_stream)
+    solver.step(max(1, args.warmup))
+    table = demos.pusht_env_table(envs)
+    res = args.obs_res
+    out = torch.empty((args.obs_envs, res, res, 3), dtype=torch.uint8, device="cuda")
+    for _ in range(3):
+        solver.render_pusht_obs(table, res, device_out=out.data_ptr())
+    solver.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(args.steps):
+        solver.render_pusht_obs(table, res, device_out=out.data_ptr())
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / args.steps
+    nbytes = args.obs_envs * res * res * 3
+    peak, kind = measured_peaks()
+    host = solver.render_pusht_obs(table, res)
+    assert np.array_equal(host, out.cpu().numpy())
+    print(json.dumps({"workload": "pusht-obs", "envs": args.obs_envs, "res": res, "bytes_per_launch": nbytes,
+                      "launches": args.steps, "ms_per_launch": ms, "achieved_gbs": nbytes / ms / 1e6,
+                      "peak_gbs": peak, "peak_kind": kind, "frac": nbytes / ms / 1e6 / peak}), flush=True)
+    solver.close()
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -544,6 +586,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.pusht_obs:
+            run_pusht_obs(args, local)
         elif args.frames_only:
             run_frames(args, local)
         else:
