@@ -188,8 +188,9 @@ void launch_soft_normals(const DevPtrs& d, uint32_t numTris, const uint32_t* sur
                          const uint32_t* vtCount, const uint32_t* vtList, uint32_t numSurf, float4* faceN,
                          float clothScale, float4* out, cudaStream_t st);
 void launch_skin_deform(const float4* posLin, const SkinBinding* b, uint32_t n, float4* out, cudaStream_t st);
+// shapes: 6 float4 of scratch per environment
 void launch_pusht_obs(const float4* posLin, const float4* posAng, const PushTDev* envs, uint32_t numEnvs,
-                      uint32_t res, uint8_t* out, cudaStream_t st);
+                      uint32_t res, float4* shapes, uint8_t* out, cudaStream_t st);
 // spinners and legacy rate motors, then the end-of-frame failure check
 void launch_frame_end(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 

@@ -167,13 +167,16 @@ __device__ __forceinline__ void heading(float4 q, float& cs, float& sn) {
 
 }  // namespace
 
-// Push-T observations (60_robotics.metal:21-69): blockIdx.y walks the
-// environments; each block sets up its environment's shapes once.
-// The pixel-centre offsets (float)j / (res - 1) - 0.5 are a shared table
-// (the same division per pixel, done once per block).  A quad of pixels
-// whose centre is farther from a shape's centre than the shape's bounding
-// radius plus two pixel widths cannot touch it, so that shape's exact test
-// is skipped (most quads are background).
+// Push-T observations (60_robotics.metal:21-69) in two passes.
+// k_pusht_shapes: one thread per environment places its shapes (goal T from
+// the table, block T and pusher from the body poses) into 24 floats.
+// k_pusht_obs: blockIdx.y walks the environments; every thread reads its
+// environment's 24 floats (the same address across the block) and
+// classifies pixels.  The pixel-centre offsets (float)j / (res - 1) - 0.5
+// are a shared table (the same division as per pixel, done once per block).
+// A quad of pixels whose centre is farther from a shape's centre than the
+// shape's bounding radius plus two pixel widths cannot touch it, so that
+// shape's exact test is skipped (most quads are background).
 // QUADS (res a multiple of 4): each thread classifies four consecutive
 // pixels of a row into three 32-bit words, the block stages its 3 KB run in
 // shared memory and writes it out as 16-byte stores (the run starts on a
@@ -186,67 +189,75 @@ __device__ __forceinline__ bool near_(float x, float y, float cx, float cy, floa
     return dx * dx + dy * dy <= r2;
 }
 
+__global__ void k_pusht_shapes(const float4* posLin, const float4* posAng, const PushTDev* envs, uint32_t numEnvs,
+                               uint32_t res, float4* shapes) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= numEnvs) return;
+    const PushTDev env = envs[e];
+    float sh[24];
+    const float gx = env.frame.z + env.frame.x, gy = env.frame.w + env.frame.y;
+    const float gc = env.goalCos, gs = env.goalSin;
+    sh[0] = gx + (-gs) * 0.125f; sh[1] = gy + gc * 0.125f;    // goal bar centre
+    sh[2] = gx + gs * 0.325f;    sh[3] = gy + (-gc) * 0.325f; // goal stem centre
+    sh[4] = gc; sh[5] = gs;
+    float cs, sn;
+    heading(posAng[env.ids.y], cs, sn);
+    sh[6] = posLin[env.ids.y].x; sh[7] = posLin[env.ids.y].y; sh[8] = cs; sh[9] = sn;
+    heading(posAng[env.ids.z], cs, sn);
+    sh[10] = posLin[env.ids.z].x; sh[11] = posLin[env.ids.z].y; sh[12] = cs; sh[13] = sn;
+    sh[14] = posLin[env.ids.x].x; sh[15] = posLin[env.ids.x].y;
+    sh[16] = env.frame.x; sh[17] = env.frame.y;
+    sh[18] = 2.0f * env.halfWin;
+    // squared cull radii: bar (0.5 x 0.125 half extents), stem (0.125 x
+    // 0.325), pusher disc (0.13), each plus two pixel widths
+    const float pw = fabsf(sh[18]) / (float)(res - 1u);
+    const float rb = 0.5154f + 2.0f * pw, rs = 0.3483f + 2.0f * pw, rt = 0.13f + 2.0f * pw;
+    sh[19] = rb * rb; sh[20] = rs * rs; sh[21] = rt * rt;
+    sh[22] = 0.0f; sh[23] = 0.0f;
+    for (int k = 0; k < 6; k++) shapes[6 * e + k] = make_float4(sh[4 * k], sh[4 * k + 1], sh[4 * k + 2], sh[4 * k + 3]);
+}
+
 template <bool QUADS>
-__global__ void __launch_bounds__(kObsThreads) k_pusht_obs(const float4* posLin, const float4* posAng,
-                                                           const PushTDev* envs, uint32_t numEnvs, uint32_t res,
+__global__ void __launch_bounds__(kObsThreads) k_pusht_obs(const float4* shapes, uint32_t numEnvs, uint32_t res,
                                                            uint8_t* out) {
     extern __shared__ float offs[];  // res entries
-    __shared__ float sh[24];
     __shared__ uint32_t words[3 * kObsThreads];
-    const uint32_t perEnv = QUADS ? res * res / 4u : res * res;
+    const uint32_t perRow = QUADS ? res / 4u : res;
+    const uint32_t perEnv = perRow * res;
     const uint32_t blockFirst = blockIdx.x * kObsThreads;
     const uint32_t valid = perEnv - blockFirst < kObsThreads ? perEnv - blockFirst : kObsThreads;
     const float denom = (float)(res - 1u);
     for (uint32_t j = threadIdx.x; j < res; j += kObsThreads) offs[j] = (float)j / denom - 0.5f;
+    __syncthreads();
+    // row and column of this thread's first pixel (quad index / row length)
+    const uint32_t i = blockFirst + threadIdx.x;
+    uint32_t py = i / perRow;
+    const uint32_t px0 = (QUADS ? 4u : 1u) * (i - py * perRow);
     for (uint32_t e = blockIdx.y; e < numEnvs; e += gridDim.y) {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const PushTDev env = envs[e];
-            const float gx = env.frame.z + env.frame.x, gy = env.frame.w + env.frame.y;
-            const float gc = env.goalCos, gs = env.goalSin;
-            sh[0] = gx + (-gs) * 0.125f; sh[1] = gy + gc * 0.125f;    // goal bar centre
-            sh[2] = gx + gs * 0.325f;    sh[3] = gy + (-gc) * 0.325f; // goal stem centre
-            sh[4] = gc; sh[5] = gs;
-            float cs, sn;
-            heading(posAng[env.ids.y], cs, sn);
-            sh[6] = posLin[env.ids.y].x; sh[7] = posLin[env.ids.y].y; sh[8] = cs; sh[9] = sn;
-            heading(posAng[env.ids.z], cs, sn);
-            sh[10] = posLin[env.ids.z].x; sh[11] = posLin[env.ids.z].y; sh[12] = cs; sh[13] = sn;
-            sh[14] = posLin[env.ids.x].x; sh[15] = posLin[env.ids.x].y;
-            sh[16] = env.frame.x; sh[17] = env.frame.y;
-            sh[18] = 2.0f * env.halfWin;
-            // squared cull radii: bar (0.5 x 0.125 half extents), stem
-            // (0.125 x 0.325), pusher disc (0.13), each plus two pixels
-            const float pw = fabsf(sh[18]) / denom;
-            const float rb = 0.5154f + 2.0f * pw, rs = 0.3483f + 2.0f * pw, rt = 0.13f + 2.0f * pw;
-            sh[19] = rb * rb; sh[20] = rs * rs; sh[21] = rt * rt;
-        }
-        __syncthreads();
-        const uint32_t i = blockFirst + threadIdx.x;
+        const float4* S = shapes + 6 * (size_t)e;
+        const float4 s0 = S[0], s1 = S[1], s2 = S[2], s3 = S[3], s4 = S[4], s5 = S[5];
         uint32_t kinds = 0;  // 2 bits per pixel: 0 background, 1 goal, 2 block, 3 pusher
-        const uint32_t first = QUADS ? 4u * i : i;
         if (threadIdx.x < valid) {
             constexpr int N = QUADS ? 4 : 1;
-            const uint32_t py = first / res, px0 = first % res;
-            const float wy = sh[17] + offs[py] * sh[18];
+            const float wy = s4.y + offs[py] * s4.z;
             float wx[N];
 #pragma unroll
-            for (int k = 0; k < N; k++) wx[k] = sh[16] + offs[px0 + k] * sh[18];
+            for (int k = 0; k < N; k++) wx[k] = s4.x + offs[px0 + k] * s4.z;
             const float cx = 0.5f * (wx[0] + wx[N - 1]);
-            const bool gBar = near_(cx, wy, sh[0], sh[1], sh[19]), gStem = near_(cx, wy, sh[2], sh[3], sh[20]);
-            const bool bBar = near_(cx, wy, sh[6], sh[7], sh[19]), bStem = near_(cx, wy, sh[10], sh[11], sh[20]);
-            const bool tip = near_(cx, wy, sh[14], sh[15], sh[21]);
+            const bool gBar = near_(cx, wy, s0.x, s0.y, s4.w), gStem = near_(cx, wy, s0.z, s0.w, s5.x);
+            const bool bBar = near_(cx, wy, s1.z, s1.w, s4.w), bStem = near_(cx, wy, s2.z, s2.w, s5.x);
+            const bool tip = near_(cx, wy, s3.z, s3.w, s5.y);
             if (gBar || gStem || bBar || bStem || tip) {
 #pragma unroll
                 for (int k = 0; k < N; k++) {
                     uint32_t kind = 0;
-                    if ((gBar && in_box(wx[k], wy, sh[0], sh[1], sh[4], sh[5], 0.5f, 0.125f)) ||
-                        (gStem && in_box(wx[k], wy, sh[2], sh[3], sh[4], sh[5], 0.125f, 0.325f)))
+                    if ((gBar && in_box(wx[k], wy, s0.x, s0.y, s1.x, s1.y, 0.5f, 0.125f)) ||
+                        (gStem && in_box(wx[k], wy, s0.z, s0.w, s1.x, s1.y, 0.125f, 0.325f)))
                         kind = 1;
-                    if (bBar && in_box(wx[k], wy, sh[6], sh[7], sh[8], sh[9], 0.5f, 0.125f)) kind = 2;
-                    if (bStem && in_box(wx[k], wy, sh[10], sh[11], sh[12], sh[13], 0.125f, 0.325f)) kind = 2;
+                    if (bBar && in_box(wx[k], wy, s1.z, s1.w, s2.x, s2.y, 0.5f, 0.125f)) kind = 2;
+                    if (bStem && in_box(wx[k], wy, s2.z, s2.w, s3.x, s3.y, 0.125f, 0.325f)) kind = 2;
                     if (tip) {
-                        const float dx = wx[k] - sh[14], dy = wy - sh[15];
+                        const float dx = wx[k] - s3.z, dy = wy - s3.w;
                         if (sqrtf(dx * dx + dy * dy) < 0.13f) kind = 3;
                     }
                     kinds |= kind << (2 * k);
@@ -266,6 +277,7 @@ __global__ void __launch_bounds__(kObsThreads) k_pusht_obs(const float4* posLin,
                 const uint32_t kind = (kinds >> (2 * k)) & 3u;
                 b[3 * k] = pal[kind][0]; b[3 * k + 1] = pal[kind][1]; b[3 * k + 2] = pal[kind][2];
             }
+            __syncthreads();  // the previous environment's words are out
             words[3 * threadIdx.x] = b[0] | (b[1] << 8) | (b[2] << 16) | (b[3] << 24);
             words[3 * threadIdx.x + 1] = b[4] | (b[5] << 8) | (b[6] << 16) | (b[7] << 24);
             words[3 * threadIdx.x + 2] = b[8] | (b[9] << 8) | (b[10] << 16) | (b[11] << 24);
@@ -279,7 +291,7 @@ __global__ void __launch_bounds__(kObsThreads) k_pusht_obs(const float4* posLin,
             for (uint32_t w = 4u * nVec + threadIdx.x; w < nWords; w += kObsThreads) dst[w] = words[w];
         } else if (threadIdx.x < valid) {
             const uint32_t kind = kinds & 3u;
-            uint8_t* o = out + ((size_t)e * res * res + first) * 3u;
+            uint8_t* o = out + ((size_t)e * res * res + i) * 3u;
             o[0] = (uint8_t)pal[kind][0]; o[1] = (uint8_t)pal[kind][1]; o[2] = (uint8_t)pal[kind][2];
         }
     }
@@ -306,14 +318,15 @@ void launch_skin_deform(const float4* posLin, const SkinBinding* b, uint32_t n, 
 }
 
 void launch_pusht_obs(const float4* posLin, const float4* posAng, const PushTDev* envs, uint32_t numEnvs,
-                      uint32_t res, uint8_t* out, cudaStream_t st) {
+                      uint32_t res, float4* shapes, uint8_t* out, cudaStream_t st) {
     if (!numEnvs) return;
+    k_pusht_shapes<<<blocks_for(numEnvs, 128), 128, 0, st>>>(posLin, posAng, envs, numEnvs, res, shapes);
     const bool quads = res % 4u == 0u;
     const uint32_t perEnv = quads ? res * res / 4u : res * res;
     const dim3 grid(blocks_for(perEnv, kObsThreads), numEnvs < 65535u ? numEnvs : 65535u);
     const size_t smem = sizeof(float) * res;  // res <= 4096: at most 16 KB
-    if (quads) k_pusht_obs<true><<<grid, kObsThreads, smem, st>>>(posLin, posAng, envs, numEnvs, res, out);
-    else k_pusht_obs<false><<<grid, kObsThreads, smem, st>>>(posLin, posAng, envs, numEnvs, res, out);
+    if (quads) k_pusht_obs<true><<<grid, kObsThreads, smem, st>>>(shapes, numEnvs, res, out);
+    else k_pusht_obs<false><<<grid, kObsThreads, smem, st>>>(shapes, numEnvs, res, out);
 }
 
 }  // namespace avbd

@@ -172,6 +172,7 @@ struct avbd_solver {
     // caller passes the same records
     std::vector<avbd_pusht_env> pushtHost;
     PushTDev* pushtDev = nullptr;
+    float4* pushtShapes = nullptr;  // 6 float4 per environment
     size_t pushtCap = 0;
 
     ~avbd_solver() {
@@ -184,6 +185,7 @@ struct avbd_solver {
         if (stage) cudaFree(stage);
         if (skin) cudaFree(skin);
         if (pushtDev) cudaFree(pushtDev);
+        if (pushtShapes) cudaFree(pushtShapes);
         if (hostLatch) cudaFreeHost(hostLatch);
         if (hostCounters) cudaFreeHost(hostCounters);
         if (forkEvent) cudaEventDestroy(forkEvent);
@@ -1258,9 +1260,13 @@ int avbd_render_pusht_obs(avbd_solver* s, const avbd_pusht_env* envs, uint32_t n
         if (!s->check(cudaStreamSynchronize(s->launch), "Push-T table")) return AVBD_ERR_RUNTIME_FAILURE;
         if (num_envs > s->pushtCap) {
             if (s->pushtDev) cudaFree(s->pushtDev);
+            if (s->pushtShapes) cudaFree(s->pushtShapes);
             s->pushtDev = nullptr;
+            s->pushtShapes = nullptr;
             s->pushtCap = 0;
-            if (cudaMalloc(&s->pushtDev, sizeof(PushTDev) * (size_t)num_envs) != cudaSuccess) return AVBD_ERR_ALLOC_FAILED;
+            if (cudaMalloc(&s->pushtDev, sizeof(PushTDev) * (size_t)num_envs) != cudaSuccess ||
+                cudaMalloc(&s->pushtShapes, 6 * sizeof(float4) * (size_t)num_envs) != cudaSuccess)
+                return AVBD_ERR_ALLOC_FAILED;
             s->pushtCap = num_envs;
         }
         if (!s->check(cudaMemcpy(s->pushtDev, table.data(), sizeof(PushTDev) * (size_t)num_envs,
@@ -1273,7 +1279,7 @@ int avbd_render_pusht_obs(avbd_solver* s, const avbd_pusht_env* envs, uint32_t n
     uint8_t* st = out_on_device ? nullptr : render_staging(s, 0, outBytes, outOff);
     if (!out_on_device && !st) return AVBD_ERR_ALLOC_FAILED;
     uint8_t* dOut = out_on_device ? out : st + outOff;
-    launch_pusht_obs(s->d.posLin, s->d.posAng, s->pushtDev, num_envs, res, dOut, s->launch);
+    launch_pusht_obs(s->d.posLin, s->d.posAng, s->pushtDev, num_envs, res, s->pushtShapes, dOut, s->launch);
     return render_finish(s, out_on_device ? nullptr : out, dOut, outBytes, "Push-T observation");
 }
 
