@@ -271,16 +271,25 @@ __global__ void __launch_bounds__(kObsThreads) k_pusht_obs(const float4* shapes,
             {to_byte(0.85f), to_byte(0.15f), to_byte(0.12f)},
             {to_byte(0.2f), to_byte(0.4f), to_byte(0.95f)}};
         if (QUADS) {
-            uint32_t b[12];
+            uint32_t w0, w1, w2;
+            if (kinds == 0u) {  // four background pixels
+                const uint32_t g = pal[0][0];
+                w0 = w1 = w2 = g | (g << 8) | (g << 16) | (g << 24);
+            } else {
+                uint32_t b[12];
 #pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const uint32_t kind = (kinds >> (2 * k)) & 3u;
-                b[3 * k] = pal[kind][0]; b[3 * k + 1] = pal[kind][1]; b[3 * k + 2] = pal[kind][2];
+                for (int k = 0; k < 4; k++) {
+                    const uint32_t kind = (kinds >> (2 * k)) & 3u;
+                    b[3 * k] = pal[kind][0]; b[3 * k + 1] = pal[kind][1]; b[3 * k + 2] = pal[kind][2];
+                }
+                w0 = b[0] | (b[1] << 8) | (b[2] << 16) | (b[3] << 24);
+                w1 = b[4] | (b[5] << 8) | (b[6] << 16) | (b[7] << 24);
+                w2 = b[8] | (b[9] << 8) | (b[10] << 16) | (b[11] << 24);
             }
             __syncthreads();  // the previous environment's words are out
-            words[3 * threadIdx.x] = b[0] | (b[1] << 8) | (b[2] << 16) | (b[3] << 24);
-            words[3 * threadIdx.x + 1] = b[4] | (b[5] << 8) | (b[6] << 16) | (b[7] << 24);
-            words[3 * threadIdx.x + 2] = b[8] | (b[9] << 8) | (b[10] << 16) | (b[11] << 24);
+            words[3 * threadIdx.x] = w0;
+            words[3 * threadIdx.x + 1] = w1;
+            words[3 * threadIdx.x + 2] = w2;
             __syncthreads();
             // 3 * valid words from byte (e * res^2 + 4 * blockFirst) * 3
             uint32_t* dst = reinterpret_cast<uint32_t*>(out + ((size_t)e * res * res + 4u * (size_t)blockFirst) * 3u);
@@ -323,7 +332,13 @@ void launch_pusht_obs(const float4* posLin, const float4* posAng, const PushTDev
     k_pusht_shapes<<<blocks_for(numEnvs, 128), 128, 0, st>>>(posLin, posAng, envs, numEnvs, res, shapes);
     const bool quads = res % 4u == 0u;
     const uint32_t perEnv = quads ? res * res / 4u : res * res;
-    const dim3 grid(blocks_for(perEnv, kObsThreads), numEnvs < 65535u ? numEnvs : 65535u);
+    // about eight resident blocks per SM in all; each block walks several
+    // environments so that its offset table is built once for many
+    const uint32_t bx = blocks_for(perEnv, kObsThreads);
+    uint32_t by = (148u * 8u + bx - 1u) / bx;
+    by = by < numEnvs ? by : numEnvs;
+    by = by < 65535u ? (by ? by : 1u) : 65535u;
+    const dim3 grid(bx, by);
     const size_t smem = sizeof(float) * res;  // res <= 4096: at most 16 KB
     if (quads) k_pusht_obs<true><<<grid, kObsThreads, smem, st>>>(shapes, numEnvs, res, out);
     else k_pusht_obs<false><<<grid, kObsThreads, smem, st>>>(shapes, numEnvs, res, out);
