@@ -4,8 +4,8 @@
 //
 // Follows Shaders/50_render.metal:7-212 and Shaders/60_robotics.metal:8-69.
 // All of them are one pass over independent records; the Push-T kernel is
-// the byte-heavy one (num_envs x res^2 x 3 bytes) and writes runs of 16
-// pixels (48 bytes) per thread as 16-byte stores.
+// the byte-heavy one (num_envs x res^2 x 3 bytes) and writes 12-byte pixel
+// quads per thread so that consecutive threads store consecutive words.
 #include "dmath.cuh"
 #include "kernels.h"
 
@@ -170,16 +170,18 @@ __device__ __forceinline__ void heading(float4 q, float& cs, float& sn) {
 // Push-T observations (60_robotics.metal:21-69) in two passes.
 // k_pusht_shapes: one thread per environment places its shapes (goal T from
 // the table, block T and pusher from the body poses) into 24 floats.
-// k_pusht_obs<G>: each thread owns a run of G consecutive pixels of a row
-// (3G bytes) and blockIdx.y walks the environments; every thread reads its
-// environment's 24 floats (the same address across the block).  The
-// pixel-centre offsets (float)j / (res - 1) - 0.5 are a shared table (the
-// same division as per pixel, done once per block).  A run whose centre is
-// farther from a shape's centre than the shape's bounding radius plus
-// (G / 2 + 1) pixel widths cannot touch it, so that shape's exact test is
-// skipped; most runs are background and store a constant pattern.  G = 16
-// (res a multiple of 16) stores three 16-byte words per thread (runs start on
-// 48-byte boundaries), G = 4 three 4-byte words, G = 1 three bytes.
+// k_pusht_obs: blockIdx.y walks the environments; every thread reads its
+// environment's 24 floats (the same address across the block) and
+// classifies pixels.  The pixel-centre offsets (float)j / (res - 1) - 0.5
+// are a shared table (the same division as per pixel, done once per block).
+// A quad of pixels whose centre is farther from a shape's centre than the
+// shape's bounding radius plus two pixel widths cannot touch it, so that
+// shape's exact test is skipped (most quads are background).
+// QUADS (res a multiple of 4): each thread classifies four consecutive
+// pixels of a row into three 32-bit words, the block stages its 3 KB run in
+// shared memory and writes it out as 16-byte stores (the run starts on a
+// 16-byte boundary: 3 * res^2 and 3072 are multiples of 48).  Otherwise one
+// thread per pixel with byte stores.
 constexpr uint32_t kObsThreads = 256;
 
 __device__ __forceinline__ bool near_(float x, float y, float cx, float cy, float r2) {
@@ -188,7 +190,7 @@ __device__ __forceinline__ bool near_(float x, float y, float cx, float cy, floa
 }
 
 __global__ void k_pusht_shapes(const float4* posLin, const float4* posAng, const PushTDev* envs, uint32_t numEnvs,
-                               uint32_t res, uint32_t run, float4* shapes) {
+                               uint32_t res, float4* shapes) {
     const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= numEnvs) return;
     const PushTDev env = envs[e];
@@ -207,85 +209,99 @@ __global__ void k_pusht_shapes(const float4* posLin, const float4* posAng, const
     sh[16] = env.frame.x; sh[17] = env.frame.y;
     sh[18] = 2.0f * env.halfWin;
     // squared cull radii: bar (0.5 x 0.125 half extents), stem (0.125 x
-    // 0.325), pusher disc (0.13), each plus half a run and one pixel width
+    // 0.325), pusher disc (0.13), each plus two pixel widths
     const float pw = fabsf(sh[18]) / (float)(res - 1u);
-    const float m = (0.5f * (float)run + 1.0f) * pw;
-    const float rb = 0.5154f + m, rs = 0.3483f + m, rt = 0.13f + m;
+    const float rb = 0.5154f + 2.0f * pw, rs = 0.3483f + 2.0f * pw, rt = 0.13f + 2.0f * pw;
     sh[19] = rb * rb; sh[20] = rs * rs; sh[21] = rt * rt;
     sh[22] = 0.0f; sh[23] = 0.0f;
     for (int k = 0; k < 6; k++) shapes[6 * e + k] = make_float4(sh[4 * k], sh[4 * k + 1], sh[4 * k + 2], sh[4 * k + 3]);
 }
 
-template <int G>
+template <bool QUADS>
 __global__ void __launch_bounds__(kObsThreads) k_pusht_obs(const float4* shapes, uint32_t numEnvs, uint32_t res,
                                                            uint8_t* out) {
     extern __shared__ float offs[];  // res entries
-    const uint32_t perRow = res / G;
+    __shared__ uint32_t words[3 * kObsThreads];
+    const uint32_t perRow = QUADS ? res / 4u : res;
     const uint32_t perEnv = perRow * res;
+    const uint32_t blockFirst = blockIdx.x * kObsThreads;
+    const uint32_t valid = perEnv - blockFirst < kObsThreads ? perEnv - blockFirst : kObsThreads;
     const float denom = (float)(res - 1u);
     for (uint32_t j = threadIdx.x; j < res; j += kObsThreads) offs[j] = (float)j / denom - 0.5f;
     __syncthreads();
-    const uint32_t i = blockIdx.x * kObsThreads + threadIdx.x;
-    if (i >= perEnv) return;  // no barrier below
-    const uint32_t py = i / perRow;
-    const uint32_t px0 = G * (i - py * perRow);
-    // the four palette entries as bytes
-    const uint32_t pal[4][3] = {
-        {to_byte(0.06f), to_byte(0.06f), to_byte(0.06f)},
-        {to_byte(0.10f), to_byte(0.55f), to_byte(0.12f)},
-        {to_byte(0.85f), to_byte(0.15f), to_byte(0.12f)},
-        {to_byte(0.2f), to_byte(0.4f), to_byte(0.95f)}};
-    const uint32_t bgByte = pal[0][0];
-    const uint32_t bgWord = bgByte | (bgByte << 8) | (bgByte << 16) | (bgByte << 24);
+    // row and column of this thread's first pixel (quad index / row length)
+    const uint32_t i = blockFirst + threadIdx.x;
+    uint32_t py = i / perRow;
+    const uint32_t px0 = (QUADS ? 4u : 1u) * (i - py * perRow);
     for (uint32_t e = blockIdx.y; e < numEnvs; e += gridDim.y) {
         const float4* S = shapes + 6 * (size_t)e;
         const float4 s0 = S[0], s1 = S[1], s2 = S[2], s3 = S[3], s4 = S[4], s5 = S[5];
-        const float wy = s4.y + offs[py] * s4.z;
-        const float cx = 0.5f * ((s4.x + offs[px0] * s4.z) + (s4.x + offs[px0 + G - 1] * s4.z));
-        const bool gBar = near_(cx, wy, s0.x, s0.y, s4.w), gStem = near_(cx, wy, s0.z, s0.w, s5.x);
-        const bool bBar = near_(cx, wy, s1.z, s1.w, s4.w), bStem = near_(cx, wy, s2.z, s2.w, s5.x);
-        const bool tip = near_(cx, wy, s3.z, s3.w, s5.y);
-        uint32_t w[(3 * G + 3) / 4];
-        constexpr int NW = (3 * G + 3) / 4;
-        if (!(gBar || gStem || bBar || bStem || tip)) {
+        uint32_t kinds = 0;  // 2 bits per pixel: 0 background, 1 goal, 2 block, 3 pusher
+        if (threadIdx.x < valid) {
+            constexpr int N = QUADS ? 4 : 1;
+            const float wy = s4.y + offs[py] * s4.z;
+            float wx[N];
 #pragma unroll
-            for (int k = 0; k < NW; k++) w[k] = bgWord;
-        } else {
-            uint32_t b[3 * G];
+            for (int k = 0; k < N; k++) wx[k] = s4.x + offs[px0 + k] * s4.z;
+            const float cx = 0.5f * (wx[0] + wx[N - 1]);
+            const bool gBar = near_(cx, wy, s0.x, s0.y, s4.w), gStem = near_(cx, wy, s0.z, s0.w, s5.x);
+            const bool bBar = near_(cx, wy, s1.z, s1.w, s4.w), bStem = near_(cx, wy, s2.z, s2.w, s5.x);
+            const bool tip = near_(cx, wy, s3.z, s3.w, s5.y);
+            if (gBar || gStem || bBar || bStem || tip) {
 #pragma unroll
-            for (int k = 0; k < G; k++) {
-                const float wx = s4.x + offs[px0 + k] * s4.z;
-                uint32_t kind = 0;  // 0 background, 1 goal, 2 block, 3 pusher
-                if ((gBar && in_box(wx, wy, s0.x, s0.y, s1.x, s1.y, 0.5f, 0.125f)) ||
-                    (gStem && in_box(wx, wy, s0.z, s0.w, s1.x, s1.y, 0.125f, 0.325f)))
-                    kind = 1;
-                if (bBar && in_box(wx, wy, s1.z, s1.w, s2.x, s2.y, 0.5f, 0.125f)) kind = 2;
-                if (bStem && in_box(wx, wy, s2.z, s2.w, s3.x, s3.y, 0.125f, 0.325f)) kind = 2;
-                if (tip) {
-                    const float dx = wx - s3.z, dy = wy - s3.w;
-                    if (sqrtf(dx * dx + dy * dy) < 0.13f) kind = 3;
+                for (int k = 0; k < N; k++) {
+                    uint32_t kind = 0;
+                    if ((gBar && in_box(wx[k], wy, s0.x, s0.y, s1.x, s1.y, 0.5f, 0.125f)) ||
+                        (gStem && in_box(wx[k], wy, s0.z, s0.w, s1.x, s1.y, 0.125f, 0.325f)))
+                        kind = 1;
+                    if (bBar && in_box(wx[k], wy, s1.z, s1.w, s2.x, s2.y, 0.5f, 0.125f)) kind = 2;
+                    if (bStem && in_box(wx[k], wy, s2.z, s2.w, s3.x, s3.y, 0.125f, 0.325f)) kind = 2;
+                    if (tip) {
+                        const float dx = wx[k] - s3.z, dy = wy - s3.w;
+                        if (sqrtf(dx * dx + dy * dy) < 0.13f) kind = 3;
+                    }
+                    kinds |= kind << (2 * k);
                 }
-                b[3 * k] = pal[kind][0]; b[3 * k + 1] = pal[kind][1]; b[3 * k + 2] = pal[kind][2];
-            }
-            if (G >= 4) {
-#pragma unroll
-                for (int k = 0; k < NW; k++)
-                    w[k] = b[4 * k] | (b[4 * k + 1] << 8) | (b[4 * k + 2] << 16) | (b[4 * k + 3] << 24);
-            } else {
-                w[0] = b[0] | (b[1] << 8) | (b[2] << 16);
             }
         }
-        uint8_t* o = out + ((size_t)e * res * res + (size_t)py * res + px0) * 3u;
-        if (G == 16) {
-            uint4* v = reinterpret_cast<uint4*>(o);
-            v[0] = make_uint4(w[0], w[1], w[2], w[3]);
-            v[1] = make_uint4(w[4], w[5], w[6], w[7]);
-            v[2] = make_uint4(w[8], w[9], w[10], w[11]);
-        } else if (G == 4) {
-            uint32_t* v = reinterpret_cast<uint32_t*>(o);
-            v[0] = w[0]; v[1] = w[1]; v[2] = w[2];
-        } else {
-            o[0] = (uint8_t)(w[0] & 0xFFu); o[1] = (uint8_t)((w[0] >> 8) & 0xFFu); o[2] = (uint8_t)((w[0] >> 16) & 0xFFu);
+        // the four palette entries as bytes
+        const uint32_t pal[4][3] = {
+            {to_byte(0.06f), to_byte(0.06f), to_byte(0.06f)},
+            {to_byte(0.10f), to_byte(0.55f), to_byte(0.12f)},
+            {to_byte(0.85f), to_byte(0.15f), to_byte(0.12f)},
+            {to_byte(0.2f), to_byte(0.4f), to_byte(0.95f)}};
+        if (QUADS) {
+            uint32_t w0, w1, w2;
+            if (kinds == 0u) {  // four background pixels
+                const uint32_t g = pal[0][0];
+                w0 = w1 = w2 = g | (g << 8) | (g << 16) | (g << 24);
+            } else {
+                uint32_t b[12];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const uint32_t kind = (kinds >> (2 * k)) & 3u;
+                    b[3 * k] = pal[kind][0]; b[3 * k + 1] = pal[kind][1]; b[3 * k + 2] = pal[kind][2];
+                }
+                w0 = b[0] | (b[1] << 8) | (b[2] << 16) | (b[3] << 24);
+                w1 = b[4] | (b[5] << 8) | (b[6] << 16) | (b[7] << 24);
+                w2 = b[8] | (b[9] << 8) | (b[10] << 16) | (b[11] << 24);
+            }
+            __syncthreads();  // the previous environment's words are out
+            words[3 * threadIdx.x] = w0;
+            words[3 * threadIdx.x + 1] = w1;
+            words[3 * threadIdx.x + 2] = w2;
+            __syncthreads();
+            // 3 * valid words from byte (e * res^2 + 4 * blockFirst) * 3
+            uint32_t* dst = reinterpret_cast<uint32_t*>(out + ((size_t)e * res * res + 4u * (size_t)blockFirst) * 3u);
+            const uint32_t nWords = 3u * valid, nVec = nWords / 4u;
+            for (uint32_t v = threadIdx.x; v < nVec; v += kObsThreads)
+                reinterpret_cast<uint4*>(dst)[v] =
+                    make_uint4(words[4 * v], words[4 * v + 1], words[4 * v + 2], words[4 * v + 3]);
+            for (uint32_t w = 4u * nVec + threadIdx.x; w < nWords; w += kObsThreads) dst[w] = words[w];
+        } else if (threadIdx.x < valid) {
+            const uint32_t kind = kinds & 3u;
+            uint8_t* o = out + ((size_t)e * res * res + i) * 3u;
+            o[0] = (uint8_t)pal[kind][0]; o[1] = (uint8_t)pal[kind][1]; o[2] = (uint8_t)pal[kind][2];
         }
     }
 }
@@ -313,9 +329,9 @@ void launch_skin_deform(const float4* posLin, const SkinBinding* b, uint32_t n, 
 void launch_pusht_obs(const float4* posLin, const float4* posAng, const PushTDev* envs, uint32_t numEnvs,
                       uint32_t res, float4* shapes, uint8_t* out, cudaStream_t st) {
     if (!numEnvs) return;
-    const uint32_t run = res % 16u == 0u ? 16u : (res % 4u == 0u ? 4u : 1u);
-    k_pusht_shapes<<<blocks_for(numEnvs, 128), 128, 0, st>>>(posLin, posAng, envs, numEnvs, res, run, shapes);
-    const uint32_t perEnv = res / run * res;
+    k_pusht_shapes<<<blocks_for(numEnvs, 128), 128, 0, st>>>(posLin, posAng, envs, numEnvs, res, shapes);
+    const bool quads = res % 4u == 0u;
+    const uint32_t perEnv = quads ? res * res / 4u : res * res;
     // about eight resident blocks per SM in all; each block walks several
     // environments so that its offset table is built once for many
     const uint32_t bx = blocks_for(perEnv, kObsThreads);
@@ -324,9 +340,8 @@ void launch_pusht_obs(const float4* posLin, const float4* posAng, const PushTDev
     by = by < 65535u ? (by ? by : 1u) : 65535u;
     const dim3 grid(bx, by);
     const size_t smem = sizeof(float) * res;  // res <= 4096: at most 16 KB
-    if (run == 16u) k_pusht_obs<16><<<grid, kObsThreads, smem, st>>>(shapes, numEnvs, res, out);
-    else if (run == 4u) k_pusht_obs<4><<<grid, kObsThreads, smem, st>>>(shapes, numEnvs, res, out);
-    else k_pusht_obs<1><<<grid, kObsThreads, smem, st>>>(shapes, numEnvs, res, out);
+    if (quads) k_pusht_obs<true><<<grid, kObsThreads, smem, st>>>(shapes, numEnvs, res, out);
+    else k_pusht_obs<false><<<grid, kObsThreads, smem, st>>>(shapes, numEnvs, res, out);
 }
 
 }  // namespace avbd
