@@ -205,14 +205,17 @@ def evaluate(make_scene: Callable[[int], object], seed: int, model: Optional[War
 
 def matched_residual_iterations(make_scene: Callable[[int], object], seed: int, model: WarmStartModel,
                                 plain_iterations: int, frames: int = 60,
-                                candidates: Sequence[int] = (4, 6, 8, 10, 12, 14, 16, 18),
+                                candidates: Sequence[int] = None,
                                 trial_sweeps: int = 1):
     """Smallest learned iteration count whose median relative residual
     (r_final / r0 of the plain warm start) is no larger than the plain warm
-    start's at `plain_iterations`.  Returns (iterations, plain residual,
-    learned residual, accepted fraction)."""
+    start's at `plain_iterations`.  Every count from 4 up is tried in turn
+    (the residual need not fall monotonically with the count).  Returns
+    (iterations, plain residual, learned residual, accepted fraction)."""
     plain = evaluate(make_scene, seed, None, frames, plain_iterations, trial_sweeps=trial_sweeps)
     target = plain["rel_residual_final"]
+    if candidates is None:
+        candidates = range(4, plain_iterations)
     for k in candidates:
         if k >= plain_iterations:
             break
