@@ -363,8 +363,10 @@ struct avbd_solver {
             if (reuseTrial) {
                 launch_learn_adopt(P, f, z, st);
             } else {
-                cudaMemcpyAsync(f.posLin, f.learnSaveLin, poseBytes, cudaMemcpyDeviceToDevice, st);
-                cudaMemcpyAsync(f.posAng, f.learnSaveAng, poseBytes, cudaMemcpyDeviceToDevice, st);
+                if (learnTrials > 0) {  // undo the plain branch's trial sweeps
+                    cudaMemcpyAsync(f.posLin, f.learnSaveLin, poseBytes, cudaMemcpyDeviceToDevice, st);
+                    cudaMemcpyAsync(f.posAng, f.learnSaveAng, poseBytes, cudaMemcpyDeviceToDevice, st);
+                }
                 launch_learn_select(P, f, z, st);
             }
         } else if (trace) {
@@ -1337,7 +1339,7 @@ int avbd_get_counters(avbd_solver* s, avbd_counters* out) {
 }
 
 int avbd_set_warm_start_model(avbd_solver* s, const float* params, const float* norm, uint32_t trial_sweeps) {
-    if (!s || !params || !norm || trial_sweeps == 0) return AVBD_ERR_INVALID_ARGUMENT;
+    if (!s || !params || !norm || trial_sweeps > 16) return AVBD_ERR_INVALID_ARGUMENT;
     if (s->z.numLearn == 0) {
         s->error = "the scene has no dynamic particles for the learned warm start (cloth is not supported)";
         return AVBD_ERR_UNSUPPORTED;

@@ -393,7 +393,9 @@ int avbd_set_capacity_for_testing(avbd_solver* solver, int which, uint32_t value
  * from local features.  In AVBD_WARM_START_LEARNED mode every frame races
  * the plain and the predicted warm start for `trial_sweeps` primal sweeps and
  * keeps the prediction only when its augmented-Lagrangian residual is no
- * larger; plain AVBD stays the fallback.  Parameters are the fp32 block of
+ * larger; plain AVBD stays the fallback.  trial_sweeps = 0 compares the
+ * residuals of the two warm starts themselves (no trial sweep); 1 keeps the
+ * winner's trial sweep as the first iteration's primal half; at most 16.  Parameters are the fp32 block of
  * avbd_mlp_param_count() floats (W1[128][32], b1, W2[128][128], b2,
  * W3[128][128], b3, W4[16][128], b4[16]); `norm` holds 96 floats: feature
  * mean[32], feature 1/std[32], target mean[16], target std[16].          */
