@@ -949,13 +949,11 @@ __global__ void k_primal(const Params P, const DevPtrs d, uint32_t color, uint32
 // squared and summed.  The square root is r_k of the iterations-to-tolerance
 // measurement.  Bodies come from the color lists (every dynamic body once).
 // ---------------------------------------------------------------------------
-__global__ void k_residual_bodies(const Params P, const DevPtrs d, uint32_t n, float* out) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t slot = tid >> 3, lane = tid & 7u;
-    if (slot >= n) return;
-    const unsigned mask = 0xFFu << (threadIdx.x & 24u);
-    const uint32_t body = d.colorList[slot];
-    const bool rigid = d.shape[body].w >= 0.0f;
+// Squared AL gradient of one rigid body (linear and angular parts) by an
+// 8-lane group: lanes stamp entries lane, lane + 8, ..., an xor butterfly
+// folds them and lane 0 writes *out.
+__device__ void rigid_residual(const Params& P, const DevPtrs& d, uint32_t body, uint32_t lane, unsigned mask,
+                               float* out) {
     Accum acc{m3_zero(), m3_zero(), m3_zero(), s3(0), s3(0)};
     const AdjView v = adj_view(d, body);
     const uint32_t cnt = v.count();
@@ -968,26 +966,21 @@ __global__ void k_residual_bodies(const Params P, const DevPtrs d, uint32_t n, f
     if (lane != 0) return;
     const float4 pl = d.posLin[body];
     const float dt2 = P.dt * P.dt;
-    float3 rl = acc.rhsLin + (xyz(pl) - xyz(d.inertLin[body])) * (pl.w / dt2);
-    float r2 = dot(rl, rl);
-    if (rigid) {
-        const float4 q = d.posAng[body];
-        const M3 inertia = m3_scale(world_inertia(q, xyz(d.props[body])), 1.0f / dt2);
-        const float3 ra = acc.rhsAng + m3_mul(inertia, q_sub(q, d.inertAng[body]));
-        r2 += dot(ra, ra);
-    }
-    out[slot] = r2;
+    const float3 rl = acc.rhsLin + (xyz(pl) - xyz(d.inertLin[body])) * (pl.w / dt2);
+    const float4 q = d.posAng[body];
+    const M3 inertia = m3_scale(world_inertia(q, xyz(d.props[body])), 1.0f / dt2);
+    const float3 ra = acc.rhsAng + m3_mul(inertia, q_sub(q, d.inertAng[body]));
+    *out = dot(rl, rl) + dot(ra, ra);
 }
 
 // Fixed-order sum of n values in one block (double accumulation): thread t
-// sums a contiguous run, a warp shuffle tree and a second tree over the
-// warps combine them, always in the same order.
+// sums v[t], v[t + 1024], ... (coalesced), a warp shuffle tree and a second
+// tree over the warps combine them, always in the same order.
 __global__ void __launch_bounds__(1024) k_sum_fixed(const float* v, uint32_t n, double* out) {
     __shared__ double part[32];
-    const uint32_t t = threadIdx.x, per = (n + blockDim.x - 1) / blockDim.x;
+    const uint32_t t = threadIdx.x;
     double s = 0.0;
-    const uint32_t b0 = t * per, b1 = min(n, b0 + per);
-    for (uint32_t i = b0; i < b1; i++) s += (double)v[i];
+    for (uint32_t i = t; i < n; i += blockDim.x) s += (double)v[i];
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((t & 31u) == 0) part[t >> 5] = s;
@@ -1276,7 +1269,12 @@ __global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevP
     const uint32_t body = d.colorList[s + slot];
     const float4 shp = d.shape[body];
     if (GENERAL && shp.w >= 0.0f) {                          // rigid: the 8-lane path
-        if (lane < 8) primal_body(P, d, body, lane, mask & (0xFFu << ((threadIdx.x & 31u) & ~(uint32_t)(LANES - 1))));
+        const unsigned mask8 = mask & (0xFFu << ((threadIdx.x & 31u) & ~(uint32_t)(LANES - 1)));
+        if (RESID) {
+            if (lane < 8) rigid_residual(P, d, body, lane, mask8, d.learnResidBodies + s + slot);
+        } else if (lane < 8) {
+            primal_body(P, d, body, lane, mask8);
+        }
         return;
     }
     // lane 0 needs these after the reduction; issue the loads now
@@ -1435,7 +1433,13 @@ void launch_residual(const Params& P, const DevPtrs& d, const Sizes& z, float* p
         // flight (measured faster than 16 or 32 for the 13,824-body soft cube)
         run(0u, n, 8u);
     } else if (n) {
-        k_residual_bodies<<<(n * 8 + 127) / 128, 128, 0, st>>>(P, d, n, perBody);
+        // rigid bodies present: particles through the primal's particle
+        // terms, rigid bodies through the generic stamps, 8 lanes per body
+        DevPtrs g = d;
+        g.learnResidBodies = perBody;
+        const uint32_t blocks = (n * 8 + 127) / 128;
+        if (P.cloth || P.ogc) k_primal_group<8, true, true, true><<<blocks, 128, 0, st>>>(P, g, 0u, n);
+        else k_primal_group<8, true, false, true><<<blocks, 128, 0, st>>>(P, g, 0u, n);
     }
     k_sum_fixed<<<1, 1024, 0, st>>>(perBody, n, total);
 }
