@@ -500,7 +500,7 @@ struct avbd_solver {
         for (uint32_t b = 0; b < nb; b++) z.numDynamicRigid += (H.posLin[b].w > 0.0f && H.shape[b].w >= 0.0f) ? 1u : 0u;
         const uint32_t scanLimit = 1024u * 1024u;
         if (P.gridHashSize > scanLimit || z.producers > scanLimit || nb > scanLimit) {
-            error = "scene exceeds the 1M-element scan limit of this build";
+            error = "scene exceeds the 1M-element scan limit of this library";
             return AVBD_ERR_UNSUPPORTED;
         }
         bool ok = true;

@@ -792,7 +792,7 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
         const uint32_t automatic = (volumetricSelf || (s->num_tris > 0 && s->num_tets == 0)) ? 2u : 1u;
         P.surfaceTruncationMode = s->truncation_selection == AVBD_TRUNCATION_AUTOMATIC ? automatic : s->truncation_selection;
     }
-    if (P.surfaceTruncationMode == 2u && s->num_tets > 0) { err = "Planar-DAT truncation of tet surfaces is not supported by this build"; return AVBD_ERR_UNSUPPORTED; }
+    if (P.surfaceTruncationMode == 2u && s->num_tets > 0) { err = "Planar-DAT truncation of tet surfaces is not supported by this library"; return AVBD_ERR_UNSUPPORTED; }
     P.cloth = (H.cloth && P.surfaceTruncationMode == 2u) ? 1u : 0u;
     H.ogc = H.ogc && P.surfaceTruncationMode == 1u;
     P.ogc = H.ogc ? 1u : 0u;

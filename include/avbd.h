@@ -37,7 +37,7 @@ enum {
     AVBD_ERR_ALLOC_FAILED = 3,       /* AVBDError.allocFailed(label)         */
     AVBD_ERR_KERNEL_MISSING = 4,     /* AVBDError.kernelMissing(name)        */
     AVBD_ERR_RUNTIME_FAILURE = 5,    /* latched RuntimeFailure, see below    */
-    AVBD_ERR_UNSUPPORTED = 6         /* scene feature outside this build     */
+    AVBD_ERR_UNSUPPORTED = 6         /* scene feature outside this library   */
 };
 
 /* Runtime failure kinds reported by avbd_runtime_failure(). */
