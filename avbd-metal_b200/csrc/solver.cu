@@ -1252,8 +1252,11 @@ __device__ __forceinline__ float3 solve3x3_particle(const M3& a, float3 b) {
 // RESID: evaluate instead of solve — lane 0 stores the body's squared
 // right-hand side (the AL gradient) in d.learnResidBodies[slot] and leaves
 // the pose alone (particle-only scenes; called over all colors at once).
+// GENERAL instances keep four blocks per SM (at most 128 registers): the
+// rigid-body path would otherwise take ~160 registers for every thread and
+// cap large colors at three blocks (measured 7% slower mixed frames).
 template <int LANES, bool GENERAL, bool CLOTH, bool RESID = false>
-__global__ void __launch_bounds__(128) k_primal_group(const Params P, const DevPtrs d, uint32_t color,
+__global__ void __launch_bounds__(128, GENERAL ? 4 : 1) k_primal_group(const Params P, const DevPtrs d, uint32_t color,
                                                       uint32_t count) {
     constexpr int GROUPS = 32 / LANES;
     pdl_prologue();
