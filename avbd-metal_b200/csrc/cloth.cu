@@ -339,7 +339,7 @@ __global__ void k_dat_pair_totals(const Params P, const DevPtrs d, uint32_t owne
 // test that opens the body test, so lane 0 visits only globals that can pass
 // it.  Otherwise one thread per triangle.
 template <bool EMIT, bool WARP>
-__global__ void __launch_bounds__(128) k_rt_emit(const Params P, const DevPtrs d) {
+__global__ void __launch_bounds__(128, 6) k_rt_emit(const Params P, const DevPtrs d) {
     const uint32_t lane = WARP ? (threadIdx.x & 31u) : 0u;
     const uint32_t step = WARP ? (gridDim.x * blockDim.x) >> 5 : gridDim.x * blockDim.x;
     const uint32_t first = WARP ? (blockIdx.x * blockDim.x + threadIdx.x) >> 5 : blockIdx.x * blockDim.x + threadIdx.x;
