@@ -974,13 +974,23 @@ __device__ void rigid_residual(const Params& P, const DevPtrs& d, uint32_t body,
 }
 
 // Fixed-order sum of n values in one block (double accumulation): thread t
-// sums v[t], v[t + 1024], ... (coalesced), a warp shuffle tree and a second
-// tree over the warps combine them, always in the same order.
+// sums the float4 groups t, t + 1024, ... (16-byte coalesced loads; v is a
+// device allocation, so 16-byte aligned), then tail element 4 * (n / 4) + t;
+// a warp shuffle tree and a second tree over the warps combine the threads,
+// always in the same order.
 __global__ void __launch_bounds__(1024) k_sum_fixed(const float* v, uint32_t n, double* out) {
     __shared__ double part[32];
-    const uint32_t t = threadIdx.x;
+    const uint32_t t = threadIdx.x, n4 = n / 4u;
+    const float4* v4 = reinterpret_cast<const float4*>(v);
     double s = 0.0;
-    for (uint32_t i = t; i < n; i += blockDim.x) s += (double)v[i];
+    for (uint32_t i = t; i < n4; i += blockDim.x) {
+        const float4 q = v4[i];
+        s += (double)q.x;
+        s += (double)q.y;
+        s += (double)q.z;
+        s += (double)q.w;
+    }
+    if (4u * n4 + t < n) s += (double)v[4u * n4 + t];
 #pragma unroll
     for (int o = 16; o >= 1; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if ((t & 31u) == 0) part[t >> 5] = s;
