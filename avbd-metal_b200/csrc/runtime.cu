@@ -157,7 +157,6 @@ struct avbd_solver {
     void* stage = nullptr;
     size_t stageBytes = 0;
     uint32_t* hostLatch = nullptr;     // pinned copy of the failure latch
-    Counters* hostCounters = nullptr;  // pinned copy of the last frame's counters
     // render surface (built on the first smooth-normals call): surface
     // vertices, their incident triangles, face normals
     bool renderSurfaceReady = false;
@@ -187,7 +186,6 @@ struct avbd_solver {
         if (pushtDev) cudaFree(pushtDev);
         if (pushtShapes) cudaFree(pushtShapes);
         if (hostLatch) cudaFreeHost(hostLatch);
-        if (hostCounters) cudaFreeHost(hostCounters);
         if (forkEvent) cudaEventDestroy(forkEvent);
         if (joinEvent) cudaEventDestroy(joinEvent);
         if (branchStream) cudaStreamDestroy(branchStream);
@@ -711,13 +709,11 @@ struct avbd_solver {
         d.numSpinners = (uint32_t)spB.size();
         d.numRateMotors = (uint32_t)rJ.size();
         if (!ok) return AVBD_ERR_ALLOC_FAILED;
-        if (cudaMallocHost(&hostLatch, 4 * sizeof(uint32_t)) != cudaSuccess ||
-            cudaMallocHost(&hostCounters, sizeof(Counters)) != cudaSuccess) {
+        if (cudaMallocHost(&hostLatch, 4 * sizeof(uint32_t)) != cudaSuccess) {
             error = "pinned allocation failed";
             return AVBD_ERR_ALLOC_FAILED;
         }
         std::memset(hostLatch, 0, 4 * sizeof(uint32_t));
-        std::memset(hostCounters, 0, sizeof(Counters));
         // Small scenes run their whole iteration loop in one thread block.
         update_small_solve();
         tuneStage = tuning_applies() ? 0 : -1;
