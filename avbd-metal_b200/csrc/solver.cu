@@ -935,12 +935,13 @@ __device__ void primal_body(const Params& P, const DevPtrs& d, uint32_t body, ui
 
 __global__ void k_primal(const Params P, const DevPtrs d, uint32_t color, uint32_t count) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t slot = tid >> 3, lane = tid & 7u;
+    const uint32_t lane = tid & 7u, groups = (gridDim.x * blockDim.x) >> 3;
     const uint32_t s = d.colorStart[color];
     const uint32_t n = count != 0xFFFFFFFFu ? count : d.colorStart[color + 1] - s;
-    if (slot >= n) return;                      // uniform across the 8-lane group
     const unsigned mask = 0xFFu << (threadIdx.x & 24u);
-    primal_body(P, d, d.colorList[s + slot], lane, mask);
+    // one 8-lane group per body, striding over the color (uniform across
+    // the group)
+    for (uint32_t slot = tid >> 3; slot < n; slot += groups) primal_body(P, d, d.colorList[s + slot], lane, mask);
 }
 
 // ---------------------------------------------------------------------------
@@ -1410,7 +1411,12 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
     const uint32_t upper = count != 0xFFFFFFFFu ? count : z.numDynamicBodies;
     if (upper == 0) return;
     if (z.dynamicColoring) {
-        k_primal<<<(upper * 8 + T - 1) / T, T, 0, st>>>(P, d, color, count);
+        // dynamic coloring: the color's size is known on the device only, so
+        // one resident wave (4 blocks per SM at 128 registers) strides over
+        // it instead of a grid sized for every dynamic body (batched worlds
+        // 1.007 -> 0.965 ms per frame; half a wave measured 1.22 ms)
+        const uint32_t need = (upper * 8 + T - 1) / T, wave = 148u * 4u;
+        k_primal<<<need < wave ? need : wave, T, 0, st>>>(P, d, color, count);
     } else {
         // the grouped kernel needs the color's body count on the host
         const uint32_t lanes_ = lanes < 8 ? 8 : (lanes > 32 ? 32 : lanes);
