@@ -227,15 +227,29 @@ __global__ void __launch_bounds__(kObsThreads) k_pusht_obs(const float4* shapes,
     const uint32_t blockFirst = blockIdx.x * kObsThreads;
     const uint32_t valid = perEnv - blockFirst < kObsThreads ? perEnv - blockFirst : kObsThreads;
     const float denom = (float)(res - 1u);
+    __shared__ float4 shs[2][6];     // QUADS: this and the next environment's shapes
     for (uint32_t j = threadIdx.x; j < res; j += kObsThreads) offs[j] = (float)j / denom - 0.5f;
+    if (QUADS && threadIdx.x < 6u && blockIdx.y < numEnvs)
+        shs[0][threadIdx.x] = shapes[6 * (size_t)blockIdx.y + threadIdx.x];
     __syncthreads();
     // row and column of this thread's first pixel (quad index / row length)
     const uint32_t i = blockFirst + threadIdx.x;
     uint32_t py = i / perRow;
     const uint32_t px0 = (QUADS ? 4u : 1u) * (i - py * perRow);
-    for (uint32_t e = blockIdx.y; e < numEnvs; e += gridDim.y) {
-        const float4* S = shapes + 6 * (size_t)e;
-        const float4 s0 = S[0], s1 = S[1], s2 = S[2], s3 = S[3], s4 = S[4], s5 = S[5];
+    uint32_t buf = 0;
+    for (uint32_t e = blockIdx.y; e < numEnvs; e += gridDim.y, buf ^= 1u) {
+        float4 s0, s1, s2, s3, s4, s5;
+        if (QUADS) {
+            // six threads fetch the next environment's shapes into the other
+            // buffer (last read an iteration ago, before that iteration's
+            // barriers); they are visible after this iteration's barriers
+            const uint32_t en = e + gridDim.y;
+            if (threadIdx.x < 6u && en < numEnvs) shs[buf ^ 1u][threadIdx.x] = shapes[6 * (size_t)en + threadIdx.x];
+            s0 = shs[buf][0]; s1 = shs[buf][1]; s2 = shs[buf][2]; s3 = shs[buf][3]; s4 = shs[buf][4]; s5 = shs[buf][5];
+        } else {
+            const float4* S = shapes + 6 * (size_t)e;
+            s0 = S[0]; s1 = S[1]; s2 = S[2]; s3 = S[3]; s4 = S[4]; s5 = S[5];
+        }
         uint32_t kinds = 0;  // 2 bits per pixel: 0 background, 1 goal, 2 block, 3 pusher
         if (threadIdx.x < valid) {
             constexpr int N = QUADS ? 4 : 1;
