@@ -14,6 +14,11 @@ from test_gpu_parity import compare_state, pair
 pytestmark = pytest.mark.gpu
 
 
+def _oracle_scenes():
+    import test_oracle_shapes
+    return test_oracle_shapes
+
+
 def manifolds_equal(g, o):
     gm = g.debug_read("MANIFOLDS", np.uint32).reshape(-1, 176)
     om = o.debug_read("MANIFOLDS", np.uint32).reshape(-1, 176)
@@ -38,6 +43,10 @@ def manifolds_equal(g, o):
     ("shapes-64", lambda: demos.shapes_scene(count=64), 200),
     ("drape-capsule", lambda: demos.drape_scene(res=16, obstacle="capsule"), 90),
     ("drape-torus", lambda: demos.drape_scene(res=16, obstacle="torus"), 90),
+    ("capsule-rest", lambda: _oracle_scenes().capsule_rest_scene(), 240),
+    ("crossed-capsules", lambda: _oracle_scenes().crossed_capsules_scene(), 240),
+    ("ball-on-capsule", lambda: _oracle_scenes().ball_on_capsule_scene(), 180),
+    ("hull-stack", lambda: _oracle_scenes().hull_stack_scene(), 240),
 ])
 def test_shape_trajectory_parity(cuda_lib, oracle_lib, name, make, frames):
     g, o = pair(make(), oracle_lib)

@@ -175,3 +175,73 @@ def test_motor_velocity_torque_and_states(oracle_lib):
     assert o.step(30) == 0
     _, v2 = o.motor_states([0])
     assert v2[0] > 0.0, "with zero effort the motor no longer drives the hinge"
+
+
+
+def capsule_rest_scene():
+    s = PhysicsScene("capsule-rest")
+    demos.add_ground(s, friction=0.6)
+    s.add_capsule(0.8, 0.15, 1.0, 0.6, (0, 0, 0.6), rotation=demos.quat_axis_angle(math.pi / 2, (0, 1, 0)))
+    return s
+
+
+def crossed_capsules_scene():
+    s = PhysicsScene("capsule-cross")
+    demos.add_ground(s)
+    s.add_capsule(1.0, 0.1, 0.0, 0.6, (0, 0, 0.1), rotation=demos.quat_axis_angle(math.pi / 2, (0, 1, 0)))
+    s.add_capsule(1.0, 0.12, 1.0, 0.6, (0, 0, 0.6), rotation=demos.quat_axis_angle(math.pi / 2, (1, 0, 0)))
+    return s
+
+
+def ball_on_capsule_scene():
+    s = PhysicsScene("ball-on-capsule")
+    demos.add_ground(s)
+    s.add_capsule(1.2, 0.2, 0.0, 0.8, (0, 0, 1.0), rotation=demos.quat_axis_angle(math.pi / 2, (0, 1, 0)))
+    s.add_sphere(0.3, 1.0, 0.8, (0.0, 0.0, 1.6))
+    return s
+
+
+def hull_stack_scene():
+    s = PhysicsScene("hull-hull")
+    demos.add_ground(s)
+    octa = [(0.3, 0, 0), (-0.3, 0, 0), (0, 0.3, 0), (0, -0.3, 0), (0, 0, 0.3), (0, 0, -0.3)]
+    base = s.add_body((1, 1, 1), 0.0, 0.5, (0, 0, 0.3), collision_enabled=False)
+    s.add_convex_collider(base, octa)
+    b = s.add_body((1, 1, 1), 0.0, 0.5, (0, 0, 1.2), mass=1.0, diagonal_inertia=(0.2, 0.2, 0.2),
+                   collision_enabled=False)
+    s.add_convex_collider(b, octa)
+    return s
+
+
+def test_capsule_rests_on_its_side(oracle_lib):
+    """A horizontal capsule dropped on the ground settles with its axis one
+    radius above it and stays horizontal (capsule-box three-seed contact)."""
+    o = run(oracle_lib, capsule_rest_scene(), 240)
+    pos, rot = o.positions()
+    assert abs(pos[1, 2] - 0.15) < 0.01, pos[1]
+    assert abs(rotate(rot[1], (0, 0, 1))[2]) < 0.05  # axis stays horizontal
+
+
+def test_crossed_capsules_stack(oracle_lib):
+    """A capsule dropped crosswise on a static one rests with the axes two
+    radii apart (capsule-capsule closest points)."""
+    o = run(oracle_lib, crossed_capsules_scene(), 240)
+    pos, _ = o.positions()
+    assert abs(pos[2, 2] - (0.1 + 0.1 + 0.12)) < 0.015, pos[2]
+    assert abs(pos[2, 0]) < 0.05 and abs(pos[2, 1]) < 0.05
+
+
+def test_sphere_rests_on_capsule(oracle_lib):
+    """A ball on top of a static horizontal capsule: centre at the capsule
+    axis height plus both radii (capsule-sphere)."""
+    o = run(oracle_lib, ball_on_capsule_scene(), 180)
+    pos, _ = o.positions()
+    assert abs(pos[2, 2] - (1.0 + 0.2 + 0.15)) < 0.01, pos[2]
+
+
+def test_hulls_do_not_collide_with_each_other(oracle_lib):
+    """Hull-hull pairs produce no contact (30_narrowphase.metal:433-440): a
+    hull body falls through a static hull onto the ground."""
+    o = run(oracle_lib, hull_stack_scene(), 240)
+    pos, _ = o.positions()
+    assert abs(pos[2, 2] - 0.3) < 0.05, pos[2]
