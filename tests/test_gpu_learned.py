@@ -60,24 +60,35 @@ def test_inference_matches_oracle(cuda_lib, oracle_lib):
     assert np.abs(y - want).max() <= 1e-3 * scale + 1e-6
 
 
-def test_zero_correction_model_reproduces_plain_frames(cuda_lib):
+@pytest.mark.parametrize("name,make,trials,frames", [
+    ("soft-cube-6, 2 trial sweeps", lambda: demos.soft_cube_scene(seed=3, n=6), 2, 40),
+    ("soft-cube-6, kept trial sweep", lambda: demos.soft_cube_scene(seed=3, n=6), 1, 40),
+    ("soft-cube-6, no trial sweep", lambda: demos.soft_cube_scene(seed=3, n=6), 0, 40),
+    ("mixed-small, kept trial sweep", lambda: demos.mixed_scene(seed=7, cubes=4, cube_n=4, boxes=4, cloth_n=10,
+                                                                  pitch=0.5), 1, 80),
+])
+def test_zero_correction_model_reproduces_plain_frames(cuda_lib, name, make, trials, frames):
     """A model whose every prediction is zero: x_learned == x_plain, the
-    trial sweeps are undone, every frame accepts, and the trajectory is the
-    plain one bit for bit."""
-    s = demos.soft_cube_scene(seed=3, n=6)
+    race is a tie that the prediction wins, and the trajectory is the plain
+    one bit for bit — with the trial sweeps undone, with the winner's sweep
+    kept as the first iteration (its OGC bound count included), without a
+    trial sweep, and in a color-Jacobi scene whose predicted branch has its
+    own pending-solve buffers."""
+    s = make()
     plain, learn = GPUSolver(s), GPUSolver(s)
     norm = np.zeros(learned.NNORM, np.float32)
     norm[learned.XI:learned.XI + learned.DIN] = 1.0
     norm[learned.YS:learned.NNORM] = 1.0
-    learn.set_warm_start_model(np.zeros(learned.NPARAM, np.float32), norm, 2)
+    learn.set_warm_start_model(np.zeros(learned.NPARAM, np.float32), norm, trials)
     learn.set_warm_start_mode(abi.WARM_START_LEARNED)
-    for f in range(40):
+    for f in range(frames):
         plain.step(1)
         learn.step(1)
         a, _ = plain.positions()
         b, _ = learn.positions()
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f
-    assert learn.counters().learn_accepted == 40
+    assert learn.counters().learn_accepted == frames
+    assert learn.counters().ogc_exceeded == plain.counters().ogc_exceeded
 
 
 def test_training_learns_the_correction(cuda_lib):
