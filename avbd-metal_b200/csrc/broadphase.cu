@@ -630,17 +630,66 @@ void launch_broadphase(const Params& P, const DevPtrs& d, const Sizes& z, cudaSt
 // memory.  The array is part of the library's device image, so every GPU that
 // loads the library holds these 4 KiB until the process exits.  Host code may
 // not use the array's name as a device address (it is a host-side stand-in);
-// the real address is looked up once per device with cudaGetSymbolAddress.
+// the real address is looked up once per CUDA context with
+// cudaGetSymbolAddress.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kNoAllocScratchWords = SCAN_BLOCK;                        // 1024 block sums
 constexpr uint32_t kNoAllocMaxElements = SCAN_BLOCK * kNoAllocScratchWords;  // 1,048,576 words
 
 static __device__ __align__(256) uint32_t g_noalloc_scan_block_sums[kNoAllocScratchWords];
 
+// In-place first pass (d_in == d_out): the same block scan as k_scan_blocks
+// with one pointer, no __restrict__.  Each thread loads its own words before
+// the block scan's barriers and stores to the same words after them.
+__global__ void k_scan_blocks_inplace(uint32_t* data, uint32_t* blockSums, uint32_t n) {
+    __shared__ uint32_t warpSums[32];
+    const uint32_t base = blockIdx.x * SCAN_BLOCK + threadIdx.x * SCAN_GRAIN;
+    uint32_t v[SCAN_GRAIN];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_GRAIN; i++) {
+        v[i] = base + i < n ? data[base + i] : 0u;
+        sum += v[i];
+    }
+    uint32_t total;
+    uint32_t run = block_exclusive_scan(sum, warpSums, total);
+#pragma unroll
+    for (int i = 0; i < SCAN_GRAIN; i++) {
+        if (base + i < n) data[base + i] = run;
+        run += v[i];
+    }
+    if (threadIdx.x == 0) blockSums[blockIdx.x] = total;
+}
+
 namespace {
-constexpr int kMaxDevices = 256;
+// The array's device address, looked up once per CUDA context: a __device__
+// symbol is loaded separately into every context, so a caller that makes a
+// non-primary context current (cuCtxCreate / cuCtxSetCurrent) gets that
+// context's copy, not the primary context's.
+struct ScratchEntry { void* ctx; uint32_t* addr; };
+constexpr int kMaxContexts = 64;
 std::mutex g_noalloc_mutex;
-uint32_t* g_noalloc_scratch[kMaxDevices] = {};   // device address per device ordinal
+ScratchEntry g_noalloc_scratch[kMaxContexts] = {};
+int g_noalloc_entries = 0;
+using CtxGetCurrentFn = int (*)(void**);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+bool g_ctx_lookup_done = false;
+
+// The current driver context (cuCtxGetCurrent through the runtime's entry
+// point table, so the library needs no link against libcuda), or null.
+void* current_context() {
+    if (!g_ctx_lookup_done) {
+        g_ctx_lookup_done = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+    }
+    void* ctx = nullptr;
+    if (!g_ctx_get_current || g_ctx_get_current(&ctx) != 0) return nullptr;
+    return ctx;
+}
 }  // namespace
 
 void set_thread_error(const char* msg);
@@ -660,30 +709,50 @@ extern "C" int avbd_exclusive_scan_noalloc(const uint32_t* d_in, uint32_t* d_out
                          "of its fixed 4 KiB scratch");
         return AVBD_ERR_INVALID_ARGUMENT;
     }
+    const uintptr_t inLo = reinterpret_cast<uintptr_t>(d_in), outLo = reinterpret_cast<uintptr_t>(d_out);
+    const uintptr_t bytes = (uintptr_t)n * sizeof(uint32_t);
+    const bool inPlace = inLo == outLo;
+    if (!inPlace && inLo < outLo + bytes && outLo < inLo + bytes) {
+        set_thread_error("avbd_exclusive_scan_noalloc: d_in and d_out overlap without being equal");
+        return AVBD_ERR_INVALID_ARGUMENT;
+    }
     int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) {
         set_thread_error("avbd_exclusive_scan_noalloc: no current CUDA device");
         return AVBD_ERR_NO_DEVICE;
     }
     uint32_t* scratch = nullptr;
     {
-        // once per device, with that device current: the device address of
-        // the fixed scratch array
+        // once per context, with it current: the device address of the
+        // fixed scratch array
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-        if (!g_noalloc_scratch[dev]) {
+        void* ctx = current_context();
+        for (int i = 0; i < g_noalloc_entries && ctx; i++)
+            if (g_noalloc_scratch[i].ctx == ctx) scratch = g_noalloc_scratch[i].addr;
+        if (!scratch) {
             void* addr = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scan_block_sums);
             if (e != cudaSuccess || !addr) {
                 set_thread_error("avbd_exclusive_scan_noalloc: cudaGetSymbolAddress failed");
                 return AVBD_ERR_KERNEL_MISSING;
             }
-            g_noalloc_scratch[dev] = static_cast<uint32_t*>(addr);
+            scratch = static_cast<uint32_t*>(addr);
+            if (ctx && g_noalloc_entries < kMaxContexts) g_noalloc_scratch[g_noalloc_entries++] = {ctx, scratch};
         }
-        scratch = g_noalloc_scratch[dev];
     }
-    // k_scan_blocks writes block sum b before k_scan_block_sums and k_scan_add
-    // read it, so the shared scratch needs no clearing between calls.
-    launch_exclusive_scan(d_in, d_out, n, scratch, static_cast<cudaStream_t>(cuda_stream));
+    // The first pass writes block sum b before the block-sum scan and the
+    // uniform add read it, so the shared scratch needs no clearing between calls.
+    cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
+    if (inPlace) {
+        const uint32_t nblocks = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+        k_scan_blocks_inplace<<<nblocks, SCAN_THREADS, 0, st>>>(d_out, scratch, n);
+        if (nblocks > 1) {
+            k_scan_block_sums<<<1, SCAN_THREADS, 0, st>>>(scratch, nblocks);
+            k_scan_add<<<nblocks, SCAN_THREADS, 0, st>>>(d_out, scratch, n);
+        }
+    } else {
+        launch_exclusive_scan(d_in, d_out, n, scratch, st);
+    }
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         set_thread_error(cudaGetErrorString(e));

@@ -469,10 +469,13 @@ int avbd_debug_read(avbd_solver* solver, int which, void* dst, size_t bytes);
  *
  * Limit: n <= 1,048,576; a larger n returns AVBD_ERR_INVALID_ARGUMENT and
  * leaves the message for avbd_last_error(NULL, ...).  d_in and d_out are
- * device pointers on the current device and may alias; `cuda_stream` is a
- * cudaStream_t passed as void* (NULL = the default stream).  The first call
- * on a device looks up the scratch array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * device pointers on the current device; they may be equal (an in-place
+ * scan) or disjoint, and a partial overlap returns AVBD_ERR_INVALID_ARGUMENT.
+ * `cuda_stream` is a cudaStream_t passed as void* (NULL = the default
+ * stream).  The first call in a CUDA context (the device's primary context,
+ * or one the caller made current with cuCtxSetCurrent) looks up that
+ * context's scratch array address (cudaGetSymbolAddress); make that first
+ * call before any stream capture.
  * All calls share the one scratch array, so calls that overlap on the GPU
  * (work on different streams running at the same time) race: serialise them.
  * Each call writes every scratch word it reads before reading it, so nothing

@@ -59,6 +59,9 @@ def lib():
         _lib.oracle_skin_deform.argtypes = [C.c_void_p, C.c_void_p]
         _lib.oracle_render_pusht_obs.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
         _lib.oracle_max_constraint_error.argtypes = [C.c_void_p, C.POINTER(C.c_float)]
+        _lib.oracle_set_residual_trace.argtypes = [C.c_void_p, C.c_int]
+        _lib.oracle_get_residual_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        _lib.oracle_residual.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
         _lib.oracle_get_counters.argtypes = [C.c_void_p, C.c_void_p]
         _lib.oracle_debug_buffer_size.argtypes = [C.c_void_p, C.c_int]
         _lib.oracle_debug_buffer_size.restype = C.c_size_t
@@ -182,6 +185,19 @@ class OracleSolver:
     def max_constraint_error(self) -> float:
         v = C.c_float()
         lib().oracle_max_constraint_error(self._h, C.byref(v))
+        return v.value
+
+    def set_residual_trace(self, enabled: bool) -> None:
+        lib().oracle_set_residual_trace(self._h, 1 if enabled else 0)
+
+    def residual_trace(self, n: int) -> np.ndarray:
+        out = np.zeros(n, np.float64)
+        lib().oracle_get_residual_trace(self._h, out.ctypes.data, n)
+        return out
+
+    def residual(self) -> float:
+        v = C.c_double()
+        lib().oracle_residual(self._h, C.byref(v))
         return v.value
 
     def counters(self):

@@ -2233,8 +2233,10 @@ float Solver::max_constraint_error() const {
         F3 pB = xform(xyz(posLin[b]), posAng[b], xyz(j.rB));
         err = fmax_(err, length(pA - pB));
     }
+    // the frame's manifolds were swapped into prevManifolds at the end of the
+    // step; diagnostics read them there (GPUSolver.swift:4846-4853)
     for (uint32_t g = 0; g < numPairs; g++) {
-        const ManifoldGPU& m = manifolds[g];
+        const ManifoldGPU& m = prevManifolds[g];
         uint32_t a = m.header.x, b = m.header.y;
         bool sphA = (m.header.w & 2u) != 0, sphB = (m.header.w & 4u) != 0;
         for (uint32_t i = 0; i < m.header.z; i++) {
@@ -2245,6 +2247,52 @@ float Solver::max_constraint_error() const {
         }
     }
     return err;
+}
+
+// ==========================================================================
+// AL residual r = ||grad of the AL objective||_2 over every dynamic DOF.  The
+// reference defines only diag_error (40_solver.metal:2189-2229); the residual
+// is the right-hand side that primal_body assembles (the stamps of
+// 40_solver.metal:741-1359 plus the inertial term M/dt^2 (x - x~)), for
+// particles over 3 DOFs and for rigid bodies over 6 (angular part with the
+// world inertia / dt^2 times q_sub(q, q~)).  Per body the squared norm is a
+// float, the total a double sum.
+// ==========================================================================
+float Solver::body_residual_sq(uint32_t body) const {
+    bool rigid = shape[body].w >= 0.0f;
+    Accum lane[8];
+    for (int l = 0; l < 8; l++) lane[l] = accum_zero();
+    uint32_t as = adjStart[body], cnt = adjCount[body];
+    for (uint32_t k = 0; k < cnt; k++) stamp_entry(adjList[as + k], body, lane[k & 7u]);
+    for (int d = 4; d >= 1; d >>= 1) {
+        F3 nl[8], na[8];
+        for (int l = 0; l < 8; l++) {
+            nl[l] = lane[l].rhsLin + lane[l ^ d].rhsLin;
+            na[l] = lane[l].rhsAng + lane[l ^ d].rhsAng;
+        }
+        for (int l = 0; l < 8; l++) { lane[l].rhsLin = nl[l]; lane[l].rhsAng = na[l]; }
+    }
+    F4 pl = posLin[body];
+    float dt2 = P.dt * P.dt;
+    F3 rl = lane[0].rhsLin + (xyz(pl) - xyz(inertLin[body])) * (pl.w / dt2);
+    if (!rigid) return dot(rl, rl);
+    F4 q = posAng[body];
+    M3 inertia = m3_scale(world_inertia(q, xyz(props[body])), 1.0f / dt2);
+    F3 ra = lane[0].rhsAng + m3_mul(inertia, q_sub(q, inertAng[body]));
+    return dot(rl, rl) + dot(ra, ra);
+}
+
+double Solver::residual() const {
+    uint32_t colorBound = dynamicColoring ? (uint32_t)MAX_COLORS : staticUsedColors;
+    uint32_t n = colorStart[colorBound];
+    std::vector<float> per(n);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(threads) if (threads > 1 && n > 256)
+#endif
+    for (int i = 0; i < (int)n; i++) per[i] = body_residual_sq(colorList[i]);
+    double s = 0.0;
+    for (uint32_t i = 0; i < n; i++) s += (double)per[i];
+    return std::sqrt(s);
 }
 
 // ==========================================================================
@@ -2284,6 +2332,10 @@ void Solver::step() {
     adjacency();
     if (dynamicColoring) dynamic_coloring();
     uint32_t colorBound = dynamicColoring ? (uint32_t)MAX_COLORS : staticUsedColors;
+    if (traceEnabled) {
+        trace.assign(2 + P.iterations, 0.0);
+        trace[0] = trace[1] = residual();
+    }
     for (uint32_t it = 0; it < P.iterations; it++) {
         ogcPass = 0;
         for (uint32_t c = 0; c < colorBound; c++) {
@@ -2300,6 +2352,7 @@ void Solver::step() {
         // were bound-limited (ogc_refresh_args, 25_cloth.metal:857-870)
         if (ogc && it + 1 < P.iterations && ogcPass * 100u > P.numParticles) ogc_refresh();
         ogcExceeded = ogcPass;
+        if (traceEnabled) trace[2 + it] = residual();
     }
     if (planar) dat_restore_failed_surface();
     finalize();
@@ -2446,6 +2499,13 @@ int oracle_get_motor_states(void* h, const uint32_t* ids, uint32_t n, float* ang
     return AVBD_OK;
 }
 float oracle_atan2(float y, float x) { return oracle::atan2_series(y, x); }
+int oracle_set_residual_trace(void* h, int enabled) { static_cast<Solver*>(h)->traceEnabled = enabled != 0; return AVBD_OK; }
+int oracle_get_residual_trace(void* h, double* out, uint32_t n) {
+    Solver* s = static_cast<Solver*>(h);
+    for (uint32_t i = 0; i < n; i++) out[i] = i < s->trace.size() ? s->trace[i] : 0.0;
+    return AVBD_OK;
+}
+int oracle_residual(void* h, double* out) { *out = static_cast<Solver*>(h)->residual(); return AVBD_OK; }
 int oracle_max_constraint_error(void* h, float* out) { *out = static_cast<Solver*>(h)->max_constraint_error(); return AVBD_OK; }
 int oracle_get_counters(void* h, avbd_counters* out) {
     Solver* s = static_cast<Solver*>(h);

@@ -297,6 +297,12 @@ struct Solver {
     void finalize();
     void advance_spinners();
     float max_constraint_error() const;
+    // AL residual: per body the squared norm of the primal's right-hand side
+    // (the gradient of the augmented-Lagrangian objective), summed in double
+    float body_residual_sq(uint32_t body) const;
+    double residual() const;
+    bool traceEnabled = false;
+    std::vector<double> trace;   // [0] warm start (plain), [1] warm start used, [2 + k] after iteration k
 };
 
 }  // namespace oracle

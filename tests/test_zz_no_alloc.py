@@ -6,8 +6,10 @@ allocation ban): its block-sum scratch is a fixed device array in the
 library, not memory the call allocates.  Here two calls in a row are checked
 word for word against the scan computed by the existing entry points — the
 solver's own exclusive scan of its hash-bucket counts (avbd_step, read back
-with avbd_debug_read).  This file sorts last so that a run stopping at the
-first failure has already run every other test; it also passes alone.
+with avbd_debug_read) — and against numpy's exclusive cumulative sum (uint32
+wraparound) of random words at ragged sizes up to the 1,048,576-word limit,
+in place and out of place.  This file sorts last so that a run stopping at
+the first failure has already run every other test; it also passes alone.
 """
 import ctypes as C
 
@@ -47,6 +49,52 @@ def test_noalloc_scan_matches_solver_scan_twice(cuda_lib):
         assert rc == abi.OK
         assert got.shape == want.shape and np.array_equal(got, want)
         solver.close()
+
+
+def bind(lib):
+    lib.avbd_exclusive_scan_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+    lib.avbd_exclusive_scan_noalloc.restype = C.c_int
+    return lib
+
+
+def exclusive_cumsum_u32(words):
+    out = np.zeros(len(words), np.uint64)
+    if len(words) > 1:
+        out[1:] = np.cumsum(words[:-1].astype(np.uint64))
+    return (out & 0xFFFFFFFF).astype(np.uint32)
+
+
+@pytest.mark.parametrize("n", [1, 1023, 1025, 1_048_575, 1_048_576])
+def test_noalloc_scan_matches_numpy(cuda_lib, n):
+    """Random words (large values, so the sums wrap around 2^32): a partial
+    last block, one word past a block, and the largest n (1024 blocks, every
+    scratch word used); out of place, then in place on the same buffer."""
+    import torch
+    lib = bind(load_library())
+    rng = np.random.default_rng(n)
+    words = rng.integers(0, 1 << 32, size=n, dtype=np.uint64).astype(np.uint32)
+    want = exclusive_cumsum_u32(words)
+    dev_in = torch.from_numpy(words.view(np.int32).copy()).cuda()
+    dev_out = torch.empty_like(dev_in)
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = lib.avbd_exclusive_scan_noalloc(C.c_void_p(dev_in.data_ptr()), C.c_void_p(dev_out.data_ptr()), n, stream)
+    torch.cuda.synchronize()
+    assert rc == abi.OK
+    assert np.array_equal(dev_out.cpu().numpy().view(np.uint32), want)
+    assert np.array_equal(dev_in.cpu().numpy().view(np.uint32), words)    # input untouched
+    rc = lib.avbd_exclusive_scan_noalloc(C.c_void_p(dev_in.data_ptr()), C.c_void_p(dev_in.data_ptr()), n, stream)
+    torch.cuda.synchronize()
+    assert rc == abi.OK
+    assert np.array_equal(dev_in.cpu().numpy().view(np.uint32), want)
+
+
+def test_noalloc_scan_rejects_partial_overlap(cuda_lib):
+    import torch
+    lib = bind(load_library())
+    buf = torch.zeros(4096, dtype=torch.int32, device="cuda")
+    rc = lib.avbd_exclusive_scan_noalloc(C.c_void_p(buf.data_ptr()), C.c_void_p(buf.data_ptr() + 4 * 16), 2048,
+                                         None)
+    assert rc == abi.ERR_INVALID_ARGUMENT
 
 
 def test_noalloc_scan_rejects_oversize(cuda_lib):
