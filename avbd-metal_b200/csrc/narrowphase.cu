@@ -267,8 +267,14 @@ __device__ void emit_round_manifold(const Params& P, const DevPtrs& d, const NPa
                 }
             }
         }
-        const float3 xAw = roundA ? xyz(p.bodyPA) + rA_ : xform(xyz(p.bodyPA), p.qBodyA, rA_);
-        const float3 xBw = roundB ? xyz(p.bodyPB) + rB_ : xform(xyz(p.bodyPB), p.qBodyB, rB_);
+        // tori measure the gap between the hit points themselves
+        // (30_narrowphase.metal:925-958); capsules and spheres between the
+        // points their stored anchors give back (:727-731, :1115-1119)
+        const bool fromHits = stickRule == STICK_NONE;
+        const float3 xAw = fromHits ? contacts[i].xA
+                                    : (roundA ? xyz(p.bodyPA) + rA_ : xform(xyz(p.bodyPA), p.qBodyA, rA_));
+        const float3 xBw = fromHits ? contacts[i].xB
+                                    : (roundB ? xyz(p.bodyPB) + rB_ : xform(xyz(p.bodyPB), p.qBodyB, rB_));
         const float3 dd = xAw - xBw;
         float3 C0 = mk3(dot(nrm, dd) + P.collisionMargin, dot(t1, dd), dot(t2, dd));
         float sx, sy;

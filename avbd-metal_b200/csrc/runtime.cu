@@ -312,7 +312,7 @@ struct avbd_solver {
         const bool tuningFrame = primalEvents != nullptr;
         const bool learned = !tuningFrame && learnMode == AVBD_WARM_START_LEARNED && modelSet && z.numLearn;
         const bool capture = !tuningFrame && learnCapture && z.numLearn;
-        const bool trace = !tuningFrame && residualTrace;
+        const bool trace = residualTrace;     // tuning frames too: they solve like any other
         // With one trial sweep the winner's swept pose is kept as the primal
         // half of the first iteration (the dual follows as usual); with more
         // trial sweeps both branches are undone and the solve restarts from

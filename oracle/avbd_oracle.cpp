@@ -846,8 +846,13 @@ static void emit_round_manifold(const Solver& S, const NPair& p, ManifoldGPU& ou
                 }
             }
         }
-        F3 xAw = roundA ? xyz(p.bodyPA) + rA_ : xform(xyz(p.bodyPA), p.qBodyA, rA_);
-        F3 xBw = roundB ? xyz(p.bodyPB) + rB_ : xform(xyz(p.bodyPB), p.qBodyB, rB_);
+        // tori measure the gap between the hit points themselves
+        // (30_narrowphase.metal:925-958); capsules between the points their
+        // stored anchors give back (:727-731)
+        F3 xAw = !capsuleRule ? contacts[i].xA
+                              : (roundA ? xyz(p.bodyPA) + rA_ : xform(xyz(p.bodyPA), p.qBodyA, rA_));
+        F3 xBw = !capsuleRule ? contacts[i].xB
+                              : (roundB ? xyz(p.bodyPB) + rB_ : xform(xyz(p.bodyPB), p.qBodyB, rB_));
         F3 d = xAw - xBw;
         F3 C0 = f3(dot(nrm, d) + P.collisionMargin, dot(t1, d), dot(t2, d));
         float sx, sy;
@@ -2308,9 +2313,15 @@ void Solver::step() {
     dat = DatCounters{};
     softRaw = 0;
     numSoft = 0;
+    hook(ST_BROADPHASE, 0, 0);
     broadphase();
+    hook(ST_BROADPHASE, 0, 1);
+    hook(ST_NARROWPHASE, 0, 0);
     narrowphase();
+    hook(ST_NARROWPHASE, 0, 1);
+    hook(ST_MAP, 0, 0);
     map_rebuild();
+    hook(ST_MAP, 0, 1);
     if (planar) {
         elem_grid();
         dat_build_pairs();                     // step-start pose
@@ -2318,8 +2329,12 @@ void Solver::step() {
     } else if (ogc) {
         ogc_detect();
     }
+    hook(ST_WARM_JOINTS, 0, 0);
     warmstart_joints();
+    hook(ST_WARM_JOINTS, 0, 1);
+    hook(ST_WARM_BODIES, 0, 0);
     warmstart_bodies();
+    hook(ST_WARM_BODIES, 0, 1);
     if (planar) {
         dat_reduce(0xFFFFFFFFu);               // predictor pass
         dat_apply_particles();
@@ -2329,8 +2344,14 @@ void Solver::step() {
         soft_map_rebuild();
         for (uint32_t v : particleIdx) ogcPrev[v] = f4(xyz(posLin[v]), 0.0f);
     }
+    hook(ST_ADJACENCY, 0, 0);
     adjacency();
-    if (dynamicColoring) dynamic_coloring();
+    hook(ST_ADJACENCY, 0, 1);
+    if (dynamicColoring) {
+        hook(ST_COLORING, 0, 0);
+        dynamic_coloring();
+        hook(ST_COLORING, 0, 1);
+    }
     uint32_t colorBound = dynamicColoring ? (uint32_t)MAX_COLORS : staticUsedColors;
     if (traceEnabled) {
         trace.assign(2 + P.iterations, 0.0);
@@ -2339,7 +2360,9 @@ void Solver::step() {
     for (uint32_t it = 0; it < P.iterations; it++) {
         ogcPass = 0;
         for (uint32_t c = 0; c < colorBound; c++) {
+            hook(ST_PRIMAL, (int)c, 0);
             primal_color(c);
+            hook(ST_PRIMAL, (int)c, 1);
             if (planar) {
                 dat_reduce(c);
                 dat_apply_color(c);
@@ -2347,7 +2370,9 @@ void Solver::step() {
                 publish_color(c);
             }
         }
+        hook(ST_DUAL, (int)it, 0);
         dual_all();
+        hook(ST_DUAL, (int)it, 1);
         // mid-solve bound refresh when more than 1% of the surface vertices
         // were bound-limited (ogc_refresh_args, 25_cloth.metal:857-870)
         if (ogc && it + 1 < P.iterations && ogcPass * 100u > P.numParticles) ogc_refresh();
@@ -2355,7 +2380,9 @@ void Solver::step() {
         if (traceEnabled) trace[2 + it] = residual();
     }
     if (planar) dat_restore_failed_surface();
+    hook(ST_FINALIZE, 0, 0);
     finalize();
+    hook(ST_FINALIZE, 0, 1);
     if (numTris > 0 && clothViscosity > 0.0f) smooth_particle_velocities();
     advance_spinners();
     frameIndex++;

@@ -301,6 +301,14 @@ struct Solver {
     // (the gradient of the augmented-Lagrangian objective), summed in double
     float body_residual_sq(uint32_t body) const;
     double residual() const;
+    // Stage observer for the pinning harness (oracle/ref_pin.cpp): called
+    // before (after = 0) and after (after = 1) every stage of a frame.
+    enum Stage { ST_BROADPHASE, ST_NARROWPHASE, ST_MAP, ST_WARM_JOINTS, ST_WARM_BODIES, ST_ADJACENCY,
+                 ST_COLORING, ST_PRIMAL, ST_DUAL, ST_FINALIZE, ST_COUNT_ };
+    typedef void (*StageHook)(Solver* s, int stage, int arg, int after, void* ctx);
+    StageHook stageHook = nullptr;
+    void* stageCtx = nullptr;
+    void hook(int stage, int arg, int after) { if (stageHook) stageHook(this, stage, arg, after, stageCtx); }
     bool traceEnabled = false;
     std::vector<double> trace;   // [0] warm start (plain), [1] warm start used, [2 + k] after iteration k
 };
