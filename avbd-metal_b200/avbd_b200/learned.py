@@ -226,6 +226,83 @@ def matched_residual_iterations(make_scene: Callable[[int], object], seed: int, 
     return plain_iterations, target, r["rel_residual_final"], r["accepted"] / max(1, r["frames"])
 
 
+class _Rollout:
+    """One solver of a seeded scene, rewound to its first frame for every
+    evaluation (no scene rebuild per iteration count)."""
+
+    def __init__(self, make_scene, seed, model, trial_sweeps):
+        self.g = GPUSolver(make_scene(seed))
+        if model is not None:
+            self.g.set_warm_start_model(model.params, model.norm, trial_sweeps)
+            self.g.set_warm_start_mode(abi.WARM_START_LEARNED)
+        self.g.set_residual_trace(True)
+        self.start = self.g.snapshot()
+
+    def run(self, iterations, frames, skip=2, tolerances=()):
+        g = self.g
+        g.restore(self.start)
+        st = g.settings
+        st.iterations = iterations
+        g.settings = st
+        its = {t: [] for t in tolerances}
+        rel_final = []
+        for f in range(frames):
+            g.step(1)
+            if f < skip:
+                continue
+            tr = g.residual_trace(2 + iterations)
+            rel_final.append(tr[-1] / max(tr[0], 1e-300))
+            for t in tolerances:
+                its[t].append(iterations_to_tolerance(tr, tr[0], t))
+        return float(np.median(rel_final)), its
+
+    def close(self):
+        self.g.close()
+
+
+def matched_comparison(make_scene: Callable[[int], object], seed: int, model: WarmStartModel,
+                       plain_iterations: int, frames: int = 120, trial_sweeps: int = 1,
+                       tolerances: Sequence[float] = (0.5, 0.3, 0.2, 0.1, 1e-2, 1e-3, 1e-6),
+                       budget: int = 60) -> Dict[str, object]:
+    """Plain vs learned warm start at a matched AL residual.
+
+    The matched level is the plain warm start's median r_final / r0 over the
+    rollout at `plain_iterations`.  For the plain form every count from 4 to
+    `plain_iterations` is evaluated (the residual need not fall monotonically
+    with the count) and the smallest that reaches the level is reported; for
+    the learned form, the smallest count from 4 up that reaches it.  Both
+    forms are also run at `budget` iterations to report, for each tolerance,
+    the median number of iterations to reach it (frames that never reach a
+    tolerance count as `budget + 1`; a tolerance neither form reaches in half
+    the frames is reported as None)."""
+    plain = _Rollout(make_scene, seed, None, trial_sweeps)
+    curve = {k: plain.run(k, frames)[0] for k in range(4, plain_iterations + 1)}
+    target = curve[plain_iterations]
+    plain_min = min(k for k, r in curve.items() if r <= target)
+    _, p_its = plain.run(budget, frames, tolerances=tolerances)
+    plain.close()
+    learned = _Rollout(make_scene, seed, model, trial_sweeps)
+    learned_k, learned_r = plain_iterations, None
+    for k in range(4, plain_iterations + 1):
+        r = learned.run(k, frames)[0]
+        if r <= target:
+            learned_k, learned_r = k, r
+            break
+    if learned_r is None:
+        learned_r = learned.run(plain_iterations, frames)[0]
+    _, q_its = learned.run(budget, frames, tolerances=tolerances)
+    learned.close()
+    itt = {}
+    for t in tolerances:
+        a = np.array([x if x > 0 else budget + 1 for x in p_its[t]])
+        b = np.array([x if x > 0 else budget + 1 for x in q_its[t]])
+        reached = (a <= budget).mean() >= 0.5 or (b <= budget).mean() >= 0.5
+        itt[f"{t:g}"] = ({"plain": float(np.median(a)), "learned": float(np.median(b))} if reached else None)
+    return {"target": float(target), "plain_curve": {str(k): float(v) for k, v in curve.items()},
+            "plain_min_iterations": int(plain_min), "learned_iterations": int(learned_k),
+            "learned_residual": float(learned_r), "iterations_to_tolerance": itt, "budget": budget}
+
+
 def _soft_cube(seed):
     from . import demos
     return demos.soft_cube_scene(seed=seed, n=24)

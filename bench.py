@@ -1,40 +1,48 @@
 #!/usr/bin/env python
 """Benchmark of the AVBD solver step on B200.
 
-Workload: the soft-body configuration — a 24x24x24-vertex lattice of a 1 m
-cube (13,824 particles, 60,835 Stable Neo-Hookean tets, 5 tets per cell),
-E = 1e5 Pa, nu = 0.4, density 1000, dropped from 0.5 m onto a static ground,
-friction 0.4, dt = 1/60, 20 iterations, static topology palette; seeded
-synthetic scene (SplitMix64).  One step = one solver frame of the whole scene.
+Default workload (one GPU): the mixed configuration — 64 soft cubes of 10^3
+vertices (Stable Neo-Hookean E=5e4 Pa, nu=0.45), 256 rigid boxes with edges
+U(0.1, 0.4) m and a 128 x 128 cloth falling together onto the ground,
+isotropic-OGC element contacts, dt = 1/60, 20 iterations; seeded synthetic
+scene (SplitMix64).  One step = one solver frame of the whole scene.
 
-Metric: vertex-steps/s (dynamic particles x frames / second), plain AVBD warm
-start.  `value` is device-timed with CUDA events on the solver's stream,
-inputs resident in HBM, L2 flushed between timed steps; `e2e` is the same
-metric through the C ABI with host buffers (positions uploaded from pinned
-memory and read back every step).
+Metric: vertex-steps/s (dynamic particles + dynamic rigid bodies, x frames,
+/ second) at matched AL residual, plain vs learned warm start.  `value` is the
+plain warm start at the configured iteration count (whose median residual
+defines the matched level); `learned_warm_start` gives the learned warm start
+at the smallest iteration count that reaches that level, beside the smallest
+plain iteration count that reaches it too, and iterations-to-tolerance of
+both forms.
+
+Every arm times the same window of the configuration: `--preroll` untimed
+frames bring the scene into its contact regime, then `--warmup` frames, then
+`--steps` timed frames.  `value` is device-timed with CUDA events on the
+solver's stream, inputs resident in HBM, L2 flushed between timed steps;
+`e2e` is the same frames through the C ABI with host buffers (positions
+uploaded from pinned memory and read back every step).  The roofline's
+per-launch time of the per-color primal comes from the same window: the
+window is replayed from a snapshot with stage timing on, and the primal's
+share of that device time scales the timed milliseconds.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload soft-cube|cloth-sphere|mixed|batched-worlds]
+                  [--workload mixed|soft-cube|cloth-sphere|batched-worlds|rigid-stack]
 
-`--workload cloth-sphere` measures the cloth configuration instead: a
-256 x 256 sheet of 2 m (65,536 particles, 130,050 StVK membranes, Bergou
-bends, hard structural rods), two pinned corners, draped over a static
-sphere, Planar-DAT truncation, dt = 1/120, 30 iterations.
-`--workload mixed` measures the mixed configuration: 64 soft cubes of 10^3
-vertices, 256 rigid boxes and a 128 x 128 cloth falling together, with
-isotropic-OGC vertex-triangle, edge-edge and rigid-triangle contacts.
-`--workload batched-worlds` measures 4096 independent articulated worlds
-per GPU (body-steps/s; new motor targets every step); under torchrun each
-rank owns its own 4096 worlds (weak scaling, no data-path collective).
+Other workloads: `soft-cube` (24^3 lattice, 60,835 tets, 20 iterations),
+`cloth-sphere` (256^2 sheet over a sphere, Planar-DAT, 30 iterations),
+`batched-worlds` (4096 articulated worlds per GPU, new motor targets every
+step, body-steps/s), `rigid-stack` (20 unit cubes, 10 iterations,
+body-steps/s; CPU baseline: the reference's CPU solver restated).
 
-Under torchrun (N > 1) every rank runs an independent replica of the scene
-("replicas only": the coupled scene has no natural partition); time is the
-max over ranks and `value` counts the vertices of all ranks.
+Under torchrun (N > 1) the default workload is `batched-worlds`: each rank
+owns its own 4096 worlds (weak scaling, no data-path collective; worlds never
+interact).  The coupled scenes have no natural partition and run as
+replicas.  Time is the max over ranks and `value` counts the units of all
+ranks.
 """
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -47,37 +55,45 @@ for _p in (ROOT, os.path.join(ROOT, "avbd-metal_b200")):
         sys.path.insert(0, _p)
 
 METRIC = "vertex-steps/s at matched AL residual: plain vs learned warm-start, 1 B200"
+
+# name -> (description, untimed frames before the window)
 WORKLOADS = {
-    "soft-cube": ("soft-cube-24: 24^3-vertex lattice of a 1 m cube, 13,824 particles, 60,835 "
-                  "Stable Neo-Hookean tets, E=1e5 Pa, nu=0.4, rho=1000, friction 0.4, dt=1/60, "
-                  "20 iterations, static palette, plain warm start"),
-    "cloth-sphere": ("cloth-sphere-256: 256^2-vertex sheet of 2 m (65,536 particles, 130,050 StVK "
-                     "membranes mu=lambda=1e4, Bergou bending 1e-3, hard structural rods), contact "
-                     "radius 2e-3 m, two pinned corners, static sphere r=0.5 m, Planar-DAT, dt=1/120, "
-                     "30 iterations, plain warm start"),
     "mixed": ("mixed-64: 64 soft cubes of 10^3 vertices (Stable Neo-Hookean E=5e4 Pa, nu=0.45, side 0.3 m), "
               "256 rigid boxes with edges U(0.1, 0.4) m and a 128^2 cloth (mu=lambda=1e4, bending 1e-3) falling "
               "together onto the ground (80,384 particles + 256 boxes, 233,280 tets, 32,258 triangles), "
-              "isotropic OGC element contacts, dt=1/60, 20 iterations, plain warm start"),
+              "isotropic OGC element contacts, dt=1/60, 20 iterations", 40),
+    "soft-cube": ("soft-cube-24: 24^3-vertex lattice of a 1 m cube, 13,824 particles, 60,835 "
+                  "Stable Neo-Hookean tets, E=1e5 Pa, nu=0.4, rho=1000, friction 0.4, dt=1/60, "
+                  "20 iterations, static palette", 40),
+    "cloth-sphere": ("cloth-sphere-256: 256^2-vertex sheet of 2 m (65,536 particles, 130,050 StVK "
+                     "membranes mu=lambda=1e4, Bergou bending 1e-3, hard structural rods), contact "
+                     "radius 2e-3 m, two pinned corners, static sphere r=0.5 m, Planar-DAT, dt=1/120, "
+                     "30 iterations", 60),
     "batched-worlds": ("batched-worlds-4096: 4096 worlds (one collision group each) of a planar 3-7 link "
                        "hinge chain with implicit PD motors (targets U(+-0.5 rad) every step) and a welded "
                        "T block on a plane, friction 0.5, dt=1/60, 8 iterations, dynamic coloring; "
-                       "worlds sharded across ranks"),
+                       "worlds sharded across ranks", 30),
+    "rigid-stack": ("rigid-stack-20: 20 unit cubes (density 1000) stacked with 1e-3 m gaps and U(+-1e-3) m "
+                    "lateral jitter on a static ground, friction 0.5, dt=1/60, 10 iterations, beta 1e5, "
+                    "alpha 0.95, gamma 0.99", 30),
 }
+MODELS = {"soft-cube": "soft_cube_24_warm_start.npz", "mixed": "mixed_warm_start.npz"}
 MOTORS = []
-WORKLOAD_KEY = "soft-cube"
-WORKLOAD = WORKLOADS[WORKLOAD_KEY]
+WORKLOAD_KEY = "mixed"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=600)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--preroll", type=int, default=-1,
+                    help="untimed frames before the warm-up (default: per workload, into the contact regime)")
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0,
-                    help="bound on the CPU baseline sample")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="soft-cube")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bound on the CPU baseline sample")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=None,
+                    help="default: mixed on one GPU, batched-worlds under torchrun with N > 1")
+    ap.add_argument("--no-learned", action="store_true", help="skip the plain-vs-learned comparison")
     ap.add_argument("--frames-only", action="store_true",
                     help="profiling runs: warm-up and timed frames of the workload only (no e2e, stage "
                          "profile, learned comparison or CPU baseline); prints ms per frame")
@@ -90,9 +106,17 @@ def parse():
     ap.add_argument("--obs-envs", type=int, default=4096)
     ap.add_argument("--obs-res", type=int, default=64)
     args = ap.parse_args()
-    global WORKLOAD_KEY, WORKLOAD
-    WORKLOAD_KEY, WORKLOAD = args.workload, WORKLOADS[args.workload]
+    global WORKLOAD_KEY
+    if args.workload is None:
+        args.workload = "batched-worlds" if int(os.environ.get("WORLD_SIZE", "1")) > 1 else "mixed"
+    WORKLOAD_KEY = args.workload
+    if args.preroll < 0:
+        args.preroll = WORKLOADS[WORKLOAD_KEY][1]
     return args
+
+
+def workload_text():
+    return WORKLOADS[WORKLOAD_KEY][0]
 
 
 def make_scene(rank=0, worlds=4096):
@@ -101,6 +125,8 @@ def make_scene(rank=0, worlds=4096):
         return demos.cloth_sphere_scene(seed=3, n=256)
     if WORKLOAD_KEY == "mixed":
         return demos.mixed_scene(seed=5)
+    if WORKLOAD_KEY == "rigid-stack":
+        return demos.rigid_stack_scene(seed=1)
     if WORKLOAD_KEY == "batched-worlds":
         # rank r owns worlds [r * worlds, (r + 1) * worlds)
         scene, motors, _ = demos.batched_worlds_scene(worlds=worlds, seed=4, first_world=worlds * rank)
@@ -111,7 +137,8 @@ def make_scene(rank=0, worlds=4096):
 
 class MotorTargets:
     """Per-step joint targets U(+-0.5 rad) of the batched workload, drawn
-    ahead of the timed region (host arrays; uploaded by set_motor_targets)."""
+    ahead of the timed region (host arrays; uploaded by set_motor_targets).
+    Frame i of the run (preroll and warm-up included) gets row i."""
 
     def __init__(self, steps, seed=11):
         import numpy as np
@@ -123,15 +150,18 @@ class MotorTargets:
         if self.t is not None:
             solver.set_motor_targets(self.ids, self.t[i % len(self.t)])
 
+    def bytes_per_step(self):
+        return 0 if self.t is None else int(self.t.shape[1] * 8)
 
-def dynamic_vertices(scene):
+
+def dynamic_units(scene):
     """Units of the metric: dynamic particles plus dynamic rigid bodies
     (vertex-steps; body-steps for a rigid-only scene)."""
     return sum(1 for b in scene.bodies if b.is_dynamic)
 
 
 def unit():
-    return "body-steps/s" if WORKLOAD_KEY == "batched-worlds" else "vertex-steps/s"
+    return "body-steps/s" if WORKLOAD_KEY in ("batched-worlds", "rigid-stack") else "vertex-steps/s"
 
 
 def host_threads():
@@ -139,6 +169,16 @@ def host_threads():
         return len(os.sched_getaffinity(0))
     except AttributeError:
         return os.cpu_count() or 1
+
+
+def config(scene, args, world):
+    """The `config` object of both arms (the same keys and values)."""
+    return {"workload": workload_text(), "units_per_step": dynamic_units(scene), "tets": len(scene.tets),
+            "triangles": len(scene.tris), "iterations": scene.settings.iterations,
+            "window": {"preroll_frames": args.preroll, "warmup_frames": args.warmup, "timed_frames": args.steps,
+                       "first_timed_frame": args.preroll + args.warmup + 1},
+            "parallelism": (f"world shards x{world}" if WORKLOAD_KEY == "batched-worlds" else f"replicas x{world}"),
+            "warm_start": "plain gamma warm start (value); learned warm start in learned_warm_start"}
 
 
 def dist_setup(args):
@@ -164,28 +204,44 @@ def max_over_ranks(x, world, device=None):
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle (the reference algorithm restated in C++) on the
-# host cores, bounded to about `seconds` of work.
+# CPU runs: the oracle (the reference's algorithm restated in C++) or, for
+# the rigid stack, the restatement of the reference's CPU solver.
 # ---------------------------------------------------------------------------
-def cpu_run(seconds, threads, warmup=1, max_frames=200):
+def cpu_solver(scene, threads):
     import oracle
+    if WORKLOAD_KEY == "rigid-stack":
+        from oracle import cpu_solver as cs
+        cs.build()
+        return cs.CPUSolver(scene), "port", 1, ("the reference's CPU solver (CPU/CPUSolver.swift) restated in C++, "
+                                                "single-threaded as the reference")
     oracle.build()
+    return (oracle.OracleSolver(scene, threads=threads), "port", threads,
+            f"the reference's GPU-path algorithm restated in C++ (Swift/Metal cannot run here), OpenMP over the "
+            f"bodies of a color, {threads} threads")
+
+
+def cpu_window(args, seconds, warmup, threads):
+    """Preroll and warm-up on the CPU, then up to args.steps frames of the
+    timed window, bounded to `seconds`."""
     scene = make_scene()
-    nv = dynamic_vertices(scene)
-    o = oracle.OracleSolver(scene, threads=threads)
-    targets = MotorTargets(max_frames + warmup)
-    for i in range(warmup):
+    nv = dynamic_units(scene)
+    o, kind, cores, what = cpu_solver(scene, threads)
+    targets = MotorTargets(args.preroll + warmup + args.steps)
+    for i in range(args.preroll + warmup):
         targets.apply(o, i)
         o.step(1)
     frames, t0 = 0, time.perf_counter()
-    while frames < max_frames:
-        targets.apply(o, warmup + frames)
+    while frames < args.steps:
+        targets.apply(o, args.preroll + warmup + frames)
         o.step(1)
         frames += 1
         if time.perf_counter() - t0 >= seconds:
             break
-    dt = time.perf_counter() - t0
-    return nv * frames / dt, frames, dt, nv
+    secs = time.perf_counter() - t0
+    first = args.preroll + warmup + 1
+    sample = (f"{WORKLOAD_KEY}, frames {first}-{first + frames - 1} of the timed window after {args.preroll} preroll "
+              f"and {warmup} warm-up frames ({frames} frames in {secs:.1f} s); {what}")
+    return nv * frames / secs, frames, secs, kind, cores, sample
 
 
 # ---------------------------------------------------------------------------
@@ -246,41 +302,31 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic_per_launch():
-    """DRAM bytes per primal launch from the committed ncu summary, or None."""
-    name = "k_primal_soft_cube_24.md" if WORKLOAD_KEY == "soft-cube" else "k_primal_cloth_sphere_256.md"
-    path = os.path.join(ROOT, "profiles", name)
-    if not os.path.exists(path):
-        return None
-    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
-    return float(m.group(1)) if m else None
-
-
 def primal_bytes_per_iteration(solver, scene):
     """Algorithmic (unique-byte) traffic of the primal over one iteration:
     per body 16 B position read + 16 B write + 16 B inertial target + 4 B
-    color-list entry + 16 B static adjacency segment + 8 B contact segment,
-    4 B per adjacency entry, one 64 B tet record per tet, 64 B manifold
-    header/basis + 80 B per active contact; cloth adds 48 B per membrane and
-    bend, 64 B per spring, 112 B per element contact."""
+    color-list entry + 16 B static adjacency segment + 8 B contact segment
+    (+48 B orientation, inertial orientation and inertia for a rigid body),
+    4 B per adjacency entry, 64 B per tet record, 64 B manifold header/basis
+    + 80 B per active contact, 224 B per active joint; cloth and element
+    contacts add 48 B per membrane and bend, 64 B per spring, 112 B per
+    element contact."""
     import numpy as np
-    nb = dynamic_vertices(scene) + sum(1 for b in scene.bodies if not b.is_particle and b.is_dynamic)
+    nb = dynamic_units(scene)
+    rigid = sum(1 for b in scene.bodies if not b.is_particle and b.is_dynamic)
     adj = int(solver.debug_read("ADJ_COUNT", np.uint32).sum())
-    man = solver.debug_read("MANIFOLDS", np.uint32).reshape(-1, 176)
+    c = solver.counters()
+    man = solver.debug_read("MANIFOLDS", np.uint32).reshape(-1, 176)[:int(c.num_pairs)]
     contacts = int(man[:, 2].sum()) if man.size else 0
     active = int((man[:, 2] > 0).sum()) if man.size else 0
     cloth = 0
     if scene.tris:
         cloth = (48 * (solver.debug_read("MEMBRANES").size // 48 + solver.debug_read("BENDS").size // 48)
-                 + 64 * len(scene.springs) + solver.debug_read("SOFT").size)
-    rigid = sum(1 for b in scene.bodies if not b.is_particle and b.is_dynamic)
+                 + 64 * len(scene.springs))
+    soft = 112 * int(c.num_soft)
     joints = sum(1 for j in scene.joints if j.stiffness_lin != 0 or j.stiffness_ang != 0 or j.motor_torque != 0)
     return (nb * (16 + 16 + 16 + 4 + 16 + 8) + 48 * rigid + 4 * adj + 64 * len(scene.tets) + 64 * active
-            + 80 * contacts + 224 * joints + cloth)
-
-
-# ---------------------------------------------------------------------------
-MODELS = {"soft-cube": "soft_cube_24_warm_start.npz", "mixed": "mixed_warm_start.npz"}
+            + 80 * contacts + 224 * joints + cloth + soft)
 
 
 def model_path():
@@ -288,15 +334,16 @@ def model_path():
     return os.path.join(ROOT, "avbd-metal_b200", "avbd_b200", "models", name) if name else None
 
 
-def timed_steps(solver, targets, first, K, stream, flush):
-    """K frames, one CUDA-event pair per frame on the solver stream, with an
-    untimed L2 flush before each; returns the summed device milliseconds."""
+def run_window(solver, targets, first, K, stream, flush, timed=True):
+    """K frames from frame index `first`, one CUDA-event pair per frame on
+    the solver stream, with an untimed L2 flush (a 256 MiB write) before
+    each; returns the summed device milliseconds."""
     import torch
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
     for i in range(K):
         flush.zero_()
-        targets.apply(solver, first + i)
+        targets.apply(solver, first + i)    # input staging, before the timed step
         starts[i].record(stream)
         solver.step(1)
         ends[i].record(stream)
@@ -304,39 +351,76 @@ def timed_steps(solver, targets, first, K, stream, flush):
     return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
 
 
-def learned_comparison(args, world, dev, stream, flush, plain_value):
-    """The same workload with the learned warm start, at the iteration count
-    whose median AL residual matches the plain warm start's."""
-    from avbd_b200 import GPUSolver, abi, demos, learned
-    model = learned.WarmStartModel.load(model_path())
-    plain_iters = make_scene().settings.iterations
-    make = learned.SCENES[WORKLOAD_KEY]
-    k, r_plain, r_learned, acc = learned.matched_residual_iterations(make, 200, model, plain_iters, frames=120)
-    scene = make_scene()
-    scene.settings.iterations = k
-    solver = GPUSolver(scene, device=dev.index)
-    solver.set_stream(stream.cuda_stream)
-    solver.set_warm_start_model(model.params, model.norm, 1)
-    solver.set_warm_start_mode(abi.WARM_START_LEARNED)
-    targets = MotorTargets(1)
-    solver.step(args.warmup)
+def preroll(solver, targets, n):
+    for i in range(n):
+        targets.apply(solver, i)
+        solver.step(1)
     solver.synchronize()
-    ms = max_over_ranks(timed_steps(solver, targets, 0, args.steps, stream, flush), world, dev)
-    nv = dynamic_vertices(scene)
-    accepted = solver.counters().learn_accepted
-    solver.close()
-    value = world * nv * args.steps / (ms / 1e3)
-    return {"warm_start": "learned: 32-128-128-128-3 MLP, BF16 tensor-core inference, kept only when its "
-                          "residual after 1 trial sweep is no worse than the plain warm start's",
-            "iterations": k, "plain_iterations": plain_iters,
-            "matched_median_rel_residual": {"plain": r_plain, "learned": r_learned,
-                                            "definition": "r_final / r0(plain warm start), r = ||AL gradient||_2 "
-                                                          "over all dynamic DOFs, median over frames 3-120 of seed 200"},
-            "value": value, "unit": unit(), "ms_per_step": ms / args.steps,
-            "speedup_vs_plain": value / plain_value,
-            "accepted_frames": accepted / float(args.warmup + args.steps),
-            "model": f"avbd_b200/models/{MODELS[WORKLOAD_KEY]} (trained on the GPU by avbd_mlp_train_step "
-                     "from plain rollouts of held-out seeds at a higher iteration count)"}
+
+
+def learned_comparison(args, world, dev, stream, flush, plain_ms):
+    """Plain vs learned warm start at matched AL residual.  The matched level
+    is the plain warm start's median r_final / r0 at the configured iteration
+    count over frames 3-120 of a held-out seed; for each form the smallest
+    iteration count whose median reaches it is found, and the window is timed
+    with both.  The claim holds only if the learned count beats the smallest
+    plain count."""
+    import numpy as np
+    from avbd_b200 import GPUSolver, abi, learned
+    model = learned.WarmStartModel.load(model_path())
+    scene0 = make_scene()
+    plain_iters = scene0.settings.iterations
+    make = learned.SCENES[WORKLOAD_KEY]
+    cmp = learned.matched_comparison(make, 200, model, plain_iters, frames=120)
+
+    def timed(k, use_model):
+        scene = make_scene()
+        solver = GPUSolver(scene, device=dev.index)
+        solver.set_stream(stream.cuda_stream)
+        targets = MotorTargets(args.preroll + args.warmup + args.steps)
+        preroll(solver, targets, args.preroll)           # the plain trajectory up to the window
+        st = solver.settings
+        st.iterations = k
+        solver.settings = st
+        if use_model:
+            solver.set_warm_start_model(model.params, model.norm, 1)
+            solver.set_warm_start_mode(abi.WARM_START_LEARNED)
+        for i in range(args.warmup):
+            targets.apply(solver, args.preroll + i)
+            solver.step(1)
+        solver.synchronize()
+        acc0 = solver.counters().learn_accepted
+        ms = max_over_ranks(run_window(solver, targets, args.preroll + args.warmup, args.steps, stream, flush),
+                            world, dev)
+        accepted = solver.counters().learn_accepted - acc0
+        solver.close()
+        return ms, accepted
+
+    nv = dynamic_units(scene0)
+    k_plain = cmp["plain_min_iterations"]
+    ms_plain_min = plain_ms if k_plain == plain_iters else timed(k_plain, False)[0]
+    ms_learned, accepted = timed(cmp["learned_iterations"], True)
+    v_plain_min = world * nv * args.steps / (ms_plain_min / 1e3)
+    v_learned = world * nv * args.steps / (ms_learned / 1e3)
+    return {
+        "definition": "r = ||AL gradient||_2 over all dynamic DOFs; matched level = median over frames 3-120 of "
+                      "seed 200 of r_final / r0(plain warm start) at the configured iteration count",
+        "matched_level": cmp["target"],
+        "plain": {"iterations_configured": plain_iters, "smallest_iterations_reaching_level": k_plain,
+                  "median_rel_residual_by_iterations": cmp["plain_curve"],
+                  "value": v_plain_min, "ms_per_step": ms_plain_min / args.steps},
+        "learned": {"iterations": cmp["learned_iterations"], "median_rel_residual": cmp["learned_residual"],
+                    "value": v_learned, "ms_per_step": ms_learned / args.steps,
+                    "accepted_frames_in_timed_window": accepted / float(args.steps),
+                    "warm_start": "32-128-128-128-3 MLP, BF16 tensor-core inference; kept only when its residual "
+                                  "after 1 trial sweep is no worse than the plain warm start's"},
+        "speedup_vs_smallest_plain": v_learned / v_plain_min,
+        "iterations_to_tolerance_median": cmp["iterations_to_tolerance"],
+        "claim_holds": bool(cmp["learned_iterations"] < k_plain and v_learned > v_plain_min),
+        "unit": unit(),
+        "model": f"avbd_b200/models/{MODELS[WORKLOAD_KEY]} (trained on the GPU by avbd_mlp_train_step from the "
+                 "solver's own rollouts of other seeds at a higher iteration count)",
+    }
 
 
 def run_frames(args, local):
@@ -353,18 +437,15 @@ def run_frames(args, local):
         model = learned.WarmStartModel.load(model_path())
         solver.set_warm_start_model(model.params, model.norm, 1)
         solver.set_warm_start_mode(abi.WARM_START_LEARNED)
-    targets = MotorTargets(args.warmup + args.steps)
-    for i in range(args.warmup):
-        targets.apply(solver, i)
-        solver.step(1)
-    solver.synchronize()
+    targets = MotorTargets(args.preroll + args.warmup + args.steps)
+    preroll(solver, targets, args.preroll + args.warmup)
     t0 = time.perf_counter()
     for i in range(args.steps):
-        targets.apply(solver, args.warmup + i)
+        targets.apply(solver, args.preroll + args.warmup + i)
         solver.step(1)
     solver.synchronize()
     print(json.dumps({"workload": WORKLOAD_KEY, "frames": args.steps, "warm_start": args.warm_start,
-                      "iterations": scene.settings.iterations,
+                      "iterations": scene.settings.iterations, "preroll": args.preroll,
                       "wall_ms_per_frame": (time.perf_counter() - t0) / max(1, args.steps) * 1e3,
                       "runtime_failure": solver.runtime_failure()}), flush=True)
     solver.close()
@@ -415,21 +496,18 @@ def run_ours(args, world, rank, local):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     scene = make_scene(rank)
-    nv = dynamic_vertices(scene)
+    nv = dynamic_units(scene)
     solver = GPUSolver(scene, device=local)
-    targets = MotorTargets(args.steps + args.warmup + 400)
+    K, W = args.steps, args.warmup
+    first = args.preroll + W
+    targets = MotorTargets(first + K)
     stream = torch.cuda.Stream(device=dev)
     solver.set_stream(stream.cuda_stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)   # > 126 MB L2
 
     with torch.cuda.stream(stream):
-        for i in range(args.warmup):
-            targets.apply(solver, i)
-            solver.step(1)
-        solver.synchronize()
-        K = args.steps
-        starts = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
-        ends = [torch.cuda.Event(enable_timing=True) for _ in range(K)]
+        preroll(solver, targets, first)          # preroll + warm-up frames
+        window = solver.snapshot()               # the state at the first timed frame
         clocks = ClockSampler(local)
         if world > 1:
             import torch.distributed as dist
@@ -437,21 +515,15 @@ def run_ours(args, world, rank, local):
         torch.cuda.synchronize()
         clocks.start()
         time.sleep(0.2)
-        for i in range(K):
-            flush.zero_()
-            targets.apply(solver, args.warmup + i)    # input staging, before the timed step
-            starts[i].record(stream)
-            solver.step(1)
-            ends[i].record(stream)
-        torch.cuda.synchronize()
+        dev_ms = run_window(solver, targets, first, K, stream, flush)
         clock = clocks.stop()
         solver.synchronize()
-        dev_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
         dev_ms = max_over_ranks(dev_ms, world, dev)
         value = world * nv * K / (dev_ms / 1e3)
 
-        # e2e through the C ABI with host buffers
-        E = min(K, 300)
+        # e2e through the C ABI with host buffers: the same window, positions
+        # uploaded from pinned memory and read back every step
+        solver.restore(window)
         pos4 = torch.empty((len(scene.bodies), 4), dtype=torch.float32, pin_memory=True).numpy()
         xyz = torch.empty((len(scene.bodies), 3), dtype=torch.float32, pin_memory=True).numpy()
         solver.read_positions_into(pos4)
@@ -461,77 +533,79 @@ def run_ours(args, world, rank, local):
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for i in range(E):
+        for i in range(K):
             solver.set_positions(xyz)            # H2D: n x 12 B from pinned memory
-            targets.apply(solver, args.warmup + K + i)
+            targets.apply(solver, first + i)
             solver.step(1)
             solver.read_positions_into(pos4)     # D2H: n x 16 B, synchronising read
             xyz[:] = pos4[:, :3]
         e2e_s = max_over_ranks(time.perf_counter() - t0, world, dev)
-        h2d = int(xyz.nbytes) + (targets.t.shape[1] * 8 if targets.t is not None else 0)
-        e2e = {"value": world * nv * E / e2e_s, "unit": unit(),
-               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": int(pos4.nbytes),
-               "steps": E}
+        e2e = {"value": world * nv * K / e2e_s, "unit": unit(),
+               "h2d_bytes_per_step": int(xyz.nbytes) + targets.bytes_per_step(),
+               "d2h_bytes_per_step": int(pos4.nbytes), "steps": K}
 
-        # roofline of the dominant kernel (the per-color primal), from a
-        # profiled pass with CUDA events around every primal launch
-        prof_frames = 20
+        # the primal's share of the same window: replayed from the snapshot
+        # with stage timing, algorithmic bytes sampled on its frames
+        solver.restore(window)
         solver.set_profiling(True)
-        for i in range(prof_frames):
-            targets.apply(solver, i)
+        bytes_iter = []
+        for i in range(K):
+            flush.zero_()
+            targets.apply(solver, first + i)
             solver.step(1)
+            if i % max(1, K // 4) == 0:
+                solver.synchronize()
+                bytes_iter.append(primal_bytes_per_iteration(solver, scene))
         prof = solver.profile()
         solver.set_profiling(False)
-        bytes_iter = primal_bytes_per_iteration(solver, scene)
         counters = solver.counters()
-        launches_iter = max(1, prof["stage_launches"]["primal"] // (prof_frames * scene.settings.iterations))
-        bytes_launch = bytes_iter / launches_iter
-        avg_ms = prof["stage_ms"]["primal"] / max(1, prof["stage_launches"]["primal"])
-        peak, peak_kind = measured_peaks()
-        achieved = bytes_launch / (avg_ms / 1e3) / 1e9
         total_ms = sum(prof["stage_ms"].values())
         stage_share = {k: round(v / total_ms, 4) for k, v in prof["stage_ms"].items() if v > 0}
+        iters = scene.settings.iterations
+        primal_launches = max(1, prof["stage_launches"]["primal"])
+        launches_iter = max(1, primal_launches // (K * iters))
+        primal_ms_frame = stage_share.get("primal", 0.0) * dev_ms / K
+        avg_launch_ms = primal_ms_frame / max(1, primal_launches / K)
+        bytes_launch = float(np.mean(bytes_iter)) / launches_iter
+        peak, peak_kind = measured_peaks()
+        achieved = bytes_launch / (avg_launch_ms / 1e3) / 1e9 if avg_launch_ms > 0 else 0.0
         kernels_per_frame = prof["kernels_per_frame"]
 
     learned_line = None
-    if model_path() and os.path.exists(model_path()):
+    if not args.no_learned and model_path() and os.path.exists(model_path()):
         with torch.cuda.stream(stream):
-            learned_line = learned_comparison(args, world, dev, stream, flush, value)
+            learned_line = learned_comparison(args, world, dev, stream, flush, dev_ms)
 
     cpu = None
     if rank == 0 and world == 1:
-        thr = host_threads()
-        cv, frames, secs, _ = cpu_run(args.cpu_seconds, thr)
-        cpu = {"value": cv, "unit": unit(), "cores": thr, "kind": "port",
-               "sample": f"{WORKLOAD.split(':')[0]}, frames 2-{frames + 1} after a 1-frame warm-up, "
-                         f"{frames} frames in {secs:.1f} s, oracle with {thr} OpenMP threads"}
+        cv, frames, secs, kind, cores, sample = cpu_window(args, args.cpu_seconds, W, host_threads())
+        cpu = {"value": cv, "unit": unit(), "cores": cores, "kind": kind, "sample": sample}
     if rank == 0:
+        cfg = config(scene, args, world)
+        cfg.update({"l2": "flushed between timed steps (256 MiB device write, untimed)",
+                    "timing": "CUDA events on the solver stream per step, max over ranks",
+                    "colors": int(counters.used_colors),
+                    "lanes_per_body": prof["color_lanes"][:int(counters.used_colors)]})
         line = {
             "metric": METRIC, "value": value, "unit": unit(), "n_gpus": world,
-            "steps": K, "warmup": args.warmup, "ms_per_step": dev_ms / K,
+            "steps": K, "warmup": W, "ms_per_step": dev_ms / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded SplitMix64 scene)",
-            "config": {"workload": WORKLOAD, "vertices_per_step": nv, "tets": len(scene.tets),
-                       "triangles": len(scene.tris),
-                       "iterations": scene.settings.iterations,
-                       "colors": int(counters.used_colors),
-                       "lanes_per_body": prof["color_lanes"][:int(counters.used_colors)],
-                       "lane_autotune": "fastest of 8/16/32 lanes per color, timed on the first 3 frames",
-                       "warm_start": "plain gamma warm start (value); learned warm start in learned_warm_start",
-                       "parallelism": (f"world shards x{world}" if WORKLOAD_KEY == "batched-worlds"
-                                       else f"replicas x{world}"),
-                       "l2": "flushed between timed steps (256 MiB device write, untimed)",
-                       "timing": "CUDA events on the solver stream per step, max over ranks"},
+            "config": cfg,
             "clocks": clock, "e2e": e2e,
             "gpu_launches": int(kernels_per_frame * K),
-            "roofline": {"bound": "hbm", "kernel": "k_primal_group (per-color block-descent primal, 8/16/32 lanes per body)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "per-color block-descent primal (k_primal_group / k_primal / k_solve_small)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_source": f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
-                         else "fallback 6.65 TB/s",
-                         "traffic": ncu_traffic_per_launch(),
+                         "peak_source": (f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
+                                         else "fallback 6.65 TB/s"),
+                         "traffic": None,
+                         "traffic_note": "DRAM bytes per launch from ncu are in profiles/ (captured on the same "
+                                         "kernel); not measured inside this run",
                          "algorithmic_bytes_per_launch": bytes_launch,
-                         "avg_launch_us": avg_ms * 1e3, "launches_per_iteration": launches_iter,
-                         "measured": f"profiled pass of {prof_frames} frames, CUDA events around every launch"},
+                         "avg_launch_us": avg_launch_ms * 1e3, "launches_per_iteration": launches_iter,
+                         "measured": "the timed window replayed from a snapshot with stage timing: primal share "
+                                     "x timed ms per step / primal launches per step"},
             "stage_share": stage_share,
             "learned_warm_start": learned_line,
             "cpu_baseline": cpu,
@@ -541,41 +615,22 @@ def run_ours(args, world, rank, local):
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the reference's algorithm on the box's host cores
+    over the same window (preroll, warm-up, timed frames) and config."""
     if rank != 0:
         return
     thr = host_threads()
-    budget = max(10.0, min(150.0, 8.0 * args.cpu_seconds))
-    import oracle
-    oracle.build()
+    budget = max(10.0, min(240.0, 20.0 * args.cpu_seconds))
+    value, frames, secs, kind, cores, sample = cpu_window(args, budget, args.warmup, thr)
     scene = make_scene()
-    nv = dynamic_vertices(scene)
-    o = oracle.OracleSolver(scene, threads=thr)
-    targets = MotorTargets(args.steps + 3)
-    for i in range(min(args.warmup, 3)):
-        targets.apply(o, i)
-        o.step(1)
-    frames, t0 = 0, time.perf_counter()
-    while frames < args.steps:
-        targets.apply(o, 3 + frames)
-        o.step(1)
-        frames += 1
-        if time.perf_counter() - t0 >= budget:
-            break
-    secs = time.perf_counter() - t0
-    value = nv * frames / secs
-    sample = (f"{WORKLOAD.split(':')[0]}, {frames} of {args.steps} requested frames after "
-              f"{min(args.warmup, 3)} warm-up frames, bounded to {budget:.0f} s; the reference's "
-              "solver restated in C++ (Swift/Metal cannot run here), OpenMP over bodies of a color")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": unit(),
-        "n_gpus": world, "steps": frames, "warmup": min(args.warmup, 3),
+        "n_gpus": world, "steps": frames, "warmup": args.warmup,
         "ms_per_step": secs / frames * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64 scene)",
-        "config": {"workload": WORKLOAD, "vertices_per_step": nv, "parallelism": "host cores"},
-        "cpu_baseline": {"value": value, "unit": unit(), "cores": thr, "kind": "port",
-                         "sample": sample},
-        "e2e": {"value": value, "unit": unit(), "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
+        "config": config(scene, args, world),
+        "cpu_baseline": {"value": value, "unit": unit(), "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": unit(), "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
