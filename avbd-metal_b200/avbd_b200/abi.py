@@ -196,7 +196,8 @@ EXPORTED = [
     "avbd_set_residual_trace", "avbd_get_residual_trace", "avbd_mlp_param_count",
     "avbd_mlp_workspace_bytes", "avbd_mlp_gradients", "avbd_mlp_train_step", "avbd_mlp_infer",
     "avbd_build_instances", "avbd_soft_normals", "avbd_set_skin_bindings", "avbd_skin_deform",
-    "avbd_render_pusht_obs",
+    "avbd_render_pusht_obs", "avbd_create_batched", "avbd_get_world_offsets", "avbd_set_world_body_states",
+    "avbd_reset_worlds", "avbd_get_world_motor_joints",
 ]
 WARM_START_PLAIN, WARM_START_LEARNED = 0, 1
 
@@ -208,4 +209,6 @@ class Profile(C.Structure):
     _fields_ = [("frames", C.c_uint64), ("kernels_per_frame", C.c_uint64),
                 ("stage_ms", C.c_double * 16),
                 ("stage_launches", C.c_uint64 * 16),
-                ("color_lanes", C.c_uint32 * 64)]
+                ("color_lanes", C.c_uint32 * 64),
+                ("dyn_blocks", C.c_uint32), ("dyn_threads", C.c_uint32),
+                ("dyn_bucket", C.c_uint32), ("dyn_candidates", C.c_uint32)]

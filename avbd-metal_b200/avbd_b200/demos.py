@@ -280,7 +280,8 @@ def cloth_sphere_scene(seed: int = 3, n: int = 256, iterations: int = 30,
     return s
 
 
-def batched_worlds_scene(worlds: int = 4096, seed: int = 4, pitch: float = 1.6, first_world: int = 0):
+def batched_worlds_scene(worlds: int = 4096, seed: int = 4, pitch: float = 1.6, first_world: int = 0,
+                         collision_groups: bool = True):
     """Batched articulated worlds packed into one scene, one collision group
     per world (the reference's vector-environment layout,
     RL/PushTEnv.swift:114-180): each world is a planar serial chain of 3-7
@@ -293,7 +294,9 @@ def batched_worlds_scene(worlds: int = 4096, seed: int = 4, pitch: float = 1.6, 
 
     World w draws from its own stream SplitMix64((seed << 32) + w), so a shard
     [first_world, first_world + worlds) builds exactly the worlds that a
-    single scene of all worlds would contain."""
+    single scene of all worlds would contain.  collision_groups=False leaves
+    every collider in group 0, for avbd_create_batched to assign the groups
+    from the world offsets."""
     s = PhysicsScene("batched-worlds")
     cols = int(math.ceil(math.sqrt(worlds)))
     rows = int(math.ceil(worlds / cols))
@@ -303,7 +306,7 @@ def batched_worlds_scene(worlds: int = 4096, seed: int = 4, pitch: float = 1.6, 
     link = (0.25, 0.06, 0.06)
     for e in range(worlds):
         rng = SplitMix64((seed << 32) + first_world + e)
-        g = e + 1
+        g = e + 1 if collision_groups else 0
         cx, cy = (e % cols) * pitch - hx, (e // cols) * pitch - hy
         offsets.append(len(s.bodies))
         n = 3 + int(rng.next_float() * 5)

@@ -88,6 +88,11 @@ def load_library() -> C.CDLL:
         "avbd_set_learning_capture": ([vp, i32], i32),
         "avbd_set_residual_trace": ([vp, i32], i32),
         "avbd_get_residual_trace": ([vp, vp, u32], i32),
+        "avbd_create_batched": ([vp, vp, u32, C.POINTER(vp)], i32),
+        "avbd_get_world_offsets": ([vp, C.POINTER(u32), vp], i32),
+        "avbd_set_world_body_states": ([vp, u32, vp, u32, vp], i32),
+        "avbd_reset_worlds": ([vp, vp, u32], i32),
+        "avbd_get_world_motor_joints": ([vp, u32, vp, u32, C.POINTER(u32)], i32),
         "avbd_mlp_param_count": ([], u32),
         "avbd_mlp_workspace_bytes": ([u32], sz),
         "avbd_mlp_gradients": ([vp, vp, vp, vp, u32, vp, vp, vp, vp], i32),
@@ -112,14 +117,22 @@ class GPUSolver:
     """AVBD solver step on one CUDA device (GPUSolver.swift:17)."""
 
     def __init__(self, scene: PhysicsScene, max_pairs_per_body: int = 16, device: int = -1,
-                 truncation: int = abi.TRUNCATION_AUTOMATIC, tet_inversion_prevention: bool = False):
+                 truncation: int = abi.TRUNCATION_AUTOMATIC, tet_inversion_prevention: bool = False,
+                 world_offsets=None):
+        """world_offsets: batched worlds (avbd_create_batched) — world w owns
+        bodies [world_offsets[w], world_offsets[w + 1]); each world gets its
+        own collision group, bodies outside every world are shared."""
         lib = load_library()
         desc, self._keep = scene.to_desc(max_pairs_per_body=max_pairs_per_body,
                                          truncation=truncation,
                                          tet_inversion_prevention=tet_inversion_prevention,
                                          device=device)
         h = C.c_void_p()
-        rc = lib.avbd_create(C.byref(desc), C.byref(h))
+        if world_offsets is None:
+            rc = lib.avbd_create(C.byref(desc), C.byref(h))
+        else:
+            offs = np.ascontiguousarray(world_offsets, dtype=np.uint32)
+            rc = lib.avbd_create_batched(C.byref(desc), offs.ctypes.data, max(0, len(offs) - 1), C.byref(h))
         if rc != abi.OK:
             raise AVBDError(rc, _last_error(None))
         self._h = h
@@ -290,6 +303,33 @@ class GPUSolver:
         return a, v
 
     # -- diagnostics -----------------------------------------------------------
+    # -- batched worlds (vector environments) ---------------------------------
+    def world_offsets(self) -> np.ndarray:
+        n = C.c_uint32()
+        self._check(load_library().avbd_get_world_offsets(self._h, C.byref(n), None))
+        out = np.zeros(n.value + 1 if n.value else 0, np.uint32)
+        if n.value:
+            self._check(load_library().avbd_get_world_offsets(self._h, C.byref(n), out.ctypes.data))
+        return out
+
+    def set_world_body_states(self, world: int, local_ids, states):
+        ids = np.ascontiguousarray(local_ids, dtype=np.uint32)
+        arr = (abi.BodyState * len(states))(*states)
+        self._check(load_library().avbd_set_world_body_states(self._h, world, ids.ctypes.data, len(ids), arr))
+
+    def reset_worlds(self, worlds):
+        w = np.ascontiguousarray(worlds, dtype=np.uint32)
+        self._check(load_library().avbd_reset_worlds(self._h, w.ctypes.data, len(w)))
+
+    def world_motor_joints(self, world: int) -> np.ndarray:
+        n = C.c_uint32()
+        self._check(load_library().avbd_get_world_motor_joints(self._h, world, None, 0, C.byref(n)))
+        out = np.zeros(n.value, np.uint32)
+        if n.value:
+            self._check(load_library().avbd_get_world_motor_joints(self._h, world, out.ctypes.data, n.value,
+                                                                   C.byref(n)))
+        return out
+
     def max_constraint_error(self) -> float:
         v = C.c_float()
         self._check(load_library().avbd_max_constraint_error(self._h, C.byref(v)))
@@ -335,7 +375,9 @@ class GPUSolver:
         return {"frames": p.frames, "kernels_per_frame": p.kernels_per_frame,
                 "stage_ms": {n: p.stage_ms[i] for i, n in enumerate(abi.STAGES)},
                 "stage_launches": {n: p.stage_launches[i] for i, n in enumerate(abi.STAGES)},
-                "color_lanes": list(p.color_lanes)}
+                "color_lanes": list(p.color_lanes),
+                "dynamic_primal_shape": {"blocks": p.dyn_blocks, "threads": p.dyn_threads,
+                                         "body_count_bucket": p.dyn_bucket, "candidates_timed": p.dyn_candidates}}
 
     # ---- learned warm start ------------------------------------------------
     def set_warm_start_model(self, params, norm, trial_sweeps: int = 1) -> None:

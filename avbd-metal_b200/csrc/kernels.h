@@ -143,6 +143,9 @@ struct Sizes {
     // static palette on the host (null with dynamic coloring)
     const uint32_t* colorCounts;
     const uint32_t* colorLanes;
+    // dynamic coloring: block shape of the rigid primal's grid-stride launch
+    // (blocks, threads per block), chosen by the runtime's autotuner
+    uint32_t dynBlocks, dynThreads;
 };
 
 // exclusive scan of n words (n <= 1024 * 1024); out may not alias in

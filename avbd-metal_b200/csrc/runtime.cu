@@ -12,6 +12,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -133,6 +134,12 @@ struct avbd_solver {
     // are re-captured) when a retired frame used more colors.
     uint32_t colorLaunchBound = 8;
     bool colorBoundFitted = false;
+    // batched worlds (avbd_create_batched): ragged body ranges, the bodies'
+    // and motors' state at creation, the motorized joints of every world
+    std::vector<uint32_t> worldOffsets;
+    std::vector<avbd_body_state> initialStates;
+    std::vector<float> initialMotorTargets;
+    std::vector<std::vector<uint32_t>> worldMotors;
     // learned warm start
     static constexpr uint32_t kTraceLength = 2 + 256;
     int learnMode = AVBD_WARM_START_PLAIN;
@@ -717,6 +724,7 @@ struct avbd_solver {
         // Small scenes run their whole iteration loop in one thread block.
         update_small_solve();
         tuneStage = tuning_applies() ? 0 : -1;
+        dyn_tune_setup();
         if (cudaDeviceSynchronize() != cudaSuccess) { error = "device error during upload"; return AVBD_ERR_NO_DEVICE; }
         return AVBD_OK;
     }
@@ -812,11 +820,89 @@ struct avbd_solver {
         return AVBD_OK;
     }
 
+    // Block-shape autotuner of the dynamic-coloring primal (rigid scenes,
+    // batched worlds).  Its grid-stride launch gives every body to one 8-lane
+    // group whatever the grid, so each candidate computes the same floats;
+    // only speed differs, and that depends on how many bodies a color holds.
+    // The first solver of a body-count bucket (floor(log2(dynamic bodies)))
+    // on a device times one eager frame per candidate, with events around
+    // every primal launch, and keeps the fastest; later solvers of the
+    // bucket reuse it.
+    struct DynShape { uint32_t blocksPerSM, threads; };
+    static constexpr DynShape kDynShapes[7] = {{1, 128}, {2, 128}, {3, 128}, {4, 128}, {4, 64}, {6, 64}, {8, 64}};
+    int dynTuneStage = -1;
+    double dynTuneMs[7] = {};
+    uint32_t dynBucket = 0, dynCandidates = 0;
+    static std::mutex& dyn_cache_mutex() { static std::mutex m; return m; }
+    static std::map<std::pair<int, uint32_t>, std::pair<uint32_t, uint32_t>>& dyn_cache() {
+        static std::map<std::pair<int, uint32_t>, std::pair<uint32_t, uint32_t>> c;
+        return c;
+    }
+    void dyn_tune_setup() {
+        z.dynBlocks = 148u * 4u;
+        z.dynThreads = 128u;
+        if (!z.dynamicColoring || smallSolve || z.numDynamicBodies == 0) return;
+        uint32_t b = 0;
+        while ((2u << b) <= z.numDynamicBodies) b++;
+        dynBucket = b;
+        std::lock_guard<std::mutex> lock(dyn_cache_mutex());
+        auto it = dyn_cache().find({device, b});
+        if (it != dyn_cache().end()) {
+            z.dynBlocks = it->second.first;
+            z.dynThreads = it->second.second;
+            return;
+        }
+        dynTuneStage = 0;
+    }
+    int dyn_tune_frame() {
+        const DynShape sh = kDynShapes[dynTuneStage];
+        z.dynBlocks = 148u * sh.blocksPerSM;
+        z.dynThreads = sh.threads;
+        const size_t need = 2 * (size_t)P.iterations * (colorLaunchBound + 1);
+        while (tuneEvents.size() < need) {
+            cudaEvent_t e;
+            if (!check(cudaEventCreate(&e), "event create")) return AVBD_ERR_RUNTIME_FAILURE;
+            tuneEvents.push_back(e);
+        }
+        const uint32_t launches = P.iterations * colorLaunchBound;
+        encode_frame_on((int)(frame & 1), launch, nullptr, tuneEvents.data());
+        if (!check(cudaGetLastError(), "tuning frame")) return AVBD_ERR_RUNTIME_FAILURE;
+        frame++;
+        if (!check(cudaStreamSynchronize(launch), "tuning frame")) return AVBD_ERR_RUNTIME_FAILURE;
+        double total = 0.0;
+        for (uint32_t k = 0; k < launches; k++) {
+            float ms = 0.0f;
+            if (!check(cudaEventElapsedTime(&ms, tuneEvents[2 * k], tuneEvents[2 * k + 1]), "tuning timing"))
+                return AVBD_ERR_RUNTIME_FAILURE;
+            total += ms;
+        }
+        dynTuneMs[dynTuneStage] = total;
+        if (++dynTuneStage == 7) {
+            int best = 3;   // the untuned default wins ties
+            for (int k = 0; k < 7; k++) if (dynTuneMs[k] < dynTuneMs[best]) best = k;
+            z.dynBlocks = 148u * kDynShapes[best].blocksPerSM;
+            z.dynThreads = kDynShapes[best].threads;
+            dynCandidates = 7;
+            {
+                std::lock_guard<std::mutex> lock(dyn_cache_mutex());
+                dyn_cache()[{device, dynBucket}] = {z.dynBlocks, z.dynThreads};
+            }
+            dynTuneStage = -1;
+            graphsValid = false;
+        }
+        return AVBD_OK;
+    }
+
     int step(uint32_t frames) {
         if (failure != AVBD_FAIL_NONE) return AVBD_ERR_RUNTIME_FAILURE;
         uint32_t f = 0;
         while (tuneStage >= 0 && f < frames) {
             int rc = tune_frame();
+            if (rc != AVBD_OK) return rc;
+            f++;
+        }
+        while (dynTuneStage >= 0 && f < frames) {
+            int rc = dyn_tune_frame();
             if (rc != AVBD_OK) return rc;
             f++;
         }
@@ -877,6 +963,137 @@ int avbd_create(const avbd_scene_desc* scene, avbd_solver** out) {
     }
     g_last_error.clear();
     *out = s;
+    return AVBD_OK;
+}
+
+// Batched worlds (vector environments): ragged body ranges packed in one
+// scene, one collision group per world (RL/PushTEnv.swift:137-180).
+int avbd_create_batched(const avbd_scene_desc* scene, const uint32_t* world_offsets, uint32_t num_worlds,
+                        avbd_solver** out) {
+    if (!out) return AVBD_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    auto fail = [](const char* msg) { g_last_error = msg; return AVBD_ERR_INVALID_ARGUMENT; };
+    if (!scene || (num_worlds && !world_offsets)) return fail("avbd_create_batched: null scene or offsets");
+    const uint32_t nb = scene->num_bodies;
+    for (uint32_t w = 0; w < num_worlds; w++)
+        if (world_offsets[w] > world_offsets[w + 1]) return fail("avbd_create_batched: world offsets must not decrease");
+    if (num_worlds && world_offsets[num_worlds] > nb) return fail("avbd_create_batched: world offsets beyond the bodies");
+    // world of every body (0xFFFFFFFF = shared)
+    std::vector<uint32_t> worldOf(nb, 0xFFFFFFFFu);
+    for (uint32_t w = 0; w < num_worlds; w++)
+        for (uint32_t b = world_offsets[w]; b < world_offsets[w + 1]; b++) worldOf[b] = w;
+    auto world_of = [&](int32_t b) { return (b < 0 || (uint32_t)b >= nb) ? 0xFFFFFFFFu : worldOf[b]; };
+    auto joins_two = [&](const int32_t* ids, int n) {
+        uint32_t seen = 0xFFFFFFFFu;
+        for (int k = 0; k < n; k++) {
+            const uint32_t w = world_of(ids[k]);
+            if (w == 0xFFFFFFFFu) continue;
+            if (seen != 0xFFFFFFFFu && seen != w) return true;
+            seen = w;
+        }
+        return false;
+    };
+    for (uint32_t i = 0; i < scene->num_joints; i++) {
+        const int32_t ids[2] = {scene->joints[i].body_a, scene->joints[i].body_b};
+        if (joins_two(ids, 2)) return fail("avbd_create_batched: a joint joins two worlds");
+    }
+    for (uint32_t i = 0; i < scene->num_springs; i++) {
+        const int32_t ids[2] = {scene->springs[i].body_a, scene->springs[i].body_b};
+        if (joins_two(ids, 2)) return fail("avbd_create_batched: a spring joins two worlds");
+    }
+    for (uint32_t i = 0; i < scene->num_tets; i++)
+        if (joins_two(scene->tets[i].ids, 4)) return fail("avbd_create_batched: a tet joins two worlds");
+    for (uint32_t i = 0; i < scene->num_tris; i++)
+        if (joins_two(scene->tris[i].ids, 3)) return fail("avbd_create_batched: a triangle joins two worlds");
+    for (uint32_t i = 0; i < scene->num_exclusions; i++) {
+        const int32_t ids[2] = {scene->exclusions[i].body_a, scene->exclusions[i].body_b};
+        if (joins_two(ids, 2)) return fail("avbd_create_batched: an exclusion joins two worlds");
+    }
+    std::vector<avbd_collider_desc> cols(scene->colliders, scene->colliders + scene->num_colliders);
+    for (avbd_collider_desc& c : cols) {
+        const uint32_t w = world_of(c.body);
+        c.collision_group = w == 0xFFFFFFFFu ? 0u : w + 1u;
+    }
+    avbd_scene_desc desc = *scene;
+    desc.colliders = cols.data();
+    avbd_solver* s = nullptr;
+    int rc = avbd_create(&desc, &s);
+    if (rc != AVBD_OK) return rc;
+    s->worldOffsets.assign(world_offsets, world_offsets + num_worlds + (num_worlds ? 1 : 0));
+    s->initialStates.resize(nb);
+    for (uint32_t b = 0; b < nb; b++) {
+        const avbd_body_desc& bd = scene->bodies[b];
+        avbd_body_state& st = s->initialStates[b];
+        std::memcpy(st.position, bd.position, sizeof st.position);
+        std::memcpy(st.rotation, bd.rotation, sizeof st.rotation);
+        std::memcpy(st.velocity, bd.velocity, sizeof st.velocity);
+        st.angular_velocity[0] = st.angular_velocity[1] = st.angular_velocity[2] = 0.0f;
+    }
+    s->worldMotors.assign(num_worlds, {});
+    s->initialMotorTargets.resize(s->H.joints.size());
+    for (uint32_t j = 0; j < s->H.joints.size(); j++) {
+        s->initialMotorTargets[j] = s->H.joints[j].motor.x;
+        if ((s->H.joints[j].header.w & MOTOR_MODE_MASK) == 0u) continue;
+        const uint32_t w = world_of((int32_t)s->H.joints[j].header.y);
+        if (w != 0xFFFFFFFFu) s->worldMotors[w].push_back(j);
+    }
+    *out = s;
+    return AVBD_OK;
+}
+
+int avbd_get_world_offsets(avbd_solver* s, uint32_t* num_worlds, uint32_t* offsets) {
+    if (!s || !num_worlds) return AVBD_ERR_INVALID_ARGUMENT;
+    *num_worlds = s->worldOffsets.empty() ? 0u : (uint32_t)s->worldOffsets.size() - 1u;
+    if (offsets) std::copy(s->worldOffsets.begin(), s->worldOffsets.end(), offsets);
+    return AVBD_OK;
+}
+
+int avbd_set_world_body_states(avbd_solver* s, uint32_t world, const uint32_t* local_ids, uint32_t n,
+                               const avbd_body_state* states) {
+    const uint32_t nw = !s || s->worldOffsets.empty() ? 0u : (uint32_t)s->worldOffsets.size() - 1u;
+    if (!s || world >= nw || (n && (!local_ids || !states))) return AVBD_ERR_INVALID_ARGUMENT;
+    const uint32_t first = s->worldOffsets[world], size = s->worldOffsets[world + 1] - first;
+    std::vector<uint32_t> ids(n);
+    for (uint32_t i = 0; i < n; i++) {
+        if (local_ids[i] >= size) return AVBD_ERR_INVALID_ARGUMENT;
+        ids[i] = first + local_ids[i];
+    }
+    return avbd_set_body_states(s, ids.data(), n, states);
+}
+
+int avbd_reset_worlds(avbd_solver* s, const uint32_t* worlds, uint32_t n) {
+    if (!s || (n && !worlds)) return AVBD_ERR_INVALID_ARGUMENT;
+    const uint32_t nw = s->worldOffsets.empty() ? 0u : (uint32_t)s->worldOffsets.size() - 1u;
+    std::vector<uint32_t> ids, motors, velMotors;
+    std::vector<avbd_body_state> states;
+    std::vector<float> targets, velTargets;
+    for (uint32_t i = 0; i < n; i++) {
+        const uint32_t w = worlds[i];
+        if (w >= nw) return AVBD_ERR_INVALID_ARGUMENT;
+        for (uint32_t b = s->worldOffsets[w]; b < s->worldOffsets[w + 1]; b++) {
+            ids.push_back(b);
+            states.push_back(s->initialStates[b]);
+        }
+        for (uint32_t j : s->worldMotors[w]) {
+            const bool velocity = (s->H.joints[j].header.w & MOTOR_MODE_MASK) == MOTOR_VELOCITY;
+            (velocity ? velMotors : motors).push_back(j);
+            (velocity ? velTargets : targets).push_back(s->initialMotorTargets[j]);
+        }
+    }
+    if (ids.empty()) return AVBD_OK;
+    int rc = avbd_set_body_states(s, ids.data(), (uint32_t)ids.size(), states.data());
+    if (rc != AVBD_OK) return rc;
+    if (!motors.empty()) rc = avbd_set_motor_targets(s, motors.data(), (uint32_t)motors.size(), targets.data());
+    if (rc == AVBD_OK && !velMotors.empty())
+        rc = avbd_set_motor_velocities(s, velMotors.data(), (uint32_t)velMotors.size(), velTargets.data());
+    return rc;
+}
+
+int avbd_get_world_motor_joints(avbd_solver* s, uint32_t world, uint32_t* ids, uint32_t cap, uint32_t* count) {
+    if (!s || !count || world >= s->worldMotors.size() || (cap && !ids)) return AVBD_ERR_INVALID_ARGUMENT;
+    const std::vector<uint32_t>& m = s->worldMotors[world];
+    *count = (uint32_t)m.size();
+    for (uint32_t i = 0; i < cap && i < m.size(); i++) ids[i] = m[i];
     return AVBD_OK;
 }
 
@@ -1477,6 +1694,10 @@ int avbd_get_profile(avbd_solver* s, avbd_profile* out) {
     *out = s->prof;
     out->kernels_per_frame = s->kernelsPerFrame;
     for (int c = 0; c < 64; c++) out->color_lanes[c] = s->H.colorLanes[c];
+    out->dyn_blocks = s->z.dynamicColoring ? s->z.dynBlocks : 0u;
+    out->dyn_threads = s->z.dynamicColoring ? s->z.dynThreads : 0u;
+    out->dyn_bucket = s->dynBucket;
+    out->dyn_candidates = s->dynCandidates;
     return AVBD_OK;
 }
 

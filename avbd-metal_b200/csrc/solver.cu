@@ -1415,8 +1415,9 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
         // one resident wave (4 blocks per SM at 128 registers) strides over
         // it instead of a grid sized for every dynamic body (batched worlds
         // 1.007 -> 0.965 ms per frame; half a wave measured 1.22 ms)
-        const uint32_t need = (upper * 8 + T - 1) / T, wave = 148u * 4u;
-        k_primal<<<need < wave ? need : wave, T, 0, st>>>(P, d, color, count);
+        const uint32_t TT = z.dynThreads ? z.dynThreads : (uint32_t)T;
+        const uint32_t need = (upper * 8 + TT - 1) / TT, wave = z.dynBlocks ? z.dynBlocks : 148u * 4u;
+        k_primal<<<need < wave ? need : wave, TT, 0, st>>>(P, d, color, count);
     } else {
         // the grouped kernel needs the color's body count on the host
         const uint32_t lanes_ = lanes < 8 ? 8 : (lanes > 32 ? 32 : lanes);

@@ -375,6 +375,14 @@ typedef struct avbd_profile {
     uint64_t stage_launches[16];  /* kernel launches per stage              */
     uint32_t color_lanes[64];     /* lanes per body of each static color's
                                    * primal, as chosen by the autotuner      */
+    /* dynamic coloring: block shape of the rigid primal's grid-stride
+     * launch, chosen per body-count bucket (floor(log2(dynamic bodies)))
+     * by timing candidate shapes on the first frames of the first solver
+     * of that bucket on the device; later solvers reuse the choice          */
+    uint32_t dyn_blocks;
+    uint32_t dyn_threads;
+    uint32_t dyn_bucket;
+    uint32_t dyn_candidates;      /* shapes timed (0: taken from the cache)  */
 } avbd_profile;
 int avbd_set_profiling(avbd_solver* solver, int enabled);
 int avbd_get_profile(avbd_solver* solver, avbd_profile* out);
@@ -454,6 +462,38 @@ enum {
 };
 size_t avbd_debug_buffer_size(avbd_solver* solver, int which);
 int avbd_debug_read(avbd_solver* solver, int which, void* dst, size_t bytes);
+
+/* ---- Batched worlds (vector environments) -------------------------------
+ * The reference batches environments by packing N replicas into one scene,
+ * one collision group per environment (RL/PushTEnv.swift:137-180), and
+ * resets them through setBodyStates (GPUSolver.swift:2409-2473).  These entry
+ * points make that layout explicit with ragged world offsets.
+ *
+ * avbd_create_batched: `scene` packs `num_worlds` worlds of uneven size;
+ * world w owns bodies [world_offsets[w], world_offsets[w + 1]) (num_worlds + 1
+ * non-decreasing offsets); bodies outside every world are shared (static
+ * ground, fixtures).  Every collider of world w's bodies is put in collision
+ * group w + 1 (whatever the description says), shared colliders in group 0,
+ * so worlds never touch one another and all meet the shared bodies.  A
+ * joint, spring, tet, triangle or exclusion that joins two different worlds
+ * is refused (AVBD_ERR_INVALID_ARGUMENT).  Otherwise as avbd_create.       */
+int avbd_create_batched(const avbd_scene_desc* scene, const uint32_t* world_offsets, uint32_t num_worlds,
+                        avbd_solver** out);
+/* Number of worlds (0 for a solver from avbd_create) and, when `offsets` is
+ * non-null, its num_worlds + 1 offsets.                                    */
+int avbd_get_world_offsets(avbd_solver* solver, uint32_t* num_worlds, uint32_t* offsets);
+/* setBodyStates for bodies addressed inside one world (local index 0 = the
+ * world's first body), with its AL-reset of incident constraints.          */
+int avbd_set_world_body_states(avbd_solver* solver, uint32_t world, const uint32_t* local_ids, uint32_t n,
+                               const avbd_body_state* states);
+/* Put each listed world back to its state at creation: body poses and
+ * velocities, motor targets, and the AL state of every joint, spring and
+ * contact touching its bodies (reset as setBodyStates does).              */
+int avbd_reset_worlds(avbd_solver* solver, const uint32_t* worlds, uint32_t n);
+/* The motorized joints of one world, in joint order: up to `cap` ids in
+ * `ids`, their number in *count.                                           */
+int avbd_get_world_motor_joints(avbd_solver* solver, uint32_t world, uint32_t* ids, uint32_t cap,
+                                uint32_t* count);
 
 /* Allocation-free exclusive prefix sum of `n` uint32 words on the current
  * device: d_out[i] = d_in[0] + ... + d_in[i-1] (the scan the solver uses for

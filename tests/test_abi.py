@@ -80,3 +80,23 @@ def test_null_arguments_are_rejected(lib):
     assert lib.avbd_create(None, None) == abi.ERR_INVALID_ARGUMENT
     assert lib.avbd_step(None, 1) == abi.ERR_INVALID_ARGUMENT
     assert lib.avbd_sync(None) == abi.ERR_INVALID_ARGUMENT
+
+
+def test_batched_create_refuses_a_joint_between_worlds(lib):
+    """avbd_create_batched validates the world partition before touching a
+    device: a joint joining two worlds is an invalid argument."""
+    from avbd_b200.scene import SceneJoint
+    s, motors, offs = demos.batched_worlds_scene(worlds=3, seed=1, collision_groups=False)
+    a, b = offs[0], offs[1]
+    s.add_joint(SceneJoint(a, b, (0, 0, 0), (0, 0, 0)))
+    with pytest.raises(AVBDError) as e:
+        GPUSolver(s, world_offsets=list(offs) + [len(s.bodies)])
+    assert e.value.status == abi.ERR_INVALID_ARGUMENT
+    assert "joins two worlds" in str(e.value)
+
+
+def test_batched_create_refuses_decreasing_offsets(lib):
+    s, motors, offs = demos.batched_worlds_scene(worlds=3, seed=1, collision_groups=False)
+    with pytest.raises(AVBDError) as e:
+        GPUSolver(s, world_offsets=[offs[1], offs[0], len(s.bodies)])
+    assert e.value.status == abi.ERR_INVALID_ARGUMENT

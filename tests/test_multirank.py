@@ -36,7 +36,7 @@ def _shard_digest(rank, worlds=WORLDS, frames=FRAMES):
         assert o.step(1) == 0
     pos, rot = o.positions()
     h = hashlib.sha256(pos.tobytes() + rot.tobytes()).hexdigest()
-    return h, len(scene.bodies), bench.dynamic_vertices(scene)
+    return h, len(scene.bodies), bench.dynamic_units(scene)
 
 
 def _rank_main(rank, world, port, out):
@@ -75,3 +75,18 @@ def test_two_gloo_ranks_shard_worlds():
     assert gathered[0][0] != gathered[1][0]
     # whole-job units = sum over ranks (weak scaling)
     assert gathered[0][2] + gathered[1][2] == sum(g[2] for g in gathered)
+
+
+def test_default_workload_under_torchrun_is_world_shards(monkeypatch):
+    """bench.py --gpus N under torchrun (WORLD_SIZE > 1) measures the natural
+    split — batched-world shards — unless a workload is named; one GPU
+    defaults to the mixed scene."""
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--gpus", "2"])
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    assert bench.parse().workload == "batched-worlds"
+    monkeypatch.setenv("WORLD_SIZE", "1")
+    monkeypatch.setattr(sys, "argv", ["bench.py"])
+    assert bench.parse().workload == "mixed"
