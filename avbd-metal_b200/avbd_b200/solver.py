@@ -98,6 +98,7 @@ def load_library() -> C.CDLL:
         "avbd_mlp_gradients": ([vp, vp, vp, vp, u32, vp, vp, vp, vp], i32),
         "avbd_mlp_train_step": ([vp, vp, vp, vp, u32, vp, vp, u32, C.c_float, vp, vp, vp], i32),
         "avbd_mlp_infer": ([vp, vp, vp, u32, vp, vp, vp], i32),
+        "avbd_mlp_infer_wait_timeout_for_testing": ([vp, vp, vp, u32, vp, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)

@@ -236,7 +236,7 @@ void launch_learn_adopt(const Params& P, const DevPtrs& d, const Sizes& z, cudaS
 void launch_learn_target(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 void launch_copy_double(const double* src, double* dst, cudaStream_t st);
 void launch_mlp_infer(const void* halfW, const float* prm, const float* norm, const float* X, uint32_t n, float* Y,
-                      cudaStream_t st);
+                      uint32_t* status, cudaStream_t st);
 void launch_mlp_mirror(const float* prm, void* halfW, cudaStream_t st);
 uint32_t mlp_param_count();
 uint32_t mlp_half_count();

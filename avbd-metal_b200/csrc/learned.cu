@@ -63,130 +63,221 @@ __device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1
 __device__ __forceinline__ uint32_t ld_pair(const bf16* p) { return *reinterpret_cast<const uint32_t*>(p); }
 
 // ---------------------------------------------------------------------------
-// Fused inference: one warp per 16 vertices, activations stay in registers
-// between layers (an m16n8 accumulator pair is exactly the next layer's
-// m16k16 operand), weights are read from L1/L2 (72 KB shared by all warps).
+// Fused inference on the Blackwell tensor cores (tcgen05): one CTA of four
+// warps per 128-row tile, persistent over the batch.  The weights are staged
+// once per CTA in shared memory in the UMMA canonical K-major layout without
+// swizzle (8-row x 16-byte core matrices: element (r, k) of an operand with
+// row-group stride `sbo` at (r / 8) sbo + (k / 8) 128 + (r % 8) 16 + (k % 8) 2
+// bytes); a layer is 2 (K = 32) or 8 (K = 128) tcgen05.mma instructions of
+// M = 128, K = 16, issued by one thread, accumulating in TMEM (128 lanes =
+// the tile's rows, N fp32 columns); each warp reads its 32 rows back with
+// tcgen05.ld, adds the bias, applies ReLU, rounds to BF16 and writes the next
+// layer's A operand in place.  Completion of every layer's MMAs is signalled
+// by tcgen05.commit on an mbarrier; every wait on it is bounded and a
+// timeout sets *status (the CTA then frees its TMEM and stops).
 // ---------------------------------------------------------------------------
-// Shared-memory copy of the BF16 weights: rows padded by 8 halves so that the
-// eight rows a fragment load touches fall in distinct banks.
-constexpr int kS1 = mlp::DIN + 8, kSH = mlp::HID + 8;
-constexpr uint32_t kSW1 = 0, kSW2 = kSW1 + mlp::HID * kS1, kSW3 = kSW2 + mlp::HID * kSH, kSW4 = kSW3 + mlp::HID * kSH,
-                   kSWN = kSW4 + mlp::DOUT * kSH;
-constexpr uint32_t kInferWarps = 4;
-constexpr size_t kInferSmem = sizeof(bf16) * kSWN;
+namespace tc {
+constexpr uint32_t ROWS = 128;
+constexpr uint32_t SBO_K128 = 2048, SBO_K32 = 512;      // row-group strides (K = 128, K = 32)
+constexpr uint32_t W1 = 0, W2 = W1 + 128 * 32 * 2, W3 = W2 + 128 * 128 * 2, W4 = W3 + 128 * 128 * 2,
+                   ACT = W4 + 16 * 128 * 2, BAR = ACT + ROWS * 128 * 2, TSLOT = BAR + 8, SMEM = TSLOT + 8;
+constexpr uint32_t TMEM_COLS = 128;
+constexpr uint64_t WAIT_NS = 1000000000ull;              // a wait gives up after one second
 
-// Fused 4-layer inference: every block stages the weights once and its warps
-// take 16-row tiles until the batch is done (m16n8k16 BF16 MMA, FP32
-// accumulation, bias / ReLU / BF16 conversion between layers in registers).
-__global__ void __launch_bounds__(128) k_mlp_infer(const bf16* __restrict__ W, const float* __restrict__ prm,
-                                                   const float* __restrict__ norm, const float* __restrict__ X,
-                                                   uint32_t n, float* __restrict__ Y) {
+__device__ __forceinline__ uint32_t off(uint32_t r, uint32_t k, uint32_t sbo) {
+    return (r >> 3) * sbo + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+// shared-memory matrix descriptor: start address, LBO = 128 B (the second
+// 8-element K chunk), SBO, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t desc(uint32_t saddr, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(sbo >> 4) << 32) |
+           (1ull << 46);
+}
+// instruction descriptor of kind::f16: F32 accumulator, BF16 A and B, both
+// K-major, N >> 3, M >> 4
+__host__ __device__ constexpr uint32_t idesc(uint32_t m, uint32_t n) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+__device__ __forceinline__ void mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t id, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        :
+        : "r"(tmem), "l"(a), "l"(b), "r"(id), "r"(acc));
+}
+__device__ __forceinline__ void commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ uint64_t now_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+// bounded wait for the mbarrier phase `parity`; false on timeout
+__device__ __forceinline__ bool wait(uint32_t bar, uint32_t parity) {
+    const uint64_t t0 = now_ns();
+    for (uint32_t i = 0;; i++) {
+        if ((i & 255u) == 255u && now_ns() - t0 > WAIT_NS) return false;
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// 32 consecutive fp32 columns of this thread's TMEM lane
+__device__ __forceinline__ void ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 32; j++) v[j] = __uint_as_float(r[j]);
+}
+__device__ __forceinline__ void ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
+}
+}  // namespace tc
+
+__global__ void __launch_bounds__(128) k_mlp_infer_tc(const bf16* __restrict__ W, const float* __restrict__ prm,
+                                                      const float* __restrict__ norm, const float* __restrict__ X,
+                                                      uint32_t n, float* __restrict__ Y, uint32_t* status,
+                                                      bool issue = true) {
     using namespace mlp;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    bf16* sw = reinterpret_cast<bf16*>(smem_raw);
-    // stage the weights: 16-byte chunks, 8 halves each
-    auto stage = [&](uint32_t dst, uint32_t src, int rows, int cols, int stride) {
-        const int chunks = rows * (cols / 8);
-        for (int c = threadIdx.x; c < chunks; c += blockDim.x) {
-            const int r = c / (cols / 8), k = (c % (cols / 8)) * 8;
-            *reinterpret_cast<uint4*>(sw + dst + r * stride + k) = *reinterpret_cast<const uint4*>(W + src + r * cols + k);
+    extern __shared__ __align__(128) unsigned char sm[];
+    const uint32_t t = threadIdx.x, warp = t >> 5;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+    const uint32_t bar = sbase + tc::BAR;
+    // weights -> canonical K-major core matrices, 16 bytes per thread-step
+    auto stage = [&](uint32_t dst, uint32_t src, uint32_t rows, uint32_t cols, uint32_t sbo) {
+        const uint32_t chunks = rows * (cols / 8);
+        for (uint32_t c = t; c < chunks; c += blockDim.x) {
+            const uint32_t r = c / (cols / 8), k = (c % (cols / 8)) * 8;
+            *reinterpret_cast<uint4*>(sm + dst + tc::off(r, k, sbo)) =
+                *reinterpret_cast<const uint4*>(W + src + r * cols + k);
         }
     };
-    stage(kSW1, HW1, HID, DIN, kS1);
-    stage(kSW2, HW2, HID, HID, kSH);
-    stage(kSW3, HW3, HID, HID, kSH);
-    stage(kSW4, HW4, DOUT, HID, kSH);
+    stage(tc::W1, HW1, HID, DIN, tc::SBO_K32);
+    stage(tc::W2, HW2, HID, HID, tc::SBO_K128);
+    stage(tc::W3, HW3, HID, HID, tc::SBO_K128);
+    stage(tc::W4, HW4, DOUT, HID, tc::SBO_K128);
+    if (t == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + tc::TSLOT),
+                     "r"(tc::TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc::fence_before();
     __syncthreads();
-    const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, q = lane & 3u;
-    const uint32_t tiles = (n + 15) / 16;
-    for (uint32_t tile = blockIdx.x * kInferWarps + (threadIdx.x >> 5); tile < tiles; tile += gridDim.x * kInferWarps) {
-    const uint32_t row0 = tile * 16u;
-    const uint32_t r0 = row0 + g, r1 = row0 + g + 8;
-    auto xin = [&](uint32_t r, uint32_t c) {
-        return r < n ? (X[r * DIN + c] - norm[NX_MEAN + c]) * norm[NX_INV + c] : 0.0f;
-    };
-    uint32_t a[8][4];
+    tc::fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + tc::TSLOT);
+    const uint32_t lane_addr = tmem + ((warp * 32u) << 16);   // this warp's 32 TMEM lanes
+    const uint32_t row = t;                                    // tile row held by this thread
+    uint32_t phase = 0;
+    bool ok = true;
+    const uint32_t tiles = (n + tc::ROWS - 1) / tc::ROWS;
+    for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
+        const uint32_t r = tile * tc::ROWS + row;
+        // layer-1 operand: normalised features, BF16
 #pragma unroll
-    for (int kb = 0; kb < DIN / 16; kb++) {
-        const uint32_t c0 = 16 * kb + 2 * q;
-        a[kb][0] = pack_bf16(xin(r0, c0), xin(r0, c0 + 1));
-        a[kb][1] = pack_bf16(xin(r1, c0), xin(r1, c0 + 1));
-        a[kb][2] = pack_bf16(xin(r0, c0 + 8), xin(r0, c0 + 9));
-        a[kb][3] = pack_bf16(xin(r1, c0 + 8), xin(r1, c0 + 9));
-    }
-    float acc[16][4];
-    // layer 1: K = DIN
+        for (uint32_t kg = 0; kg < DIN / 8; kg++) {
+            uint32_t w[4];
 #pragma unroll
-    for (int j = 0; j < 16; j++) {
-        acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
-#pragma unroll
-        for (int kb = 0; kb < DIN / 16; kb++) {
-            const bf16* w = sw + kSW1 + (8 * j + g) * kS1 + 16 * kb + 2 * q;
-            mma_bf16(acc[j], a[kb][0], a[kb][1], a[kb][2], a[kb][3], ld_pair(w), ld_pair(w + 8));
+            for (int e = 0; e < 4; e++) {
+                const uint32_t c = kg * 8 + 2 * e;
+                const float a = r < n ? (X[(size_t)r * DIN + c] - norm[NX_MEAN + c]) * norm[NX_INV + c] : 0.0f;
+                const float b = r < n ? (X[(size_t)r * DIN + c + 1] - norm[NX_MEAN + c + 1]) * norm[NX_INV + c + 1]
+                                      : 0.0f;
+                w[e] = pack_bf16(a, b);
+            }
+            *reinterpret_cast<uint4*>(sm + tc::ACT + tc::off(row, kg * 8, tc::SBO_K128)) = make_uint4(w[0], w[1], w[2], w[3]);
         }
-    }
-    const float* bias = prm + OB1;
-    const bf16* Wl = sw + kSW2;
+        for (int layer = 0; layer < 4 && ok; layer++) {
+            tc::fence_proxy();          // the operand writes above are read by the tensor core
+            tc::fence_before();
+            __syncthreads();
+            tc::fence_after();
+            if (t == 0 && issue) {       // issue = false only in the timeout test: nothing ever arrives
+                const uint32_t wbase = layer == 0 ? tc::W1 : (layer == 1 ? tc::W2 : (layer == 2 ? tc::W3 : tc::W4));
+                const uint32_t wsbo = layer == 0 ? tc::SBO_K32 : tc::SBO_K128;
+                const uint32_t steps = layer == 0 ? DIN / 16 : HID / 16;
+                const uint32_t id = tc::idesc(128, layer == 3 ? DOUT : HID);
+                for (uint32_t s = 0; s < steps; s++)
+                    tc::mma(tmem, tc::desc(sbase + tc::ACT + 256u * s, tc::SBO_K128),
+                            tc::desc(sbase + wbase + 256u * s, wsbo), id, s > 0 ? 1u : 0u);
+                tc::commit(bar);
+            }
+            // block-uniform outcome: every thread leaves the loop together
+            ok = __syncthreads_and(tc::wait(bar, phase) ? 1 : 0) != 0;
+            phase ^= 1u;
+            tc::fence_after();
+            if (!ok) break;
+            if (layer < 3) {
+                // bias, ReLU, BF16: the next layer's operand, written in place
+                const float* bias = prm + (layer == 0 ? OB1 : (layer == 1 ? OB2 : OB3));
 #pragma unroll 1
-    for (int layer = 0; layer < 2; layer++) {
-        // epilogue: bias, ReLU, BF16 -> operand of the next layer
+                for (uint32_t c0 = 0; c0 < HID; c0 += 32) {
+                    float v[32];
+                    tc::ld32(lane_addr + c0, v);
 #pragma unroll
-        for (int kb = 0; kb < 8; kb++) {
-            const float b00 = bias[16 * kb + 2 * q], b01 = bias[16 * kb + 2 * q + 1];
-            const float b10 = bias[16 * kb + 8 + 2 * q], b11 = bias[16 * kb + 8 + 2 * q + 1];
-            a[kb][0] = pack_bf16(fmaxf(acc[2 * kb][0] + b00, 0.0f), fmaxf(acc[2 * kb][1] + b01, 0.0f));
-            a[kb][1] = pack_bf16(fmaxf(acc[2 * kb][2] + b00, 0.0f), fmaxf(acc[2 * kb][3] + b01, 0.0f));
-            a[kb][2] = pack_bf16(fmaxf(acc[2 * kb + 1][0] + b10, 0.0f), fmaxf(acc[2 * kb + 1][1] + b11, 0.0f));
-            a[kb][3] = pack_bf16(fmaxf(acc[2 * kb + 1][2] + b10, 0.0f), fmaxf(acc[2 * kb + 1][3] + b11, 0.0f));
-        }
+                    for (uint32_t kg = 0; kg < 4; kg++) {
+                        uint32_t w[4];
 #pragma unroll
-        for (int j = 0; j < 16; j++) {
-            acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+                        for (int e = 0; e < 4; e++) {
+                            const uint32_t j = kg * 8 + 2 * e;
+                            w[e] = pack_bf16(fmaxf(v[j] + bias[c0 + j], 0.0f), fmaxf(v[j + 1] + bias[c0 + j + 1], 0.0f));
+                        }
+                        *reinterpret_cast<uint4*>(sm + tc::ACT + tc::off(row, c0 + kg * 8, tc::SBO_K128)) =
+                            make_uint4(w[0], w[1], w[2], w[3]);
+                    }
+                }
+            } else {
+                float v[16];
+                tc::ld16(lane_addr, v);
+                if (r < n) {
 #pragma unroll
-            for (int kb = 0; kb < 8; kb++) {
-                const bf16* w = Wl + (8 * j + g) * kSH + 16 * kb + 2 * q;
-                mma_bf16(acc[j], a[kb][0], a[kb][1], a[kb][2], a[kb][3], ld_pair(w), ld_pair(w + 8));
+                    for (uint32_t c = 0; c < (uint32_t)USED_OUT; c++) {
+                        const float y = v[c] + prm[OB4 + c];
+                        Y[(size_t)r * USED_OUT + c] = y * norm[NY_STD + c] + norm[NY_MEAN + c];
+                    }
+                }
             }
         }
-        bias = layer == 0 ? prm + OB2 : prm + OB3;
-        Wl = sw + kSW3;
+        // every lane's TMEM reads are done before the next tile's MMAs
+        tc::fence_before();
+        __syncthreads();
+        tc::fence_after();
     }
-#pragma unroll
-    for (int kb = 0; kb < 8; kb++) {
-        const float b00 = bias[16 * kb + 2 * q], b01 = bias[16 * kb + 2 * q + 1];
-        const float b10 = bias[16 * kb + 8 + 2 * q], b11 = bias[16 * kb + 8 + 2 * q + 1];
-        a[kb][0] = pack_bf16(fmaxf(acc[2 * kb][0] + b00, 0.0f), fmaxf(acc[2 * kb][1] + b01, 0.0f));
-        a[kb][1] = pack_bf16(fmaxf(acc[2 * kb][2] + b00, 0.0f), fmaxf(acc[2 * kb][3] + b01, 0.0f));
-        a[kb][2] = pack_bf16(fmaxf(acc[2 * kb + 1][0] + b10, 0.0f), fmaxf(acc[2 * kb + 1][1] + b11, 0.0f));
-        a[kb][3] = pack_bf16(fmaxf(acc[2 * kb + 1][2] + b10, 0.0f), fmaxf(acc[2 * kb + 1][3] + b11, 0.0f));
-    }
-    // layer 4: N = 16 (two tiles), only columns 0..2 are read
-    float o[2][4];
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-        o[j][0] = o[j][1] = o[j][2] = o[j][3] = 0.0f;
-#pragma unroll
-        for (int kb = 0; kb < 8; kb++) {
-            const bf16* w = sw + kSW4 + (8 * j + g) * kSH + 16 * kb + 2 * q;
-            mma_bf16(o[j], a[kb][0], a[kb][1], a[kb][2], a[kb][3], ld_pair(w), ld_pair(w + 8));
-        }
-    }
-    // columns 2q, 2q+1 of tile 0 live in lane q; denormalise and store
-    if (q < 2) {
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const uint32_t r = h == 0 ? r0 : r1;
-            if (r >= n) continue;
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const uint32_t c = 2 * q + e;
-                if (c >= (uint32_t)USED_OUT) continue;
-                const float v = o[0][2 * h + e] + prm[OB4 + c];
-                Y[r * USED_OUT + c] = v * norm[NY_STD + c] + norm[NY_MEAN + c];
-            }
-        }
-    }
-    }
+    if (!ok && t == 0) atomicCAS(status, 0u, (uint32_t)AVBD_FAIL_WAIT_TIMEOUT);
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tc::TMEM_COLS)
+                     : "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -641,16 +732,18 @@ void launch_learn_target(const Params& P, const DevPtrs& d, const Sizes& z, cuda
 void launch_copy_double(const double* src, double* dst, cudaStream_t st) { k_copy_double<<<1, 32, 0, st>>>(src, dst); }
 
 void launch_mlp_infer(const void* halfW, const float* prm, const float* norm, const float* X, uint32_t n, float* Y,
-                      cudaStream_t st) {
+                      uint32_t* status, cudaStream_t st) {
     if (n == 0) return;
-    static bool attr = false;     // the weights need more than the default 48 KiB of shared memory
+    static bool attr = false;     // weights + one activation tile: 108 KiB of shared memory
     if (!attr) {
-        cudaFuncSetAttribute(k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInferSmem);
+        cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM);
         attr = true;
     }
-    const uint32_t tiles = (n + 15) / 16;
-    const uint32_t blocks = std::min<uint32_t>((tiles + kInferWarps - 1) / kInferWarps, 2u * 148u);
-    k_mlp_infer<<<blocks, 32 * kInferWarps, kInferSmem, st>>>(static_cast<const bf16*>(halfW), prm, norm, X, n, Y);
+    // two CTAs per SM (108 KiB of shared memory and 128 TMEM columns each),
+    // every CTA walking 128-row tiles
+    const uint32_t tiles = (n + tc::ROWS - 1) / tc::ROWS;
+    const uint32_t blocks = std::min<uint32_t>(tiles, 2u * 148u);
+    k_mlp_infer_tc<<<blocks, 128, tc::SMEM, st>>>(static_cast<const bf16*>(halfW), prm, norm, X, n, Y, status);
 }
 
 void launch_mlp_mirror(const float* prm, void* halfW, cudaStream_t st) {
@@ -702,13 +795,37 @@ int avbd_mlp_train_step(float* params, const float* norm, const float* features,
     return cudaGetLastError() == cudaSuccess ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
 }
 
-int avbd_mlp_infer(const float* params, const float* norm, const float* features, uint32_t n, float* out,
-                   void* workspace, void* stream) {
+static int mlp_infer(const float* params, const float* norm, const float* features, uint32_t n, float* out,
+                     void* workspace, void* stream, bool issue) {
     if (!params || !norm || !features || !out || !workspace) return AVBD_ERR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the BF16 weight mirror, then the kernel's status word
+    uint32_t* status = reinterpret_cast<uint32_t*>(static_cast<char*>(workspace) +
+                                                   ((sizeof(bf16) * mlp::NHALF + 255) / 256) * 256);
+    cudaMemsetAsync(status, 0, sizeof(uint32_t), st);
     launch_mlp_mirror(params, workspace, st);
-    launch_mlp_infer(workspace, params, norm, features, n, out, st);
-    return cudaGetLastError() == cudaSuccess ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+    if (issue) {
+        launch_mlp_infer(workspace, params, norm, features, n, out, status, st);
+    } else if (n) {
+        cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM);
+        k_mlp_infer_tc<<<1, 128, tc::SMEM, st>>>(static_cast<const bf16*>(workspace), params, norm, features, n, out,
+                                                 status, false);
+    }
+    uint32_t h = 0;
+    if (cudaMemcpyAsync(&h, status, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return AVBD_ERR_RUNTIME_FAILURE;
+    return h == 0 ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+}
+
+int avbd_mlp_infer(const float* params, const float* norm, const float* features, uint32_t n, float* out,
+                   void* workspace, void* stream) {
+    return mlp_infer(params, norm, features, n, out, workspace, stream, true);
+}
+
+int avbd_mlp_infer_wait_timeout_for_testing(const float* params, const float* norm, const float* features,
+                                            uint32_t n, float* out, void* workspace, void* stream) {
+    return mlp_infer(params, norm, features, n, out, workspace, stream, false);
 }
 
 }  // extern "C"

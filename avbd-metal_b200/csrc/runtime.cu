@@ -343,7 +343,8 @@ struct avbd_solver {
             fb.posAng = f.learnSweptAng;
             // the trial sweeps count OGC bound exceeders in slots 2 (plain) and 3 (predicted)
             if (ogcSlots) { fp.ogcExceed = ogcSlots + 2; fb.ogcExceed = ogcSlots + 3; }
-            launch_mlp_infer(f.learnHalf, f.learnPrm, f.learnNorm, f.learnFeat, z.numLearn, f.learnPred, st);
+            launch_mlp_infer(f.learnHalf, f.learnPrm, f.learnNorm, f.learnFeat, z.numLearn, f.learnPred,
+                             f.failureLatch, st);
             launch_learn_branch(P, f, z, st);
             if (trace) launch_residual(P, fb, z, f.learnResidBodies, f.learnTrace + 1, st);
             // The two trial branches touch disjoint pose buffers (in
@@ -760,6 +761,9 @@ struct avbd_solver {
             else if (failure == AVBD_FAIL_PLANAR_DAT_GRID_SPAN)
                 std::snprintf(buf, sizeof buf, "Planar-DAT element grid span exceeded at frame %u: %u elements",
                               hostLatch[1], hostLatch[2]);
+            else if (failure == AVBD_FAIL_WAIT_TIMEOUT)
+                std::snprintf(buf, sizeof buf, "a bounded device wait (warm-start MLP inference) gave up during "
+                              "frame %u", hostLatch[1]);
             else if (failure == AVBD_FAIL_PLANAR_DAT_INVALID_ANCHOR)
                 std::snprintf(buf, sizeof buf, "Planar-DAT invalid anchor at frame %u: %u pairs", hostLatch[1],
                               hostLatch[2]);

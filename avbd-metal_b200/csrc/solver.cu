@@ -1266,8 +1266,11 @@ __device__ __forceinline__ float3 solve3x3_particle(const M3& a, float3 b) {
 // GENERAL instances keep four blocks per SM (at most 128 registers): the
 // rigid-body path would otherwise take ~160 registers for every thread and
 // cap large colors at three blocks (measured 7% slower mixed frames).
+#ifndef AVBD_PARTICLE_PRIMAL_MIN_BLOCKS
+#define AVBD_PARTICLE_PRIMAL_MIN_BLOCKS 1
+#endif
 template <int LANES, bool GENERAL, bool CLOTH, bool RESID = false>
-__global__ void __launch_bounds__(128, GENERAL ? 4 : 1) k_primal_group(const Params P, const DevPtrs d, uint32_t color,
+__global__ void __launch_bounds__(128, GENERAL ? 4 : AVBD_PARTICLE_PRIMAL_MIN_BLOCKS) k_primal_group(const Params P, const DevPtrs d, uint32_t color,
                                                       uint32_t count) {
     constexpr int GROUPS = 32 / LANES;
     pdl_prologue();
@@ -1629,9 +1632,16 @@ __global__ void __launch_bounds__(256) k_solve_small(const Params P, const DevPt
     const uint32_t groups = blockDim.x >> 3;
     const uint32_t group = threadIdx.x >> 3, lane = threadIdx.x & 7u;
     const unsigned mask = 0xFFu << (threadIdx.x & 24u);
+    // the color offsets do not change during the solve: one copy in shared
+    // memory instead of a dependent global load per color per iteration
+    __shared__ uint32_t cs[MAX_COLORS + 1];
+    for (uint32_t c = threadIdx.x; c <= colorBound && c <= (uint32_t)MAX_COLORS; c += blockDim.x) cs[c] = d.colorStart[c];
+    __syncthreads();
+    uint32_t last = 0;                           // one past the last non-empty color
+    for (uint32_t c = 0; c < colorBound; c++) if (cs[c + 1] != cs[c]) last = c + 1;
     for (uint32_t it = 0; it < P.iterations; it++) {
-        for (uint32_t c = 0; c < colorBound; c++) {
-            const uint32_t s = d.colorStart[c], e = d.colorStart[c + 1];
+        for (uint32_t c = 0; c < last; c++) {
+            const uint32_t s = cs[c], e = cs[c + 1];
             if (s == e) continue;                // block-uniform
             for (uint32_t slot = group; s + slot < e; slot += groups)
                 primal_body(P, d, d.colorList[s + slot], lane, mask);

@@ -431,9 +431,19 @@ int avbd_mlp_gradients(const float* params, const float* norm, const float* feat
 int avbd_mlp_train_step(float* params, const float* norm, const float* features,
                         const float* targets, uint32_t batch, float* adam_m, float* adam_v,
                         uint32_t step, float lr, void* workspace, float* loss_out, void* stream);
-/* Inference over n feature rows into out[n][3] (workspace >= 80 KiB).     */
+/* Inference over n feature rows into out[n][3] on the tensor cores
+ * (tcgen05.mma, accumulators in tensor memory); synchronises `stream` and
+ * returns AVBD_ERR_RUNTIME_FAILURE if the kernel's bounded wait for its MMA
+ * completion gave up (workspace >= 80 KiB).                               */
 int avbd_mlp_infer(const float* params, const float* norm, const float* features, uint32_t n,
                    float* out, void* workspace, void* stream);
+/* Test of the inference kernel's bounded wait: the same launch with no
+ * tensor-core work issued, so its wait for the MMA completion barrier runs
+ * out (after about one second), the CTA frees its tensor memory and the call
+ * returns AVBD_ERR_RUNTIME_FAILURE with the device still usable.  No
+ * counterpart in the reference.                                            */
+int avbd_mlp_infer_wait_timeout_for_testing(const float* params, const float* norm, const float* features,
+                                            uint32_t n, float* out, void* workspace, void* stream);
 
 /* Read-only access to one internal buffer for parity checks and tools
  * (no counterpart in the reference's public API; its tests read the same

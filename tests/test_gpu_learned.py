@@ -47,17 +47,49 @@ def test_gradients_match_float64_oracle(cuda_lib, oracle_lib, B):
         assert err <= 5e-3, (name, err)
 
 
-def test_inference_matches_oracle(cuda_lib, oracle_lib):
+@pytest.mark.parametrize("n", [1, 127, 1000, 128 * 296 + 37])
+def test_inference_matches_oracle(cuda_lib, oracle_lib, n):
+    """The tcgen05 inference kernel (128-row tiles, persistent CTAs) against
+    the float64 network with BF16-rounded weights and activations: a single
+    row, a partial tile, several tiles, and more tiles than CTAs."""
     from oracle import mlp_oracle as M
     rng = np.random.default_rng(7)
     p = learned.init_params(seed=3)
     p[M.OB4:M.OB4 + 3] = [0.1, -0.2, 0.3]
     norm = _norm(rng)
-    X, _ = _random_batch(rng, 1000)
+    X, _ = _random_batch(rng, n)
     y = learned.infer(p, norm, X)
     want = M.predict(p, norm, X, rounded=True)
     scale = np.abs(want).max()
     assert np.abs(y - want).max() <= 1e-3 * scale + 1e-6
+
+
+def test_inference_wait_gives_up_and_leaves_the_device_usable(cuda_lib):
+    """The inference kernel's wait for its MMA completion barrier is bounded:
+    with no tensor-core work issued nothing ever arrives, the wait gives up
+    after about a second, the call reports a runtime failure, and the next
+    inference on the same device is correct."""
+    import ctypes as C
+    import torch
+    from avbd_b200.solver import load_library
+    rng = np.random.default_rng(1)
+    p = learned.init_params(seed=2)
+    norm = _norm(rng)
+    X, _ = _random_batch(rng, 256)
+    dev = torch.device("cuda", 0)
+    prm = torch.from_numpy(p.astype(np.float32)).to(dev)
+    nrm = torch.from_numpy(norm.astype(np.float32)).to(dev)
+    Xd = torch.from_numpy(X.astype(np.float32)).to(dev)
+    out = torch.zeros((256, 3), dtype=torch.float32, device=dev)
+    ws = torch.empty(1 << 17, dtype=torch.uint8, device=dev)
+    rc = load_library().avbd_mlp_infer_wait_timeout_for_testing(
+        prm.data_ptr(), nrm.data_ptr(), Xd.data_ptr(), 256, out.data_ptr(), ws.data_ptr(),
+        C.c_void_p(torch.cuda.current_stream(dev).cuda_stream))
+    assert rc == abi.ERR_RUNTIME_FAILURE
+    from oracle import mlp_oracle as M
+    y = learned.infer(p, norm, X)
+    want = M.predict(p, norm, X, rounded=True)
+    assert np.abs(y - want).max() <= 1e-3 * np.abs(want).max() + 1e-6
 
 
 @pytest.mark.parametrize("name,make,trials,frames", [
