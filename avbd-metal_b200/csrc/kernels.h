@@ -59,6 +59,7 @@ struct DevPtrs {
     uint32_t* dynSplit;                   // manifold entries at the head of each sorted dyn segment
     uint32_t* adjLongQueue;               // bodies with long contact segments this frame
     uint32_t* postTets;                   // tet entries at the head of each static post segment
+    const TetGPU* tetInc;                 // tet records in postList order (null without tets)
     // coloring
     uint32_t *colorsA, *colorsB, *colorList, *bodySlot;
     // control

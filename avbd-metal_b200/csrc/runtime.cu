@@ -571,6 +571,14 @@ struct avbd_solver {
         ok = ok && upload(d.preList, H.preList, "preList") && upload(d.postList, H.postList, "postList");
         ok = ok && alloc(d.dynCount, nb, "dynCount") && alloc(d.dynStart, nb, "dynStart") && alloc(d.dynCursor, nb, "dynCursor");
         ok = ok && alloc(d.dynSplit, nb, "dynSplit") && upload(d.postTets, H.postTets, "postTets");
+        d.tetInc = nullptr;
+#ifndef AVBD_NO_TET_INCIDENCE
+        if (ok && !H.tetInc.empty()) {
+            TetGPU* ti = nullptr;
+            ok = upload(ti, H.tetInc, "tetIncidence");
+            d.tetInc = ti;
+        }
+#endif
         ok = ok && alloc(d.adjLongQueue, nb, "adjLongQueue");
         ok = ok && alloc(d.dynList, 2 * (size_t)H.maxPairs + ((P.cloth || P.ogc) ? 4 * (size_t)P.maxSoft : 0), "dynList");
         // coloring

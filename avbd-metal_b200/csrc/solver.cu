@@ -324,7 +324,7 @@ void launch_adjacency(const Params& P, const DevPtrs& d, const Sizes& z, cudaStr
 struct AdjView {
     const uint32_t* pre; uint32_t nPre;
     const uint32_t* dyn; uint32_t nMan, nDyn;
-    const uint32_t* post; uint32_t nTet, nPost;
+    const uint32_t* post; uint32_t nTet, nPost, postBase;
     __device__ __forceinline__ uint32_t count() const { return nPre + nDyn + nPost; }
     __device__ __forceinline__ uint32_t at(uint32_t k) const {
         if (k < nPre) return pre[k];
@@ -342,7 +342,7 @@ __device__ __forceinline__ AdjView adj_view(const DevPtrs& d, uint32_t b) {
     AdjView v;
     v.pre = d.preList + s.x; v.nPre = s.y;
     v.dyn = d.dynList + d.dynStart[b]; v.nDyn = d.dynCount[b]; v.nMan = d.dynSplit[b];
-    v.post = d.postList + s.z; v.nPost = s.w; v.nTet = d.postTets[b];
+    v.post = d.postList + s.z; v.nPost = s.w; v.nTet = d.postTets[b]; v.postBase = s.z;
     return v;
 }
 
@@ -1028,40 +1028,44 @@ struct ParticleTerms {
     uint32_t kind;       // TERM_*
 };
 
+// Stable Neo-Hookean tet terms of vertex `self` (stampTet, 40_solver.metal:972-1024)
+__device__ __forceinline__ void tet_terms(const DevPtrs& d, const TetGPU& tt, uint32_t self, ParticleTerms& t) {
+    const float3 x0 = xyz(d.posLin[tt.ids.x]), x1 = xyz(d.posLin[tt.ids.y]);
+    const float3 x2 = xyz(d.posLin[tt.ids.z]), x3 = xyz(d.posLin[tt.ids.w]);
+    const float muV = tt.r1.w, lamV = tt.r2.w;
+    const float alphaT = 1.0f + muV / mx(lamV, 1e-9f);
+    const float3 d0 = x1 - x0, d1 = x2 - x0, d2 = x3 - x0;
+    const float3 m0 = xyz(tt.r0), m1 = xyz(tt.r1), m2 = xyz(tt.r2);
+    const float3 f0 = d0 * m0.x + d1 * m1.x + d2 * m2.x;
+    const float3 f1 = d0 * m0.y + d1 * m1.y + d2 * m2.y;
+    const float3 f2 = d0 * m0.z + d1 * m1.z + d2 * m2.z;
+    const float J = dot(f0, cross(f1, f2));
+    const float3 j0 = cross(f1, f2), j1 = cross(f2, f0), j2 = cross(f0, f1);
+    const float s2 = lamV * (J - alphaT);
+    const float3 p0 = muV * f0 + s2 * j0;
+    const float3 p1 = muV * f1 + s2 * j1;
+    const float3 p2 = muV * f2 + s2 * j2;
+    float3 w;
+    if (self == tt.ids.y) w = m0;
+    else if (self == tt.ids.z) w = m1;
+    else if (self == tt.ids.w) w = m2;
+    else w = -mk3(m0.x + m1.x + m2.x, m0.y + m1.y + m2.y, m0.z + m1.z + m2.z);
+    t.rhs = p0 * w.x + p1 * w.y + p2 * w.z;
+    const float3 g = j0 * w.x + j1 * w.y + j2 * w.z;
+    // lamV * outer(g, g) is exactly symmetric: g_i g_j == g_j g_i
+    t.a = mk3((g.x * g.x) * lamV, (g.y * g.y) * lamV, (g.z * g.z) * lamV);
+    t.b = mk3((g.y * g.x) * lamV, (g.z * g.x) * lamV, (g.z * g.y) * lamV);
+    t.c = mk3(muV * dot(w, w), 0.0f, 0.0f);
+    t.kind = 1;
+}
+
 template <bool CLOTH>
 __device__ __forceinline__ void particle_terms(const Params& P, const DevPtrs& d, uint32_t entry,
                                                uint32_t self, ParticleTerms& t) {
     const uint32_t kind = entry >> ADJ_KIND_SHIFT, idx = entry & ADJ_INDEX_MASK;
     t.kind = 3;
     if (kind == FK_TET) {
-        const TetGPU tt = d.tets[idx];
-        const float3 x0 = xyz(d.posLin[tt.ids.x]), x1 = xyz(d.posLin[tt.ids.y]);
-        const float3 x2 = xyz(d.posLin[tt.ids.z]), x3 = xyz(d.posLin[tt.ids.w]);
-        const float muV = tt.r1.w, lamV = tt.r2.w;
-        const float alphaT = 1.0f + muV / mx(lamV, 1e-9f);
-        const float3 d0 = x1 - x0, d1 = x2 - x0, d2 = x3 - x0;
-        const float3 m0 = xyz(tt.r0), m1 = xyz(tt.r1), m2 = xyz(tt.r2);
-        const float3 f0 = d0 * m0.x + d1 * m1.x + d2 * m2.x;
-        const float3 f1 = d0 * m0.y + d1 * m1.y + d2 * m2.y;
-        const float3 f2 = d0 * m0.z + d1 * m1.z + d2 * m2.z;
-        const float J = dot(f0, cross(f1, f2));
-        const float3 j0 = cross(f1, f2), j1 = cross(f2, f0), j2 = cross(f0, f1);
-        const float s2 = lamV * (J - alphaT);
-        const float3 p0 = muV * f0 + s2 * j0;
-        const float3 p1 = muV * f1 + s2 * j1;
-        const float3 p2 = muV * f2 + s2 * j2;
-        float3 w;
-        if (self == tt.ids.y) w = m0;
-        else if (self == tt.ids.z) w = m1;
-        else if (self == tt.ids.w) w = m2;
-        else w = -mk3(m0.x + m1.x + m2.x, m0.y + m1.y + m2.y, m0.z + m1.z + m2.z);
-        t.rhs = p0 * w.x + p1 * w.y + p2 * w.z;
-        const float3 g = j0 * w.x + j1 * w.y + j2 * w.z;
-        // lamV * outer(g, g) is exactly symmetric: g_i g_j == g_j g_i
-        t.a = mk3((g.x * g.x) * lamV, (g.y * g.y) * lamV, (g.z * g.z) * lamV);
-        t.b = mk3((g.y * g.x) * lamV, (g.z * g.x) * lamV, (g.z * g.y) * lamV);
-        t.c = mk3(muV * dot(w, w), 0.0f, 0.0f);
-        t.kind = 1;
+        tet_terms(d, d.tets[idx], self, t);
     } else if (kind == FK_MANIFOLD) {
         const ManifoldGPU& m = d.manifolds[idx];
         const u4 h = m.header;
@@ -1266,6 +1270,10 @@ __device__ __forceinline__ float3 solve3x3_particle(const M3& a, float3 b) {
 // GENERAL instances keep four blocks per SM (at most 128 registers): the
 // rigid-body path would otherwise take ~160 registers for every thread and
 // cap large colors at three blocks (measured 7% slower mixed frames).
+#ifndef AVBD_PRIMAL_UNROLL
+#define AVBD_PRIMAL_UNROLL 1
+#endif
+constexpr int kPrimalUnroll = AVBD_PRIMAL_UNROLL;
 #ifndef AVBD_PARTICLE_PRIMAL_MIN_BLOCKS
 #define AVBD_PARTICLE_PRIMAL_MIN_BLOCKS 1
 #endif
@@ -1300,14 +1308,23 @@ __global__ void __launch_bounds__(128, GENERAL ? 4 : AVBD_PARTICLE_PRIMAL_MIN_BL
     ParticleAccum acc{m3_zero(), s3(0)};
     const AdjView v = adj_view(d, body);
     const uint32_t cnt = v.count();
+#pragma unroll (kPrimalUnroll)
     for (uint32_t base = 0; base < cnt; base += LANES) {
         const uint32_t k = base + lane;
         ParticleTerms t;
         t.kind = 0;
         uint32_t entry = 0;
         if (k < cnt) {
-            entry = v.at(k);
-            particle_terms<CLOTH>(P, d, entry, body, t);
+            // a tet entry reads its record from the body's incidence slot
+            // (contiguous over the lanes) instead of through the entry
+            const uint32_t kt = k - v.nPre - v.nMan;
+            if (d.tetInc && k >= v.nPre + v.nMan && kt < v.nTet) {
+                entry = (FK_TET << ADJ_KIND_SHIFT);
+                tet_terms(d, d.tetInc[v.postBase + kt], body, t);
+            } else {
+                entry = v.at(k);
+                particle_terms<CLOTH>(P, d, entry, body, t);
+            }
         }
 #pragma unroll
         for (int j = 0; j < LANES / 8; j++) {

@@ -746,6 +746,17 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
         H.preList.insert(H.preList.end(), pre[b].begin(), pre[b].end());
         H.postList.insert(H.postList.end(), post[b].begin(), post[b].end());
     }
+    // tet records in incidence order: a vertex's lanes read its tets'
+    // records contiguously instead of following each entry to the record
+    H.tetInc.clear();
+    if (!H.tets.empty()) {
+        H.tetInc.assign(H.postList.size(), TetGPU{});
+        for (uint32_t b = 0; b < nb; b++)
+            for (uint32_t i = 0; i < H.postTets[b]; i++) {
+                const uint32_t q = H.staticSeg[b].z + i;
+                H.tetInc[q] = H.tets[H.postList[q] & ADJ_INDEX_MASK];
+            }
+    }
 
     H.learnIdx.clear();
     for (uint32_t b = 0; b < nb; b++)

@@ -58,6 +58,9 @@ struct HostScene {
     // tets (kind 3) at the head of each post segment: element contacts
     // (kind 4) go between them and the membranes / bends (kinds 5, 6)
     std::vector<uint32_t> postTets;
+    // every tet record once per incident vertex, at the position of its entry
+    // in postList (tets lead each body's static post segment)
+    std::vector<TetGPU> tetInc;
 
     // cloth (authored triangles): element topology and elements.  In cloth
     // scenes the post segment holds membranes and bends (kinds 5, 6) and the

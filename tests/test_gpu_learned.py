@@ -61,7 +61,13 @@ def test_inference_matches_oracle(cuda_lib, oracle_lib, n):
     y = learned.infer(p, norm, X)
     want = M.predict(p, norm, X, rounded=True)
     scale = np.abs(want).max()
-    assert np.abs(y - want).max() <= 1e-3 * scale + 1e-6
+    # the activations are rounded to BF16 (8-bit mantissa) between layers;
+    # a different FP32 accumulation order can move a rounding by one BF16
+    # ulp, so over tens of thousands of rows the largest deviation reaches a
+    # few 1e-3 of the output scale while the typical one stays far below
+    err = np.abs(y - want)
+    assert err.max() <= 3e-3 * scale + 1e-6
+    assert err.mean() <= 1e-4 * scale + 1e-7
 
 
 def test_inference_wait_gives_up_and_leaves_the_device_usable(cuda_lib):
