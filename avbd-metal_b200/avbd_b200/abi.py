@@ -192,7 +192,8 @@ EXPORTED = [
     "avbd_last_error", "avbd_snapshot_capture", "avbd_snapshot_restore",
     "avbd_snapshot_free", "avbd_debug_buffer_size", "avbd_debug_read", "avbd_set_stream",
     "avbd_set_profiling", "avbd_get_profile", "avbd_exclusive_scan_noalloc", "avbd_set_capacity_for_testing",
-    "avbd_set_warm_start_model", "avbd_set_warm_start_mode", "avbd_set_learning_capture",
+    "avbd_set_warm_start_model", "avbd_set_warm_start_mode", "avbd_set_warm_start_rigid",
+    "avbd_set_learning_capture",
     "avbd_set_residual_trace", "avbd_get_residual_trace", "avbd_mlp_param_count",
     "avbd_mlp_workspace_bytes", "avbd_mlp_gradients", "avbd_mlp_train_step", "avbd_mlp_infer", "avbd_mlp_infer_wait_timeout_for_testing",
     "avbd_build_instances", "avbd_soft_normals", "avbd_set_skin_bindings", "avbd_skin_deform",

@@ -2,8 +2,11 @@
 training with the library's BF16 tensor-core kernels, and evaluation in
 iterations-to-tolerance against the plain gamma warm start.
 
-The network (csrc/learned.cu) maps 32 per-vertex features to the correction
-the solve applies to the plain warm start.  Training runs on the GPU through
+The network (csrc/learned.cu) maps 32 per-body features to the correction
+the solve applies to the plain warm start: outputs 0-2 move a particle or a
+rigid body's centre, outputs 3-5 rotate a rigid body (arc length at its
+bounding radius); a model with `rigid=True` is applied to the rigid bodies
+too.  Training runs on the GPU through
 avbd_mlp_train_step (forward, backward and Adam are the library's kernels;
 torch only owns the device buffers).
 """
@@ -19,7 +22,8 @@ import numpy as np
 from . import abi
 from .solver import GPUSolver, load_library
 
-DIN, HID, DOUT, USED = 32, 128, 16, 3
+DIN, HID, DOUT, USED = 32, 128, 16, 6
+RING = slice(25, 28)            # 1-ring aggregates among the features
 NNORM, XM, XI, YM, YS = 96, 0, 32, 64, 80
 NPARAM = HID * DIN + HID + 2 * (HID * HID + HID) + DOUT * HID + DOUT
 
@@ -55,29 +59,41 @@ class WarmStartModel:
     params: np.ndarray
     norm: np.ndarray
     history: List[float] = field(default_factory=list)
+    rigid: bool = False            # trained on rigid-body rows as well as particles
 
     def save(self, path: str) -> None:
-        np.savez(path, params=self.params, norm=self.norm, history=np.array(self.history, np.float32))
+        np.savez(path, params=self.params, norm=self.norm, history=np.array(self.history, np.float32),
+                 rigid=np.array(self.rigid))
 
     @staticmethod
     def load(path: str) -> "WarmStartModel":
         z = np.load(path)
         return WarmStartModel(z["params"].astype(np.float32), z["norm"].astype(np.float32),
-                              list(z["history"]) if "history" in z else [])
+                              list(z["history"]) if "history" in z else [],
+                              bool(z["rigid"]) if "rigid" in z else False)
 
 
 def collect(make_scene: Callable[[int], object], seeds: Sequence[int], frames: int, skip: int = 2,
-            every: int = 1, motor_targets: Optional[Callable] = None, fraction: float = 1.0):
+            every: int = 1, motor_targets: Optional[Callable] = None, fraction: float = 1.0,
+            rigid: bool = False):
     """Roll out the plain solver on seeded scene variants and record, per
     frame, the features and the solve's correction of the plain warm start
-    (of a seeded random `fraction` of the vertices, for large scenes)."""
+    (of a seeded random `fraction` of the rows, for large scenes); with
+    `rigid` the rigid bodies' rows are recorded after the particles'.
+    `motor_targets(solver, frame)` (default: the scene's `motor_drive`, if
+    it has one) drives the scene's motors."""
     feats, targs = [], []
     rng = np.random.default_rng(12345)
     for seed in seeds:
         scene = make_scene(seed)
+        drive = motor_targets or getattr(scene, "motor_drive", None)
         g = GPUSolver(scene)
+        if rigid:
+            g.set_warm_start_rigid(True)
         g.set_learning_capture(True)
         for f in range(frames):
+            if drive is not None:
+                drive(g, f)
             g.step(1)
             if f >= skip and (f - skip) % every == 0:
                 x, t = g.learning_sample()
@@ -147,7 +163,7 @@ def gradients(params, norm, features, targets, device: int = 0):
 
 
 def infer(params, norm, features, device: int = 0) -> np.ndarray:
-    """Predictions [n][3] from the fused inference kernel."""
+    """Predictions [n][6] from the fused inference kernel."""
     import torch
     lib = load_library()
     dev = torch.device("cuda", device)
@@ -179,14 +195,17 @@ def evaluate(make_scene: Callable[[int], object], seed: int, model: Optional[War
     or the learned warm start, at `iterations` iterations per frame."""
     scene = make_scene(seed)
     scene.settings.iterations = iterations
+    drive = getattr(scene, "motor_drive", None)
     g = GPUSolver(scene)
     if model is not None:
-        g.set_warm_start_model(model.params, model.norm, trial_sweeps)
+        g.set_warm_start_model(model.params, model.norm, trial_sweeps, rigid=model.rigid)
         g.set_warm_start_mode(abi.WARM_START_LEARNED)
     g.set_residual_trace(True)
     its = {t: [] for t in tolerances}
     rel_final, rel_first = [], []
     for f in range(frames):
+        if drive is not None:
+            drive(g, f)
         g.step(1)
         if f < skip:
             continue
@@ -231,9 +250,11 @@ class _Rollout:
     evaluation (no scene rebuild per iteration count)."""
 
     def __init__(self, make_scene, seed, model, trial_sweeps):
-        self.g = GPUSolver(make_scene(seed))
+        scene = make_scene(seed)
+        self.drive = getattr(scene, "motor_drive", None)
+        self.g = GPUSolver(scene)
         if model is not None:
-            self.g.set_warm_start_model(model.params, model.norm, trial_sweeps)
+            self.g.set_warm_start_model(model.params, model.norm, trial_sweeps, rigid=model.rigid)
             self.g.set_warm_start_mode(abi.WARM_START_LEARNED)
         self.g.set_residual_trace(True)
         self.start = self.g.snapshot()
@@ -247,6 +268,8 @@ class _Rollout:
         its = {t: [] for t in tolerances}
         rel_final = []
         for f in range(frames):
+            if self.drive is not None:
+                self.drive(g, f)
             g.step(1)
             if f < skip:
                 continue
@@ -313,8 +336,34 @@ def _mixed(seed):
     return demos.mixed_scene(seed=seed)
 
 
-# scene families with a trained model (avbd_b200/models)
-SCENES = {"soft-cube": _soft_cube, "mixed": _mixed}
+class MotorDrive:
+    """Joint targets U(+-0.5 rad) for every motor, a fresh draw each frame;
+    frame f's draw depends only on (seed, f), so a rewound rollout replays
+    the same targets."""
+
+    def __init__(self, motors, seed):
+        self.ids = np.asarray(motors, np.uint32)
+        self.seed = seed
+
+    def __call__(self, solver, frame):
+        rng = np.random.default_rng((self.seed, frame))
+        solver.set_motor_targets(self.ids, rng.uniform(-0.5, 0.5, len(self.ids)).astype(np.float32))
+
+
+def _batched_worlds(seed):
+    from . import demos
+    scene, motors, _ = demos.batched_worlds_scene(worlds=4096, seed=seed)
+    scene.motor_drive = MotorDrive(motors, seed)
+    return scene
+
+
+def _rigid_stack(seed):
+    from . import demos
+    return demos.rigid_stack_scene(seed=seed)
+
+
+# scene families of the learned warm start (trained models: avbd_b200/models)
+SCENES = {"soft-cube": _soft_cube, "mixed": _mixed, "batched-worlds": _batched_worlds, "rigid-stack": _rigid_stack}
 
 
 def _main(argv=None):
@@ -334,7 +383,9 @@ def _main(argv=None):
                     help="iterations of the rollouts that give the targets (a more converged solve than the "
                          "iteration counts the model is used at)")
     ap.add_argument("--drop-ring", action="store_true",
-                    help="train without the 1-ring features (16-31): their inputs and first-layer weights are zero")
+                    help="train without the 1-ring features (25-27): their inputs and first-layer weights are zero")
+    ap.add_argument("--rigid", action="store_true",
+                    help="learn the rigid bodies' corrections as well as the particles'")
     ap.add_argument("--steps", type=int, default=6000)
     ap.add_argument("--batch", type=int, default=8192)
     ap.add_argument("--lr", type=float, default=1e-3)
@@ -347,12 +398,13 @@ def _main(argv=None):
         sc.settings.iterations = a.target_iterations
         return sc
 
-    X, T = collect(rollout_scene, a.seeds, a.frames, every=a.every, fraction=a.fraction)
+    X, T = collect(rollout_scene, a.seeds, a.frames, every=a.every, fraction=a.fraction, rigid=a.rigid)
     if a.drop_ring:
-        X[:, 16:] = 0.0
+        X[:, RING] = 0.0
     model = train(X, T, steps=a.steps, batch=a.batch, lr=a.lr)
+    model.rigid = a.rigid
     if a.drop_ring:
-        model.params[:HID * DIN].reshape(HID, DIN)[:, 16:] = 0.0
+        model.params[:HID * DIN].reshape(HID, DIN)[:, RING] = 0.0
     model.save(a.out)
     print(f"samples {len(X)}, loss {model.history[0]:.4f} -> {model.history[-1]:.4f}")
     for iters in (10, 20):

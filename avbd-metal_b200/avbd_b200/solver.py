@@ -9,6 +9,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+from typing import Optional
 
 import numpy as np
 
@@ -85,6 +86,7 @@ def load_library() -> C.CDLL:
         "avbd_get_profile": ([vp, vp], i32),
         "avbd_set_warm_start_model": ([vp, vp, vp, u32], i32),
         "avbd_set_warm_start_mode": ([vp, i32], i32),
+        "avbd_set_warm_start_rigid": ([vp, i32], i32),
         "avbd_set_learning_capture": ([vp, i32], i32),
         "avbd_set_residual_trace": ([vp, i32], i32),
         "avbd_get_residual_trace": ([vp, vp, u32], i32),
@@ -381,12 +383,20 @@ class GPUSolver:
                                          "body_count_bucket": p.dyn_bucket, "candidates_timed": p.dyn_candidates}}
 
     # ---- learned warm start ------------------------------------------------
-    def set_warm_start_model(self, params, norm, trial_sweeps: int = 1) -> None:
-        """Upload an MLP (fp32 parameter block and 96-float normalisation)."""
+    def set_warm_start_model(self, params, norm, trial_sweeps: int = 1, rigid: Optional[bool] = None) -> None:
+        """Upload an MLP (fp32 parameter block and 96-float normalisation);
+        `rigid` (when given) sets whether it predicts the rigid bodies too."""
         p = np.ascontiguousarray(params, np.float32)
         n = np.ascontiguousarray(norm, np.float32)
         self._check(load_library().avbd_set_warm_start_model(self._h, p.ctypes.data, n.ctypes.data,
                                                              int(trial_sweeps)))
+        if rigid is not None:
+            self.set_warm_start_rigid(rigid)
+
+    def set_warm_start_rigid(self, enabled: bool) -> None:
+        """Learned rows: the particles (False) or the particles and the
+        dynamic rigid bodies (True)."""
+        self._check(load_library().avbd_set_warm_start_rigid(self._h, 1 if enabled else 0))
 
     def set_warm_start_mode(self, mode: int) -> None:
         self._check(load_library().avbd_set_warm_start_mode(self._h, int(mode)))
@@ -404,9 +414,10 @@ class GPUSolver:
         return out
 
     def learning_sample(self):
-        """(features [n][32], targets [n][3]) of the last captured frame."""
+        """(features [n][32], targets [n][6]) of the last captured frame:
+        particle rows first, then the rigid bodies when they are learned."""
         f = self.debug_read("LEARN_FEATURES", np.float32).reshape(-1, 32)
-        t = self.debug_read("LEARN_TARGETS", np.float32).reshape(-1, 3)
+        t = self.debug_read("LEARN_TARGETS", np.float32).reshape(-1, 6)
         return f, t
 
     def debug_read(self, name: str, dtype=np.uint8):

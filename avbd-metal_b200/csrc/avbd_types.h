@@ -119,6 +119,9 @@ struct Params {
     // the scene has torus, capsule or convex-hull colliders (second
     // narrowphase pass)
     uint32_t roundShapes;
+    // learned warm start: particle rows lead the learned list, dynamic rigid
+    // bodies follow; learnRigid = the model predicts rigid corrections too
+    uint32_t learnParticles, learnRigid;
 };
 
 // Device counters of one frame (the reference's CTR_* layout, trimmed).

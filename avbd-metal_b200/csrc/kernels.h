@@ -123,7 +123,7 @@ struct DevPtrs {
     float *learnPrm, *learnNorm, *learnResidBodies;
     float* learnResidBodies2;                   // per-body residual scratch of the predicted branch
     float4 *learnNextLin, *learnNextAng;        // pending solves of the predicted branch (color-Jacobi scenes)
-    void* learnHalf;                            // BF16 weight mirror
+    void* learnHalf;                            // BF16 weight image of the inference kernel (UMMA layout)
     double* learnResid;                         // [0] plain, [1] predicted, [2] scratch
     double* learnTrace;                         // residual trace of the last frame
     uint32_t* learnAccepted;                    // frames whose prediction was kept (running)
@@ -138,7 +138,8 @@ struct Sizes {
     // cloth
     uint32_t numTris, numParticles, numEdges, numMembranes, numBends;
     uint32_t maxDatPairs, maxSoft, elemHashSize;
-    uint32_t numLearn;
+    uint32_t numLearn;        // learned rows in use (particles, plus rigid bodies with learnRigid)
+    uint32_t numLearnAll;     // learned rows allocated: every dynamic particle and rigid body
     uint32_t numDynamicRigid;
     uint32_t numHeavyProducers;
     // static palette on the host (null with dynamic coloring)

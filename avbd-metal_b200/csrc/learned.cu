@@ -5,14 +5,21 @@
 //
 // The MLP predicts the correction the solve applies to the plain warm start
 // of every dynamic particle, in units of s = max(|g|, 1) dt^2:
-//   x0 = x_plain + s * MLP(features).
+//   x0 = x_plain + s * MLP(features)[0-2],
+// and, when the model covers rigid bodies (Params::learnRigid), of every
+// dynamic rigid body's pose, the rotation as the arc length it sweeps at the
+// body's bounding radius r:
+//   q0 = q_plain (+) (s / r) * MLP(features)[3-5]   (q_addw, tangent space).
+// Learned rows list the particles first, then the rigid bodies.
 // Features (32, normalised by per-feature mean and 1/std stored with the
 // model): [0-2] inertial offset (x~ - x_start)/s, [3-5] plain warm-start
 // offset (x_plain - x_start)/s, [6-8] previous-frame displacement
 // v_prev dt / s, [9] incident contact count / 4, [10-12] summed oriented
 // contact normal, [13] smallest contact gap / s (clipped), [14] log(1 +
-// stiffness dt^2 / m) of the incident elements, [15] 1; [16-24] reserved
-// zeros; 1-ring aggregates over the vertices sharing a tet or spring: [25]
+// stiffness dt^2 / m) of the incident elements, [15] 1; rigid rows only
+// (zeros for particles): [16] 1, [17-19] plain warm-start rotation
+// q_sub(q_plain, q_start) r / s, [20-22] world up axis in the body frame,
+// [23] log(1 + r / s) / 10, [24] reserved zero; 1-ring aggregates over the vertices sharing a tet or spring: [25]
 // ring size / 10, [26] mean neighbour contact count / 4, [27] smallest
 // neighbour contact gap / s (clipped); [28-31] reserved zeros.  Contacts are
 // rigid manifolds and element contacts alike.
@@ -23,6 +30,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "../../include/avbd.h"
 #include "dmath.cuh"
@@ -31,7 +39,7 @@
 namespace avbd {
 
 namespace mlp {
-constexpr int DIN = 32, HID = 128, DOUT = 16, USED_OUT = 3;
+constexpr int DIN = 32, HID = 128, DOUT = 16, USED_OUT = 6;
 constexpr uint32_t OW1 = 0, OB1 = OW1 + HID * DIN, OW2 = OB1 + HID, OB2 = OW2 + HID * HID, OW3 = OB2 + HID,
                    OB3 = OW3 + HID * HID, OW4 = OB3 + HID, OB4 = OW4 + DOUT * HID, NPARAM = OB4 + DOUT;
 // bf16 weight mirror: W1 | W2 | W3 | W4
@@ -64,11 +72,12 @@ __device__ __forceinline__ uint32_t ld_pair(const bf16* p) { return *reinterpret
 
 // ---------------------------------------------------------------------------
 // Fused inference on the Blackwell tensor cores (tcgen05): one CTA of four
-// warps per 128-row tile, persistent over the batch.  The weights are staged
-// once per CTA in shared memory in the UMMA canonical K-major layout without
-// swizzle (8-row x 16-byte core matrices: element (r, k) of an operand with
-// row-group stride `sbo` at (r / 8) sbo + (k / 8) 128 + (r % 8) 16 + (k % 8) 2
-// bytes); a layer is 2 (K = 32) or 8 (K = 128) tcgen05.mma instructions of
+// warps per 128-row tile, persistent over the batch.  The weights live in
+// global memory as an image of their shared-memory form — the UMMA canonical
+// K-major layout without swizzle (8-row x 16-byte core matrices: element
+// (r, k) of an operand with row-group stride `sbo` at (r / 8) sbo + (k / 8)
+// 128 + (r % 8) 16 + (k % 8) 2 bytes) — and each CTA stages them once with
+// bulk asynchronous copies completing on an mbarrier; a layer is 2 (K = 32) or 8 (K = 128) tcgen05.mma instructions of
 // M = 128, K = 16, issued by one thread, accumulating in TMEM (128 lanes =
 // the tile's rows, N fp32 columns); each warp reads its 32 rows back with
 // tcgen05.ld, adds the bias, applies ReLU, rounds to BF16 and writes the next
@@ -80,7 +89,9 @@ namespace tc {
 constexpr uint32_t ROWS = 128;
 constexpr uint32_t SBO_K128 = 2048, SBO_K32 = 512;      // row-group strides (K = 128, K = 32)
 constexpr uint32_t W1 = 0, W2 = W1 + 128 * 32 * 2, W3 = W2 + 128 * 128 * 2, W4 = W3 + 128 * 128 * 2,
-                   ACT = W4 + 16 * 128 * 2, BAR = ACT + ROWS * 128 * 2, TSLOT = BAR + 8, SMEM = TSLOT + 8;
+                   ACT = W4 + 16 * 128 * 2, BAR = ACT + ROWS * 128 * 2, WBAR = BAR + 8, TSLOT = WBAR + 8,
+                   SMEM = TSLOT + 8;
+constexpr uint32_t WBYTES = ACT - W1;                    // the weight image: 77,824 bytes
 constexpr uint32_t TMEM_COLS = 128;
 constexpr uint64_t WAIT_NS = 1000000000ull;              // a wait gives up after one second
 
@@ -132,6 +143,16 @@ __device__ __forceinline__ bool wait(uint32_t bar, uint32_t parity) {
     }
     return false;
 }
+// bulk asynchronous copy global -> this CTA's shared memory (no multicast),
+// completing `bytes` of the barrier's transaction count
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -171,21 +192,19 @@ __global__ void __launch_bounds__(128) k_mlp_infer_tc(const bf16* __restrict__ W
     extern __shared__ __align__(128) unsigned char sm[];
     const uint32_t t = threadIdx.x, warp = t >> 5;
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
-    const uint32_t bar = sbase + tc::BAR;
-    // weights -> canonical K-major core matrices, 16 bytes per thread-step
-    auto stage = [&](uint32_t dst, uint32_t src, uint32_t rows, uint32_t cols, uint32_t sbo) {
-        const uint32_t chunks = rows * (cols / 8);
-        for (uint32_t c = t; c < chunks; c += blockDim.x) {
-            const uint32_t r = c / (cols / 8), k = (c % (cols / 8)) * 8;
-            *reinterpret_cast<uint4*>(sm + dst + tc::off(r, k, sbo)) =
-                *reinterpret_cast<const uint4*>(W + src + r * cols + k);
-        }
-    };
-    stage(tc::W1, HW1, HID, DIN, tc::SBO_K32);
-    stage(tc::W2, HW2, HID, HID, tc::SBO_K128);
-    stage(tc::W3, HW3, HID, HID, tc::SBO_K128);
-    stage(tc::W4, HW4, DOUT, HID, tc::SBO_K128);
-    if (t == 0) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    const uint32_t bar = sbase + tc::BAR, wbar = sbase + tc::WBAR;
+    // the weight image (already in the canonical layout) in four bulk copies
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(wbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        tc::expect_tx(wbar, tc::WBYTES);
+        const unsigned char* img = reinterpret_cast<const unsigned char*>(W);
+        tc::bulk_load(sbase + tc::W1, img + tc::W1, tc::W2 - tc::W1, wbar);
+        tc::bulk_load(sbase + tc::W2, img + tc::W2, tc::W3 - tc::W2, wbar);
+        tc::bulk_load(sbase + tc::W3, img + tc::W3, tc::W4 - tc::W3, wbar);
+        tc::bulk_load(sbase + tc::W4, img + tc::W4, tc::ACT - tc::W4, wbar);
+    }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + tc::TSLOT),
                      "r"(tc::TMEM_COLS)
@@ -199,20 +218,27 @@ __global__ void __launch_bounds__(128) k_mlp_infer_tc(const bf16* __restrict__ W
     const uint32_t lane_addr = tmem + ((warp * 32u) << 16);   // this warp's 32 TMEM lanes
     const uint32_t row = t;                                    // tile row held by this thread
     uint32_t phase = 0;
-    bool ok = true;
+    // the weights have landed (bounded wait; block-uniform outcome)
+    bool ok = __syncthreads_and(tc::wait(wbar, 0) ? 1 : 0) != 0;
+    if (!ok) tc::wait(wbar, 0);        // give copies still in flight one more bounded wait
     const uint32_t tiles = (n + tc::ROWS - 1) / tc::ROWS;
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const uint32_t r = tile * tc::ROWS + row;
-        // layer-1 operand: normalised features, BF16
+        // layer-1 operand: normalised features, BF16 (the row's 128 bytes as
+        // eight 16-byte loads, all in flight together)
+        float4 xr[DIN / 4];
+#pragma unroll
+        for (uint32_t q = 0; q < DIN / 4; q++)
+            xr[q] = r < n ? reinterpret_cast<const float4*>(X + (size_t)r * DIN)[q] : make_float4(0, 0, 0, 0);
 #pragma unroll
         for (uint32_t kg = 0; kg < DIN / 8; kg++) {
+            const float* xv = reinterpret_cast<const float*>(&xr[2 * kg]);
             uint32_t w[4];
 #pragma unroll
             for (int e = 0; e < 4; e++) {
                 const uint32_t c = kg * 8 + 2 * e;
-                const float a = r < n ? (X[(size_t)r * DIN + c] - norm[NX_MEAN + c]) * norm[NX_INV + c] : 0.0f;
-                const float b = r < n ? (X[(size_t)r * DIN + c + 1] - norm[NX_MEAN + c + 1]) * norm[NX_INV + c + 1]
-                                      : 0.0f;
+                const float a = r < n ? (xv[2 * e] - norm[NX_MEAN + c]) * norm[NX_INV + c] : 0.0f;
+                const float b = r < n ? (xv[2 * e + 1] - norm[NX_MEAN + c + 1]) * norm[NX_INV + c + 1] : 0.0f;
                 w[e] = pack_bf16(a, b);
             }
             *reinterpret_cast<uint4*>(sm + tc::ACT + tc::off(row, kg * 8, tc::SBO_K128)) = make_uint4(w[0], w[1], w[2], w[3]);
@@ -461,6 +487,21 @@ __global__ void k_mirror(const float* prm, bf16* half) {
     if (h >= 0) half[h] = __float2bfloat16(prm[i]);
 }
 
+// BF16 weight image of the inference kernel: W1..W4 in the UMMA canonical
+// K-major layout, byte for byte the kernel's shared-memory weight region.
+__global__ void k_mirror_umma(const float* prm, unsigned char* img) {
+    using namespace mlp;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= NHALF) return;
+    uint32_t src, base, cols, sbo, j;
+    if (i < HW2) { j = i - HW1; src = OW1; base = tc::W1; cols = DIN; sbo = tc::SBO_K32; }
+    else if (i < HW3) { j = i - HW2; src = OW2; base = tc::W2; cols = HID; sbo = tc::SBO_K128; }
+    else if (i < HW4) { j = i - HW3; src = OW3; base = tc::W3; cols = HID; sbo = tc::SBO_K128; }
+    else { j = i - HW4; src = OW4; base = tc::W4; cols = HID; sbo = tc::SBO_K128; }
+    const uint32_t r = j / cols, k = j % cols;
+    *reinterpret_cast<bf16*>(img + base + tc::off(r, k, sbo)) = __float2bfloat16(prm[src + j]);
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -557,6 +598,21 @@ namespace {
 
 __device__ __forceinline__ float step_scale(const Params& P) { return fmaxf(fabsf(P.gravity), 1.0f) * P.dt * P.dt; }
 
+// bounding radius of a rigid body (the rotation's length scale)
+__device__ __forceinline__ float learn_radius(const DevPtrs& d, uint32_t v) { return fmaxf(d.shape[v].w, 1e-6f); }
+
+// Pose of learned row i moved by its prediction y from the plain warm start
+// (xp, qp).  A zero rotation prediction keeps qp bit for bit.
+__device__ __forceinline__ void learn_pose(const Params& P, const DevPtrs& d, uint32_t i, uint32_t v, float4 xp,
+                                           float4 qp, float4& x, float4& q) {
+    const float s = step_scale(P);
+    const float* y = d.learnPred + (size_t)i * mlp::USED_OUT;
+    x = mk4(xyz(xp) + mk3(y[0], y[1], y[2]) * s, xp.w);
+    q = qp;
+    if (i >= P.learnParticles && (y[3] != 0.0f || y[4] != 0.0f || y[5] != 0.0f))
+        q = q_addw(qp, mk3(y[3], y[4], y[5]) * (s / learn_radius(d, v)));
+}
+
 // Per-vertex features at the plain warm start (see the file comment).  The
 // contact features walk the body's per-frame segment (manifolds, element
 // contacts), the stiffness feature its static segments (springs; tets,
@@ -623,7 +679,17 @@ __global__ void k_learn_features(const Params P, const DevPtrs d, uint32_t n) {
     }
     const float inv = ringN > 0.0f ? 1.0f / ringN : 0.0f;
     float* f = d.learnFeat + (size_t)i * mlp::DIN;
-    for (int k = 16; k < 25; k++) f[k] = 0.0f;          // reserved
+    for (int k = 16; k < 25; k++) f[k] = 0.0f;          // rigid slots, reserved
+    if (i >= P.learnParticles) {
+        const float r = learn_radius(d, v);
+        const float4 q = d.posAng[v];
+        const float3 wq = q_sub(q, d.initAng[v]) * (r / s);
+        const float3 up = q_rotate(q_conj(q), mk3(0, 0, 1));
+        f[16] = 1.0f;
+        f[17] = wq.x; f[18] = wq.y; f[19] = wq.z;
+        f[20] = up.x; f[21] = up.y; f[22] = up.z;
+        f[23] = 0.1f * log1pf(r / s);
+    }
     f[25] = ringN * 0.1f;
     f[26] = ringContacts * inv * 0.25f;
     f[27] = ringContacts > 0.0f ? fminf(fmaxf(ringGap / s, -10.0f), 10.0f) : 10.0f;
@@ -638,15 +704,12 @@ __global__ void k_learn_features(const Params P, const DevPtrs d, uint32_t n) {
     f[15] = 1.0f;
 }
 
-// x0 = x_plain + s * prediction for every learned vertex
+// x0 = x_plain + s * prediction for every learned row
 __global__ void k_learn_apply(const Params P, const DevPtrs d, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t v = d.learnIdx[i];
-    const float s = step_scale(P);
-    const float4 xp = d.learnSaveLin[v];
-    const float* y = d.learnPred + (size_t)i * mlp::USED_OUT;
-    d.posLin[v] = mk4(xyz(xp) + mk3(y[0], y[1], y[2]) * s, xp.w);
+    learn_pose(P, d, i, v, d.learnSaveLin[v], d.learnSaveAng[v], d.posLin[v], d.posAng[v]);
 }
 
 // keep the prediction when its residual after the trial sweeps is no worse
@@ -656,26 +719,21 @@ __global__ void k_learn_select(const Params P, const DevPtrs d, uint32_t n) {
     if (i == 0 && accept) atomicAdd(d.learnAccepted, 1u);
     if (i >= n || !accept) return;
     const uint32_t v = d.learnIdx[i];
-    const float s = step_scale(P);
-    const float4 xp = d.learnSaveLin[v];
-    const float* y = d.learnPred + (size_t)i * mlp::USED_OUT;
-    d.posLin[v] = mk4(xyz(xp) + mk3(y[0], y[1], y[2]) * s, xp.w);
+    learn_pose(P, d, i, v, d.learnSaveLin[v], d.learnSaveAng[v], d.posLin[v], d.posAng[v]);
 }
 
 // Pose buffers of the predicted branch: the solver's pose with every
-// learned vertex moved to x_plain + s * prediction.
-__global__ void k_learn_branch(const Params P, const DevPtrs d, uint32_t nb) {
+// learned row (the first n slots) moved by its prediction.
+__global__ void k_learn_branch(const Params P, const DevPtrs d, uint32_t nb, uint32_t n) {
     const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
-    const float4 x = d.posLin[b];
     const uint32_t slot = d.learnSlot[b];
-    if (slot != 0xFFFFFFFFu) {
-        const float* y = d.learnPred + (size_t)slot * mlp::USED_OUT;
-        d.learnSweptLin[b] = mk4(xyz(x) + mk3(y[0], y[1], y[2]) * step_scale(P), x.w);
+    if (slot < n) {
+        learn_pose(P, d, slot, b, d.posLin[b], d.posAng[b], d.learnSweptLin[b], d.learnSweptAng[b]);
     } else {
-        d.learnSweptLin[b] = x;
+        d.learnSweptLin[b] = d.posLin[b];
+        d.learnSweptAng[b] = d.posAng[b];
     }
-    d.learnSweptAng[b] = d.posAng[b];
 }
 
 // After both trial sweeps: adopt the predicted branch's swept pose when its
@@ -692,15 +750,19 @@ __global__ void k_learn_adopt(const Params P, const DevPtrs d, uint32_t nb) {
     d.posAng[b] = d.learnSweptAng[b];
 }
 
-// training target: the solve's correction of the plain warm start
+// training target: the solve's correction of the plain warm start (the
+// rotation part zero for particles)
 __global__ void k_learn_target(const Params P, const DevPtrs d, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t v = d.learnIdx[i];
     const float s = step_scale(P);
     const float3 t = (xyz(d.posLin[v]) - xyz(d.learnSaveLin[v])) / s;
+    const float3 w = i >= P.learnParticles ? q_sub(d.posAng[v], d.learnSaveAng[v]) * (learn_radius(d, v) / s)
+                                           : s3(0.0f);
     float* y = d.learnTarget + (size_t)i * mlp::USED_OUT;
     y[0] = t.x; y[1] = t.y; y[2] = t.z;
+    y[3] = w.x; y[4] = w.y; y[5] = w.z;
 }
 
 __global__ void k_copy_double(const double* src, double* dst) {
@@ -721,7 +783,7 @@ void launch_learn_select(const Params& P, const DevPtrs& d, const Sizes& z, cuda
     k_learn_select<<<(z.numLearn + 128) / 128, 128, 0, st>>>(P, d, z.numLearn);
 }
 void launch_learn_branch(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
-    k_learn_branch<<<(z.numBodies + 127) / 128, 128, 0, st>>>(P, d, z.numBodies);
+    k_learn_branch<<<(z.numBodies + 127) / 128, 128, 0, st>>>(P, d, z.numBodies, z.numLearn);
 }
 void launch_learn_adopt(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     k_learn_adopt<<<(z.numBodies + 127) / 128, 128, 0, st>>>(P, d, z.numBodies);
@@ -731,14 +793,21 @@ void launch_learn_target(const Params& P, const DevPtrs& d, const Sizes& z, cuda
 }
 void launch_copy_double(const double* src, double* dst, cudaStream_t st) { k_copy_double<<<1, 32, 0, st>>>(src, dst); }
 
+// weights + one activation tile: 108 KiB of shared memory (set once per device)
+static void mlp_infer_attributes() {
+    static std::atomic<uint64_t> done{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load() & bit) return;
+    cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM);
+    done.fetch_or(bit);
+}
+
 void launch_mlp_infer(const void* halfW, const float* prm, const float* norm, const float* X, uint32_t n, float* Y,
                       uint32_t* status, cudaStream_t st) {
     if (n == 0) return;
-    static bool attr = false;     // weights + one activation tile: 108 KiB of shared memory
-    if (!attr) {
-        cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM);
-        attr = true;
-    }
+    mlp_infer_attributes();
     // two CTAs per SM (108 KiB of shared memory and 128 TMEM columns each),
     // every CTA walking 128-row tiles
     const uint32_t tiles = (n + tc::ROWS - 1) / tc::ROWS;
@@ -747,7 +816,7 @@ void launch_mlp_infer(const void* halfW, const float* prm, const float* norm, co
 }
 
 void launch_mlp_mirror(const float* prm, void* halfW, cudaStream_t st) {
-    k_mirror<<<blocks(mlp::NPARAM, 256), 256, 0, st>>>(prm, static_cast<bf16*>(halfW));
+    k_mirror_umma<<<blocks(mlp::NHALF, 256), 256, 0, st>>>(prm, static_cast<unsigned char*>(halfW));
 }
 
 uint32_t mlp_param_count() { return mlp::NPARAM; }
@@ -798,6 +867,9 @@ int avbd_mlp_train_step(float* params, const float* norm, const float* features,
 static int mlp_infer(const float* params, const float* norm, const float* features, uint32_t n, float* out,
                      void* workspace, void* stream, bool issue) {
     if (!params || !norm || !features || !out || !workspace) return AVBD_ERR_INVALID_ARGUMENT;
+    // bulk copies read the weight image and the feature rows in 16-byte units
+    if ((reinterpret_cast<uintptr_t>(workspace) | reinterpret_cast<uintptr_t>(features)) & 15u)
+        return AVBD_ERR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // the BF16 weight mirror, then the kernel's status word
     uint32_t* status = reinterpret_cast<uint32_t*>(static_cast<char*>(workspace) +
@@ -807,7 +879,7 @@ static int mlp_infer(const float* params, const float* norm, const float* featur
     if (issue) {
         launch_mlp_infer(workspace, params, norm, features, n, out, status, st);
     } else if (n) {
-        cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM);
+        mlp_infer_attributes();
         k_mlp_infer_tc<<<1, 128, tc::SMEM, st>>>(static_cast<const bf16*>(workspace), params, norm, features, n, out,
                                                  status, false);
     }

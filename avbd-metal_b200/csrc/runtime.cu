@@ -499,7 +499,8 @@ struct avbd_solver {
         z.maxDatPairs = H.maxDatPairs;
         z.maxSoft = P.maxSoft;
         z.elemHashSize = H.elemHashSize;
-        z.numLearn = P.cloth ? 0u : (uint32_t)H.learnIdx.size();
+        z.numLearnAll = P.cloth ? 0u : (uint32_t)H.learnIdx.size();
+        z.numLearn = P.cloth ? 0u : P.learnParticles;
         z.colorCounts = H.dynamicColoring ? nullptr : H.colorCounts.data();
         z.colorLanes = H.colorLanes.data();
         z.numDynamicRigid = 0;
@@ -597,8 +598,8 @@ struct avbd_solver {
         if (H.dynamicColoring)
             d.colorStart = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(d.counters) + offsetof(Counters, colorStart));
         if (ok) d.ogcExceed = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(d.counters) + offsetof(Counters, ogcSlots));
-        if (z.numLearn) {
-            const uint32_t nl = z.numLearn;
+        if (z.numLearnAll) {
+            const uint32_t nl = z.numLearnAll;
             ok = ok && upload(d.learnIdx, H.learnIdx, "learnIdx");
             std::vector<uint32_t> slot(nb, 0xFFFFFFFFu);
             for (uint32_t i = 0; i < nl; i++) slot[H.learnIdx[i]] = i;
@@ -647,8 +648,8 @@ struct avbd_solver {
             ok = ok && upload(d.learnStiff, stiff, "learnStiffness") && upload(d.learnRingN, ringN, "learnRingSize");
             ok = ok && upload(d.learnRingStart, ringStart, "learnRingStart") && upload(d.learnRing, ring, "learnRing");
             ok = ok && alloc(d.learnStat, nl, "learnContactState") && alloc(d.learnGap, nl, "learnContactGap");
-            ok = ok && alloc(d.learnFeat, 32 * (size_t)nl, "learnFeatures") && alloc(d.learnPred, 3 * (size_t)nl, "learnPrediction");
-            ok = ok && alloc(d.learnTarget, 3 * (size_t)nl, "learnTarget");
+            ok = ok && alloc(d.learnFeat, 32 * (size_t)nl, "learnFeatures") && alloc(d.learnPred, 6 * (size_t)nl, "learnPrediction");
+            ok = ok && alloc(d.learnTarget, 6 * (size_t)nl, "learnTarget");
             ok = ok && alloc(d.learnPrm, mlp_param_count(), "mlpParams") && alloc(d.learnNorm, mlp_norm_count(), "mlpNorm");
             uint16_t* half = nullptr;
             ok = ok && alloc(half, mlp_half_count(), "mlpWeightsBF16");
@@ -658,7 +659,7 @@ struct avbd_solver {
         ok = ok && alloc(d.learnSweptLin, nb, "plainTrialLin") && alloc(d.learnSweptAng, nb, "plainTrialAng");
         ok = ok && alloc(d.learnResidBodies, std::max<uint32_t>(1, H.numDynamicBodies), "residualBodies");
         ok = ok && alloc(d.learnResidBodies2, std::max<uint32_t>(1, H.numDynamicBodies), "residualBodiesBranch");
-        if (z.numLearn && P.colorJacobi)
+        if (z.numLearnAll && P.colorJacobi)
             ok = ok && alloc(d.learnNextLin, nb, "branchNextLin") && alloc(d.learnNextAng, nb, "branchNextAng");
         ok = ok && alloc(d.learnResid, 4, "residual") && alloc(d.learnTrace, kTraceLength, "residualTrace");
         ok = ok && alloc(d.learnAccepted, 1, "learnAccepted", true);
@@ -1565,8 +1566,8 @@ int avbd_get_counters(avbd_solver* s, avbd_counters* out) {
 
 int avbd_set_warm_start_model(avbd_solver* s, const float* params, const float* norm, uint32_t trial_sweeps) {
     if (!s || !params || !norm || trial_sweeps > 16) return AVBD_ERR_INVALID_ARGUMENT;
-    if (s->z.numLearn == 0) {
-        s->error = "the scene has no dynamic particles for the learned warm start (cloth is not supported)";
+    if (s->z.numLearnAll == 0) {
+        s->error = "the scene has no dynamic bodies for the learned warm start (cloth is not supported)";
         return AVBD_ERR_UNSUPPORTED;
     }
     int rc = s->retire();
@@ -1589,6 +1590,10 @@ int avbd_set_warm_start_mode(avbd_solver* s, int mode) {
         s->error = "no warm-start model: call avbd_set_warm_start_model first";
         return AVBD_ERR_INVALID_ARGUMENT;
     }
+    if (mode == AVBD_WARM_START_LEARNED && s->z.numLearn == 0) {
+        s->error = "the learned rows cover no body of this scene (rigid bodies need avbd_set_warm_start_rigid)";
+        return AVBD_ERR_UNSUPPORTED;
+    }
     s->learnMode = mode;
     s->update_small_solve();
     s->graphsValid = false;
@@ -1598,10 +1603,29 @@ int avbd_set_warm_start_mode(avbd_solver* s, int mode) {
 int avbd_set_learning_capture(avbd_solver* s, int enabled) {
     if (!s) return AVBD_ERR_INVALID_ARGUMENT;
     if (enabled && s->z.numLearn == 0) {
-        s->error = "the scene has no dynamic particles to learn from";
+        s->error = "the learned rows cover no body of this scene (rigid bodies need avbd_set_warm_start_rigid)";
         return AVBD_ERR_UNSUPPORTED;
     }
     s->learnCapture = enabled != 0;
+    s->update_small_solve();
+    s->graphsValid = false;
+    return AVBD_OK;
+}
+
+int avbd_set_warm_start_rigid(avbd_solver* s, int enabled) {
+    if (!s) return AVBD_ERR_INVALID_ARGUMENT;
+    if (s->z.numLearnAll == 0) {
+        s->error = "the scene has no dynamic bodies for the learned warm start (cloth is not supported)";
+        return AVBD_ERR_UNSUPPORTED;
+    }
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    s->P.learnRigid = enabled ? 1u : 0u;
+    s->z.numLearn = enabled ? s->z.numLearnAll : s->P.learnParticles;
+    if (s->z.numLearn == 0) {    // a rigid-only scene without rigid rows: learning and the learned mode stop
+        s->learnCapture = false;
+        if (s->learnMode == AVBD_WARM_START_LEARNED) s->learnMode = AVBD_WARM_START_PLAIN;
+    }
     s->update_small_solve();
     s->graphsValid = false;
     return AVBD_OK;
@@ -1756,7 +1780,7 @@ size_t avbd_debug_buffer_size(avbd_solver* s, int which) {
     case AVBD_BUF_OGC_PREV: return (s->P.cloth || s->P.ogc) ? nb * 16 : 0;
     case AVBD_BUF_LEARN_IDX: return (size_t)s->z.numLearn * 4;
     case AVBD_BUF_LEARN_FEATURES: return (size_t)s->z.numLearn * 128;
-    case AVBD_BUF_LEARN_TARGETS: case AVBD_BUF_LEARN_PREDICTIONS: return (size_t)s->z.numLearn * 12;
+    case AVBD_BUF_LEARN_TARGETS: case AVBD_BUF_LEARN_PREDICTIONS: return (size_t)s->z.numLearn * 24;
     case AVBD_BUF_SOFT: case AVBD_BUF_DAT_PAIRS: {
         if (!s->P.cloth && !(s->P.ogc && which == AVBD_BUF_SOFT)) return 0;
         Counters c{};

@@ -761,9 +761,15 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
             }
     }
 
+    // learned warm start rows: every dynamic particle, then every dynamic
+    // rigid body (3-DOF and 6-DOF corrections)
     H.learnIdx.clear();
     for (uint32_t b = 0; b < nb; b++)
         if (s->bodies[b].is_particle && H.posLin[b].w > 0.0f) H.learnIdx.push_back(b);
+    H.P.learnParticles = (uint32_t)H.learnIdx.size();
+    for (uint32_t b = 0; b < nb; b++)
+        if (!s->bodies[b].is_particle && H.posLin[b].w > 0.0f) H.learnIdx.push_back(b);
+    H.P.learnRigid = 0;
 
     // ---- spinners and parameters (GPUSolver.swift:630-637, :2052-2080)
     H.spinners.assign(s->spinners, s->spinners + s->num_spinners);

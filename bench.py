@@ -103,6 +103,9 @@ def parse():
     ap.add_argument("--pusht-obs", action="store_true",
                     help="time the Push-T pixel-observation kernel instead (--obs-envs x --obs-res^2 x 3 "
                          "bytes per launch) and print its own JSON line")
+    ap.add_argument("--mlp-rows", type=int, default=0,
+                    help="time the warm-start MLP inference kernel instead on this many feature rows "
+                         "(77,824 FLOP a row) and print its own JSON line")
     ap.add_argument("--obs-envs", type=int, default=4096)
     ap.add_argument("--obs-res", type=int, default=64)
     args = ap.parse_args()
@@ -383,7 +386,7 @@ def learned_comparison(args, world, dev, stream, flush, plain_ms):
         st.iterations = k
         solver.settings = st
         if use_model:
-            solver.set_warm_start_model(model.params, model.norm, 1)
+            solver.set_warm_start_model(model.params, model.norm, 1, rigid=model.rigid)
             solver.set_warm_start_mode(abi.WARM_START_LEARNED)
         for i in range(args.warmup):
             targets.apply(solver, args.preroll + i)
@@ -412,8 +415,10 @@ def learned_comparison(args, world, dev, stream, flush, plain_ms):
         "learned": {"iterations": cmp["learned_iterations"], "median_rel_residual": cmp["learned_residual"],
                     "value": v_learned, "ms_per_step": ms_learned / args.steps,
                     "accepted_frames_in_timed_window": accepted / float(args.steps),
-                    "warm_start": "32-128-128-128-3 MLP, BF16 tensor-core inference; kept only when its residual "
-                                  "after 1 trial sweep is no worse than the plain warm start's"},
+                    "warm_start": "32-128-128-128-16 MLP (6 outputs used: centre and, for rigid bodies, rotation), "
+                                  "BF16 tcgen05 inference; kept only when its residual after 1 trial sweep is "
+                                  "no worse than the plain warm start's",
+                    "rows": "particles and rigid bodies" if model.rigid else "particles"},
         "speedup_vs_smallest_plain": v_learned / v_plain_min,
         "iterations_to_tolerance_median": cmp["iterations_to_tolerance"],
         "claim_holds": bool(cmp["learned_iterations"] < k_plain and v_learned > v_plain_min),
@@ -435,7 +440,7 @@ def run_frames(args, local):
     solver = GPUSolver(scene, device=local)
     if args.warm_start == "learned":
         model = learned.WarmStartModel.load(model_path())
-        solver.set_warm_start_model(model.params, model.norm, 1)
+        solver.set_warm_start_model(model.params, model.norm, 1, rigid=model.rigid)
         solver.set_warm_start_mode(abi.WARM_START_LEARNED)
     targets = MotorTargets(args.preroll + args.warmup + args.steps)
     preroll(solver, targets, args.preroll + args.warmup)
@@ -486,6 +491,64 @@ def run_pusht_obs(args, local):
                       "launches": args.steps, "ms_per_launch": ms, "achieved_gbs": nbytes / ms / 1e6,
                       "peak_gbs": peak, "peak_kind": kind, "frac": nbytes / ms / 1e6 / peak}), flush=True)
     solver.close()
+
+
+def run_mlp_infer(args, local):
+    """The learned warm start's MLP inference (tcgen05) alone on --mlp-rows
+    seeded feature rows resident in HBM, --steps back-to-back calls of
+    avbd_mlp_infer timed with CUDA events on one stream.  A call is the
+    weight-image kernel (77,824 B), the inference kernel and a 4-byte status
+    read; the FLOPs counted are the network's dense products only:
+    2 (32 x 128 + 2 x 128 x 128 + 128 x 16) = 77,824 per row."""
+    import numpy as np
+    import torch
+    from avbd_b200 import learned
+    from avbd_b200.solver import load_library
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.mlp_rows
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(3)
+    X = torch.randn((n, learned.DIN), generator=gen, device=dev, dtype=torch.float32)
+    Y = torch.empty((n, learned.USED), device=dev, dtype=torch.float32)
+    prm = torch.from_numpy(learned.init_params(seed=1)).to(dev)
+    norm = np.zeros(learned.NNORM, np.float32)
+    norm[learned.XI:learned.XI + learned.DIN] = 1.0
+    norm[learned.YS:learned.NNORM] = 1.0
+    nrm = torch.from_numpy(norm).to(dev)
+    ws = torch.empty(1 << 17, dtype=torch.uint8, device=dev)
+    lib = load_library()
+    stream = torch.cuda.Stream(device=dev)
+    h = stream.cuda_stream
+
+    def call():
+        rc = lib.avbd_mlp_infer(prm.data_ptr(), nrm.data_ptr(), X.data_ptr(), n, Y.data_ptr(), ws.data_ptr(), h)
+        if rc != 0:
+            raise RuntimeError(f"avbd_mlp_infer failed: {rc}")
+
+    for _ in range(max(3, args.warmup)):
+        call()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(args.steps):
+        call()
+    b.record(stream)
+    torch.cuda.synchronize()
+    clock = clocks.stop()
+    ms = a.elapsed_time(b) / args.steps
+    flops = 77824.0 * n
+    with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+        peaks = json.load(f)
+    assert torch.isfinite(Y).all().item()
+    tflops = flops / ms / 1e9
+    print(json.dumps({"workload": "mlp-infer", "rows": n, "flop_per_call": flops, "calls": args.steps,
+                      "ms_per_call": ms, "achieved_tflops": tflops,
+                      "peak_tflops": peaks["bf16_tflops"], "peak_kind": "measured bf16 burst",
+                      "frac": tflops / peaks["bf16_tflops"], "input_bytes": n * 128,
+                      "clocks": clock}), flush=True)
 
 
 def run_ours(args, world, rank, local):
@@ -643,6 +706,8 @@ def main():
             run_reference(args, world, rank)
         elif args.pusht_obs:
             run_pusht_obs(args, local)
+        elif args.mlp_rows:
+            run_mlp_infer(args, local)
         elif args.frames_only:
             run_frames(args, local)
         else:

@@ -398,7 +398,10 @@ int avbd_set_capacity_for_testing(avbd_solver* solver, int which, uint32_t value
 /* ---- Learned warm start (no counterpart in the reference) -------------
  * A 32-128-128-128-16 MLP (BF16 weights/activations, FP32 accumulation)
  * predicts each dynamic particle's correction of the plain gamma warm start
- * from local features.  In AVBD_WARM_START_LEARNED mode every frame races
+ * from local features (outputs 0-2, in units of s = max(|g|, 1) dt^2) and,
+ * after avbd_set_warm_start_rigid(solver, 1), each dynamic rigid body's
+ * (outputs 3-5: the rotation as arc length at the body's bounding radius,
+ * in the same units).  In AVBD_WARM_START_LEARNED mode every frame races
  * the plain and the predicted warm start for `trial_sweeps` primal sweeps and
  * keeps the prediction only when its augmented-Lagrangian residual is no
  * larger; plain AVBD stays the fallback.  trial_sweeps = 0 compares the
@@ -411,8 +414,13 @@ enum { AVBD_WARM_START_PLAIN = 0, AVBD_WARM_START_LEARNED = 1 };
 int avbd_set_warm_start_model(avbd_solver* solver, const float* params, const float* norm,
                               uint32_t trial_sweeps);
 int avbd_set_warm_start_mode(avbd_solver* solver, int mode);
-/* Record every frame's features [n][32] and training targets (the solve's
- * correction of the plain warm start) in the LEARN_* debug buffers.       */
+/* Learned rows: the dynamic particles (enabled = 0, the default) or the
+ * particles followed by the dynamic rigid bodies (enabled = 1).  On a scene
+ * without particles, learning and the learned mode need enabled = 1.      */
+int avbd_set_warm_start_rigid(avbd_solver* solver, int enabled);
+/* Record every frame's features [n][32] and training targets [n][6] (the
+ * solve's correction of the plain warm start; the rotation part zero for
+ * particles) in the LEARN_* debug buffers.                                */
 int avbd_set_learning_capture(avbd_solver* solver, int enabled);
 /* Per-frame residual trace: out[0] at the plain warm start, out[1] at the
  * warm start used, out[2 + k] after iteration k (sqrt of the summed squared
@@ -421,7 +429,7 @@ int avbd_set_residual_trace(avbd_solver* solver, int enabled);
 int avbd_get_residual_trace(avbd_solver* solver, double* out, uint32_t n);
 
 /* Training kernels (device pointers; stream may be null).  A batch is
- * features[batch][32] and targets[batch][3] (raw, normalised with `norm`);
+ * features[batch][32] and targets[batch][6] (raw, normalised with `norm`);
  * the workspace holds avbd_mlp_workspace_bytes(batch) bytes.             */
 uint32_t avbd_mlp_param_count(void);
 size_t avbd_mlp_workspace_bytes(uint32_t batch);
@@ -431,7 +439,7 @@ int avbd_mlp_gradients(const float* params, const float* norm, const float* feat
 int avbd_mlp_train_step(float* params, const float* norm, const float* features,
                         const float* targets, uint32_t batch, float* adam_m, float* adam_v,
                         uint32_t step, float lr, void* workspace, float* loss_out, void* stream);
-/* Inference over n feature rows into out[n][3] on the tensor cores
+/* Inference over n feature rows into out[n][6] on the tensor cores
  * (tcgen05.mma, accumulators in tensor memory); synchronises `stream` and
  * returns AVBD_ERR_RUNTIME_FAILURE if the kernel's bounded wait for its MMA
  * completion gave up (workspace >= 80 KiB).                               */

@@ -1,7 +1,7 @@
 """Float64 forward/backward of the warm-start MLP — TEST INFRASTRUCTURE.
 
 The network is the one of avbd-metal_b200/csrc/learned.cu: 32 -> 128 -> 128
--> 128 -> 16 with ReLU, the first 3 outputs used, mean-squared-error loss on
+-> 128 -> 16 with ReLU, the first 6 outputs used, mean-squared-error loss on
 targets normalised by (ymean, ystd).  With `rounded=True` the oracle rounds
 exactly where the kernels store BF16 (normalised inputs, weights, hidden
 activations and backward operands) and evaluates everything else in float64,
@@ -13,7 +13,7 @@ Only tests/ may import this module.
 """
 import numpy as np
 
-DIN, HID, DOUT, USED = 32, 128, 16, 3
+DIN, HID, DOUT, USED = 32, 128, 16, 6
 XM, XI, YM, YS = 0, 32, 64, 80          # offsets in the 96-float normalisation block
 OW1 = 0
 OB1 = OW1 + HID * DIN
@@ -46,7 +46,7 @@ def unpack(params):
 
 
 def forward_backward(params, norm, X, T, rounded=True):
-    """Returns (loss, gradient) for features X [B][16] and targets T [B][3]."""
+    """Returns (loss, gradient) for features X [B][32] and targets T [B][6]."""
     R = bf16 if rounded else (lambda a: np.asarray(a, np.float64))
     F = f32 if rounded else (lambda a: np.asarray(a, np.float64))
     W1, b1, W2, b2, W3, b3, W4, b4 = unpack(params)
@@ -86,7 +86,7 @@ def forward_backward(params, norm, X, T, rounded=True):
 
 
 def predict(params, norm, X, rounded=True):
-    """Denormalised outputs [B][3] of the network."""
+    """Denormalised outputs [B][6] of the network."""
     R = bf16 if rounded else (lambda a: np.asarray(a, np.float64))
     F = f32 if rounded else (lambda a: np.asarray(a, np.float64))
     W1, b1, W2, b2, W3, b3, W4, b4 = unpack(params)

@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 def _random_batch(rng, B):
     X = rng.normal(size=(B, learned.DIN)).astype(np.float32)
     X[:, 15] = 1.0
-    T = rng.normal(size=(B, 3)).astype(np.float32)
+    T = rng.normal(size=(B, learned.USED)).astype(np.float32)
     return X, T
 
 
@@ -22,9 +22,9 @@ def _norm(rng):
     n = np.zeros(learned.NNORM, np.float32)
     n[learned.XM:learned.XM + learned.DIN] = rng.normal(0, 0.1, learned.DIN)
     n[learned.XI:learned.XI + learned.DIN] = rng.uniform(0.5, 2.0, learned.DIN)
-    n[learned.YM:learned.YM + 3] = rng.normal(0, 0.1, 3)
+    n[learned.YM:learned.YM + learned.USED] = rng.normal(0, 0.1, learned.USED)
     n[learned.YS:learned.NNORM] = 1.0
-    n[learned.YS:learned.YS + 3] = rng.uniform(0.5, 2.0, 3)
+    n[learned.YS:learned.YS + learned.USED] = rng.uniform(0.5, 2.0, learned.USED)
     return n
 
 
@@ -55,7 +55,7 @@ def test_inference_matches_oracle(cuda_lib, oracle_lib, n):
     from oracle import mlp_oracle as M
     rng = np.random.default_rng(7)
     p = learned.init_params(seed=3)
-    p[M.OB4:M.OB4 + 3] = [0.1, -0.2, 0.3]
+    p[M.OB4:M.OB4 + 6] = [0.1, -0.2, 0.3, 0.05, -0.05, 0.15]
     norm = _norm(rng)
     X, _ = _random_batch(rng, n)
     y = learned.infer(p, norm, X)
@@ -86,7 +86,7 @@ def test_inference_wait_gives_up_and_leaves_the_device_usable(cuda_lib):
     prm = torch.from_numpy(p.astype(np.float32)).to(dev)
     nrm = torch.from_numpy(norm.astype(np.float32)).to(dev)
     Xd = torch.from_numpy(X.astype(np.float32)).to(dev)
-    out = torch.zeros((256, 3), dtype=torch.float32, device=dev)
+    out = torch.zeros((256, learned.USED), dtype=torch.float32, device=dev)
     ws = torch.empty(1 << 17, dtype=torch.uint8, device=dev)
     rc = load_library().avbd_mlp_infer_wait_timeout_for_testing(
         prm.data_ptr(), nrm.data_ptr(), Xd.data_ptr(), 256, out.data_ptr(), ws.data_ptr(),
@@ -98,37 +98,46 @@ def test_inference_wait_gives_up_and_leaves_the_device_usable(cuda_lib):
     assert np.abs(y - want).max() <= 1e-3 * np.abs(want).max() + 1e-6
 
 
-@pytest.mark.parametrize("name,make,trials,frames", [
-    ("soft-cube-6, 2 trial sweeps", lambda: demos.soft_cube_scene(seed=3, n=6), 2, 40),
-    ("soft-cube-6, kept trial sweep", lambda: demos.soft_cube_scene(seed=3, n=6), 1, 40),
-    ("soft-cube-6, no trial sweep", lambda: demos.soft_cube_scene(seed=3, n=6), 0, 40),
-    ("mixed-small, kept trial sweep", lambda: demos.mixed_scene(seed=7, cubes=4, cube_n=4, boxes=4, cloth_n=10,
-                                                                  pitch=0.5), 1, 80),
+def _mixed_small():
+    return demos.mixed_scene(seed=7, cubes=4, cube_n=4, boxes=4, cloth_n=10, pitch=0.5)
+
+
+@pytest.mark.parametrize("name,make,trials,frames,rigid", [
+    ("soft-cube-6, 2 trial sweeps", lambda: demos.soft_cube_scene(seed=3, n=6), 2, 40, False),
+    ("soft-cube-6, kept trial sweep", lambda: demos.soft_cube_scene(seed=3, n=6), 1, 40, False),
+    ("soft-cube-6, no trial sweep", lambda: demos.soft_cube_scene(seed=3, n=6), 0, 40, False),
+    ("mixed-small, kept trial sweep", _mixed_small, 1, 80, False),
+    ("mixed-small, rigid rows", _mixed_small, 1, 80, True),
+    ("rigid-stack-20, rigid rows", lambda: demos.rigid_stack_scene(seed=1), 1, 60, True),
+    ("batched-worlds-16, rigid rows, no trial sweep", lambda: demos.batched_worlds_scene(worlds=16, seed=4)[0],
+     0, 40, True),
 ])
-def test_zero_correction_model_reproduces_plain_frames(cuda_lib, name, make, trials, frames):
+def test_zero_correction_model_reproduces_plain_frames(cuda_lib, name, make, trials, frames, rigid):
     """A model whose every prediction is zero: x_learned == x_plain, the
     race is a tie that the prediction wins, and the trajectory is the plain
     one bit for bit — with the trial sweeps undone, with the winner's sweep
     kept as the first iteration (its OGC bound count included), without a
-    trial sweep, and in a color-Jacobi scene whose predicted branch has its
-    own pending-solve buffers."""
+    trial sweep, in a color-Jacobi scene whose predicted branch has its own
+    pending-solve buffers, and with rigid-body rows (positions and
+    orientations)."""
     s = make()
     plain, learn = GPUSolver(s), GPUSolver(s)
     norm = np.zeros(learned.NNORM, np.float32)
     norm[learned.XI:learned.XI + learned.DIN] = 1.0
     norm[learned.YS:learned.NNORM] = 1.0
-    learn.set_warm_start_model(np.zeros(learned.NPARAM, np.float32), norm, trials)
+    learn.set_warm_start_model(np.zeros(learned.NPARAM, np.float32), norm, trials, rigid=rigid)
     learn.set_warm_start_mode(abi.WARM_START_LEARNED)
     for f in range(frames):
         plain.step(1)
         learn.step(1)
-        a, _ = plain.positions()
-        b, _ = learn.positions()
+        a, qa = plain.positions()
+        b, qb = learn.positions()
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f
-    # every raced frame is a tie the prediction wins; the first three frames
-    # of a scene whose color launches are tuned time the lane widths instead
-    # of racing
-    assert frames - 3 <= learn.counters().learn_accepted <= frames
+        assert np.array_equal(qa.view(np.uint32), qb.view(np.uint32)), f
+    # every raced frame is a tie the prediction wins; the first frames of a
+    # scene whose color launches are tuned (three lane widths, or up to seven
+    # dynamic-coloring block shapes) time the launches instead of racing
+    assert frames - (7 if rigid else 3) <= learn.counters().learn_accepted <= frames
     assert learn.counters().ogc_exceeded == plain.counters().ogc_exceeded
 
 
@@ -136,10 +145,11 @@ def test_training_learns_the_correction(cuda_lib):
     """Trained on the solver's own rollouts, the network explains most of the
     variance of the solve's correction of the plain warm start."""
     X, T = learned.collect(lambda seed: demos.soft_cube_scene(seed=seed, n=10), seeds=[1, 2], frames=60)
-    assert X.shape[1] == learned.DIN and T.shape[1] == 3 and X.shape[0] == T.shape[0] > 1000
+    assert X.shape[1] == learned.DIN and T.shape[1] == learned.USED and X.shape[0] == T.shape[0] > 1000
+    assert not T[:, 3:].any()                          # particles: no rotation part
     m = learned.train(X, T, steps=800, batch=4096, lr=1e-3, log_every=100)
     pred = learned.infer(m.params, m.norm, X)
-    explained = 1.0 - ((pred - T) ** 2).mean(axis=0) / T.var(axis=0)
+    explained = 1.0 - ((pred[:, :3] - T[:, :3]) ** 2).mean(axis=0) / T[:, :3].var(axis=0)
     print("loss history", [round(h, 4) for h in m.history], "explained variance", np.round(explained, 3))
     assert explained[2] > 0.5 and np.mean(m.history[-3:]) < np.mean(m.history[:2])
 

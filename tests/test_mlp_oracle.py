@@ -12,7 +12,7 @@ def test_oracle_backward_matches_finite_differences():
     norm[M.XI:M.XI + M.DIN] = 1.0
     norm[M.YS:96] = 1.0
     X = rng.normal(size=(7, M.DIN))
-    T = rng.normal(size=(7, 3))
+    T = rng.normal(size=(7, M.USED))
     loss, g = M.forward_backward(p, norm, X, T, rounded=False)
     h = 1e-6
     for block, (a, b) in {"W1": (M.OW1, M.OB1), "b1": (M.OB1, M.OW2), "W2": (M.OW2, M.OB2),
