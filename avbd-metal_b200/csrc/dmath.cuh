@@ -254,4 +254,14 @@ __device__ __forceinline__ bool ball_misses_box(float3 p, float reach, float4 lo
     return dx * dx + dy * dy + dz * dz > r * r;
 }
 
+// Hinge twist of qB relative to qAr about `axis` (B local), in (-pi, pi].
+__device__ __forceinline__ float twist_angle(float4 qAr, float4 qB, float3 axis) {
+    float4 r = q_mul(q_inv(qAr), qB);
+    if (r.w < 0.0f) r = neg4(r);
+    return 2.0f * atan2_series(dot(xyz(r), axis), r.w);
+}
+__device__ __forceinline__ float wrap_pi(float x) {
+    return x - 6.2831853f * floorf((x + 3.14159265f) / 6.2831853f);
+}
+
 }  // namespace avbd

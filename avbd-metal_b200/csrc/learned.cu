@@ -19,10 +19,13 @@
 // stiffness dt^2 / m) of the incident elements, [15] 1; rigid rows only
 // (zeros for particles): [16] 1, [17-19] plain warm-start rotation
 // q_sub(q_plain, q_start) r / s, [20-22] world up axis in the body frame,
-// [23] log(1 + r / s) / 10, [24] reserved zero; 1-ring aggregates over the vertices sharing a tet or spring: [25]
+// [23] log(1 + r / s) / 10, [24] incident position-PD hinge motors / 4,
+// [28-30] the rotation those motors ask for at the plain warm start (sum
+// of hinge axis x -(twist - target), as arc length at r in units of s),
+// [31] log(1 + sum kp dt^2 / (m r^2)); 1-ring aggregates over the vertices sharing a tet or spring: [25]
 // ring size / 10, [26] mean neighbour contact count / 4, [27] smallest
-// neighbour contact gap / s (clipped); [28-31] reserved zeros.  Contacts are
-// rigid manifolds and element contacts alike.
+// neighbour contact gap / s (clipped).  Contacts are rigid manifolds and
+// element contacts alike.
 //
 // Parameter block (fp32, also the layout of the gradients): W1[128][32], b1,
 // W2[128][128], b2, W3[128][128], b3, W4[16][128], b4[16].  The weights are
@@ -88,10 +91,13 @@ __device__ __forceinline__ uint32_t ld_pair(const bf16* p) { return *reinterpret
 namespace tc {
 constexpr uint32_t ROWS = 128;
 constexpr uint32_t SBO_K128 = 2048, SBO_K32 = 512;      // row-group strides (K = 128, K = 32)
+// shared memory: weight image | layer operand | biases b1 b2 b3 b4 (fp32) |
+// normalisation block (fp32) | MMA barrier | staging barrier | TMEM address
 constexpr uint32_t W1 = 0, W2 = W1 + 128 * 32 * 2, W3 = W2 + 128 * 128 * 2, W4 = W3 + 128 * 128 * 2,
-                   ACT = W4 + 16 * 128 * 2, BAR = ACT + ROWS * 128 * 2, WBAR = BAR + 8, TSLOT = WBAR + 8,
-                   SMEM = TSLOT + 8;
+                   ACT = W4 + 16 * 128 * 2, BIAS = ACT + ROWS * 128 * 2, NORM = BIAS + (3 * 128 + 16) * 4,
+                   BAR = NORM + 96 * 4, WBAR = BAR + 8, TSLOT = WBAR + 8, SMEM = TSLOT + 8;
 constexpr uint32_t WBYTES = ACT - W1;                    // the weight image: 77,824 bytes
+constexpr uint32_t STAGED = WBYTES + (NORM - BIAS) + 96 * 4;   // every byte the staging barrier expects
 constexpr uint32_t TMEM_COLS = 128;
 constexpr uint64_t WAIT_NS = 1000000000ull;              // a wait gives up after one second
 
@@ -193,17 +199,23 @@ __global__ void __launch_bounds__(128) k_mlp_infer_tc(const bf16* __restrict__ W
     const uint32_t t = threadIdx.x, warp = t >> 5;
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
     const uint32_t bar = sbase + tc::BAR, wbar = sbase + tc::WBAR;
-    // the weight image (already in the canonical layout) in four bulk copies
+    // the weight image (already in the canonical layout), the biases and the
+    // normalisation block: nine bulk copies on one barrier
     if (t == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(wbar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        tc::expect_tx(wbar, tc::WBYTES);
+        tc::expect_tx(wbar, tc::STAGED);
         const unsigned char* img = reinterpret_cast<const unsigned char*>(W);
         tc::bulk_load(sbase + tc::W1, img + tc::W1, tc::W2 - tc::W1, wbar);
         tc::bulk_load(sbase + tc::W2, img + tc::W2, tc::W3 - tc::W2, wbar);
         tc::bulk_load(sbase + tc::W3, img + tc::W3, tc::W4 - tc::W3, wbar);
         tc::bulk_load(sbase + tc::W4, img + tc::W4, tc::ACT - tc::W4, wbar);
+        tc::bulk_load(sbase + tc::BIAS, prm + OB1, 128 * 4, wbar);
+        tc::bulk_load(sbase + tc::BIAS + 512, prm + OB2, 128 * 4, wbar);
+        tc::bulk_load(sbase + tc::BIAS + 1024, prm + OB3, 128 * 4, wbar);
+        tc::bulk_load(sbase + tc::BIAS + 1536, prm + OB4, 16 * 4, wbar);
+        tc::bulk_load(sbase + tc::NORM, norm, 96 * 4, wbar);
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + tc::TSLOT),
@@ -221,6 +233,8 @@ __global__ void __launch_bounds__(128) k_mlp_infer_tc(const bf16* __restrict__ W
     // the weights have landed (bounded wait; block-uniform outcome)
     bool ok = __syncthreads_and(tc::wait(wbar, 0) ? 1 : 0) != 0;
     if (!ok) tc::wait(wbar, 0);        // give copies still in flight one more bounded wait
+    const float* sbias = reinterpret_cast<const float*>(sm + tc::BIAS);
+    const float* snorm = reinterpret_cast<const float*>(sm + tc::NORM);
     const uint32_t tiles = (n + tc::ROWS - 1) / tc::ROWS;
     for (uint32_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x) {
         const uint32_t r = tile * tc::ROWS + row;
@@ -237,8 +251,8 @@ __global__ void __launch_bounds__(128) k_mlp_infer_tc(const bf16* __restrict__ W
 #pragma unroll
             for (int e = 0; e < 4; e++) {
                 const uint32_t c = kg * 8 + 2 * e;
-                const float a = r < n ? (xv[2 * e] - norm[NX_MEAN + c]) * norm[NX_INV + c] : 0.0f;
-                const float b = r < n ? (xv[2 * e + 1] - norm[NX_MEAN + c + 1]) * norm[NX_INV + c + 1] : 0.0f;
+                const float a = r < n ? (xv[2 * e] - snorm[NX_MEAN + c]) * snorm[NX_INV + c] : 0.0f;
+                const float b = r < n ? (xv[2 * e + 1] - snorm[NX_MEAN + c + 1]) * snorm[NX_INV + c + 1] : 0.0f;
                 w[e] = pack_bf16(a, b);
             }
             *reinterpret_cast<uint4*>(sm + tc::ACT + tc::off(row, kg * 8, tc::SBO_K128)) = make_uint4(w[0], w[1], w[2], w[3]);
@@ -265,7 +279,7 @@ __global__ void __launch_bounds__(128) k_mlp_infer_tc(const bf16* __restrict__ W
             if (!ok) break;
             if (layer < 3) {
                 // bias, ReLU, BF16: the next layer's operand, written in place
-                const float* bias = prm + (layer == 0 ? OB1 : (layer == 1 ? OB2 : OB3));
+                const float* bias = sbias + 128 * layer;
 #pragma unroll 1
                 for (uint32_t c0 = 0; c0 < HID; c0 += 32) {
                     float v[32];
@@ -288,8 +302,8 @@ __global__ void __launch_bounds__(128) k_mlp_infer_tc(const bf16* __restrict__ W
                 if (r < n) {
 #pragma unroll
                     for (uint32_t c = 0; c < (uint32_t)USED_OUT; c++) {
-                        const float y = v[c] + prm[OB4 + c];
-                        Y[(size_t)r * USED_OUT + c] = y * norm[NY_STD + c] + norm[NY_MEAN + c];
+                        const float y = v[c] + sbias[3 * 128 + c];
+                        Y[(size_t)r * USED_OUT + c] = y * snorm[NY_STD + c] + snorm[NY_MEAN + c];
                     }
                 }
             }
@@ -694,6 +708,34 @@ __global__ void k_learn_features(const Params P, const DevPtrs d, uint32_t n) {
     f[26] = ringContacts * inv * 0.25f;
     f[27] = ringContacts > 0.0f ? fminf(fmaxf(ringGap / s, -10.0f), 10.0f) : 10.0f;
     f[28] = 0.0f; f[29] = 0.0f; f[30] = 0.0f; f[31] = 0.0f;
+    if (i >= P.learnParticles) {
+        // position-PD hinge motors acting on the body (they are in its
+        // static segment): the rotation each asks for, and their gains
+        const float r = learn_radius(d, v);
+        const uint4 sg = d.staticSeg[v];
+        float motors = 0.0f, gain = 0.0f;
+        float3 want = s3(0.0f);
+        for (uint32_t k = 0; k < sg.y; k++) {
+            const uint32_t e = d.preList[sg.x + k];
+            if ((e >> ADJ_KIND_SHIFT) != FK_JOINT) continue;
+            const JointGPU& j = d.joints[e & ADJ_INDEX_MASK];
+            const uint32_t mode = j.header.w & MOTOR_MODE_MASK;
+            if (!(j.motor.y > 0.0f) || j.hingeAxis.w == 0.0f || mode == MOTOR_EXPLICIT || mode == MOTOR_VELOCITY)
+                continue;
+            const uint32_t a = j.header.x, b = j.header.y;
+            const float4 qA = a == WORLD_BODY ? make_float4(0, 0, 0, 1) : d.posAng[a];
+            const float4 qB = d.posAng[b];
+            const float3 axis = xyz(j.hingeAxis);
+            const float Cm = wrap_pi(twist_angle(q_mul(qA, tof(j.restRel)), qB, axis) - j.motor.x);
+            want += q_rotate(qB, axis) * (v == a ? Cm : -Cm);
+            motors += 1.0f;
+            gain += j.motor.w;
+        }
+        const float3 w = want * (r / s);
+        f[24] = motors * 0.25f;
+        f[28] = w.x; f[29] = w.y; f[30] = w.z;
+        f[31] = log1pf(gain * P.dt * P.dt / fmaxf(pl.w * r * r, 1e-12f));
+    }
     f[0] = fi.x; f[1] = fi.y; f[2] = fi.z;
     f[3] = fp.x; f[4] = fp.y; f[5] = fp.z;
     f[6] = fv.x; f[7] = fv.y; f[8] = fv.z;
@@ -793,7 +835,8 @@ void launch_learn_target(const Params& P, const DevPtrs& d, const Sizes& z, cuda
 }
 void launch_copy_double(const double* src, double* dst, cudaStream_t st) { k_copy_double<<<1, 32, 0, st>>>(src, dst); }
 
-// weights + one activation tile: 108 KiB of shared memory (set once per device)
+// weights, one activation tile, biases and normalisation: 110 KiB of shared
+// memory (set once per device)
 static void mlp_infer_attributes() {
     static std::atomic<uint64_t> done{0};
     int dev = 0;
@@ -808,7 +851,7 @@ void launch_mlp_infer(const void* halfW, const float* prm, const float* norm, co
                       uint32_t* status, cudaStream_t st) {
     if (n == 0) return;
     mlp_infer_attributes();
-    // two CTAs per SM (108 KiB of shared memory and 128 TMEM columns each),
+    // two CTAs per SM (110 KiB of shared memory and 128 TMEM columns each),
     // every CTA walking 128-row tiles
     const uint32_t tiles = (n + tc::ROWS - 1) / tc::ROWS;
     const uint32_t blocks = std::min<uint32_t>(tiles, 2u * 148u);
@@ -867,8 +910,10 @@ int avbd_mlp_train_step(float* params, const float* norm, const float* features,
 static int mlp_infer(const float* params, const float* norm, const float* features, uint32_t n, float* out,
                      void* workspace, void* stream, bool issue) {
     if (!params || !norm || !features || !out || !workspace) return AVBD_ERR_INVALID_ARGUMENT;
-    // bulk copies read the weight image and the feature rows in 16-byte units
-    if ((reinterpret_cast<uintptr_t>(workspace) | reinterpret_cast<uintptr_t>(features)) & 15u)
+    // bulk copies and vector loads read the weight image, the biases, the
+    // normalisation block and the feature rows in 16-byte units
+    if ((reinterpret_cast<uintptr_t>(workspace) | reinterpret_cast<uintptr_t>(features) |
+         reinterpret_cast<uintptr_t>(params) | reinterpret_cast<uintptr_t>(norm)) & 15u)
         return AVBD_ERR_INVALID_ARGUMENT;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     // the BF16 weight mirror, then the kernel's status word

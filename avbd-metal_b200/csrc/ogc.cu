@@ -20,6 +20,7 @@
 //     owner order: rigid-triangle records, then V-T by particle, then E-E by
 //     edge.
 #include "elements.cuh"
+#include "pdl.cuh"
 
 namespace avbd {
 
@@ -661,6 +662,7 @@ __global__ void k_ogc_totals(const Params P, const DevPtrs d, uint32_t owners) {
 // every bound from the tracked sets.
 // ---------------------------------------------------------------------------
 __global__ void k_ogc_refresh(const Params P, const DevPtrs d, const uint32_t* readSlot, uint32_t* zeroSlot) {
+    pdl_prologue();
     const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid == 0) *zeroSlot = 0u;
     if (!(*readSlot * 100u > P.numParticles) || gid >= P.numParticles) return;
@@ -702,6 +704,7 @@ __global__ void k_ogc_refresh(const Params P, const DevPtrs d, const uint32_t* r
 
 // Color-Jacobi commit of one color (the primal of the color wrote posNext).
 __global__ void k_publish_color(const DevPtrs d, uint32_t color, uint32_t count) {
+    pdl_prologue();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     const uint32_t v = d.colorList[d.colorStart[color] + i];
@@ -744,12 +747,12 @@ void launch_ogc_detect(const Params& P, const DevPtrs& d, const Sizes& z, cudaSt
 void launch_publish_color(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count, cudaStream_t st) {
     (void)P;
     if (count == 0) return;
-    k_publish_color<<<(count + 127) / 128, 128, 0, st>>>(d, color, count);
+    launch_pdl(k_publish_color, (count + 127) / 128, 128, st, d, color, count);
 }
 
 void launch_ogc_refresh(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t* readSlot, uint32_t* zeroSlot,
                         cudaStream_t st) {
-    k_ogc_refresh<<<(z.numParticles + 127) / 128, 128, 0, st>>>(P, d, readSlot, zeroSlot);
+    launch_pdl(k_ogc_refresh, (z.numParticles + 127) / 128, 128, st, P, d, readSlot, zeroSlot);
 }
 
 }  // namespace avbd

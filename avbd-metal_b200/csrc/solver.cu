@@ -16,35 +16,12 @@
 
 #include "dmath.cuh"
 #include "kernels.h"
+#include "pdl.cuh"
 
 namespace avbd {
 
 constexpr float FLT_BIG = 3.402823466e38f;
 
-// Programmatic dependent launch: the iteration loop is a chain of ~120
-// dependent kernels per frame.  Each kernel lets the next one be scheduled as
-// soon as all of its own blocks are running, and waits for the previous grid
-// to complete (and its writes to be visible) before touching solver state.
-__device__ __forceinline__ void pdl_prologue() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    asm volatile("griddepcontrol.wait;" ::: "memory");
-}
-
-template <typename... KArgs, typename... Args>
-static void launch_pdl(void (*kernel)(KArgs...), uint32_t blocks, uint32_t threads, cudaStream_t st,
-                       Args&&... args) {
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(blocks);
-    cfg.blockDim = dim3(threads);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
-}
 // failure kinds (mirrors AVBD_FAIL_* of include/avbd.h)
 constexpr uint32_t AVBD_FAIL_RIGID_PAIR_CAPACITY_ = 2;
 constexpr uint32_t AVBD_FAIL_UNRESOLVED_COLORING_ = 5;
@@ -62,12 +39,6 @@ static uint32_t stride_blocks(uint32_t upper, int threads) {
 // ---------------------------------------------------------------------------
 // Warm start (40_solver.metal:546-722)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float twist_angle(float4 qAr, float4 qB, float3 axis) {
-    float4 r = q_mul(q_inv(qAr), qB);
-    if (r.w < 0.0f) r = neg4(r);
-    return 2.0f * atan2_series(dot(xyz(r), axis), r.w);
-}
-
 __global__ void k_warmstart_constraints(const Params P, const DevPtrs d, uint32_t nJ, uint32_t nS) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nJ + nS) return;
@@ -485,9 +456,6 @@ __device__ __forceinline__ M3 geom_stiff_ball_socket(int k, float3 v) {
     else if (k == 1) { m.r0.y += v.x; m.r1.y += v.y; m.r2.y += v.z; }
     else { m.r0.z += v.x; m.r1.z += v.y; m.r2.z += v.z; }
     return m;
-}
-__device__ __forceinline__ float wrap_pi(float x) {
-    return x - 6.2831853f * floorf((x + 3.14159265f) / 6.2831853f);
 }
 
 __device__ void stamp_joint(const Params& P, const DevPtrs& d, const JointGPU& j, uint32_t self, Accum& acc) {
@@ -934,6 +902,7 @@ __device__ void primal_body(const Params& P, const DevPtrs& d, uint32_t body, ui
 }
 
 __global__ void k_primal(const Params P, const DevPtrs d, uint32_t color, uint32_t count) {
+    pdl_prologue();
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t lane = tid & 7u, groups = (gridDim.x * blockDim.x) >> 3;
     const uint32_t s = d.colorStart[color];
@@ -1437,7 +1406,7 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
         // 1.007 -> 0.965 ms per frame; half a wave measured 1.22 ms)
         const uint32_t TT = z.dynThreads ? z.dynThreads : (uint32_t)T;
         const uint32_t need = (upper * 8 + TT - 1) / TT, wave = z.dynBlocks ? z.dynBlocks : 148u * 4u;
-        k_primal<<<need < wave ? need : wave, TT, 0, st>>>(P, d, color, count);
+        launch_pdl(k_primal, need < wave ? need : wave, TT, st, P, d, color, count);
     } else {
         // the grouped kernel needs the color's body count on the host
         const uint32_t lanes_ = lanes < 8 ? 8 : (lanes > 32 ? 32 : lanes);
@@ -1681,6 +1650,7 @@ void launch_solve_small(const Params& P, const DevPtrs& d, const Sizes& z, uint3
 // with a block barrier between them — the same per-body solve in the same
 // color order.
 __global__ void __launch_bounds__(256) k_primal_tail(const Params P, const DevPtrs d, uint32_t first) {
+    pdl_prologue();
     const uint32_t groups = blockDim.x >> 3;
     const uint32_t group = threadIdx.x >> 3, lane = threadIdx.x & 7u;
     const unsigned mask = 0xFFu << (threadIdx.x & 24u);
@@ -1694,7 +1664,7 @@ __global__ void __launch_bounds__(256) k_primal_tail(const Params P, const DevPt
 }
 
 void launch_primal_tail(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t first, cudaStream_t st) {
-    if (first < (uint32_t)MAX_COLORS) k_primal_tail<<<1, 256, 0, st>>>(P, d, first);
+    if (first < (uint32_t)MAX_COLORS) launch_pdl(k_primal_tail, 1, 256, st, P, d, first);
 }
 
 // ---------------------------------------------------------------------------
