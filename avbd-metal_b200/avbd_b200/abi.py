@@ -7,6 +7,7 @@ import ctypes as C
 
 ABI_VERSION = 3
 CAPACITY_SOFT_CONTACTS, CAPACITY_PLANAR_DAT_PAIRS = 0, 1
+PRIMAL_VARIANT_AUTO, PRIMAL_VARIANT_STAGED = 0, 1
 
 # status codes
 OK = 0
@@ -191,7 +192,7 @@ EXPORTED = [
     "avbd_max_constraint_error", "avbd_get_counters", "avbd_runtime_failure",
     "avbd_last_error", "avbd_snapshot_capture", "avbd_snapshot_restore",
     "avbd_snapshot_free", "avbd_debug_buffer_size", "avbd_debug_read", "avbd_set_stream",
-    "avbd_set_profiling", "avbd_get_profile", "avbd_exclusive_scan_noalloc", "avbd_set_capacity_for_testing",
+    "avbd_set_profiling", "avbd_get_profile", "avbd_set_primal_variant", "avbd_exclusive_scan_noalloc", "avbd_set_capacity_for_testing",
     "avbd_set_warm_start_model", "avbd_set_warm_start_mode", "avbd_set_warm_start_rigid",
     "avbd_set_learning_capture",
     "avbd_set_residual_trace", "avbd_get_residual_trace", "avbd_mlp_param_count",

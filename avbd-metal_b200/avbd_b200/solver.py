@@ -82,6 +82,7 @@ def load_library() -> C.CDLL:
         "avbd_debug_read": ([vp, i32, vp, sz], i32),
         "avbd_set_stream": ([vp, vp], i32),
         "avbd_set_profiling": ([vp, i32], i32),
+        "avbd_set_primal_variant": ([vp, u32], i32),
         "avbd_set_capacity_for_testing": ([vp, i32, u32], i32),
         "avbd_get_profile": ([vp, vp], i32),
         "avbd_set_warm_start_model": ([vp, vp, vp, u32], i32),
@@ -368,6 +369,12 @@ class GPUSolver:
         """Lower the soft-contact or Planar-DAT pair capacity (abi.CAPACITY_*)
         to provoke its capacity failure on a small scene."""
         self._check(load_library().avbd_set_capacity_for_testing(self._h, int(which), int(value)))
+
+    def set_primal_variant(self, variant: int):
+        """Pin every static color's primal to one variant: 8, 16 or 32 lanes
+        per body, abi.PRIMAL_VARIANT_STAGED, or abi.PRIMAL_VARIANT_AUTO to
+        re-run the autotuner.  All variants compute the same floats."""
+        self._check(load_library().avbd_set_primal_variant(self._h, int(variant)))
 
     def set_profiling(self, enabled: bool):
         self._check(load_library().avbd_set_profiling(self._h, 1 if enabled else 0))

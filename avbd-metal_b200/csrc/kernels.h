@@ -62,6 +62,7 @@ struct DevPtrs {
     const TetGPU* tetInc;                 // tet records in postList order (null without tets)
     // coloring
     uint32_t *colorsA, *colorsB, *colorList, *bodySlot;
+    uint32_t* colorLaunch;                // static palette: primal launch order per color
     // control
     Counters* counters;
     uint32_t* scanScratch;                // block sums of the exclusive scans
@@ -145,6 +146,7 @@ struct Sizes {
     // static palette on the host (null with dynamic coloring)
     const uint32_t* colorCounts;
     const uint32_t* colorLanes;
+    const uint32_t* colorLean;            // lean particles at the head of each color's launch order
     // dynamic coloring: block shape of the rigid primal's grid-stride launch
     // (blocks, threads per block), chosen by the runtime's autotuner
     uint32_t dynBlocks, dynThreads;
@@ -161,7 +163,11 @@ void launch_warmstart(const Params& P, const DevPtrs& d, const Sizes& z, cudaStr
 void launch_adjacency(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 void launch_dynamic_coloring(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 // one color of the block-descent primal; `count` is the color's body count
-// when known on the host (static palette), else 0xFFFFFFFF (read on device)
+// when known on the host (static palette), else 0xFFFFFFFF (read on device);
+// `lanes` is 8, 16 or 32 lanes per body (grouped kernel) or
+// AVBD_PRIMAL_STAGED (staged kernel: block-wide term evaluation, then an
+// 8-lane fold per body), every choice computing the same floats
+constexpr uint32_t AVBD_PRIMAL_STAGED = 1;
 void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color,
                          uint32_t count, uint32_t lanes, cudaStream_t st);
 // squared AL-gradient norm of every dynamic body (perBody[numDynamicBodies])

@@ -503,6 +503,7 @@ struct avbd_solver {
         z.numLearn = P.cloth ? 0u : P.learnParticles;
         z.colorCounts = H.dynamicColoring ? nullptr : H.colorCounts.data();
         z.colorLanes = H.colorLanes.data();
+        z.colorLean = H.colorLean.data();
         z.numDynamicRigid = 0;
         for (uint32_t b = 0; b < nb; b++) z.numDynamicRigid += (H.posLin[b].w > 0.0f && H.shape[b].w >= 0.0f) ? 1u : 0u;
         const uint32_t scanLimit = 1024u * 1024u;
@@ -589,6 +590,7 @@ struct avbd_solver {
             ok = ok && alloc(d.colorList, nb, "colorList");
         } else {
             ok = ok && upload(d.colorList, H.colorList, "colorList");
+            ok = ok && upload(d.colorLaunch, H.colorLaunch, "colorLaunch");
             ok = ok && upload(d.colorStart, H.colorStart, "colorStart");
         }
         // control
@@ -784,15 +786,17 @@ struct avbd_solver {
         return failure == AVBD_FAIL_NONE ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
     }
 
-    // Lane-width autotuner.  Each static color's primal can run with 8, 16 or
-    // 32 lanes per body; the fold order is fixed, so every width computes the
-    // same floats and only speed differs (it depends on the color's body
-    // count and adjacency sizes).  The first three frames run eagerly, one
-    // width each, with events around every primal launch; each color then
-    // keeps its fastest width and the frame graphs are captured with it.
-    static constexpr uint32_t kTuneWidths[3] = {8, 16, 32};
-    int tuneStage = -1;                       // -1 off / done, 0..2 next width
-    double tuneMs[3][MAX_COLORS] = {};
+    // Primal variant autotuner.  Each static color's primal can run the
+    // grouped kernel with 8, 16 or 32 lanes per body or the staged kernel;
+    // the fold order is fixed, so every variant computes the same floats and
+    // only speed differs (it depends on the color's body count and adjacency
+    // sizes).  The first four frames run eagerly, one variant each, with
+    // events around every primal launch; each color then keeps its fastest
+    // variant and the frame graphs are captured with it.
+    static constexpr int kTuneVariants = 4;
+    static constexpr uint32_t kTuneWidths[kTuneVariants] = {8, 16, 32, AVBD_PRIMAL_STAGED};
+    int tuneStage = -1;                       // -1 off / done, else the next variant
+    double tuneMs[kTuneVariants][MAX_COLORS] = {};
     std::vector<cudaEvent_t> tuneEvents;
 
     bool tuning_applies() const { return !z.dynamicColoring && !smallSolve && H.staticUsedColors > 0; }
@@ -821,10 +825,10 @@ struct avbd_solver {
                 tuneMs[tuneStage][c] += ms;
                 k++;
             }
-        if (++tuneStage == 3) {
+        if (++tuneStage == kTuneVariants) {
             for (uint32_t c = 0; c < colorBound; c++) {
                 int best = 0;
-                for (int w = 1; w < 3; w++) if (tuneMs[w][c] < tuneMs[best][c]) best = w;
+                for (int w = 1; w < kTuneVariants; w++) if (tuneMs[w][c] < tuneMs[best][c]) best = w;
                 H.colorLanes[c] = kTuneWidths[best];
             }
             tuneStage = -1;
@@ -1721,6 +1725,23 @@ int avbd_set_profiling(avbd_solver* s, int enabled) {
         s->graphsValid = false;
     }
     std::memset(&s->prof, 0, sizeof(s->prof));
+    return AVBD_OK;
+}
+
+int avbd_set_primal_variant(avbd_solver* s, uint32_t variant) {
+    if (!s) return AVBD_ERR_INVALID_ARGUMENT;
+    if (variant != 0 && variant != AVBD_PRIMAL_STAGED && variant != 8 && variant != 16 && variant != 32)
+        return AVBD_ERR_INVALID_ARGUMENT;
+    int rc = s->retire();
+    if (rc != AVBD_OK) return rc;
+    if (variant == 0) {
+        s->tuneStage = s->tuning_applies() ? 0 : -1;
+        std::memset(s->tuneMs, 0, sizeof(s->tuneMs));
+    } else {
+        s->tuneStage = -1;
+        for (auto& l : s->H.colorLanes) l = variant;
+    }
+    s->graphsValid = false;
     return AVBD_OK;
 }
 

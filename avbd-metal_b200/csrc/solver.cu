@@ -640,39 +640,76 @@ __device__ __forceinline__ float3 contact_force(const ContactGPU& c, float3 nrm,
     return F;
 }
 
-__device__ void stamp_manifold(const Params& P, const DevPtrs& d, const ManifoldGPU& m, uint32_t self, Accum& acc) {
+// What one contact point (or one rigid element-contact slot) adds to a
+// body's 6x6 system: each accumulator component takes exactly one add per
+// point, so a point's increment can be formed anywhere and added later in
+// the original order with the same result.
+struct PointInc { M3 lhsLin, lhsAng, lhsCross; float3 rhsLin, rhsAng; };
+__device__ __forceinline__ void add_inc(Accum& acc, const PointInc& x) {
+    acc.lhsLin = m3_add(acc.lhsLin, x.lhsLin);
+    acc.lhsAng = m3_add(acc.lhsAng, x.lhsAng);
+    acc.lhsCross = m3_add(acc.lhsCross, x.lhsCross);
+    acc.rhsLin += x.rhsLin;
+    acc.rhsAng += x.rhsAng;
+}
+// Jacobian-weighted increment of a contact frame with world lever rW.
+__device__ __forceinline__ PointInc point_inc(const M3& jLin, float3 rW, const M3& K, float3 F) {
+    const M3 jAng = M3{cross(rW, jLin.r0), cross(rW, jLin.r1), cross(rW, jLin.r2)};
+    const M3 jLinT = m3_transpose(jLin), jAngT = m3_transpose(jAng);
+    const M3 jAngTk = m3_mulm(jAngT, K);
+    PointInc x;
+    x.lhsLin = m3_mulm(m3_mulm(jLinT, K), jLin);
+    x.lhsAng = m3_mulm(jAngTk, jAng);
+    x.lhsCross = m3_mulm(jAngTk, jLin);
+    x.rhsLin = m3_mul(jLinT, F);
+    x.rhsAng = m3_mul(jAngT, F);
+    return x;
+}
+
+// Pose data of a manifold's two bodies shared by its contact points.
+struct ManifoldCtx {
+    float4 qa, qb;
+    float3 dqALin, dqAAng, dqBLin, dqBAng, nrm, t1, t2;
+    float dynF, statF;
+    bool isA, sphA, sphB;
+};
+__device__ __forceinline__ ManifoldCtx manifold_ctx(const DevPtrs& d, const ManifoldGPU& m, uint32_t self) {
     const u4 h = m.header;
-    const uint32_t a = h.x, b = h.y, n = h.z;
-    const bool isA = self == a;
-    const bool sphA = (h.w & 2u) != 0, sphB = (h.w & 4u) != 0;
-    const float4 qa = d.posAng[a], qb = d.posAng[b];
-    const float3 dqALin = xyz(d.posLin[a]) - xyz(d.initLin[a]);
-    const float3 dqAAng = q_sub(qa, d.initAng[a]);
-    const float3 dqBLin = xyz(d.posLin[b]) - xyz(d.initLin[b]);
-    const float3 dqBAng = q_sub(qb, d.initAng[b]);
-    const float3 nrm = xyz(m.basisN), t1 = xyz(m.basisT1), t2 = cross(nrm, t1);
-    const float dynF = m.basisN.w, statF = m.basisT1.w;
-    for (uint32_t i = 0; i < n; i++) {
-        const ContactGPU c = m.contacts[i];
-        const float3 rAW = sphA ? xyz(c.rA) : q_rotate(qa, xyz(c.rA));
-        const float3 rBW = sphB ? xyz(c.rB) : q_rotate(qb, xyz(c.rB));
-        float3 C;
-        float fs, bnd;
-        const float3 F = contact_force(c, nrm, t1, t2, dynF, statF, P.alpha, dqALin, dqAAng, dqBLin, dqBAng,
-                                       rAW, rBW, C, fs, bnd);
-        const float s = isA ? 1.0f : -1.0f;
-        const M3 jLin = M3{nrm * s, t1 * s, t2 * s};
-        const float3 rW = isA ? rAW : rBW;
-        const M3 jAng = M3{cross(rW, jLin.r0), cross(rW, jLin.r1), cross(rW, jLin.r2)};
-        const M3 K = m3_diag(xyz(c.penalty));
-        const M3 jLinT = m3_transpose(jLin), jAngT = m3_transpose(jAng);
-        const M3 jAngTk = m3_mulm(jAngT, K);
-        acc.lhsLin = m3_add(acc.lhsLin, m3_mulm(m3_mulm(jLinT, K), jLin));
-        acc.lhsAng = m3_add(acc.lhsAng, m3_mulm(jAngTk, jAng));
-        acc.lhsCross = m3_add(acc.lhsCross, m3_mulm(jAngTk, jLin));
-        acc.rhsLin += m3_mul(jLinT, F);
-        acc.rhsAng += m3_mul(jAngT, F);
-    }
+    const uint32_t a = h.x, b = h.y;
+    ManifoldCtx x;
+    x.isA = self == a;
+    x.sphA = (h.w & 2u) != 0;
+    x.sphB = (h.w & 4u) != 0;
+    x.qa = d.posAng[a];
+    x.qb = d.posAng[b];
+    x.dqALin = xyz(d.posLin[a]) - xyz(d.initLin[a]);
+    x.dqAAng = q_sub(x.qa, d.initAng[a]);
+    x.dqBLin = xyz(d.posLin[b]) - xyz(d.initLin[b]);
+    x.dqBAng = q_sub(x.qb, d.initAng[b]);
+    x.nrm = xyz(m.basisN);
+    x.t1 = xyz(m.basisT1);
+    x.t2 = cross(x.nrm, x.t1);
+    x.dynF = m.basisN.w;
+    x.statF = m.basisT1.w;
+    return x;
+}
+// Increment of contact point i of a manifold.
+__device__ __forceinline__ PointInc manifold_point_inc(const Params& P, const ManifoldCtx& x, const ContactGPU& c) {
+    const float3 rAW = x.sphA ? xyz(c.rA) : q_rotate(x.qa, xyz(c.rA));
+    const float3 rBW = x.sphB ? xyz(c.rB) : q_rotate(x.qb, xyz(c.rB));
+    float3 C;
+    float fs, bnd;
+    const float3 F = contact_force(c, x.nrm, x.t1, x.t2, x.dynF, x.statF, P.alpha, x.dqALin, x.dqAAng, x.dqBLin,
+                                   x.dqBAng, rAW, rBW, C, fs, bnd);
+    const float s = x.isA ? 1.0f : -1.0f;
+    const M3 jLin = M3{x.nrm * s, x.t1 * s, x.t2 * s};
+    return point_inc(jLin, x.isA ? rAW : rBW, m3_diag(xyz(c.penalty)), F);
+}
+
+__device__ void stamp_manifold(const Params& P, const DevPtrs& d, const ManifoldGPU& m, uint32_t self, Accum& acc) {
+    const uint32_t n = m.header.z;
+    const ManifoldCtx x = manifold_ctx(d, m, self);
+    for (uint32_t i = 0; i < n; i++) add_inc(acc, manifold_point_inc(P, x, m.contacts[i]));
 }
 
 // StVK membrane, Gauss-Newton Hessian (40_solver.metal:1088-1134).
@@ -749,11 +786,14 @@ __device__ float3 soft_c(const Params& P, const DevPtrs& d, const SoftContactGPU
     return C;
 }
 
-// softContactForce with the two-stage barrier and stampSoft (40_solver.metal:1265-1359).
-__device__ void stamp_soft(const Params& P, const DevPtrs& d, const SoftContactGPU& sc, uint32_t self, Accum& acc) {
-    float3 n, t1, t2, rAW;
-    bool rigidA;
-    const float3 C = soft_c(P, d, sc, n, t1, t2, rAW, rigidA);
+// softContactForce with the two-stage barrier (40_solver.metal:1265-1359):
+// the force, the normal stiffness and the frame of an element contact, and
+// which of its four slots `self` is (-1: none) with that slot's weight.
+struct SoftForce { float3 n, t1, t2, rAW, F; float kN, w; int slot; bool rigidA; };
+__device__ __forceinline__ SoftForce soft_force(const Params& P, const DevPtrs& d, const SoftContactGPU& sc,
+                                                uint32_t self) {
+    SoftForce r;
+    const float3 C = soft_c(P, d, sc, r.n, r.t1, r.t2, r.rAW, r.rigidA);
     float3 F = xyz(sc.penalty) * C + xyz(sc.lambda);
     float kN = sc.penalty.x;
     const float rT = sc.anchorA.x;
@@ -768,34 +808,38 @@ __device__ void stamp_soft(const Params& P, const DevPtrs& d, const SoftContactG
     const float bounds = fabsf(F.x) * sc.normal.w;
     const float fs = sqrtf(F.y * F.y + F.z * F.z);
     if (fs > bounds && fs > 0.0f) {
-        const float r = bounds / fs;
-        F.y *= r;
-        F.z *= r;
+        const float q = bounds / fs;
+        F.y *= q;
+        F.z *= q;
     }
-    int slot = -1;
-    if (sc.ids.x == self) slot = 0;
-    else if (sc.ids.y == self) slot = 1;
-    else if (sc.ids.z == self) slot = 2;
-    else if (sc.ids.w == self) slot = 3;
-    if (slot < 0) return;
-    const float w = slot == 0 ? sc.weights.x : (slot == 1 ? sc.weights.y : (slot == 2 ? sc.weights.z : sc.weights.w));
-    if (slot == 0 && rigidA) {
-        const M3 jLin = M3{n * w, t1 * w, t2 * w};
-        const M3 jAng = M3{cross(rAW, jLin.r0), cross(rAW, jLin.r1), cross(rAW, jLin.r2)};
-        const M3 K = m3_diag(mk3(kN, sc.penalty.y, sc.penalty.z));
-        const M3 jLinT = m3_transpose(jLin), jAngT = m3_transpose(jAng);
-        const M3 jAngTk = m3_mulm(jAngT, K);
-        acc.lhsLin = m3_add(acc.lhsLin, m3_mulm(m3_mulm(jLinT, K), jLin));
-        acc.lhsAng = m3_add(acc.lhsAng, m3_mulm(jAngTk, jAng));
-        acc.lhsCross = m3_add(acc.lhsCross, m3_mulm(jAngTk, jLin));
-        acc.rhsLin += m3_mul(jLinT, F);
-        acc.rhsAng += m3_mul(jAngT, F);
+    r.F = F;
+    r.kN = kN;
+    r.slot = -1;
+    if (sc.ids.x == self) r.slot = 0;
+    else if (sc.ids.y == self) r.slot = 1;
+    else if (sc.ids.z == self) r.slot = 2;
+    else if (sc.ids.w == self) r.slot = 3;
+    r.w = r.slot == 0 ? sc.weights.x : (r.slot == 1 ? sc.weights.y : (r.slot == 2 ? sc.weights.z : sc.weights.w));
+    return r;
+}
+// Increment of the rigid slot 0 of an element contact (stampSoft's 6-DOF branch).
+__device__ __forceinline__ PointInc soft_rigid_inc(const SoftContactGPU& sc, const SoftForce& f) {
+    const float w = f.w;
+    return point_inc(M3{f.n * w, f.t1 * w, f.t2 * w}, f.rAW, m3_diag(mk3(f.kN, sc.penalty.y, sc.penalty.z)), f.F);
+}
+
+// stampSoft (40_solver.metal:1265-1359).
+__device__ void stamp_soft(const Params& P, const DevPtrs& d, const SoftContactGPU& sc, uint32_t self, Accum& acc) {
+    const SoftForce f = soft_force(P, d, sc, self);
+    if (f.slot < 0) return;
+    if (f.slot == 0 && f.rigidA) {
+        add_inc(acc, soft_rigid_inc(sc, f));
     } else {
-        const float w2 = w * w;
-        acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(n, n), kN * w2));
-        acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(t1, t1), sc.penalty.y * w2));
-        acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(t2, t2), sc.penalty.z * w2));
-        acc.rhsLin += (n * F.x + t1 * F.y + t2 * F.z) * w;
+        const float w2 = f.w * f.w;
+        acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(f.n, f.n), f.kN * w2));
+        acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(f.t1, f.t1), sc.penalty.y * w2));
+        acc.lhsLin = m3_add(acc.lhsLin, m3_scale(m3_outer(f.t2, f.t2), sc.penalty.z * w2));
+        acc.rhsLin += (f.n * f.F.x + f.t1 * f.F.y + f.t2 * f.F.z) * f.w;
     }
 }
 
@@ -843,14 +887,11 @@ __device__ __forceinline__ void keep_body(const Params& P, const DevPtrs& d, uin
     if (rigid) d.angNext[body] = d.posAng[body];
 }
 
-// One body on an 8-lane group; lane 0 writes the result.
-__device__ void primal_body(const Params& P, const DevPtrs& d, uint32_t body, uint32_t lane, unsigned mask) {
-    const float4 shp = d.shape[body];
+// The 8 lanes' partial systems of one body (lane l stamped entries l,
+// l + 8, ...) folded by an xor butterfly; lane 0 solves and writes.
+__device__ __forceinline__ void body_commit(const Params& P, const DevPtrs& d, uint32_t body, float4 shp,
+                                            uint32_t lane, unsigned mask, Accum acc) {
     const bool rigid = shp.w >= 0.0f;
-    Accum acc{m3_zero(), m3_zero(), m3_zero(), s3(0), s3(0)};
-    const AdjView v = adj_view(d, body);
-    const uint32_t cnt = v.count();
-    for (uint32_t k = lane; k < cnt; k += 8) stamp_entry(P, d, v.at(k), body, acc);
 #pragma unroll
     for (int o = 4; o >= 1; o >>= 1) {
         add_shfl3(mask, acc.lhsLin.r0, o);
@@ -901,6 +942,16 @@ __device__ void primal_body(const Params& P, const DevPtrs& d, uint32_t body, ui
     if (rigid) d.posAng[body] = q_addw(d.posAng[body], dxAng);
 }
 
+// One body on an 8-lane group; lane 0 writes the result.
+__device__ void primal_body(const Params& P, const DevPtrs& d, uint32_t body, uint32_t lane, unsigned mask) {
+    const float4 shp = d.shape[body];
+    Accum acc{m3_zero(), m3_zero(), m3_zero(), s3(0), s3(0)};
+    const AdjView v = adj_view(d, body);
+    const uint32_t cnt = v.count();
+    for (uint32_t k = lane; k < cnt; k += 8) stamp_entry(P, d, v.at(k), body, acc);
+    body_commit(P, d, body, shp, lane, mask, acc);
+}
+
 __global__ void k_primal(const Params P, const DevPtrs d, uint32_t color, uint32_t count) {
     pdl_prologue();
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -911,6 +962,103 @@ __global__ void k_primal(const Params P, const DevPtrs d, uint32_t color, uint32
     // one 8-lane group per body, striding over the color (uniform across
     // the group)
     for (uint32_t slot = tid >> 3; slot < n; slot += groups) primal_body(P, d, d.colorList[s + slot], lane, mask);
+}
+
+// ---------------------------------------------------------------------------
+// Wide primal: one block per body, for a static color's non-lean bodies
+// (rigid bodies and particles with joints).  A rigid body under a pile of
+// particles carries hundreds of contact entries; on an 8-lane group its
+// lanes would stamp them one after another while the rest of the color has
+// long finished.  Here the block evaluates the contact points of every
+// manifold entry and every rigid element-contact slot at once into shared
+// memory, then 8 lanes add them in the 8-lane order (lane l: entries l,
+// l + 8, ...; each entry's points in order) — every accumulator component
+// takes one add per point, so the sums are those of the sequential stamps.
+// Other entries, and points past the staging capacity, are stamped inline
+// by the folding lanes in the same order.
+// ---------------------------------------------------------------------------
+constexpr int kWideThreads = 128;
+constexpr int kWideEntries = 512;          // entries whose points may be staged
+constexpr int kWidePoints = 320;           // staged points (33 floats each)
+constexpr uint32_t kWideInline = 0xFFFFFFFFu;
+
+__global__ void __launch_bounds__(kWideThreads) k_primal_wide(const Params P, const DevPtrs d, uint32_t color,
+                                                             uint32_t first) {
+    __shared__ PointInc pts[kWidePoints];
+    __shared__ uint32_t entOff[kWideEntries];  // (first point << 8) | points, or kWideInline
+    __shared__ uint32_t warpSums[kWideThreads / 32];
+    pdl_prologue();
+    const uint32_t tid = threadIdx.x, lane32 = tid & 31u, warp = tid >> 5;
+    const uint32_t body = d.colorLaunch[d.colorStart[color] + first + blockIdx.x];
+    const float4 shp = d.shape[body];
+    const AdjView v = adj_view(d, body);
+    const uint32_t cnt = v.count();
+    const uint32_t staged = min(cnt, (uint32_t)kWideEntries);
+    uint32_t base = 0;                          // points taken by earlier chunks
+    for (uint32_t c0 = 0; c0 < staged; c0 += kWideThreads) {
+        const uint32_t k = c0 + tid;
+        uint32_t entry = 0, np = 0;
+        if (k < staged) {
+            entry = v.at(k);
+            const uint32_t kind = entry >> ADJ_KIND_SHIFT, idx = entry & ADJ_INDEX_MASK;
+            if (kind == FK_MANIFOLD) {
+                np = d.manifolds[idx].header.z;
+            } else if (kind == FK_SOFT) {
+                const SoftContactGPU& sc = d.soft[idx];
+                const bool rigidA = (__float_as_uint(sc.anchorA.w) & SCF_RIGID_A) != 0;
+                np = (rigidA && sc.ids.x == body) ? 1u : 0u;
+            }
+        }
+        // exclusive scan of the chunk's point counts
+        uint32_t incl = np;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((int)lane32 >= o) incl += y;
+        }
+        if (lane32 == 31) warpSums[warp] = incl;
+        __syncthreads();
+        uint32_t before = base, total = 0;
+#pragma unroll
+        for (int w = 0; w < kWideThreads / 32; w++) {
+            const uint32_t ws = warpSums[w];
+            if (w < (int)warp) before += ws;
+            total += ws;
+        }
+        const uint32_t off = before + incl - np;
+        const bool fits = np > 0 && off + np <= (uint32_t)kWidePoints;
+        if (k < staged) entOff[k] = fits ? ((off << 8) | np) : kWideInline;
+        if (fits) {
+            const uint32_t kind = entry >> ADJ_KIND_SHIFT, idx = entry & ADJ_INDEX_MASK;
+            if (kind == FK_MANIFOLD) {
+                const ManifoldGPU& m = d.manifolds[idx];
+                const ManifoldCtx x = manifold_ctx(d, m, body);
+                for (uint32_t i = 0; i < np; i++) pts[off + i] = manifold_point_inc(P, x, m.contacts[i]);
+            } else {
+                const SoftContactGPU& sc = d.soft[idx];
+                pts[off] = soft_rigid_inc(sc, soft_force(P, d, sc, body));
+            }
+        }
+        base += total;
+        __syncthreads();                        // warpSums is reused by the next chunk
+    }
+    if (tid >= 8) return;
+    Accum acc{m3_zero(), m3_zero(), m3_zero(), s3(0), s3(0)};
+    for (uint32_t k = tid; k < cnt; k += 8) {
+        const uint32_t eo = k < (uint32_t)kWideEntries ? entOff[k] : kWideInline;
+        if (eo != kWideInline) {
+            const uint32_t off = eo >> 8, np = eo & 0xFFu;
+            for (uint32_t i = 0; i < np; i++) add_inc(acc, pts[off + i]);
+        } else {
+            stamp_entry(P, d, v.at(k), body, acc);
+        }
+    }
+    body_commit(P, d, body, shp, tid, 0xFFu, acc);
+}
+
+void launch_primal_wide(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count, uint32_t first,
+                        cudaStream_t st) {
+    if (count) launch_pdl(k_primal_wide, count, kWideThreads, st, P, d, color, first);
 }
 
 // ---------------------------------------------------------------------------
@@ -1198,6 +1346,61 @@ __device__ __forceinline__ void stamp_entry_particle(const Params& P, const DevP
     acc->rhs = full.rhsLin;
 }
 
+// Terms of adjacency entry k of particle `body`.  A tet entry reads its
+// record from the body's incidence slot (contiguous over consecutive k)
+// instead of through the entry; `entry` is what the generic stamp needs.
+template <bool CLOTH>
+__device__ __forceinline__ void particle_entry_terms(const Params& P, const DevPtrs& d, const AdjView& v,
+                                                     uint32_t body, uint32_t k, ParticleTerms& t, uint32_t& entry) {
+    const uint32_t kt = k - v.nPre - v.nMan;
+    if (d.tetInc && k >= v.nPre + v.nMan && kt < v.nTet) {
+        entry = (FK_TET << ADJ_KIND_SHIFT);
+        tet_terms(d, d.tetInc[v.postBase + kt], body, t);
+    } else {
+        entry = v.at(k);
+        particle_terms<CLOTH>(P, d, entry, body, t);
+    }
+}
+
+// Adds one entry's terms to a particle's linear system, in the order of
+// operations of the stamps (every instance folds through this function, so
+// any lane layout yields the same floats).
+template <bool GENERAL, bool CLOTH>
+__device__ __forceinline__ void fold_particle_term(const Params& P, const DevPtrs& d, const ParticleTerms& u,
+                                                   uint32_t e, uint32_t body, ParticleAccum& acc) {
+    if (u.kind == 1u) {
+        acc.rhs += u.rhs;
+        acc.lhs = m3_add(acc.lhs, m3_diag(s3(u.c.x)));
+        acc.lhs = m3_add(acc.lhs, M3{mk3(u.a.x, u.b.x, u.b.y), mk3(u.b.x, u.a.y, u.b.z),
+                                     mk3(u.b.y, u.b.z, u.a.z)});
+    } else if (u.kind == 2u) {
+        acc.lhs = m3_add(acc.lhs, M3{u.a, u.b, u.c});
+        acc.rhs += u.rhs;
+    } else if (CLOTH && u.kind == TERM_MEMBRANE) {
+        acc.rhs += u.rhs;
+        acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.a, u.a), u.s.x));
+        acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.b, u.b), u.s.x));
+        acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.c, u.c), u.s.y));
+        acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.e, u.e), u.s.z));
+    } else if (CLOTH && u.kind == TERM_BEND) {
+        acc.rhs += u.rhs;
+        acc.lhs = m3_add(acc.lhs, m3_diag(s3(u.s.x)));
+    } else if (CLOTH && u.kind == TERM_SPRING) {
+        acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.a, u.a), u.s.x));
+        acc.rhs += u.rhs;
+        if (u.s.y > 0.0f)
+            acc.lhs = m3_add(acc.lhs, m3_add(m3_diag(s3(u.s.y)), m3_scale(m3_outer(u.a, u.a), -u.s.y)));
+    } else if (CLOTH && u.kind == TERM_SOFT) {
+        acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.a, u.a), u.s.x));
+        acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.b, u.b), u.s.y));
+        acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.c, u.c), u.s.z));
+        acc.rhs += u.rhs;
+    } else if (GENERAL && u.kind != TERM_NONE) {
+        stamp_entry_particle(P, d, e, body, &acc);
+    }
+}
+
+
 // The particle system's angular block is the identity and its cross block
 // zero.  Every term of the 6x6 LDL^T that involves them is then an exact
 // "x - (+0)" (L4x..L6x, y4..y6, z4..z6 and xAng are all +0), so this 3x3
@@ -1229,6 +1432,24 @@ __device__ __forceinline__ float3 solve3x3_particle(const M3& a, float3 b) {
     return mk3(x.x * s1, x.y * s2, x.z * s3_);
 }
 
+// Inertia, solve, trust region, OGC bound and commit of a particle whose
+// stamped system is (acc.lhs, acc.rhs); lane 0 of its group calls this.
+__device__ __forceinline__ void particle_commit(const Params& P, const DevPtrs& d, uint32_t body, float4 shp,
+                                                float4 pl, float4 inert, ParticleAccum acc) {
+    const float mass = pl.w;
+    const float dt2 = P.dt * P.dt;
+    acc.lhs = m3_add(acc.lhs, m3_diag(s3(mass / dt2)));
+    acc.rhs += (xyz(pl) - xyz(inert)) * (mass / dt2);
+    float3 dxLin = solve3x3_particle(acc.lhs, -acc.rhs);
+    if (!finite3(dxLin)) { keep_body(P, d, body, pl, false); return; }
+    const float maxLin = 0.35f * fabsf(shp.w);
+    const float lin2 = dot(dxLin, dxLin);
+    if (lin2 > maxLin * maxLin) dxLin *= maxLin * rsq(lin2);
+    if (P.ogc) dxLin = ogc_truncate(d, body, dxLin, xyz(pl), -shp.w);
+    if (P.colorJacobi) { d.posNext[body] = mk4(xyz(pl) + dxLin, mass); return; }
+    d.posLin[body] = mk4(xyz(pl) + dxLin, mass);
+}
+
 // Primal for one color with LANES consecutive lanes per body (8, 16 or 32,
 // chosen per color from its bodies' adjacency sizes).  Lane p of a group
 // evaluates entry base + p; logical lane l < 8 then folds entries
@@ -1246,9 +1467,12 @@ constexpr int kPrimalUnroll = AVBD_PRIMAL_UNROLL;
 #ifndef AVBD_PARTICLE_PRIMAL_MIN_BLOCKS
 #define AVBD_PARTICLE_PRIMAL_MIN_BLOCKS 1
 #endif
+#ifndef AVBD_LEAN_CLOTH_MIN_BLOCKS
+#define AVBD_LEAN_CLOTH_MIN_BLOCKS 5
+#endif
 template <int LANES, bool GENERAL, bool CLOTH, bool RESID = false>
-__global__ void __launch_bounds__(128, GENERAL ? 4 : AVBD_PARTICLE_PRIMAL_MIN_BLOCKS) k_primal_group(const Params P, const DevPtrs d, uint32_t color,
-                                                      uint32_t count) {
+__global__ void __launch_bounds__(128, GENERAL ? 4 : (CLOTH ? AVBD_LEAN_CLOTH_MIN_BLOCKS : AVBD_PARTICLE_PRIMAL_MIN_BLOCKS)) k_primal_group(const Params P, const DevPtrs d, uint32_t color,
+                                                      uint32_t count, uint32_t first) {
     constexpr int GROUPS = 32 / LANES;
     pdl_prologue();
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1260,7 +1484,9 @@ __global__ void __launch_bounds__(128, GENERAL ? 4 : AVBD_PARTICLE_PRIMAL_MIN_BL
     const unsigned mask = LANES == 32 ? 0xffffffffu
                                       : (((1u << LANES) - 1u) << ((threadIdx.x & 31u) & ~(uint32_t)(LANES - 1)));
     (void)GROUPS;
-    const uint32_t body = d.colorList[s + slot];
+    // the solve takes its body from the color's launch order (lean
+    // particles first); the residual pass walks the color list itself
+    const uint32_t body = RESID ? d.colorList[s + slot] : d.colorLaunch[s + first + slot];
     const float4 shp = d.shape[body];
     if (GENERAL && shp.w >= 0.0f) {                          // rigid: the 8-lane path
         const unsigned mask8 = mask & (0xFFu << ((threadIdx.x & 31u) & ~(uint32_t)(LANES - 1)));
@@ -1283,18 +1509,7 @@ __global__ void __launch_bounds__(128, GENERAL ? 4 : AVBD_PARTICLE_PRIMAL_MIN_BL
         ParticleTerms t;
         t.kind = 0;
         uint32_t entry = 0;
-        if (k < cnt) {
-            // a tet entry reads its record from the body's incidence slot
-            // (contiguous over the lanes) instead of through the entry
-            const uint32_t kt = k - v.nPre - v.nMan;
-            if (d.tetInc && k >= v.nPre + v.nMan && kt < v.nTet) {
-                entry = (FK_TET << ADJ_KIND_SHIFT);
-                tet_terms(d, d.tetInc[v.postBase + kt], body, t);
-            } else {
-                entry = v.at(k);
-                particle_terms<CLOTH>(P, d, entry, body, t);
-            }
-        }
+        if (k < cnt) particle_entry_terms<CLOTH>(P, d, v, body, k, t, entry);
 #pragma unroll
         for (int j = 0; j < LANES / 8; j++) {
             const int src = (int)(lane & 7u) + 8 * j;
@@ -1322,38 +1537,7 @@ __global__ void __launch_bounds__(128, GENERAL ? 4 : AVBD_PARTICLE_PRIMAL_MIN_BL
             }
             e = __shfl_sync(mask, entry, src, LANES);
             }
-            if (lane < 8) {
-                if (u.kind == 1u) {
-                    acc.rhs += u.rhs;
-                    acc.lhs = m3_add(acc.lhs, m3_diag(s3(u.c.x)));
-                    acc.lhs = m3_add(acc.lhs, M3{mk3(u.a.x, u.b.x, u.b.y), mk3(u.b.x, u.a.y, u.b.z),
-                                                 mk3(u.b.y, u.b.z, u.a.z)});
-                } else if (u.kind == 2u) {
-                    acc.lhs = m3_add(acc.lhs, M3{u.a, u.b, u.c});
-                    acc.rhs += u.rhs;
-                } else if (CLOTH && u.kind == TERM_MEMBRANE) {
-                    acc.rhs += u.rhs;
-                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.a, u.a), u.s.x));
-                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.b, u.b), u.s.x));
-                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.c, u.c), u.s.y));
-                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.e, u.e), u.s.z));
-                } else if (CLOTH && u.kind == TERM_BEND) {
-                    acc.rhs += u.rhs;
-                    acc.lhs = m3_add(acc.lhs, m3_diag(s3(u.s.x)));
-                } else if (CLOTH && u.kind == TERM_SPRING) {
-                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.a, u.a), u.s.x));
-                    acc.rhs += u.rhs;
-                    if (u.s.y > 0.0f)
-                        acc.lhs = m3_add(acc.lhs, m3_add(m3_diag(s3(u.s.y)), m3_scale(m3_outer(u.a, u.a), -u.s.y)));
-                } else if (CLOTH && u.kind == TERM_SOFT) {
-                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.a, u.a), u.s.x));
-                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.b, u.b), u.s.y));
-                    acc.lhs = m3_add(acc.lhs, m3_scale(m3_outer(u.c, u.c), u.s.z));
-                    acc.rhs += u.rhs;
-                } else if (GENERAL && u.kind != TERM_NONE) {
-                    stamp_entry_particle(P, d, e, body, &acc);
-                }
-            }
+            if (lane < 8) fold_particle_term<GENERAL, CLOTH>(P, d, u, e, body, acc);
         }
     }
     // xor butterfly over the 8 logical lanes (offsets 4, 2, 1)
@@ -1365,33 +1549,168 @@ __global__ void __launch_bounds__(128, GENERAL ? 4 : AVBD_PARTICLE_PRIMAL_MIN_BL
         acc.rhs = acc.rhs + mk3(__shfl_xor_sync(mask, acc.rhs.x, o, LANES), __shfl_xor_sync(mask, acc.rhs.y, o, LANES), __shfl_xor_sync(mask, acc.rhs.z, o, LANES));
     }
     if (lane != 0) return;
-    const float mass = pl.w;
-    const float dt2 = P.dt * P.dt;
     if (RESID) {
-        const float3 r = acc.rhs + (xyz(pl) - xyz(inert)) * (mass / dt2);
+        const float3 r = acc.rhs + (xyz(pl) - xyz(inert)) * (pl.w / (P.dt * P.dt));
         d.learnResidBodies[s + slot] = dot(r, r);
         return;
     }
-    acc.lhs = m3_add(acc.lhs, m3_diag(s3(mass / dt2)));
-    acc.rhs += (xyz(pl) - xyz(inert)) * (mass / dt2);
-    float3 dxLin = solve3x3_particle(acc.lhs, -acc.rhs);
-    if (!finite3(dxLin)) { keep_body(P, d, body, pl, false); return; }
-    const float maxLin = 0.35f * fabsf(shp.w);
-    const float lin2 = dot(dxLin, dxLin);
-    if (lin2 > maxLin * maxLin) dxLin *= maxLin * rsq(lin2);
-    if (P.ogc) dxLin = ogc_truncate(d, body, dxLin, xyz(pl), -shp.w);
-    if (P.colorJacobi) { d.posNext[body] = mk4(xyz(pl) + dxLin, mass); return; }
-    d.posLin[body] = mk4(xyz(pl) + dxLin, mass);
+    particle_commit(P, d, body, shp, pl, inert, acc);
 }
 
 template <bool GENERAL, bool CLOTH>
 static void launch_primal_group(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count,
-                                uint32_t lanes, cudaStream_t st) {
+                                uint32_t first, uint32_t lanes, cudaStream_t st) {
     const int T = 128;
     const uint32_t blocks = (count * lanes + T - 1) / T;
-    if (lanes <= 8) launch_pdl(k_primal_group<8, GENERAL, CLOTH>, blocks, T, st, P, d, color, count);
-    else if (lanes <= 16) launch_pdl(k_primal_group<16, GENERAL, CLOTH>, blocks, T, st, P, d, color, count);
-    else launch_pdl(k_primal_group<32, GENERAL, CLOTH>, blocks, T, st, P, d, color, count);
+    if (lanes <= 8) launch_pdl(k_primal_group<8, GENERAL, CLOTH>, blocks, T, st, P, d, color, count, first);
+    else if (lanes <= 16) launch_pdl(k_primal_group<16, GENERAL, CLOTH>, blocks, T, st, P, d, color, count, first);
+    else launch_pdl(k_primal_group<32, GENERAL, CLOTH>, blocks, T, st, P, d, color, count, first);
+}
+
+// ---------------------------------------------------------------------------
+// Staged primal.  A block takes 16 bodies of the color (one 8-lane group
+// each, the reference's SIMD layout) and evaluates the terms of all their
+// adjacency entries as one flat list — every thread of the block on
+// consecutive entries, whatever each body's entry count — into shared
+// memory; each group then folds its body's entries in the fixed order
+// (logical lane l: entries l, l + 8, ...; xor butterfly 4, 2, 1) and lane 0
+// solves.  The grouped kernel above idles the lanes past a body's last
+// entry and moves every term through warp shuffles; here the evaluation
+// runs dense and the fold reads shared memory.  Entries past the block's
+// staging capacity are evaluated inline by the fold, in the same order.
+// Rigid bodies (GENERAL) take the 8-lane 6x6 path unchanged.
+// ---------------------------------------------------------------------------
+constexpr int kStagedThreads = 128;
+constexpr int kStagedGroups = kStagedThreads / 8;
+constexpr int kStagedSlots = 512;       // staged entries per block
+constexpr int kStagedWords = 16;        // kind, rhs, a, b, c, s (e = a + b is recomputed)
+
+struct StagedBody {
+    uint32_t body, cnt, staged, off;
+    uint32_t preBase, nPre, dynBase, nMan, nDyn, postBase, nTet, nPost;
+};
+
+__device__ __forceinline__ AdjView staged_view(const DevPtrs& d, const StagedBody& b) {
+    AdjView v;
+    v.pre = d.preList + b.preBase; v.nPre = b.nPre;
+    v.dyn = d.dynList + b.dynBase; v.nDyn = b.nDyn; v.nMan = b.nMan;
+    v.post = d.postList + b.postBase; v.nPost = b.nPost; v.nTet = b.nTet; v.postBase = b.postBase;
+    return v;
+}
+
+template <bool GENERAL, bool CLOTH>
+__global__ void __launch_bounds__(kStagedThreads, GENERAL ? 4 : 5)
+k_primal_staged(const Params P, const DevPtrs d, uint32_t color, uint32_t count, uint32_t first) {
+    __shared__ float slots[kStagedWords][kStagedSlots];
+    __shared__ StagedBody info[kStagedGroups];
+    __shared__ uint32_t offs[kStagedGroups + 1];
+    pdl_prologue();
+    const uint32_t tid = threadIdx.x;
+    const uint32_t s = d.colorStart[color] + first;
+    const uint32_t head = blockIdx.x * kStagedGroups;
+    // bodies of the block, their adjacency views and an exclusive scan of
+    // their entry counts (warp 0, one lane per group)
+    if (tid < 32) {
+        uint32_t cnt = 0, body = 0xFFFFFFFFu;
+        StagedBody b{};
+        if (tid < kStagedGroups && head + tid < count) {
+            body = d.colorLaunch[s + head + tid];
+            const float4 shp = d.shape[body];
+            const uint4 seg = d.staticSeg[body];
+            b.preBase = seg.x; b.nPre = seg.y; b.postBase = seg.z; b.nPost = seg.w;
+            b.dynBase = d.dynStart[body]; b.nDyn = d.dynCount[body]; b.nMan = d.dynSplit[body];
+            b.nTet = d.postTets[body];
+            cnt = b.nPre + b.nDyn + b.nPost;
+            b.cnt = cnt;
+            if (GENERAL && shp.w >= 0.0f) cnt = 0;           // rigid: stages nothing
+        }
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if ((int)tid >= o) incl += y;
+        }
+        const uint32_t off = incl - cnt;
+        if (tid < kStagedGroups) {
+            b.body = body;
+            b.off = off;
+            b.staged = off >= (uint32_t)kStagedSlots ? 0u : min(cnt, (uint32_t)kStagedSlots - off);
+            info[tid] = b;
+            offs[tid] = off;
+        }
+        if (tid == kStagedGroups - 1) offs[kStagedGroups] = min(incl, (uint32_t)kStagedSlots);
+    }
+    __syncthreads();
+    // every staged entry of the block, dense over the threads
+    const uint32_t total = offs[kStagedGroups];
+    for (uint32_t i = tid; i < total; i += kStagedThreads) {
+        uint32_t g = 0;
+#pragma unroll
+        for (uint32_t step = kStagedGroups / 2; step >= 1; step >>= 1)
+            if (offs[g + step] <= i) g += step;
+        const StagedBody& b = info[g];
+        const AdjView v = staged_view(d, b);
+        ParticleTerms t;
+        uint32_t entry = 0;
+        particle_entry_terms<CLOTH>(P, d, v, b.body, i - b.off, t, entry);
+        slots[0][i] = __uint_as_float(t.kind);
+        slots[1][i] = t.kind == TERM_SERIAL ? __uint_as_float(entry) : t.rhs.x;
+        slots[2][i] = t.rhs.y;  slots[3][i] = t.rhs.z;
+        slots[4][i] = t.a.x;    slots[5][i] = t.a.y;    slots[6][i] = t.a.z;
+        slots[7][i] = t.b.x;    slots[8][i] = t.b.y;    slots[9][i] = t.b.z;
+        slots[10][i] = t.c.x;   slots[11][i] = t.c.y;   slots[12][i] = t.c.z;
+        if (CLOTH) { slots[13][i] = t.s.x; slots[14][i] = t.s.y; slots[15][i] = t.s.z; }
+    }
+    __syncthreads();
+    // the fold: group g, logical lane l
+    const uint32_t g = tid >> 3, lane = tid & 7u;
+    if (head + g >= count) return;
+    const StagedBody b = info[g];
+    const unsigned mask8 = 0xFFu << (tid & 24u);
+    const float4 shp = d.shape[b.body];
+    if (GENERAL && shp.w >= 0.0f) {
+        primal_body(P, d, b.body, lane, mask8);
+        return;
+    }
+    float4 pl = make_float4(0, 0, 0, 0), inert = make_float4(0, 0, 0, 0);
+    if (lane == 0) { pl = d.posLin[b.body]; inert = d.inertLin[b.body]; }
+    ParticleAccum acc{m3_zero(), s3(0)};
+    for (uint32_t k = lane; k < b.cnt; k += 8) {
+        ParticleTerms u;
+        uint32_t e = 0;
+        if (k < b.staged) {
+            const uint32_t i = b.off + k;
+            u.kind = __float_as_uint(slots[0][i]);
+            e = __float_as_uint(slots[1][i]);
+            u.rhs = mk3(slots[1][i], slots[2][i], slots[3][i]);
+            u.a = mk3(slots[4][i], slots[5][i], slots[6][i]);
+            u.b = mk3(slots[7][i], slots[8][i], slots[9][i]);
+            u.c = mk3(slots[10][i], slots[11][i], slots[12][i]);
+            if (CLOTH) {
+                u.s = mk3(slots[13][i], slots[14][i], slots[15][i]);
+                u.e = u.a + u.b;                             // as the membrane terms form it
+            }
+        } else {
+            particle_entry_terms<CLOTH>(P, d, staged_view(d, b), b.body, k, u, e);
+        }
+        fold_particle_term<GENERAL, CLOTH>(P, d, u, e, b.body, acc);
+    }
+#pragma unroll
+    for (int o = 4; o >= 1; o >>= 1) {
+        add_shfl3(mask8, acc.lhs.r0, o);
+        add_shfl3(mask8, acc.lhs.r1, o);
+        add_shfl3(mask8, acc.lhs.r2, o);
+        add_shfl3(mask8, acc.rhs, o);
+    }
+    if (lane != 0) return;
+    particle_commit(P, d, b.body, shp, pl, inert, acc);
+}
+
+template <bool GENERAL, bool CLOTH>
+static void launch_primal_staged(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count,
+                                 uint32_t first, cudaStream_t st) {
+    const uint32_t blocks = (count + kStagedGroups - 1) / kStagedGroups;
+    launch_pdl(k_primal_staged<GENERAL, CLOTH>, blocks, kStagedThreads, st, P, d, color, count, first);
 }
 
 void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color, uint32_t count,
@@ -1408,12 +1727,26 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
         const uint32_t need = (upper * 8 + TT - 1) / TT, wave = z.dynBlocks ? z.dynBlocks : 148u * 4u;
         launch_pdl(k_primal, need < wave ? need : wave, TT, st, P, d, color, count);
     } else {
-        // the grouped kernel needs the color's body count on the host
-        const uint32_t lanes_ = lanes < 8 ? 8 : (lanes > 32 ? 32 : lanes);
-        const uint32_t w = lanes_ <= 8 ? 8 : (lanes_ <= 16 ? 16 : 32);
-        if (z.particleFastPath) launch_primal_group<false, false>(P, d, color, upper, w, st);
-        else if (P.cloth || P.ogc) launch_primal_group<true, true>(P, d, color, upper, w, st);
-        else launch_primal_group<true, false>(P, d, color, upper, w, st);
+        // The grouped and staged kernels need the color's body count on the
+        // host.  The color's lean particles (the head of its launch order)
+        // run in the instance without the rigid and generic-stamp paths,
+        // which needs far fewer registers; the rest in the general one.
+        const bool cloth = P.cloth || P.ogc;
+        const uint32_t lean = z.particleFastPath ? upper : (z.colorLean ? min(z.colorLean[color], upper) : 0u);
+        const uint32_t rest = upper - lean;
+        if (lean) {
+            if (lanes == AVBD_PRIMAL_STAGED) {
+                if (cloth) launch_primal_staged<false, true>(P, d, color, lean, 0, st);
+                else launch_primal_staged<false, false>(P, d, color, lean, 0, st);
+            } else {
+                const uint32_t lanes_ = lanes < 8 ? 8 : (lanes > 32 ? 32 : lanes);
+                const uint32_t w = lanes_ <= 8 ? 8 : (lanes_ <= 16 ? 16 : 32);
+                if (cloth) launch_primal_group<false, true>(P, d, color, lean, 0, w, st);
+                else launch_primal_group<false, false>(P, d, color, lean, 0, w, st);
+            }
+        }
+        // the rest: a block per body (rigid bodies with many contacts)
+        launch_primal_wide(P, d, color, rest, lean, st);
     }
 }
 
@@ -1429,13 +1762,13 @@ void launch_residual(const Params& P, const DevPtrs& d, const Sizes& z, float* p
             const uint32_t w = lanes <= 8 ? 8u : (lanes <= 16 ? 16u : 32u);
             const uint32_t blocks = (count * w + 127) / 128;
             if (z.particleFastPath) {
-                if (w == 8) k_primal_group<8, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count);
-                else if (w == 16) k_primal_group<16, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count);
-                else k_primal_group<32, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count);
+                if (w == 8) k_primal_group<8, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count, 0u);
+                else if (w == 16) k_primal_group<16, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count, 0u);
+                else k_primal_group<32, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count, 0u);
             } else if (P.cloth || P.ogc) {
-                k_primal_group<32, true, true, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, g, color, count);
+                k_primal_group<32, true, true, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, g, color, count, 0u);
             } else {
-                k_primal_group<32, true, false, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, g, color, count);
+                k_primal_group<32, true, false, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, g, color, count, 0u);
             }
         };
         // every body at once: 8 lanes per body keep the most bodies in
@@ -1447,8 +1780,8 @@ void launch_residual(const Params& P, const DevPtrs& d, const Sizes& z, float* p
         DevPtrs g = d;
         g.learnResidBodies = perBody;
         const uint32_t blocks = (n * 8 + 127) / 128;
-        if (P.cloth || P.ogc) k_primal_group<8, true, true, true><<<blocks, 128, 0, st>>>(P, g, 0u, n);
-        else k_primal_group<8, true, false, true><<<blocks, 128, 0, st>>>(P, g, 0u, n);
+        if (P.cloth || P.ogc) k_primal_group<8, true, true, true><<<blocks, 128, 0, st>>>(P, g, 0u, n, 0u);
+        else k_primal_group<8, true, false, true><<<blocks, 128, 0, st>>>(P, g, 0u, n, 0u);
     }
     k_sum_fixed<<<1, 1024, 0, st>>>(perBody, n, total);
 }

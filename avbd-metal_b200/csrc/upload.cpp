@@ -735,6 +735,32 @@ int upload_scene(const avbd_scene_desc* s, HostScene& H, std::string& err) {
             H.colorLanes[c] = mx <= 8 ? 8u : (mx <= 16 ? 16u : 32u);
         }
     }
+    // launch order of each static color: lean particles, then the rest
+    // (bodies are independent within a color, so the order only decides
+    // which kernel instance takes a body)
+    H.colorLaunch.clear();
+    H.colorLean.assign(MAX_COLORS, 0);
+    if (!H.dynamicColoring) {
+        const bool clothKinds = H.cloth || H.ogc;
+        auto lean = [&](uint32_t b) {
+            if (H.shape[b].w >= 0.0f) return false;                       // rigid
+            for (uint32_t e : pre[b])
+                if (!clothKinds || (e >> ADJ_KIND_SHIFT) != FK_SPRING) return false;
+            if (!clothKinds)
+                for (uint32_t e : post[b])
+                    if ((e >> ADJ_KIND_SHIFT) != FK_TET) return false;
+            return true;
+        };
+        H.colorLaunch.reserve(H.colorList.size());
+        for (int c = 0; c < MAX_COLORS; c++) {
+            const uint32_t s0 = H.colorStart[c], s1 = H.colorStart[c + 1];
+            for (uint32_t i = s0; i < s1; i++)
+                if (lean(H.colorList[i])) H.colorLaunch.push_back(H.colorList[i]);
+            H.colorLean[c] = (uint32_t)H.colorLaunch.size() - s0;
+            for (uint32_t i = s0; i < s1; i++)
+                if (!lean(H.colorList[i])) H.colorLaunch.push_back(H.colorList[i]);
+        }
+    }
     H.staticSeg.assign(nb, u4{});
     H.postTets.assign(nb, 0);
     for (uint32_t b = 0; b < nb; b++) {

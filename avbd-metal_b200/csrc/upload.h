@@ -48,6 +48,12 @@ struct HostScene {
     // static palette (soft scenes) in final form
     std::vector<uint32_t> colors, colorStart, colorList, colorCounts;
     std::vector<uint32_t> colorLanes;      // lanes per body for each static color
+    // Primal launch order of each static color: the color's "lean"
+    // particles first (every adjacency entry one of the particle term kinds:
+    // tets, one-point manifolds, and with cloth or OGC also springs,
+    // membranes, bends and element contacts), then the rest (rigid bodies,
+    // particles with joints).  colorLean[c] counts the lean ones.
+    std::vector<uint32_t> colorLaunch, colorLean;
 
     // Static per-body adjacency, split around the per-frame contact entries:
     // pre = joints + springs (kinds 0, 1), post = tets (kind 3), each sorted.

@@ -373,8 +373,10 @@ typedef struct avbd_profile {
     uint64_t kernels_per_frame;   /* kernel nodes in one frame's graph      */
     double stage_ms[16];          /* summed GPU time per stage              */
     uint64_t stage_launches[16];  /* kernel launches per stage              */
-    uint32_t color_lanes[64];     /* lanes per body of each static color's
-                                   * primal, as chosen by the autotuner      */
+    uint32_t color_lanes[64];     /* primal variant of each static color's
+                                   * lean particles, as chosen by the
+                                   * autotuner: 8, 16 or 32 lanes per body
+                                   * or AVBD_PRIMAL_VARIANT_STAGED           */
     /* dynamic coloring: block shape of the rigid primal's grid-stride
      * launch, chosen per body-count bucket (floor(log2(dynamic bodies)))
      * by timing candidate shapes on the first frames of the first solver
@@ -384,6 +386,15 @@ typedef struct avbd_profile {
     uint32_t dyn_bucket;
     uint32_t dyn_candidates;      /* shapes timed (0: taken from the cache)  */
 } avbd_profile;
+/* Pin the per-color primal variant of a static-palette scene: 8, 16 or 32
+ * lanes per body (grouped kernel), AVBD_PRIMAL_VARIANT_STAGED (block-wide
+ * term evaluation into shared memory, then an 8-lane fold per body), or 0 to
+ * re-run the autotuner, which times every variant on the next frames and
+ * keeps the fastest per color (the default).  Every variant computes the
+ * same floats.  No counterpart in the reference, whose primal has one
+ * launch shape (primal_particles_split, 40_solver.metal:1544-1686).        */
+enum { AVBD_PRIMAL_VARIANT_AUTO = 0, AVBD_PRIMAL_VARIANT_STAGED = 1 };
+int avbd_set_primal_variant(avbd_solver* solver, uint32_t variant);
 int avbd_set_profiling(avbd_solver* solver, int enabled);
 int avbd_get_profile(avbd_solver* solver, avbd_profile* out);
 
