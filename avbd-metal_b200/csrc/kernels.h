@@ -167,9 +167,13 @@ void launch_dynamic_coloring(const Params& P, const DevPtrs& d, const Sizes& z, 
 // `lanes` is 8, 16 or 32 lanes per body (grouped kernel) or
 // AVBD_PRIMAL_STAGED (staged kernel: block-wide term evaluation, then an
 // 8-lane fold per body), every choice computing the same floats
+// With a side stream and two events, the color's non-lean bodies (a block
+// each) run on the side stream beside the lean particles (a fork and a join
+// on `st`; in a captured frame, two parallel graph branches).
 constexpr uint32_t AVBD_PRIMAL_STAGED = 1;
 void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color,
-                         uint32_t count, uint32_t lanes, cudaStream_t st);
+                         uint32_t count, uint32_t lanes, cudaStream_t st, cudaStream_t side = nullptr,
+                         cudaEvent_t fork = nullptr, cudaEvent_t join = nullptr);
 // squared AL-gradient norm of every dynamic body (perBody[numDynamicBodies])
 // and their fixed-order sum (total)
 void launch_residual(const Params& P, const DevPtrs& d, const Sizes& z, float* perBody, double* total,

@@ -120,6 +120,7 @@ struct avbd_solver {
     // one on this stream (fork / join by events inside the frame)
     cudaStream_t branchStream = nullptr;
     cudaEvent_t forkEvent = nullptr, joinEvent = nullptr;
+    cudaEvent_t wideFork = nullptr, wideJoin = nullptr;   // per-color side branch of the primal
     // per-stage profiling: events at stage boundaries inside the frame graph
     bool profiling = false;
     std::vector<cudaEvent_t> events;
@@ -195,6 +196,8 @@ struct avbd_solver {
         if (hostLatch) cudaFreeHost(hostLatch);
         if (forkEvent) cudaEventDestroy(forkEvent);
         if (joinEvent) cudaEventDestroy(joinEvent);
+        if (wideFork) cudaEventDestroy(wideFork);
+        if (wideJoin) cudaEventDestroy(wideJoin);
         if (branchStream) cudaStreamDestroy(branchStream);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -391,7 +394,8 @@ struct avbd_solver {
                     if (count == 0) continue;
                     mark(AVBD_STAGE_PRIMAL);
                     if (primalEvents) cudaEventRecord(primalEvents[2 * primalLaunch], st);
-                    launch_primal_color(P, g, z, c, count, lanes ? lanes[c] : H.colorLanes[c], st);
+                    launch_primal_color(P, g, z, c, count, lanes ? lanes[c] : H.colorLanes[c], st, branchStream,
+                                        wideFork, wideJoin);
                     if (primalEvents) cudaEventRecord(primalEvents[2 * primalLaunch + 1], st);
                     primalLaunch++;
                     if (P.cloth) {
@@ -472,7 +476,9 @@ struct avbd_solver {
         if (cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaStreamCreateWithFlags(&branchStream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&forkEvent, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&joinEvent, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&joinEvent, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&wideFork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&wideJoin, cudaEventDisableTiming) != cudaSuccess) {
             error = "stream creation failed";
             return AVBD_ERR_NO_DEVICE;
         }

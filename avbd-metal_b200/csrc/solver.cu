@@ -1714,7 +1714,7 @@ static void launch_primal_staged(const Params& P, const DevPtrs& d, uint32_t col
 }
 
 void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color, uint32_t count,
-                         uint32_t lanes, cudaStream_t st) {
+                         uint32_t lanes, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join) {
     const int T = 128;
     const uint32_t upper = count != 0xFFFFFFFFu ? count : z.numDynamicBodies;
     if (upper == 0) return;
@@ -1734,6 +1734,12 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
         const bool cloth = P.cloth || P.ogc;
         const uint32_t lean = z.particleFastPath ? upper : (z.colorLean ? min(z.colorLean[color], upper) : 0u);
         const uint32_t rest = upper - lean;
+        const bool split = rest && lean && side && fork && join;
+        if (split) {
+            cudaEventRecord(fork, st);
+            cudaStreamWaitEvent(side, fork, 0);
+            launch_primal_wide(P, d, color, rest, lean, side);
+        }
         if (lean) {
             if (lanes == AVBD_PRIMAL_STAGED) {
                 if (cloth) launch_primal_staged<false, true>(P, d, color, lean, 0, st);
@@ -1746,7 +1752,12 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
             }
         }
         // the rest: a block per body (rigid bodies with many contacts)
-        launch_primal_wide(P, d, color, rest, lean, st);
+        if (split) {
+            cudaEventRecord(join, side);
+            cudaStreamWaitEvent(st, join, 0);
+        } else {
+            launch_primal_wide(P, d, color, rest, lean, st);
+        }
     }
 }
 
