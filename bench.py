@@ -100,6 +100,8 @@ def parse():
     ap.add_argument("--warm-start", choices=["plain", "learned"], default="plain",
                     help="with --frames-only: the warm start of the frames")
     ap.add_argument("--iterations", type=int, default=0, help="with --frames-only: override the iterations")
+    ap.add_argument("--primal-variant", choices=["auto", "staged", "8", "16", "32"], default="auto",
+                    help="with --frames-only: pin the static-palette primal variant (default: autotuned)")
     ap.add_argument("--pusht-obs", action="store_true",
                     help="time the Push-T pixel-observation kernel instead (--obs-envs x --obs-res^2 x 3 "
                          "bytes per launch) and print its own JSON line")
@@ -438,6 +440,9 @@ def run_frames(args, local):
     if args.iterations:
         scene.settings.iterations = args.iterations
     solver = GPUSolver(scene, device=local)
+    if args.primal_variant != "auto":
+        solver.set_primal_variant(abi.PRIMAL_VARIANT_STAGED if args.primal_variant == "staged"
+                                  else int(args.primal_variant))
     if args.warm_start == "learned":
         model = learned.WarmStartModel.load(model_path())
         solver.set_warm_start_model(model.params, model.norm, 1, rigid=model.rigid)
@@ -658,7 +663,7 @@ def run_ours(args, world, rank, local):
             "clocks": clock, "e2e": e2e,
             "gpu_launches": int(kernels_per_frame * K),
             "roofline": {"bound": "hbm",
-                         "kernel": "per-color block-descent primal (k_primal_group / k_primal / k_solve_small)",
+                         "kernel": "per-color block-descent primal (k_primal_group lean particles, k_primal_wide rigid and joint-carrying bodies beside them, k_primal_staged where tuned; k_primal / k_solve_small for dynamic coloring and small scenes)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "peak_source": (f"{peak_kind} hbm_gbs (MEASURED_PEAKS.json)" if peak_kind == "measured"
                                          else "fallback 6.65 TB/s"),
