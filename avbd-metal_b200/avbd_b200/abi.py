@@ -196,7 +196,7 @@ EXPORTED = [
     "avbd_set_warm_start_model", "avbd_set_warm_start_mode", "avbd_set_warm_start_rigid",
     "avbd_set_learning_capture",
     "avbd_set_residual_trace", "avbd_get_residual_trace", "avbd_mlp_param_count",
-    "avbd_mlp_workspace_bytes", "avbd_mlp_gradients", "avbd_mlp_train_step", "avbd_mlp_infer", "avbd_mlp_infer_wait_timeout_for_testing",
+    "avbd_mlp_workspace_bytes", "avbd_mlp_gradients", "avbd_mlp_train_step", "avbd_mlp_workspace_status", "avbd_mlp_infer", "avbd_mlp_infer_wait_timeout_for_testing",
     "avbd_build_instances", "avbd_soft_normals", "avbd_set_skin_bindings", "avbd_skin_deform",
     "avbd_render_pusht_obs", "avbd_create_batched", "avbd_get_world_offsets", "avbd_set_world_body_states",
     "avbd_reset_worlds", "avbd_get_world_motor_joints",

@@ -137,6 +137,10 @@ def train(features: np.ndarray, targets: np.ndarray, steps: int = 2000, batch: i
         if rc != 0:
             raise RuntimeError(f"avbd_mlp_train_step failed: {rc}")
         if step % log_every == 0 or step == steps:
+            # the steps run asynchronously; a tensor-core wait that gave up
+            # since step 1 is latched in the workspace
+            if lib.avbd_mlp_workspace_status(ws.data_ptr(), batch, stream) != 0:
+                raise RuntimeError("avbd_mlp_train_step: a tensor-core wait gave up")
             hist.append(float(loss.item()) / USED)           # per-component mean squared error
     return WarmStartModel(prm.cpu().numpy(), norm, hist)
 

@@ -100,6 +100,7 @@ def load_library() -> C.CDLL:
         "avbd_mlp_workspace_bytes": ([u32], sz),
         "avbd_mlp_gradients": ([vp, vp, vp, vp, u32, vp, vp, vp, vp], i32),
         "avbd_mlp_train_step": ([vp, vp, vp, vp, u32, vp, vp, u32, C.c_float, vp, vp, vp], i32),
+        "avbd_mlp_workspace_status": ([vp, u32, vp], i32),
         "avbd_mlp_infer": ([vp, vp, vp, u32, vp, vp, vp], i32),
         "avbd_mlp_infer_wait_timeout_for_testing": ([vp, vp, vp, u32, vp, vp, vp], i32),
     }

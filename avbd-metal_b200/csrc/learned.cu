@@ -61,17 +61,6 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
     return *reinterpret_cast<const uint32_t*>(&v);
 }
 
-// D = A * B + C for one m16n8k16 tile, BF16 inputs, FP32 accumulate.
-__device__ __forceinline__ void mma_bf16(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3,
-                                         uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-        "{%0,%1,%2,%3};"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-__device__ __forceinline__ uint32_t ld_pair(const bf16* p) { return *reinterpret_cast<const uint32_t*>(p); }
 
 // ---------------------------------------------------------------------------
 // Fused inference on the Blackwell tensor cores (tcgen05): one CTA of four
@@ -321,70 +310,141 @@ __global__ void __launch_bounds__(128) k_mlp_infer_tc(const bf16* __restrict__ W
 }
 
 // ---------------------------------------------------------------------------
-// Training GEMM: C[M][N] (fp32) = op(A) op(B) with BF16 operands, FP32
-// accumulation.  A is [M][K] (lda = K) or, with TA, stored [K][M]; B is
-// [N][K] or, with TB, stored [K][N].  64 x 64 tiles, 4 warps of 32 x 32,
-// K in steps of 32 staged through shared memory; split-K writes one partial
-// per z-slice (reduced in a fixed order by k_split_sum).
+// Training GEMM on the tensor cores: C[M][N] (fp32) = op(A) op(B), BF16
+// operands, FP32 accumulation in TMEM.  A is [M][K] (lda = K) or, with TA,
+// stored [K][M]; B is [N][K] or, with TB, stored [K][N].  A CTA of four warps
+// owns a 128-row x BN-column tile (BN = N rounded up to 16, at most 128;
+// rows past M are zero): K runs in chunks of 64 through two shared-memory
+// stages in the UMMA canonical K-major layout (row-group stride 1024 B),
+// staged by all threads (transposing on the fly) while the previous chunk's
+// four M = 128, K = 16 tcgen05.mma instructions run; each stage is reused
+// only after the tcgen05.commit of its MMAs has arrived on its mbarrier.
+// Every wait is bounded (one second); a timeout sets *status and the CTA
+// frees its TMEM and stops.  Split-K writes one partial per z-slice
+// (reduced in a fixed order by k_split_sum).
 // ---------------------------------------------------------------------------
-template <bool TA, bool TB>
-__global__ void __launch_bounds__(128) k_gemm(const bf16* __restrict__ A, const bf16* __restrict__ B,
-                                              float* __restrict__ C, uint32_t M, uint32_t N, uint32_t K,
-                                              uint32_t kPerSplit) {
-    __shared__ __align__(16) bf16 As[64][40];
-    __shared__ __align__(16) bf16 Bs[64][40];
-    const uint32_t m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
-    const uint32_t kBeg = blockIdx.z * kPerSplit, kEnd = min(K, kBeg + kPerSplit);
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u, g = lane >> 2, q = lane & 3u;
-    const uint32_t wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    float acc[2][4][4] = {};
-    for (uint32_t k0 = kBeg; k0 < kEnd; k0 += 32) {
-        for (uint32_t i = threadIdx.x; i < 64 * 32; i += 128) {
-            const uint32_t r = i >> 5, c = i & 31u;          // tile row (m or n), tile column (k)
-            const uint32_t gm = m0 + r, gn = n0 + r, gk = k0 + c;
-            bf16 av = __float2bfloat16(0.0f), bv = __float2bfloat16(0.0f);
-            if (gm < M && gk < kEnd) av = TA ? A[(size_t)gk * M + gm] : A[(size_t)gm * K + gk];
-            if (gn < N && gk < kEnd) bv = TB ? B[(size_t)gk * N + gn] : B[(size_t)gn * K + gk];
-            As[r][c] = av;
-            Bs[r][c] = bv;
-        }
-        __syncthreads();
+namespace tg {
+constexpr uint32_t BK = 64, SBO = (BK / 8) * 128;          // chunk of K; row-group stride (1024 B)
+constexpr uint32_t STAGE = 128 * BK * 2;                    // one operand tile (16 KiB)
+constexpr uint32_t A0 = 0, B0 = A0 + 2 * STAGE, BAR = B0 + 2 * STAGE, TSLOT = BAR + 16, SMEM = TSLOT + 16;
+constexpr uint32_t TMEM_COLS = 128;
+}  // namespace tg
+
+// one 8-element K group of row r of an operand tile: 16 bytes in the
+// canonical layout; T: the operand is stored transposed ([K][rows], ld = rows)
+template <bool T>
+__device__ __forceinline__ uint4 stage_group(const bf16* __restrict__ X, uint32_t rows, uint32_t K, uint32_t row,
+                                             uint32_t k, uint32_t kEnd) {
+    uint32_t w[4];
+    if (!T && row < rows && k + 8 <= kEnd && (K & 7u) == 0u)
+        return *reinterpret_cast<const uint4*>(X + (size_t)row * K + k);
 #pragma unroll
-        for (int kk = 0; kk < 32; kk += 16) {
-            uint32_t af[2][4], bfr[4][2];
-#pragma unroll
-            for (int i = 0; i < 2; i++) {
-                const uint32_t r = wm + 16 * i + g;
-                af[i][0] = ld_pair(&As[r][kk + 2 * q]);
-                af[i][1] = ld_pair(&As[r + 8][kk + 2 * q]);
-                af[i][2] = ld_pair(&As[r][kk + 8 + 2 * q]);
-                af[i][3] = ld_pair(&As[r + 8][kk + 8 + 2 * q]);
-            }
-#pragma unroll
-            for (int j = 0; j < 4; j++) {
-                const uint32_t c = wn + 8 * j + g;
-                bfr[j][0] = ld_pair(&Bs[c][kk + 2 * q]);
-                bfr[j][1] = ld_pair(&Bs[c][kk + 8 + 2 * q]);
-            }
-#pragma unroll
-            for (int i = 0; i < 2; i++)
-#pragma unroll
-                for (int j = 0; j < 4; j++)
-                    mma_bf16(acc[i][j], af[i][0], af[i][1], af[i][2], af[i][3], bfr[j][0], bfr[j][1]);
-        }
-        __syncthreads();
+    for (int e = 0; e < 4; e++) {
+        const uint32_t k0 = k + 2 * e, k1 = k0 + 1;
+        bf16 lo = __float2bfloat16(0.0f), hi = __float2bfloat16(0.0f);
+        if (row < rows && k0 < kEnd) lo = T ? X[(size_t)k0 * rows + row] : X[(size_t)row * K + k0];
+        if (row < rows && k1 < kEnd) hi = T ? X[(size_t)k1 * rows + row] : X[(size_t)row * K + k1];
+        w[e] = (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
     }
-    float* Cz = C + (size_t)blockIdx.z * M * N;
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const uint32_t r = m0 + wm + 16 * i + g, c = n0 + wn + 8 * j + 2 * q;
-            if (r < M && c < N) Cz[(size_t)r * N + c] = acc[i][j][0];
-            if (r < M && c + 1 < N) Cz[(size_t)r * N + c + 1] = acc[i][j][1];
-            if (r + 8 < M && c < N) Cz[(size_t)(r + 8) * N + c] = acc[i][j][2];
-            if (r + 8 < M && c + 1 < N) Cz[(size_t)(r + 8) * N + c + 1] = acc[i][j][3];
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(128) k_gemm_tc(const bf16* __restrict__ A, const bf16* __restrict__ B,
+                                                 float* __restrict__ C, uint32_t M, uint32_t N, uint32_t K,
+                                                 uint32_t kPerSplit, uint32_t bn, uint32_t* status) {
+    extern __shared__ __align__(1024) unsigned char sm[];
+    const uint32_t t = threadIdx.x, warp = t >> 5;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(sm);
+    const uint32_t m0 = blockIdx.y * 128u, n0 = blockIdx.x * bn;
+    const uint32_t kBeg = blockIdx.z * kPerSplit, kEnd = min(K, kBeg + kPerSplit);
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sbase + tg::BAR) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sbase + tg::BAR + 8) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sbase + tg::TSLOT),
+                     "r"(tg::TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t*>(sm + tg::TSLOT);
+    const uint32_t id = tc::idesc(128, bn);
+    const uint32_t chunks = kEnd > kBeg ? (kEnd - kBeg + tg::BK - 1) / tg::BK : 0u;
+    bool ok = true;
+    for (uint32_t c = 0; c < chunks && ok; c++) {
+        const uint32_t buf = c & 1u, bar = sbase + tg::BAR + 8u * buf;
+        if (c >= 2) {
+            // the MMAs that last read this stage have completed (block-uniform)
+            ok = __syncthreads_and(tc::wait(bar, ((c >> 1) - 1u) & 1u) ? 1 : 0) != 0;
+            if (!ok) break;
         }
+        const uint32_t k0 = kBeg + c * tg::BK;
+        unsigned char* sa = sm + tg::A0 + buf * tg::STAGE;
+        unsigned char* sb = sm + tg::B0 + buf * tg::STAGE;
+        // thread t stages row t of the A tile and (t < bn) row t of the B tile
+#pragma unroll 2
+        for (uint32_t kg = 0; kg < tg::BK / 8; kg++) {
+            *reinterpret_cast<uint4*>(sa + tc::off(t, kg * 8, tg::SBO)) =
+                stage_group<TA>(A, M, K, m0 + t, k0 + kg * 8, kEnd);
+            if (t < bn)
+                *reinterpret_cast<uint4*>(sb + tc::off(t, kg * 8, tg::SBO)) =
+                    stage_group<TB>(B, N, K, n0 + t, k0 + kg * 8, kEnd);
+        }
+        tc::fence_proxy();               // generic-proxy writes, read by the tensor core
+        tc::fence_before();
+        __syncthreads();
+        tc::fence_after();
+        if (t == 0) {
+            const uint32_t steps = min(tg::BK, kEnd - k0 + 15u) / 16u;
+            const uint32_t a = sbase + tg::A0 + buf * tg::STAGE, b = sbase + tg::B0 + buf * tg::STAGE;
+            for (uint32_t s = 0; s < steps; s++)
+                tc::mma(tmem, tc::desc(a + 256u * s, tg::SBO), tc::desc(b + 256u * s, tg::SBO), id,
+                        (c > 0 || s > 0) ? 1u : 0u);
+            tc::commit(bar);
+        }
+    }
+    if (ok && chunks) {
+        // the last commit covers every MMA issued before it
+        const uint32_t last = chunks - 1u;
+        ok = __syncthreads_and(tc::wait(sbase + tg::BAR + 8u * (last & 1u), (last >> 1) & 1u) ? 1 : 0) != 0;
+        tc::fence_after();
+    }
+    if (ok) {
+        const uint32_t r = m0 + t;
+        const uint32_t lane_addr = tmem + ((warp * 32u) << 16);
+        float* Cz = C + (size_t)blockIdx.z * M * N;
+        for (uint32_t c0 = 0; c0 < bn; c0 += 16) {
+            float v[16];
+            if (chunks) {
+                tc::ld16(lane_addr + c0, v);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; j++) v[j] = 0.0f;
+            }
+            if (r < M) {
+#pragma unroll
+                for (uint32_t j = 0; j < 16; j++)
+                    if (n0 + c0 + j < N) Cz[(size_t)r * N + n0 + c0 + j] = v[j];
+            }
+        }
+    } else if (t == 0) {
+        atomicCAS(status, 0u, (uint32_t)AVBD_FAIL_WAIT_TIMEOUT);
+    }
+    if (!ok) {
+        // let MMAs still in flight finish (bounded) before the TMEM is freed
+        for (uint32_t b = 0; b < 2; b++) tc::wait(sbase + tg::BAR + 8u * b, 0u);
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tg::TMEM_COLS)
+                     : "memory");
 }
 
 __global__ void k_split_sum(const float* part, uint32_t splits, uint32_t count, float* out) {
@@ -523,10 +583,11 @@ __global__ void k_mirror_umma(const float* prm, unsigned char* img) {
 // Workspace layout for a batch of B rows (all offsets 256-byte aligned).
 // ---------------------------------------------------------------------------
 namespace {
-constexpr uint32_t kSplits = 16;
+constexpr uint32_t kSplits = 32;
 struct Work {
     bf16 *Xb, *H1, *H2, *H3, *dYb, *dH3b, *dH2b, *dH1b, *half;
     float *Z, *dY, *dH, *part, *grad, *lossPart;
+    uint32_t* status;        // nonzero when a tensor-core wait gave up
 };
 size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 size_t work_layout(uint32_t B, char* base, Work* w) {
@@ -550,19 +611,42 @@ size_t work_layout(uint32_t B, char* base, Work* w) {
     p = take((size_t)kSplits * HID * HID * 4); if (w) w->part = (float*)p;
     p = take((size_t)NPARAM * 4); if (w) w->grad = (float*)p;
     p = take(((Bp * DOUT + 255) / 256) * 4 + 4); if (w) w->lossPart = (float*)p;
+    p = take(4); if (w) w->status = (uint32_t*)p;
     return off;
 }
 
+// 64 KiB of dynamic shared memory for the two stages (set once per device)
+template <bool TA, bool TB>
+void gemm_attributes() {
+    static std::atomic<uint64_t> done{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const uint64_t bit = 1ull << (dev & 63);
+    if (done.load() & bit) return;
+    cudaFuncSetAttribute(k_gemm_tc<TA, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tg::SMEM);
+    done.fetch_or(bit);
+}
+
+template <bool TA, bool TB>
+void launch_gemm_tc(dim3 grid, const bf16* A, const bf16* B, float* dst, uint32_t M, uint32_t N, uint32_t K,
+                    uint32_t kPer, uint32_t bn, uint32_t* status, cudaStream_t st) {
+    gemm_attributes<TA, TB>();
+    k_gemm_tc<TA, TB><<<grid, 128, tg::SMEM, st>>>(A, B, dst, M, N, K, kPer, bn, status);
+}
+
 void gemm(const bf16* A, bool ta, const bf16* B, bool tb, float* C, uint32_t M, uint32_t N, uint32_t K,
-          uint32_t splits, float* part, cudaStream_t st) {
-    const uint32_t kPer = ((K + splits - 1) / splits + 31) / 32 * 32;
+          uint32_t splits, float* part, uint32_t* status, cudaStream_t st) {
+    const uint32_t kPer = ((K + splits - 1) / splits + 63) / 64 * 64;
     splits = (K + kPer - 1) / kPer;
-    dim3 grid((N + 63) / 64, (M + 63) / 64, splits);
+    // 64-column tiles: two column blocks for the 128-wide layers (more CTAs
+    // for the batch-row GEMMs, which have only 64 row blocks at batch 8,192)
+    const uint32_t bn = std::min<uint32_t>(64u, (N + 15u) / 16u * 16u);
+    dim3 grid((N + bn - 1) / bn, (M + 127) / 128, splits);
     float* dst = splits > 1 ? part : C;
-    if (!ta && !tb) k_gemm<false, false><<<grid, 128, 0, st>>>(A, B, dst, M, N, K, kPer);
-    else if (!ta && tb) k_gemm<false, true><<<grid, 128, 0, st>>>(A, B, dst, M, N, K, kPer);
-    else if (ta && !tb) k_gemm<true, false><<<grid, 128, 0, st>>>(A, B, dst, M, N, K, kPer);
-    else k_gemm<true, true><<<grid, 128, 0, st>>>(A, B, dst, M, N, K, kPer);
+    if (!ta && !tb) launch_gemm_tc<false, false>(grid, A, B, dst, M, N, K, kPer, bn, status, st);
+    else if (!ta && tb) launch_gemm_tc<false, true>(grid, A, B, dst, M, N, K, kPer, bn, status, st);
+    else if (ta && !tb) launch_gemm_tc<true, false>(grid, A, B, dst, M, N, K, kPer, bn, status, st);
+    else launch_gemm_tc<true, true>(grid, A, B, dst, M, N, K, kPer, bn, status, st);
     if (splits > 1) k_split_sum<<<(M * N + 255) / 256, 256, 0, st>>>(part, splits, M * N, C);
 }
 
@@ -575,33 +659,33 @@ void forward_backward(const float* prm, const float* norm, const float* X, const
     k_mirror<<<blocks(NPARAM, 256), 256, 0, st>>>(prm, w.half);
     k_norm_input<<<blocks((size_t)B * DIN, 256), 256, 0, st>>>(X, norm, B, w.Xb);
     // forward: Z = Hprev W^T (W stored [out][in] = [N][K])
-    gemm(w.Xb, false, w.half + HW1, false, w.Z, B, HID, DIN, 1, w.part, st);
+    gemm(w.Xb, false, w.half + HW1, false, w.Z, B, HID, DIN, 1, w.part, w.status, st);
     k_bias_relu<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, prm + OB1, B, HID, w.H1);
-    gemm(w.H1, false, w.half + HW2, false, w.Z, B, HID, HID, 1, w.part, st);
+    gemm(w.H1, false, w.half + HW2, false, w.Z, B, HID, HID, 1, w.part, w.status, st);
     k_bias_relu<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, prm + OB2, B, HID, w.H2);
-    gemm(w.H2, false, w.half + HW3, false, w.Z, B, HID, HID, 1, w.part, st);
+    gemm(w.H2, false, w.half + HW3, false, w.Z, B, HID, HID, 1, w.part, w.status, st);
     k_bias_relu<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, prm + OB3, B, HID, w.H3);
-    gemm(w.H3, false, w.half + HW4, false, w.Z, B, DOUT, HID, 1, w.part, st);
+    gemm(w.H3, false, w.half + HW4, false, w.Z, B, DOUT, HID, 1, w.part, w.status, st);
     const uint32_t lb = blocks((size_t)B * DOUT, 256);
     k_loss_grad<<<lb, 256, 0, st>>>(w.Z, prm + OB4, T, norm, B, w.dY, w.dYb, w.lossPart);
     k_fixed_sum<<<1, 32, 0, st>>>(w.lossPart, lb, 1.0f / (float)B, w.lossPart + lb);   // mean over the batch
     // backward.  dW = dH^T Hprev: A = dH stored [B][out] = [K][M] (TA),
     // B-operand = Hprev stored [B][in] = [K][N] (TB).  dHprev = dH W:
     // A = dH [B][out] = [M][K], B-operand W stored [out][in] = [K][N] (TB).
-    gemm(w.dYb, true, w.H3, true, w.grad + OW4, DOUT, HID, B, kSplits, w.part, st);
+    gemm(w.dYb, true, w.H3, true, w.grad + OW4, DOUT, HID, B, kSplits, w.part, w.status, st);
     k_col_sum<<<1, DOUT, 0, st>>>(w.dY, B, DOUT, w.grad + OB4);
-    gemm(w.dYb, false, w.half + HW4, true, w.Z, B, HID, DOUT, 1, w.part, st);
+    gemm(w.dYb, false, w.half + HW4, true, w.Z, B, HID, DOUT, 1, w.part, w.status, st);
     k_relu_back<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, w.H3, B * HID, w.dH, w.dH3b);
     k_col_sum<<<1, HID, 0, st>>>(w.dH, B, HID, w.grad + OB3);
-    gemm(w.dH3b, true, w.H2, true, w.grad + OW3, HID, HID, B, kSplits, w.part, st);
-    gemm(w.dH3b, false, w.half + HW3, true, w.Z, B, HID, HID, 1, w.part, st);
+    gemm(w.dH3b, true, w.H2, true, w.grad + OW3, HID, HID, B, kSplits, w.part, w.status, st);
+    gemm(w.dH3b, false, w.half + HW3, true, w.Z, B, HID, HID, 1, w.part, w.status, st);
     k_relu_back<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, w.H2, B * HID, w.dH, w.dH2b);
     k_col_sum<<<1, HID, 0, st>>>(w.dH, B, HID, w.grad + OB2);
-    gemm(w.dH2b, true, w.H1, true, w.grad + OW2, HID, HID, B, kSplits, w.part, st);
-    gemm(w.dH2b, false, w.half + HW2, true, w.Z, B, HID, HID, 1, w.part, st);
+    gemm(w.dH2b, true, w.H1, true, w.grad + OW2, HID, HID, B, kSplits, w.part, w.status, st);
+    gemm(w.dH2b, false, w.half + HW2, true, w.Z, B, HID, HID, 1, w.part, w.status, st);
     k_relu_back<<<blocks((size_t)B * HID, 256), 256, 0, st>>>(w.Z, w.H1, B * HID, w.dH, w.dH1b);
     k_col_sum<<<1, HID, 0, st>>>(w.dH, B, HID, w.grad + OB1);
-    gemm(w.dH1b, true, w.Xb, true, w.grad + OW1, HID, DIN, B, kSplits, w.part, st);
+    gemm(w.dH1b, true, w.Xb, true, w.grad + OW1, HID, DIN, B, kSplits, w.part, w.status, st);
 }
 }  // namespace
 
@@ -880,28 +964,57 @@ uint32_t avbd_mlp_param_count(void) { return mlp::NPARAM; }
 
 size_t avbd_mlp_workspace_bytes(uint32_t batch) { return work_layout(batch, nullptr, nullptr); }
 
-int avbd_mlp_gradients(const float* params, const float* norm, const float* features, const float* targets,
-                       uint32_t batch, void* workspace, float* grad_out, float* loss_out, void* stream) {
+// status word of a workspace: cleared, or read after a synchronisation
+static int workspace_status(const Work& w, cudaStream_t st) {
+    uint32_t h = 0;
+    if (cudaMemcpyAsync(&h, w.status, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return AVBD_ERR_RUNTIME_FAILURE;
+    return h == 0 ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+}
+
+static int gradients(const float* params, const float* norm, const float* features, const float* targets,
+                     uint32_t batch, void* workspace, float* grad_out, float* loss_out, cudaStream_t st,
+                     bool check) {
     if (!params || !norm || !features || !targets || !workspace || batch == 0) return AVBD_ERR_INVALID_ARGUMENT;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
     Work w{};
     work_layout(batch, static_cast<char*>(workspace), &w);
+    if (check) cudaMemsetAsync(w.status, 0, sizeof(uint32_t), st);
     forward_backward(params, norm, features, targets, batch, w, st);
     const uint32_t lb = blocks((size_t)batch * mlp::DOUT, 256);
     if (grad_out) cudaMemcpyAsync(grad_out, w.grad, sizeof(float) * mlp::NPARAM, cudaMemcpyDeviceToDevice, st);
     if (loss_out) cudaMemcpyAsync(loss_out, w.lossPart + lb, sizeof(float), cudaMemcpyDeviceToDevice, st);
-    return cudaGetLastError() == cudaSuccess ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;
+    if (cudaGetLastError() != cudaSuccess) return AVBD_ERR_RUNTIME_FAILURE;
+    // a tensor-core wait that gave up fails the call (the GEMM kernels latch
+    // it in the workspace's status word)
+    return check ? workspace_status(w, st) : AVBD_OK;
+}
+
+int avbd_mlp_gradients(const float* params, const float* norm, const float* features, const float* targets,
+                       uint32_t batch, void* workspace, float* grad_out, float* loss_out, void* stream) {
+    return gradients(params, norm, features, targets, batch, workspace, grad_out, loss_out,
+                     static_cast<cudaStream_t>(stream), true);
+}
+
+int avbd_mlp_workspace_status(const void* workspace, uint32_t batch, void* stream) {
+    if (!workspace || batch == 0) return AVBD_ERR_INVALID_ARGUMENT;
+    Work w{};
+    work_layout(batch, static_cast<char*>(const_cast<void*>(workspace)), &w);
+    return workspace_status(w, static_cast<cudaStream_t>(stream));
 }
 
 int avbd_mlp_train_step(float* params, const float* norm, const float* features, const float* targets,
                         uint32_t batch, float* adam_m, float* adam_v, uint32_t step, float lr, void* workspace,
                         float* loss_out, void* stream) {
     if (!params || !adam_m || !adam_v || step == 0) return AVBD_ERR_INVALID_ARGUMENT;
-    int rc = avbd_mlp_gradients(params, norm, features, targets, batch, workspace, nullptr, loss_out, stream);
-    if (rc != AVBD_OK) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     Work w{};
-    work_layout(batch, static_cast<char*>(workspace), &w);
+    if (workspace && batch) {
+        work_layout(batch, static_cast<char*>(workspace), &w);
+        if (step == 1) cudaMemsetAsync(w.status, 0, sizeof(uint32_t), st);   // sticky from here on
+    }
+    int rc = gradients(params, norm, features, targets, batch, workspace, nullptr, loss_out, st, false);
+    if (rc != AVBD_OK) return rc;
     k_adam<<<blocks(mlp::NPARAM, 256), 256, 0, st>>>(params, w.grad, adam_m, adam_v, step, lr, 0.9f, 0.999f, 1e-8f,
                                                      w.half);
     return cudaGetLastError() == cudaSuccess ? AVBD_OK : AVBD_ERR_RUNTIME_FAILURE;

@@ -441,7 +441,13 @@ int avbd_get_residual_trace(avbd_solver* solver, double* out, uint32_t n);
 
 /* Training kernels (device pointers; stream may be null).  A batch is
  * features[batch][32] and targets[batch][6] (raw, normalised with `norm`);
- * the workspace holds avbd_mlp_workspace_bytes(batch) bytes.             */
+ * the workspace holds avbd_mlp_workspace_bytes(batch) bytes.  The GEMMs run
+ * on the tensor cores (tcgen05.mma, accumulators in tensor memory) and give
+ * up a wait for their MMA completion after about one second, latching a
+ * status word in the workspace.  avbd_mlp_gradients synchronises `stream`
+ * and fails on it; avbd_mlp_train_step stays asynchronous (the word is
+ * cleared at step 1 and sticky afterwards) and avbd_mlp_workspace_status
+ * synchronises and reports it.                                             */
 uint32_t avbd_mlp_param_count(void);
 size_t avbd_mlp_workspace_bytes(uint32_t batch);
 int avbd_mlp_gradients(const float* params, const float* norm, const float* features,
@@ -450,6 +456,7 @@ int avbd_mlp_gradients(const float* params, const float* norm, const float* feat
 int avbd_mlp_train_step(float* params, const float* norm, const float* features,
                         const float* targets, uint32_t batch, float* adam_m, float* adam_v,
                         uint32_t step, float lr, void* workspace, float* loss_out, void* stream);
+int avbd_mlp_workspace_status(const void* workspace, uint32_t batch, void* stream);
 /* Inference over n feature rows into out[n][6] on the tensor cores
  * (tcgen05.mma, accumulators in tensor memory); synchronises `stream` and
  * returns AVBD_ERR_RUNTIME_FAILURE if the kernel's bounded wait for its MMA
