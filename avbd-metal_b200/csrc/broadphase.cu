@@ -8,6 +8,7 @@
 // with it the manifold index of every pair — is the same on every run.
 #include <mutex>
 
+#include "bucket_sort.cuh"
 #include "../../include/avbd.h"
 #include "dmath.cuh"
 #include "kernels.h"
@@ -188,42 +189,37 @@ static uint32_t stride_blocks_bp(uint32_t threads, int T) {
 // per lane instead of a serial insertion sort.
 __global__ void k_bp_sort_cells(const uint32_t* count, const uint32_t* start, const uint32_t* tmp, uint32_t* out,
                                 uint32_t buckets) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < buckets; h += warps) {
-        const uint32_t n = count[h];
-        if (n == 0) continue;
-        const uint32_t s = start[h];
-        const uint32_t* src = tmp + s;
-        for (uint32_t i = lane; i < n; i += 32) {
-            const uint32_t v = src[i];
-            uint32_t rank = 0;
-            for (uint32_t j = 0; j < n; j++) rank += src[j] < v ? 1u : 0u;
-            out[s + rank] = v;
-        }
-    }
+    rank_sort_buckets(count, start, tmp, out, buckets);
 }
 
-// The rigid colliders of every bucket, in bucket (collider) order: one warp
-// per bucket compacts the sorted bucket.
+// The rigid colliders of every bucket, in bucket (collider) order: a warp
+// reads 32 buckets' rigid counts at once and compacts each bucket that has
+// any, one after another.
 __global__ void k_bp_rigid_compact(const Params P, const DevPtrs d) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < P.gridHashSize; h += warps) {
-        if (d.cellRigid[h] == 0) continue;
-        const uint32_t s = d.cellStart[h], n = d.cellCount[h];
-        uint32_t out = d.rigidStart[h];
-        for (uint32_t k0 = 0; k0 < n; k0 += 32) {
-            const uint32_t k = k0 + lane;
-            uint32_t c = 0;
-            bool rigid = false;
-            if (k < n) {
-                c = d.cellBodies[s + k];
-                rigid = d.colShape[c].w >= 0.0f;
+    // 32 buckets' rigid counts per coalesced load, then one bucket at a time
+    for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < P.gridHashSize;
+         base += warps * 32u) {
+        const uint32_t hl = base + lane;
+        uint32_t live = __ballot_sync(0xffffffffu, hl < P.gridHashSize && d.cellRigid[hl] != 0u);
+        while (live) {
+            const uint32_t h = base + (uint32_t)(__ffs(live) - 1);
+            live &= live - 1u;
+            const uint32_t s = d.cellStart[h], n = d.cellCount[h];
+            uint32_t out = d.rigidStart[h];
+            for (uint32_t k0 = 0; k0 < n; k0 += 32) {
+                const uint32_t k = k0 + lane;
+                uint32_t c = 0;
+                bool rigid = false;
+                if (k < n) {
+                    c = d.cellBodies[s + k];
+                    rigid = d.colShape[c].w >= 0.0f;
+                }
+                const uint32_t ballot = __ballot_sync(0xffffffffu, rigid);
+                if (rigid) d.rigidCells[out + __popc(ballot & ((1u << lane) - 1u))] = c;
+                out += __popc(ballot);
             }
-            const uint32_t ballot = __ballot_sync(0xffffffffu, rigid);
-            if (rigid) d.rigidCells[out + __popc(ballot & ((1u << lane) - 1u))] = c;
-            out += __popc(ballot);
         }
     }
 }
@@ -429,24 +425,34 @@ __global__ void __launch_bounds__(128) k_bp_pairs(const Params P, const DevPtrs 
         const uint32_t gslot = __shfl_sync(0xffffffffu, slot, 27);
         const uint32_t below = (1u << lane) - 1u;
         uint32_t gcount = 0;
-        for (uint32_t gb = g0 & ~31u; gb < P.numGlobals; gb += 32) {
-            if (P.numGlobals > 32) {
-                const float4* box = d.globalChunk + 4 * (size_t)(gb >> 5);
-                if (ball_misses_box(pa, ra, box[0], box[1])) continue;
+        // chunks whose boxes the producer's ball misses are skipped; lane l
+        // tests chunk c0 + l, 32 chunks per load, and the kept ones are
+        // visited in order
+        const uint32_t chunks = (P.numGlobals + 31u) / 32u;
+        for (uint32_t c0 = g0 >> 5; c0 < chunks; c0 += 32) {
+            bool keep = c0 + lane < chunks;
+            if (keep && P.numGlobals > 32) {
+                const float4* box = d.globalChunk + 4 * (size_t)(c0 + lane);
+                keep = !ball_misses_box(pa, ra, box[0], box[1]);
             }
-            const uint32_t g = gb + lane;
-            uint32_t b = 0;
-            bool pass = false;
-            if (g >= g0 && g < P.numGlobals) {
-                b = d.globalIdx[g];
-                if (!(ga != 0 && d.colMeta[b].w == ga)) pass = visit(b, 0u, 0u, false);
+            uint32_t live = __ballot_sync(0xffffffffu, keep);
+            while (live) {
+                const uint32_t gb = (c0 + (uint32_t)(__ffs(live) - 1)) * 32u;
+                live &= live - 1u;
+                const uint32_t g = gb + lane;
+                uint32_t b = 0;
+                bool pass = false;
+                if (g >= g0 && g < P.numGlobals) {
+                    b = d.globalIdx[g];
+                    if (!(ga != 0 && d.colMeta[b].w == ga)) pass = visit(b, 0u, 0u, false);
+                }
+                const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
+                if (emit && pass) {
+                    const uint32_t o = gslot + gcount + __popc(ballot & below);
+                    if (o < P.maxPairs) d.pairs[o] = make_uint2(min(a, b), max(a, b));
+                }
+                gcount += __popc(ballot);
             }
-            const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
-            if (emit && pass) {
-                const uint32_t o = gslot + gcount + __popc(ballot & below);
-                if (o < P.maxPairs) d.pairs[o] = make_uint2(min(a, b), max(a, b));
-            }
-            gcount += __popc(ballot);
         }
         if (lane == 27) count = gcount;
     };
@@ -552,24 +558,32 @@ __global__ void __launch_bounds__(128) k_bp_heavy(const Params P, const DevPtrs 
             }
         }
     } else {
-        for (uint32_t g0 = 0; g0 < P.numGlobals; g0 += 32) {
-            if (P.numGlobals > 32) {
-                const float4* box = d.globalChunk + 4 * (size_t)(g0 >> 5);
-                if (ball_misses_box(pa, ra, box[0], box[1])) continue;
+        // kept chunks in order, 32 chunk boxes tested per load (as above)
+        const uint32_t chunks = (P.numGlobals + 31u) / 32u;
+        for (uint32_t c0 = 0; c0 < chunks; c0 += 32) {
+            bool keep = c0 + lane < chunks;
+            if (keep && P.numGlobals > 32) {
+                const float4* box = d.globalChunk + 4 * (size_t)(c0 + lane);
+                keep = !ball_misses_box(pa, ra, box[0], box[1]);
             }
-            const uint32_t g = g0 + lane;
-            uint32_t b = 0;
-            bool pass = false;
-            if (g < P.numGlobals) {
-                b = d.globalIdx[g];
-                pass = !(ga != 0 && d.colMeta[b].w == ga) && accept(b);
+            uint32_t live = __ballot_sync(0xffffffffu, keep);
+            while (live) {
+                const uint32_t g0 = (c0 + (uint32_t)(__ffs(live) - 1)) * 32u;
+                live &= live - 1u;
+                const uint32_t g = g0 + lane;
+                uint32_t b = 0;
+                bool pass = false;
+                if (g < P.numGlobals) {
+                    b = d.globalIdx[g];
+                    pass = !(ga != 0 && d.colMeta[b].w == ga) && accept(b);
+                }
+                const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
+                if (EMIT && pass) {
+                    const uint32_t o = slot + count + __popc(ballot & below);
+                    if (o < P.maxPairs) d.pairs[o] = make_uint2(min(a, b), max(a, b));
+                }
+                count += __popc(ballot);
             }
-            const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
-            if (EMIT && pass) {
-                const uint32_t o = slot + count + __popc(ballot & below);
-                if (o < P.maxPairs) d.pairs[o] = make_uint2(min(a, b), max(a, b));
-            }
-            count += __popc(ballot);
         }
     }
     if (!EMIT && lane == 0) d.pairLaneCount[(size_t)producer * 32 + s] = count;

@@ -489,25 +489,36 @@ __global__ void __launch_bounds__(128, 6) k_rt_emit(const Params P, const DevPtr
             }
             if (WARP) {
                 emitted = __shfl_sync(0xffffffffu, emitted, 0);
-                for (uint32_t gb = 0; gb < P.numGlobals && emitted < RT_MAX_PER_TRI; gb += 32) {
-                    // a chunk whose bodies all lie beyond the reach test is skipped
-                    const float4* box = d.globalChunk + 4 * (size_t)(gb >> 5);
-                    if (ball_misses_box(m, rT + P.collisionMargin, box[2], box[3])) continue;
-                    const uint32_t g = gb + lane;
-                    bool cand = false;
-                    if (g < P.numGlobals) {
-                        const uint32_t o = d.colOwner[d.globalIdx[g]];
-                        cand = d.shape[o].w >= 0.0f && near_body(o);
+                const uint32_t chunks = (P.numGlobals + 31u) / 32u;
+                for (uint32_t c0 = 0; c0 < chunks && emitted < RT_MAX_PER_TRI; c0 += 32) {
+                    // a chunk whose bodies all lie beyond the reach test is
+                    // skipped; lane l tests chunk c0 + l, so a warp culls 32
+                    // chunks with one load instead of one chunk per load
+                    bool keep = false;
+                    if (c0 + lane < chunks) {
+                        const float4* box = d.globalChunk + 4 * (size_t)(c0 + lane);
+                        keep = !ball_misses_box(m, rT + P.collisionMargin, box[2], box[3]);
                     }
-                    uint32_t ballot = __ballot_sync(0xffffffffu, cand);
-                    if (lane == 0) {
-                        while (ballot && emitted < RT_MAX_PER_TRI) {
-                            const uint32_t j = __ffs(ballot) - 1;
-                            ballot &= ballot - 1;
-                            test_body(d.colOwner[d.globalIdx[gb + j]]);
+                    uint32_t live = __ballot_sync(0xffffffffu, keep);
+                    while (live && emitted < RT_MAX_PER_TRI) {
+                        const uint32_t gb = (c0 + (uint32_t)(__ffs(live) - 1)) * 32u;
+                        live &= live - 1u;
+                        const uint32_t g = gb + lane;
+                        bool cand = false;
+                        if (g < P.numGlobals) {
+                            const uint32_t o = d.colOwner[d.globalIdx[g]];
+                            cand = d.shape[o].w >= 0.0f && near_body(o);
                         }
+                        uint32_t ballot = __ballot_sync(0xffffffffu, cand);
+                        if (lane == 0) {
+                            while (ballot && emitted < RT_MAX_PER_TRI) {
+                                const uint32_t j = __ffs(ballot) - 1;
+                                ballot &= ballot - 1;
+                                test_body(d.colOwner[d.globalIdx[gb + j]]);
+                            }
+                        }
+                        emitted = __shfl_sync(0xffffffffu, emitted, 0);
                     }
-                    emitted = __shfl_sync(0xffffffffu, emitted, 0);
                 }
             } else {
                 for (uint32_t g = 0; g < P.numGlobals && emitted < RT_MAX_PER_TRI; g++) {

@@ -19,6 +19,7 @@
 //   * contact records are counted per query owner, scanned and written in
 //     owner order: rigid-triangle records, then V-T by particle, then E-E by
 //     edge.
+#include "bucket_sort.cuh"
 #include "elements.cuh"
 #include "pdl.cuh"
 
@@ -104,23 +105,10 @@ __global__ void k_ogc_bin(const Params P, const DevPtrs d, uint32_t total) {
     }
 }
 
-// One warp per bucket places every entry at its rank (entries of a bucket
-// are distinct element indices).
+// Every bucket in element order (entries of a bucket are distinct element
+// indices): the ballot bucket sort of bucket_sort.cuh.
 __global__ void k_ogc_sort_cells(const DevPtrs d, uint32_t buckets) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < buckets; h += warps) {
-        const uint32_t n = d.elemCellCount[h];
-        if (n == 0) continue;
-        const uint32_t s = d.elemCellStart[h];
-        const uint32_t* src = d.elemCellsTmp + s;
-        for (uint32_t i = lane; i < n; i += 32) {
-            const uint32_t v = src[i];
-            uint32_t rank = 0;
-            for (uint32_t j = 0; j < n; j++) rank += src[j] < v ? 1u : 0u;
-            d.elemCells[s + rank] = v;
-        }
-    }
+    rank_sort_buckets(d.elemCellCount, d.elemCellStart, d.elemCellsTmp, d.elemCells, buckets);
 }
 
 // ---------------------------------------------------------------------------
@@ -598,20 +586,27 @@ __global__ void __launch_bounds__(128) k_ogc_reseed(const Params P, const DevPtr
             cc = cell_of((qe.a0 + qe.a1) * 0.5f, P.elemCellSize);
             half = P.elemHashSize;
         }
-        // candidate j of the stream arrives as 4 + j; lane l takes j = l mod 32
+        // candidate j of the stream arrives as 4 + j; lane l takes j = l mod 32.
+        // Lane c < 27 first loads the range of bucket c (cells in (dz, dy, dx)
+        // order), so the 27 buckets cost one dependent load, not 27.
+        uint32_t cellS = 0, cellN = 0;
+        if (lane < 27) {
+            const int dz = (int)(lane / 9u) - 1, dy = (int)((lane / 3u) % 3u) - 1, dx = (int)(lane % 3u) - 1;
+            const uint32_t h = half + elem_hash(I3{cc.x + dx, cc.y + dy, cc.z + dz}, P.elemHashSize);
+            cellS = d.elemCellStart[h];
+            cellN = d.elemCellCount[h];
+        }
         uint32_t base = 0;
-        for (int dz = -1; dz <= 1; dz++)
-            for (int dy = -1; dy <= 1; dy++)
-                for (int dx = -1; dx <= 1; dx++) {
-                    const uint32_t h = half + elem_hash(I3{cc.x + dx, cc.y + dy, cc.z + dz}, P.elemHashSize);
-                    const uint32_t s0 = d.elemCellStart[h], cnt = d.elemCellCount[h];
-                    for (uint32_t k = (lane - base) & 31u; k < cnt; k += 32) {
-                        const uint32_t arr = 4u + base + k;
-                        if (vt) vt_consider_lane(P, d, qv, loc, ownB2, d.elemCells[s0 + k], arr);
-                        else ee_consider_lane(P, d, qe, loc, ownB2, d.elemCells[s0 + k], arr);
-                    }
-                    base += cnt;
-                }
+        for (uint32_t c = 0; c < 27; c++) {
+            const uint32_t s0 = __shfl_sync(0xffffffffu, cellS, (int)c);
+            const uint32_t cnt = __shfl_sync(0xffffffffu, cellN, (int)c);
+            for (uint32_t k = (lane - base) & 31u; k < cnt; k += 32) {
+                const uint32_t arr = 4u + base + k;
+                if (vt) vt_consider_lane(P, d, qv, loc, ownB2, d.elemCells[s0 + k], arr);
+                else ee_consider_lane(P, d, qe, loc, ownB2, d.elemCells[s0 + k], arr);
+            }
+            base += cnt;
+        }
         Best4 best;
         warp_merge(loc, best, lane);
 #pragma unroll

@@ -65,7 +65,7 @@ SCENES = [
     ("pinned-soft-block-10", lambda: demos.pinned_soft_block_scene(10), 20),
     ("mixed-small", lambda: demos.mixed_scene(seed=7, cubes=4, cube_n=4, boxes=4, cloth_n=10, pitch=0.5), 40),
     # 40 boxes: more than 32 global colliders, so the rigid-triangle
-    # emission takes its warp path through the global grid
+    # emission takes its warp path over the global chunks
     ("mixed-40-boxes", lambda: demos.mixed_scene(seed=9, cubes=4, cube_n=4, boxes=40, cloth_n=16, pitch=0.5), 40),
     ("drape-20", lambda: demos.drape_scene(res=20), 30),
     ("tet-fan", lambda: tet_fan_scene(), 10),
