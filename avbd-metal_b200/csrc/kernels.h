@@ -147,6 +147,7 @@ struct Sizes {
     const uint32_t* colorCounts;
     const uint32_t* colorLanes;
     const uint32_t* colorLean;            // lean particles at the head of each color's launch order
+    const uint32_t* colorStartHost;       // static palette: each color's start in the list
     // dynamic coloring: block shape of the rigid primal's grid-stride launch
     // (blocks, threads per block), chosen by the runtime's autotuner
     uint32_t dynBlocks, dynThreads;
@@ -170,6 +171,7 @@ void launch_dynamic_coloring(const Params& P, const DevPtrs& d, const Sizes& z, 
 // With a side stream and two events, the color's non-lean bodies (a block
 // each) run on the side stream beside the lean particles (a fork and a join
 // on `st`; in a captured frame, two parallel graph branches).
+constexpr uint32_t NO_HOST_START = 0xFFFFFFFFu;   // a color start the kernel reads on the device
 constexpr uint32_t AVBD_PRIMAL_STAGED = 1;
 void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color,
                          uint32_t count, uint32_t lanes, cudaStream_t st, cudaStream_t side = nullptr,
@@ -232,7 +234,10 @@ void launch_soft_map(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t
 // and element contact records, soft map (once per frame, before warm start)
 void launch_ogc_detect(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st);
 // publish one color's solve (posNext -> posLin) in color-Jacobi scenes
-void launch_publish_color(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count, cudaStream_t st);
+// `start`: the color's start in the color list when known on the host
+// (static palette), else NO_HOST_START (read on the device)
+void launch_publish_color(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count, uint32_t start,
+                          cudaStream_t st);
 // mid-solve OGC bound refresh when more than 1% of surface vertices hit their
 // bound in the pass counted by `readSlot`; zeroes `zeroSlot` for the next pass
 void launch_ogc_refresh(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t* readSlot, uint32_t* zeroSlot,

@@ -698,13 +698,18 @@ __global__ void k_ogc_refresh(const Params P, const DevPtrs d, const uint32_t* r
 }
 
 // Color-Jacobi commit of one color (the primal of the color wrote posNext).
-__global__ void k_publish_color(const DevPtrs d, uint32_t color, uint32_t count) {
-    pdl_prologue();
+__global__ void k_publish_color(const DevPtrs d, uint32_t color, uint32_t count, uint32_t start) {
+    pdl_trigger();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    const uint32_t v = d.colorList[d.colorStart[color] + i];
+    // with the start known on the host, the color list and the shape (set
+    // at upload) are read before waiting for the previous grid
+    if (start == NO_HOST_START) pdl_wait();
+    const uint32_t v = d.colorList[(start == NO_HOST_START ? d.colorStart[color] : start) + i];
+    const bool rigid = d.shape[v].w >= 0.0f;
+    if (start != NO_HOST_START) pdl_wait();
     d.posLin[v] = mk4(xyz(d.posNext[v]), d.posLin[v].w);
-    if (d.shape[v].w >= 0.0f) d.posAng[v] = d.angNext[v];
+    if (rigid) d.posAng[v] = d.angNext[v];
 }
 
 uint32_t grid_for(uint32_t n, uint32_t threads, uint32_t cap = 148u * 16u) {
@@ -739,10 +744,11 @@ void launch_ogc_detect(const Params& P, const DevPtrs& d, const Sizes& z, cudaSt
     launch_soft_map(P, d, z, owners, st);
 }
 
-void launch_publish_color(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count, cudaStream_t st) {
+void launch_publish_color(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count, uint32_t start,
+                          cudaStream_t st) {
     (void)P;
     if (count == 0) return;
-    launch_pdl(k_publish_color, (count + 127) / 128, 128, st, d, color, count);
+    launch_pdl(k_publish_color, (count + 127) / 128, 128, st, d, color, count, start);
 }
 
 void launch_ogc_refresh(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t* readSlot, uint32_t* zeroSlot,

@@ -10,10 +10,13 @@
 
 namespace avbd {
 
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_prologue() {
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    asm volatile("griddepcontrol.wait;" ::: "memory");
+    pdl_trigger();
+    pdl_wait();
 }
+
 
 template <typename... KArgs, typename... Args>
 static void launch_pdl(void (*kernel)(KArgs...), uint32_t blocks, uint32_t threads, cudaStream_t st,

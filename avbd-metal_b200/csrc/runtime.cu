@@ -315,7 +315,8 @@ struct avbd_solver {
                 const uint32_t count = z.dynamicColoring ? 0xFFFFFFFFu : H.colorCounts[c];
                 if (count == 0) continue;
                 launch_primal_color(P, g, z, c, count, H.colorLanes[c], sst);
-                if (P.ogc) launch_publish_color(P, g, c, count, sst);
+                if (P.ogc)
+                    launch_publish_color(P, g, c, count, z.dynamicColoring ? NO_HOST_START : H.colorStart[c], sst);
             }
             if (z.dynamicColoring) launch_primal_tail(P, g, z, colorLaunchBound, sst);
         };
@@ -402,7 +403,8 @@ struct avbd_solver {
                         mark(AVBD_STAGE_TRUNCATION);
                         launch_dat_color(P, f, z, c, count, st);
                     } else if (P.ogc) {
-                        launch_publish_color(P, f, c, count, st);
+                        launch_publish_color(P, f, c, count, z.dynamicColoring ? NO_HOST_START : H.colorStart[c],
+                                             st);
                     }
                 }
                 if (z.dynamicColoring && !(reuseTrial && it == 0)) launch_primal_tail(P, g, z, colorLaunchBound, st);
@@ -510,6 +512,7 @@ struct avbd_solver {
         z.colorCounts = H.dynamicColoring ? nullptr : H.colorCounts.data();
         z.colorLanes = H.colorLanes.data();
         z.colorLean = H.colorLean.data();
+        z.colorStartHost = H.dynamicColoring ? nullptr : H.colorStart.data();
         z.numDynamicRigid = 0;
         for (uint32_t b = 0; b < nb; b++) z.numDynamicRigid += (H.posLin[b].w > 0.0f && H.shape[b].w >= 0.0f) ? 1u : 0u;
         const uint32_t scanLimit = 1024u * 1024u;

@@ -308,6 +308,15 @@ struct AdjView {
         return post[nTet + k - (nDyn - nMan)];
     }
 };
+// The view from the body's static segment (set at upload) and this frame's
+// contact segment.
+__device__ __forceinline__ AdjView adj_view_from(const DevPtrs& d, uint32_t b, uint4 s, uint32_t nTet) {
+    AdjView v;
+    v.pre = d.preList + s.x; v.nPre = s.y;
+    v.dyn = d.dynList + d.dynStart[b]; v.nDyn = d.dynCount[b]; v.nMan = d.dynSplit[b];
+    v.post = d.postList + s.z; v.nPost = s.w; v.nTet = nTet; v.postBase = s.z;
+    return v;
+}
 __device__ __forceinline__ AdjView adj_view(const DevPtrs& d, uint32_t b) {
     const uint4 s = d.staticSeg[b];
     AdjView v;
@@ -983,15 +992,21 @@ constexpr int kWidePoints = 320;           // staged points (33 floats each)
 constexpr uint32_t kWideInline = 0xFFFFFFFFu;
 
 __global__ void __launch_bounds__(kWideThreads) k_primal_wide(const Params P, const DevPtrs d, uint32_t color,
-                                                             uint32_t first) {
+                                                             uint32_t first, uint32_t start) {
     __shared__ PointInc pts[kWidePoints];
     __shared__ uint32_t entOff[kWideEntries];  // (first point << 8) | points, or kWideInline
     __shared__ uint32_t warpSums[kWideThreads / 32];
-    pdl_prologue();
+    pdl_trigger();
     const uint32_t tid = threadIdx.x, lane32 = tid & 31u, warp = tid >> 5;
-    const uint32_t body = d.colorLaunch[d.colorStart[color] + first + blockIdx.x];
+    // with the start known on the host, the static data (launch order,
+    // shape, static segment) is read before waiting for the previous grid
+    if (start == NO_HOST_START) pdl_wait();
+    const uint32_t body = d.colorLaunch[(start == NO_HOST_START ? d.colorStart[color] : start) + first + blockIdx.x];
     const float4 shp = d.shape[body];
-    const AdjView v = adj_view(d, body);
+    const uint4 seg = d.staticSeg[body];
+    const uint32_t nTet = d.postTets[body];
+    if (start != NO_HOST_START) pdl_wait();
+    const AdjView v = adj_view_from(d, body, seg, nTet);
     const uint32_t cnt = v.count();
     const uint32_t staged = min(cnt, (uint32_t)kWideEntries);
     uint32_t base = 0;                          // points taken by earlier chunks
@@ -1057,8 +1072,8 @@ __global__ void __launch_bounds__(kWideThreads) k_primal_wide(const Params P, co
 }
 
 void launch_primal_wide(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count, uint32_t first,
-                        cudaStream_t st) {
-    if (count) launch_pdl(k_primal_wide, count, kWideThreads, st, P, d, color, first);
+                        uint32_t start, cudaStream_t st) {
+    if (count) launch_pdl(k_primal_wide, count, kWideThreads, st, P, d, color, first, start);
 }
 
 // ---------------------------------------------------------------------------
@@ -1472,22 +1487,42 @@ constexpr int kPrimalUnroll = AVBD_PRIMAL_UNROLL;
 #endif
 template <int LANES, bool GENERAL, bool CLOTH, bool RESID = false>
 __global__ void __launch_bounds__(128, GENERAL ? 4 : (CLOTH ? AVBD_LEAN_CLOTH_MIN_BLOCKS : AVBD_PARTICLE_PRIMAL_MIN_BLOCKS)) k_primal_group(const Params P, const DevPtrs d, uint32_t color,
-                                                      uint32_t count, uint32_t first) {
+                                                      uint32_t count, uint32_t first, uint32_t start) {
     constexpr int GROUPS = 32 / LANES;
-    pdl_prologue();
+    pdl_trigger();
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t slot = tid / LANES;
     const uint32_t lane = tid & (LANES - 1);
-    const uint32_t s = d.colorStart[color];
-    const uint32_t n = count != 0xFFFFFFFFu ? count : d.colorStart[color + 1] - s;
-    if (slot >= n) return;                                   // uniform across the group
+    // The solve takes its body from the color's launch order (lean
+    // particles first); the residual pass walks the color list itself.
+    // With the color's start known on the host, the launch order, the
+    // body's shape and its static adjacency segment (none written after
+    // upload) are read before waiting for the previous grid.
+    uint32_t s, body;
+    float4 shp;
+    uint4 seg;
+    uint32_t nTet;
+    if (!RESID && start != NO_HOST_START) {
+        s = start;
+        if (slot >= count) return;                           // uniform across the group
+        body = d.colorLaunch[s + first + slot];
+        shp = d.shape[body];
+        seg = d.staticSeg[body];
+        nTet = d.postTets[body];
+        pdl_wait();
+    } else {
+        pdl_wait();
+        s = d.colorStart[color];
+        const uint32_t n = count != 0xFFFFFFFFu ? count : d.colorStart[color + 1] - s;
+        if (slot >= n) return;                               // uniform across the group
+        body = RESID ? d.colorList[s + slot] : d.colorLaunch[s + first + slot];
+        shp = d.shape[body];
+        seg = d.staticSeg[body];
+        nTet = d.postTets[body];
+    }
     const unsigned mask = LANES == 32 ? 0xffffffffu
                                       : (((1u << LANES) - 1u) << ((threadIdx.x & 31u) & ~(uint32_t)(LANES - 1)));
     (void)GROUPS;
-    // the solve takes its body from the color's launch order (lean
-    // particles first); the residual pass walks the color list itself
-    const uint32_t body = RESID ? d.colorList[s + slot] : d.colorLaunch[s + first + slot];
-    const float4 shp = d.shape[body];
     if (GENERAL && shp.w >= 0.0f) {                          // rigid: the 8-lane path
         const unsigned mask8 = mask & (0xFFu << ((threadIdx.x & 31u) & ~(uint32_t)(LANES - 1)));
         if (RESID) {
@@ -1501,7 +1536,7 @@ __global__ void __launch_bounds__(128, GENERAL ? 4 : (CLOTH ? AVBD_LEAN_CLOTH_MI
     float4 pl = make_float4(0, 0, 0, 0), inert = make_float4(0, 0, 0, 0);
     if (lane == 0) { pl = d.posLin[body]; inert = d.inertLin[body]; }
     ParticleAccum acc{m3_zero(), s3(0)};
-    const AdjView v = adj_view(d, body);
+    const AdjView v = adj_view_from(d, body, seg, nTet);
     const uint32_t cnt = v.count();
 #pragma unroll (kPrimalUnroll)
     for (uint32_t base = 0; base < cnt; base += LANES) {
@@ -1559,12 +1594,13 @@ __global__ void __launch_bounds__(128, GENERAL ? 4 : (CLOTH ? AVBD_LEAN_CLOTH_MI
 
 template <bool GENERAL, bool CLOTH>
 static void launch_primal_group(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count,
-                                uint32_t first, uint32_t lanes, cudaStream_t st) {
+                                uint32_t first, uint32_t start, uint32_t lanes, cudaStream_t st) {
     const int T = 128;
     const uint32_t blocks = (count * lanes + T - 1) / T;
-    if (lanes <= 8) launch_pdl(k_primal_group<8, GENERAL, CLOTH>, blocks, T, st, P, d, color, count, first);
-    else if (lanes <= 16) launch_pdl(k_primal_group<16, GENERAL, CLOTH>, blocks, T, st, P, d, color, count, first);
-    else launch_pdl(k_primal_group<32, GENERAL, CLOTH>, blocks, T, st, P, d, color, count, first);
+    if (lanes <= 8) launch_pdl(k_primal_group<8, GENERAL, CLOTH>, blocks, T, st, P, d, color, count, first, start);
+    else if (lanes <= 16)
+        launch_pdl(k_primal_group<16, GENERAL, CLOTH>, blocks, T, st, P, d, color, count, first, start);
+    else launch_pdl(k_primal_group<32, GENERAL, CLOTH>, blocks, T, st, P, d, color, count, first, start);
 }
 
 // ---------------------------------------------------------------------------
@@ -1600,29 +1636,38 @@ __device__ __forceinline__ AdjView staged_view(const DevPtrs& d, const StagedBod
 
 template <bool GENERAL, bool CLOTH>
 __global__ void __launch_bounds__(kStagedThreads, GENERAL ? 4 : 5)
-k_primal_staged(const Params P, const DevPtrs d, uint32_t color, uint32_t count, uint32_t first) {
+k_primal_staged(const Params P, const DevPtrs d, uint32_t color, uint32_t count, uint32_t first, uint32_t start) {
     __shared__ float slots[kStagedWords][kStagedSlots];
     __shared__ StagedBody info[kStagedGroups];
     __shared__ uint32_t offs[kStagedGroups + 1];
-    pdl_prologue();
+    pdl_trigger();
     const uint32_t tid = threadIdx.x;
-    const uint32_t s = d.colorStart[color] + first;
     const uint32_t head = blockIdx.x * kStagedGroups;
+    const bool early = start != NO_HOST_START;
     // bodies of the block, their adjacency views and an exclusive scan of
-    // their entry counts (warp 0, one lane per group)
+    // their entry counts (warp 0, one lane per group); with the start known
+    // on the host the static part (launch order, shape, static segment) is
+    // read before waiting for the previous grid
+    if (!early) pdl_wait();
+    const uint32_t s = (early ? start : d.colorStart[color]) + first;
+    uint32_t cnt = 0, body = 0xFFFFFFFFu;
+    StagedBody sb{};
+    const bool mine = tid < kStagedGroups && head + tid < count;
+    float4 bodyShape = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (mine) {
+        body = d.colorLaunch[s + head + tid];
+        bodyShape = d.shape[body];
+        const uint4 seg = d.staticSeg[body];
+        sb.preBase = seg.x; sb.nPre = seg.y; sb.postBase = seg.z; sb.nPost = seg.w;
+        sb.nTet = d.postTets[body];
+    }
+    if (early) pdl_wait();                                   // every thread, before any per-frame read
     if (tid < 32) {
-        uint32_t cnt = 0, body = 0xFFFFFFFFu;
-        StagedBody b{};
-        if (tid < kStagedGroups && head + tid < count) {
-            body = d.colorLaunch[s + head + tid];
-            const float4 shp = d.shape[body];
-            const uint4 seg = d.staticSeg[body];
-            b.preBase = seg.x; b.nPre = seg.y; b.postBase = seg.z; b.nPost = seg.w;
-            b.dynBase = d.dynStart[body]; b.nDyn = d.dynCount[body]; b.nMan = d.dynSplit[body];
-            b.nTet = d.postTets[body];
-            cnt = b.nPre + b.nDyn + b.nPost;
-            b.cnt = cnt;
-            if (GENERAL && shp.w >= 0.0f) cnt = 0;           // rigid: stages nothing
+        if (mine) {
+            sb.dynBase = d.dynStart[body]; sb.nDyn = d.dynCount[body]; sb.nMan = d.dynSplit[body];
+            cnt = sb.nPre + sb.nDyn + sb.nPost;
+            sb.cnt = cnt;
+            if (GENERAL && bodyShape.w >= 0.0f) cnt = 0;           // rigid: stages nothing
         }
         uint32_t incl = cnt;
 #pragma unroll
@@ -1632,10 +1677,10 @@ k_primal_staged(const Params P, const DevPtrs d, uint32_t color, uint32_t count,
         }
         const uint32_t off = incl - cnt;
         if (tid < kStagedGroups) {
-            b.body = body;
-            b.off = off;
-            b.staged = off >= (uint32_t)kStagedSlots ? 0u : min(cnt, (uint32_t)kStagedSlots - off);
-            info[tid] = b;
+            sb.body = body;
+            sb.off = off;
+            sb.staged = off >= (uint32_t)kStagedSlots ? 0u : min(cnt, (uint32_t)kStagedSlots - off);
+            info[tid] = sb;
             offs[tid] = off;
         }
         if (tid == kStagedGroups - 1) offs[kStagedGroups] = min(incl, (uint32_t)kStagedSlots);
@@ -1708,9 +1753,9 @@ k_primal_staged(const Params P, const DevPtrs d, uint32_t color, uint32_t count,
 
 template <bool GENERAL, bool CLOTH>
 static void launch_primal_staged(const Params& P, const DevPtrs& d, uint32_t color, uint32_t count,
-                                 uint32_t first, cudaStream_t st) {
+                                 uint32_t first, uint32_t start, cudaStream_t st) {
     const uint32_t blocks = (count + kStagedGroups - 1) / kStagedGroups;
-    launch_pdl(k_primal_staged<GENERAL, CLOTH>, blocks, kStagedThreads, st, P, d, color, count, first);
+    launch_pdl(k_primal_staged<GENERAL, CLOTH>, blocks, kStagedThreads, st, P, d, color, count, first, start);
 }
 
 void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color, uint32_t count,
@@ -1734,21 +1779,22 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
         const bool cloth = P.cloth || P.ogc;
         const uint32_t lean = z.particleFastPath ? upper : (z.colorLean ? min(z.colorLean[color], upper) : 0u);
         const uint32_t rest = upper - lean;
+        const uint32_t start = z.colorStartHost ? z.colorStartHost[color] : NO_HOST_START;
         const bool split = rest && lean && side && fork && join;
         if (split) {
             cudaEventRecord(fork, st);
             cudaStreamWaitEvent(side, fork, 0);
-            launch_primal_wide(P, d, color, rest, lean, side);
+            launch_primal_wide(P, d, color, rest, lean, start, side);
         }
         if (lean) {
             if (lanes == AVBD_PRIMAL_STAGED) {
-                if (cloth) launch_primal_staged<false, true>(P, d, color, lean, 0, st);
-                else launch_primal_staged<false, false>(P, d, color, lean, 0, st);
+                if (cloth) launch_primal_staged<false, true>(P, d, color, lean, 0, start, st);
+                else launch_primal_staged<false, false>(P, d, color, lean, 0, start, st);
             } else {
                 const uint32_t lanes_ = lanes < 8 ? 8 : (lanes > 32 ? 32 : lanes);
                 const uint32_t w = lanes_ <= 8 ? 8 : (lanes_ <= 16 ? 16 : 32);
-                if (cloth) launch_primal_group<false, true>(P, d, color, lean, 0, w, st);
-                else launch_primal_group<false, false>(P, d, color, lean, 0, w, st);
+                if (cloth) launch_primal_group<false, true>(P, d, color, lean, 0, start, w, st);
+                else launch_primal_group<false, false>(P, d, color, lean, 0, start, w, st);
             }
         }
         // the rest: a block per body (rigid bodies with many contacts)
@@ -1756,7 +1802,7 @@ void launch_primal_color(const Params& P, const DevPtrs& d, const Sizes& z, uint
             cudaEventRecord(join, side);
             cudaStreamWaitEvent(st, join, 0);
         } else {
-            launch_primal_wide(P, d, color, rest, lean, st);
+            launch_primal_wide(P, d, color, rest, lean, start, st);
         }
     }
 }
@@ -1773,13 +1819,13 @@ void launch_residual(const Params& P, const DevPtrs& d, const Sizes& z, float* p
             const uint32_t w = lanes <= 8 ? 8u : (lanes <= 16 ? 16u : 32u);
             const uint32_t blocks = (count * w + 127) / 128;
             if (z.particleFastPath) {
-                if (w == 8) k_primal_group<8, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count, 0u);
-                else if (w == 16) k_primal_group<16, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count, 0u);
-                else k_primal_group<32, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count, 0u);
+                if (w == 8) k_primal_group<8, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count, 0u, NO_HOST_START);
+                else if (w == 16) k_primal_group<16, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count, 0u, NO_HOST_START);
+                else k_primal_group<32, false, false, true><<<blocks, 128, 0, st>>>(P, g, color, count, 0u, NO_HOST_START);
             } else if (P.cloth || P.ogc) {
-                k_primal_group<32, true, true, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, g, color, count, 0u);
+                k_primal_group<32, true, true, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, g, color, count, 0u, NO_HOST_START);
             } else {
-                k_primal_group<32, true, false, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, g, color, count, 0u);
+                k_primal_group<32, true, false, true><<<(count * 32 + 127) / 128, 128, 0, st>>>(P, g, color, count, 0u, NO_HOST_START);
             }
         };
         // every body at once: 8 lanes per body keep the most bodies in
@@ -1791,8 +1837,8 @@ void launch_residual(const Params& P, const DevPtrs& d, const Sizes& z, float* p
         DevPtrs g = d;
         g.learnResidBodies = perBody;
         const uint32_t blocks = (n * 8 + 127) / 128;
-        if (P.cloth || P.ogc) k_primal_group<8, true, true, true><<<blocks, 128, 0, st>>>(P, g, 0u, n, 0u);
-        else k_primal_group<8, true, false, true><<<blocks, 128, 0, st>>>(P, g, 0u, n, 0u);
+        if (P.cloth || P.ogc) k_primal_group<8, true, true, true><<<blocks, 128, 0, st>>>(P, g, 0u, n, 0u, NO_HOST_START);
+        else k_primal_group<8, true, false, true><<<blocks, 128, 0, st>>>(P, g, 0u, n, 0u, NO_HOST_START);
     }
     k_sum_fixed<<<1, 1024, 0, st>>>(perBody, n, total);
 }
