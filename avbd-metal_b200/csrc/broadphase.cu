@@ -193,16 +193,18 @@ __global__ void k_bp_sort_cells(const uint32_t* count, const uint32_t* start, co
 }
 
 // The rigid colliders of every bucket, in bucket (collider) order: a warp
-// reads 32 buckets' rigid counts at once and compacts each bucket that has
-// any, one after another.
+// reads a group of buckets' rigid counts at once (bucket_group) and
+// compacts each bucket that has any, one after another.
 __global__ void k_bp_rigid_compact(const Params P, const DevPtrs d) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
-    // 32 buckets' rigid counts per coalesced load, then one bucket at a time
-    for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u; base < P.gridHashSize;
-         base += warps * 32u) {
+    // a group of buckets' rigid counts per coalesced load, then one bucket
+    // at a time
+    const uint32_t G = bucket_group(P.gridHashSize, warps);
+    for (uint32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * G; base < P.gridHashSize;
+         base += warps * G) {
         const uint32_t hl = base + lane;
-        uint32_t live = __ballot_sync(0xffffffffu, hl < P.gridHashSize && d.cellRigid[hl] != 0u);
+        uint32_t live = __ballot_sync(0xffffffffu, lane < G && hl < P.gridHashSize && d.cellRigid[hl] != 0u);
         while (live) {
             const uint32_t h = base + (uint32_t)(__ffs(live) - 1);
             live &= live - 1u;
