@@ -85,6 +85,10 @@ __global__ void k_elem_bin(const Params P, const DevPtrs d, uint32_t total) {
         if (!SCATTER && (raw.x - c0.x > 3 || raw.y - c0.y > 3 || raw.z - c0.z > 3))
             atomicAdd(&d.counters->datGridOverflow, 1u);
         const I3 c1 = imin3(raw, iadd(c0, 3));
+        // the range the candidate tests compare against (they computed it
+        // from the same padded box, to the same bits)
+        if (!SCATTER)
+            d.elemRange[gid] = make_int4(c0.x, c0.y, c0.z, (c1.x - c0.x) | ((c1.y - c0.y) << 2) | ((c1.z - c0.z) << 4));
         const bool tri = gid < P.numTris;
         const uint32_t entry = tri ? gid : gid - P.numTris;
         const uint32_t half = tri ? 0u : P.elemHashSize;
@@ -115,14 +119,17 @@ __global__ void k_elem_bin(const Params P, const DevPtrs d, uint32_t total) {
 __device__ __forceinline__ bool vt_candidate(const Params& P, const DevPtrs& d, uint32_t v, float3 p, I3 cell,
                                              uint32_t ns, uint32_t ne, uint32_t entry, float query2) {
     if (entry >= P.numTris) return false;
+    // the triangle's binned cell range (from its padded box) must hold the
+    // query cell; then the box prefilter (independent predicates, so the
+    // cheaper one goes first)
+    const int4 rg = d.elemRange[entry];
+    const I3 tc0{rg.x, rg.y, rg.z};
+    const I3 tc1{rg.x + (rg.w & 3), rg.y + ((rg.w >> 2) & 3), rg.z + ((rg.w >> 4) & 3)};
+    if (cell.x < tc0.x || cell.y < tc0.y || cell.z < tc0.z || cell.x > tc1.x || cell.y > tc1.y || cell.z > tc1.z)
+        return false;
     const float4 bl = d.elemBox[2 * entry], bh = d.elemBox[2 * entry + 1];
     const float r = prefilter_reach(P);
     if (p.x < bl.x - r || p.y < bl.y - r || p.z < bl.z - r || p.x > bh.x + r || p.y > bh.y + r || p.z > bh.z + r)
-        return false;
-    const float3 lo = xyz(bl) - s3(P.queryRadius), hi = xyz(bh) + s3(P.queryRadius);
-    const I3 tc0 = cell_of(lo, P.elemCellSize);
-    const I3 tc1 = imin3(cell_of(hi, P.elemCellSize), iadd(tc0, 3));
-    if (cell.x < tc0.x || cell.y < tc0.y || cell.z < tc0.z || cell.x > tc1.x || cell.y > tc1.y || cell.z > tc1.z)
         return false;
     const uint4 t = d.tris[entry];
     if (t.x == v || t.y == v || t.z == v) return false;
@@ -146,17 +153,21 @@ __device__ __forceinline__ bool ee_candidate(const Params& P, const DevPtrs& d, 
                                              float3 a1, float3 alo, float3 ahi, I3 ac0, I3 ac1, I3 cell,
                                              uint32_t other, float query2, uint32_t& flags) {
     if (other <= gid || other >= P.numEdges) return false;
+    // the pair is taken in the first cell the two binned ranges share (each
+    // range from the element's padded box, stored by the binning pass); this
+    // rejects the pair in every other shared cell before the box prefilter
+    // (independent predicates, so the cheaper one goes first)
+    const int4 rg = d.elemRange[P.numTris + other];
+    const I3 bc0{rg.x, rg.y, rg.z};
+    const I3 bc1{rg.x + (rg.w & 3), rg.y + ((rg.w >> 2) & 3), rg.z + ((rg.w >> 4) & 3)};
+    const I3 o0 = imax3(ac0, bc0), o1 = imin3(ac1, bc1);
+    if (o0.x > o1.x || o0.y > o1.y || o0.z > o1.z) return false;
+    if (cell.x != o0.x || cell.y != o0.y || cell.z != o0.z) return false;
     const float4 bl = d.elemBox[2 * (P.numTris + other)], bh = d.elemBox[2 * (P.numTris + other) + 1];
     const float r = prefilter_reach(P);
     if (bl.x - ahi.x > r || bl.y - ahi.y > r || bl.z - ahi.z > r || alo.x - bh.x > r || alo.y - bh.y > r ||
         alo.z - bh.z > r)
         return false;
-    const float3 blo = xyz(bl) - s3(P.queryRadius), bhi = xyz(bh) + s3(P.queryRadius);
-    const I3 bc0 = cell_of(blo, P.elemCellSize);
-    const I3 bc1 = imin3(cell_of(bhi, P.elemCellSize), iadd(bc0, 3));
-    const I3 o0 = imax3(ac0, bc0), o1 = imin3(ac1, bc1);
-    if (o0.x > o1.x || o0.y > o1.y || o0.z > o1.z) return false;
-    if (cell.x != o0.x || cell.y != o0.y || cell.z != o0.z) return false;
     const uint2 b = d.edges[other];
     if (b.x == a.x || b.x == a.y || b.y == a.x || b.y == a.y) return false;
     float sb, tb;

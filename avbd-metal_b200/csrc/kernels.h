@@ -88,6 +88,8 @@ struct DevPtrs {
     // cloth: per frame
     uint32_t *elemCellCount, *elemCellStart, *elemCursor, *elemCells;   // 2H buckets: triangles, edges
     float4* elemBox;                            // tight AABB per element (lo, hi)
+    int4* elemRange;                            // binned cell range per element: first cell,
+                                                // w = extents (x | y << 2 | z << 4, each 0..3)
     uint32_t *datOwnerCount, *datOwnerStart;    // pairs per query owner (particles, edges)
     uint4* datPairs;                            // (kind, owner, other, flags)
     uint2* datCache;                            // first pairs of each owner from the counting pass (other, flags)

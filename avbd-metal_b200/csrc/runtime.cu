@@ -705,6 +705,7 @@ struct avbd_solver {
         if (P.cloth) {
             const size_t elems = (size_t)H.numTris + H.numEdges;
             ok = ok && alloc(d.elemBox, 2 * elems, "elemBox");
+            ok = ok && alloc(d.elemRange, elems, "elemRange");
             ok = ok && alloc(d.datPairs, H.maxDatPairs, "planarDATPairs");
             ok = ok && alloc(d.datCache, 16 * ((size_t)P.numParticles + H.numEdges), "planarDATPairCache");
             std::vector<uint32_t> ones(nb, 0x3F800000u);
