@@ -183,7 +183,8 @@ def config(scene, args, world):
             "window": {"preroll_frames": args.preroll, "warmup_frames": args.warmup, "timed_frames": args.steps,
                        "first_timed_frame": args.preroll + args.warmup + 1},
             "parallelism": (f"world shards x{world}" if WORKLOAD_KEY == "batched-worlds" else f"replicas x{world}"),
-            "warm_start": "plain gamma warm start (value); learned warm start in learned_warm_start"}
+            "warm_start": "plain gamma warm start (value); learned warm start in learned_warm_start",
+            "l2": "GPU arm: flushed between timed steps (256 MiB device write, untimed)"}
 
 
 def dist_setup(args):
@@ -654,16 +655,17 @@ def run_ours(args, world, rank, local):
         cpu = {"value": cv, "unit": unit(), "cores": cores, "kind": kind, "sample": sample}
     if rank == 0:
         cfg = config(scene, args, world)
-        cfg.update({"l2": "flushed between timed steps (256 MiB device write, untimed)",
-                    "timing": "CUDA events on the solver stream per step, max over ranks",
-                    "colors": int(counters.used_colors),
-                    "lanes_per_body": prof["color_lanes"][:int(counters.used_colors)]})
         line = {
             "metric": METRIC, "value": value, "unit": unit(), "n_gpus": world,
             "steps": K, "warmup": W, "ms_per_step": dev_ms / K,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded SplitMix64 scene)",
             "config": cfg,
+            "timing": "CUDA events on the solver stream per step, max over ranks",
+            # per static color: the primal variant the autotuner kept for its
+            # lean particles (8 / 16 / 32 lanes per body, 1 = staged kernel)
+            "primal_launch": {"colors": int(counters.used_colors),
+                              "lanes_per_body": prof["color_lanes"][:int(counters.used_colors)]},
             "clocks": clock, "e2e": e2e,
             "gpu_launches": int(kernels_per_frame * K),
             "roofline": {"bound": "hbm",
