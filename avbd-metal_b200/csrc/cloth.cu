@@ -116,8 +116,11 @@ __global__ void k_elem_bin(const Params P, const DevPtrs d, uint32_t total) {
 // The reference's V-T acceptance is a conjunction of pure predicates
 // (27_planar_dat.metal:75-101); they are evaluated cheapest first, after a
 // conservative box test that every accepted pair passes.
-__device__ __forceinline__ bool vt_candidate(const Params& P, const DevPtrs& d, uint32_t v, float3 p, I3 cell,
-                                             uint32_t ns, uint32_t ne, uint32_t entry, float query2) {
+// The conjunction is split in two: the cheap predicates (index, cell range,
+// box prefilter) and the rest (topology, exact distance, exclusions), so the
+// pair kernel can run the second part only on the candidates that pass the
+// first, packed onto full warps.
+__device__ __forceinline__ bool vt_cheap(const Params& P, const DevPtrs& d, float3 p, I3 cell, uint32_t entry) {
     if (entry >= P.numTris) return false;
     // the triangle's binned cell range (from its padded box) must hold the
     // query cell; then the box prefilter (independent predicates, so the
@@ -129,8 +132,10 @@ __device__ __forceinline__ bool vt_candidate(const Params& P, const DevPtrs& d, 
         return false;
     const float4 bl = d.elemBox[2 * entry], bh = d.elemBox[2 * entry + 1];
     const float r = prefilter_reach(P);
-    if (p.x < bl.x - r || p.y < bl.y - r || p.z < bl.z - r || p.x > bh.x + r || p.y > bh.y + r || p.z > bh.z + r)
-        return false;
+    return !(p.x < bl.x - r || p.y < bl.y - r || p.z < bl.z - r || p.x > bh.x + r || p.y > bh.y + r || p.z > bh.z + r);
+}
+__device__ __forceinline__ bool vt_full(const Params& P, const DevPtrs& d, uint32_t v, float3 p, uint32_t ns,
+                                        uint32_t ne, uint32_t entry, float query2) {
     const uint4 t = d.tris[entry];
     if (t.x == v || t.y == v || t.z == v) return false;
     float3 bary;
@@ -149,9 +154,8 @@ __device__ __forceinline__ bool vt_candidate(const Params& P, const DevPtrs& d, 
 
 // E-E acceptance (27_planar_dat.metal:155-204), cheapest predicates first
 // after a conservative box-separation test.
-__device__ __forceinline__ bool ee_candidate(const Params& P, const DevPtrs& d, uint32_t gid, uint2 a, float3 a0,
-                                             float3 a1, float3 alo, float3 ahi, I3 ac0, I3 ac1, I3 cell,
-                                             uint32_t other, float query2, uint32_t& flags) {
+__device__ __forceinline__ bool ee_cheap(const Params& P, const DevPtrs& d, uint32_t gid, float3 alo, float3 ahi,
+                                         I3 ac0, I3 ac1, I3 cell, uint32_t other) {
     if (other <= gid || other >= P.numEdges) return false;
     // the pair is taken in the first cell the two binned ranges share (each
     // range from the element's padded box, stored by the binning pass); this
@@ -165,9 +169,11 @@ __device__ __forceinline__ bool ee_candidate(const Params& P, const DevPtrs& d, 
     if (cell.x != o0.x || cell.y != o0.y || cell.z != o0.z) return false;
     const float4 bl = d.elemBox[2 * (P.numTris + other)], bh = d.elemBox[2 * (P.numTris + other) + 1];
     const float r = prefilter_reach(P);
-    if (bl.x - ahi.x > r || bl.y - ahi.y > r || bl.z - ahi.z > r || alo.x - bh.x > r || alo.y - bh.y > r ||
-        alo.z - bh.z > r)
-        return false;
+    return !(bl.x - ahi.x > r || bl.y - ahi.y > r || bl.z - ahi.z > r || alo.x - bh.x > r || alo.y - bh.y > r ||
+             alo.z - bh.z > r);
+}
+__device__ __forceinline__ bool ee_full(const Params& P, const DevPtrs& d, uint32_t gid, uint2 a, float3 a0,
+                                        float3 a1, uint32_t other, float query2, uint32_t& flags) {
     const uint2 b = d.edges[other];
     if (b.x == a.x || b.x == a.y || b.y == a.x || b.y == a.y) return false;
     float sb, tb;
@@ -209,16 +215,57 @@ constexpr uint32_t kDatCache = 16;
 
 // Eight blocks per SM (at most 64 registers, no spills): the pair scan is
 // latency bound and gains from the extra warps (cloth frame 4.93 -> 4.66 ms).
+// A warp's candidates first pass the cheap predicates on every lane; the
+// survivors queue up in shared memory and the rest of the test runs on 32
+// of them at a time, so the expensive part (exact distance, exclusions)
+// keeps every lane busy instead of the few whose candidate survived.  The
+// accepted set is the same; its discovery order differs, and each owner's
+// pairs are sorted by `other` after the emitting pass.
 template <bool EMIT>
 __global__ void __launch_bounds__(128, 8) k_dat_pairs(const Params P, const DevPtrs d, uint32_t owners) {
+    __shared__ uint32_t survivors[4][64];
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     const float query2 = P.queryRadius * P.queryRadius;
     const uint32_t below = (1u << lane) - 1u;
+    uint32_t* q = survivors[threadIdx.x >> 5];
     for (uint32_t owner = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; owner < owners; owner += warps) {
-        uint32_t count = 0;
+        uint32_t count = 0, qn = 0;                           // qn: queued survivors (warp-uniform)
         const uint32_t base = EMIT ? d.datOwnerStart[owner] : 0u;
         uint2* cache = d.datCache + (size_t)owner * kDatCache;
+        // one full-test result per lane: count it, cache the first ones, emit
+        auto record = [&](bool pass, uint32_t kind, uint32_t id, uint32_t entry, uint32_t flags) {
+            const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
+            if (EMIT && pass) {
+                const uint32_t slot = base + count + __popc(ballot & below);
+                if (slot < P.maxDatPairs) d.datPairs[slot] = make_uint4(kind, id, entry, flags);
+            }
+            if (!EMIT && pass && count + __popc(ballot & below) < kDatCache)
+                cache[count + __popc(ballot & below)] = make_uint2(entry, flags);
+            count += __popc(ballot);
+        };
+        // queue this lane's survivor of the cheap predicates
+        auto enqueue = [&](bool cand, uint32_t entry) {
+            const uint32_t ballot = __ballot_sync(0xffffffffu, cand);
+            if (cand) q[qn + __popc(ballot & below)] = entry;
+            qn += __popc(ballot);
+            __syncwarp();
+        };
+        // take up to 32 queued entries (one per lane) and move the rest to
+        // the head of the queue
+        auto dequeue = [&](uint32_t& entry) -> bool {
+            const uint32_t take = qn < 32u ? qn : 32u;
+            const bool mine = lane < take;
+            if (mine) entry = q[lane];
+            const uint32_t rest = qn - take;
+            uint32_t moved = 0;
+            if (lane < rest) moved = q[take + lane];
+            __syncwarp();
+            if (lane < rest) q[lane] = moved;
+            __syncwarp();
+            qn = rest;
+            return mine;
+        };
         if (EMIT) {
             const uint32_t n = d.datOwnerCount[owner];
             if (n <= kDatCache) {
@@ -251,24 +298,25 @@ __global__ void __launch_bounds__(128, 8) k_dat_pairs(const Params P, const DevP
             const uint32_t h = elem_hash(cell, P.elemHashSize);           // triangle half
             const uint32_t s0 = d.elemCellStart[h], e0 = s0 + d.elemCellCount[h];
             const uint32_t ns = d.nbrStart[v], ne = ns + d.nbrCount[v];
+            auto drain = [&](bool all) {
+                while (qn >= 32u || (all && qn > 0u)) {
+                    uint32_t entry = 0;
+                    const bool pass = dequeue(entry) && vt_full(P, d, v, p, ns, ne, entry, query2);
+                    record(pass, DAT_PAIR_VT, v, entry, DAT_PAIR_TRUNCATE | DAT_PAIR_CONTACT);
+                }
+            };
             for (uint32_t k0 = s0; k0 < e0; k0 += 32) {
                 const uint32_t k = k0 + lane;
                 uint32_t entry = 0;
-                bool pass = false;
+                bool cand = false;
                 if (k < e0) {
                     entry = d.elemCells[k];
-                    pass = vt_candidate(P, d, v, p, cell, ns, ne, entry, query2);
+                    cand = vt_cheap(P, d, p, cell, entry);
                 }
-                const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
-                if (EMIT && pass) {
-                    const uint32_t slot = base + count + __popc(ballot & below);
-                    if (slot < P.maxDatPairs)
-                        d.datPairs[slot] = make_uint4(DAT_PAIR_VT, v, entry, DAT_PAIR_TRUNCATE | DAT_PAIR_CONTACT);
-                }
-                if (!EMIT && pass && count + __popc(ballot & below) < kDatCache)
-                    cache[count + __popc(ballot & below)] = make_uint2(entry, DAT_PAIR_TRUNCATE | DAT_PAIR_CONTACT);
-                count += __popc(ballot);
+                enqueue(cand, entry);
+                drain(false);
             }
+            drain(true);
         } else {
             const uint32_t gid = owner - P.numParticles;
             const uint2 a = d.edges[gid];
@@ -287,6 +335,13 @@ __global__ void __launch_bounds__(128, 8) k_dat_pairs(const Params P, const DevP
                 atomicAdd(&d.counters->datGridOverflow, 1u);
             const I3 ac1 = imin3(raw, iadd(ac0, 3));
             const float3 alo = vmin(a0, a1), ahi = vmax(a0, a1);
+            auto drain = [&](bool all) {
+                while (qn >= 32u || (all && qn > 0u)) {
+                    uint32_t entry = 0, flags = 0;
+                    const bool pass = dequeue(entry) && ee_full(P, d, gid, a, a0, a1, entry, query2, flags);
+                    record(pass, DAT_PAIR_EE, gid, entry, flags);
+                }
+            };
             for (int z = ac0.z; z <= ac1.z; z++)
                 for (int y = ac0.y; y <= ac1.y; y++)
                     for (int x = ac0.x; x <= ac1.x; x++) {
@@ -295,23 +350,17 @@ __global__ void __launch_bounds__(128, 8) k_dat_pairs(const Params P, const DevP
                         const uint32_t s0 = d.elemCellStart[h], e0 = s0 + d.elemCellCount[h];
                         for (uint32_t k0 = s0; k0 < e0; k0 += 32) {
                             const uint32_t k = k0 + lane;
-                            uint32_t entry = 0, flags = 0;
-                            bool pass = false;
+                            uint32_t entry = 0;
+                            bool cand = false;
                             if (k < e0) {
                                 entry = d.elemCells[k];
-                                pass = ee_candidate(P, d, gid, a, a0, a1, alo, ahi, ac0, ac1, cell, entry, query2, flags);
+                                cand = ee_cheap(P, d, gid, alo, ahi, ac0, ac1, cell, entry);
                             }
-                            const uint32_t ballot = __ballot_sync(0xffffffffu, pass);
-                            if (EMIT && pass) {
-                                const uint32_t slot = base + count + __popc(ballot & below);
-                                if (slot < P.maxDatPairs)
-                                    d.datPairs[slot] = make_uint4(DAT_PAIR_EE, gid, entry, flags);
-                            }
-                            if (!EMIT && pass && count + __popc(ballot & below) < kDatCache)
-                                cache[count + __popc(ballot & below)] = make_uint2(entry, flags);
-                            count += __popc(ballot);
+                            enqueue(cand, entry);
+                            drain(false);
                         }
                     }
+            drain(true);
         }
         if (!EMIT) {
             if (lane == 0) d.datOwnerCount[owner] = count;
