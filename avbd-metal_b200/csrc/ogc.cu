@@ -506,14 +506,19 @@ __device__ void warp_merge(Best4A& loc, Best4& out, uint32_t lane) {
 
 // The serial tracked-set update of vt_consider without the held-set test
 // (duplicates are removed by the merge; their bound contributions repeat).
-__device__ void vt_consider_lane(const Params& P, const DevPtrs& d, const VtQuery& q, Best4A& loc, float& ownB2,
-                                 uint32_t t, uint32_t arr) {
-    if (t >= P.numTris) return;
+// Split in two for the reseed's packed lanes: the topological rejections
+// (index, own triangle, same closed solid) and the rest, which is only run
+// on the candidates the first part keeps.
+__device__ __forceinline__ bool vt_kept(const Params& P, const DevPtrs& d, const VtQuery& q, uint32_t t) {
+    if (t >= P.numTris) return false;
     const uint4 tid = d.tris[t];
-    if (tid.x == q.v || tid.y == q.v || tid.z == q.v) return;
-    if (q.solidV && d.clothGroup[tid.x] == q.gv && d.clothGroup[tid.y] == q.gv && d.clothGroup[tid.z] == q.gv &&
-        d.clothVert[tid.x] == 0u && d.clothVert[tid.y] == 0u && d.clothVert[tid.z] == 0u)
-        return;
+    if (tid.x == q.v || tid.y == q.v || tid.z == q.v) return false;
+    return !(q.solidV && d.clothGroup[tid.x] == q.gv && d.clothGroup[tid.y] == q.gv && d.clothGroup[tid.z] == q.gv &&
+             d.clothVert[tid.x] == 0u && d.clothVert[tid.y] == 0u && d.clothVert[tid.z] == 0u);
+}
+__device__ void vt_consider_kept(const Params& P, const DevPtrs& d, const VtQuery& q, Best4A& loc, float& ownB2,
+                                 uint32_t t, uint32_t arr) {
+    const uint4 tid = d.tris[t];
     float3 bary;
     const float3 cp = closest_pt_triangle(q.pv, xyz(d.posLin[tid.x]), xyz(d.posLin[tid.y]), xyz(d.posLin[tid.z]), bary);
     const float3 dd = q.pv - cp;
@@ -531,14 +536,16 @@ __device__ void vt_consider_lane(const Params& P, const DevPtrs& d, const VtQuer
     }
 }
 
-__device__ void ee_consider_lane(const Params& P, const DevPtrs& d, const EeQuery& q, Best4A& loc, float& ownB2,
-                                 uint32_t e, uint32_t arr) {
-    if (e >= P.numEdges || e == q.gid) return;
+__device__ __forceinline__ bool ee_kept(const Params& P, const DevPtrs& d, const EeQuery& q, uint32_t e) {
+    if (e >= P.numEdges || e == q.gid) return false;
     const uint2 eB = d.edges[e];
-    if (eB.x == q.eA.x || eB.x == q.eA.y || eB.y == q.eA.x || eB.y == q.eA.y) return;
-    if (q.solidA && d.clothGroup[eB.x] == q.gA && d.clothGroup[eB.y] == q.gA && d.clothVert[eB.x] == 0u &&
-        d.clothVert[eB.y] == 0u)
-        return;
+    if (eB.x == q.eA.x || eB.x == q.eA.y || eB.y == q.eA.x || eB.y == q.eA.y) return false;
+    return !(q.solidA && d.clothGroup[eB.x] == q.gA && d.clothGroup[eB.y] == q.gA && d.clothVert[eB.x] == 0u &&
+             d.clothVert[eB.y] == 0u);
+}
+__device__ void ee_consider_kept(const Params& P, const DevPtrs& d, const EeQuery& q, Best4A& loc, float& ownB2,
+                                 uint32_t e, uint32_t arr) {
+    const uint2 eB = d.edges[e];
     float s, t;
     const float3 b0 = xyz(d.posLin[eB.x]), b1 = xyz(d.posLin[eB.y]);
     closest_seg_seg(q.a0, q.a1, b0, b1, s, t);
@@ -560,8 +567,12 @@ __device__ void ee_consider_lane(const Params& P, const DevPtrs& d, const EeQuer
 }
 
 __global__ void __launch_bounds__(128) k_ogc_reseed(const Params P, const DevPtrs d) {
+    // per warp: the queue of candidates kept by the topological tests
+    // (element, arrival), drained 32 at a time onto the lanes
+    __shared__ uint32_t keptId[4][64], keptArr[4][64];
     const uint32_t n = d.counters->ogcQueue;
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t w = threadIdx.x >> 5, below = (1u << lane) - 1u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
         const uint32_t o = d.datOwnerCount[i];
@@ -586,9 +597,14 @@ __global__ void __launch_bounds__(128) k_ogc_reseed(const Params P, const DevPtr
             cc = cell_of((qe.a0 + qe.a1) * 0.5f, P.elemCellSize);
             half = P.elemHashSize;
         }
-        // candidate j of the stream arrives as 4 + j; lane l takes j = l mod 32.
-        // Lane c < 27 first loads the range of bucket c (cells in (dz, dy, dx)
-        // order), so the 27 buckets cost one dependent load, not 27.
+        // Candidate j of the stream arrives as 4 + j.  Every lane applies the
+        // topological rejections to consecutive candidates; the kept ones
+        // queue in arrival order and the distance part runs on 32 of them
+        // at a time, lane l taking the l-th of each batch — every lane still
+        // sees its candidates in increasing arrival order, which is all the
+        // per-lane lists and the warp merge need.  Lane c < 27 first loads
+        // the range of bucket c (cells in (dz, dy, dx) order), so the 27
+        // buckets cost one dependent load, not 27.
         uint32_t cellS = 0, cellN = 0;
         if (lane < 27) {
             const int dz = (int)(lane / 9u) - 1, dy = (int)((lane / 3u) % 3u) - 1, dx = (int)(lane % 3u) - 1;
@@ -596,17 +612,48 @@ __global__ void __launch_bounds__(128) k_ogc_reseed(const Params P, const DevPtr
             cellS = d.elemCellStart[h];
             cellN = d.elemCellCount[h];
         }
+        uint32_t qn = 0;                                      // queued (warp-uniform)
+        auto drain = [&](bool all) {
+            while (qn >= 32u || (all && qn > 0u)) {
+                const uint32_t take = qn < 32u ? qn : 32u, rest = qn - take;
+                const bool mine = lane < take;
+                uint32_t id = 0, arr = 0, mid = 0, marr = 0;
+                if (mine) { id = keptId[w][lane]; arr = keptArr[w][lane]; }
+                if (lane < rest) { mid = keptId[w][take + lane]; marr = keptArr[w][take + lane]; }
+                __syncwarp();
+                if (lane < rest) { keptId[w][lane] = mid; keptArr[w][lane] = marr; }
+                __syncwarp();
+                qn = rest;
+                if (mine) {
+                    if (vt) vt_consider_kept(P, d, qv, loc, ownB2, id, arr);
+                    else ee_consider_kept(P, d, qe, loc, ownB2, id, arr);
+                }
+            }
+        };
         uint32_t base = 0;
         for (uint32_t c = 0; c < 27; c++) {
             const uint32_t s0 = __shfl_sync(0xffffffffu, cellS, (int)c);
             const uint32_t cnt = __shfl_sync(0xffffffffu, cellN, (int)c);
-            for (uint32_t k = (lane - base) & 31u; k < cnt; k += 32) {
-                const uint32_t arr = 4u + base + k;
-                if (vt) vt_consider_lane(P, d, qv, loc, ownB2, d.elemCells[s0 + k], arr);
-                else ee_consider_lane(P, d, qe, loc, ownB2, d.elemCells[s0 + k], arr);
+            for (uint32_t k0 = 0; k0 < cnt; k0 += 32) {
+                const uint32_t k = k0 + lane;
+                uint32_t id = 0;
+                bool kept = false;
+                if (k < cnt) {
+                    id = d.elemCells[s0 + k];
+                    kept = vt ? vt_kept(P, d, qv, id) : ee_kept(P, d, qe, id);
+                }
+                const uint32_t ballot = __ballot_sync(0xffffffffu, kept);
+                if (kept) {
+                    keptId[w][qn + __popc(ballot & below)] = id;
+                    keptArr[w][qn + __popc(ballot & below)] = 4u + base + k;
+                }
+                qn += __popc(ballot);
+                __syncwarp();
+                drain(false);
             }
             base += cnt;
         }
+        drain(true);
         Best4 best;
         warp_merge(loc, best, lane);
 #pragma unroll
