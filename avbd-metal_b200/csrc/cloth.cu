@@ -24,6 +24,7 @@
 // primal writes posNext, so bodies of one color read each other's pre-color
 // pose.
 #include "elements.cuh"
+#include "pdl.cuh"
 
 namespace avbd {
 
@@ -842,6 +843,7 @@ __device__ __forceinline__ float3 cur_pos(const Params& P, const DevPtrs& d, uin
 }
 
 __global__ void k_dat_reduce(const Params P, const DevPtrs d, uint32_t color) {
+    pdl_prologue();
     const uint32_t count = d.counters->datStored;
     const float relax = P.planarDATRelaxation;
     const bool full = color == FULL_PASS;
@@ -1021,13 +1023,19 @@ __global__ void k_dat_apply_particles(const Params P, const DevPtrs d) {
 
 // Publish one color's solve: surface vertices through their fraction, every
 // other body of the color as solved.
-__global__ void k_dat_apply_color(const Params P, const DevPtrs d, uint32_t color, uint32_t count) {
+__global__ void k_dat_apply_color(const Params P, const DevPtrs d, uint32_t color, uint32_t count, uint32_t start) {
+    pdl_trigger();
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    const uint32_t v = d.colorList[d.colorStart[color] + i];
+    // with the color's start known on the host, the color list and the cloth
+    // group (set at upload) are read before waiting for the previous grid
+    if (start == NO_HOST_START) pdl_wait();
+    const uint32_t v = d.colorList[(start == NO_HOST_START ? d.colorStart[color] : start) + i];
+    const bool unclothed = d.clothGroup[v] == 0u;
+    if (start != NO_HOST_START) pdl_wait();
     const float mass = d.posLin[v].w;
     const float3 next = xyz(d.posNext[v]);
-    if (d.clothGroup[v] == 0u) {
+    if (unclothed) {
         d.posLin[v] = mk4(next, mass);
         d.posAng[v] = d.angNext[v];
         return;
@@ -1126,8 +1134,10 @@ void launch_cloth_accept(const Params& P, const DevPtrs& d, const Sizes& z, cuda
 void launch_dat_color(const Params& P, const DevPtrs& d, const Sizes& z, uint32_t color, uint32_t count,
                       cudaStream_t st) {
     if (count == 0) return;
-    k_dat_reduce<<<blocks_for(z.maxDatPairs, 128), 128, 0, st>>>(P, d, color);
-    k_dat_apply_color<<<(count + 127) / 128, 128, 0, st>>>(P, d, color, count);
+    // programmatic dependent launches, as the primal before them
+    launch_pdl(k_dat_reduce, blocks_for(z.maxDatPairs, 128), 128, st, P, d, color);
+    launch_pdl(k_dat_apply_color, (count + 127) / 128, 128, st, P, d, color, count,
+               z.colorStartHost ? z.colorStartHost[color] : NO_HOST_START);
 }
 
 void launch_cloth_restore(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
