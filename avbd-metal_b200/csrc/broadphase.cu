@@ -275,8 +275,13 @@ __global__ void k_global_chunks(const Params P, const DevPtrs d) {
         clo = xyz(cc) - s3(cc.w);
         chi = xyz(cc) + s3(cc.w);
         const uint32_t o = d.colOwner[c];
+        const float4 shp = d.shape[o];
         const float3 po = xyz(d.posLin[o]);
-        const float rb = fabsf(d.shape[o].w);
+        const float rb = fabsf(shp.w);
+        // the owner's pose and shape in one record for the global scans
+        d.globalRec[3 * (size_t)g] = mk4(po, shp.w);
+        d.globalRec[3 * (size_t)g + 1] = d.posAng[o];
+        d.globalRec[3 * (size_t)g + 2] = mk4(xyz(shp), __uint_as_float(d.bodyShape[o]));
         blo = po - s3(rb);
         bhi = po + s3(rb);
         // a non-finite member makes the chunk unbounded (never skipped)

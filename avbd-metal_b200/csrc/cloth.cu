@@ -506,17 +506,6 @@ __global__ void __launch_bounds__(128, 6) k_rt_emit(const Params P, const DevPtr
                     emitted++;
                 }
             };
-            auto near_body = [&](uint32_t o) {
-                const float4 sh = d.shape[o];
-                const float3 po = xyz(d.posLin[o]);
-                bool nearO = dist3(po, m) <= rT + fabsf(sh.w) + P.collisionMargin;
-                if (nearO && d.bodyShape[o] == AVBD_SHAPE_BOX) {
-                    const float3 lm = q_rotate(q_conj(d.posAng[o]), m - po);
-                    const float3 dq2 = mx3(abs3(lm) - xyz(sh) * 0.5f, s3(0.0f));
-                    nearO = len3(dq2) <= rT + P.collisionMargin + 0.05f;
-                }
-                return nearO;
-            };
             if (lane == 0) {
             if (P.numHashedRigid > 0 && P.numHashedRigid <= 8) {
                 for (uint32_t ri = 0; ri < P.numHashed && emitted < RT_MAX_PER_TRI; ri++) {
@@ -567,15 +556,28 @@ __global__ void __launch_bounds__(128, 6) k_rt_emit(const Params P, const DevPtr
                         const uint32_t g = gb + lane;
                         bool cand = false;
                         if (g < P.numGlobals) {
-                            const uint32_t o = d.colOwner[d.globalIdx[g]];
-                            cand = d.shape[o].w >= 0.0f && near_body(o);
+                            // the owner's reach test (its bounding sphere, then a
+                            // box's padded extent) on the global's record (pose
+                            // and shape, written this frame by the chunk pass):
+                            // one load level instead of three
+                            const float4 r0 = d.globalRec[3 * (size_t)g];
+                            const float3 po = xyz(r0);
+                            cand = r0.w >= 0.0f && dist3(po, m) <= rT + fabsf(r0.w) + P.collisionMargin;
+                            if (cand) {
+                                const float4 r2 = d.globalRec[3 * (size_t)g + 2];
+                                if (__float_as_uint(r2.w) == AVBD_SHAPE_BOX) {
+                                    const float3 lm = q_rotate(q_conj(d.globalRec[3 * (size_t)g + 1]), m - po);
+                                    const float3 dq2 = mx3(abs3(lm) - xyz(r2) * 0.5f, s3(0.0f));
+                                    cand = len3(dq2) <= rT + P.collisionMargin + 0.05f;
+                                }
+                            }
                         }
                         uint32_t ballot = __ballot_sync(0xffffffffu, cand);
                         if (lane == 0) {
                             while (ballot && emitted < RT_MAX_PER_TRI) {
                                 const uint32_t j = __ffs(ballot) - 1;
                                 ballot &= ballot - 1;
-                                test_body(d.colOwner[d.globalIdx[gb + j]]);
+                                test_body(d.globalOwner[gb + j]);
                             }
                         }
                         emitted = __shfl_sync(0xffffffffu, emitted, 0);

@@ -38,6 +38,12 @@ struct DevPtrs {
     // box of their collider spheres (lo, hi) and of their bodies' bounding
     // spheres (lo, hi), this frame
     float4* globalChunk;
+    // per global collider g: its owner body (set at upload) and, rewritten
+    // by the chunk pass every frame, the owner's pose and shape in one place:
+    // [3g] position + bounding radius (shape.w), [3g+1] rotation,
+    // [3g+2] shape.xyz + AVBD_SHAPE_* kind (as float bits)
+    uint32_t* globalOwner;
+    float4* globalRec;
     uint2* bodyCellSlot;
     uint32_t *pairCount, *pairStart, *pairLaneCount;
     uint2* pairs;

@@ -568,6 +568,12 @@ struct avbd_solver {
         ok = ok && alloc(d.pairs, H.maxPairs, "pairs");
         ok = ok && alloc(d.colCenter, nc, "colliderCenter") && alloc(d.colMeta, nc, "colliderMeta");
         ok = ok && alloc(d.globalChunk, 4 * (size_t)std::max<uint32_t>(1, (P.numGlobals + 31) / 32), "globalChunkBoxes");
+        {
+            std::vector<uint32_t> owners(std::max<size_t>(1, H.globalIdx.size()), 0u);
+            for (size_t g = 0; g < H.globalIdx.size(); g++) owners[g] = H.colOwner[H.globalIdx[g]];
+            ok = ok && upload(d.globalOwner, owners, "globalOwner");
+            ok = ok && alloc(d.globalRec, 3 * (size_t)std::max<uint32_t>(1, P.numGlobals), "globalRecords");
+        }
         ok = ok && alloc(d.manifolds, H.maxPairs, "manifolds", true) && alloc(d.prevManifolds, H.maxPairs, "prevManifolds", true);
         ok = ok && alloc(d.mapKeyA, H.mapCapacity, "mapKeyA", true) && alloc(d.mapKeyB, H.mapCapacity, "mapKeyB", true);
         ok = ok && alloc(d.mapVal, H.mapCapacity, "mapVal", true);
