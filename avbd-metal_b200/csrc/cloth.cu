@@ -399,7 +399,10 @@ __global__ void k_dat_pair_totals(const Params P, const DevPtrs d, uint32_t owne
 // serial order and the warp pre-tests 32 globals at a time with the reach
 // test that opens the body test, so lane 0 visits only globals that can pass
 // it.  Otherwise one thread per triangle.
-template <bool EMIT, bool WARP>
+// This search runs once per frame: it counts each triangle's records and
+// keeps their (body, feature) in the triangle's RT_MAX_PER_TRI slots of
+// rtCand; k_rt_write writes the records at the scanned offsets.
+template <bool WARP>
 __global__ void __launch_bounds__(128, 6) k_rt_emit(const Params P, const DevPtrs d) {
     const uint32_t lane = WARP ? (threadIdx.x & 31u) : 0u;
     const uint32_t step = WARP ? (gridDim.x * blockDim.x) >> 5 : gridDim.x * blockDim.x;
@@ -413,7 +416,6 @@ __global__ void __launch_bounds__(128, 6) k_rt_emit(const Params P, const DevPtr
         float3 triN = cross(b - a, c - a);
         const float tnLen = len3(triN);
         uint32_t emitted = 0;
-        const uint32_t base = EMIT ? d.rtStart[gid] : 0u;
         if (!(tnLen < 1e-12f)) {
             triN = triN / tnLen;
             const float3 velT = (xyz(d.velLin[tid.x]) + xyz(d.velLin[tid.y]) + xyz(d.velLin[tid.z])) / 3.0f;
@@ -483,26 +485,7 @@ __global__ void __launch_bounds__(128, 6) k_rt_emit(const Params P, const DevPtr
                     if (mC > 0.0f) minMass = mn(minMass, mC);
                     if (minMass == FLT_BIG_) continue;
                     if (is_excluded()) return;
-                    if (EMIT) {
-                        const float side = dot(dv, triN) >= 0.0f ? 1.0f : -1.0f;
-                        const uint32_t keyA = (SC_RT << 28) | o;
-                        const uint32_t keyB = gid * 16u + fid[fi];
-                        const float proposed = dot(po - q, triN) >= 0.0f ? 1.0f : -1.0f;
-                        const bool interior = bary.x > 0.02f && bary.y > 0.02f && bary.z > 0.02f;
-                        const float sMem = interior ? soft_prev_side(P, d, keyA, keyB, proposed) : proposed;
-                        float3 n;
-                        float g;
-                        if (dist > 1e-7f && side == sMem) { n = dv / dist; g = dist; }
-                        else { n = triN * sMem; g = -dist; }
-                        const float fricT = (d.props[tid.x].w + d.props[tid.y].w + d.props[tid.z].w) / 3.0f;
-                        const float friction = sqrtf(mx(d.props[o].w * fricT, 0.0f));
-                        const bool roundA = sk != AVBD_SHAPE_BOX;
-                        const float3 anchor = roundA ? (fw[fi] - po) : q_rotate(q_conj(qo), fw[fi] - po);
-                        soft_write(P, d, base + emitted, make_uint4(o, tid.x, tid.y, tid.z),
-                                   make_float4(1.0f, -bary.x, -bary.y, -bary.z), n, friction, anchor,
-                                   g - hSum + P.elemMargin, hSum - P.elemMargin, soft_lambda_cap(P, minMass), minMass,
-                                   SC_RT, true, roundA, sMem < 0.0f, keyA, keyB);
-                    }
+                    d.rtCand[(size_t)gid * RT_MAX_PER_TRI + emitted] = make_uint2(o, fid[fi]);
                     emitted++;
                 }
             };
@@ -591,7 +574,79 @@ __global__ void __launch_bounds__(128, 6) k_rt_emit(const Params P, const DevPtr
                 }
             }
         }
-        if (!EMIT && lane == 0) d.rtCount[gid] = emitted;
+        if (lane == 0) d.rtCount[gid] = emitted;
+    }
+}
+
+// A record's feature point from its id (the ids k_rt_emit gives: box corners
+// 0-7, sphere centre 8, capsule axis spheres 9-11), by the expressions the
+// search evaluates, so the point is the same float.
+__device__ __forceinline__ void rt_feature(float4 sh, float3 po, float4 qo, uint32_t sk, uint32_t f, float3& w,
+                                           float& r) {
+    if (sk == AVBD_SHAPE_SPHERE) {
+        w = po; r = sh.x * 0.5f;
+    } else if (sk == AVBD_SHAPE_CAPSULE) {
+        const float half_ = sh.x * 0.5f;
+        const float3 ax = q_rotate(qo, mk3(0, 0, 1));
+        w = po + ax * (half_ * (float)((int)f - 10)); r = sh.y;
+    } else {
+        const float3 h3 = xyz(sh) * 0.5f;
+        const float3 local = mk3((f & 1) ? h3.x : -h3.x, (f & 2) ? h3.y : -h3.y, (f & 4) ? h3.z : -h3.z);
+        w = xform(po, qo, local); r = 0.0f;
+    }
+}
+
+// One thread per triangle writes the records k_rt_emit found, in its order,
+// from the triangle's scanned offset (25_cloth.metal:1080-1142 is the record).
+__global__ void __launch_bounds__(128) k_rt_write(const Params P, const DevPtrs d) {
+    for (uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x; gid < P.numTris; gid += gridDim.x * blockDim.x) {
+        const uint32_t count = d.rtCount[gid];
+        if (count == 0) continue;
+        const uint4 tid = d.tris[gid];
+        const float3 a = xyz(d.posLin[tid.x]), b = xyz(d.posLin[tid.y]), c = xyz(d.posLin[tid.z]);
+        const float rt_ = mx(fabsf(d.shape[tid.x].w), mx(fabsf(d.shape[tid.y].w), fabsf(d.shape[tid.z].w)));
+        float3 triN = cross(b - a, c - a);
+        triN = triN / len3(triN);
+        const uint32_t base = d.rtStart[gid];
+        for (uint32_t k = 0; k < count; k++) {
+            const uint2 cf = d.rtCand[(size_t)gid * RT_MAX_PER_TRI + k];
+            const uint32_t o = cf.x;
+            const float4 sh = d.shape[o];
+            const float4 po4 = d.posLin[o];
+            const float3 po = xyz(po4);
+            const float4 qo = d.posAng[o];
+            const uint32_t sk = d.bodyShape[o];
+            float3 w;
+            float fr;
+            rt_feature(sh, po, qo, sk, cf.y, w, fr);
+            float3 bary;
+            const float3 q = closest_pt_triangle(w, a, b, c, bary);
+            const float3 dv = w - q;
+            const float dist = len3(dv);
+            const float hSum = rt_ + fr;
+            float minMass = po4.w > 0.0f ? po4.w : FLT_BIG_;
+            const float mA = d.posLin[tid.x].w, mB = d.posLin[tid.y].w, mC = d.posLin[tid.z].w;
+            if (mA > 0.0f) minMass = mn(minMass, mA);
+            if (mB > 0.0f) minMass = mn(minMass, mB);
+            if (mC > 0.0f) minMass = mn(minMass, mC);
+            const float side = dot(dv, triN) >= 0.0f ? 1.0f : -1.0f;
+            const uint32_t keyA = (SC_RT << 28) | o;
+            const uint32_t keyB = gid * 16u + cf.y;
+            const float proposed = dot(po - q, triN) >= 0.0f ? 1.0f : -1.0f;
+            const bool interior = bary.x > 0.02f && bary.y > 0.02f && bary.z > 0.02f;
+            const float sMem = interior ? soft_prev_side(P, d, keyA, keyB, proposed) : proposed;
+            float3 n;
+            float g;
+            if (dist > 1e-7f && side == sMem) { n = dv / dist; g = dist; }
+            else { n = triN * sMem; g = -dist; }
+            const float fricT = (d.props[tid.x].w + d.props[tid.y].w + d.props[tid.z].w) / 3.0f;
+            const float friction = sqrtf(mx(d.props[o].w * fricT, 0.0f));
+            const bool roundA = sk != AVBD_SHAPE_BOX;
+            const float3 anchor = roundA ? (w - po) : q_rotate(q_conj(qo), w - po);
+            soft_write(P, d, base + k, make_uint4(o, tid.x, tid.y, tid.z), make_float4(1.0f, -bary.x, -bary.y, -bary.z),
+                       n, friction, anchor, g - hSum + P.elemMargin, hSum - P.elemMargin, soft_lambda_cap(P, minMass),
+                       minMass, SC_RT, true, roundA, sMem < 0.0f, keyA, keyB);
+        }
     }
 }
 
@@ -1096,11 +1151,10 @@ void build_pairs(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t
 void launch_rt_emit(const Params& P, const DevPtrs& d, const Sizes& z, cudaStream_t st) {
     if (z.numTris == 0) return;
     const bool warp = P.numGlobals > 32;
-    if (warp) k_rt_emit<false, true><<<blocks_for(z.numTris * 32u, 128), 128, 0, st>>>(P, d);
-    else k_rt_emit<false, false><<<blocks_for(z.numTris, 128), 128, 0, st>>>(P, d);
+    if (warp) k_rt_emit<true><<<blocks_for(z.numTris * 32u, 128), 128, 0, st>>>(P, d);
+    else k_rt_emit<false><<<blocks_for(z.numTris, 128), 128, 0, st>>>(P, d);
     launch_exclusive_scan_large(d.rtCount, d.rtStart, z.numTris, d.bigScanScratch, st);
-    if (warp) k_rt_emit<true, true><<<blocks_for(z.numTris * 32u, 128), 128, 0, st>>>(P, d);
-    else k_rt_emit<true, false><<<blocks_for(z.numTris, 128), 128, 0, st>>>(P, d);
+    k_rt_write<<<blocks_for(z.numTris, 128), 128, 0, st>>>(P, d);
     k_rt_totals<<<1, 32, 0, st>>>(P, d);
 }
 

@@ -100,6 +100,7 @@ struct DevPtrs {
     uint4* datPairs;                            // (kind, owner, other, flags)
     uint2* datCache;                            // first pairs of each owner from the counting pass (other, flags)
     uint32_t *rtCount, *rtStart;                // rigid-triangle records per triangle
+    uint2* rtCand;                              // (body, feature) of each record, RT_MAX_PER_TRI per triangle
     uint32_t *datEmit, *datEmitStart;           // element contacts per query owner
     SoftContactGPU *soft, *prevSoft;
     uint32_t *softKeyA, *softKeyB, *softVal;

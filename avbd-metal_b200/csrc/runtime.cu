@@ -700,6 +700,7 @@ struct avbd_solver {
             ok = ok && alloc(d.datOwnerCount, owners, "datOwnerCount") && alloc(d.datOwnerStart, owners, "datOwnerStart");
             ok = ok && alloc(d.datEmit, owners, "datEmit") && alloc(d.datEmitStart, owners, "datEmitStart");
             ok = ok && alloc(d.rtCount, H.numTris, "rtCount") && alloc(d.rtStart, H.numTris, "rtStart");
+            ok = ok && alloc(d.rtCand, RT_MAX_PER_TRI * (size_t)H.numTris, "rtCandidates");
             ok = ok && alloc(d.soft, P.maxSoft, "softContacts", true) && alloc(d.prevSoft, P.maxSoft, "prevSoftContacts", true);
             ok = ok && alloc(d.softKeyA, P.softMapCapacity, "softMapKeyA", true);
             ok = ok && alloc(d.softKeyB, P.softMapCapacity, "softMapKeyB", true) &&
