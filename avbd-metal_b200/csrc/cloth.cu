@@ -395,8 +395,8 @@ __global__ void k_dat_pair_totals(const Params P, const DevPtrs d, uint32_t owne
 // triangle, at most four records.  Bodies are reached through their
 // collider's owner; the grid sweep visits each distinct bucket once.
 // ---------------------------------------------------------------------------
-// WARP (many global colliders): one warp per triangle, lane 0 emits in the
-// serial order and the warp pre-tests 32 globals at a time with the reach
+// WARP (many global colliders): one warp per triangle, lane 0 takes the
+// candidates in the serial order and the warp pre-tests 32 globals at a time with the reach
 // test that opens the body test, so lane 0 visits only globals that can pass
 // it.  Otherwise one thread per triangle.
 // This search runs once per frame: it counts each triangle's records and
